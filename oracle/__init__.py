@@ -1,0 +1,218 @@
+"""CPU oracle for the render hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl
+reference legs may import this package, and only as the checker or the CPU
+baseline.  The product package (vkpathtracer_b200) never imports it.
+
+Two interchangeable implementations of oracle/vkpt_oracle.h:
+  "reference"  oracle/_ref/libvkptref.so   -- the reference's own CPU tracer,
+               compiled from its unmodified sources by oracle/Makefile.
+  "port"       oracle/_build/libvkptport.so -- restatement (oracle/port.cpp),
+               pinned bit-for-bit to "reference" by tests/test_oracle_pin.py.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libvkptref.so")
+PORT_LIB = os.path.join(HERE, "_build", "libvkptport.so")
+REFERENCE_SRC = "/root/reference/src"
+
+
+class VkoScene(ctypes.Structure):
+    _fields_ = [
+        ("vertices", ctypes.c_void_p), ("vertex_count", ctypes.c_uint32),
+        ("indices", ctypes.c_void_p), ("index_count", ctypes.c_uint32),
+        ("instances", ctypes.c_void_p), ("instance_count", ctypes.c_uint32),
+        ("materials", ctypes.c_void_p), ("material_count", ctypes.c_uint32),
+        ("lights", ctypes.c_void_p), ("light_count", ctypes.c_uint32),
+        ("environment", ctypes.c_float * 3),
+        ("camera_position", ctypes.c_float * 3),
+        ("camera_target", ctypes.c_float * 3),
+        ("camera_up", ctypes.c_float * 3),
+        ("camera_fov_deg", ctypes.c_float),
+        ("camera_aperture_radius", ctypes.c_float),
+        ("camera_focus_distance", ctypes.c_float),
+    ]
+
+
+class VkoSettings(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+        ("enable_nee", ctypes.c_uint32), ("enable_mis", ctypes.c_uint32), ("rr_start", ctypes.c_uint32),
+        ("rr_min", ctypes.c_float), ("rr_max", ctypes.c_float), ("seed", ctypes.c_uint64),
+        ("firefly_clamp", ctypes.c_float), ("_pad", ctypes.c_uint32),
+    ]
+
+
+class VkoCounters(ctypes.Structure):
+    _fields_ = [
+        ("samples", ctypes.c_uint64), ("rays", ctypes.c_uint64), ("triangle_tests", ctypes.c_uint64),
+        ("triangle_hits", ctypes.c_uint64), ("bvh_node_visits", ctypes.c_uint64),
+        ("bvh_leaf_visits", ctypes.c_uint64), ("shadow_tests", ctypes.c_uint64),
+        ("render_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def build_port(quiet: bool = True) -> str:
+    """Compile the restatement with g++ (no reference sources needed)."""
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    src = os.path.join(HERE, "port.cpp")
+    if (not os.path.exists(PORT_LIB)) or os.path.getmtime(PORT_LIB) < max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "vkpt_oracle.h"))):
+        cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-o", PORT_LIB, src, "-lpthread"]
+        subprocess.run(cmd, check=True, capture_output=quiet)
+    return PORT_LIB
+
+
+def build_ref(quiet: bool = True) -> Optional[str]:
+    """Compile the reference oracle where the reference sources exist; else None."""
+    if not os.path.isdir(REFERENCE_SRC):
+        return REF_LIB if os.path.exists(REF_LIB) else None
+    subprocess.run(["make", "-C", HERE, "ref", f"REF={REFERENCE_SRC}", "-j8"], check=True,
+                   capture_output=quiet)
+    return REF_LIB
+
+
+class Oracle:
+    def __init__(self, path: str):
+        self.path = path
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.vko_render.restype = ctypes.c_int
+        L.vko_render.argtypes = [ctypes.POINTER(VkoScene), ctypes.POINTER(VkoSettings), ctypes.c_uint32,
+                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 ctypes.POINTER(VkoCounters)]
+        L.vko_build_bvh.restype = ctypes.c_int
+        L.vko_build_bvh.argtypes = [ctypes.POINTER(VkoScene), ctypes.c_uint32, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p]
+        L.vko_intersect.restype = ctypes.c_int
+        L.vko_intersect.argtypes = [ctypes.POINTER(VkoScene), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.POINTER(ctypes.c_double)]
+        L.vko_last_error.restype = ctypes.c_char_p
+        L.vko_impl_name.restype = ctypes.c_char_p
+        self.kind = L.vko_impl_name().decode()
+
+    # -- helpers
+    @staticmethod
+    def make_scene(scene):
+        keep = (scene.vertices, scene.indices, scene.instances, scene.materials, scene.lights)
+        s = VkoScene()
+        s.vertices, s.vertex_count = _ptr(scene.vertices), scene.vertices.shape[0]
+        s.indices, s.index_count = _ptr(scene.indices), scene.indices.size
+        s.instances, s.instance_count = _ptr(scene.instances), scene.instances.shape[0]
+        s.materials, s.material_count = _ptr(scene.materials), scene.materials.shape[0]
+        s.lights, s.light_count = (_ptr(scene.lights) if scene.lights.size else None), scene.lights.shape[0]
+        s.environment[:] = scene.environment
+        c = scene.camera
+        s.camera_position[:] = c.position
+        s.camera_target[:] = c.target
+        s.camera_up[:] = c.up
+        s.camera_fov_deg = c.fov_deg
+        s.camera_aperture_radius = c.aperture_radius
+        s.camera_focus_distance = c.focus_distance
+        return s, keep
+
+    @staticmethod
+    def make_settings(st):
+        s = VkoSettings()
+        s.width, s.height, s.max_depth = st.width, st.height, st.max_depth
+        s.enable_nee, s.enable_mis = int(st.enable_nee), int(st.enable_mis)
+        s.rr_start = st.russian_roulette_start_depth
+        s.rr_min, s.rr_max = st.russian_roulette_min_survival, st.russian_roulette_max_survival
+        s.seed = st.seed
+        s.firefly_clamp = st.firefly_clamp
+        return s
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise RuntimeError(f"oracle ({self.kind}) failed: {self.lib.vko_last_error().decode()}")
+
+    # -- API
+    def render(self, scene, settings, first_sample: int = 0, n_samples: Optional[int] = None,
+               threads: int = 1, pixels: Optional[np.ndarray] = None, per_sample: bool = False):
+        """Returns dict(sum=(H,W,3), count=(H,W), invalid=(H,W), samples=(n,H,W,3)|None, counters)."""
+        n = settings.spp if n_samples is None else n_samples
+        W, H = settings.width, settings.height
+        sc, keep = self.make_scene(scene)
+        st = self.make_settings(settings)
+        film = np.zeros((H, W, 3), np.float32)
+        count = np.zeros((H, W), np.uint32)
+        invalid = np.zeros((H, W), np.float32)
+        samples = np.zeros((n, H, W, 3), np.float32) if per_sample else None
+        px = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint32)
+        ctr = VkoCounters()
+        rc = self.lib.vko_render(ctypes.byref(sc), ctypes.byref(st), first_sample, n, threads,
+                                 _ptr(px), 0 if px is None else px.size, _ptr(film), _ptr(count),
+                                 _ptr(invalid), _ptr(samples), ctypes.byref(ctr))
+        del keep
+        self._check(rc)
+        return {"sum": film, "count": count, "invalid": invalid, "samples": samples,
+                "counters": ctr.as_dict()}
+
+    def build_bvh(self, scene, leaf_threshold: int = 4, deterministic: bool = True):
+        sc, keep = self.make_scene(scene)
+        n = scene.triangle_count
+        nodes = np.zeros((max(1, 2 * n - 1), 10), np.uint32)
+        prim = np.zeros(max(1, n), np.uint32)
+        cnt = ctypes.c_uint32(0)
+        rc = self.lib.vko_build_bvh(ctypes.byref(sc), leaf_threshold, int(deterministic), _ptr(nodes),
+                                    ctypes.byref(cnt), _ptr(prim))
+        del keep
+        self._check(rc)
+        return nodes[:cnt.value].copy(), prim[:n].copy()
+
+    def intersect(self, scene, rays: np.ndarray, threads: int = 1, stats: bool = False):
+        """Closest-hit: returns (prim uint32 [0xFFFFFFFF = miss], t float32, stats|None, ms)."""
+        sc, keep = self.make_scene(scene)
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        prim = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float32)
+        st = np.zeros(4, np.uint64) if stats else None
+        ms = ctypes.c_double(0.0)
+        rc = self.lib.vko_intersect(ctypes.byref(sc), _ptr(rays), n, threads, _ptr(prim), _ptr(t), _ptr(st),
+                                    ctypes.byref(ms))
+        del keep
+        self._check(rc)
+        return prim, t, st, ms.value
+
+
+_CACHE = {}
+
+
+def load(kind: str = "auto") -> Oracle:
+    """kind: "reference", "port" or "auto" (reference when built, else port)."""
+    if kind == "auto":
+        kind = "reference" if os.path.exists(REF_LIB) else "port"
+    if kind in _CACHE:
+        return _CACHE[kind]
+    if kind == "reference":
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError("reference oracle not built (oracle/_ref/libvkptref.so)")
+        o = Oracle(REF_LIB)
+    elif kind == "port":
+        o = Oracle(build_port())
+    else:
+        raise ValueError(kind)
+    _CACHE[kind] = o
+    return o
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_LIB)

@@ -1,0 +1,819 @@
+// port.cpp -- TEST INFRASTRUCTURE: CPU restatement of the reference's render hot path.
+//
+// A line-by-line restatement (own code, same floating-point operation order)
+// of the reference's scalar CPU tracer, used as the checker wherever the
+// reference sources are not available (the GPU box).  It is pinned
+// bit-for-bit against the reference itself (oracle/_ref/libvkptref.so) by
+// tests/test_oracle_pin.py: identical films, counters, BVH nodes and hit ids.
+// The product library never links this file.
+//
+// Followed, function by function (paths within the reference project):
+//   splitmix64, Rng                 src/pathtracer/ScalarCpuPathTracer.cpp:36-41, 383-393
+//   compute_camera_basis            src/pathtracer/ScalarCpuPathTracer.cpp:139-152
+//   camera_rays                     src/pathtracer/ScalarCpuPathTracer.Render.cpp:55-119
+//   shade_pixel                     src/pathtracer/ScalarCpuPathTracer.Render.cpp:228-284
+//   trace                           src/pathtracer/ScalarCpuPathTracer.cpp:1148-1289
+//   sample_direct_light             src/pathtracer/ScalarCpuPathTracer.cpp:1022-1118
+//   light_pdf_for_direction, Mis    src/pathtracer/ScalarCpuPathTracer.cpp:1120-1146
+//   sample_hemisphere / phong lobe  src/pathtracer/ScalarCpuPathTracer.cpp:978-1020
+//   apply_material_effect (0 only)  src/pathtracer/ScalarCpuPathTracer.cpp:264-355
+//   schlick_fresnel, refract_dir    src/pathtracer/ScalarCpuPathTracer.cpp:357-377
+//   accelerator build / intersect   src/pathtracer/CpuBvhAccelerator.cpp:84-154, 161-263, 360-477
+//   midpoint BVH builder            src/cpu/ParallelBvhBuilder.cpp:13-257
+//   leaf triangle batch             src/cpu/BvhTriangleIntersector.cpp:25-74, 186-209
+//   FilmBuffer::add_sample          src/pathtracer/FilmBuffer.cpp:80-91
+
+#include "vkpt_oracle.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+int fail(const std::string& m) { g_error = m; return 1; }
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kInvPi = 0.31830988618f;
+constexpr float kEps = 1e-4f;
+
+struct V3 { float x, y, z; };
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 neg(V3 a) { return {-a.x, -a.y, -a.z}; }
+inline V3 mul(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 mulv(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline V3 divs(V3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float fmax_std(float a, float b) { return (a < b) ? b : a; }   // std::max
+inline float fmin_std(float a, float b) { return (b < a) ? b : a; }   // std::min
+inline float clampf(float v, float lo, float hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); }
+// normalize(): division by the length, (0,1,0) below 1e-4.
+inline V3 unit(V3 v) {
+  const float l = std::sqrt(dot(v, v));
+  if (l <= kEps) return {0.0f, 1.0f, 0.0f};
+  return divs(v, l);
+}
+inline float clamp01(float v) {
+  if (!std::isfinite(v)) return 0.0f;
+  return fmin_std(1.0f, fmax_std(0.0f, v));
+}
+inline float pow5(float v) { const float v2 = v * v; return v2 * v2 * v; }
+inline V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+
+uint64_t mix64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ULL;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+  return x ^ (x >> 31);
+}
+
+struct Stream {
+  uint64_t s;
+  // key order: seed, frame, sample, path_id, dimension, depth, pixel
+  Stream(uint64_t seed, uint64_t frame, uint64_t sample, uint64_t path_id, uint64_t dim, uint64_t depth,
+         uint64_t pixel) {
+    const uint64_t m = mix64(seed ^ mix64(frame) ^ mix64(sample) ^ mix64(path_id) ^ mix64(dim) ^ mix64(depth));
+    s = mix64(m + mix64(pixel));
+  }
+  float u() {
+    s = mix64(s);
+    return static_cast<float>((s >> 8) & 0x00ffffffu) * (1.0f / 16777215.0f);
+  }
+};
+
+struct Material {
+  V3 albedo, emissive;
+  float roughness, metallic, ior, transmission, clearcoat, sheen, alpha;
+  uint32_t model, effect;
+  bool emissive_any() const { return emissive.x > 0.0f || emissive.y > 0.0f || emissive.z > 0.0f; }
+};
+
+struct Light {
+  V3 pos, color, dir;
+  float intensity, radius, inner, outer;
+};
+
+struct Prim {
+  uint32_t material, index;
+  V3 v0, e1, e2, n;
+};
+
+struct Box { float lo[3], hi[3]; };
+struct Node { Box box; int32_t left, right, first, count; };
+
+struct Stats { uint64_t tri_tests = 0, tri_hits = 0, nodes = 0, leaves = 0, shadow = 0; };
+
+// ----------------------------------------------------------------- BVH build
+struct Builder {
+  const std::vector<Box>* boxes;
+  std::vector<Node>* nodes;
+  std::vector<uint32_t>* order;
+  int32_t next = 1;
+  bool stable = true;
+  size_t leaf = 4;
+
+  static float centroid(const Box& b, int ax) { return 0.5f * (b.lo[ax] + b.hi[ax]); }
+
+  void build(int32_t id, uint32_t* idx, size_t n) {
+    Box bb;
+    Box cb;
+    for (int a = 0; a < 3; ++a) {
+      bb.lo[a] = cb.lo[a] = std::numeric_limits<float>::max();
+      bb.hi[a] = cb.hi[a] = -std::numeric_limits<float>::max();
+    }
+    for (size_t i = 0; i < n; ++i) {
+      const Box& p = (*boxes)[idx[i]];
+      for (int a = 0; a < 3; ++a) {
+        bb.lo[a] = fmin_std(bb.lo[a], p.lo[a]);
+        bb.hi[a] = fmax_std(bb.hi[a], p.hi[a]);
+      }
+    }
+    (*nodes)[id].box = bb;
+    if (n <= leaf) {
+      Node& nd = (*nodes)[id];
+      nd.left = nd.right = -1;
+      nd.first = static_cast<int32_t>(idx - order->data());
+      nd.count = static_cast<int32_t>(n);
+      return;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      const Box& p = (*boxes)[idx[i]];
+      for (int a = 0; a < 3; ++a) {
+        const float c = centroid(p, a);
+        cb.lo[a] = fmin_std(cb.lo[a], c);
+        cb.hi[a] = fmax_std(cb.hi[a], c);
+      }
+    }
+    int axis = 0;
+    float ext = cb.hi[0] - cb.lo[0];
+    for (int a = 1; a < 3; ++a) {
+      const float e = cb.hi[a] - cb.lo[a];
+      if (e > ext) { ext = e; axis = a; }
+    }
+    const float split = 0.5f * (cb.lo[axis] + cb.hi[axis]);
+    auto pred = [&](uint32_t k) { return centroid((*boxes)[k], axis) < split; };
+    uint32_t* mid = stable ? std::stable_partition(idx, idx + n, pred) : std::partition(idx, idx + n, pred);
+    size_t nl = static_cast<size_t>(mid - idx);
+    if (nl == 0 || nl == n) nl = n / 2;
+    const int32_t l = next++;
+    const int32_t r = next++;
+    Node& nd = (*nodes)[id];
+    nd.left = l;
+    nd.right = r;
+    nd.first = -1;
+    nd.count = 0;
+    build(l, idx, nl);
+    build(r, idx + nl, n - nl);
+  }
+};
+
+// --------------------------------------------------------------- the scene
+struct World {
+  std::vector<Prim> prims;
+  std::vector<Box> boxes;
+  std::vector<Node> nodes;
+  std::vector<uint32_t> order;
+  std::vector<Material> mats;
+  std::vector<Light> lights;
+  V3 env{};
+  V3 cam_pos{}, cam_fwd{}, cam_right{}, cam_up{};
+  float fov = 60.0f;
+  float aperture = 0.0f, focus = 0.0f;
+
+  void load(const vko_scene& s, bool stable = true, size_t leaf = 4) {
+    for (uint32_t i = 0; i < s.instance_count; ++i) {
+      const uint32_t first = s.instances[3 * i], count = s.instances[3 * i + 1], mat = s.instances[3 * i + 2];
+      for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t base = (first + k) * 3u;
+        if (base + 2u >= s.index_count) continue;
+        const uint32_t a = s.indices[base], b = s.indices[base + 1], c = s.indices[base + 2];
+        if (a >= s.vertex_count || b >= s.vertex_count || c >= s.vertex_count) continue;
+        const V3 v0 = ld3(s.vertices + 3 * a), v1 = ld3(s.vertices + 3 * b), v2 = ld3(s.vertices + 3 * c);
+        Box bx;
+        bx.lo[0] = std::min({v0.x, v1.x, v2.x}) - kEps;
+        bx.lo[1] = std::min({v0.y, v1.y, v2.y}) - kEps;
+        bx.lo[2] = std::min({v0.z, v1.z, v2.z}) - kEps;
+        bx.hi[0] = std::max({v0.x, v1.x, v2.x}) + kEps;
+        bx.hi[1] = std::max({v0.y, v1.y, v2.y}) + kEps;
+        bx.hi[2] = std::max({v0.z, v1.z, v2.z}) + kEps;
+        Prim p;
+        p.material = mat;
+        p.index = static_cast<uint32_t>(prims.size());
+        p.v0 = v0;
+        p.e1 = sub(v1, v0);
+        p.e2 = sub(v2, v0);
+        // normalize_vec3 of the accelerator: multiply by 1/sqrt(len^2).
+        const V3 cr = cross(p.e1, p.e2);
+        const float l2 = dot(cr, cr);
+        p.n = (l2 <= kEps * kEps) ? V3{0.0f, 1.0f, 0.0f} : mul(cr, 1.0f / std::sqrt(l2));
+        prims.push_back(p);
+        boxes.push_back(bx);
+      }
+    }
+    if (!prims.empty()) {
+      nodes.assign(2 * prims.size() - 1, Node{});
+      order.resize(prims.size());
+      std::iota(order.begin(), order.end(), 0u);
+      Builder b{&boxes, &nodes, &order, 1, stable, leaf};
+      b.build(0, order.data(), order.size());
+      nodes.resize(static_cast<size_t>(b.next));
+    }
+    for (uint32_t i = 0; i < s.material_count; ++i) {
+      const float* m = s.materials + 16 * i;
+      Material q;
+      q.albedo = ld3(m);
+      q.emissive = ld3(m + 3);
+      q.roughness = m[6];
+      q.model = static_cast<uint32_t>(m[7] + 0.5f);
+      q.metallic = m[8];
+      q.ior = m[9];
+      q.transmission = m[10];
+      q.clearcoat = m[11];
+      q.sheen = m[12];
+      q.alpha = m[14];
+      q.effect = static_cast<uint32_t>(m[15] + 0.5f) & 1023u;
+      mats.push_back(q);
+    }
+    if (mats.empty()) {
+      Material q{};
+      q.albedo = {1.0f, 1.0f, 1.0f};
+      q.emissive = {0.0f, 0.0f, 0.0f};
+      q.roughness = 1.0f;
+      q.ior = 1.5f;
+      q.alpha = 1.0f;
+      mats.push_back(q);
+    }
+    for (uint32_t i = 0; i < s.light_count; ++i) {
+      const float* l = s.lights + 16 * i;
+      lights.push_back(Light{ld3(l), ld3(l + 3), ld3(l + 8), l[6], l[7], l[11], l[12]});
+    }
+    env = ld3(s.environment);
+    cam_pos = ld3(s.camera_position);
+    fov = s.camera_fov_deg;
+    aperture = s.camera_aperture_radius;
+    focus = s.camera_focus_distance;
+    // camera basis
+    cam_fwd = unit(sub(ld3(s.camera_target), cam_pos));
+    cam_right = unit(cross(cam_fwd, ld3(s.camera_up)));
+    if (dot(cam_right, cam_right) <= kEps * kEps) cam_right = {1.0f, 0.0f, 0.0f};
+    cam_up = unit(cross(cam_right, cam_fwd));
+    if (dot(cam_up, cam_up) <= kEps * kEps) cam_up = {0.0f, 1.0f, 0.0f};
+  }
+
+  // Slab test with per-axis early exit; axes with |d| <= 1e-4 use an inside test.
+  struct RayBox { float o[3], inv[3]; bool par[3]; };
+  static RayBox prep(V3 o, V3 d) {
+    RayBox r;
+    const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+    for (int a = 0; a < 3; ++a) {
+      r.o[a] = oo[a];
+      r.par[a] = std::fabs(dd[a]) <= kEps;
+      r.inv[a] = r.par[a] ? 0.0f : 1.0f / dd[a];
+    }
+    return r;
+  }
+  static bool slab(const Box& b, const RayBox& r, float tmax_in, float& tnear) {
+    float lo = kEps, hi = tmax_in;
+    for (int a = 0; a < 3; ++a) {
+      if (r.par[a]) {
+        if (r.o[a] < b.lo[a] || r.o[a] > b.hi[a]) return false;
+        continue;
+      }
+      float t0 = (b.lo[a] - r.o[a]) * r.inv[a];
+      float t1 = (b.hi[a] - r.o[a]) * r.inv[a];
+      if (t0 > t1) std::swap(t0, t1);
+      lo = fmax_std(lo, t0);
+      hi = fmin_std(hi, t1);
+      if (lo > hi) return false;
+    }
+    tnear = lo;
+    return hi > kEps;
+  }
+
+  // Closest hit: returns prim slot or -1, with t.
+  int64_t closest(V3 o, V3 d, float& t_out, Stats& st) const {
+    if (nodes.empty() || prims.empty()) return -1;
+    float best = std::numeric_limits<float>::infinity();
+    int64_t hit = -1;
+    const RayBox rb = prep(o, d);
+    std::vector<int32_t> stack;
+    stack.reserve(128);
+    stack.push_back(0);
+    while (!stack.empty()) {
+      const int32_t id = stack.back();
+      stack.pop_back();
+      if (id < 0 || static_cast<size_t>(id) >= nodes.size()) continue;
+      const Node& nd = nodes[static_cast<size_t>(id)];
+      ++st.nodes;
+      float tn = 0.0f;
+      if (!slab(nd.box, rb, best, tn)) continue;
+      if (nd.count > 0) {
+        ++st.leaves;
+        // Leaf batches of up to 8 lanes; a lane commits only when 1e-4 < t < best.
+        st.tri_tests += static_cast<uint64_t>(nd.count);
+        if (!(best > kEps)) continue;
+        for (int32_t i = 0; i < nd.count; ++i) {
+          const uint32_t pi = order[static_cast<size_t>(nd.first + i)];
+          const Prim& p = prims[pi];
+          const float hx = d.y * p.e2.z - d.z * p.e2.y;
+          const float hy = d.z * p.e2.x - d.x * p.e2.z;
+          const float hz = d.x * p.e2.y - d.y * p.e2.x;
+          const float det = p.e1.x * hx + p.e1.y * hy + p.e1.z * hz;
+          if (std::fabs(det) < kEps) continue;
+          const float inv = 1.0f / det;
+          const float sx = o.x - p.v0.x, sy = o.y - p.v0.y, sz = o.z - p.v0.z;
+          const float u = (sx * hx + sy * hy + sz * hz) * inv;
+          if (u < 0.0f || u > 1.0f) continue;
+          const float qx = sy * p.e1.z - sz * p.e1.y;
+          const float qy = sz * p.e1.x - sx * p.e1.z;
+          const float qz = sx * p.e1.y - sy * p.e1.x;
+          const float v = (d.x * qx + d.y * qy + d.z * qz) * inv;
+          if (v < 0.0f || u + v > 1.0f) continue;
+          const float t = (p.e2.x * qx + p.e2.y * qy + p.e2.z * qz) * inv;
+          if (t <= kEps || t >= best) continue;
+          ++st.tri_hits;
+          best = t;
+          hit = pi;
+        }
+        continue;
+      }
+      float tl = 0.0f, tr = 0.0f;
+      const bool hl = nd.left >= 0 && slab(nodes[static_cast<size_t>(nd.left)].box, rb, best, tl);
+      const bool hr = nd.right >= 0 && slab(nodes[static_cast<size_t>(nd.right)].box, rb, best, tr);
+      if (hl && hr) {
+        if (tl <= tr) { stack.push_back(nd.right); stack.push_back(nd.left); }
+        else { stack.push_back(nd.left); stack.push_back(nd.right); }
+      } else if (hl) {
+        stack.push_back(nd.left);
+      } else if (hr) {
+        stack.push_back(nd.right);
+      }
+    }
+    t_out = best;
+    return hit;
+  }
+
+  struct Hit { bool hit; float t; V3 p, n; uint32_t mat; };
+
+  bool intersect(V3 o, V3 d, Hit& h, Stats& st) const {
+    h = Hit{false, 0.0f, {}, {}, 0};
+    float t = 0.0f;
+    const int64_t k = closest(o, d, t, st);
+    if (k < 0) return false;
+    const Prim& p = prims[static_cast<size_t>(k)];
+    h.hit = true;
+    h.t = t;
+    h.p = add(o, mul(d, t));
+    h.n = p.n;
+    h.mat = p.material;
+    return true;
+  }
+
+  const Material& mat(uint32_t i) const { return mats[std::min<size_t>(i, mats.size() - 1)]; }
+};
+
+// ---------------------------------------------------------------- integrator
+struct Integrator {
+  const World& w;
+  const vko_settings& cfg;
+
+  V3 albedo_of(const Material& m) const {
+    // Effect 0 (the only one these scenes use): albedo clamped to [0, 1.5].
+    const V3 c = m.albedo;
+    return {fmin_std(1.5f, fmax_std(0.0f, c.x)), fmin_std(1.5f, fmax_std(0.0f, c.y)),
+            fmin_std(1.5f, fmax_std(0.0f, c.z))};
+  }
+
+  V3 hemisphere(Stream& rng, V3 n) const {
+    const float u1 = rng.u();
+    const float u2 = rng.u();
+    const float r = std::sqrt(fmax_std(0.0f, 1.0f - u1));
+    const float phi = 2.0f * kPi * u2;
+    const V3 loc{r * std::cos(phi), r * std::sin(phi), std::sqrt(fmax_std(0.0f, u1))};
+    V3 t = cross((std::fabs(n.z) < 0.999f) ? V3{0.0f, 0.0f, 1.0f} : V3{0.0f, 1.0f, 0.0f}, n);
+    t = unit(t);
+    const V3 b = cross(n, t);
+    return unit(add(add(mul(t, loc.x), mul(b, loc.y)), mul(n, loc.z)));
+  }
+
+  V3 phong(Stream& rng, V3 refl, float expo, V3 n) const {
+    const float u1 = rng.u();
+    const float u2 = rng.u();
+    const float ct = std::pow(fmax_std(0.0f, u1), 1.0f / (expo + 1.0f));
+    const float sn = std::sqrt(fmax_std(0.0f, 1.0f - ct * ct));
+    const float phi = 2.0f * kPi * u2;
+    const V3 ref = (std::fabs(refl.z) < 0.999f) ? V3{0.0f, 0.0f, 1.0f} : V3{0.0f, 1.0f, 0.0f};
+    const V3 t = unit(cross(ref, refl));
+    const V3 b = cross(refl, t);
+    V3 out = unit(add(add(mul(t, sn * std::cos(phi)), mul(b, sn * std::sin(phi))), mul(refl, ct)));
+    if (dot(out, n) <= 0.0f) {
+      out = sub(out, mul(n, 2.0f * dot(out, n)));
+      if (dot(out, n) <= 0.0f) return hemisphere(rng, n);
+    }
+    return out;
+  }
+
+  static float spot(const Light& l, V3 from_light) {
+    if (l.inner <= -0.999f) return 1.0f;
+    const float cone = dot(unit(from_light), unit(l.dir));
+    if (cone <= l.outer) return 0.0f;
+    if (cone >= l.inner || l.inner <= l.outer) return 1.0f;
+    const float t = clampf((cone - l.outer) / (l.inner - l.outer), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+  }
+
+  // NEE toward one uniformly picked light; returns false when no contribution.
+  bool direct(const World::Hit& h, V3 view, Stream& rng, V3& out, Stats& st) const {
+    if (w.lights.empty()) return false;
+    const size_t nl = w.lights.size();
+    const size_t pick = std::min(static_cast<size_t>(rng.u() * static_cast<float>(nl)), nl - 1u);
+    const Light& L = w.lights[pick];
+    V3 lp = L.pos;
+    if (L.radius > 1.0e-5f) {
+      const float uz = 1.0f - 2.0f * rng.u();
+      const float r = std::sqrt(fmax_std(0.0f, 1.0f - uz * uz));
+      const float phi = 6.28318530718f * rng.u();
+      lp = add(lp, mul(V3{r * std::cos(phi), uz, r * std::sin(phi)}, L.radius));
+    }
+    const V3 tl = sub(lp, h.p);
+    const float d2 = dot(tl, tl);
+    const float dist = std::sqrt(d2);
+    if (dist < kEps) return false;
+    const V3 ldir = divs(tl, dist);
+    const float cth = dot(h.n, ldir);
+    if (cth <= 0.0f) return false;
+    const float sf = spot(L, neg(ldir));
+    if (sf <= 0.0f) return false;
+    const Material& m = w.mat(h.mat);
+    const float rough = clamp01(m.roughness);
+    const bool mirror = m.model == 2u || rough <= 0.001f;
+    const bool metal = m.model == 4u || m.metallic > 0.65f;
+    const bool trans = m.model == 5u || m.transmission > 0.05f;
+    const bool coat = m.model == 7u || m.clearcoat > 0.05f;
+    ++st.shadow;
+    V3 so = add(h.p, mul(h.n, 0.002f));
+    float remain = dist - 0.004f;
+    for (uint32_t skips = 0; skips < 8u && remain > 0.004f; ++skips) {
+      World::Hit sh;
+      if (!w.intersect(so, ldir, sh, st) || sh.t >= remain) break;
+      const Material& sm = w.mat(sh.mat);
+      if (!(sm.model == 5u || sm.transmission > 0.05f)) return false;
+      const float adv = sh.t + 0.004f;
+      so = add(so, mul(ldir, adv));
+      remain -= adv;
+    }
+    const V3 alb = albedo_of(m);
+    const V3 irr = mul(L.color, (L.intensity * sf) / (d2 + kEps));
+    V3 acc{0.0f, 0.0f, 0.0f};
+    if (!mirror && !trans) {
+      acc = add(acc, mul(mul(mulv(mul(alb, kInvPi), irr), cth), static_cast<float>(nl)));
+    }
+    if (mirror || metal || coat || trans || rough < 0.65f) {
+      const V3 hv = unit(add(ldir, unit(view)));
+      const float er = fmax_std(0.025f, rough * (metal ? 0.65f : 1.0f));
+      const float a2 = er * er;
+      const float pw = clampf(2.0f / fmax_std(0.0005f, a2 * a2) - 2.0f, 4.0f, 96.0f);
+      const float spec = std::pow(fmax_std(0.0f, dot(h.n, hv)), pw);
+      const float cv = fmax_std(0.0f, dot(h.n, unit(view)));
+      float f0 = (1.0f - m.ior) / (1.0f + m.ior);
+      f0 *= f0;
+      const float fr = f0 + (1.0f - f0) * pow5(1.0f - cv);
+      const float ss = clamp01((1.0f - rough) * 0.8f + m.metallic * 0.45f + m.clearcoat * 0.35f +
+                               (mirror ? 0.75f : 0.0f) + (trans ? fr : 0.0f));
+      const V3 tint = add(mul(V3{1.0f, 1.0f, 1.0f}, metal ? 0.15f : 0.88f), mul(alb, metal ? 0.85f : 0.12f));
+      acc = add(acc, mul(mulv(tint, irr), spec * cth * static_cast<float>(nl) * fmax_std(0.15f, ss)));
+    }
+    out = acc;
+    return true;
+  }
+
+  float light_pdf(V3 p, V3 dir) const {
+    if (w.lights.empty()) return 0.0f;
+    const float inv_n = 1.0f / static_cast<float>(w.lights.size());
+    float total = 0.0f;
+    for (const Light& L : w.lights) {
+      const V3 tl = sub(L.pos, p);
+      const float dist = std::sqrt(dot(tl, tl));
+      if (dist < kEps) continue;
+      if (dot(divs(tl, dist), dir) > 0.9999f) total += inv_n / (dist * dist + kEps);
+    }
+    return total;
+  }
+
+  static float mis(float a, float b) {
+    const float a2 = a * a, b2 = b * b, den = a2 + b2;
+    if (den <= 0.0f) return 1.0f;
+    return a2 / den;
+  }
+
+  static float schlick(float c, float ior) {
+    const float si = fmax_std(1.01f, ior);
+    float r0 = (1.0f - si) / (1.0f + si);
+    r0 *= r0;
+    const float m = 1.0f - fmin_std(1.0f, fmax_std(0.0f, c));
+    return r0 + (1.0f - r0) * m * m * m * m * m;
+  }
+
+  static V3 refract(V3 i, V3 n, float eta, bool& tir) {
+    const float ci = fmin_std(1.0f, fmax_std(0.0f, dot(neg(i), n)));
+    const float k = 1.0f - eta * eta * (1.0f - ci * ci);
+    if (k < 0.0f) { tir = true; return {0.0f, 0.0f, 0.0f}; }
+    tir = false;
+    return unit(add(mul(i, eta), mul(n, eta * ci - std::sqrt(k))));
+  }
+
+  V3 trace(V3 o, V3 d, Stream& rng, uint64_t& segs, Stats& st) const {
+    V3 rad{0.0f, 0.0f, 0.0f};
+    V3 thr{1.0f, 1.0f, 1.0f};
+    for (uint32_t depth = 0; depth < cfg.max_depth; ++depth) {
+      ++segs;
+      World::Hit h;
+      if (!w.intersect(o, d, h, st)) {
+        rad = add(rad, mulv(thr, w.env));
+        break;
+      }
+      const bool entering = dot(d, h.n) < 0.0f;
+      const V3 n = entering ? h.n : neg(h.n);
+      const Material& m = w.mat(h.mat);
+      const V3 alb = albedo_of(m);
+      const float rough = clamp01(m.roughness);
+      const bool emissive_model = m.model == 1u || m.emissive_any();
+      const bool mirror = m.model == 2u || rough <= 0.001f;
+      const bool metal = m.model == 4u || m.metallic > 0.65f;
+      const bool trans = m.model == 5u || m.transmission > 0.05f;
+      const bool diffuse = rough >= 0.999f && !mirror && !metal && !trans;
+      const bool sheen = m.model == 6u;
+      const bool coat = m.model == 7u || m.clearcoat > 0.05f;
+      const bool toon = m.model == 8u;
+
+      if (!cfg.enable_nee || depth == 0) {
+        rad = add(rad, mulv(thr, m.emissive));
+      } else if (cfg.enable_mis && emissive_model) {
+        const float bp = fmax_std(0.0f, dot(n, neg(d))) * kInvPi;
+        const float lp = light_pdf(o, d);
+        rad = add(rad, mul(mulv(thr, m.emissive), mis(bp, lp)));
+      }
+
+      if (cfg.enable_nee && depth < cfg.max_depth - 1u) {
+        World::Hit lh = h;
+        lh.n = n;
+        V3 nee{};
+        if (direct(lh, neg(d), rng, nee, st)) {
+          if (cfg.enable_mis) {
+            const V3 tl = w.lights.empty() ? V3{0.0f, 0.0f, 0.0f} : sub(w.lights[0].pos, h.p);
+            const V3 ld = unit(tl);
+            const float bp = fmax_std(0.0f, dot(n, ld)) * kInvPi;
+            const float lp = w.lights.empty() ? 1.0f : (1.0f / static_cast<float>(w.lights.size()));
+            rad = add(rad, mul(mulv(thr, nee), mis(lp, bp)));
+          } else {
+            rad = add(rad, mulv(thr, nee));
+          }
+        }
+      }
+
+      V3 out;
+      bool refracted = false;
+      const V3 refl = sub(d, mul(n, 2.0f * dot(n, d)));
+      if (mirror) {
+        out = refl;
+      } else if (trans) {
+        const float ct = fmax_std(0.0f, dot(n, neg(d)));
+        const float fr = schlick(ct, m.ior);
+        if (rng.u() < fmin_std(0.98f, fr + m.clearcoat * 0.015f)) {
+          out = refl;
+        } else {
+          bool tir = false;
+          const float si = fmax_std(1.01f, m.ior);
+          out = refract(d, n, entering ? (1.0f / si) : si, tir);
+          if (tir || dot(out, out) <= 1.0e-8f) out = refl;
+          else refracted = true;
+        }
+      } else if (diffuse || toon) {
+        out = hemisphere(rng, n);
+      } else {
+        const float er = fmax_std(0.025f, rough * (metal ? 0.75f : 1.0f) * (coat ? 0.65f : 1.0f));
+        const float a2 = er * er;
+        const float ex = fmax_std(0.0f, 2.0f / (a2 * a2) - 2.0f);
+        out = phong(rng, refl, ex, n);
+        if (sheen && rng.u() < m.sheen * 0.35f) out = hemisphere(rng, n);
+      }
+      if (!trans && dot(out, n) <= 0.0f) break;
+      V3 wgt = alb;
+      if (metal || mirror) {
+        wgt = mul(alb, 0.65f + 0.35f * m.metallic);
+      } else if (trans) {
+        const float ts = clamp01(m.alpha) * m.transmission;
+        wgt = add(mul(V3{1.0f, 1.0f, 1.0f}, 1.0f - ts), mul(alb, ts));
+        if (refracted) wgt = mul(wgt, fmax_std(0.55f, m.transmission));
+      }
+      if (toon) wgt = mul(wgt, dot(out, n) > 0.55f ? 1.0f : 0.45f);
+      thr = mulv(thr, wgt);
+      const float tmax = fmax_std(thr.x, fmax_std(thr.y, thr.z));
+      if (tmax < 0.001f) break;
+      const float rr = fmin_std(cfg.rr_max, fmax_std(cfg.rr_min, tmax));
+      if (depth >= cfg.rr_start && rng.u() > rr) break;
+      thr = divs(thr, rr);
+      o = add(h.p, mul(out, 0.002f));
+      d = out;
+    }
+    return rad;
+  }
+
+  // One camera path of pixel (x, y); returns false when the sample is not finite.
+  bool shade(uint32_t x, uint32_t y, uint32_t sample, V3& out, uint64_t& segs, Stats& st) const {
+    const uint32_t W = cfg.width, H = cfg.height;
+    const uint64_t sample_seed = (static_cast<uint64_t>(y) << 32) | x;
+    const uint64_t path_id = sample_seed + sample + 0u;
+    uint64_t cam_seed = 0;
+    // Camera stream: pixel = y*W + x, path id truncated to 32 bits.
+    Stream crng(cfg.seed, 0u, sample, static_cast<uint32_t>(path_id), 0u, 0u,
+                static_cast<uint64_t>(y) * W + x);
+    const float fx = (static_cast<float>(x) + crng.u()) / static_cast<float>(std::max(1u, W));
+    const float fy = (static_cast<float>(y) + crng.u()) / static_cast<float>(std::max(1u, H));
+    cam_seed ^= static_cast<uint64_t>(crng.u() * static_cast<float>(0xffffu));
+    const float aspect = static_cast<float>(W) / fmax_std(1.0f, static_cast<float>(H));
+    const float thf = std::tan(0.5f * (w.fov * (kPi / 180.0f)));
+    const float nx = (2.0f * fx - 1.0f) * aspect * thf;
+    const float ny = (1.0f - 2.0f * fy) * thf;
+    const V3 dir = unit(add(add(w.cam_fwd, mul(w.cam_right, nx)), mul(w.cam_up, ny)));
+    V3 o = w.cam_pos;
+    V3 d = dir;
+    if (w.aperture > 0.0f && w.focus > kEps) {
+      const float lr = std::sqrt(crng.u());
+      const float lphi = 2.0f * kPi * crng.u();
+      const float r = w.aperture * lr;
+      const V3 off = add(mul(w.cam_right, r * std::cos(lphi) * 1.0f), mul(w.cam_up, r * std::sin(lphi)));
+      const V3 fp = add(w.cam_pos, mul(dir, w.focus));
+      o = add(w.cam_pos, off);
+      d = unit(sub(fp, o));
+    }
+    Stream prng(cfg.seed + sample_seed + cam_seed, 0u, sample, path_id, 0u, 0u, sample_seed);
+    uint64_t path_segs = 0;
+    V3 c = trace(o, d, prng, path_segs, st);
+    // A non-finite sample is dropped together with its segment count.
+    if (!(std::isfinite(c.x) && std::isfinite(c.y) && std::isfinite(c.z))) return false;
+    segs += path_segs;
+    if (cfg.firefly_clamp > 0.0f) {
+      c.x = fmin_std(c.x, cfg.firefly_clamp);
+      c.y = fmin_std(c.y, cfg.firefly_clamp);
+      c.z = fmin_std(c.z, cfg.firefly_clamp);
+    }
+    out = c;
+    return true;
+  }
+};
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vko_last_error(void) { return g_error.c_str(); }
+const char* vko_impl_name(void) { return "port"; }
+
+int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t first_sample,
+               uint32_t n_samples, uint32_t threads, const uint32_t* pixels, uint32_t pixel_count,
+               float* film_sum, uint32_t* film_count, float* film_invalid, float* per_sample,
+               vko_counters* counters) {
+  if (!scene || !settings) return fail("null scene or settings");
+  for (uint32_t i = 0; i < scene->material_count; ++i) {
+    const uint32_t effect = static_cast<uint32_t>(scene->materials[16 * i + 15] + 0.5f) & 1023u;
+    if (effect != 0u) return fail("port oracle implements material effect 0 only");
+  }
+  World w;
+  w.load(*scene);
+  Integrator it{w, *settings};
+  const uint32_t W = settings->width, H = settings->height;
+  const size_t npx = static_cast<size_t>(W) * H;
+  std::vector<uint32_t> list;
+  if (pixels) {
+    list.assign(pixels, pixels + pixel_count);
+  } else {
+    list.resize(npx);
+    std::iota(list.begin(), list.end(), 0u);
+  }
+  std::vector<float> sum(3 * npx, 0.0f);
+  std::vector<uint32_t> cnt(npx, 0u);
+  std::vector<float> inv(npx, 0.0f);
+  const uint32_t nt = std::max(1u, threads);
+  std::vector<Stats> stats(nt);
+  std::vector<uint64_t> segs(nt, 0u), samples(nt, 0u);
+  double ms = 0.0;
+  for (uint32_t k = 0; k < n_samples; ++k) {
+    const uint32_t s = first_sample + k;
+    float* ps = per_sample ? per_sample + static_cast<size_t>(k) * 3 * npx : nullptr;
+    if (ps) std::fill(ps, ps + 3 * npx, 0.0f);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto work = [&](uint32_t t) {
+      const size_t b = list.size() * t / nt, e = list.size() * (t + 1) / nt;
+      for (size_t i = b; i < e; ++i) {
+        const uint32_t p = list[i];
+        if (p >= npx) continue;
+        V3 c{};
+        const bool ok = it.shade(p % W, p / W, s, c, segs[t], stats[t]);
+        if (!ok) { inv[p] += 1.0f; continue; }   // non-finite: dropped
+        ++samples[t];
+        sum[3 * p + 0] = sum[3 * p + 0] + c.x;
+        sum[3 * p + 1] = sum[3 * p + 1] + c.y;
+        sum[3 * p + 2] = sum[3 * p + 2] + c.z;
+        cnt[p] += 1u;
+        if (ps) { ps[3 * p] = c.x; ps[3 * p + 1] = c.y; ps[3 * p + 2] = c.z; }
+      }
+    };
+    if (nt == 1) {
+      work(0);
+    } else {
+      std::vector<std::thread> pool;
+      for (uint32_t t = 0; t < nt; ++t) pool.emplace_back(work, t);
+      for (auto& th : pool) th.join();
+    }
+    ms += ms_since(t0);
+  }
+  // The reference drops a non-finite sample before the film sees it
+  // (ScalarCpuPathTracer.Render.cpp:268-275), so invalid_samples stays 0.
+  std::fill(inv.begin(), inv.end(), 0.0f);
+  if (film_sum) std::memcpy(film_sum, sum.data(), sum.size() * sizeof(float));
+  if (film_count) std::memcpy(film_count, cnt.data(), cnt.size() * sizeof(uint32_t));
+  if (film_invalid) std::memcpy(film_invalid, inv.data(), inv.size() * sizeof(float));
+  if (counters) {
+    std::memset(counters, 0, sizeof(*counters));
+    for (uint32_t t = 0; t < nt; ++t) {
+      counters->samples += samples[t];
+      counters->rays += segs[t];
+      counters->triangle_tests += stats[t].tri_tests;
+      counters->triangle_hits += stats[t].tri_hits;
+      counters->bvh_node_visits += stats[t].nodes;
+      counters->bvh_leaf_visits += stats[t].leaves;
+      counters->shadow_tests += stats[t].shadow;
+    }
+    counters->render_ms = ms;
+  }
+  return 0;
+}
+
+int vko_build_bvh(const vko_scene* scene, uint32_t leaf_threshold, int deterministic, uint32_t* nodes_out,
+                  uint32_t* node_count, uint32_t* prim_indices_out) {
+  if (!scene || !nodes_out || !node_count || !prim_indices_out) return fail("null argument");
+  World w;
+  w.load(*scene, deterministic != 0, leaf_threshold == 0 ? 4u : leaf_threshold);
+  *node_count = static_cast<uint32_t>(w.nodes.size());
+  for (size_t i = 0; i < w.nodes.size(); ++i) {
+    const Node& n = w.nodes[i];
+    uint32_t* o = nodes_out + 10 * i;
+    std::memcpy(o, n.box.lo, 12);
+    std::memcpy(o + 3, n.box.hi, 12);
+    std::memcpy(o + 6, &n.left, 4);
+    std::memcpy(o + 7, &n.right, 4);
+    std::memcpy(o + 8, &n.first, 4);
+    std::memcpy(o + 9, &n.count, 4);
+  }
+  std::copy(w.order.begin(), w.order.end(), prim_indices_out);
+  return 0;
+}
+
+int vko_intersect(const vko_scene* scene, const float* rays, uint64_t ray_count, uint32_t threads,
+                  uint32_t* prim_out, float* t_out, uint64_t* stats, double* elapsed_ms) {
+  if (!scene || !rays || !prim_out || !t_out) return fail("null argument");
+  World w;
+  w.load(*scene);
+  const uint32_t nt = std::max(1u, threads);
+  std::vector<Stats> st(nt);
+  const auto t0 = std::chrono::steady_clock::now();
+  auto work = [&](uint32_t t) {
+    const uint64_t b = ray_count * t / nt, e = ray_count * (t + 1) / nt;
+    for (uint64_t i = b; i < e; ++i) {
+      float tt = 0.0f;
+      const int64_t k = w.closest(ld3(rays + 6 * i), ld3(rays + 6 * i + 3), tt, st[t]);
+      prim_out[i] = k < 0 ? 0xFFFFFFFFu : w.prims[static_cast<size_t>(k)].index;
+      t_out[i] = k < 0 ? std::numeric_limits<float>::infinity() : tt;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t t = 0; t < nt; ++t) pool.emplace_back(work, t);
+  for (auto& th : pool) th.join();
+  if (elapsed_ms) *elapsed_ms = ms_since(t0);
+  if (stats) {
+    std::memset(stats, 0, 4 * sizeof(uint64_t));
+    for (const Stats& s : st) {
+      stats[0] += s.tri_tests;
+      stats[1] += s.tri_hits;
+      stats[2] += s.nodes;
+      stats[3] += s.leaves;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

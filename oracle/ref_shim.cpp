@@ -1,0 +1,416 @@
+// ref_shim.cpp -- TEST INFRASTRUCTURE: drives the reference's own CPU tracer.
+//
+// Compiled by oracle/Makefile together with the reference's unmodified
+// translation units into oracle/_ref/libvkptref.so.  It only converts the POD
+// scene of vkpt_oracle.h into the reference's PathTracerSceneSnapshot and calls
+// the reference's public classes:
+//   ScalarCpuPathTracer   (src/pathtracer/PathTracer.h:1232-1370)
+//   TiledCpuPathTracer    (src/cpu/TiledCpuPathTracer.h:47-130)
+//   CreateCpuBvhAccelerator / IRayAccelerator::intersect
+//                         (src/pathtracer/PathTracer.h:1001-1036,
+//                          src/pathtracer/CpuBvhAccelerator.cpp:360-477)
+//   ParallelBvhBuilder    (src/cpu/ParallelBvhBuilder.cpp:165-257)
+// The product library never links this file.
+
+#include "../oracle/vkpt_oracle.h"
+
+#include "core/Logging.h"
+#include "cpu/ParallelBvhBuilder.h"
+#include "cpu/TiledCpuPathTracer.h"
+#include "pathtracer/PathTracer.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace pt = vkpt::pathtracer;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(const std::string& message) {
+  g_error = message;
+  return 1;
+}
+
+void quiet_logs() {
+  vkpt::log::Logger::instance().set_min_severity(vkpt::log::Severity::Fatal);
+}
+
+pt::Vec3 v3(const float* p) { return pt::Vec3{p[0], p[1], p[2]}; }
+
+pt::PathTracerSceneSnapshot to_snapshot(const vko_scene& s) {
+  pt::PathTracerSceneSnapshot out;
+  out.vertices.resize(s.vertex_count);
+  for (uint32_t i = 0; i < s.vertex_count; ++i) out.vertices[i] = v3(s.vertices + 3 * i);
+  out.indices.assign(s.indices, s.indices + s.index_count);
+  out.instances.resize(s.instance_count);
+  for (uint32_t i = 0; i < s.instance_count; ++i) {
+    out.instances[i].entity_id = i + 1u;
+    out.instances[i].first_triangle = s.instances[3 * i + 0];
+    out.instances[i].triangle_count = s.instances[3 * i + 1];
+    out.instances[i].material_index = s.instances[3 * i + 2];
+  }
+  out.materials.resize(s.material_count);
+  for (uint32_t i = 0; i < s.material_count; ++i) {
+    const float* m = s.materials + 16 * i;
+    pt::RTMaterial& r = out.materials[i];
+    r.albedo = v3(m + 0);
+    r.emissive = v3(m + 3);
+    r.roughness = m[6];
+    r.material_model = static_cast<uint32_t>(m[7] + 0.5f);
+    r.metallic = m[8];
+    r.ior = m[9];
+    r.transmission = m[10];
+    r.clearcoat = m[11];
+    r.sheen = m[12];
+    r.anisotropy = m[13];
+    r.alpha = m[14];
+    const uint32_t packed = static_cast<uint32_t>(m[15] + 0.5f);
+    r.material_effect = packed & 1023u;
+    r.material_flags = (packed & 1024u) ? 1u : 0u;
+  }
+  out.lights.resize(s.light_count);
+  for (uint32_t i = 0; i < s.light_count; ++i) {
+    const float* l = s.lights + 16 * i;
+    pt::RTHitLight& r = out.lights[i];
+    r.position = v3(l + 0);
+    r.color = v3(l + 3);
+    r.intensity = l[6];
+    r.radius = l[7];
+    r.direction = v3(l + 8);
+    r.spot_inner_cos = l[11];
+    r.spot_outer_cos = l[12];
+  }
+  out.environment_color = v3(s.environment);
+  out.camera_position = v3(s.camera_position);
+  out.camera_target = v3(s.camera_target);
+  out.camera_up = v3(s.camera_up);
+  out.camera_fov_deg = s.camera_fov_deg;
+  out.camera_aperture_radius = s.camera_aperture_radius;
+  out.camera_focus_distance = s.camera_focus_distance;
+  return out;
+}
+
+pt::RenderSettings to_settings(const vko_settings& s, uint32_t spp) {
+  pt::RenderSettings r;
+  r.width = s.width;
+  r.height = s.height;
+  r.spp = spp;
+  r.max_depth = s.max_depth;
+  r.seed = s.seed;
+  r.enable_nee = s.enable_nee != 0;
+  r.enable_mis = s.enable_mis != 0;
+  r.deterministic = true;
+  r.russian_roulette_start_depth = s.rr_start;
+  r.russian_roulette_min_survival = s.rr_min;
+  r.russian_roulette_max_survival = s.rr_max;
+  return r;
+}
+
+void read_film(const pt::FilmBuffer& film, float* sum, uint32_t* count, float* invalid) {
+  const auto& raw = film.raw();
+  const auto& cnt = film.sample_counts();
+  const auto& inv = film.invalid_samples();
+  for (std::size_t i = 0; i < raw.size(); ++i) {
+    if (sum) {
+      sum[3 * i + 0] = raw[i].x;
+      sum[3 * i + 1] = raw[i].y;
+      sum[3 * i + 2] = raw[i].z;
+    }
+    if (count) count[i] = cnt[i];
+    if (invalid) invalid[i] = inv[i];
+  }
+}
+
+void add_counters(vko_counters* out, const pt::SampleCounters& c) {
+  out->samples += c.samples;
+  out->rays += c.rays;
+  out->triangle_tests += c.triangle_tests;
+  out->triangle_hits += c.triangle_hits;
+  out->bvh_node_visits += c.bvh_node_visits;
+  out->bvh_leaf_visits += c.bvh_leaf_visits;
+  out->shadow_tests += c.shadow_tests;
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Full-frame render through one IPathTracer, one render_tile per sample, as
+// ptbench's `run` loop does (src/benchmark/BenchmarkRuntime.cpp:682-693).
+int render_full(pt::IPathTracer& tracer, const vko_settings& st, uint32_t first, uint32_t n,
+                float* film_sum, uint32_t* film_count, float* film_invalid, float* per_sample,
+                vko_counters* counters) {
+  const std::size_t npx = static_cast<std::size_t>(st.width) * st.height;
+  std::vector<float> total(per_sample ? 3 * npx : 0, 0.0f);
+  std::vector<uint32_t> total_count(per_sample ? npx : 0, 0u);
+  std::vector<float> total_invalid(per_sample ? npx : 0, 0.0f);
+  double ms = 0.0;
+  for (uint32_t k = 0; k < n; ++k) {
+    if (per_sample && !tracer.reset_accumulation()) return fail("reset_accumulation failed");
+    pt::RenderTile tile;
+    tile.width = st.width;
+    tile.height = st.height;
+    tile.sample_index = first + k;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!tracer.render_tile(tile, 0u)) return fail("render_tile failed: " + tracer.status().last_error);
+    ms += ms_since(t0);
+    // reset_accumulation clears the counters, so per-sample mode sums them here.
+    if (counters && per_sample) add_counters(counters, tracer.read_counters());
+    if (per_sample) {
+      const auto& raw = tracer.film().raw();
+      const auto& cnt = tracer.film().sample_counts();
+      const auto& inv = tracer.film().invalid_samples();
+      float* dst = per_sample + static_cast<std::size_t>(k) * 3 * npx;
+      for (std::size_t i = 0; i < npx; ++i) {
+        dst[3 * i + 0] = raw[i].x;
+        dst[3 * i + 1] = raw[i].y;
+        dst[3 * i + 2] = raw[i].z;
+        if (cnt[i] != 0u) {
+          total[3 * i + 0] = total[3 * i + 0] + raw[i].x;
+          total[3 * i + 1] = total[3 * i + 1] + raw[i].y;
+          total[3 * i + 2] = total[3 * i + 2] + raw[i].z;
+        }
+        total_count[i] += cnt[i];
+        total_invalid[i] += inv[i];
+      }
+    }
+  }
+  if (per_sample) {
+    if (film_sum) std::memcpy(film_sum, total.data(), total.size() * sizeof(float));
+    if (film_count) std::memcpy(film_count, total_count.data(), total_count.size() * sizeof(uint32_t));
+    if (film_invalid) std::memcpy(film_invalid, total_invalid.data(), total_invalid.size() * sizeof(float));
+  } else {
+    read_film(tracer.film(), film_sum, film_count, film_invalid);
+    if (counters) add_counters(counters, tracer.read_counters());
+  }
+  if (counters) counters->render_ms += ms;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vko_last_error(void) { return g_error.c_str(); }
+const char* vko_impl_name(void) { return "reference"; }
+
+int vko_render(const vko_scene* scene, const vko_settings* settings,
+               uint32_t first_sample, uint32_t n_samples, uint32_t threads,
+               const uint32_t* pixels, uint32_t pixel_count,
+               float* film_sum, uint32_t* film_count, float* film_invalid,
+               float* per_sample, vko_counters* counters) {
+  quiet_logs();
+  if (!scene || !settings) return fail("null scene or settings");
+  if (settings->firefly_clamp != 0.0f) return fail("the reference has no firefly clamp");
+  if (counters) std::memset(counters, 0, sizeof(*counters));
+  const auto snap = to_snapshot(*scene);
+  const auto rs = to_settings(*settings, first_sample + n_samples);
+  const std::size_t npx = static_cast<std::size_t>(settings->width) * settings->height;
+
+  if (pixels == nullptr) {
+    if (threads <= 1u) {
+      pt::ScalarCpuPathTracer tracer;
+      if (!tracer.configure(rs) || !tracer.load_scene_snapshot(snap) ||
+          !tracer.build_or_update_acceleration() || !tracer.reset_accumulation()) {
+        return fail("scalar tracer setup failed: " + tracer.status().last_error);
+      }
+      return render_full(tracer, *settings, first_sample, n_samples, film_sum, film_count,
+                         film_invalid, per_sample, counters);
+    }
+    vkpt::cpu::TiledRenderConfig cfg;
+    cfg.tile_height = 16u;
+    cfg.worker_count = threads;
+    cfg.deterministic = false;
+    vkpt::cpu::TiledCpuPathTracer tracer(cfg);
+    if (!tracer.configure(rs) || !tracer.load_scene_snapshot(snap) ||
+        !tracer.build_or_update_acceleration() || !tracer.reset_accumulation()) {
+      return fail("tiled tracer setup failed: " + tracer.status().last_error);
+    }
+    return render_full(tracer, *settings, first_sample, n_samples, film_sum, film_count,
+                       film_invalid, per_sample, counters);
+  }
+
+  // Sparse pixel list: render_sample_pixels (src/pathtracer/ScalarCpuPathTracer.Render.cpp:335-381)
+  // on `threads` tracers that share one accelerator, as TiledCpuPathTracer's
+  // tiles do (src/cpu/TiledCpuPathTracer.cpp:279-323).
+  const uint32_t nt = std::max(1u, std::min(threads, std::max(1u, pixel_count)));
+  auto accel = pt::CreateCpuBvhAccelerator();
+  if (!accel->build(snap, true)) return fail("accelerator build failed");
+  std::vector<std::unique_ptr<pt::ScalarCpuPathTracer>> tracers(nt);
+  for (auto& tr : tracers) {
+    tr = std::make_unique<pt::ScalarCpuPathTracer>();
+    if (!tr->configure(rs) || !tr->set_accelerator(accel.get()) || !tr->load_scene_snapshot(snap) ||
+        !tr->update_camera(snap.camera_position, snap.camera_target, snap.camera_up, snap.camera_fov_deg) ||
+        !tr->reset_accumulation()) {
+      return fail("pixel-list tracer setup failed");
+    }
+  }
+  std::vector<std::vector<uint32_t>> lists(nt);
+  for (uint32_t i = 0; i < pixel_count; ++i) lists[i % nt].push_back(pixels[i]);
+  std::vector<float> total(3 * npx, 0.0f);
+  std::vector<uint32_t> total_count(npx, 0u);
+  std::vector<float> total_invalid(npx, 0.0f);
+  double ms = 0.0;
+  for (uint32_t k = 0; k < n_samples; ++k) {
+    std::atomic<int> bad{0};
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t < nt; ++t) {
+      pool.emplace_back([&, t]() {
+        if (per_sample) tracers[t]->reset_accumulation();
+        if (!lists[t].empty() &&
+            !tracers[t]->render_sample_pixels(lists[t].data(), static_cast<uint32_t>(lists[t].size()),
+                                              first_sample + k, 0u)) {
+          bad.fetch_add(1);
+        }
+      });
+    }
+    for (auto& th : pool) th.join();
+    ms += ms_since(t0);
+    if (bad.load() != 0) return fail("render_sample_pixels failed");
+    if (per_sample) {
+      float* dst = per_sample + static_cast<std::size_t>(k) * 3 * npx;
+      std::fill(dst, dst + 3 * npx, 0.0f);
+      for (uint32_t t = 0; t < nt; ++t) {
+        const auto& raw = tracers[t]->film().raw();
+        const auto& cnt = tracers[t]->film().sample_counts();
+        const auto& inv = tracers[t]->film().invalid_samples();
+        for (uint32_t p : lists[t]) {
+          if (p >= npx) continue;
+          dst[3 * p + 0] = raw[p].x;
+          dst[3 * p + 1] = raw[p].y;
+          dst[3 * p + 2] = raw[p].z;
+          if (cnt[p] != 0u) {
+            total[3 * p + 0] = total[3 * p + 0] + raw[p].x;
+            total[3 * p + 1] = total[3 * p + 1] + raw[p].y;
+            total[3 * p + 2] = total[3 * p + 2] + raw[p].z;
+          }
+          total_count[p] += cnt[p];
+          total_invalid[p] += inv[p];
+        }
+      }
+    }
+  }
+  if (!per_sample) {
+    for (uint32_t t = 0; t < nt; ++t) {
+      const auto& raw = tracers[t]->film().raw();
+      const auto& cnt = tracers[t]->film().sample_counts();
+      const auto& inv = tracers[t]->film().invalid_samples();
+      for (uint32_t p : lists[t]) {
+        if (p >= npx) continue;
+        total[3 * p + 0] = raw[p].x;
+        total[3 * p + 1] = raw[p].y;
+        total[3 * p + 2] = raw[p].z;
+        total_count[p] = cnt[p];
+        total_invalid[p] = inv[p];
+      }
+    }
+  }
+  if (film_sum) std::memcpy(film_sum, total.data(), total.size() * sizeof(float));
+  if (film_count) std::memcpy(film_count, total_count.data(), total_count.size() * sizeof(uint32_t));
+  if (film_invalid) std::memcpy(film_invalid, total_invalid.data(), total_invalid.size() * sizeof(float));
+  if (counters) {
+    for (auto& tr : tracers) add_counters(counters, tr->read_counters());
+    counters->render_ms = ms;
+  }
+  return 0;
+}
+
+int vko_build_bvh(const vko_scene* scene, uint32_t leaf_threshold, int deterministic,
+                  uint32_t* nodes_out, uint32_t* node_count, uint32_t* prim_indices_out) {
+  quiet_logs();
+  if (!scene || !nodes_out || !node_count || !prim_indices_out) return fail("null argument");
+  // Primitive AABBs in the accelerator's flattening order, padded by 1e-4
+  // (src/pathtracer/CpuBvhAccelerator.cpp:84-95, 173-247).
+  const float eps = 1e-4f;
+  std::vector<vkpt::cpu::BvhAabb> boxes;
+  for (uint32_t inst = 0; inst < scene->instance_count; ++inst) {
+    const uint32_t first = scene->instances[3 * inst + 0];
+    const uint32_t count = scene->instances[3 * inst + 1];
+    for (uint32_t k = 0; k < count; ++k) {
+      const uint32_t base = (first + k) * 3u;
+      if (base + 2u >= scene->index_count) continue;
+      const uint32_t i0 = scene->indices[base], i1 = scene->indices[base + 1], i2 = scene->indices[base + 2];
+      if (i0 >= scene->vertex_count || i1 >= scene->vertex_count || i2 >= scene->vertex_count) continue;
+      const float* a = scene->vertices + 3 * i0;
+      const float* b = scene->vertices + 3 * i1;
+      const float* c = scene->vertices + 3 * i2;
+      vkpt::cpu::BvhAabb box;
+      for (int ax = 0; ax < 3; ++ax) {
+        box.min[ax] = std::min({a[ax], b[ax], c[ax]}) - eps;
+        box.max[ax] = std::max({a[ax], b[ax], c[ax]}) + eps;
+      }
+      boxes.push_back(box);
+    }
+  }
+  vkpt::cpu::ParallelBvhBuilder builder;
+  const auto result = builder.build(boxes, nullptr, deterministic != 0, leaf_threshold);
+  *node_count = static_cast<uint32_t>(result.nodes.size());
+  for (std::size_t i = 0; i < result.nodes.size(); ++i) {
+    const auto& n = result.nodes[i];
+    uint32_t* w = nodes_out + 10 * i;
+    std::memcpy(w + 0, n.aabb.min, 12);
+    std::memcpy(w + 3, n.aabb.max, 12);
+    std::memcpy(w + 6, &n.left_child, 4);
+    std::memcpy(w + 7, &n.right_child, 4);
+    std::memcpy(w + 8, &n.first_prim, 4);
+    std::memcpy(w + 9, &n.prim_count, 4);
+  }
+  std::copy(result.prim_indices.begin(), result.prim_indices.end(), prim_indices_out);
+  return 0;
+}
+
+int vko_intersect(const vko_scene* scene, const float* rays, uint64_t ray_count,
+                  uint32_t threads, uint32_t* prim_out, float* t_out,
+                  uint64_t* stats, double* elapsed_ms) {
+  quiet_logs();
+  if (!scene || !rays || !prim_out || !t_out) return fail("null argument");
+  const auto snap = to_snapshot(*scene);
+  auto accel = pt::CreateCpuBvhAccelerator();
+  if (!accel->build(snap, true)) return fail("accelerator build failed");
+  const uint32_t nt = std::max(1u, threads);
+  std::vector<pt::RayQueryStats> per(nt);
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  for (uint32_t t = 0; t < nt; ++t) {
+    pool.emplace_back([&, t]() {
+      const uint64_t begin = ray_count * t / nt;
+      const uint64_t end = ray_count * (t + 1) / nt;
+      for (uint64_t i = begin; i < end; ++i) {
+        pt::Ray ray{v3(rays + 6 * i), v3(rays + 6 * i + 3)};
+        pt::RayQueryHit hit;
+        if (accel->intersect(ray, hit, stats ? &per[t] : nullptr) && hit.hit) {
+          prim_out[i] = hit.primitive_index;
+          t_out[i] = hit.t;
+        } else {
+          prim_out[i] = 0xFFFFFFFFu;
+          t_out[i] = std::numeric_limits<float>::infinity();
+        }
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+  if (elapsed_ms) *elapsed_ms = ms_since(t0);
+  if (stats) {
+    std::memset(stats, 0, 4 * sizeof(uint64_t));
+    for (const auto& s : per) {
+      stats[0] += s.triangle_tests;
+      stats[1] += s.triangle_hits;
+      stats[2] += s.bvh_node_visits;
+      stats[3] += s.bvh_leaf_visits;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

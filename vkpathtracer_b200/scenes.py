@@ -1,0 +1,538 @@
+"""Seeded synthetic scenes and ray sets for the render hot path.
+
+Every workload is generated here from a documented splitmix64 stream, so the
+CUDA path, the CPU oracle and the benchmark see bit-identical float32 inputs.
+There is no dataset: the reference's own fixtures are binary LFS assets, so
+each workload is procedural with the shapes, sizes and value ranges of the
+benchmark configurations:
+
+  cornell_box()          closed box scene (36 triangles), 256x256, 16 spp, depth 8
+  displaced_sphere()     1,046,904-triangle value-noise sphere + 8,388,608 query rays
+  sphere_grid()          64x64 displaced spheres (~2M triangles), 1920x1080, 64 spp, depth 16
+  batch_jobs()           64 uneven render jobs for the persistent batched renderer
+  inverse_box_scene()    the box room with 16 boxes and a 64-parameter material vector
+
+Scene records use the reference's standard GPU word maps
+(src/gpu/VulkanGpuPathTracer.cpp:323-338 for materials, :381-396 for lights),
+so a packed buffer from the reference's Vulkan backend is accepted unchanged.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional
+
+import numpy as np
+
+MASK64 = (1 << 64) - 1
+
+# Material word offsets (16 floats per material).
+M_ALBEDO, M_EMISSIVE, M_ROUGHNESS, M_MODEL, M_METALLIC, M_IOR = 0, 3, 6, 7, 8, 9
+M_TRANSMISSION, M_CLEARCOAT, M_SHEEN, M_ANISO, M_ALPHA, M_EFFECT = 10, 11, 12, 13, 14, 15
+# Light word offsets (16 floats per light).
+L_POS, L_COLOR, L_INTENSITY, L_RADIUS, L_DIR, L_INNER, L_OUTER = 0, 3, 6, 7, 8, 11, 12
+
+
+def splitmix64(x: int) -> int:
+    """One splitmix64 step on a Python int (same constants as the reference RNG)."""
+    x = (x + 0x9E3779B97F4A7C15) & MASK64
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & MASK64
+    return x ^ (x >> 31)
+
+
+def splitmix64_np(x: np.ndarray) -> np.ndarray:
+    """Vectorised splitmix64 over a uint64 array (wrapping arithmetic)."""
+    x = x.astype(np.uint64, copy=True)
+    with np.errstate(over="ignore"):
+        x += np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+class Stream:
+    """Generator stream: state_{k+1} = splitmix64(state_k); uniform = top 24 bits / 2^24."""
+
+    def __init__(self, seed: int):
+        self.state = splitmix64(seed & MASK64)
+
+    def next_u64(self) -> int:
+        self.state = splitmix64(self.state)
+        return self.state
+
+    def uniform(self, lo: float = 0.0, hi: float = 1.0) -> float:
+        u = (self.next_u64() >> 40) * (1.0 / 16777216.0)
+        return lo + (hi - lo) * u
+
+    def randint(self, lo: int, hi: int) -> int:
+        """Integer in [lo, hi]."""
+        return lo + int(self.uniform() * (hi - lo + 1)) if hi > lo else lo
+
+    def uniform_np(self, n: int) -> np.ndarray:
+        """n uniforms in [0,1) as float64, from a counter-keyed block of this stream."""
+        base = self.next_u64()
+        keys = np.arange(n, dtype=np.uint64) + np.uint64(base)
+        return (splitmix64_np(keys) >> np.uint64(40)).astype(np.float64) * (1.0 / 16777216.0)
+
+
+@dataclasses.dataclass
+class Camera:
+    position: tuple = (0.0, 0.0, 0.0)
+    target: tuple = (0.0, 0.0, -1.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    fov_deg: float = 60.0
+    aperture_radius: float = 0.0
+    focus_distance: float = 0.0
+
+
+@dataclasses.dataclass
+class Scene:
+    """Flattened scene in the layout of the reference's PathTracerSceneSnapshot."""
+    vertices: np.ndarray            # (V,3) float32
+    indices: np.ndarray             # (T,3) uint32
+    instances: np.ndarray           # (I,3) uint32: first_triangle, triangle_count, material_index
+    materials: np.ndarray           # (M,16) float32
+    lights: np.ndarray              # (L,16) float32
+    environment: tuple = (0.0, 0.0, 0.0)
+    camera: Camera = dataclasses.field(default_factory=Camera)
+    name: str = "scene"
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.indices.shape[0])
+
+    def contiguous(self) -> "Scene":
+        self.vertices = np.ascontiguousarray(self.vertices, dtype=np.float32)
+        self.indices = np.ascontiguousarray(self.indices, dtype=np.uint32)
+        self.instances = np.ascontiguousarray(self.instances, dtype=np.uint32).reshape(-1, 3)
+        self.materials = np.ascontiguousarray(self.materials, dtype=np.float32).reshape(-1, 16)
+        self.lights = np.ascontiguousarray(self.lights, dtype=np.float32).reshape(-1, 16)
+        return self
+
+
+@dataclasses.dataclass
+class RenderSettings:
+    """Mirror of the reference's RenderSettings (src/pathtracer/PathTracer.h:134-178)."""
+    width: int = 256
+    height: int = 256
+    spp: int = 8
+    max_depth: int = 6
+    seed: int = 0x12345678
+    enable_nee: bool = True
+    enable_mis: bool = True
+    deterministic: bool = True
+    russian_roulette_start_depth: int = 3
+    russian_roulette_min_survival: float = 0.1
+    russian_roulette_max_survival: float = 0.99
+    camera_aperture_radius: float = 0.0
+    camera_focus_distance: float = 0.0
+    # Extension absent from the reference: per-channel clamp of each sample's
+    # radiance before accumulation (0 = off, the reference's behaviour).
+    firefly_clamp: float = 0.0
+
+
+def material(albedo=(1.0, 1.0, 1.0), emissive=(0.0, 0.0, 0.0), roughness=1.0, model=0,
+             metallic=0.0, ior=1.5, transmission=0.0, clearcoat=0.0, sheen=0.0,
+             anisotropy=0.0, alpha=1.0, effect=0, double_sided=False) -> np.ndarray:
+    m = np.zeros(16, dtype=np.float32)
+    m[0:3] = albedo
+    m[3:6] = emissive
+    m[M_ROUGHNESS] = roughness
+    m[M_MODEL] = float(model)
+    m[M_METALLIC] = metallic
+    m[M_IOR] = ior
+    m[M_TRANSMISSION] = transmission
+    m[M_CLEARCOAT] = clearcoat
+    m[M_SHEEN] = sheen
+    m[M_ANISO] = anisotropy
+    m[M_ALPHA] = alpha
+    m[M_EFFECT] = float((effect & 1023) | (1024 if double_sided else 0))
+    return m
+
+
+def point_light(position, color, intensity, radius=0.0, direction=(0.0, -1.0, 0.0),
+                spot_inner_cos=-1.0, spot_outer_cos=-1.0) -> np.ndarray:
+    l = np.zeros(16, dtype=np.float32)
+    l[0:3] = position
+    l[3:6] = color
+    l[L_INTENSITY] = intensity
+    l[L_RADIUS] = max(0.0, radius)
+    l[8:11] = direction
+    l[L_INNER] = spot_inner_cos
+    l[L_OUTER] = spot_outer_cos
+    return l
+
+
+class _Builder:
+    def __init__(self):
+        self.verts: List[np.ndarray] = []
+        self.tris: List[np.ndarray] = []
+        self.instances: List[tuple] = []
+        self.nv = 0
+        self.nt = 0
+
+    def add(self, verts: np.ndarray, tris: np.ndarray, material_index: int):
+        verts = np.asarray(verts, dtype=np.float32).reshape(-1, 3)
+        tris = np.asarray(tris, dtype=np.int64).reshape(-1, 3) + self.nv
+        self.instances.append((self.nt, tris.shape[0], material_index))
+        self.verts.append(verts)
+        self.tris.append(tris.astype(np.uint32))
+        self.nv += verts.shape[0]
+        self.nt += tris.shape[0]
+
+    def arrays(self):
+        return (np.concatenate(self.verts).astype(np.float32),
+                np.concatenate(self.tris).astype(np.uint32),
+                np.array(self.instances, dtype=np.uint32).reshape(-1, 3))
+
+
+def _quad(p0, p1, p2, p3):
+    """Quad p0-p1-p2-p3 as two triangles (0,1,2), (0,2,3)."""
+    return np.array([p0, p1, p2, p3], dtype=np.float32), np.array([[0, 1, 2], [0, 2, 3]])
+
+
+def _box(center, half, yaw_deg):
+    """Axis-aligned box rotated about +y; 8 vertices, 12 triangles."""
+    cx, cy, cz = center
+    hx, hy, hz = half
+    a = math.radians(yaw_deg)
+    c, s = math.cos(a), math.sin(a)
+    corners = []
+    for (sx, sy, sz) in [(-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1),
+                         (-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1)]:
+        x, y, z = sx * hx, sy * hy, sz * hz
+        corners.append((cx + c * x + s * z, cy + y, cz - s * x + c * z))
+    tris = [[0, 5, 4], [0, 1, 5], [3, 7, 6], [3, 6, 2], [0, 2, 1], [0, 3, 2],
+            [4, 5, 6], [4, 6, 7], [0, 4, 7], [0, 7, 3], [1, 2, 6], [1, 6, 5]]
+    return np.array(corners, dtype=np.float32), np.array(tris)
+
+
+def _room(b: _Builder, materials: list, st: Stream, albedo_lo=0.1, albedo_hi=0.8):
+    """Unit box x,z in [-0.5,0.5], y in [0,1], open towards +z: 5 inward quads (10 tris)."""
+    walls = [
+        ((-0.5, 0, -0.5), (-0.5, 0, 0.5), (0.5, 0, 0.5), (0.5, 0, -0.5)),      # floor
+        ((-0.5, 1, -0.5), (0.5, 1, -0.5), (0.5, 1, 0.5), (-0.5, 1, 0.5)),      # ceiling
+        ((-0.5, 0, -0.5), (0.5, 0, -0.5), (0.5, 1, -0.5), (-0.5, 1, -0.5)),    # back
+        ((-0.5, 0, -0.5), (-0.5, 1, -0.5), (-0.5, 1, 0.5), (-0.5, 0, 0.5)),    # left
+        ((0.5, 0, -0.5), (0.5, 0, 0.5), (0.5, 1, 0.5), (0.5, 1, -0.5)),        # right
+    ]
+    for w in walls:
+        alb = tuple(st.uniform(albedo_lo, albedo_hi) for _ in range(3))
+        materials.append(material(albedo=alb, roughness=1.0))
+        v, t = _quad(*w)
+        b.add(v, t, len(materials) - 1)
+
+
+def _ceiling_light(b: _Builder, materials: list, lights: list, size=0.25, radiance=(17.0, 12.0, 4.0),
+                   height=0.999, center=(0.0, 0.0)):
+    """Emissive quad plus the co-located point light that drives NEE.
+
+    The reference's NEE samples only point/sphere lights, so an area light is
+    represented as in its Cornell fixture (assets/scenes/cornell_native.json:
+    emissive quad + point light at the same spot): intensity = quad area.
+    """
+    h = size * 0.5
+    cx, cz = center
+    materials.append(material(albedo=(0.78, 0.78, 0.78), emissive=radiance, roughness=1.0))
+    v, t = _quad((cx - h, height, cz - h), (cx + h, height, cz - h), (cx + h, height, cz + h), (cx - h, height, cz + h))
+    b.add(v, t, len(materials) - 1)
+    lights.append(point_light((cx, height - 0.001, cz), radiance, size * size))
+
+
+def cornell_box(seed: int = 1) -> Scene:
+    """Closed box (10 tris) + 2 boxes rotated U[-30,30] deg (24 tris) + 0.25x0.25 light (2 tris)."""
+    st = Stream(seed)
+    b = _Builder()
+    mats: list = []
+    lights: list = []
+    _room(b, mats, st)
+    for center, half in [((-0.17, 0.3, -0.15), (0.14, 0.3, 0.14)), ((0.18, 0.15, 0.12), (0.14, 0.15, 0.14))]:
+        alb = tuple(st.uniform(0.1, 0.8) for _ in range(3))
+        mats.append(material(albedo=alb, roughness=1.0))
+        yaw = st.uniform(-30.0, 30.0)
+        v, t = _box(center, half, yaw)
+        b.add(v, t, len(mats) - 1)
+    _ceiling_light(b, mats, lights)
+    v, t, inst = b.arrays()
+    cam = Camera(position=(0.0, 0.5, 1.9), target=(0.0, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0)
+    return Scene(v, t, inst, np.array(mats), np.array(lights), (0.0, 0.0, 0.0), cam, "cornell_box").contiguous()
+
+
+def cornell_settings(width=256, height=256, spp=16) -> RenderSettings:
+    return RenderSettings(width=width, height=height, spp=spp, max_depth=8, seed=1234,
+                          enable_nee=True, enable_mis=True)
+
+
+# ---------------------------------------------------------------- value noise
+def _lattice(ix, iy, iz, octave: int, seed: int) -> np.ndarray:
+    key = (ix.astype(np.int64).astype(np.uint64) * np.uint64(0x9E3779B1)) ^ \
+          (iy.astype(np.int64).astype(np.uint64) * np.uint64(0x85EBCA77) << np.uint64(20)) ^ \
+          (iz.astype(np.int64).astype(np.uint64) * np.uint64(0xC2B2AE3D) << np.uint64(40))
+    key = key ^ np.uint64(splitmix64((seed * 131 + octave) & MASK64))
+    return (splitmix64_np(key) >> np.uint64(40)).astype(np.float64) * (1.0 / 16777216.0)
+
+
+def value_noise(p: np.ndarray, octaves: int, seed: int) -> np.ndarray:
+    """fBm of trilinear value noise with smoothstep weights, in [-1, 1] (float64)."""
+    total = np.zeros(p.shape[0])
+    norm = 0.0
+    amp = 1.0
+    freq = 2.0
+    for o in range(octaves):
+        q = p * freq
+        i0 = np.floor(q)
+        f = q - i0
+        w = f * f * (3.0 - 2.0 * f)
+        ix, iy, iz = i0[:, 0], i0[:, 1], i0[:, 2]
+        acc = np.zeros(p.shape[0])
+        for dx in (0, 1):
+            wx = w[:, 0] if dx else 1.0 - w[:, 0]
+            for dy in (0, 1):
+                wy = w[:, 1] if dy else 1.0 - w[:, 1]
+                for dz in (0, 1):
+                    wz = w[:, 2] if dz else 1.0 - w[:, 2]
+                    acc += wx * wy * wz * _lattice(ix + dx, iy + dy, iz + dz, o, seed)
+        total += amp * (2.0 * acc - 1.0)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return total / norm
+
+
+def _uv_sphere(n_lat: int, n_lon: int):
+    """Grid sphere: n_lat rows pole to pole x n_lon columns; 2*(n_lat-1)*n_lon triangles."""
+    theta = np.linspace(0.0, math.pi, n_lat)
+    phi = np.arange(n_lon) * (2.0 * math.pi / n_lon)
+    st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
+    dirs = np.stack([st * np.cos(phi)[None, :], np.broadcast_to(ct, (n_lat, n_lon)), st * np.sin(phi)[None, :]], axis=-1)
+    dirs = dirs.reshape(-1, 3)
+    i = np.arange(n_lat - 1)[:, None]
+    j = np.arange(n_lon)[None, :]
+    a = i * n_lon + j
+    b2 = i * n_lon + (j + 1) % n_lon
+    c = (i + 1) * n_lon + j
+    d = (i + 1) * n_lon + (j + 1) % n_lon
+    t1 = np.stack([a, c, b2], axis=-1).reshape(-1, 3)
+    t2 = np.stack([b2, c, d], axis=-1).reshape(-1, 3)
+    tris = np.stack([t1, t2], axis=1).reshape(-1, 3)
+    return dirs, tris
+
+
+def displaced_sphere(resolution: int = 724, amplitude: float = 0.05, octaves: int = 8,
+                     seed: int = 2, scale: float = 16.0) -> Scene:
+    """Grid sphere (resolution x resolution vertices), radius 1 displaced radially by
+    value-noise fBm of the given amplitude, then scaled uniformly.
+
+    At resolution 724 this is 2*723*724 = 1,046,904 triangles.  The scale factor
+    16 keeps triangles clear of the reference's absolute |det| < 1e-4 cull,
+    which rejects every triangle of the unit-radius mesh.
+    """
+    dirs, tris = _uv_sphere(resolution, resolution)
+    r = 1.0 + amplitude * value_noise(dirs, octaves, seed)
+    verts = (dirs * (r * scale)[:, None]).astype(np.float32)
+    mats = np.array([material(albedo=(0.7, 0.7, 0.7), roughness=1.0)])
+    inst = np.array([[0, tris.shape[0], 0]], dtype=np.uint32)
+    cam = Camera(position=(0.0, 0.0, 3.0 * scale), target=(0.0, 0.0, 0.0), fov_deg=45.0)
+    return Scene(verts, tris.astype(np.uint32), inst, mats, np.zeros((0, 16), np.float32),
+                 (0.0, 0.0, 0.0), cam, "displaced_sphere").contiguous()
+
+
+def _normalize_f32(v: np.ndarray) -> np.ndarray:
+    v = v.astype(np.float32)
+    n = np.sqrt((v * v).sum(axis=1, dtype=np.float32)).astype(np.float32)
+    return (v / n[:, None]).astype(np.float32)
+
+
+def primary_rays(camera: Camera, width: int, height: int) -> np.ndarray:
+    """Pinhole rays through pixel centres, (N,6) float32 rows o3,d3, row-major pixels."""
+    pos = np.array(camera.position, np.float64)
+    fwd = np.array(camera.target, np.float64) - pos
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, np.array(camera.up, np.float64))
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    th = math.tan(0.5 * math.radians(camera.fov_deg))
+    aspect = width / height
+    xs = (2.0 * (np.arange(width) + 0.5) / width - 1.0) * aspect * th
+    ys = (1.0 - 2.0 * (np.arange(height) + 0.5) / height) * th
+    nx, ny = np.meshgrid(xs, ys)
+    d = fwd[None, :] + right[None, :] * nx.reshape(-1, 1) + up[None, :] * ny.reshape(-1, 1)
+    d = _normalize_f32(d)
+    o = np.broadcast_to(pos.astype(np.float32), d.shape)
+    return np.ascontiguousarray(np.concatenate([o, d], axis=1), dtype=np.float32)
+
+
+def random_rays(n: int, half_extent: float, seed: int) -> np.ndarray:
+    """Origins uniform in [-h,h]^3, directions uniform on the unit sphere; (n,6) float32."""
+    st = Stream(seed)
+    ox, oy, oz = (st.uniform_np(n) * 2.0 - 1.0) * half_extent, (st.uniform_np(n) * 2.0 - 1.0) * half_extent, \
+                 (st.uniform_np(n) * 2.0 - 1.0) * half_extent
+    z = 1.0 - 2.0 * st.uniform_np(n)
+    ph = 2.0 * math.pi * st.uniform_np(n)
+    rr = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    d = _normalize_f32(np.stack([rr * np.cos(ph), rr * np.sin(ph), z], axis=1))
+    o = np.stack([ox, oy, oz], axis=1).astype(np.float32)
+    return np.ascontiguousarray(np.concatenate([o, d], axis=1), dtype=np.float32)
+
+
+def ray_query_rays(scene: Scene, primary_side: int = 2048, random_count: int = 4194304,
+                   scale: float = 16.0, seed: int = 3) -> np.ndarray:
+    """The ray-query workload: primary_side^2 coherent camera rays followed by
+    random_count incoherent rays (origins in [-1.5,1.5]^3 * scale)."""
+    prim = primary_rays(scene.camera, primary_side, primary_side)
+    rnd = random_rays(random_count, 1.5 * scale, seed)
+    return np.ascontiguousarray(np.concatenate([prim, rnd], axis=0))
+
+
+# ----------------------------------------------------------------- sphere grid
+def _displaced_unit_sphere_mesh(n_lat: int, n_lon: int, amplitude: float, seed: int, octaves: int = 4):
+    dirs, tris = _uv_sphere(n_lat, n_lon)
+    r = 1.0 + amplitude * value_noise(dirs, octaves, seed)
+    return dirs * r[:, None], tris
+
+
+def sphere_field(grid: int, n_lat: int, n_lon: int, seed: int, spacing: float = 3.0, radius: float = 1.0,
+                 n_lights: int = 16, environment: float = 0.1, light_size: float = 6.0,
+                 light_height: float = 14.0) -> Scene:
+    """grid x grid displaced spheres with the mixed material set:
+    50% Lambert (albedo U[0.05,0.9]^3), 30% glossy (roughness U[0.05,0.5], F0 U[0.02,0.9]),
+    20% mirror; n_lights quad area lights with radiance U[1,20]^3; constant environment.
+
+    "GGX glossy (roughness, F0)" maps onto the reference's glossy lobe: a
+    roughness-driven Phong lobe with ior = (1+sqrt(F0))/(1-sqrt(F0)), since the
+    reference integrator has no GGX (src/pathtracer/ScalarCpuPathTracer.cpp:1240-1251).
+    """
+    st = Stream(seed)
+    b = _Builder()
+    mats: list = []
+    lights: list = []
+    # A handful of distinct sphere shapes, instanced by translation (vertices are baked).
+    shapes = [_displaced_unit_sphere_mesh(n_lat, n_lon, 0.05, seed * 17 + k) for k in range(8)]
+    half = 0.5 * (grid - 1) * spacing
+    for gy in range(grid):
+        for gx in range(grid):
+            dirs, tris = shapes[st.randint(0, len(shapes) - 1)]
+            center = np.array([gx * spacing - half, radius, gy * spacing - half])
+            pick = st.uniform()
+            if pick < 0.5:
+                alb = tuple(st.uniform(0.05, 0.9) for _ in range(3))
+                mats.append(material(albedo=alb, roughness=1.0, model=0))
+            elif pick < 0.8:
+                alb = tuple(st.uniform(0.05, 0.9) for _ in range(3))
+                rough = st.uniform(0.05, 0.5)
+                f0 = st.uniform(0.02, 0.9)
+                sf = math.sqrt(f0)
+                ior = (1.0 + sf) / max(1e-6, 1.0 - sf)
+                mats.append(material(albedo=alb, roughness=rough, model=3, ior=ior))
+            else:
+                alb = tuple(st.uniform(0.7, 0.98) for _ in range(3))
+                mats.append(material(albedo=alb, roughness=0.0, model=2))
+            b.add(center[None, :] + dirs * radius, tris, len(mats) - 1)
+    # Ground plane under the field.
+    mats.append(material(albedo=(0.5, 0.5, 0.5), roughness=1.0))
+    g = half + 2.0 * spacing
+    v, t = _quad((-g, 0.0, -g), (-g, 0.0, g), (g, 0.0, g), (g, 0.0, -g))
+    b.add(v, t, len(mats) - 1)
+    # Quad area lights on a 4x4 lattice above the field.
+    side = int(math.ceil(math.sqrt(n_lights)))
+    for k in range(n_lights):
+        lx = ((k % side) + 0.5) / side * 2.0 * half - half
+        lz = ((k // side) + 0.5) / side * 2.0 * half - half
+        le = tuple(st.uniform(1.0, 20.0) for _ in range(3))
+        hs = 0.5 * light_size
+        mats.append(material(albedo=(0.78, 0.78, 0.78), emissive=le, roughness=1.0))
+        v, t = _quad((lx - hs, light_height, lz - hs), (lx + hs, light_height, lz - hs),
+                     (lx + hs, light_height, lz + hs), (lx - hs, light_height, lz + hs))
+        b.add(v, t, len(mats) - 1)
+        lights.append(point_light((lx, light_height - 0.001, lz), le, light_size * light_size))
+    v, t, inst = b.arrays()
+    cam = Camera(position=(0.0, 0.55 * half + 6.0, half + 0.45 * half), target=(0.0, 0.0, 0.1 * half),
+                 fov_deg=50.0)
+    return Scene(v, t, inst, np.array(mats), np.array(lights),
+                 (environment, environment, environment), cam, f"sphere_field_{grid}").contiguous()
+
+
+def sphere_grid(seed: int = 4, grid: int = 64) -> Scene:
+    """64x64 displaced spheres of 2*14*18 = 504 triangles: 2,064,386 triangles with lights and ground."""
+    return sphere_field(grid, 15, 18, seed)
+
+
+def sphere_grid_settings(width=1920, height=1080, spp=64) -> RenderSettings:
+    return RenderSettings(width=width, height=height, spp=spp, max_depth=16, seed=1234,
+                          enable_nee=True, enable_mis=True, firefly_clamp=10.0)
+
+
+# ---------------------------------------------------------------- batched jobs
+@dataclasses.dataclass
+class Job:
+    scene: Scene
+    settings: RenderSettings
+    target_triangles: int
+
+
+def _log_uniform(st: Stream, lo: float, hi: float) -> float:
+    return math.exp(st.uniform(math.log(lo), math.log(hi)))
+
+
+def batch_jobs(count: int = 64, seed: int = 5, max_triangles: int = 500_000, max_side: int = 1024,
+               min_triangles: int = 1_000, min_side: int = 128) -> List[Job]:
+    """Uneven render jobs: triangle count log-uniform in [min,max], square side
+    log-uniform in [min_side,max_side], spp in {4,8,16,32,64}, depth in {4,8,16},
+    the sphere-field material mix; each job's seeds derive from the master seed."""
+    st = Stream(seed)
+    jobs = []
+    for k in range(count):
+        tris = _log_uniform(st, min_triangles, max_triangles)
+        side = int(round(_log_uniform(st, min_side, max_side)))
+        spp = [4, 8, 16, 32, 64][st.randint(0, 4)]
+        depth = [4, 8, 16][st.randint(0, 2)]
+        job_seed = st.next_u64() & 0xFFFFFFFF
+        # Choose sphere resolution and grid so grid^2 * 2*(n_lat-1)*n_lon ~ tris.
+        n_lat, n_lon = 15, 18
+        per = 2 * (n_lat - 1) * n_lon
+        grid = max(1, int(round(math.sqrt(tris / per))))
+        if grid * grid * per > max_triangles * 1.2:
+            grid = max(1, grid - 1)
+        scene = sphere_field(grid, n_lat, n_lon, job_seed % 100000 + 7, n_lights=min(16, max(1, grid)),
+                             light_size=max(1.0, 0.1 * grid * 3.0), light_height=max(4.0, 0.25 * grid * 3.0))
+        settings = RenderSettings(width=side, height=side, spp=spp, max_depth=depth, seed=job_seed,
+                                  enable_nee=True, enable_mis=True, firefly_clamp=10.0)
+        jobs.append(Job(scene, settings, int(tris)))
+    return jobs
+
+
+# -------------------------------------------------------- inverse rendering
+def inverse_box_scene(params: Optional[np.ndarray] = None, seed: int = 6, n_objects: int = 16) -> Scene:
+    """Box room + n_objects seeded boxes (12 tris each).  params is the (n_objects,4)
+    vector of per-object RGB albedo and roughness; None draws the held-out
+    target parameters U[0.1,0.8]."""
+    st = Stream(seed)
+    b = _Builder()
+    mats: list = []
+    lights: list = []
+    _room(b, mats, Stream(seed + 1000))
+    if params is None:
+        pst = Stream(seed + 2000)
+        params = np.array([[pst.uniform(0.1, 0.8) for _ in range(4)] for _ in range(n_objects)], np.float32)
+    params = np.asarray(params, np.float32).reshape(n_objects, 4)
+    for k in range(n_objects):
+        cx = st.uniform(-0.38, 0.38)
+        cz = st.uniform(-0.38, 0.38)
+        hy = st.uniform(0.03, 0.12)
+        hx = st.uniform(0.03, 0.07)
+        hz = st.uniform(0.03, 0.07)
+        cy = st.uniform(hy, 0.7)
+        yaw = st.uniform(-30.0, 30.0)
+        mats.append(material(albedo=tuple(params[k, :3]), roughness=float(params[k, 3]), model=3, ior=1.5))
+        v, t = _box((cx, cy, cz), (hx, hy, hz), yaw)
+        b.add(v, t, len(mats) - 1)
+    _ceiling_light(b, mats, lights)
+    v, t, inst = b.arrays()
+    cam = Camera(position=(0.0, 0.5, 1.9), target=(0.0, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0)
+    return Scene(v, t, inst, np.array(mats), np.array(lights), (0.0, 0.0, 0.0), cam, "inverse_box").contiguous()
+
+
+def inverse_settings(width=128, height=128, spp=32) -> RenderSettings:
+    return RenderSettings(width=width, height=height, spp=spp, max_depth=6, seed=4321,
+                          enable_nee=True, enable_mis=True)
