@@ -1,0 +1,240 @@
+/*
+ * vkptc.h -- C ABI of libvkpt_cuda, the sm_100a render backend for vkPathTracer.
+ *
+ * This is the boundary a `src/gpu/cuda` IPathTracer adapter in the reference
+ * binds.  Plain pointers and sizes only; every call
+ * returns a vkptc_status_code (the numeric values of vkpt::core::StatusCode,
+ * src/core/contracts/Result.h:13-23) and never throws.  Host buffers passed
+ * in are read or written synchronously before the call returns; the context
+ * owns all device memory (scene, BVH, film, path queues).
+ *
+ * Threading: one thread drives a context (the reference's contract for an
+ * IPathTracer, src/render/RenderCoordinator.cpp:412); distinct contexts may
+ * be driven concurrently.
+ *
+ * Record layouts follow the reference's standard GPU word maps
+ * (src/pathtracer/PathTracer.h:778-786, src/gpu/VulkanGpuPathTracer.cpp:323-396):
+ *   material[16] = albedo3, emissive3, roughness, model, metallic, ior,
+ *                  transmission, clearcoat, sheen, anisotropy, alpha,
+ *                  effect | (double_sided << 10)
+ *   light[16]    = position3, color3, intensity, radius, direction3,
+ *                  spot_inner_cos, spot_outer_cos, 0, 0, 0
+ */
+#ifndef VKPTC_H
+#define VKPTC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VKPTC_ABI_VERSION 1u
+
+typedef enum vkptc_status {
+  VKPTC_OK = 0,
+  VKPTC_UNSUPPORTED = 1,
+  VKPTC_INVALID_ARGUMENT = 2,
+  VKPTC_NOT_READY = 3,
+  VKPTC_BUSY = 4,
+  VKPTC_ALLOC_FAILED = 5,
+  VKPTC_TIMEOUT = 6,
+  VKPTC_CANCELLED = 7,
+  VKPTC_INTERNAL_ERROR = 8
+} vkptc_status_code;
+
+/* Mirrors PathTracerLifecycle (src/pathtracer/PathTracer.h:485-491). */
+typedef enum vkptc_lifecycle {
+  VKPTC_UNINITIALIZED = 0,
+  VKPTC_CONFIGURED = 1,
+  VKPTC_SCENE_LOADED = 2,
+  VKPTC_READY = 3,
+  VKPTC_FAILED = 4
+} vkptc_lifecycle;
+
+typedef struct vkptc_ctx vkptc_ctx;
+
+typedef struct vkptc_config {
+  int32_t device;            /* CUDA device ordinal */
+  uint32_t block_size;       /* threads per block of the wavefront kernels; 0 = autotuned/default */
+  uint32_t stack_depth;      /* traversal stack entries per thread in shared memory; 0 = from the BVH */
+  uint32_t math_mode;        /* 0 = parity (transcendentals in FP64, rounded once), 1 = fast FP32 */
+  uint32_t collect_stats;    /* 1 = count node/leaf/triangle visits (device counters) */
+  uint32_t reserved[3];
+} vkptc_config;
+
+/* Mirrors RenderSettings (src/pathtracer/PathTracer.h:134-178). */
+typedef struct vkptc_render_settings {
+  uint32_t width;
+  uint32_t height;
+  uint32_t spp;
+  uint32_t max_depth;
+  uint64_t seed;
+  uint32_t enable_nee;
+  uint32_t enable_mis;
+  uint32_t deterministic;
+  uint32_t rr_start_depth;
+  float rr_min_survival;
+  float rr_max_survival;
+  float camera_aperture_radius;
+  float camera_focus_distance;
+  float firefly_clamp;       /* extension: per-channel clamp of each sample, 0 = off (reference) */
+  uint32_t reserved;
+} vkptc_render_settings;
+
+/* POD view of PathTracerSceneSnapshot (src/pathtracer/PathTracer.h:358-409):
+ * the triangle subset the render path consumes. */
+typedef struct vkptc_scene_view {
+  const float* vertices;       uint32_t vertex_count;     /* xyz per vertex */
+  const uint32_t* indices;     uint32_t index_count;      /* 3 per triangle */
+  const uint32_t* instances;   uint32_t instance_count;   /* first_triangle, triangle_count, material_index */
+  const float* materials;      uint32_t material_count;   /* 16 floats each */
+  const float* lights;         uint32_t light_count;      /* 16 floats each */
+  float environment[3];
+  float camera_position[3];
+  float camera_target[3];
+  float camera_up[3];
+  float camera_fov_deg;
+  float camera_aperture_radius;
+  float camera_focus_distance;
+} vkptc_scene_view;
+
+/* Binary BVH as ParallelBvhBuilder returns it (src/cpu/ParallelBvhBuilder.h:22-39):
+ * per node min3, max3 (f32) then left, right, first_prim, prim_count (i32). */
+typedef struct vkptc_bvh_view {
+  const uint32_t* nodes;       /* 10 words per node */
+  uint32_t node_count;
+  const uint32_t* prim_indices;
+  uint32_t prim_count;
+} vkptc_bvh_view;
+
+/* Mirrors RenderTile (src/pathtracer/PathTracer.h:914-922). */
+typedef struct vkptc_tile {
+  uint32_t x, y, width, height;
+  uint32_t sample_index;
+  uint32_t tile_id;
+  uint32_t gpu_id;
+} vkptc_tile;
+
+/* Mirrors SampleCounters (src/pathtracer/PathTracer.h:218-230); the
+ * traversal counters count this backend's wide-BVH work. */
+typedef struct vkptc_counters {
+  uint64_t samples;
+  uint64_t rays;               /* bounce segments, the reference's definition */
+  uint64_t triangle_tests;
+  uint64_t sdf_tests;
+  uint64_t sdf_steps;
+  uint64_t triangle_hits;
+  uint64_t sdf_hits;
+  uint64_t sdf_misses;
+  uint64_t bvh_node_visits;
+  uint64_t bvh_leaf_visits;
+  uint64_t shadow_tests;
+} vkptc_counters;
+
+/* Mirrors PathTracerStatus (src/pathtracer/PathTracer.h:854-865). */
+typedef struct vkptc_tracer_status {
+  uint32_t lifecycle;          /* vkptc_lifecycle */
+  uint32_t scene_loaded;
+  uint32_t accel_valid;
+  uint32_t ready_to_render;
+  uint32_t current_sample;
+  uint32_t reserved;
+  uint64_t last_sample_us;
+  uint64_t total_samples;
+  uint64_t accumulation_gen;
+} vkptc_tracer_status;
+
+typedef struct vkptc_accel_info {
+  uint32_t primitive_count;
+  uint32_t binary_node_count;
+  uint32_t binary_leaf_count;
+  uint32_t wide_node_count;
+  uint32_t wide_depth;
+  uint32_t stack_required;     /* traversal stack entries the BVH can need */
+  double build_ms;
+  uint64_t device_bytes;       /* BVH + triangle bytes resident in HBM */
+} vkptc_accel_info;
+
+#define VKPTC_QUERY_CLOSEST 0u
+#define VKPTC_QUERY_ANY 1u
+
+/* ---- lifecycle --------------------------------------------------------------
+ * replaces: the IPathTracer object itself (src/pathtracer/PathTracer.h:1069-1184) */
+int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx);
+int32_t vkptc_destroy(vkptc_ctx* ctx);
+/* replaces IPathTracer::configure (src/pathtracer/PathTracer.h:1074) */
+int32_t vkptc_configure(vkptc_ctx* ctx, const vkptc_render_settings* settings);
+/* replaces IPathTracer::load_scene_snapshot (src/pathtracer/PathTracer.h:1088) */
+int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene);
+/* replaces IPathTracer::build_or_update_acceleration (src/pathtracer/PathTracer.h:1092):
+ * builds the binary midpoint BVH on the host exactly as ParallelBvhBuilder
+ * does (deterministic mode) and flattens it into the wide HBM layout. */
+int32_t vkptc_build_acceleration(vkptc_ctx* ctx);
+/* Same, from an externally built binary BVH (the reference's ParallelBvhBuilder
+ * output over the accelerator's primitive order, CpuBvhAccelerator.cpp:247-256). */
+int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh);
+int32_t vkptc_get_accel_info(vkptc_ctx* ctx, vkptc_accel_info* out);
+/* Host-only (no device needed): the binary BVH vkptc_build_acceleration
+ * builds, in ParallelBvhBuilder's layout, for callers that keep a CPU copy.
+ * replaces ParallelBvhBuilder::build (src/cpu/ParallelBvhBuilder.cpp:165-257)
+ * as CpuBvhAccelerator::build calls it (deterministic, leaf threshold 4).
+ * nodes_out: capacity 2*prims-1 nodes of 10 words; prim_out: capacity prims.
+ * *node_count and *prim_count receive the sizes. */
+int32_t vkptc_build_binary_bvh(const vkptc_scene_view* scene, uint32_t* nodes_out, uint32_t* node_count,
+                               uint32_t* prim_out, uint32_t* prim_count);
+/* replaces IPathTracer::reset_accumulation (src/pathtracer/PathTracer.h:1096) */
+int32_t vkptc_reset(vkptc_ctx* ctx);
+/* replaces IPathTracer::shutdown (src/pathtracer/PathTracer.h:1182) */
+int32_t vkptc_shutdown(vkptc_ctx* ctx);
+
+/* ---- rendering --------------------------------------------------------------
+ * replaces IPathTracer::render_tile / render_tile_cancellable / render_tiles
+ * (src/pathtracer/PathTracer.h:1142-1170).  Each tile renders one sample
+ * (tile.sample_index) of frame `frame` for every pixel it covers.  cancel_flag
+ * (may be NULL) is polled before each tile; a set flag returns VKPTC_CANCELLED. */
+int32_t vkptc_render(vkptc_ctx* ctx, const vkptc_tile* tiles, uint32_t tile_count, uint32_t frame,
+                     const volatile int32_t* cancel_flag);
+/* Renders samples [first_sample, first_sample + sample_count) of the full
+ * frame; the samples are independent, so this is the batched form of
+ * sample_count full-frame render_tile calls. */
+int32_t vkptc_render_frame(vkptc_ctx* ctx, uint32_t first_sample, uint32_t sample_count, uint32_t frame);
+/* Blocks until queued device work is done. */
+int32_t vkptc_synchronize(vkptc_ctx* ctx);
+
+/* ---- film ---------------------------------------------------------------------
+ * replaces IPathTracer::film() / FilmBuffer raw access (src/pathtracer/PathTracer.h:937-974):
+ * sum_rgb (3*W*H floats), count (W*H), invalid (W*H); any may be NULL. */
+int32_t vkptc_read_film(vkptc_ctx* ctx, float* sum_rgb, uint32_t* count, float* invalid);
+/* replaces IPathTracer::resolve_hdr / FilmBuffer::resolve_hdr (src/pathtracer/FilmBuffer.cpp:160-214) */
+int32_t vkptc_resolve_hdr(vkptc_ctx* ctx, float* rgb);
+/* replaces IPathTracer::replace_film_history (src/pathtracer/PathTracer.h:1099):
+ * loads a saved film (resume = reload the film, continue at the next sample). */
+int32_t vkptc_write_film(vkptc_ctx* ctx, const float* sum_rgb, const uint32_t* count, const float* invalid);
+/* replaces IPathTracer::read_counters (src/pathtracer/PathTracer.h:1180) */
+int32_t vkptc_read_counters(vkptc_ctx* ctx, vkptc_counters* out);
+/* replaces IPathTracer::status (src/pathtracer/PathTracer.h:1181) */
+int32_t vkptc_get_status(vkptc_ctx* ctx, vkptc_tracer_status* out);
+/* Last error message of this context (empty when none); valid until the next call. */
+const char* vkptc_last_error(vkptc_ctx* ctx);
+
+/* ---- ray queries --------------------------------------------------------------
+ * replaces IRayAccelerator::intersect (src/pathtracer/PathTracer.h:1001-1036), one
+ * virtual call per ray there, batched here.  rays: 6 floats per ray (origin,
+ * direction), HOST memory.  tmax (may be NULL = +inf) bounds any-hit queries.
+ * prim_out: the hit primitive's index in the accelerator's flattened order
+ * (RayQueryHit::primitive_index) or 0xFFFFFFFF; t_out (may be NULL): distance.
+ * For VKPTC_QUERY_ANY, prim_out[i] is 1 when occluded before tmax, else 0. */
+int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, uint64_t ray_count,
+                         uint32_t mode, uint32_t* prim_out, float* t_out);
+/* Same with DEVICE pointers already resident in HBM, enqueued on `stream`
+ * (a cudaStream_t; 0 = the context's stream).  No host synchronisation. */
+int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float* d_tmax, uint64_t ray_count,
+                                uint32_t mode, uint32_t* d_prim_out, float* d_t_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VKPTC_H */

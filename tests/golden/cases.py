@@ -1,0 +1,91 @@
+"""Small parity cases shared by the golden fixtures and the parity tests.
+
+Each case: (scene factory, render-settings factory or None, ray factory or None).
+Sizes are chosen so the CPU oracle finishes each in well under a second.
+"""
+import numpy as np
+
+from vkpathtracer_b200 import scenes
+
+
+def _box():
+    return scenes.cornell_box(seed=1)
+
+
+def _box_settings():
+    return scenes.RenderSettings(width=48, height=40, spp=3, max_depth=8, seed=1234, enable_nee=True, enable_mis=True)
+
+
+def _box_rays(scene):
+    prim = scenes.primary_rays(scene.camera, 64, 48)
+    rnd = scenes.random_rays(2048, 0.45, seed=11)
+    rnd[:, 1] += 0.5   # origins inside the room
+    return np.ascontiguousarray(np.concatenate([prim, rnd]))
+
+
+def _field():
+    return scenes.sphere_field(3, 9, 10, seed=21, n_lights=3, light_size=1.5, light_height=5.0)
+
+
+def _field_settings():
+    return scenes.RenderSettings(width=40, height=30, spp=2, max_depth=6, seed=77, enable_nee=True, enable_mis=True)
+
+
+def _field_rays(scene):
+    return scenes.primary_rays(scene.camera, 48, 36)
+
+
+def _sphere():
+    return scenes.displaced_sphere(resolution=64, amplitude=0.05, octaves=8, seed=2, scale=16.0)
+
+
+def _sphere_rays(scene):
+    return scenes.ray_query_rays(scene, primary_side=48, random_count=4096, scale=16.0, seed=3)
+
+
+CASES = {
+    "box": (_box, _box_settings, _box_rays),
+    "field": (_field, _field_settings, _field_rays),
+    "sphere": (_sphere, None, _sphere_rays),
+}
+
+
+# ---- fixture (de)serialisation: the fixtures carry their exact inputs
+def scene_to_arrays(scene):
+    c = scene.camera
+    return {
+        "vertices": scene.vertices, "indices": scene.indices, "instances": scene.instances,
+        "materials": scene.materials, "lights": scene.lights,
+        "environment": np.array(scene.environment, np.float32),
+        "camera": np.array(list(c.position) + list(c.target) + list(c.up) +
+                           [c.fov_deg, c.aperture_radius, c.focus_distance], np.float32),
+    }
+
+
+def scene_from_arrays(d):
+    cam = d["camera"].astype(np.float64)
+    camera = scenes.Camera(tuple(cam[0:3]), tuple(cam[3:6]), tuple(cam[6:9]), float(cam[9]), float(cam[10]),
+                           float(cam[11]))
+    return scenes.Scene(d["vertices"], d["indices"], d["instances"], d["materials"], d["lights"],
+                        tuple(float(x) for x in d["environment"]), camera, "fixture").contiguous()
+
+
+def settings_to_arrays(st):
+    return {"settings": np.array([st.width, st.height, st.spp, st.max_depth, st.seed, int(st.enable_nee),
+                                  int(st.enable_mis), st.russian_roulette_start_depth], np.uint64),
+            "settings_rr": np.array([st.russian_roulette_min_survival, st.russian_roulette_max_survival], np.float32)}
+
+
+def settings_from_arrays(d):
+    a = [int(x) for x in d["settings"]]
+    rr = d["settings_rr"]
+    return scenes.RenderSettings(width=a[0], height=a[1], spp=a[2], max_depth=a[3], seed=a[4],
+                                 enable_nee=bool(a[5]), enable_mis=bool(a[6]), russian_roulette_start_depth=a[7],
+                                 russian_roulette_min_survival=float(rr[0]),
+                                 russian_roulette_max_survival=float(rr[1]))
+
+
+def load_fixture(name):
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"{name}.npz")
+    return dict(np.load(path))

@@ -1,0 +1,262 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+* Closest-hit primitive ids and distances: bit-exact.
+* Any-hit: exactly the oracle's (closest t < tmax).
+* Films: per-pixel agreement with the oracle at the same seed and spp --
+  bit-identical for the pixels whose paths take no transcendental whose
+  last bit differs from glibc's, and within a stated RMSE and a 3-sigma
+  per-pixel mean test over the oracle's own per-sample spread.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tests.golden import cases
+from vkpathtracer_b200 import native, scenes
+from vkpathtracer_b200.tracer import CudaPathTracer, RenderTile
+
+pytestmark = pytest.mark.gpu
+
+# Film tolerances (float32 radiance, same seed and spp as the oracle).
+RMSE_REL_TOL = 1e-3        # RMSE(gpu - oracle) / mean(oracle)
+SIGMA3_FAIL_FRAC = 0.003   # fraction of pixel channels allowed outside 3 sigma
+BIT_EXACT_FRAC = 0.97      # fraction of pixels expected bit-identical in parity math mode
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def make_tracer(scene, st, **kw):
+    t = CudaPathTracer(**kw)
+    assert t.configure(st)
+    assert t.load_scene_snapshot(scene)
+    assert t.build_or_update_acceleration()
+    assert t.reset_accumulation()
+    return t
+
+
+def film_report(gpu_sum, ref_sum, ref_samples, spp):
+    g = gpu_sum / spp
+    r = ref_sum / spp
+    diff = g - r
+    rmse = float(np.sqrt(np.mean(diff ** 2)))
+    mean = float(np.mean(r)) + 1e-12
+    if ref_samples is not None and ref_samples.shape[0] > 1:
+        sd = np.std(ref_samples, axis=0, ddof=1) / np.sqrt(ref_samples.shape[0])
+        fail = np.abs(diff) > 3.0 * sd + 1e-6 * (1.0 + np.abs(r))
+        sigma3 = float(np.mean(fail))
+    else:
+        sigma3 = 0.0
+    exact = float(np.mean(np.all(bits(gpu_sum) == bits(ref_sum), axis=-1)))
+    return {"rmse_rel": rmse / mean, "sigma3_fail": sigma3, "bit_exact": exact}
+
+
+# ------------------------------------------------------------------ hit ids
+@pytest.mark.parametrize("name", ["box", "field", "sphere"])
+def test_closest_hit_ids_bit_exact_vs_reference_golden(name):
+    d = cases.load_fixture(name)
+    sc = cases.scene_from_arrays(d)
+    st = scenes.RenderSettings(width=8, height=8, spp=1)
+    with make_tracer(sc, st) as t:
+        p, tt = t.trace_rays(d["rays"])
+    assert np.array_equal(p, d["hit_prim"]), f"{np.sum(p != d['hit_prim'])} mismatching ids"
+    assert np.array_equal(bits(tt), bits(d["hit_t"]))
+
+
+def test_closest_hit_ids_bit_exact_larger_sphere():
+    sc = scenes.displaced_sphere(resolution=256, seed=2)
+    rays = scenes.ray_query_rays(sc, primary_side=256, random_count=65536, seed=4)
+    o = oracle.load("auto")
+    pr, tr, _, _ = o.intersect(sc, rays, threads=8)
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+        p, tt = t.trace_rays(rays)
+        info = t.accel_info()
+    assert info["primitive_count"] == sc.triangle_count
+    assert np.array_equal(p, pr), f"{np.sum(p != pr)} mismatching ids of {len(p)}"
+    assert np.array_equal(bits(tt), bits(tr))
+
+
+def test_exact_ties_follow_reference_visit_order():
+    """Rays through shared quad diagonals and box edges produce exact-t ties."""
+    sc = scenes.cornell_box(seed=1)
+    cam = sc.camera
+    rays = scenes.primary_rays(cam, 512, 512)
+    o = oracle.load("auto")
+    pr, tr, _, _ = o.intersect(sc, rays, threads=8)
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+        p, tt = t.trace_rays(rays)
+    assert np.array_equal(p, pr)
+    assert np.array_equal(bits(tt), bits(tr))
+
+
+def test_parallel_axis_rays_match_reference_rule():
+    sc = scenes.displaced_sphere(resolution=64, seed=5)
+    rng = np.random.default_rng(7)
+    n = 20000
+    o = rng.uniform(-30, 30, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d[: n // 3, 1] = rng.uniform(-1e-4, 1e-4, n // 3)
+    d[n // 3: 2 * n // 3, 2] = 0.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.ascontiguousarray(np.concatenate([o, d.astype(np.float32)], 1), np.float32)
+    pr, tr, _, _ = oracle.load("auto").intersect(sc, rays, threads=8)
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+        p, tt = t.trace_rays(rays)
+    assert np.array_equal(p, pr)
+
+
+def test_any_hit_equals_closest_hit_before_tmax():
+    d = cases.load_fixture("sphere")
+    sc = cases.scene_from_arrays(d)
+    rays = d["rays"]
+    tref = d["hit_t"]
+    rng = np.random.default_rng(3)
+    tmax = np.where(np.isfinite(tref), tref * rng.uniform(0.5, 1.5, tref.shape), rng.uniform(1, 80, tref.shape))
+    tmax = tmax.astype(np.float32)
+    tmax[:50] = tref[:50]          # t == tmax exactly: not occluded (strict)
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+        occ, _ = t.trace_rays(rays, mode=native.QUERY_ANY, tmax=tmax)
+        occ_inf, _ = t.trace_rays(rays, mode=native.QUERY_ANY)
+    expect = (tref < tmax) & np.isfinite(tref)
+    assert np.array_equal(occ.astype(bool), expect)
+    assert np.array_equal(occ_inf.astype(bool), np.isfinite(tref))
+
+
+def test_external_bvh_gives_same_hits():
+    d = cases.load_fixture("field")
+    sc = cases.scene_from_arrays(d)
+    nodes, prim = oracle.load("auto").build_bvh(sc)
+    t = CudaPathTracer()
+    assert t.configure(scenes.RenderSettings(width=8, height=8, spp=1))
+    assert t.load_scene_snapshot(sc)
+    assert t.load_bvh(nodes, prim)
+    p, _ = t.trace_rays(d["rays"])
+    t.close()
+    assert np.array_equal(p, d["hit_prim"])
+
+
+# ------------------------------------------------------------------ films
+@pytest.mark.parametrize("name", ["box", "field"])
+def test_film_matches_reference_golden(name):
+    d = cases.load_fixture(name)
+    sc, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
+    with make_tracer(sc, st) as t:
+        for s in range(st.spp):
+            assert t.render_tile(RenderTile(0, 0, st.width, st.height, s), 0)
+        g, cnt, inv = t.film()
+        c = t.read_counters()
+    assert np.array_equal(cnt, d["film_count"])
+    rep = film_report(g, d["film_sum"], d["samples"], st.spp)
+    print(name, rep)
+    assert rep["rmse_rel"] < RMSE_REL_TOL
+    assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
+    assert rep["bit_exact"] >= BIT_EXACT_FRAC
+    assert c["samples"] == int(d["counters"][0])
+
+
+def test_film_matches_oracle_sphere_field_mixed_materials():
+    sc = scenes.sphere_field(8, 15, 18, seed=4, light_size=3.0, light_height=8.0)
+    st = scenes.RenderSettings(width=96, height=64, spp=4, max_depth=10, seed=1234)
+    ref = oracle.load("auto").render(sc, st, threads=8, per_sample=True)
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp)
+        g, cnt, _ = t.film()
+    rep = film_report(g, ref["sum"], ref["samples"], st.spp)
+    print(rep)
+    assert np.array_equal(cnt, ref["count"])
+    assert rep["rmse_rel"] < RMSE_REL_TOL
+    assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
+
+
+def test_render_frame_batches_equal_per_tile_calls():
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(40, 32, 5)
+    with make_tracer(sc, st) as a:
+        for s in range(st.spp):
+            assert a.render_tile(RenderTile(0, 0, 40, 32, s), 0)
+        fa, ca, _ = a.film()
+    with make_tracer(sc, st, wave_paths=40 * 32 * 2) as b:
+        b.render_frame(0, st.spp)
+        fb, cb, _ = b.film()
+    assert np.array_equal(bits(fa), bits(fb)) and np.array_equal(ca, cb)
+
+
+def test_tiles_equal_full_frame_and_partial_tile_touches_only_its_pixels():
+    """The reference's CheckScalarRenderTilePrimitive (tests/snapshot_bus_smoke.cpp:1368-1435)."""
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(40, 32, 2)
+    with make_tracer(sc, st) as full, make_tracer(sc, st) as tiled, make_tracer(sc, st) as part:
+        for s in range(2):
+            assert full.render_tile(RenderTile(0, 0, 40, 32, s), 0)
+            assert tiled.render_tiles([RenderTile(0, 0, 40, 16, s), RenderTile(0, 16, 40, 16, s)], 0)
+        assert part.render_tile(RenderTile(8, 4, 10, 7, 0), 0)
+        ff, fc, _ = full.film()
+        tf, tc, _ = tiled.film()
+        pf, pc, _ = part.film()
+    assert np.array_equal(bits(ff), bits(tf)) and np.array_equal(fc, tc)
+    mask = np.zeros((32, 40), bool)
+    mask[4:11, 8:18] = True
+    assert np.all(pc[mask] == 1) and np.all(pc[~mask] == 0)
+    assert np.all(pf[~mask] == 0)
+
+
+def test_lifecycle_and_reset_preserve_acceleration():
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(16, 16, 1)
+    t = CudaPathTracer()
+    assert t.status().lifecycle == "uninitialized"
+    assert not t.render_tile(RenderTile(0, 0, 16, 16, 0), 0)
+    assert t.load_scene_snapshot(sc).code == native.NOT_READY
+    assert t.configure(st)
+    assert t.status().lifecycle == "configured"
+    assert t.build_or_update_acceleration().code == native.NOT_READY
+    assert t.load_scene_snapshot(sc)
+    assert t.status().lifecycle == "scene_loaded"
+    assert not t.render_tile(RenderTile(0, 0, 16, 16, 0), 0)
+    assert "acceleration" in t.status().last_error
+    assert t.build_or_update_acceleration()
+    s = t.status()
+    assert s.lifecycle == "ready" and s.ready_to_render
+    assert t.render_tile(RenderTile(0, 0, 16, 16, 0), 0)
+    a, _, _ = t.film()
+    gen = t.status().accumulation_gen
+    assert t.reset_accumulation()
+    s = t.status()
+    assert s.accel_valid and s.accumulation_gen == gen + 1 and s.total_samples == 0
+    assert t.render_tile(RenderTile(0, 0, 16, 16, 0), 0)
+    b, _, _ = t.film()
+    assert np.array_equal(bits(a), bits(b))
+    t.shutdown()
+    assert t.status().lifecycle == "uninitialized"
+    t.close()
+
+
+def test_resolve_hdr_and_film_resume():
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(24, 16, 4)
+    with make_tracer(sc, st) as a:
+        a.render_frame(0, 4)
+        fa, ca, _ = a.film()
+        hdr = a.resolve_hdr()
+    assert np.array_equal(bits(hdr), bits(fa * (np.float32(1.0) / ca[..., None].astype(np.float32))))
+    with make_tracer(sc, st) as b:
+        b.render_frame(0, 2)
+        half_f, half_c, _ = b.film()
+    with make_tracer(sc, st) as c:
+        assert c.replace_film_history(half_f, half_c)
+        c.render_frame(2, 2)
+        fc, cc, _ = c.film()
+    assert np.array_equal(bits(fa), bits(fc)) and np.array_equal(ca, cc)
+
+
+def test_fast_math_mode_is_statistically_equal():
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(48, 40, 16)
+    ref = oracle.load("auto").render(sc, st, threads=8, per_sample=True)
+    with make_tracer(sc, st, math_mode=1) as t:
+        t.render_frame(0, st.spp)
+        g, _, _ = t.film()
+    rep = film_report(g, ref["sum"], ref["samples"], st.spp)
+    print(rep)
+    assert rep["rmse_rel"] < 0.05

@@ -1,0 +1,331 @@
+// bvh_host.cpp -- primitive flattening, binary midpoint BVH, wide collapse.
+//
+// The binary builder must produce the same tree as the reference's
+// ParallelBvhBuilder in deterministic mode (src/cpu/ParallelBvhBuilder.cpp:61-257):
+// the traversal kernels reproduce the reference's closest-hit primitive ids
+// bit-exactly, and on exact distance ties that needs the reference's tree
+// (its depth-first near-first visiting order).  The steps are therefore the
+// reference's: node bounds = union of primitive boxes; split the widest
+// centroid axis at its midpoint; stable-partition by `centroid < split`;
+// fall back to count/2 when one side is empty; leaves hold <= 4 primitives;
+// child ids are allocated as (left, right) pairs in recursion order.
+#include "bvh_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <limits>
+#include <numeric>
+
+namespace vkptc {
+namespace {
+
+constexpr float kPad = 1e-4f;
+
+inline float lt_max(float a, float b) { return (a < b) ? b : a; }   // std::max order
+inline float lt_min(float a, float b) { return (b < a) ? b : a; }   // std::min order
+
+struct Builder {
+  const float* boxes;   // 6 per prim
+  std::vector<BinNode>* nodes;
+  uint32_t* base;
+  uint32_t leaf_threshold;
+  int32_t next_id = 1;
+
+  float centroid(uint32_t p, int axis) const {
+    return 0.5f * (boxes[6 * p + axis] + boxes[6 * p + 3 + axis]);
+  }
+
+  void build(int32_t id, uint32_t* idx, size_t n) {
+    BinNode& nd0 = (*nodes)[static_cast<size_t>(id)];
+    for (int a = 0; a < 3; ++a) {
+      nd0.lo[a] = std::numeric_limits<float>::max();
+      nd0.hi[a] = -std::numeric_limits<float>::max();
+    }
+    for (size_t i = 0; i < n; ++i) {
+      const float* b = boxes + 6 * idx[i];
+      for (int a = 0; a < 3; ++a) {
+        nd0.lo[a] = lt_min(nd0.lo[a], b[a]);
+        nd0.hi[a] = lt_max(nd0.hi[a], b[3 + a]);
+      }
+    }
+    if (n <= leaf_threshold) {
+      nd0.left = nd0.right = -1;
+      nd0.first = static_cast<int32_t>(idx - base);
+      nd0.count = static_cast<int32_t>(n);
+      return;
+    }
+    float clo[3], chi[3];
+    for (int a = 0; a < 3; ++a) {
+      clo[a] = std::numeric_limits<float>::max();
+      chi[a] = -std::numeric_limits<float>::max();
+    }
+    for (size_t i = 0; i < n; ++i) {
+      for (int a = 0; a < 3; ++a) {
+        const float c = centroid(idx[i], a);
+        clo[a] = lt_min(clo[a], c);
+        chi[a] = lt_max(chi[a], c);
+      }
+    }
+    int axis = 0;
+    float widest = chi[0] - clo[0];
+    for (int a = 1; a < 3; ++a) {
+      const float e = chi[a] - clo[a];
+      if (e > widest) {
+        widest = e;
+        axis = a;
+      }
+    }
+    const float split = 0.5f * (clo[axis] + chi[axis]);
+    uint32_t* mid = std::stable_partition(idx, idx + n, [&](uint32_t p) { return centroid(p, axis) < split; });
+    size_t left_n = static_cast<size_t>(mid - idx);
+    if (left_n == 0 || left_n == n) left_n = n / 2;
+    const int32_t l = next_id++;
+    const int32_t r = next_id++;
+    BinNode& nd = (*nodes)[static_cast<size_t>(id)];
+    nd.left = l;
+    nd.right = r;
+    nd.first = -1;
+    nd.count = 0;
+    build(l, idx, left_n);
+    build(r, idx + left_n, n - left_n);
+  }
+};
+
+float surface_area(const BinNode& n) {
+  const float dx = n.hi[0] - n.lo[0], dy = n.hi[1] - n.lo[1], dz = n.hi[2] - n.lo[2];
+  return dx * dy + dy * dz + dz * dx;
+}
+
+}  // namespace
+
+bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
+                  const uint32_t* instances, uint32_t instance_count, SceneGeometry& out, std::string& error) {
+  out.prims.clear();
+  out.boxes.clear();
+  if (instance_count > 0 && instances == nullptr) {
+    error = "instances pointer is null";
+    return false;
+  }
+  size_t capacity = 0;
+  for (uint32_t i = 0; i < instance_count; ++i) capacity += instances[3 * i + 1];
+  out.prims.reserve(capacity);
+  out.boxes.reserve(6 * capacity);
+  for (uint32_t i = 0; i < instance_count; ++i) {
+    const uint32_t first = instances[3 * i], count = instances[3 * i + 1], mat = instances[3 * i + 2];
+    for (uint32_t k = 0; k < count; ++k) {
+      const uint64_t base = (static_cast<uint64_t>(first) + k) * 3u;
+      if (base + 2u >= index_count) continue;
+      const uint32_t ia = indices[base], ib = indices[base + 1], ic = indices[base + 2];
+      if (ia >= vertex_count || ib >= vertex_count || ic >= vertex_count) continue;
+      const float* a = vertices + 3 * static_cast<size_t>(ia);
+      const float* b = vertices + 3 * static_cast<size_t>(ib);
+      const float* c = vertices + 3 * static_cast<size_t>(ic);
+      HostPrim p;
+      for (int ax = 0; ax < 3; ++ax) {
+        p.v0[ax] = a[ax];
+        p.e1[ax] = b[ax] - a[ax];
+        p.e2[ax] = c[ax] - a[ax];
+      }
+      // Geometric normal: cross(e1, e2) times 1/sqrt(|.|^2), (0,1,0) when degenerate
+      // (normalize_vec3 in src/pathtracer/CpuBvhAccelerator.cpp:75-82).
+      const float cx = p.e1[1] * p.e2[2] - p.e1[2] * p.e2[1];
+      const float cy = p.e1[2] * p.e2[0] - p.e1[0] * p.e2[2];
+      const float cz = p.e1[0] * p.e2[1] - p.e1[1] * p.e2[0];
+      const float l2 = cx * cx + cy * cy + cz * cz;
+      if (l2 <= kPad * kPad) {
+        p.n[0] = 0.0f;
+        p.n[1] = 1.0f;
+        p.n[2] = 0.0f;
+      } else {
+        const float inv = 1.0f / std::sqrt(l2);
+        p.n[0] = cx * inv;
+        p.n[1] = cy * inv;
+        p.n[2] = cz * inv;
+      }
+      p.material = mat;
+      out.prims.push_back(p);
+      for (int ax = 0; ax < 3; ++ax) out.boxes.push_back(std::min({a[ax], b[ax], c[ax]}) - kPad);
+      for (int ax = 0; ax < 3; ++ax) out.boxes.push_back(std::max({a[ax], b[ax], c[ax]}) + kPad);
+    }
+  }
+  return true;
+}
+
+void BuildBinaryBvh(const SceneGeometry& geo, uint32_t leaf_threshold, std::vector<BinNode>& nodes,
+                    std::vector<uint32_t>& prim_indices) {
+  const size_t n = geo.prims.size();
+  nodes.clear();
+  prim_indices.clear();
+  if (n == 0) return;
+  nodes.assign(2 * n - 1, BinNode{});
+  prim_indices.resize(n);
+  std::iota(prim_indices.begin(), prim_indices.end(), 0u);
+  Builder b{geo.boxes.data(), &nodes, prim_indices.data(), leaf_threshold == 0 ? 4u : leaf_threshold};
+  b.build(0, prim_indices.data(), n);
+  nodes.resize(static_cast<size_t>(b.next_id));
+}
+
+bool ValidateBinaryBvh(const std::vector<BinNode>& nodes, const std::vector<uint32_t>& prim_indices,
+                       size_t prim_count, std::string& error) {
+  if (nodes.empty()) {
+    error = "empty BVH";
+    return false;
+  }
+  if (prim_indices.size() != prim_count) {
+    error = "prim_indices size does not match the flattened primitive count";
+    return false;
+  }
+  for (uint32_t p : prim_indices) {
+    if (p >= prim_count) {
+      error = "prim_indices entry out of range";
+      return false;
+    }
+  }
+  // Every node reachable once from the root; leaves within range.
+  std::vector<uint8_t> seen(nodes.size(), 0);
+  std::vector<int32_t> stack{0};
+  while (!stack.empty()) {
+    const int32_t id = stack.back();
+    stack.pop_back();
+    if (id < 0 || static_cast<size_t>(id) >= nodes.size() || seen[static_cast<size_t>(id)]) {
+      error = "BVH child index out of range or shared";
+      return false;
+    }
+    seen[static_cast<size_t>(id)] = 1;
+    const BinNode& nd = nodes[static_cast<size_t>(id)];
+    if (nd.count > 0) {
+      if (nd.first < 0 || static_cast<size_t>(nd.first) + static_cast<size_t>(nd.count) > prim_indices.size() ||
+          nd.count > 8) {
+        error = "BVH leaf range out of bounds (or more than 8 primitives)";
+        return false;
+      }
+    } else {
+      stack.push_back(nd.left);
+      stack.push_back(nd.right);
+    }
+  }
+  return true;
+}
+
+void CollapseToWide(const SceneGeometry& geo, const std::vector<BinNode>& bin,
+                    const std::vector<uint32_t>& prim_indices, WideBvh& out) {
+  out = WideBvh{};
+  if (bin.empty()) return;
+  out.binary_nodes = static_cast<uint32_t>(bin.size());
+  // Tie records: bounds, parent and depth of every binary node.
+  out.tie_nodes.resize(bin.size());
+  std::vector<int32_t> parent(bin.size(), -1), depth(bin.size(), 0);
+  {
+    std::vector<int32_t> st{0};
+    while (!st.empty()) {
+      const int32_t id = st.back();
+      st.pop_back();
+      const BinNode& nd = bin[static_cast<size_t>(id)];
+      if (nd.count > 0) {
+        ++out.binary_leaves;
+        continue;
+      }
+      for (int32_t c : {nd.left, nd.right}) {
+        parent[static_cast<size_t>(c)] = id;
+        depth[static_cast<size_t>(c)] = depth[static_cast<size_t>(id)] + 1;
+        st.push_back(c);
+      }
+    }
+  }
+  for (size_t i = 0; i < bin.size(); ++i) {
+    TieNode& t = out.tie_nodes[i];
+    t.lox = bin[i].lo[0];
+    t.loy = bin[i].lo[1];
+    t.loz = bin[i].lo[2];
+    t.hix = bin[i].hi[0];
+    t.hiy = bin[i].hi[1];
+    t.hiz = bin[i].hi[2];
+    t.parent = parent[i];
+    t.depth = depth[i];
+  }
+
+  auto emit_leaf = [&](int32_t leaf_id) -> int32_t {
+    const BinNode& lf = bin[static_cast<size_t>(leaf_id)];
+    const uint32_t first = static_cast<uint32_t>(out.tris.size());
+    for (int32_t i = 0; i < lf.count; ++i) {
+      const uint32_t p = prim_indices[static_cast<size_t>(lf.first + i)];
+      const HostPrim& hp = geo.prims[p];
+      TriRecord r;
+      r.v0x = hp.v0[0];
+      r.v0y = hp.v0[1];
+      r.v0z = hp.v0[2];
+      r.e1x = hp.e1[0];
+      r.e1y = hp.e1[1];
+      r.e1z = hp.e1[2];
+      r.e2x = hp.e2[0];
+      r.e2y = hp.e2[1];
+      r.e2z = hp.e2[2];
+      r.prim = p;
+      r.leaf = static_cast<uint32_t>(leaf_id);
+      r.lane = static_cast<uint32_t>(i);
+      out.tris.push_back(r);
+    }
+    return ~static_cast<int32_t>((first << 3) | static_cast<uint32_t>(lf.count - 1));
+  };
+
+  // Depth-first, pre-order allocation of wide nodes.
+  std::function<int32_t(int32_t, uint32_t, uint32_t)> make = [&](int32_t bin_id, uint32_t level,
+                                                                  uint32_t stack_so_far) -> int32_t {
+    const int32_t wide_id = static_cast<int32_t>(out.nodes.size());
+    out.nodes.push_back(WideNode{});
+    std::vector<int32_t> slots;
+    const BinNode& root = bin[static_cast<size_t>(bin_id)];
+    if (root.count > 0) {
+      slots.push_back(bin_id);
+    } else {
+      slots = {root.left, root.right};
+      while (slots.size() < 4) {
+        int best = -1;
+        float best_area = -1.0f;
+        for (size_t s = 0; s < slots.size(); ++s) {
+          const BinNode& c = bin[static_cast<size_t>(slots[s])];
+          if (c.count > 0) continue;
+          const float a = surface_area(c);
+          if (a > best_area) {
+            best_area = a;
+            best = static_cast<int>(s);
+          }
+        }
+        if (best < 0) break;
+        const BinNode& c = bin[static_cast<size_t>(slots[static_cast<size_t>(best)])];
+        slots[static_cast<size_t>(best)] = c.left;
+        slots.insert(slots.begin() + best + 1, c.right);
+      }
+    }
+    const uint32_t stack_here = stack_so_far + static_cast<uint32_t>(slots.size()) - 1u;
+    out.depth = std::max(out.depth, level + 1u);
+    out.stack_required = std::max(out.stack_required, stack_here);
+    WideNode wn{};
+    for (int k = 0; k < 4; ++k) {
+      wn.lox[k] = wn.loy[k] = wn.loz[k] = 1.0f;
+      wn.hix[k] = wn.hiy[k] = wn.hiz[k] = -1.0f;
+      wn.child[k] = 0;
+    }
+    wn.meta[0] = static_cast<int32_t>(slots.size());
+    for (size_t s = 0; s < slots.size(); ++s) {
+      const BinNode& c = bin[static_cast<size_t>(slots[s])];
+      wn.lox[s] = c.lo[0];
+      wn.loy[s] = c.lo[1];
+      wn.loz[s] = c.lo[2];
+      wn.hix[s] = c.hi[0];
+      wn.hiy[s] = c.hi[1];
+      wn.hiz[s] = c.hi[2];
+    }
+    for (size_t s = 0; s < slots.size(); ++s) {
+      const BinNode& c = bin[static_cast<size_t>(slots[s])];
+      wn.child[s] = (c.count > 0) ? emit_leaf(slots[s]) : make(slots[s], level + 1u, stack_here);
+    }
+    out.nodes[static_cast<size_t>(wide_id)] = wn;
+    return wide_id;
+  };
+  make(0, 0u, 0u);
+  out.stack_required += 1u;
+}
+
+}  // namespace vkptc

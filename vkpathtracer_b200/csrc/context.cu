@@ -1,0 +1,744 @@
+// context.cu -- the C ABI of libvkpt_cuda (include/vkptc.h).
+//
+// One vkptc_ctx is one IPathTracer instance (src/pathtracer/PathTracer.h:1069-1184):
+// it follows that interface's state machine (Uninitialized -> Configured ->
+// SceneLoaded -> Ready; reset is film-only and keeps the acceleration
+// structure), returns its StatusCode values, and keeps a last-error string.
+// All device memory (scene, wide BVH, film, wave queues) belongs to the context.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/vkptc.h"
+#include "bvh_host.h"
+#include "kernels.cuh"
+
+using namespace vkptc;
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  cudaError_t alloc(size_t n) {
+    if (n <= count && ptr) return cudaSuccess;
+    release();
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T));
+    if (e == cudaSuccess) count = n;
+    else ptr = nullptr;
+    return e;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+struct HostCamera {
+  float pos[3], target[3], up[3];
+  float fov, aperture, focus;
+};
+
+}  // namespace
+
+struct vkptc_ctx {
+  vkptc_config config{};
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  bool configured = false, has_scene = false, accel_valid = false;
+  uint32_t current_sample = 0;
+  uint64_t last_sample_us = 0, accumulation_gen = 0;
+  vkptc_render_settings settings{};
+
+  // scene (host copies needed to rebuild)
+  SceneGeometry geo;
+  std::vector<float> materials, lights;
+  float env[3] = {0, 0, 0};
+  HostCamera cam{};
+  bool has_transmissive = false;
+
+  // device scene
+  DevBuf<float4> d_nodes, d_tris, d_shade, d_tie;
+  DevBuf<float> d_materials, d_lights;
+  WideBvh wide;
+  vkptc_accel_info accel{};
+
+  // film
+  DevBuf<float4> d_film_sum;
+  DevBuf<uint32_t> d_film_count;
+  DevBuf<float> d_film_invalid;
+
+  // wave state
+  DevBuf<uint64_t> w_rng;
+  DevBuf<float4> w_ray_o, w_ray_d, w_thr, w_rad, w_sh_o, w_sh_d, w_sh_c;
+  DevBuf<float2> w_hit;
+  DevBuf<uint32_t> w_q0, w_q1, w_sh_path, w_counts;
+  uint32_t wave_capacity = 0;
+  size_t smem_configured = 48 * 1024;
+
+  // counters and error word
+  DevBuf<DevCounters> d_ctr;
+  DevBuf<uint32_t> d_err;
+
+  // ray-query scratch for host-buffer calls
+  DevBuf<float> q_rays, q_tmax, q_t;
+  DevBuf<uint32_t> q_prim;
+};
+
+namespace {
+
+int32_t fail(vkptc_ctx* ctx, int32_t code, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return code;
+}
+
+int32_t cuda_fail(vkptc_ctx* ctx, cudaError_t e, const char* what) {
+  const int32_t code = (e == cudaErrorMemoryAllocation) ? VKPTC_ALLOC_FAILED : VKPTC_INTERNAL_ERROR;
+  return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define VKPTC_CUDA(ctx, call, what)            \
+  do {                                         \
+    cudaError_t e_ = (call);                   \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+  } while (0)
+
+vkptc_lifecycle lifecycle(const vkptc_ctx* c) {
+  if (!c->configured) return VKPTC_UNINITIALIZED;
+  if (!c->has_scene) return VKPTC_CONFIGURED;
+  if (!c->accel_valid) return VKPTC_SCENE_LOADED;
+  return VKPTC_READY;
+}
+
+// Camera basis and tan(fov/2) computed on the host exactly as the reference
+// does (compute_camera_basis, ScalarCpuPathTracer.cpp:139-152; camera_rays,
+// ScalarCpuPathTracer.Render.cpp:78) so primary rays are bit-identical.
+void camera_basis(const HostCamera& c, V3& fwd, V3& right, V3& up) {
+  fwd = unit(sub(mk(c.target[0], c.target[1], c.target[2]), mk(c.pos[0], c.pos[1], c.pos[2])));
+  right = unit(cross(fwd, mk(c.up[0], c.up[1], c.up[2])));
+  if (dot(right, right) <= kEps * kEps) right = mk(1.0f, 0.0f, 0.0f);
+  up = unit(cross(right, fwd));
+  if (dot(up, up) <= kEps * kEps) up = mk(0.0f, 1.0f, 0.0f);
+}
+
+DevScene dev_scene(const vkptc_ctx* c) {
+  DevScene s{};
+  s.nodes = c->d_nodes.ptr;
+  s.tris = c->d_tris.ptr;
+  s.shade = c->d_shade.ptr;
+  s.tie = c->d_tie.ptr;
+  s.materials = c->d_materials.ptr;
+  s.lights = c->d_lights.ptr;
+  s.material_count = static_cast<uint32_t>(c->materials.size() / 16);
+  s.light_count = static_cast<uint32_t>(c->lights.size() / 16);
+  s.prim_count = static_cast<uint32_t>(c->geo.prims.size());
+  s.has_transmissive = c->has_transmissive ? 1u : 0u;
+  s.env = mk(c->env[0], c->env[1], c->env[2]);
+  s.cam_pos = mk(c->cam.pos[0], c->cam.pos[1], c->cam.pos[2]);
+  camera_basis(c->cam, s.cam_fwd, s.cam_right, s.cam_up);
+  const float radians = c->cam.fov * (kPi / 180.0f);
+  s.tan_half_fov = std::tan(0.5f * radians);
+  s.aperture = c->cam.aperture > 0.0f ? c->cam.aperture : c->settings.camera_aperture_radius;
+  s.focus = c->cam.focus > 0.0f ? c->cam.focus : c->settings.camera_focus_distance;
+  s.stack_required = c->wide.stack_required;
+  return s;
+}
+
+DevSettings dev_settings(const vkptc_ctx* c, uint32_t frame) {
+  DevSettings st{};
+  st.width = c->settings.width;
+  st.height = c->settings.height;
+  st.max_depth = c->settings.max_depth;
+  st.enable_nee = c->settings.enable_nee;
+  st.enable_mis = c->settings.enable_mis;
+  st.rr_start = c->settings.rr_start_depth;
+  st.rr_min = c->settings.rr_min_survival;
+  st.rr_max = c->settings.rr_max_survival;
+  st.seed = c->settings.seed;
+  st.firefly_clamp = c->settings.firefly_clamp;
+  st.frame = frame;
+  return st;
+}
+
+int block_size(const vkptc_ctx* c) {
+  const uint32_t b = c->config.block_size;
+  if (b == 0) return 128;
+  return static_cast<int>(std::min<uint32_t>(256u, std::max<uint32_t>(32u, (b + 31u) / 32u * 32u)));
+}
+
+int stack_cap(const vkptc_ctx* c) {
+  const int need = static_cast<int>(std::max<uint32_t>(1u, c->wide.stack_required));
+  const int asked = static_cast<int>(c->config.stack_depth);
+  return std::max(need, asked);
+}
+
+int32_t ensure_stack_smem(vkptc_ctx* c, const LaunchShape& ls);
+
+// Block size, stack capacity and a grid of (resident blocks per SM) x SMs for
+// the grid-stride stage kernels; raises the shared-memory limit first.
+int32_t launch_shape(vkptc_ctx* c, cudaStream_t stream, LaunchShape& ls) {
+  ls.block = block_size(c);
+  ls.stack_cap = stack_cap(c);
+  ls.stream = stream;
+  const int32_t rc = ensure_stack_smem(c, ls);
+  if (rc != VKPTC_OK) return rc;
+  const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
+  const int per_sm = ExtendBlocksPerSm(ls.block, smem);
+  ls.grid = c->sm_count * per_sm;
+  return VKPTC_OK;
+}
+
+int32_t ensure_stack_smem(vkptc_ctx* c, const LaunchShape& ls) {
+  const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
+  int max_optin = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if (smem > static_cast<size_t>(max_optin)) {
+    return fail(c, VKPTC_UNSUPPORTED, "traversal stack does not fit in shared memory (BVH too deep for this block size)");
+  }
+  if (smem > c->smem_configured) {
+    VKPTC_CUDA(c, ConfigureStackSmem(smem), "shared memory limit");
+    c->smem_configured = smem;
+  }
+  return VKPTC_OK;
+}
+
+int32_t ensure_wave(vkptc_ctx* c, uint32_t paths) {
+  if (paths <= c->wave_capacity) return VKPTC_OK;
+  const size_t n = paths;
+  VKPTC_CUDA(c, c->w_rng.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_ray_o.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_ray_d.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_thr.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_rad.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_hit.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_q0.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_q1.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_sh_path.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_sh_o.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_sh_d.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_sh_c.alloc(n), "wave alloc");
+  VKPTC_CUDA(c, c->w_counts.alloc(4), "wave alloc");
+  c->wave_capacity = paths;
+  return VKPTC_OK;
+}
+
+WaveState wave_state(vkptc_ctx* c) {
+  WaveState w{};
+  w.rng = c->w_rng.ptr;
+  w.ray_o = c->w_ray_o.ptr;
+  w.ray_d = c->w_ray_d.ptr;
+  w.thr = c->w_thr.ptr;
+  w.rad = c->w_rad.ptr;
+  w.hit = c->w_hit.ptr;
+  w.sh_path = c->w_sh_path.ptr;
+  w.sh_o = c->w_sh_o.ptr;
+  w.sh_d = c->w_sh_d.ptr;
+  w.sh_c = c->w_sh_c.ptr;
+  w.q[0] = c->w_q0.ptr;
+  w.q[1] = c->w_q1.ptr;
+  w.counts = c->w_counts.ptr;
+  w.capacity = c->wave_capacity;
+  return w;
+}
+
+Film film_of(vkptc_ctx* c) {
+  Film f{};
+  f.sum = c->d_film_sum.ptr;
+  f.count = c->d_film_count.ptr;
+  f.invalid = c->d_film_invalid.ptr;
+  f.width = c->settings.width;
+  f.height = c->settings.height;
+  return f;
+}
+
+int32_t check_device_error(vkptc_ctx* c) {
+  uint32_t err = 0;
+  VKPTC_CUDA(c, cudaMemcpyAsync(&err, c->d_err.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream), "error word");
+  VKPTC_CUDA(c, cudaStreamSynchronize(c->stream), "synchronize");
+  if (err != 0u) return fail(c, VKPTC_INTERNAL_ERROR, "device traversal stack overflow");
+  return VKPTC_OK;
+}
+
+int32_t upload_accel(vkptc_ctx* c, const std::vector<BinNode>& bin, const std::vector<uint32_t>& prim_indices,
+                     double build_ms) {
+  CollapseToWide(c->geo, bin, prim_indices, c->wide);
+  const WideBvh& w = c->wide;
+  VKPTC_CUDA(c, c->d_nodes.alloc(std::max<size_t>(1, w.nodes.size() * 8)), "bvh alloc");
+  VKPTC_CUDA(c, c->d_tris.alloc(std::max<size_t>(1, w.tris.size() * 3)), "bvh alloc");
+  VKPTC_CUDA(c, c->d_tie.alloc(std::max<size_t>(1, w.tie_nodes.size() * 2)), "bvh alloc");
+  VKPTC_CUDA(c, c->d_shade.alloc(std::max<size_t>(1, c->geo.prims.size())), "bvh alloc");
+  if (!w.nodes.empty()) {
+    VKPTC_CUDA(c, cudaMemcpy(c->d_nodes.ptr, w.nodes.data(), w.nodes.size() * sizeof(WideNode), cudaMemcpyHostToDevice), "bvh upload");
+    VKPTC_CUDA(c, cudaMemcpy(c->d_tris.ptr, w.tris.data(), w.tris.size() * sizeof(TriRecord), cudaMemcpyHostToDevice), "bvh upload");
+    VKPTC_CUDA(c, cudaMemcpy(c->d_tie.ptr, w.tie_nodes.data(), w.tie_nodes.size() * sizeof(TieNode), cudaMemcpyHostToDevice), "bvh upload");
+  }
+  std::vector<float4> shade(c->geo.prims.size());
+  for (size_t i = 0; i < c->geo.prims.size(); ++i) {
+    const HostPrim& p = c->geo.prims[i];
+    float m;
+    std::memcpy(&m, &p.material, 4);
+    shade[i] = make_float4(p.n[0], p.n[1], p.n[2], m);
+  }
+  if (!shade.empty())
+    VKPTC_CUDA(c, cudaMemcpy(c->d_shade.ptr, shade.data(), shade.size() * sizeof(float4), cudaMemcpyHostToDevice), "bvh upload");
+  c->accel = vkptc_accel_info{};
+  c->accel.primitive_count = static_cast<uint32_t>(c->geo.prims.size());
+  c->accel.binary_node_count = w.binary_nodes;
+  c->accel.binary_leaf_count = w.binary_leaves;
+  c->accel.wide_node_count = static_cast<uint32_t>(w.nodes.size());
+  c->accel.wide_depth = w.depth;
+  c->accel.stack_required = w.stack_required;
+  c->accel.build_ms = build_ms;
+  c->accel.device_bytes = w.nodes.size() * sizeof(WideNode) + w.tris.size() * sizeof(TriRecord);
+  c->accel_valid = true;
+  return VKPTC_OK;
+}
+
+int32_t run_wave(vkptc_ctx* c, const WaveTile& tile, uint32_t frame) {
+  const uint32_t paths = tile.w * tile.h * tile.sample_count;
+  int32_t rc = ensure_wave(c, paths);
+  if (rc != VKPTC_OK) return rc;
+  LaunchShape ls;
+  rc = launch_shape(c, c->stream, ls);
+  if (rc != VKPTC_OK) return rc;
+  const DevScene s = dev_scene(c);
+  const DevSettings st = dev_settings(c, frame);
+  VKPTC_CUDA(c, LaunchWave(s, st, wave_state(c), tile, film_of(c), c->config.math_mode == 0u,
+                           c->config.collect_stats != 0u, ls, c->d_ctr.ptr, c->d_err.ptr),
+             "wave launch");
+  return VKPTC_OK;
+}
+
+constexpr uint32_t kDefaultWavePaths = 1u << 22;
+
+uint32_t wave_paths(const vkptc_ctx* c) {
+  return c->config.reserved[0] ? c->config.reserved[0] : kDefaultWavePaths;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
+  if (!out_ctx) return VKPTC_INVALID_ARGUMENT;
+  *out_ctx = nullptr;
+  auto* c = new (std::nothrow) vkptc_ctx();
+  if (!c) return VKPTC_ALLOC_FAILED;
+  if (config) c->config = *config;
+  c->device = c->config.device;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    delete c;
+    return VKPTC_UNSUPPORTED;
+  }
+  if (c->device < 0 || c->device >= count) {
+    delete c;
+    return VKPTC_INVALID_ARGUMENT;
+  }
+  if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return VKPTC_INTERNAL_ERROR;
+  }
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+  if (c->d_ctr.alloc(1) != cudaSuccess || c->d_err.alloc(1) != cudaSuccess ||
+      cudaMemset(c->d_ctr.ptr, 0, sizeof(DevCounters)) != cudaSuccess ||
+      cudaMemset(c->d_err.ptr, 0, sizeof(uint32_t)) != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return VKPTC_ALLOC_FAILED;
+  }
+  *out_ctx = c;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_destroy(vkptc_ctx* ctx) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStream_t s = ctx->stream;
+  delete ctx;
+  if (s) cudaStreamDestroy(s);
+  return VKPTC_OK;
+}
+
+int32_t vkptc_configure(vkptc_ctx* ctx, const vkptc_render_settings* settings) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!settings) return fail(ctx, VKPTC_INVALID_ARGUMENT, "settings is null");
+  if (settings->max_depth > 1024u) return fail(ctx, VKPTC_INVALID_ARGUMENT, "max_depth above 1024");
+  const uint64_t px = static_cast<uint64_t>(settings->width) * settings->height;
+  if (px > (1ull << 28)) return fail(ctx, VKPTC_INVALID_ARGUMENT, "film larger than 2^28 pixels");
+  cudaSetDevice(ctx->device);
+  ctx->settings = *settings;
+  VKPTC_CUDA(ctx, ctx->d_film_sum.alloc(std::max<uint64_t>(1, px)), "film alloc");
+  VKPTC_CUDA(ctx, ctx->d_film_count.alloc(std::max<uint64_t>(1, px)), "film alloc");
+  VKPTC_CUDA(ctx, ctx->d_film_invalid.alloc(std::max<uint64_t>(1, px)), "film alloc");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_film_sum.ptr, 0, ctx->d_film_sum.bytes(), ctx->stream), "film clear");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_film_count.ptr, 0, ctx->d_film_count.bytes(), ctx->stream), "film clear");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_film_invalid.ptr, 0, ctx->d_film_invalid.bytes(), ctx->stream), "film clear");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr.ptr, 0, sizeof(DevCounters), ctx->stream), "counter clear");
+  ctx->configured = true;
+  ctx->has_scene = false;
+  ctx->accel_valid = false;
+  ctx->current_sample = 0;
+  ctx->accumulation_gen = 0;
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "load_scene_snapshot called before configure");
+  if (!scene) return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene is null");
+  if ((scene->vertex_count && !scene->vertices) || (scene->index_count && !scene->indices) ||
+      (scene->material_count && !scene->materials) || (scene->light_count && !scene->lights)) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene array pointer is null");
+  }
+  for (uint32_t i = 0; i < scene->material_count; ++i) {
+    const uint32_t effect = static_cast<uint32_t>(scene->materials[16 * i + 15] + 0.5f) & 1023u;
+    if (effect != 0u) return fail(ctx, VKPTC_UNSUPPORTED, "procedural material effects (effect != 0) are not supported");
+  }
+  cudaSetDevice(ctx->device);
+  std::string err;
+  SceneGeometry geo;
+  if (!FlattenScene(scene->vertices, scene->vertex_count, scene->indices, scene->index_count, scene->instances,
+                    scene->instance_count, geo, err)) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, err);
+  }
+  ctx->geo = std::move(geo);
+  ctx->materials.assign(scene->materials, scene->materials + 16 * static_cast<size_t>(scene->material_count));
+  if (ctx->materials.empty()) {
+    // The reference substitutes one default RTMaterial (ScalarCpuPathTracer.cpp:468-470).
+    const float def[16] = {1, 1, 1, 0, 0, 0, 1, 0, 0, 1.5f, 0, 0, 0, 0, 1, 0};
+    ctx->materials.assign(def, def + 16);
+  }
+  ctx->lights.assign(scene->lights, scene->lights + 16 * static_cast<size_t>(scene->light_count));
+  for (size_t i = 0; i < ctx->lights.size() / 16; ++i) ctx->lights[16 * i + 7] = std::max(0.0f, ctx->lights[16 * i + 7]);
+  ctx->has_transmissive = false;
+  for (size_t i = 0; i < ctx->materials.size() / 16; ++i) {
+    const float* m = &ctx->materials[16 * i];
+    if (static_cast<uint32_t>(m[7] + 0.5f) == 5u || m[10] > 0.05f) ctx->has_transmissive = true;
+  }
+  std::memcpy(ctx->env, scene->environment, sizeof(ctx->env));
+  std::memcpy(ctx->cam.pos, scene->camera_position, 12);
+  std::memcpy(ctx->cam.target, scene->camera_target, 12);
+  std::memcpy(ctx->cam.up, scene->camera_up, 12);
+  ctx->cam.fov = scene->camera_fov_deg;
+  ctx->cam.aperture = scene->camera_aperture_radius;
+  ctx->cam.focus = scene->camera_focus_distance;
+  VKPTC_CUDA(ctx, ctx->d_materials.alloc(ctx->materials.size()), "material alloc");
+  VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_materials.ptr, ctx->materials.data(), ctx->materials.size() * sizeof(float),
+                             cudaMemcpyHostToDevice), "material upload");
+  VKPTC_CUDA(ctx, ctx->d_lights.alloc(std::max<size_t>(16, ctx->lights.size())), "light alloc");
+  if (!ctx->lights.empty())
+    VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_lights.ptr, ctx->lights.data(), ctx->lights.size() * sizeof(float),
+                               cudaMemcpyHostToDevice), "light upload");
+  ctx->has_scene = true;
+  ctx->accel_valid = false;
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_build_acceleration(vkptc_ctx* ctx) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "build_or_update_acceleration called before load_scene_snapshot");
+  cudaSetDevice(ctx->device);
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<BinNode> bin;
+  std::vector<uint32_t> order;
+  BuildBinaryBvh(ctx->geo, 4u, bin, order);
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  const int32_t rc = upload_accel(ctx, bin, order, ms);
+  if (rc == VKPTC_OK) ctx->last_error.clear();
+  return rc;
+}
+
+int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "load_bvh called before load_scene_snapshot");
+  if (!bvh || !bvh->nodes || !bvh->prim_indices) return fail(ctx, VKPTC_INVALID_ARGUMENT, "bvh view is null");
+  cudaSetDevice(ctx->device);
+  std::vector<BinNode> bin(bvh->node_count);
+  for (uint32_t i = 0; i < bvh->node_count; ++i) {
+    const uint32_t* w = bvh->nodes + 10 * static_cast<size_t>(i);
+    std::memcpy(bin[i].lo, w, 12);
+    std::memcpy(bin[i].hi, w + 3, 12);
+    std::memcpy(&bin[i].left, w + 6, 4);
+    std::memcpy(&bin[i].right, w + 7, 4);
+    std::memcpy(&bin[i].first, w + 8, 4);
+    std::memcpy(&bin[i].count, w + 9, 4);
+  }
+  std::vector<uint32_t> order(bvh->prim_indices, bvh->prim_indices + bvh->prim_count);
+  std::string err;
+  if (!ValidateBinaryBvh(bin, order, ctx->geo.prims.size(), err)) return fail(ctx, VKPTC_INVALID_ARGUMENT, err);
+  const int32_t rc = upload_accel(ctx, bin, order, 0.0);
+  if (rc == VKPTC_OK) ctx->last_error.clear();
+  return rc;
+}
+
+int32_t vkptc_build_binary_bvh(const vkptc_scene_view* scene, uint32_t* nodes_out, uint32_t* node_count,
+                               uint32_t* prim_out, uint32_t* prim_count) {
+  if (!scene || !nodes_out || !node_count || !prim_out || !prim_count) return VKPTC_INVALID_ARGUMENT;
+  SceneGeometry geo;
+  std::string err;
+  if (!FlattenScene(scene->vertices, scene->vertex_count, scene->indices, scene->index_count, scene->instances,
+                    scene->instance_count, geo, err)) {
+    return VKPTC_INVALID_ARGUMENT;
+  }
+  std::vector<BinNode> bin;
+  std::vector<uint32_t> order;
+  BuildBinaryBvh(geo, 4u, bin, order);
+  for (size_t i = 0; i < bin.size(); ++i) {
+    uint32_t* w = nodes_out + 10 * i;
+    std::memcpy(w, bin[i].lo, 12);
+    std::memcpy(w + 3, bin[i].hi, 12);
+    std::memcpy(w + 6, &bin[i].left, 4);
+    std::memcpy(w + 7, &bin[i].right, 4);
+    std::memcpy(w + 8, &bin[i].first, 4);
+    std::memcpy(w + 9, &bin[i].count, 4);
+  }
+  std::copy(order.begin(), order.end(), prim_out);
+  *node_count = static_cast<uint32_t>(bin.size());
+  *prim_count = static_cast<uint32_t>(order.size());
+  return VKPTC_OK;
+}
+
+int32_t vkptc_get_accel_info(vkptc_ctx* ctx, vkptc_accel_info* out) {
+  if (!ctx || !out) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "acceleration structure not built");
+  *out = ctx->accel;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_reset(vkptc_ctx* ctx) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "reset_accumulation called before configure");
+  cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_film_sum.ptr, 0, ctx->d_film_sum.bytes(), ctx->stream), "film clear");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_film_count.ptr, 0, ctx->d_film_count.bytes(), ctx->stream), "film clear");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_film_invalid.ptr, 0, ctx->d_film_invalid.bytes(), ctx->stream), "film clear");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr.ptr, 0, sizeof(DevCounters), ctx->stream), "counter clear");
+  ctx->current_sample = 0;
+  ++ctx->accumulation_gen;
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_shutdown(vkptc_ctx* ctx) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->configured = ctx->has_scene = ctx->accel_valid = false;
+  ctx->geo = SceneGeometry{};
+  ctx->wide = WideBvh{};
+  ctx->d_nodes.release();
+  ctx->d_tris.release();
+  ctx->d_tie.release();
+  ctx->d_shade.release();
+  ctx->d_materials.release();
+  ctx->d_lights.release();
+  ctx->d_film_sum.release();
+  ctx->d_film_count.release();
+  ctx->d_film_invalid.release();
+  ctx->current_sample = 0;
+  ctx->accumulation_gen = 0;
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_render(vkptc_ctx* ctx, const vkptc_tile* tiles, uint32_t tile_count, uint32_t frame,
+                     const volatile int32_t* cancel_flag) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured || !ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "render_tile requires a configured tracer with a scene");
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "render_tile requires a built acceleration structure");
+  if (tile_count && !tiles) return fail(ctx, VKPTC_INVALID_ARGUMENT, "tiles is null");
+  cudaSetDevice(ctx->device);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (uint32_t k = 0; k < tile_count; ++k) {
+    if (cancel_flag && *cancel_flag) return fail(ctx, VKPTC_CANCELLED, "render_tile cancelled");
+    const vkptc_tile& t = tiles[k];
+    // Clip to the film as the reference does (ScalarCpuPathTracer.Render.cpp:171-176).
+    const uint32_t x0 = std::min(t.x, ctx->settings.width), y0 = std::min(t.y, ctx->settings.height);
+    const uint32_t x1 = static_cast<uint32_t>(std::min<uint64_t>(ctx->settings.width, static_cast<uint64_t>(x0) + t.width));
+    const uint32_t y1 = static_cast<uint32_t>(std::min<uint64_t>(ctx->settings.height, static_cast<uint64_t>(y0) + t.height));
+    if (x0 >= x1 || y0 >= y1) continue;
+    WaveTile wt{x0, y0, x1 - x0, y1 - y0, t.sample_index, 1u};
+    const int32_t rc = run_wave(ctx, wt, frame);
+    if (rc != VKPTC_OK) return rc;
+    ctx->current_sample = std::max(ctx->current_sample, t.sample_index + 1u);
+  }
+  const int32_t rc = check_device_error(ctx);
+  ctx->last_sample_us = static_cast<uint64_t>(
+      std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count());
+  if (rc == VKPTC_OK) ctx->last_error.clear();
+  return rc;
+}
+
+int32_t vkptc_render_frame(vkptc_ctx* ctx, uint32_t first_sample, uint32_t sample_count, uint32_t frame) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured || !ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "render requires a configured tracer with a scene");
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "render requires a built acceleration structure");
+  cudaSetDevice(ctx->device);
+  const uint32_t px = ctx->settings.width * ctx->settings.height;
+  if (px == 0 || sample_count == 0) return VKPTC_OK;
+  const uint32_t per_wave = std::max(1u, std::min(sample_count, wave_paths(ctx) / px));
+  for (uint32_t s = 0; s < sample_count; s += per_wave) {
+    const uint32_t n = std::min(per_wave, sample_count - s);
+    WaveTile wt{0u, 0u, ctx->settings.width, ctx->settings.height, first_sample + s, n};
+    const int32_t rc = run_wave(ctx, wt, frame);
+    if (rc != VKPTC_OK) return rc;
+  }
+  ctx->current_sample = std::max(ctx->current_sample, first_sample + sample_count);
+  return VKPTC_OK;
+}
+
+int32_t vkptc_synchronize(vkptc_ctx* ctx) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  return check_device_error(ctx);
+}
+
+int32_t vkptc_read_film(vkptc_ctx* ctx, float* sum_rgb, uint32_t* count, float* invalid) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "film not configured");
+  cudaSetDevice(ctx->device);
+  const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
+  if (sum_rgb) {
+    std::vector<float4> tmp(px);
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(tmp.data(), ctx->d_film_sum.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream), "film read");
+    VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "film read");
+    for (size_t i = 0; i < px; ++i) {
+      sum_rgb[3 * i] = tmp[i].x;
+      sum_rgb[3 * i + 1] = tmp[i].y;
+      sum_rgb[3 * i + 2] = tmp[i].z;
+    }
+  }
+  if (count) VKPTC_CUDA(ctx, cudaMemcpyAsync(count, ctx->d_film_count.ptr, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream), "film read");
+  if (invalid) VKPTC_CUDA(ctx, cudaMemcpyAsync(invalid, ctx->d_film_invalid.ptr, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream), "film read");
+  VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "film read");
+  return VKPTC_OK;
+}
+
+int32_t vkptc_write_film(vkptc_ctx* ctx, const float* sum_rgb, const uint32_t* count, const float* invalid) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "replace_film_history called before configure");
+  if (!sum_rgb || !count) return fail(ctx, VKPTC_INVALID_ARGUMENT, "film arrays are null");
+  cudaSetDevice(ctx->device);
+  const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
+  std::vector<float4> tmp(px);
+  for (size_t i = 0; i < px; ++i) tmp[i] = make_float4(sum_rgb[3 * i], sum_rgb[3 * i + 1], sum_rgb[3 * i + 2], 0.0f);
+  VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_film_sum.ptr, tmp.data(), px * sizeof(float4), cudaMemcpyHostToDevice), "film write");
+  VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_film_count.ptr, count, px * sizeof(uint32_t), cudaMemcpyHostToDevice), "film write");
+  if (invalid) VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_film_invalid.ptr, invalid, px * sizeof(float), cudaMemcpyHostToDevice), "film write");
+  else VKPTC_CUDA(ctx, cudaMemset(ctx->d_film_invalid.ptr, 0, px * sizeof(float)), "film write");
+  return VKPTC_OK;
+}
+
+int32_t vkptc_resolve_hdr(vkptc_ctx* ctx, float* rgb) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "film not configured");
+  if (!rgb) return fail(ctx, VKPTC_INVALID_ARGUMENT, "rgb is null");
+  cudaSetDevice(ctx->device);
+  const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
+  float* d_rgb = nullptr;
+  VKPTC_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&d_rgb), std::max<size_t>(1, 3 * px) * sizeof(float), ctx->stream), "resolve alloc");
+  cudaError_t e = LaunchResolveHdr(film_of(ctx), d_rgb, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rgb, d_rgb, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(d_rgb, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "resolve");
+  return VKPTC_OK;
+}
+
+int32_t vkptc_read_counters(vkptc_ctx* ctx, vkptc_counters* out) {
+  if (!ctx || !out) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  DevCounters dc{};
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(&dc, ctx->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost, ctx->stream), "counter read");
+  VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "counter read");
+  std::memset(out, 0, sizeof(*out));
+  out->samples = dc.samples;
+  out->rays = dc.rays;
+  out->shadow_tests = dc.shadow_tests;
+  out->triangle_tests = dc.tris + dc.shadow_tris;
+  out->bvh_node_visits = dc.nodes + dc.shadow_nodes;
+  out->bvh_leaf_visits = dc.leaves + dc.shadow_leaves;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_get_status(vkptc_ctx* ctx, vkptc_tracer_status* out) {
+  if (!ctx || !out) return VKPTC_INVALID_ARGUMENT;
+  vkptc_counters c{};
+  const int32_t rc = vkptc_read_counters(ctx, &c);
+  std::memset(out, 0, sizeof(*out));
+  out->lifecycle = lifecycle(ctx);
+  out->scene_loaded = ctx->has_scene;
+  out->accel_valid = ctx->accel_valid;
+  out->ready_to_render = ctx->configured && ctx->has_scene && ctx->accel_valid;
+  out->current_sample = ctx->current_sample;
+  out->last_sample_us = ctx->last_sample_us;
+  out->total_samples = c.samples;
+  out->accumulation_gen = ctx->accumulation_gen;
+  return rc == VKPTC_OK ? VKPTC_OK : rc;
+}
+
+const char* vkptc_last_error(vkptc_ctx* ctx) {
+  if (!ctx) return "null context";
+  return ctx->last_error.c_str();
+}
+
+int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float* d_tmax, uint64_t ray_count,
+                                uint32_t mode, uint32_t* d_prim_out, float* d_t_out, void* stream) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "acceleration structure not built");
+  if (mode > VKPTC_QUERY_ANY) return fail(ctx, VKPTC_INVALID_ARGUMENT, "unknown query mode");
+  if (ray_count && (!d_rays || !d_prim_out)) return fail(ctx, VKPTC_INVALID_ARGUMENT, "ray or output pointer is null");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  LaunchShape ls;
+  int32_t rc = launch_shape(ctx, st, ls);
+  if (rc != VKPTC_OK) return rc;
+  VKPTC_CUDA(ctx, LaunchTraceRays(dev_scene(ctx), d_rays, d_tmax, ray_count, mode == VKPTC_QUERY_ANY, d_prim_out,
+                                  d_t_out, ls, ctx->config.collect_stats ? ctx->d_ctr.ptr : nullptr, ctx->d_err.ptr),
+             "trace launch");
+  return VKPTC_OK;
+}
+
+int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, uint64_t ray_count, uint32_t mode,
+                         uint32_t* prim_out, float* t_out) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "acceleration structure not built");
+  if (ray_count && (!rays || !prim_out)) return fail(ctx, VKPTC_INVALID_ARGUMENT, "ray or output pointer is null");
+  if (ray_count == 0) return VKPTC_OK;
+  cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, ctx->q_rays.alloc(6 * ray_count), "query alloc");
+  VKPTC_CUDA(ctx, ctx->q_prim.alloc(ray_count), "query alloc");
+  VKPTC_CUDA(ctx, ctx->q_t.alloc(ray_count), "query alloc");
+  if (tmax) VKPTC_CUDA(ctx, ctx->q_tmax.alloc(ray_count), "query alloc");
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(ctx->q_rays.ptr, rays, 6 * ray_count * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "ray upload");
+  if (tmax) VKPTC_CUDA(ctx, cudaMemcpyAsync(ctx->q_tmax.ptr, tmax, ray_count * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "ray upload");
+  int32_t rc = vkptc_trace_rays_device(ctx, ctx->q_rays.ptr, tmax ? ctx->q_tmax.ptr : nullptr, ray_count, mode,
+                                       ctx->q_prim.ptr, ctx->q_t.ptr, nullptr);
+  if (rc != VKPTC_OK) return rc;
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(prim_out, ctx->q_prim.ptr, ray_count * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream), "result download");
+  if (t_out) VKPTC_CUDA(ctx, cudaMemcpyAsync(t_out, ctx->q_t.ptr, ray_count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream), "result download");
+  rc = check_device_error(ctx);
+  if (rc == VKPTC_OK) ctx->last_error.clear();
+  return rc;
+}
+
+}  // extern "C"

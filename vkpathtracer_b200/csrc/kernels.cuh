@@ -1,0 +1,77 @@
+// kernels.cuh -- launch interface of the wavefront render and ray-query kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace vkptc {
+
+// Queue and path-state buffers of one wave (structure of arrays, indexed by
+// path slot).  A wave is `sample_count` samples of every pixel of one
+// rectangular tile: slot = sample_local * tile_pixels + pixel_local.
+struct WaveState {
+  // path state
+  uint64_t* rng;
+  float4* ray_o;      // origin xyz
+  float4* ray_d;      // direction xyz
+  float4* thr;        // throughput xyz
+  float4* rad;        // radiance xyz, w = segment count
+  float2* hit;        // t, primitive index bits
+  // shadow queries
+  uint32_t* sh_path;
+  float4* sh_o;       // origin xyz, w = max distance
+  float4* sh_d;       // direction xyz
+  float4* sh_c;       // contribution to add when visible
+  // queues: q[0], q[1] ping-pong extension queues; counts[0..1] their sizes,
+  // counts[2] the shadow queue size
+  uint32_t* q[2];
+  uint32_t* counts;
+  uint32_t capacity;
+};
+
+struct WaveTile {
+  uint32_t x, y, w, h;     // pixel rectangle
+  uint32_t first_sample, sample_count;
+};
+
+struct Film {
+  float4* sum;           // rgb sum per pixel
+  uint32_t* count;
+  float* invalid;
+  uint32_t width, height;
+};
+
+struct DevCounters {
+  unsigned long long samples, rays, shadow_tests, dropped;
+  unsigned long long nodes, leaves, tris;
+  unsigned long long shadow_nodes, shadow_leaves, shadow_tris;
+};
+
+struct LaunchShape {
+  int grid;
+  int block;
+  int stack_cap;      // stack entries per thread
+  cudaStream_t stream;
+};
+
+size_t StackSmemBytes(int block, int cap);
+// Resident blocks per SM of the traversal stage for this block size and stack.
+int ExtendBlocksPerSm(int block, size_t smem);
+// Raises the dynamic shared-memory limit of every stack-using kernel.
+cudaError_t ConfigureStackSmem(size_t bytes);
+
+// Ray queries over one scene (rays: 6 floats each).
+cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* tmax, uint64_t n, bool any_hit,
+                            uint32_t* prim_out, float* t_out, const LaunchShape& ls, DevCounters* ctr,
+                            uint32_t* err);
+
+// One wave: raygen, max_depth x (extend, shade, shadow), accumulate.
+cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState& w, const WaveTile& tile,
+                       const Film& film, bool parity, bool stats, const LaunchShape& ls, DevCounters* ctr,
+                       uint32_t* err);
+
+// Film helpers.
+cudaError_t LaunchResolveHdr(const Film& film, float* rgb_out, cudaStream_t stream);
+
+}  // namespace vkptc

@@ -1,0 +1,348 @@
+// traverse.cuh -- wide-BVH closest-hit and any-hit traversal for sm_100a.
+//
+// Semantics are those of the reference accelerator
+// (src/pathtracer/CpuBvhAccelerator.cpp:113-154, 360-477) and its leaf test
+// (src/cpu/BvhTriangleIntersector.cpp:25-74):
+//  * Moller-Trumbore with |det| < 1e-4 rejected, no backface culling, a hit
+//    accepted when 1e-4 < t < best; evaluated in the reference's exact
+//    operation order without fused multiply-adds, so t is bit-identical.
+//  * Box test: slab from t = 1e-4, an axis with |d| <= 1e-4 is "parallel" and
+//    only checks that the origin lies inside the slab.  The node test here
+//    uses a fused lo*inv - o*inv form for speed; every triangle box is padded
+//    by 1e-4, which keeps a box that holds a valid hit inside the interval by
+//    far more than the rounding difference, so the set of reachable hits, and
+//    the parallel-axis culling, are the reference's.
+//  * Exact distance ties: the reference keeps the first triangle it visits
+//    (strict t < best), i.e. the earlier lane of one leaf, or for two leaves
+//    the one under the nearer child of their lowest common binary ancestor
+//    (left first when the entry distances are equal), since it traverses the
+//    binary tree depth first, near child first.  tie_candidate_wins()
+//    evaluates exactly that order from the binary tree kept beside the wide one.
+// Nodes are 128-byte lines fetched as eight 128-bit loads; triangles are
+// three 128-bit loads.  The stack holds (child ref, entry distance) pairs in
+// shared memory, interleaved per thread, and is sized on the host from the
+// BVH's exact worst case so it cannot overflow.
+#pragma once
+
+#include "common.cuh"
+
+namespace vkptc {
+
+#define kInf __int_as_float(0x7f800000)
+
+struct RayPrep {
+  float ox, oy, oz, dx, dy, dz;
+  float ix, iy, iz;      // 1/d, 0 on parallel axes
+  float nix, niy, niz;   // -o/d (for the fused node test)
+  uint32_t par;          // bit k: axis k is parallel
+};
+
+__device__ __forceinline__ RayPrep prep_ray(V3 o, V3 d) {
+  RayPrep r;
+  r.ox = o.x; r.oy = o.y; r.oz = o.z;
+  r.dx = d.x; r.dy = d.y; r.dz = d.z;
+  r.par = (fabsf(d.x) <= kEps ? 1u : 0u) | (fabsf(d.y) <= kEps ? 2u : 0u) | (fabsf(d.z) <= kEps ? 4u : 0u);
+  r.ix = (r.par & 1u) ? 0.0f : __fdiv_rn(1.0f, d.x);
+  r.iy = (r.par & 2u) ? 0.0f : __fdiv_rn(1.0f, d.y);
+  r.iz = (r.par & 4u) ? 0.0f : __fdiv_rn(1.0f, d.z);
+  r.nix = -(o.x * r.ix);
+  r.niy = -(o.y * r.iy);
+  r.niz = -(o.z * r.iz);
+  return r;
+}
+
+// The reference's slab test verbatim (no fusion); returns the entry distance.
+__device__ __forceinline__ bool ref_slab(const float lo[3], const float hi[3], const RayPrep& r, float tmax_in,
+                                         float& tnear) {
+  const float o[3] = {r.ox, r.oy, r.oz};
+  const float iv[3] = {r.ix, r.iy, r.iz};
+  float t_min = kEps, t_max = tmax_in;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (r.par & (1u << a)) {
+      if (o[a] < lo[a] || o[a] > hi[a]) return false;
+      continue;
+    }
+    float t0 = __fmul_rn(__fsub_rn(lo[a], o[a]), iv[a]);
+    float t1 = __fmul_rn(__fsub_rn(hi[a], o[a]), iv[a]);
+    if (t0 > t1) {
+      const float tmp = t0;
+      t0 = t1;
+      t1 = tmp;
+    }
+    t_min = smax(t_min, t0);
+    t_max = smin(t_max, t1);
+    if (t_min > t_max) return false;
+  }
+  tnear = t_min;
+  return t_max > kEps;
+}
+
+// Fused node test of one child slot; exact parallel-axis rule.
+__device__ __forceinline__ bool node_slab(float lx, float hx, float ly, float hy, float lz, float hz,
+                                          const RayPrep& r, float tmax_in, float& tnear) {
+  float ax0 = __fmaf_rn(lx, r.ix, r.nix), ax1 = __fmaf_rn(hx, r.ix, r.nix);
+  float ay0 = __fmaf_rn(ly, r.iy, r.niy), ay1 = __fmaf_rn(hy, r.iy, r.niy);
+  float az0 = __fmaf_rn(lz, r.iz, r.niz), az1 = __fmaf_rn(hz, r.iz, r.niz);
+  float nx = fminf(ax0, ax1), fx = fmaxf(ax0, ax1);
+  float ny = fminf(ay0, ay1), fy = fmaxf(ay0, ay1);
+  float nz = fminf(az0, az1), fz = fmaxf(az0, az1);
+  if (r.par) {
+    if (r.par & 1u) {
+      const bool in = !(r.ox < lx || r.ox > hx);
+      nx = in ? -kInf : kInf;
+      fx = kInf;
+    }
+    if (r.par & 2u) {
+      const bool in = !(r.oy < ly || r.oy > hy);
+      ny = in ? -kInf : kInf;
+      fy = kInf;
+    }
+    if (r.par & 4u) {
+      const bool in = !(r.oz < lz || r.oz > hz);
+      nz = in ? -kInf : kInf;
+      fz = kInf;
+    }
+  }
+  const float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, kEps));
+  const float tf = fminf(fminf(fx, fy), fminf(fz, tmax_in));
+  tnear = tn;
+  return tn <= tf && tf > kEps;
+}
+
+// Moller-Trumbore in the reference's operation order; returns t or -1.
+__device__ __forceinline__ float mt_test(const float4 a, const float4 b, const float4 c, const RayPrep& r) {
+  const float v0x = a.x, v0y = a.y, v0z = a.z;
+  const float e1x = a.w, e1y = b.x, e1z = b.y;
+  const float e2x = b.z, e2y = b.w, e2z = c.x;
+  const float hx = __fsub_rn(__fmul_rn(r.dy, e2z), __fmul_rn(r.dz, e2y));
+  const float hy = __fsub_rn(__fmul_rn(r.dz, e2x), __fmul_rn(r.dx, e2z));
+  const float hz = __fsub_rn(__fmul_rn(r.dx, e2y), __fmul_rn(r.dy, e2x));
+  const float det = __fadd_rn(__fadd_rn(__fmul_rn(e1x, hx), __fmul_rn(e1y, hy)), __fmul_rn(e1z, hz));
+  if (fabsf(det) < kEps) return -1.0f;
+  const float inv = __fdiv_rn(1.0f, det);
+  const float sx = __fsub_rn(r.ox, v0x), sy = __fsub_rn(r.oy, v0y), sz = __fsub_rn(r.oz, v0z);
+  const float u = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(sx, hx), __fmul_rn(sy, hy)), __fmul_rn(sz, hz)), inv);
+  if (u < 0.0f || u > 1.0f) return -1.0f;
+  const float qx = __fsub_rn(__fmul_rn(sy, e1z), __fmul_rn(sz, e1y));
+  const float qy = __fsub_rn(__fmul_rn(sz, e1x), __fmul_rn(sx, e1z));
+  const float qz = __fsub_rn(__fmul_rn(sx, e1y), __fmul_rn(sy, e1x));
+  const float v = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, qx), __fmul_rn(r.dy, qy)), __fmul_rn(r.dz, qz)), inv);
+  if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return -1.0f;
+  const float t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(e2x, qx), __fmul_rn(e2y, qy)), __fmul_rn(e2z, qz)), inv);
+  return t;
+}
+
+__device__ __forceinline__ void tie_box(const float4* tie, int32_t id, float lo[3], float hi[3]) {
+  const float4 a = __ldg(tie + 2 * id);
+  const float4 b = __ldg(tie + 2 * id + 1);
+  lo[0] = a.x; lo[1] = a.y; lo[2] = a.z;
+  hi[0] = b.x; hi[1] = b.y; hi[2] = b.z;
+}
+__device__ __forceinline__ int32_t tie_parent(const float4* tie, int32_t id) {
+  return __float_as_int(__ldg(tie + 2 * id).w);
+}
+__device__ __forceinline__ int32_t tie_depth(const float4* tie, int32_t id) {
+  return __float_as_int(__ldg(tie + 2 * id + 1).w);
+}
+
+// True when the candidate (leaf_b, lane_b) is visited before the incumbent
+// (leaf_a, lane_a) by the reference's depth-first near-first traversal.
+__device__ __noinline__ bool tie_candidate_wins(const float4* tie, const RayPrep& r, uint32_t leaf_a,
+                                                uint32_t lane_a, uint32_t leaf_b, uint32_t lane_b) {
+  if (leaf_a == leaf_b) return lane_b < lane_a;
+  int32_t a = static_cast<int32_t>(leaf_a), b = static_cast<int32_t>(leaf_b);
+  int32_t da = tie_depth(tie, a), db = tie_depth(tie, b);
+  while (da > db && a > 0) { a = tie_parent(tie, a); --da; }
+  while (db > da && b > 0) { b = tie_parent(tie, b); --db; }
+  // Climb together to the children of the lowest common ancestor; the root
+  // (id 0, parent -1) ends the walk on malformed input.
+  while (a > 0 && b > 0 && tie_parent(tie, a) != tie_parent(tie, b)) {
+    a = tie_parent(tie, a);
+    b = tie_parent(tie, b);
+  }
+  if (a <= 0 || b <= 0) return false;
+  float lo[3], hi[3];
+  float ta = 0.0f, tb = 0.0f;
+  tie_box(tie, a, lo, hi);
+  ref_slab(lo, hi, r, kInf, ta);
+  tie_box(tie, b, lo, hi);
+  ref_slab(lo, hi, r, kInf, tb);
+  // Sibling ids are allocated (left, right) consecutively: left is the smaller.
+  const bool a_left = a < b;
+  const float t_left = a_left ? ta : tb, t_right = a_left ? tb : ta;
+  const bool left_first = t_left <= t_right;
+  const bool a_first = (a_left == left_first);
+  return !a_first;
+}
+
+struct TraceStats {
+  uint32_t nodes = 0, leaves = 0, tris = 0;
+};
+
+// Shared-memory stack, interleaved so consecutive threads hit distinct banks.
+struct SmemStack {
+  int2* base;     // entry i of this thread at base[i * stride]
+  int stride;
+  int cap;
+};
+
+__device__ __forceinline__ int32_t leaf_first(int32_t ref) { return static_cast<int32_t>((~ref) >> 3); }
+__device__ __forceinline__ int32_t leaf_count(int32_t ref) { return ((~ref) & 7) + 1; }
+
+// Closest hit.  best_t = +inf and prim = kMiss on a miss.  `err` receives 1 on
+// a stack overflow (which the host-side sizing rules out).
+template <bool kStats>
+__device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& r, SmemStack stk, float& best_t,
+                                              uint32_t& best_prim, TraceStats& st, uint32_t& err) {
+  best_t = kInf;
+  best_prim = kMiss;
+  uint32_t best_leaf = 0u, best_lane = 0u;
+  int sp = 0;
+  int32_t ref = 0;
+  if (s.prim_count == 0u) return;
+  while (true) {
+    if (ref >= 0) {
+      const float4* np = s.nodes + 8 * ref;
+      const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+      const int n = __ldg(reinterpret_cast<const int*>(np + 7));
+      if (kStats) ++st.nodes;
+      float t[4];
+      int32_t c[4] = {ch.x, ch.y, ch.z, ch.w};
+      bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, best_t, t[0]);
+      bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, best_t, t[1]) && n > 1;
+      bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, best_t, t[2]) && n > 2;
+      bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, best_t, t[3]) && n > 3;
+      t[0] = h0 ? t[0] : kInf;
+      t[1] = h1 ? t[1] : kInf;
+      t[2] = h2 ? t[2] : kInf;
+      t[3] = h3 ? t[3] : kInf;
+      const int hits = int(h0) + int(h1) + int(h2) + int(h3);
+      // Sort (t, c) ascending with a 5-comparator network; misses sink (t = inf).
+#define VKPTC_CSWAP(i, j)                         \
+  if (t[j] < t[i]) {                              \
+    const float tt = t[i]; t[i] = t[j]; t[j] = tt; \
+    const int32_t cc = c[i]; c[i] = c[j]; c[j] = cc; \
+  }
+      VKPTC_CSWAP(0, 1) VKPTC_CSWAP(2, 3) VKPTC_CSWAP(0, 2) VKPTC_CSWAP(1, 3) VKPTC_CSWAP(1, 2)
+#undef VKPTC_CSWAP
+      if (hits > 0) {
+        // Push the farther hits, farthest first, continue with the nearest.
+#pragma unroll
+        for (int k = 3; k >= 1; --k) {
+          if (k < hits) {
+            if (sp < stk.cap) {
+              stk.base[sp * stk.stride] = make_int2(c[k], __float_as_int(t[k]));
+              ++sp;
+            } else {
+              err = 1u;
+            }
+          }
+        }
+        ref = c[0];
+        continue;
+      }
+    } else {
+      const int32_t first = leaf_first(ref);
+      const int32_t count = leaf_count(ref);
+      if (kStats) {
+        ++st.leaves;
+        st.tris += static_cast<uint32_t>(count);
+      }
+      for (int32_t i = 0; i < count; ++i) {
+        const float4* tp = s.tris + 3 * (first + i);
+        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+        const float th = mt_test(a, b, cc, r);
+        if (th <= kEps) continue;   // also rejects the -1 miss code
+        if (th < best_t) {
+          best_t = th;
+          best_prim = __float_as_uint(cc.y);
+          best_leaf = __float_as_uint(cc.z);
+          best_lane = __float_as_uint(cc.w);
+        } else if (th == best_t &&
+                   tie_candidate_wins(s.tie, r, best_leaf, best_lane, __float_as_uint(cc.z), __float_as_uint(cc.w))) {
+          best_prim = __float_as_uint(cc.y);
+          best_leaf = __float_as_uint(cc.z);
+          best_lane = __float_as_uint(cc.w);
+        }
+      }
+    }
+    // Pop the next entry that can still hold a hit no farther than best_t.
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      const int2 e = stk.base[sp * stk.stride];
+      if (__int_as_float(e.y) <= best_t) {
+        ref = e.x;
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+}
+
+// Any hit with 1e-4 < t < tmax.  Returns true when occluded.
+template <bool kStats>
+__device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, float tmax, SmemStack stk,
+                                          TraceStats& st, uint32_t& err) {
+  if (s.prim_count == 0u || !(tmax > kEps)) return false;
+  int sp = 0;
+  int32_t ref = 0;
+  while (true) {
+    if (ref >= 0) {
+      const float4* np = s.nodes + 8 * ref;
+      const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+      const int n = __ldg(reinterpret_cast<const int*>(np + 7));
+      if (kStats) ++st.nodes;
+      float t0, t1, t2, t3;
+      const bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, tmax, t0);
+      const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, tmax, t1) && n > 1;
+      const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, tmax, t2) && n > 2;
+      const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, tmax, t3) && n > 3;
+      int32_t next = 0;
+      bool have = false;
+      const int32_t cs[4] = {ch.x, ch.y, ch.z, ch.w};
+      const bool hs[4] = {h0, h1, h2, h3};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (!hs[k]) continue;
+        if (!have) {
+          next = cs[k];
+          have = true;
+        } else if (sp < stk.cap) {
+          stk.base[sp * stk.stride] = make_int2(cs[k], 0);
+          ++sp;
+        } else {
+          err = 1u;
+        }
+      }
+      if (have) {
+        ref = next;
+        continue;
+      }
+    } else {
+      const int32_t first = leaf_first(ref);
+      const int32_t count = leaf_count(ref);
+      if (kStats) {
+        ++st.leaves;
+        st.tris += static_cast<uint32_t>(count);
+      }
+      for (int32_t i = 0; i < count; ++i) {
+        const float4* tp = s.tris + 3 * (first + i);
+        const float th = mt_test(__ldg(tp), __ldg(tp + 1), __ldg(tp + 2), r);
+        if (th > kEps && th < tmax) return true;
+      }
+    }
+    if (sp == 0) break;
+    --sp;
+    ref = stk.base[sp * stk.stride].x;
+  }
+  return false;
+}
+
+}  // namespace vkptc

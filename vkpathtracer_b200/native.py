@@ -1,0 +1,138 @@
+"""ctypes binding of libvkpt_cuda (include/vkptc.h).
+
+The library is built in-tree (vkpathtracer_b200/_lib/libvkpt_cuda.so).  There
+is no fallback: if the library is missing or has no CUDA device, loading or
+creating a context raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libvkpt_cuda.so")
+
+STATUS_NAMES = ["Ok", "Unsupported", "InvalidArgument", "NotReady", "Busy", "AllocFailed", "Timeout",
+                "Cancelled", "InternalError"]
+OK, UNSUPPORTED, INVALID_ARGUMENT, NOT_READY, BUSY, ALLOC_FAILED, TIMEOUT, CANCELLED, INTERNAL_ERROR = range(9)
+LIFECYCLE_NAMES = ["uninitialized", "configured", "scene_loaded", "ready", "failed"]
+QUERY_CLOSEST, QUERY_ANY = 0, 1
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
+                ("math_mode", ctypes.c_uint32), ("collect_stats", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 3)]
+
+
+class RenderSettingsC(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("max_depth", ctypes.c_uint32), ("seed", ctypes.c_uint64), ("enable_nee", ctypes.c_uint32),
+                ("enable_mis", ctypes.c_uint32), ("deterministic", ctypes.c_uint32),
+                ("rr_start_depth", ctypes.c_uint32), ("rr_min_survival", ctypes.c_float),
+                ("rr_max_survival", ctypes.c_float), ("camera_aperture_radius", ctypes.c_float),
+                ("camera_focus_distance", ctypes.c_float), ("firefly_clamp", ctypes.c_float),
+                ("reserved", ctypes.c_uint32)]
+
+
+class SceneView(ctypes.Structure):
+    _fields_ = [("vertices", ctypes.c_void_p), ("vertex_count", ctypes.c_uint32),
+                ("indices", ctypes.c_void_p), ("index_count", ctypes.c_uint32),
+                ("instances", ctypes.c_void_p), ("instance_count", ctypes.c_uint32),
+                ("materials", ctypes.c_void_p), ("material_count", ctypes.c_uint32),
+                ("lights", ctypes.c_void_p), ("light_count", ctypes.c_uint32),
+                ("environment", ctypes.c_float * 3), ("camera_position", ctypes.c_float * 3),
+                ("camera_target", ctypes.c_float * 3), ("camera_up", ctypes.c_float * 3),
+                ("camera_fov_deg", ctypes.c_float), ("camera_aperture_radius", ctypes.c_float),
+                ("camera_focus_distance", ctypes.c_float)]
+
+
+class BvhView(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("node_count", ctypes.c_uint32),
+                ("prim_indices", ctypes.c_void_p), ("prim_count", ctypes.c_uint32)]
+
+
+class Tile(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("sample_index", ctypes.c_uint32), ("tile_id", ctypes.c_uint32),
+                ("gpu_id", ctypes.c_uint32)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("samples", "rays", "triangle_tests", "sdf_tests", "sdf_steps",
+                                                "triangle_hits", "sdf_hits", "sdf_misses", "bvh_node_visits",
+                                                "bvh_leaf_visits", "shadow_tests")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+class TracerStatusC(ctypes.Structure):
+    _fields_ = [("lifecycle", ctypes.c_uint32), ("scene_loaded", ctypes.c_uint32), ("accel_valid", ctypes.c_uint32),
+                ("ready_to_render", ctypes.c_uint32), ("current_sample", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("last_sample_us", ctypes.c_uint64),
+                ("total_samples", ctypes.c_uint64), ("accumulation_gen", ctypes.c_uint64)]
+
+
+class AccelInfo(ctypes.Structure):
+    _fields_ = [("primitive_count", ctypes.c_uint32), ("binary_node_count", ctypes.c_uint32),
+                ("binary_leaf_count", ctypes.c_uint32), ("wide_node_count", ctypes.c_uint32),
+                ("wide_depth", ctypes.c_uint32), ("stack_required", ctypes.c_uint32),
+                ("build_ms", ctypes.c_double), ("device_bytes", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+P = ctypes.c_void_p
+U32, U64, I32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
+
+# name -> (restype, argtypes); every symbol include/vkptc.h declares.
+SIGNATURES = {
+    "vkptc_create": (I32, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
+    "vkptc_destroy": (I32, [P]),
+    "vkptc_configure": (I32, [P, ctypes.POINTER(RenderSettingsC)]),
+    "vkptc_load_scene": (I32, [P, ctypes.POINTER(SceneView)]),
+    "vkptc_build_acceleration": (I32, [P]),
+    "vkptc_load_bvh": (I32, [P, ctypes.POINTER(BvhView)]),
+    "vkptc_get_accel_info": (I32, [P, ctypes.POINTER(AccelInfo)]),
+    "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),
+    "vkptc_reset": (I32, [P]),
+    "vkptc_shutdown": (I32, [P]),
+    "vkptc_render": (I32, [P, ctypes.POINTER(Tile), U32, U32, P]),
+    "vkptc_render_frame": (I32, [P, U32, U32, U32]),
+    "vkptc_synchronize": (I32, [P]),
+    "vkptc_read_film": (I32, [P, P, P, P]),
+    "vkptc_resolve_hdr": (I32, [P, P]),
+    "vkptc_write_film": (I32, [P, P, P, P]),
+    "vkptc_read_counters": (I32, [P, ctypes.POINTER(Counters)]),
+    "vkptc_get_status": (I32, [P, ctypes.POINTER(TracerStatusC)]),
+    "vkptc_last_error": (ctypes.c_char_p, [P]),
+    "vkptc_trace_rays": (I32, [P, P, P, U64, U32, P, P]),
+    "vkptc_trace_rays_device": (I32, [P, P, P, U64, U32, P, P, P]),
+}
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libvkpt_cuda.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"libvkpt_cuda.so is not built ({path}); run `python -m vkpathtracer_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class VkptcError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        self.code = code
+        name = STATUS_NAMES[code] if 0 <= code < len(STATUS_NAMES) else str(code)
+        super().__init__(f"{name}: {message}")

@@ -1,0 +1,260 @@
+"""CudaPathTracer: the reference's IPathTracer contract over libvkpt_cuda.
+
+Method names, argument meaning and error behaviour follow
+`vkpt::pathtracer::IPathTracer` (src/pathtracer/PathTracer.h:1069-1184):
+configure / load_scene_snapshot / build_or_update_acceleration return a Status;
+reset_accumulation / render_tile / render_tiles return bool and record
+status().last_error; resolve_hdr returns the averaged film; read_counters
+returns SampleCounters.  trace_rays is the batched form of
+IRayAccelerator::intersect (src/pathtracer/PathTracer.h:1001-1036).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import threading
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import native
+from .scenes import RenderSettings, Scene
+
+
+@dataclasses.dataclass
+class Status:
+    code: int
+    message: str = ""
+
+    @property
+    def ok(self) -> bool:
+        return self.code == native.OK
+
+    def __bool__(self) -> bool:
+        return self.ok
+
+
+@dataclasses.dataclass
+class RenderTile:
+    """Mirror of RenderTile (src/pathtracer/PathTracer.h:914-922)."""
+    x: int = 0
+    y: int = 0
+    width: int = 0
+    height: int = 0
+    sample_index: int = 0
+    tile_id: int = 0
+    gpu_id: int = 0
+
+
+@dataclasses.dataclass
+class PathTracerStatus:
+    backend: str
+    lifecycle: str
+    scene_loaded: bool
+    accel_valid: bool
+    ready_to_render: bool
+    current_sample: int
+    last_sample_us: int
+    total_samples: int
+    accumulation_gen: int
+    last_error: str
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class CudaPathTracer:
+    """One GPU render context.  Not re-entrant: drive it from one thread."""
+
+    backend_name = "cuda-wavefront"
+
+    def __init__(self, device: int = 0, block_size: int = 0, stack_depth: int = 0, math_mode: int = 0,
+                 collect_stats: bool = False, wave_paths: int = 0):
+        self._lib = native.load()
+        cfg = native.Config()
+        cfg.device = device
+        cfg.block_size = block_size
+        cfg.stack_depth = stack_depth
+        cfg.math_mode = math_mode
+        cfg.collect_stats = int(collect_stats)
+        cfg.reserved[0] = wave_paths
+        handle = ctypes.c_void_p()
+        rc = self._lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle))
+        if rc != native.OK:
+            raise native.VkptcError(rc, "vkptc_create failed (no CUDA device?)")
+        self._ctx = handle
+        self._settings: Optional[RenderSettings] = None
+        self._keep = None
+
+    # ------------------------------------------------------------ plumbing
+    def _err(self) -> str:
+        return self._lib.vkptc_last_error(self._ctx).decode()
+
+    def _status(self, rc: int) -> Status:
+        return Status(rc, "" if rc == native.OK else self._err())
+
+    def _check(self, rc: int):
+        if rc != native.OK:
+            raise native.VkptcError(rc, self._err())
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.vkptc_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------ lifecycle
+    def configure(self, settings: RenderSettings) -> Status:
+        s = native.RenderSettingsC()
+        s.width, s.height, s.spp, s.max_depth = settings.width, settings.height, settings.spp, settings.max_depth
+        s.seed = settings.seed
+        s.enable_nee, s.enable_mis = int(settings.enable_nee), int(settings.enable_mis)
+        s.deterministic = int(settings.deterministic)
+        s.rr_start_depth = settings.russian_roulette_start_depth
+        s.rr_min_survival = settings.russian_roulette_min_survival
+        s.rr_max_survival = settings.russian_roulette_max_survival
+        s.camera_aperture_radius = settings.camera_aperture_radius
+        s.camera_focus_distance = settings.camera_focus_distance
+        s.firefly_clamp = settings.firefly_clamp
+        st = self._status(self._lib.vkptc_configure(self._ctx, ctypes.byref(s)))
+        if st.ok:
+            self._settings = settings
+        return st
+
+    def load_scene_snapshot(self, scene: Scene) -> Status:
+        v = native.SceneView()
+        keep = (np.ascontiguousarray(scene.vertices, np.float32), np.ascontiguousarray(scene.indices, np.uint32),
+                np.ascontiguousarray(scene.instances, np.uint32), np.ascontiguousarray(scene.materials, np.float32),
+                np.ascontiguousarray(scene.lights, np.float32))
+        v.vertices, v.vertex_count = _ptr(keep[0]), keep[0].shape[0]
+        v.indices, v.index_count = _ptr(keep[1]), keep[1].size
+        v.instances, v.instance_count = _ptr(keep[2]), keep[2].shape[0]
+        v.materials, v.material_count = _ptr(keep[3]), keep[3].shape[0]
+        v.lights, v.light_count = (_ptr(keep[4]) if keep[4].size else None), keep[4].shape[0]
+        v.environment[:] = scene.environment
+        c = scene.camera
+        v.camera_position[:] = c.position
+        v.camera_target[:] = c.target
+        v.camera_up[:] = c.up
+        v.camera_fov_deg = c.fov_deg
+        v.camera_aperture_radius = c.aperture_radius
+        v.camera_focus_distance = c.focus_distance
+        return self._status(self._lib.vkptc_load_scene(self._ctx, ctypes.byref(v)))
+
+    def build_or_update_acceleration(self) -> Status:
+        return self._status(self._lib.vkptc_build_acceleration(self._ctx))
+
+    def load_bvh(self, nodes: np.ndarray, prim_indices: np.ndarray) -> Status:
+        """Adopts an externally built binary BVH (ParallelBvhBuilder layout, 10 words per node)."""
+        nodes = np.ascontiguousarray(nodes, np.uint32).reshape(-1, 10)
+        prim = np.ascontiguousarray(prim_indices, np.uint32)
+        b = native.BvhView(_ptr(nodes), nodes.shape[0], _ptr(prim), prim.size)
+        return self._status(self._lib.vkptc_load_bvh(self._ctx, ctypes.byref(b)))
+
+    def accel_info(self) -> dict:
+        a = native.AccelInfo()
+        self._check(self._lib.vkptc_get_accel_info(self._ctx, ctypes.byref(a)))
+        return a.as_dict()
+
+    def reset_accumulation(self) -> bool:
+        return self._lib.vkptc_reset(self._ctx) == native.OK
+
+    def shutdown(self):
+        self._lib.vkptc_shutdown(self._ctx)
+        self._settings = None
+
+    # ------------------------------------------------------------ rendering
+    def supports_tile_rendering(self) -> bool:
+        return True
+
+    def supports_tile_batching(self) -> bool:
+        return True
+
+    def render_tile(self, tile: RenderTile, frame_index: int = 0) -> bool:
+        return self.render_tiles([tile], frame_index)
+
+    def render_tile_cancellable(self, tile: RenderTile, frame_index: int, stop: Optional[threading.Event]) -> bool:
+        return self.render_tiles([tile], frame_index, stop)
+
+    def render_tiles(self, tiles: Sequence[RenderTile], frame_index: int = 0,
+                     stop: Optional[threading.Event] = None) -> bool:
+        if stop is not None and stop.is_set():
+            return False
+        arr = (native.Tile * max(1, len(tiles)))()
+        for i, t in enumerate(tiles):
+            arr[i] = native.Tile(t.x, t.y, t.width, t.height, t.sample_index, t.tile_id, t.gpu_id)
+        flag = ctypes.c_int32(0)
+        rc = self._lib.vkptc_render(self._ctx, arr, len(tiles), frame_index, ctypes.byref(flag))
+        return rc == native.OK
+
+    def render_frame(self, first_sample: int, sample_count: int, frame_index: int = 0, sync: bool = True):
+        """Renders full-frame samples [first, first+count) (batched render_tile calls)."""
+        self._check(self._lib.vkptc_render_frame(self._ctx, first_sample, sample_count, frame_index))
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        self._check(self._lib.vkptc_synchronize(self._ctx))
+
+    # ------------------------------------------------------------ film
+    def film(self):
+        """Raw film: (sum (H,W,3) float32, count (H,W) uint32, invalid (H,W) float32)."""
+        st = self._settings
+        W, H = st.width, st.height
+        s = np.zeros((H, W, 3), np.float32)
+        c = np.zeros((H, W), np.uint32)
+        inv = np.zeros((H, W), np.float32)
+        self._check(self._lib.vkptc_read_film(self._ctx, _ptr(s), _ptr(c), _ptr(inv)))
+        return s, c, inv
+
+    def resolve_hdr(self) -> np.ndarray:
+        st = self._settings
+        out = np.zeros((st.height, st.width, 3), np.float32)
+        self._check(self._lib.vkptc_resolve_hdr(self._ctx, _ptr(out)))
+        return out
+
+    def replace_film_history(self, film_sum: np.ndarray, count: np.ndarray, invalid: Optional[np.ndarray] = None) -> bool:
+        s = np.ascontiguousarray(film_sum, np.float32)
+        c = np.ascontiguousarray(count, np.uint32)
+        i = None if invalid is None else np.ascontiguousarray(invalid, np.float32)
+        return self._lib.vkptc_write_film(self._ctx, _ptr(s), _ptr(c), _ptr(i)) == native.OK
+
+    def read_counters(self) -> dict:
+        c = native.Counters()
+        self._check(self._lib.vkptc_read_counters(self._ctx, ctypes.byref(c)))
+        return c.as_dict()
+
+    def status(self) -> PathTracerStatus:
+        s = native.TracerStatusC()
+        self._lib.vkptc_get_status(self._ctx, ctypes.byref(s))
+        return PathTracerStatus("cuda-wavefront", native.LIFECYCLE_NAMES[s.lifecycle], bool(s.scene_loaded),
+                                bool(s.accel_valid), bool(s.ready_to_render), int(s.current_sample),
+                                int(s.last_sample_us), int(s.total_samples), int(s.accumulation_gen), self._err())
+
+    # ------------------------------------------------------------ ray queries
+    def trace_rays(self, rays: np.ndarray, mode: int = native.QUERY_CLOSEST, tmax: Optional[np.ndarray] = None):
+        """rays (N,6) float32 on the host -> (prim uint32, t float32)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        prim = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float32)
+        tm = None if tmax is None else np.ascontiguousarray(tmax, np.float32)
+        self._check(self._lib.vkptc_trace_rays(self._ctx, _ptr(rays), _ptr(tm), n, mode, _ptr(prim), _ptr(t)))
+        return prim, t
+
+    def trace_rays_device(self, d_rays: int, d_tmax: int, n: int, mode: int, d_prim: int, d_t: int, stream: int = 0):
+        """Device-pointer variant (e.g. torch tensors' data_ptr()); enqueued, not synchronised."""
+        self._check(self._lib.vkptc_trace_rays_device(self._ctx, d_rays, d_tmax or None, n, mode, d_prim,
+                                                      d_t or None, stream or None))
