@@ -202,6 +202,15 @@ int32_t vkptc_render(vkptc_ctx* ctx, const vkptc_tile* tiles, uint32_t tile_coun
 int32_t vkptc_render_frame(vkptc_ctx* ctx, uint32_t first_sample, uint32_t sample_count, uint32_t frame);
 /* Blocks until queued device work is done. */
 int32_t vkptc_synchronize(vkptc_ctx* ctx);
+/* Enqueues all further work of this context on `stream` (a cudaStream_t of
+ * the caller, e.g. its framework's current stream); NULL restores the
+ * context's own stream.  No synchronisation is implied. */
+int32_t vkptc_set_stream(vkptc_ctx* ctx, void* stream);
+/* Per-stage device time (CUDA events around every stage launch; enabled by
+ * vkptc_config.reserved[1] = 1).  ms_out[0..4] = raygen, extend (closest-hit
+ * traversal), shade, shadow (any-hit traversal), accumulate; launches_out
+ * (may be NULL) receives the launch count of each stage.  Reading resets. */
+int32_t vkptc_read_stage_times(vkptc_ctx* ctx, double* ms_out, uint64_t* launches_out);
 
 /* ---- film ---------------------------------------------------------------------
  * replaces IPathTracer::film() / FilmBuffer raw access (src/pathtracer/PathTracer.h:937-974):
@@ -214,6 +223,11 @@ int32_t vkptc_resolve_hdr(vkptc_ctx* ctx, float* rgb);
 int32_t vkptc_write_film(vkptc_ctx* ctx, const float* sum_rgb, const uint32_t* count, const float* invalid);
 /* replaces IPathTracer::read_counters (src/pathtracer/PathTracer.h:1180) */
 int32_t vkptc_read_counters(vkptc_ctx* ctx, vkptc_counters* out);
+/* This backend's traversal work, split by query kind (needs
+ * vkptc_config.collect_stats = 1): extension (closest-hit) rays, wide-node
+ * visits, leaf visits, triangle tests, then shadow (any-hit) rays, node
+ * visits, leaf visits, triangle tests -- out[8]. */
+int32_t vkptc_read_traversal_stats(vkptc_ctx* ctx, uint64_t* out);
 /* replaces IPathTracer::status (src/pathtracer/PathTracer.h:1181) */
 int32_t vkptc_get_status(vkptc_ctx* ctx, vkptc_tracer_status* out);
 /* Last error message of this context (empty when none); valid until the next call. */

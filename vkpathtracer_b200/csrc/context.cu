@@ -57,8 +57,14 @@ struct vkptc_ctx {
   vkptc_config config{};
   int device = 0;
   int sm_count = 148;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream all work is enqueued on
+  cudaStream_t own_stream = nullptr;  // the context's own stream
   std::string last_error;
+  // per-stage timing
+  StageTimer timer;
+  std::vector<cudaEvent_t> timer_events;
+  double stage_ms[StageTimer::kStages] = {0, 0, 0, 0, 0};
+  uint64_t stage_launches[StageTimer::kStages] = {0, 0, 0, 0, 0};
   bool configured = false, has_scene = false, accel_valid = false;
   uint32_t current_sample = 0;
   uint64_t last_sample_us = 0, accumulation_gen = 0;
@@ -317,9 +323,21 @@ int32_t run_wave(vkptc_ctx* c, const WaveTile& tile, uint32_t frame) {
   if (rc != VKPTC_OK) return rc;
   const DevScene s = dev_scene(c);
   const DevSettings st = dev_settings(c, frame);
+  StageTimer* timer = c->config.reserved[1] ? &c->timer : nullptr;
   VKPTC_CUDA(c, LaunchWave(s, st, wave_state(c), tile, film_of(c), c->config.math_mode == 0u,
-                           c->config.collect_stats != 0u, ls, c->d_ctr.ptr, c->d_err.ptr),
+                           c->config.collect_stats != 0u, ls, c->d_ctr.ptr, c->d_err.ptr, timer),
              "wave launch");
+  if (timer) {
+    // Fold this wave's event pairs into the per-stage totals.
+    VKPTC_CUDA(c, cudaStreamSynchronize(c->stream), "timer sync");
+    for (int k = 0; k < timer->used; ++k) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, timer->events[2 * k], timer->events[2 * k + 1]);
+      c->stage_ms[timer->stage_of[k]] += ms;
+      c->stage_launches[timer->stage_of[k]] += 1;
+    }
+    timer->used = 0;
+  }
   return VKPTC_OK;
 }
 
@@ -350,9 +368,16 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
     delete c;
     return VKPTC_INVALID_ARGUMENT;
   }
-  if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return VKPTC_INTERNAL_ERROR;
+  }
+  c->stream = c->own_stream;
+  if (c->config.reserved[1]) {
+    c->timer_events.resize(2 * 4096);
+    for (auto& e : c->timer_events) cudaEventCreate(&e);
+    c->timer.events = c->timer_events.data();
+    c->timer.capacity = 4096;
   }
   cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
   if (c->d_ctr.alloc(1) != cudaSuccess || c->d_err.alloc(1) != cudaSuccess ||
@@ -370,7 +395,8 @@ int32_t vkptc_destroy(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  cudaStream_t s = ctx->stream;
+  cudaStream_t s = ctx->own_stream;
+  for (auto& e : ctx->timer_events) cudaEventDestroy(e);
   delete ctx;
   if (s) cudaStreamDestroy(s);
   return VKPTC_OK;
@@ -606,6 +632,24 @@ int32_t vkptc_render_frame(vkptc_ctx* ctx, uint32_t first_sample, uint32_t sampl
   return VKPTC_OK;
 }
 
+int32_t vkptc_set_stream(vkptc_ctx* ctx, void* stream) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_read_stage_times(vkptc_ctx* ctx, double* ms_out, uint64_t* launches_out) {
+  if (!ctx || !ms_out) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->config.reserved[1]) return fail(ctx, VKPTC_UNSUPPORTED, "stage timing not enabled in vkptc_config");
+  for (int k = 0; k < StageTimer::kStages; ++k) {
+    ms_out[k] = ctx->stage_ms[k];
+    if (launches_out) launches_out[k] = ctx->stage_launches[k];
+    ctx->stage_ms[k] = 0.0;
+    ctx->stage_launches[k] = 0;
+  }
+  return VKPTC_OK;
+}
+
 int32_t vkptc_synchronize(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
@@ -677,6 +721,23 @@ int32_t vkptc_read_counters(vkptc_ctx* ctx, vkptc_counters* out) {
   out->triangle_tests = dc.tris + dc.shadow_tris;
   out->bvh_node_visits = dc.nodes + dc.shadow_nodes;
   out->bvh_leaf_visits = dc.leaves + dc.shadow_leaves;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_read_traversal_stats(vkptc_ctx* ctx, uint64_t* out) {
+  if (!ctx || !out) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  DevCounters dc{};
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(&dc, ctx->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost, ctx->stream), "counter read");
+  VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "counter read");
+  out[0] = dc.ext_rays;
+  out[1] = dc.nodes;
+  out[2] = dc.leaves;
+  out[3] = dc.tris;
+  out[4] = dc.shadow_rays;
+  out[5] = dc.shadow_nodes;
+  out[6] = dc.shadow_leaves;
+  out[7] = dc.shadow_tris;
   return VKPTC_OK;
 }
 

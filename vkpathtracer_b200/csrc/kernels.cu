@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_
       warp_count(&ctr->nodes, st.nodes);
       warp_count(&ctr->leaves, st.leaves);
       warp_count(&ctr->tris, st.tris);
+      warp_count(&ctr->ext_rays, j < n ? 1u : 0u);
     }
   }
   if (local_err) atomicOr(err, local_err);
@@ -532,6 +533,7 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene s, WaveState w, int cap
       warp_count(&ctr->shadow_nodes, st.nodes);
       warp_count(&ctr->shadow_leaves, st.leaves);
       warp_count(&ctr->shadow_tris, st.tris);
+      warp_count(&ctr->shadow_rays, j < n ? 1u : 0u);
     }
   }
   if (local_err) atomicOr(err, local_err);
@@ -579,23 +581,35 @@ __global__ void __launch_bounds__(256) k_accumulate(DevSettings st, WaveState w,
 
 cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState& w, const WaveTile& tile,
                        const Film& film, bool parity, bool stats, const LaunchShape& ls, DevCounters* ctr,
-                       uint32_t* err) {
+                       uint32_t* err, StageTimer* timer) {
   const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
+  StageTimer dummy;
+  StageTimer& tm = timer ? *timer : dummy;
+  tm.begin(0, ls.stream);
   if (parity) k_raygen<true><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, tile);
   else k_raygen<false><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, tile);
+  tm.end(ls.stream);
   uint32_t cur = 0u;
   for (uint32_t depth = 0; depth < st.max_depth; ++depth) {
+    tm.begin(1, ls.stream);
     if (stats) k_extend<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.stack_cap, ctr, err);
     else k_extend<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.stack_cap, ctr, err);
+    tm.end(ls.stream);
+    tm.begin(2, ls.stream);
     if (parity) k_shade<true><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
     else k_shade<false><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
+    tm.end(ls.stream);
     if (st.enable_nee) {
+      tm.begin(3, ls.stream);
       if (stats) k_shadow<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
       else k_shadow<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
+      tm.end(ls.stream);
     }
     cur ^= 1u;
   }
+  tm.begin(4, ls.stream);
   k_accumulate<<<ls.grid, ls.block, 0, ls.stream>>>(st, w, tile, film, ctr);
+  tm.end(ls.stream);
   return cudaGetLastError();
 }
 

@@ -46,6 +46,7 @@ struct DevCounters {
   unsigned long long samples, rays, shadow_tests, dropped;
   unsigned long long nodes, leaves, tris;
   unsigned long long shadow_nodes, shadow_leaves, shadow_tris;
+  unsigned long long ext_rays, shadow_rays;   // traversal queries issued (stats mode)
 };
 
 struct LaunchShape {
@@ -66,10 +67,29 @@ cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* t
                             uint32_t* prim_out, float* t_out, const LaunchShape& ls, DevCounters* ctr,
                             uint32_t* err);
 
+// Optional per-stage event timing: pairs of events recorded around each launch.
+struct StageTimer {
+  static constexpr int kStages = 5;   // raygen, extend, shade, shadow, accumulate
+  cudaEvent_t* events = nullptr;      // pool of event pairs
+  int capacity = 0;                   // pairs
+  int used = 0;
+  int stage_of[4096];
+  void begin(int stage, cudaStream_t s) {
+    if (!events || used >= capacity) return;
+    stage_of[used] = stage;
+    cudaEventRecord(events[2 * used], s);
+  }
+  void end(cudaStream_t s) {
+    if (!events || used >= capacity) return;
+    cudaEventRecord(events[2 * used + 1], s);
+    ++used;
+  }
+};
+
 // One wave: raygen, max_depth x (extend, shade, shadow), accumulate.
 cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState& w, const WaveTile& tile,
                        const Film& film, bool parity, bool stats, const LaunchShape& ls, DevCounters* ctr,
-                       uint32_t* err);
+                       uint32_t* err, StageTimer* timer);
 
 // Film helpers.
 cudaError_t LaunchResolveHdr(const Film& film, float* rgb_out, cudaStream_t stream);

@@ -102,11 +102,14 @@ SIGNATURES = {
     "vkptc_render": (I32, [P, ctypes.POINTER(Tile), U32, U32, P]),
     "vkptc_render_frame": (I32, [P, U32, U32, U32]),
     "vkptc_synchronize": (I32, [P]),
+    "vkptc_set_stream": (I32, [P, P]),
+    "vkptc_read_stage_times": (I32, [P, P, P]),
     "vkptc_read_film": (I32, [P, P, P, P]),
     "vkptc_resolve_hdr": (I32, [P, P]),
     "vkptc_write_film": (I32, [P, P, P, P]),
     "vkptc_read_counters": (I32, [P, ctypes.POINTER(Counters)]),
     "vkptc_get_status": (I32, [P, ctypes.POINTER(TracerStatusC)]),
+    "vkptc_read_traversal_stats": (I32, [P, P]),
     "vkptc_last_error": (ctypes.c_char_p, [P]),
     "vkptc_trace_rays": (I32, [P, P, P, U64, U32, P, P]),
     "vkptc_trace_rays_device": (I32, [P, P, P, U64, U32, P, P, P]),

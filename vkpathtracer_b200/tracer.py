@@ -70,7 +70,7 @@ class CudaPathTracer:
     backend_name = "cuda-wavefront"
 
     def __init__(self, device: int = 0, block_size: int = 0, stack_depth: int = 0, math_mode: int = 0,
-                 collect_stats: bool = False, wave_paths: int = 0):
+                 collect_stats: bool = False, wave_paths: int = 0, stage_timing: bool = False):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -79,6 +79,7 @@ class CudaPathTracer:
         cfg.math_mode = math_mode
         cfg.collect_stats = int(collect_stats)
         cfg.reserved[0] = wave_paths
+        cfg.reserved[1] = int(stage_timing)
         handle = ctypes.c_void_p()
         rc = self._lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle))
         if rc != native.OK:
@@ -208,6 +209,19 @@ class CudaPathTracer:
     def synchronize(self):
         self._check(self._lib.vkptc_synchronize(self._ctx))
 
+    def set_stream(self, stream_handle: int):
+        """Enqueue all further work on this cudaStream_t (0 = the context's own stream)."""
+        self._check(self._lib.vkptc_set_stream(self._ctx, stream_handle or None))
+
+    STAGES = ("raygen", "extend", "shade", "shadow", "accumulate")
+
+    def read_stage_times(self) -> dict:
+        """{stage: (ms, launches)} since the last read (needs stage_timing=True)."""
+        ms = (ctypes.c_double * 5)()
+        n = (ctypes.c_uint64 * 5)()
+        self._check(self._lib.vkptc_read_stage_times(self._ctx, ms, n))
+        return {k: (ms[i], int(n[i])) for i, k in enumerate(self.STAGES)}
+
     # ------------------------------------------------------------ film
     def film(self):
         """Raw film: (sum (H,W,3) float32, count (H,W) uint32, invalid (H,W) float32)."""
@@ -235,6 +249,17 @@ class CudaPathTracer:
         c = native.Counters()
         self._check(self._lib.vkptc_read_counters(self._ctx, ctypes.byref(c)))
         return c.as_dict()
+
+    def traversal_stats(self) -> dict:
+        """Wide-BVH work split by query kind (needs collect_stats=True)."""
+        a = (ctypes.c_uint64 * 8)()
+        self._check(self._lib.vkptc_read_traversal_stats(self._ctx, a))
+        keys = ("rays", "nodes", "leaves", "tris", "shadow_rays", "shadow_nodes", "shadow_leaves", "shadow_tris")
+        return {k: int(a[i]) for i, k in enumerate(keys)}
+
+    def extension_counters(self) -> dict:
+        s = self.traversal_stats()
+        return {"rays": s["rays"], "nodes": s["nodes"], "tris": s["tris"], "leaves": s["leaves"]}
 
     def status(self) -> PathTracerStatus:
         s = native.TracerStatusC()
