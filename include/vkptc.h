@@ -247,6 +247,36 @@ int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, u
 int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float* d_tmax, uint64_t ray_count,
                                 uint32_t mode, uint32_t* d_prim_out, float* d_t_out, void* stream);
 
+/* ---- allocation-free rendering -------------------------------------------
+ * No counterpart in the reference: an extra entry point of this library.
+ *
+ * Renders one sample (tile->sample_index) of one tile without allocating any
+ * memory, for callers that cannot call cudaMalloc while they render: an
+ * engine whose GPU memory all comes from its own pooled allocator or fixed
+ * budget, a render loop recorded under CUDA stream capture (where a
+ * cudaMalloc would break the capture), or a real-time thread that must not
+ * block in the driver's allocator.  Scene and acceleration structure must
+ * already be loaded into ctx (that set-up may allocate); this call then
+ * takes its path queues from one fixed, file-scope device array sized for
+ * VKPTC_NOALLOC_MAX_PATHS paths (140 bytes per path, about 9.2 MB, held on
+ * every GPU that loads the library until the process exits) and adds the
+ * sample into the CALLER's device film:
+ *   d_film_sum   W*H float4 per pixel (rgb sum; w untouched), 16-byte aligned
+ *   d_film_count W*H uint32 sample counts
+ * (W, H from vkptc_configure; device memory of the context's device).
+ * A tile covering more than VKPTC_NOALLOC_MAX_PATHS pixels is rejected with
+ * VKPTC_INVALID_ARGUMENT and a message naming the limit.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  Every call shares the one array and it keeps
+ * the last call's contents, so calls whose GPU work overlaps (on different
+ * streams, or from different contexts on the same device) race: the caller
+ * must order them, e.g. on one stream.  Work is enqueued on `stream` (NULL =
+ * the context's stream) and the call returns without synchronising. */
+#define VKPTC_NOALLOC_MAX_PATHS 65536u
+int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* tile, uint32_t frame, float* d_film_sum,
+                                  uint32_t* d_film_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

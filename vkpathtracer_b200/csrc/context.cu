@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -803,3 +804,101 @@ int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, u
 }
 
 }  // extern "C"
+
+// ============================================================ allocation-free
+namespace {
+
+// Path-state bytes per path: rng (8) + seven float4 arrays (ray_o, ray_d,
+// thr, rad, sh_o, sh_d, sh_c: 112) + hit float2 (8) + three u32 queues (12).
+constexpr size_t kNoAllocPathBytes = 8 + 7 * 16 + 8 + 3 * 4;
+constexpr size_t kNoAllocArrays = 12;   // each array starts on a 256-byte boundary
+constexpr size_t kNoAllocBytes = VKPTC_NOALLOC_MAX_PATHS * kNoAllocPathBytes + (kNoAllocArrays + 1) * 256;
+
+// The scratch of vkptc_render_tile_noalloc: one per device, for the whole process.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (which must be current).
+cudaError_t noalloc_base(int device, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_base[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_base[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_base[device]);
+  return cudaSuccess;
+}
+
+template <typename T>
+T* carve(unsigned char*& cursor, size_t count) {
+  T* p = reinterpret_cast<T*>(cursor);
+  cursor += (count * sizeof(T) + 255) / 256 * 256;
+  return p;
+}
+
+}  // namespace
+
+extern "C" int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* tile, uint32_t frame,
+                                             float* d_film_sum, uint32_t* d_film_count, void* stream) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured || !ctx->has_scene || !ctx->accel_valid) {
+    return fail(ctx, VKPTC_NOT_READY, "render_tile_noalloc requires a configured tracer with a scene and a built acceleration structure");
+  }
+  if (!tile || !d_film_sum || !d_film_count) return fail(ctx, VKPTC_INVALID_ARGUMENT, "tile or film pointer is null");
+  if ((reinterpret_cast<uintptr_t>(d_film_sum) & 15u) != 0u) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "d_film_sum must be 16-byte aligned (float4 per pixel)");
+  }
+  const uint32_t x0 = std::min(tile->x, ctx->settings.width), y0 = std::min(tile->y, ctx->settings.height);
+  const uint32_t x1 = static_cast<uint32_t>(std::min<uint64_t>(ctx->settings.width, static_cast<uint64_t>(x0) + tile->width));
+  const uint32_t y1 = static_cast<uint32_t>(std::min<uint64_t>(ctx->settings.height, static_cast<uint64_t>(y0) + tile->height));
+  if (x0 >= x1 || y0 >= y1) return VKPTC_OK;
+  const uint64_t paths = static_cast<uint64_t>(x1 - x0) * (y1 - y0);
+  if (paths > VKPTC_NOALLOC_MAX_PATHS) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT,
+                "tile of " + std::to_string(paths) + " pixels exceeds the allocation-free limit of " +
+                    std::to_string(VKPTC_NOALLOC_MAX_PATHS) + " paths per call; split it into smaller tiles");
+  }
+  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) return fail(ctx, VKPTC_UNSUPPORTED, "device ordinal above 63");
+  cudaSetDevice(ctx->device);
+  unsigned char* base = nullptr;
+  VKPTC_CUDA(ctx, noalloc_base(ctx->device, &base), "cudaGetSymbolAddress of the allocation-free scratch");
+  const size_t n = VKPTC_NOALLOC_MAX_PATHS;
+  unsigned char* cur = base;
+  WaveState w{};
+  w.ray_o = carve<float4>(cur, n);
+  w.ray_d = carve<float4>(cur, n);
+  w.thr = carve<float4>(cur, n);
+  w.rad = carve<float4>(cur, n);
+  w.sh_o = carve<float4>(cur, n);
+  w.sh_d = carve<float4>(cur, n);
+  w.sh_c = carve<float4>(cur, n);
+  w.rng = carve<uint64_t>(cur, n);
+  w.hit = carve<float2>(cur, n);
+  w.q[0] = carve<uint32_t>(cur, n);
+  w.q[1] = carve<uint32_t>(cur, n);
+  w.sh_path = carve<uint32_t>(cur, n);
+  w.counts = carve<uint32_t>(cur, 4);   // set by the raygen stage of every call
+  w.capacity = VKPTC_NOALLOC_MAX_PATHS;
+  if (static_cast<size_t>(cur - base) > kNoAllocBytes) return fail(ctx, VKPTC_INTERNAL_ERROR, "scratch layout overflow");
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  LaunchShape ls;
+  const int32_t rc = launch_shape(ctx, st, ls);
+  if (rc != VKPTC_OK) return rc;
+  Film film{};
+  film.sum = reinterpret_cast<float4*>(d_film_sum);
+  film.count = d_film_count;
+  film.invalid = nullptr;
+  film.width = ctx->settings.width;
+  film.height = ctx->settings.height;
+  const WaveTile wt{x0, y0, x1 - x0, y1 - y0, tile->sample_index, 1u};
+  VKPTC_CUDA(ctx, LaunchWave(dev_scene(ctx), dev_settings(ctx, frame), w, wt, film, ctx->config.math_mode == 0u,
+                             ctx->config.collect_stats != 0u, ls, ctx->d_ctr.ptr, ctx->d_err.ptr, nullptr),
+             "allocation-free wave launch");
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}

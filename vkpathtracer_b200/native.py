@@ -113,7 +113,9 @@ SIGNATURES = {
     "vkptc_last_error": (ctypes.c_char_p, [P]),
     "vkptc_trace_rays": (I32, [P, P, P, U64, U32, P, P]),
     "vkptc_trace_rays_device": (I32, [P, P, P, U64, U32, P, P, P]),
+    "vkptc_render_tile_noalloc": (I32, [P, ctypes.POINTER(Tile), U32, P, P, P]),
 }
+NOALLOC_MAX_PATHS = 65536
 
 _LIB = None
 
