@@ -84,6 +84,10 @@ def build_ref(quiet: bool = True) -> Optional[str]:
         return REF_LIB if os.path.exists(REF_LIB) else None
     subprocess.run(["make", "-C", HERE, "ref", f"REF={REFERENCE_SRC}", "-j8"], check=True,
                    capture_output=quiet)
+    # The C++ IPathTracer adapter checker links the library; build it when the library exists.
+    lib = os.path.join(os.path.dirname(HERE), "vkpathtracer_b200", "_lib", "libvkpt_cuda.so")
+    if os.path.exists(lib):
+        subprocess.run(["make", "-C", HERE, "adapter", f"REF={REFERENCE_SRC}"], check=True, capture_output=quiet)
     return REF_LIB
 
 

@@ -1,0 +1,199 @@
+// adapter_check.cpp -- TEST: runs the reference's ScalarCpuPathTracer and the
+// cuda backend's CudaPathTracer through the reference's IPathTracer interface
+// on the same scene, with ptbench's render loop
+// (src/benchmark/BenchmarkRuntime.cpp:672-693), and compares the films.
+//
+// usage: adapter_check nodevice            (expects no CUDA device)
+//        adapter_check <scene.bin>         (scene + settings written by tests/test_adapter.py)
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "CudaPathTracer.h"
+#include "core/Logging.h"
+#include "pathtracer/PathTracer.h"
+
+namespace pt = vkpt::pathtracer;
+
+namespace {
+
+template <typename T>
+bool read_vec(std::ifstream& f, std::vector<T>& v, size_t n) {
+  v.resize(n);
+  return static_cast<bool>(f.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(n * sizeof(T))));
+}
+
+bool load(const char* path, pt::PathTracerSceneSnapshot& s, pt::RenderSettings& st) {
+  std::ifstream f(path, std::ios::binary);
+  uint32_t c[5];
+  if (!f.read(reinterpret_cast<char*>(c), sizeof(c))) return false;
+  std::vector<float> verts, mats, lights, env, cam;
+  std::vector<uint32_t> idx, inst, sets;
+  if (!read_vec(f, verts, 3 * c[0]) || !read_vec(f, idx, c[1]) || !read_vec(f, inst, 3 * c[2]) ||
+      !read_vec(f, mats, 16 * c[3]) || !read_vec(f, lights, 16 * c[4]) || !read_vec(f, env, 3) ||
+      !read_vec(f, cam, 12) || !read_vec(f, sets, 7)) {
+    return false;
+  }
+  uint64_t seed = 0;
+  float rr[2];
+  f.read(reinterpret_cast<char*>(&seed), 8);
+  f.read(reinterpret_cast<char*>(rr), 8);
+  for (uint32_t i = 0; i < c[0]; ++i) s.vertices.push_back(pt::Vec3{verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]});
+  s.indices = idx;
+  for (uint32_t i = 0; i < c[2]; ++i) {
+    pt::RTInstance r;
+    r.entity_id = i + 1;
+    r.first_triangle = inst[3 * i];
+    r.triangle_count = inst[3 * i + 1];
+    r.material_index = inst[3 * i + 2];
+    s.instances.push_back(r);
+  }
+  for (uint32_t i = 0; i < c[3]; ++i) {
+    const float* m = &mats[16 * i];
+    pt::RTMaterial r;
+    r.albedo = {m[0], m[1], m[2]};
+    r.emissive = {m[3], m[4], m[5]};
+    r.roughness = m[6];
+    r.material_model = static_cast<uint32_t>(m[7] + 0.5f);
+    r.metallic = m[8];
+    r.ior = m[9];
+    r.transmission = m[10];
+    r.clearcoat = m[11];
+    r.sheen = m[12];
+    r.anisotropy = m[13];
+    r.alpha = m[14];
+    s.materials.push_back(r);
+  }
+  for (uint32_t i = 0; i < c[4]; ++i) {
+    const float* l = &lights[16 * i];
+    pt::RTHitLight r;
+    r.position = {l[0], l[1], l[2]};
+    r.color = {l[3], l[4], l[5]};
+    r.intensity = l[6];
+    r.radius = l[7];
+    r.direction = {l[8], l[9], l[10]};
+    r.spot_inner_cos = l[11];
+    r.spot_outer_cos = l[12];
+    s.lights.push_back(r);
+  }
+  s.environment_color = {env[0], env[1], env[2]};
+  s.camera_position = {cam[0], cam[1], cam[2]};
+  s.camera_target = {cam[3], cam[4], cam[5]};
+  s.camera_up = {cam[6], cam[7], cam[8]};
+  s.camera_fov_deg = cam[9];
+  s.camera_aperture_radius = cam[10];
+  s.camera_focus_distance = cam[11];
+  st.width = sets[0];
+  st.height = sets[1];
+  st.spp = sets[2];
+  st.max_depth = sets[3];
+  st.enable_nee = sets[4] != 0;
+  st.enable_mis = sets[5] != 0;
+  st.russian_roulette_start_depth = sets[6];
+  st.seed = seed;
+  st.russian_roulette_min_survival = rr[0];
+  st.russian_roulette_max_survival = rr[1];
+  return true;
+}
+
+int failures = 0;
+void check(bool ok, const char* what) {
+  std::printf("%s %s\n", ok ? "PASS" : "FAIL", what);
+  if (!ok) ++failures;
+}
+
+bool render(pt::IPathTracer& t, const pt::PathTracerSceneSnapshot& s, const pt::RenderSettings& st) {
+  if (!t.configure(st) || !t.load_scene_snapshot(s) || !t.build_or_update_acceleration()) return false;
+  t.reset_accumulation();
+  for (uint32_t k = 0; k < st.spp; ++k) {
+    pt::RenderTile tile;
+    tile.width = st.width;
+    tile.height = st.height;
+    tile.sample_index = k;
+    if (!t.render_tile(tile, 0u)) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  vkpt::log::Logger::instance().set_min_severity(vkpt::log::Severity::Fatal);
+  if (argc < 2) return 2;
+  if (std::strcmp(argv[1], "nodevice") == 0) {
+    vkpt::gpu::cuda::CudaPathTracer t;
+    check(!t.is_valid(), "no device: context not created");
+    pt::RenderSettings st;
+    const auto s = t.configure(st);
+    check(!s && s.code == vkpt::core::StatusCode::Unsupported, "no device: configure returns Unsupported");
+    check(!t.render_tile(pt::RenderTile{}, 0), "no device: render_tile fails");
+    return failures == 0 ? 0 : 1;
+  }
+  pt::PathTracerSceneSnapshot scene;
+  pt::RenderSettings st;
+  if (!load(argv[1], scene, st)) {
+    std::printf("FAIL cannot read %s\n", argv[1]);
+    return 2;
+  }
+  check(pt::ValidateStandardPathTracerContract(pt::BuildStandardPathTracerContract()), "standard contract");
+
+  pt::ScalarCpuPathTracer ref;
+  vkpt::gpu::cuda::CudaPathTracer gpu;
+  check(gpu.is_valid(), "cuda context created");
+  // lifecycle errors before configure / before the scene
+  check(!gpu.render_tile(pt::RenderTile{}, 0), "render before configure fails");
+  check(gpu.status().lifecycle == pt::PathTracerLifecycle::Uninitialized, "lifecycle uninitialized");
+  check(render(ref, scene, st), "reference renders");
+  check(render(gpu, scene, st), "cuda backend renders through IPathTracer");
+  check(gpu.status().lifecycle == pt::PathTracerLifecycle::Ready && gpu.status().ready_to_render, "lifecycle ready");
+
+  const auto& a = ref.film();
+  const auto& b = gpu.film();
+  size_t same = 0, n = a.raw().size();
+  double se = 0.0, mean = 0.0;
+  bool counts_equal = a.sample_counts() == b.sample_counts();
+  for (size_t i = 0; i < n; ++i) {
+    const pt::Vec3 p = a.raw()[i], q = b.raw()[i];
+    if (std::memcmp(&p, &q, sizeof(p)) == 0) ++same;
+    se += (p.x - q.x) * (p.x - q.x) + (p.y - q.y) * (p.y - q.y) + (p.z - q.z) * (p.z - q.z);
+    mean += p.x + p.y + p.z;
+  }
+  const double rmse_rel = std::sqrt(se / (3.0 * n)) / (mean / (3.0 * n) + 1e-12);
+  std::printf("pixels %zu bit_identical %.4f rmse_rel %.3e\n", n, double(same) / n, rmse_rel);
+  check(counts_equal, "sample counts equal");
+  check(double(same) / n >= 0.97, "at least 97% of pixels bit-identical");
+  check(rmse_rel < 1e-3, "relative RMSE below 1e-3");
+  const auto ca = ref.read_counters(), cb = gpu.read_counters();
+  std::printf("samples %llu/%llu segments %llu/%llu shadow %llu/%llu\n", (unsigned long long)ca.samples,
+              (unsigned long long)cb.samples, (unsigned long long)ca.rays, (unsigned long long)cb.rays,
+              (unsigned long long)ca.shadow_tests, (unsigned long long)cb.shadow_tests);
+  check(ca.samples == cb.samples, "sample counters equal");
+  const auto hdr_a = ref.resolve_hdr(), hdr_b = gpu.resolve_hdr();
+  check(hdr_a.width == hdr_b.width && hdr_a.rgbf.size() == hdr_b.rgbf.size(), "resolve_hdr shape");
+  const auto ldr = gpu.resolve_ldr();
+  check(ldr.rgba8.size() == 4u * st.width * st.height, "resolve_ldr through the reference's ApplyFilmResolve");
+  // reset keeps the acceleration structure; the film starts over
+  check(gpu.reset_accumulation() && gpu.status().accel_valid && gpu.read_counters().samples == 0, "reset is film-only");
+  // tiles = full frame (CheckScalarRenderTilePrimitive, tests/snapshot_bus_smoke.cpp:1368-1435)
+  vkpt::gpu::cuda::CudaPathTracer tiled;
+  bool ok = tiled.configure(st) && tiled.load_scene_snapshot(scene) && tiled.build_or_update_acceleration();
+  tiled.reset_accumulation();
+  for (uint32_t k = 0; k < st.spp && ok; ++k) {
+    std::vector<pt::RenderTile> tiles(2);
+    tiles[0].width = tiles[1].width = st.width;
+    tiles[0].height = st.height / 2;
+    tiles[1].y = st.height / 2;
+    tiles[1].height = st.height - st.height / 2;
+    tiles[0].sample_index = tiles[1].sample_index = k;
+    ok = tiled.render_tiles(tiles, 0u, {});
+  }
+  const auto& c = tiled.film();
+  check(ok && std::memcmp(c.raw().data(), b.raw().data(), n * sizeof(pt::Vec3)) == 0, "render_tiles equals full frame");
+  gpu.shutdown();
+  check(gpu.status().lifecycle == pt::PathTracerLifecycle::Uninitialized, "shutdown");
+  return failures == 0 ? 0 : 1;
+}

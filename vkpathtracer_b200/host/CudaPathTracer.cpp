@@ -1,0 +1,266 @@
+// CudaPathTracer.cpp -- IPathTracer over libvkpt_cuda (see CudaPathTracer.h).
+#include "CudaPathTracer.h"
+
+#include <algorithm>
+#include <vector>
+
+#include "vkptc.h"
+
+namespace vkpt::gpu::cuda {
+
+namespace pt = vkpt::pathtracer;
+using vkpt::core::Status;
+using vkpt::core::StatusCode;
+
+CudaPathTracer::CudaPathTracer(CudaPathTracerConfig config) {
+  vkptc_config c{};
+  c.device = config.device;
+  c.block_size = config.block_size;
+  c.math_mode = config.math_mode;
+  c.collect_stats = config.collect_stats ? 1u : 0u;
+  const int32_t rc = vkptc_create(&c, &m_ctx);
+  if (rc != VKPTC_OK) {
+    m_ctx = nullptr;
+    m_last_error = rc == VKPTC_UNSUPPORTED ? "no CUDA device available for the cuda backend"
+                                           : "vkptc_create failed";
+  }
+}
+
+CudaPathTracer::~CudaPathTracer() {
+  if (m_ctx) vkptc_destroy(m_ctx);
+}
+
+bool CudaPathTracer::fail(const std::string& message) const {
+  m_last_error = message;
+  return false;
+}
+
+Status CudaPathTracer::status_from(int32_t code, const char* operation) const {
+  if (code == VKPTC_OK) {
+    m_last_error.clear();
+    return Status::ok(std::string(operation) + " succeeded");
+  }
+  m_last_error = m_ctx ? vkptc_last_error(m_ctx) : m_last_error;
+  if (m_last_error.empty()) m_last_error = std::string(operation) + " failed";
+  return Status::error(static_cast<StatusCode>(code), m_last_error);
+}
+
+Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
+  if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
+  vkptc_render_settings s{};
+  s.width = settings.width;
+  s.height = settings.height;
+  s.spp = settings.spp;
+  s.max_depth = settings.max_depth;
+  s.seed = settings.seed;
+  s.enable_nee = settings.enable_nee ? 1u : 0u;
+  s.enable_mis = settings.enable_mis ? 1u : 0u;
+  s.deterministic = settings.deterministic ? 1u : 0u;
+  s.rr_start_depth = settings.russian_roulette_start_depth;
+  s.rr_min_survival = settings.russian_roulette_min_survival;
+  s.rr_max_survival = settings.russian_roulette_max_survival;
+  s.camera_aperture_radius = settings.camera_aperture_radius;
+  s.camera_focus_distance = settings.camera_focus_distance;
+  const Status st = status_from(vkptc_configure(m_ctx, &s), "configure");
+  if (st) {
+    m_settings = settings;
+    m_resolve = settings.film_resolve;
+    m_film = pt::FilmBuffer{settings.width, settings.height};
+    m_film.set_resolve_settings(m_resolve);
+  }
+  return st;
+}
+
+Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& scene) {
+  if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
+  if (!scene.sdf_primitives.empty() || !scene.environment_map.empty()) {
+    fail("the cuda backend renders triangle scenes with a constant environment (no SDF primitives, no environment map)");
+    return Status::error(StatusCode::Unsupported, m_last_error);
+  }
+  for (const auto& inst : scene.instances) {
+    if (inst.has_flag(pt::kRTInstanceFlagDynamicTransform) && inst.local_vertex_count > 0u &&
+        inst.local_index_count > 0u) {
+      fail("dynamic-transform instances with local geometry are not supported by the cuda backend yet");
+      return Status::error(StatusCode::Unsupported, m_last_error);
+    }
+  }
+  // Standard GPU word maps (src/gpu/VulkanGpuPathTracer.cpp:323-338, 381-396).
+  std::vector<float> mats(16 * scene.materials.size(), 0.0f);
+  for (size_t i = 0; i < scene.materials.size(); ++i) {
+    const pt::RTMaterial& m = scene.materials[i];
+    float* w = &mats[16 * i];
+    w[0] = m.albedo.x; w[1] = m.albedo.y; w[2] = m.albedo.z;
+    w[3] = m.emissive.x; w[4] = m.emissive.y; w[5] = m.emissive.z;
+    w[6] = m.roughness;
+    w[7] = static_cast<float>(m.material_model);
+    w[8] = m.metallic; w[9] = m.ior; w[10] = m.transmission; w[11] = m.clearcoat;
+    w[12] = m.sheen; w[13] = m.anisotropy; w[14] = m.alpha;
+    w[15] = static_cast<float>((m.material_effect & 1023u) | ((m.material_flags & 1u) ? 1024u : 0u));
+  }
+  std::vector<float> lights(16 * scene.lights.size(), 0.0f);
+  for (size_t i = 0; i < scene.lights.size(); ++i) {
+    const pt::RTHitLight& l = scene.lights[i];
+    float* w = &lights[16 * i];
+    w[0] = l.position.x; w[1] = l.position.y; w[2] = l.position.z;
+    w[3] = l.color.x; w[4] = l.color.y; w[5] = l.color.z;
+    w[6] = l.intensity; w[7] = std::max(0.0f, l.radius);
+    w[8] = l.direction.x; w[9] = l.direction.y; w[10] = l.direction.z;
+    w[11] = l.spot_inner_cos; w[12] = l.spot_outer_cos;
+  }
+  std::vector<uint32_t> inst(3 * scene.instances.size());
+  for (size_t i = 0; i < scene.instances.size(); ++i) {
+    inst[3 * i + 0] = scene.instances[i].first_triangle;
+    inst[3 * i + 1] = scene.instances[i].triangle_count;
+    inst[3 * i + 2] = scene.instances[i].material_index;
+  }
+  vkptc_scene_view v{};
+  v.vertices = reinterpret_cast<const float*>(scene.vertices.data());   // Vec3 is three packed floats
+  v.vertex_count = static_cast<uint32_t>(scene.vertices.size());
+  v.indices = scene.indices.data();
+  v.index_count = static_cast<uint32_t>(scene.indices.size());
+  v.instances = inst.data();
+  v.instance_count = static_cast<uint32_t>(scene.instances.size());
+  v.materials = mats.data();
+  v.material_count = static_cast<uint32_t>(scene.materials.size());
+  v.lights = lights.empty() ? nullptr : lights.data();
+  v.light_count = static_cast<uint32_t>(scene.lights.size());
+  v.environment[0] = scene.environment_color.x;
+  v.environment[1] = scene.environment_color.y;
+  v.environment[2] = scene.environment_color.z;
+  const pt::Vec3 cam[3] = {scene.camera_position, scene.camera_target, scene.camera_up};
+  float* dst[3] = {v.camera_position, v.camera_target, v.camera_up};
+  for (int k = 0; k < 3; ++k) {
+    dst[k][0] = cam[k].x;
+    dst[k][1] = cam[k].y;
+    dst[k][2] = cam[k].z;
+  }
+  v.camera_fov_deg = scene.camera_fov_deg;
+  v.camera_aperture_radius = scene.camera_aperture_radius;
+  v.camera_focus_distance = scene.camera_focus_distance;
+  const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
+  if (st) m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
+  return st;
+}
+
+Status CudaPathTracer::build_or_update_acceleration() {
+  if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
+  return status_from(vkptc_build_acceleration(m_ctx), "build_or_update_acceleration");
+}
+
+bool CudaPathTracer::reset_accumulation() {
+  if (!m_ctx) return fail("no cuda context");
+  return static_cast<bool>(status_from(vkptc_reset(m_ctx), "reset_accumulation"));
+}
+
+bool CudaPathTracer::replace_film_history(const pt::FilmBuffer& film) {
+  if (!m_ctx) return fail("no cuda context");
+  if (film.width() != m_settings.width || film.height() != m_settings.height) {
+    return fail("replace_film_history dimensions do not match");
+  }
+  const auto& raw = film.raw();
+  return static_cast<bool>(status_from(
+      vkptc_write_film(m_ctx, reinterpret_cast<const float*>(raw.data()), film.sample_counts().data(),
+                       film.invalid_samples().data()),
+      "replace_film_history"));
+}
+
+bool CudaPathTracer::render_tile(const pt::RenderTile& tile, uint32_t frame_index) {
+  return render_tile_cancellable(tile, frame_index, {});
+}
+
+bool CudaPathTracer::render_tile_cancellable(const pt::RenderTile& tile, uint32_t frame_index,
+                                             std::stop_token stop) {
+  const pt::RenderTile one[1] = {tile};
+  return render_tiles(std::span<const pt::RenderTile>(one, 1), frame_index, stop);
+}
+
+bool CudaPathTracer::render_tiles(std::span<const pt::RenderTile> tiles, std::uint32_t frame_index,
+                                  std::stop_token stop) {
+  if (!m_ctx) return fail("no cuda context");
+  if (stop.stop_requested()) return fail("render_tile cancelled before work started");
+  std::vector<vkptc_tile> t(tiles.size());
+  for (size_t i = 0; i < tiles.size(); ++i) {
+    t[i] = vkptc_tile{tiles[i].x, tiles[i].y, tiles[i].width, tiles[i].height, tiles[i].sample_index,
+                      tiles[i].tile_id, tiles[i].gpu_id};
+  }
+  return static_cast<bool>(status_from(
+      vkptc_render(m_ctx, t.data(), static_cast<uint32_t>(t.size()), frame_index, nullptr), "render_tile"));
+}
+
+const pt::FilmBuffer& CudaPathTracer::film() const {
+  if (!m_ctx) return m_film;
+  const size_t n = static_cast<size_t>(m_settings.width) * m_settings.height;
+  std::vector<float> sum(3 * n);
+  std::vector<uint32_t> cnt(n);
+  std::vector<float> inv(n);
+  if (vkptc_read_film(m_ctx, sum.data(), cnt.data(), inv.data()) != VKPTC_OK) {
+    m_last_error = vkptc_last_error(m_ctx);
+    return m_film;
+  }
+  for (uint32_t y = 0; y < m_settings.height; ++y) {
+    for (uint32_t x = 0; x < m_settings.width; ++x) {
+      const size_t i = static_cast<size_t>(y) * m_settings.width + x;
+      m_film.set_pixel_raw(x, y, pt::Vec3{sum[3 * i], sum[3 * i + 1], sum[3 * i + 2]}, cnt[i], inv[i]);
+    }
+  }
+  return m_film;
+}
+
+pt::FilmHdr CudaPathTracer::resolve_hdr() const {
+  pt::FilmHdr out;
+  if (!m_ctx) return out;
+  out.width = m_settings.width;
+  out.height = m_settings.height;
+  out.rgbf.resize(3 * static_cast<size_t>(out.width) * out.height);
+  if (vkptc_resolve_hdr(m_ctx, out.rgbf.data()) != VKPTC_OK) {
+    m_last_error = vkptc_last_error(m_ctx);
+    return pt::FilmHdr{};
+  }
+  return out;
+}
+
+pt::FilmLdr CudaPathTracer::resolve_ldr() const {
+  // Tone mapping stays the reference's own host code (ApplyFilmResolve); only HDR comes from the device.
+  return pt::ApplyFilmResolve(resolve_hdr(), m_film.resolve_settings());
+}
+
+pt::SampleCounters CudaPathTracer::read_counters() const {
+  pt::SampleCounters out{};
+  vkptc_counters c{};
+  if (m_ctx && vkptc_read_counters(m_ctx, &c) == VKPTC_OK) {
+    out.samples = c.samples;
+    out.rays = c.rays;
+    out.triangle_tests = c.triangle_tests;
+    out.triangle_hits = c.triangle_hits;
+    out.bvh_node_visits = c.bvh_node_visits;
+    out.bvh_leaf_visits = c.bvh_leaf_visits;
+    out.shadow_tests = c.shadow_tests;
+  }
+  return out;
+}
+
+pt::PathTracerStatus CudaPathTracer::status() const {
+  pt::PathTracerStatus out;
+  out.backend = "cuda-wavefront";
+  out.last_error = m_last_error;
+  vkptc_tracer_status s{};
+  if (m_ctx && vkptc_get_status(m_ctx, &s) == VKPTC_OK) {
+    out.lifecycle = static_cast<pt::PathTracerLifecycle>(s.lifecycle);
+    out.scene_loaded = s.scene_loaded != 0u;
+    out.accel_valid = s.accel_valid != 0u;
+    out.ready_to_render = s.ready_to_render != 0u;
+    out.current_sample = s.current_sample;
+    out.last_sample_us = s.last_sample_us;
+    out.total_samples = s.total_samples;
+    out.accumulation_gen = s.accumulation_gen;
+  }
+  return out;
+}
+
+void CudaPathTracer::shutdown() {
+  if (m_ctx) vkptc_shutdown(m_ctx);
+  m_film = pt::FilmBuffer{};
+  m_last_error.clear();
+}
+
+}  // namespace vkpt::gpu::cuda
