@@ -58,9 +58,12 @@ typedef struct vkptc_ctx vkptc_ctx;
 typedef struct vkptc_config {
   int32_t device;            /* CUDA device ordinal */
   uint32_t block_size;       /* threads per block of the wavefront kernels; 0 = autotuned/default */
-  uint32_t stack_depth;      /* traversal stack entries per thread in shared memory; 0 = from the BVH */
+  uint32_t stack_depth;      /* traversal stack entries per thread kept in shared memory (the rest
+                                spill to global memory); 0 = 16 */
   uint32_t math_mode;        /* 0 = parity (transcendentals in FP64, rounded once), 1 = fast FP32 */
   uint32_t collect_stats;    /* 1 = count node/leaf/triangle visits (device counters) */
+  /* reserved[0]: paths per wave (0 = 4 Mi); reserved[1]: 1 = per-stage CUDA-event timing;
+   * reserved[2]: traversal steps between warp refills (0 = 4) */
   uint32_t reserved[3];
 } vkptc_config;
 

@@ -97,9 +97,11 @@ struct vkptc_ctx {
   uint32_t wave_capacity = 0;
   size_t smem_configured = 48 * 1024;
 
-  // counters and error word
+  // counters, error word, fetch counter of the ray-query kernel, stack spill
   DevBuf<DevCounters> d_ctr;
   DevBuf<uint32_t> d_err;
+  DevBuf<uint32_t> d_fetch;
+  DevBuf<int2> d_spill;
 
   // ray-query scratch for host-buffer calls
   DevBuf<float> q_rays, q_tmax, q_t;
@@ -188,37 +190,52 @@ int block_size(const vkptc_ctx* c) {
 }
 
 int stack_cap(const vkptc_ctx* c) {
-  const int need = static_cast<int>(std::max<uint32_t>(1u, c->wide.stack_required));
-  const int asked = static_cast<int>(c->config.stack_depth);
-  return std::max(need, asked);
+  return static_cast<int>(std::max<uint32_t>(1u, c->wide.stack_required));
 }
+
+constexpr int kDefaultSmemEntries = 16;
+constexpr int kDefaultSteps = 4;
 
 int32_t ensure_stack_smem(vkptc_ctx* c, const LaunchShape& ls);
 
-// Block size, stack capacity and a grid of (resident blocks per SM) x SMs for
-// the grid-stride stage kernels; raises the shared-memory limit first.
-int32_t launch_shape(vkptc_ctx* c, cudaStream_t stream, LaunchShape& ls) {
+// Block size, stack split (shared-memory entries + global spill), steps between
+// warp refills, and a grid of (resident blocks per SM) x SMs: the traversal
+// kernels are persistent.  allow_spill = false keeps the whole stack in
+// shared memory (no spill buffer is needed, none is allocated).
+int32_t launch_shape(vkptc_ctx* c, cudaStream_t stream, LaunchShape& ls, bool allow_spill = true) {
   ls.block = block_size(c);
   ls.stack_cap = stack_cap(c);
+  const int asked = c->config.stack_depth ? static_cast<int>(c->config.stack_depth) : kDefaultSmemEntries;
+  ls.smem_entries = allow_spill ? std::min(ls.stack_cap, std::max(1, asked)) : ls.stack_cap;
+  ls.steps = c->config.reserved[2] ? static_cast<int>(c->config.reserved[2]) : kDefaultSteps;
   ls.stream = stream;
+  ls.spill = nullptr;
   const int32_t rc = ensure_stack_smem(c, ls);
   if (rc != VKPTC_OK) return rc;
-  const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
+  const size_t smem = StackSmemBytes(ls.block, ls.smem_entries);
   const int per_sm = ExtendBlocksPerSm(ls.block, smem);
   ls.grid = c->sm_count * per_sm;
+  const size_t spill = SpillEntries(ls);
+  if (spill > 0) {
+    if (c->d_spill.count < spill) VKPTC_CUDA(c, c->d_spill.alloc(spill), "stack spill alloc");
+    ls.spill = c->d_spill.ptr;
+  }
   return VKPTC_OK;
 }
 
 int32_t ensure_stack_smem(vkptc_ctx* c, const LaunchShape& ls) {
-  const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
+  const size_t smem = StackSmemBytes(ls.block, ls.smem_entries);
+  // The transmissive shadow kernel keeps its whole stack in shared memory.
+  const size_t smem_full = c->has_transmissive ? StackSmemBytes(ls.block, ls.stack_cap) : smem;
+  const size_t need = std::max(smem, smem_full);
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
-  if (smem > static_cast<size_t>(max_optin)) {
+  if (need > static_cast<size_t>(max_optin)) {
     return fail(c, VKPTC_UNSUPPORTED, "traversal stack does not fit in shared memory (BVH too deep for this block size)");
   }
-  if (smem > c->smem_configured) {
-    VKPTC_CUDA(c, ConfigureStackSmem(smem), "shared memory limit");
-    c->smem_configured = smem;
+  if (need > c->smem_configured) {
+    VKPTC_CUDA(c, ConfigureStackSmem(need), "shared memory limit");
+    c->smem_configured = need;
   }
   return VKPTC_OK;
 }
@@ -238,7 +255,7 @@ int32_t ensure_wave(vkptc_ctx* c, uint32_t paths) {
   VKPTC_CUDA(c, c->w_sh_o.alloc(n), "wave alloc");
   VKPTC_CUDA(c, c->w_sh_d.alloc(n), "wave alloc");
   VKPTC_CUDA(c, c->w_sh_c.alloc(n), "wave alloc");
-  VKPTC_CUDA(c, c->w_counts.alloc(4), "wave alloc");
+  VKPTC_CUDA(c, c->w_counts.alloc(8), "wave alloc");
   c->wave_capacity = paths;
   return VKPTC_OK;
 }
@@ -381,7 +398,7 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
     c->timer.capacity = 4096;
   }
   cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
-  if (c->d_ctr.alloc(1) != cudaSuccess || c->d_err.alloc(1) != cudaSuccess ||
+  if (c->d_ctr.alloc(1) != cudaSuccess || c->d_err.alloc(1) != cudaSuccess || c->d_fetch.alloc(1) != cudaSuccess ||
       cudaMemset(c->d_ctr.ptr, 0, sizeof(DevCounters)) != cudaSuccess ||
       cudaMemset(c->d_err.ptr, 0, sizeof(uint32_t)) != cudaSuccess) {
     cudaStreamDestroy(c->stream);
@@ -774,8 +791,10 @@ int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float
   LaunchShape ls;
   int32_t rc = launch_shape(ctx, st, ls);
   if (rc != VKPTC_OK) return rc;
+  if (ray_count > 0xFFFFFFF0ull) return fail(ctx, VKPTC_INVALID_ARGUMENT, "at most 2^32 - 16 rays per call");
   VKPTC_CUDA(ctx, LaunchTraceRays(dev_scene(ctx), d_rays, d_tmax, ray_count, mode == VKPTC_QUERY_ANY, d_prim_out,
-                                  d_t_out, ls, ctx->config.collect_stats ? ctx->d_ctr.ptr : nullptr, ctx->d_err.ptr),
+                                  d_t_out, ls, ctx->config.collect_stats ? ctx->d_ctr.ptr : nullptr, ctx->d_err.ptr,
+                                  ctx->d_fetch.ptr),
              "trace launch");
   return VKPTC_OK;
 }
@@ -882,12 +901,12 @@ extern "C" int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* t
   w.q[0] = carve<uint32_t>(cur, n);
   w.q[1] = carve<uint32_t>(cur, n);
   w.sh_path = carve<uint32_t>(cur, n);
-  w.counts = carve<uint32_t>(cur, 4);   // set by the raygen stage of every call
+  w.counts = carve<uint32_t>(cur, 8);   // set by the raygen stage of every call
   w.capacity = VKPTC_NOALLOC_MAX_PATHS;
   if (static_cast<size_t>(cur - base) > kNoAllocBytes) return fail(ctx, VKPTC_INTERNAL_ERROR, "scratch layout overflow");
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
   LaunchShape ls;
-  const int32_t rc = launch_shape(ctx, st, ls);
+  const int32_t rc = launch_shape(ctx, st, ls, /*allow_spill=*/false);
   if (rc != VKPTC_OK) return rc;
   Film film{};
   film.sum = reinterpret_cast<float4*>(d_film_sum);

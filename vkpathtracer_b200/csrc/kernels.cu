@@ -23,66 +23,122 @@ namespace vkptc {
 
 size_t StackSmemBytes(int block, int cap) { return static_cast<size_t>(block) * cap * sizeof(int2); }
 
+size_t SpillEntries(const LaunchShape& ls) {
+  const int extra = ls.stack_cap - ls.smem_entries;
+  return extra > 0 ? static_cast<size_t>(ls.grid) * ls.block * extra : 0u;
+}
+
+// ============================================================ query sources
+// Each source supplies queries to persistent_traverse() and consumes results.
+struct RaysSource {   // batched ray queries from a ray array
+  const float* rays;
+  const float* tmax;
+  uint32_t* prim_out;
+  float* t_out;
+  bool any;
+  __device__ __forceinline__ void load(uint32_t j, V3& o, V3& d, float& tm) const {
+    const float2* rp = reinterpret_cast<const float2*>(rays + 6ull * j);
+    const float2 a = __ldg(rp), b = __ldg(rp + 1), c = __ldg(rp + 2);
+    o = mk(a.x, a.y, b.x);
+    d = mk(b.y, c.x, c.y);
+    tm = tmax ? __ldg(tmax + j) : kInf;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, float t, uint32_t prim) const {
+    prim_out[j] = prim;
+    if (t_out) t_out[j] = any ? (prim ? 0.0f : kInf) : t;
+  }
+};
+
+struct ExtendSource {  // closest hit for the queued paths of a wave
+  const uint32_t* q;
+  const float4* ray_o;
+  const float4* ray_d;
+  float2* hit;
+  __device__ __forceinline__ void load(uint32_t j, V3& o, V3& d, float& tm) const {
+    const uint32_t p = q[j];
+    const float4 a = ray_o[p], b = ray_d[p];
+    o = mk(a.x, a.y, a.z);
+    d = mk(b.x, b.y, b.z);
+    tm = kInf;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, float t, uint32_t prim) const {
+    hit[q[j]] = make_float2(t, __uint_as_float(prim));
+  }
+};
+
+struct ShadowSource {  // any hit for the NEE queries; adds the term when visible
+  const float4* sh_o;
+  const float4* sh_d;
+  const float4* sh_c;
+  const uint32_t* sh_path;
+  float4* rad;
+  __device__ __forceinline__ void load(uint32_t j, V3& o, V3& d, float& tm) const {
+    const float4 a = sh_o[j], b = sh_d[j];
+    o = mk(a.x, a.y, a.z);
+    d = mk(b.x, b.y, b.z);
+    tm = a.w;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, float, uint32_t occluded) const {
+    if (occluded) return;
+    const uint32_t p = sh_path[j];
+    const float4 c = sh_c[j];
+    float4 r = rad[p];
+    r.x = r.x + c.x;
+    r.y = r.y + c.y;
+    r.z = r.z + c.z;
+    rad[p] = r;
+  }
+};
+
+template <class Src, bool kAny, bool kStats>
+__device__ __forceinline__ void run_persistent(const DevScene& s, const Src& src, uint32_t n, uint32_t* fetch,
+                                               int scap, int2* spill, int total, int steps,
+                                               unsigned long long* c_nodes, unsigned long long* c_leaves,
+                                               unsigned long long* c_tris, unsigned long long* c_rays, uint32_t* err) {
+  extern __shared__ int2 smem_stack[];
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gstride = static_cast<int>(gridDim.x * blockDim.x);
+  TwoLevelStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), scap,
+                    spill ? spill + gtid : nullptr, gstride, total};
+  TraceStats st;
+  uint32_t lerr = 0u;
+  persistent_traverse<Src, kAny, kStats>(s, src, n, fetch, stk, steps, st, lerr);
+  if (kStats) {
+    warp_count(c_nodes, st.nodes);
+    warp_count(c_leaves, st.leaves);
+    warp_count(c_tris, st.tris);
+    warp_count(c_rays, st.rays);
+  }
+  if (lerr) atomicOr(err, lerr);
+}
+
 // =============================================================== ray queries
 template <bool kAny, bool kStats>
-__global__ void __launch_bounds__(256) k_trace_rays(DevScene s, const float* __restrict__ rays,
-                                                    const float* __restrict__ tmax, uint64_t n,
-                                                    uint32_t* __restrict__ prim_out, float* __restrict__ t_out,
-                                                    int cap, DevCounters* ctr, uint32_t* err) {
-  extern __shared__ int2 smem_stack[];
-  SmemStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), cap};
-  uint32_t local_err = 0u;
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x; base < n; base += stride) {
-    const uint64_t i = base + threadIdx.x;
-    TraceStats st;
-    if (i < n) {
-      const float2* rp = reinterpret_cast<const float2*>(rays + 6 * i);
-      const float2 a = __ldg(rp), b = __ldg(rp + 1), c = __ldg(rp + 2);
-      const RayPrep r = prep_ray(mk(a.x, a.y, b.x), mk(b.y, c.x, c.y));
-      if (kAny) {
-        const float tm = tmax ? __ldg(tmax + i) : kInf;
-        const bool occ = trace_any<kStats>(s, r, tm, stk, st, local_err);
-        prim_out[i] = occ ? 1u : 0u;
-        if (t_out) t_out[i] = occ ? 0.0f : kInf;
-      } else {
-        float t;
-        uint32_t p;
-        trace_closest<kStats>(s, r, stk, t, p, st, local_err);
-        prim_out[i] = p;
-        if (t_out) t_out[i] = t;
-      }
-    }
-    if (kStats) {
-      warp_count(&ctr->nodes, st.nodes);
-      warp_count(&ctr->leaves, st.leaves);
-      warp_count(&ctr->tris, st.tris);
-    }
-  }
-  if (local_err) atomicOr(err, local_err);
+__global__ void __launch_bounds__(256) k_trace_rays(DevScene s, RaysSource src, uint32_t n, uint32_t* fetch, int scap,
+                                                    int2* spill, int total, int steps, DevCounters* ctr, uint32_t* err) {
+  run_persistent<RaysSource, kAny, kStats>(s, src, n, fetch, scap, spill, total, steps, &ctr->nodes, &ctr->leaves,
+                                           &ctr->tris, &ctr->ext_rays, err);
 }
 
 cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* tmax, uint64_t n, bool any_hit,
                             uint32_t* prim_out, float* t_out, const LaunchShape& ls, DevCounters* ctr,
-                            uint32_t* err) {
+                            uint32_t* err, uint32_t* fetch) {
   if (n == 0) return cudaSuccess;
-  const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
-  const bool stats = ctr != nullptr;
+  const size_t smem = StackSmemBytes(ls.block, ls.smem_entries);
+  cudaError_t e = cudaMemsetAsync(fetch, 0, sizeof(uint32_t), ls.stream);
+  if (e != cudaSuccess) return e;
+  const RaysSource src{rays, tmax, prim_out, t_out, any_hit};
+  const uint32_t n32 = static_cast<uint32_t>(n);
+#define VKPTC_TR(A, S) \
+  k_trace_rays<A, S><<<ls.grid, ls.block, smem, ls.stream>>>(s, src, n32, fetch, ls.smem_entries, ls.spill, ls.stack_cap, ls.steps, ctr, err)
   if (any_hit) {
-    if (stats)
-      k_trace_rays<true, true><<<ls.grid, ls.block, smem, ls.stream>>>(s, rays, tmax, n, prim_out, t_out,
-                                                                       ls.stack_cap, ctr, err);
-    else
-      k_trace_rays<true, false><<<ls.grid, ls.block, smem, ls.stream>>>(s, rays, tmax, n, prim_out, t_out,
-                                                                        ls.stack_cap, ctr, err);
+    if (ctr) VKPTC_TR(true, true);
+    else VKPTC_TR(true, false);
   } else {
-    if (stats)
-      k_trace_rays<false, true><<<ls.grid, ls.block, smem, ls.stream>>>(s, rays, tmax, n, prim_out, t_out,
-                                                                        ls.stack_cap, ctr, err);
-    else
-      k_trace_rays<false, false><<<ls.grid, ls.block, smem, ls.stream>>>(s, rays, tmax, n, prim_out, t_out,
-                                                                         ls.stack_cap, ctr, err);
+    if (ctr) VKPTC_TR(false, true);
+    else VKPTC_TR(false, false);
   }
+#undef VKPTC_TR
   return cudaGetLastError();
 }
 
@@ -129,42 +185,25 @@ __global__ void __launch_bounds__(256) k_raygen(DevScene s, DevSettings st, Wave
     w.counts[0] = n;
     w.counts[1] = 0u;
     w.counts[2] = 0u;
+    w.counts[3] = 0u;   // extension fetch counter
+    w.counts[4] = 0u;   // shadow fetch counter
   }
 }
 
 // ==================================================================== extend
+// Closest-hit traversal of the current extension queue (persistent warps).
+// Zeroes the next queue's and the shadow queue's sizes for the shade stage.
 template <bool kStats>
-__global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_t cur, int cap, DevCounters* ctr,
-                                                uint32_t* err) {
-  extern __shared__ int2 smem_stack[];
-  SmemStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), cap};
+__global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_t cur, int scap, int2* spill,
+                                                int total, int steps, DevCounters* ctr, uint32_t* err) {
   const uint32_t n = w.counts[cur];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     w.counts[cur ^ 1u] = 0u;
     w.counts[2] = 0u;
   }
-  uint32_t local_err = 0u;
-  const uint32_t* q = w.q[cur];
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t j = base + threadIdx.x;
-    TraceStats st;
-    if (j < n) {
-      const uint32_t p = q[j];
-      const float4 o = w.ray_o[p], d = w.ray_d[p];
-      const RayPrep r = prep_ray(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z));
-      float t;
-      uint32_t prim;
-      trace_closest<kStats>(s, r, stk, t, prim, st, local_err);
-      w.hit[p] = make_float2(t, __uint_as_float(prim));
-    }
-    if (kStats) {
-      warp_count(&ctr->nodes, st.nodes);
-      warp_count(&ctr->leaves, st.leaves);
-      warp_count(&ctr->tris, st.tris);
-      warp_count(&ctr->ext_rays, j < n ? 1u : 0u);
-    }
-  }
-  if (local_err) atomicOr(err, local_err);
+  const ExtendSource src{w.q[cur], w.ray_o, w.ray_d, w.hit};
+  run_persistent<ExtendSource, false, kStats>(s, src, n, &w.counts[3], scap, spill, total, steps, &ctr->nodes,
+                                              &ctr->leaves, &ctr->tris, &ctr->ext_rays, err);
 }
 
 // ===================================================================== shade
@@ -316,6 +355,10 @@ __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveS
   }
   const float* lights = staged ? sm_lights : s.lights;
   const uint32_t n = w.counts[cur];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    w.counts[3] = 0u;   // the extension stage of the next depth fetches from 0
+    w.counts[4] = 0u;   // the shadow stage of this depth fetches from 0
+  }
   const uint32_t* q = w.q[cur];
   uint32_t* qn = w.q[cur ^ 1u];
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -479,8 +522,21 @@ __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveS
 }
 
 // ==================================================================== shadow
+// Any-hit visibility of the NEE queries (persistent warps); adds the NEE term
+// of every visible query to its path's radiance.
 template <bool kStats>
-__global__ void __launch_bounds__(256) k_shadow(DevScene s, WaveState w, int cap, DevCounters* ctr, uint32_t* err) {
+__global__ void __launch_bounds__(256) k_shadow(DevScene s, WaveState w, int scap, int2* spill, int total, int steps,
+                                                DevCounters* ctr, uint32_t* err) {
+  const uint32_t n = w.counts[2];
+  const ShadowSource src{w.sh_o, w.sh_d, w.sh_c, w.sh_path, w.rad};
+  run_persistent<ShadowSource, true, kStats>(s, src, n, &w.counts[4], scap, spill, total, steps, &ctr->shadow_nodes,
+                                             &ctr->shadow_leaves, &ctr->shadow_tris, &ctr->shadow_rays, err);
+}
+
+// Scenes with transmissive materials: the reference's closest-hit loop that
+// steps through up to 8 transmissive occluders (one query per thread).
+template <bool kStats>
+__global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveState w, int cap, DevCounters* ctr, uint32_t* err) {
   extern __shared__ int2 smem_stack[];
   SmemStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), cap};
   const uint32_t n = w.counts[2];
@@ -582,7 +638,8 @@ __global__ void __launch_bounds__(256) k_accumulate(DevSettings st, WaveState w,
 cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState& w, const WaveTile& tile,
                        const Film& film, bool parity, bool stats, const LaunchShape& ls, DevCounters* ctr,
                        uint32_t* err, StageTimer* timer) {
-  const size_t smem = StackSmemBytes(ls.block, ls.stack_cap);
+  const size_t smem = StackSmemBytes(ls.block, ls.smem_entries);
+  const size_t smem_full = StackSmemBytes(ls.block, ls.stack_cap);
   StageTimer dummy;
   StageTimer& tm = timer ? *timer : dummy;
   tm.begin(0, ls.stream);
@@ -592,8 +649,12 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
   uint32_t cur = 0u;
   for (uint32_t depth = 0; depth < st.max_depth; ++depth) {
     tm.begin(1, ls.stream);
-    if (stats) k_extend<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.stack_cap, ctr, err);
-    else k_extend<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.stack_cap, ctr, err);
+    if (stats)
+      k_extend<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.smem_entries, ls.spill, ls.stack_cap,
+                                                            ls.steps, ctr, err);
+    else
+      k_extend<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.smem_entries, ls.spill, ls.stack_cap,
+                                                             ls.steps, ctr, err);
     tm.end(ls.stream);
     tm.begin(2, ls.stream);
     if (parity) k_shade<true><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
@@ -601,8 +662,17 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
     tm.end(ls.stream);
     if (st.enable_nee) {
       tm.begin(3, ls.stream);
-      if (stats) k_shadow<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
-      else k_shadow<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
+      if (s.has_transmissive) {
+        if (stats) k_shadow_transmissive<true><<<ls.grid, ls.block, smem_full, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
+        else k_shadow_transmissive<false><<<ls.grid, ls.block, smem_full, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
+      } else {
+        if (stats)
+          k_shadow<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.smem_entries, ls.spill, ls.stack_cap,
+                                                                ls.steps, ctr, err);
+        else
+          k_shadow<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.smem_entries, ls.spill, ls.stack_cap,
+                                                                 ls.steps, ctr, err);
+      }
       tm.end(ls.stream);
     }
     cur ^= 1u;
@@ -642,6 +712,8 @@ cudaError_t ConfigureStackSmem(size_t bytes) {
   if (e == cudaSuccess) e = set_smem(k_extend<false>, b);
   if (e == cudaSuccess) e = set_smem(k_shadow<true>, b);
   if (e == cudaSuccess) e = set_smem(k_shadow<false>, b);
+  if (e == cudaSuccess) e = set_smem(k_shadow_transmissive<true>, b);
+  if (e == cudaSuccess) e = set_smem(k_shadow_transmissive<false>, b);
   return e;
 }
 

@@ -50,22 +50,28 @@ struct DevCounters {
 };
 
 struct LaunchShape {
-  int grid;
+  int grid;           // resident blocks x SMs (the traversal kernels are persistent)
   int block;
-  int stack_cap;      // stack entries per thread
+  int stack_cap;      // traversal stack entries per thread (worst case of the BVH)
+  int smem_entries;   // of which held in shared memory; the rest spill to `spill`
+  int steps;          // traversal steps between warp refills
+  int2* spill;        // grid*block*(stack_cap - smem_entries) entries, or null
   cudaStream_t stream;
 };
 
 size_t StackSmemBytes(int block, int cap);
+// Spill entries the launch needs beyond shared memory.
+size_t SpillEntries(const LaunchShape& ls);
 // Resident blocks per SM of the traversal stage for this block size and stack.
 int ExtendBlocksPerSm(int block, size_t smem);
 // Raises the dynamic shared-memory limit of every stack-using kernel.
 cudaError_t ConfigureStackSmem(size_t bytes);
 
 // Ray queries over one scene (rays: 6 floats each).
+// `fetch` is a device counter the persistent kernel claims query ids from.
 cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* tmax, uint64_t n, bool any_hit,
                             uint32_t* prim_out, float* t_out, const LaunchShape& ls, DevCounters* ctr,
-                            uint32_t* err);
+                            uint32_t* err, uint32_t* fetch);
 
 // Optional per-stage event timing: pairs of events recorded around each launch.
 struct StageTimer {

@@ -148,9 +148,16 @@ __device__ __forceinline__ int32_t tie_depth(const float4* tie, int32_t id) {
 
 // True when the candidate (leaf_b, lane_b) is visited before the incumbent
 // (leaf_a, lane_a) by the reference's depth-first near-first traversal.
-__device__ __noinline__ bool tie_candidate_wins(const float4* tie, const RayPrep& r, uint32_t leaf_a,
-                                                uint32_t lane_a, uint32_t leaf_b, uint32_t lane_b) {
+// Takes the ray by value (origin, reciprocal direction, parallel mask) so the
+// caller's ray state can stay in registers across this rarely taken call.
+__device__ __forceinline__ bool tie_candidate_wins_v(const float4* tie, float ox, float oy, float oz, float ix, float iy,
+                                                  float iz, uint32_t par, uint32_t leaf_a, uint32_t lane_a,
+                                                  uint32_t leaf_b, uint32_t lane_b) {
   if (leaf_a == leaf_b) return lane_b < lane_a;
+  RayPrep r;
+  r.ox = ox; r.oy = oy; r.oz = oz;
+  r.ix = ix; r.iy = iy; r.iz = iz;
+  r.par = par;
   int32_t a = static_cast<int32_t>(leaf_a), b = static_cast<int32_t>(leaf_b);
   int32_t da = tie_depth(tie, a), db = tie_depth(tie, b);
   while (da > db && a > 0) { a = tie_parent(tie, a); --da; }
@@ -176,8 +183,13 @@ __device__ __noinline__ bool tie_candidate_wins(const float4* tie, const RayPrep
   return !a_first;
 }
 
+__device__ __forceinline__ bool tie_candidate_wins(const float4* tie, const RayPrep& r, uint32_t leaf_a,
+                                                   uint32_t lane_a, uint32_t leaf_b, uint32_t lane_b) {
+  return tie_candidate_wins_v(tie, r.ox, r.oy, r.oz, r.ix, r.iy, r.iz, r.par, leaf_a, lane_a, leaf_b, lane_b);
+}
+
 struct TraceStats {
-  uint32_t nodes = 0, leaves = 0, tris = 0;
+  uint32_t nodes = 0, leaves = 0, tris = 0, rays = 0;
 };
 
 // Shared-memory stack, interleaved so consecutive threads hit distinct banks.
@@ -343,6 +355,184 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, f
     ref = stk.base[sp * stk.stride].x;
   }
   return false;
+}
+
+
+// ================================================================ persistent
+// Lane-level traversal state machine for the persistent kernels: one call of
+// lane_step() processes one wide node or one leaf, so a warp can re-converge
+// every few steps and hand finished lanes new rays (dynamic ray fetch).
+
+// Stack of (ref, entry distance): the first `scap` entries in shared memory
+// (interleaved per thread), the rest in a per-thread slab in global memory.
+struct TwoLevelStack {
+  int2* smem;     // this thread's entry 0; entry i at smem[i * sstride]
+  int sstride;
+  int scap;
+  int2* spill;    // this thread's spill entry 0; entry i at spill[i * gstride]
+  int gstride;
+  int total;      // scap + spill entries
+  __device__ __forceinline__ void put(int i, int2 e) const {
+    if (i < scap) smem[i * sstride] = e;
+    else spill[(i - scap) * gstride] = e;
+  }
+  __device__ __forceinline__ int2 get(int i) const {
+    return i < scap ? smem[i * sstride] : spill[(i - scap) * gstride];
+  }
+};
+
+struct LaneState {
+  RayPrep r;
+  float t;          // closest: best distance so far; any: the query's upper bound
+  uint32_t prim;    // closest: primitive; any: 1 when occluded
+  uint32_t leaf, lane;
+  int32_t ref;
+  int sp;
+};
+
+__device__ __forceinline__ void lane_begin(LaneState& L, V3 o, V3 d, float tmax, bool any) {
+  L.r = prep_ray(o, d);
+  L.t = any ? tmax : kInf;
+  L.prim = any ? 0u : kMiss;
+  L.leaf = L.lane = 0u;
+  L.ref = 0;
+  L.sp = 0;
+}
+
+// Returns true when the query has finished.
+template <bool kAny, bool kStats>
+__device__ __forceinline__ bool lane_step(const DevScene& s, LaneState& L, const TwoLevelStack& stk,
+                                          TraceStats& st, uint32_t& err) {
+  if (L.ref >= 0) {
+    const float4* np = s.nodes + 8 * L.ref;
+    const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+    const int n = __ldg(reinterpret_cast<const int*>(np + 7));
+    if (kStats) ++st.nodes;
+    float t[4];
+    int32_t c[4] = {ch.x, ch.y, ch.z, ch.w};
+    const bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, L.r, L.t, t[0]);
+    const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, L.r, L.t, t[1]) && n > 1;
+    const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, L.r, L.t, t[2]) && n > 2;
+    const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, L.r, L.t, t[3]) && n > 3;
+    t[0] = h0 ? t[0] : kInf;
+    t[1] = h1 ? t[1] : kInf;
+    t[2] = h2 ? t[2] : kInf;
+    t[3] = h3 ? t[3] : kInf;
+    const int hits = int(h0) + int(h1) + int(h2) + int(h3);
+#define VKPTC_CSWAP(i, j)                            \
+  if (t[j] < t[i]) {                                 \
+    const float tt = t[i]; t[i] = t[j]; t[j] = tt;   \
+    const int32_t cc = c[i]; c[i] = c[j]; c[j] = cc; \
+  }
+    VKPTC_CSWAP(0, 1) VKPTC_CSWAP(2, 3) VKPTC_CSWAP(0, 2) VKPTC_CSWAP(1, 3) VKPTC_CSWAP(1, 2)
+#undef VKPTC_CSWAP
+    if (hits > 0) {
+#pragma unroll
+      for (int k = 3; k >= 1; --k) {
+        if (k < hits) {
+          if (L.sp < stk.total) {
+            stk.put(L.sp, make_int2(c[k], __float_as_int(t[k])));
+            ++L.sp;
+          } else {
+            err = 1u;
+          }
+        }
+      }
+      L.ref = c[0];
+      return false;
+    }
+  } else {
+    const int32_t first = leaf_first(L.ref);
+    const int32_t count = leaf_count(L.ref);
+    if (kStats) {
+      ++st.leaves;
+      st.tris += static_cast<uint32_t>(count);
+    }
+    for (int32_t i = 0; i < count; ++i) {
+      const float4* tp = s.tris + 3 * (first + i);
+      const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+      const float th = mt_test(a, b, cc, L.r);
+      if (th <= kEps) continue;
+      if (kAny) {
+        if (th < L.t) {
+          L.prim = 1u;
+          return true;
+        }
+      } else if (th < L.t) {
+        L.t = th;
+        L.prim = __float_as_uint(cc.y);
+        L.leaf = __float_as_uint(cc.z);
+        L.lane = __float_as_uint(cc.w);
+      } else if (th == L.t &&
+                 tie_candidate_wins(s.tie, L.r, L.leaf, L.lane, __float_as_uint(cc.z), __float_as_uint(cc.w))) {
+        L.prim = __float_as_uint(cc.y);
+        L.leaf = __float_as_uint(cc.z);
+        L.lane = __float_as_uint(cc.w);
+      }
+    }
+  }
+  while (L.sp > 0) {
+    --L.sp;
+    const int2 e = stk.get(L.sp);
+    if (kAny || __int_as_float(e.y) <= L.t) {
+      L.ref = e.x;
+      return false;
+    }
+  }
+  return true;
+}
+
+// Persistent traversal over `n` queries supplied by Src:
+//   Src::load(j, o, d, tmax) and Src::finish(j, t, prim) (any-hit: prim = occluded).
+// Each warp keeps its lanes busy: whenever lanes are idle it claims that many
+// query ids with one atomic (warp-aggregated) and refills them; lanes run up
+// to `steps` node/leaf steps between refills.
+template <class Src, bool kAny, bool kStats>
+__device__ __forceinline__ void persistent_traverse(const DevScene& s, const Src& src, uint32_t n, uint32_t* fetch,
+                                                    TwoLevelStack stk, int steps, TraceStats& st, uint32_t& err) {
+  const unsigned lane_id = threadIdx.x & 31u;
+  LaneState L;
+  bool active = false;
+  bool exhausted = false;
+  uint32_t tag = 0u;
+  while (true) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (idle != 0u && !exhausted) {
+      uint32_t base = 0u;
+      if (lane_id == 0u) base = atomicAdd(fetch, static_cast<uint32_t>(__popc(idle)));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) exhausted = true;
+      if (!active) {
+        const uint32_t j = base + static_cast<uint32_t>(__popc(idle & ((1u << lane_id) - 1u)));
+        if (j < n && j >= base) {
+          V3 o, d;
+          float tmax;
+          src.load(j, o, d, tmax);
+          lane_begin(L, o, d, tmax, kAny);
+          if (s.prim_count == 0u || (kAny && !(tmax > kEps))) {
+            src.finish(j, L.t, L.prim);
+            if (kStats) ++st.rays;
+          } else {
+            tag = j;
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active) {
+      for (int k = 0; k < steps; ++k) {
+        if (lane_step<kAny, kStats>(s, L, stk, st, err)) {
+          src.finish(tag, L.t, L.prim);
+          if (kStats) ++st.rays;
+          active = false;
+          break;
+        }
+      }
+    }
+  }
 }
 
 }  // namespace vkptc

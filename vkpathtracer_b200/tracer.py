@@ -70,7 +70,8 @@ class CudaPathTracer:
     backend_name = "cuda-wavefront"
 
     def __init__(self, device: int = 0, block_size: int = 0, stack_depth: int = 0, math_mode: int = 0,
-                 collect_stats: bool = False, wave_paths: int = 0, stage_timing: bool = False):
+                 collect_stats: bool = False, wave_paths: int = 0, stage_timing: bool = False,
+                 steps: int = 0):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -80,6 +81,7 @@ class CudaPathTracer:
         cfg.collect_stats = int(collect_stats)
         cfg.reserved[0] = wave_paths
         cfg.reserved[1] = int(stage_timing)
+        cfg.reserved[2] = steps
         handle = ctypes.c_void_p()
         rc = self._lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle))
         if rc != native.OK:
