@@ -250,6 +250,56 @@ int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, u
 int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float* d_tmax, uint64_t ray_count,
                                 uint32_t mode, uint32_t* d_prim_out, float* d_t_out, void* stream);
 
+/* ---- batched rendering ------------------------------------------------------
+ * No single reference counterpart: the reference renders jobs one
+ * IPathTracer at a time (ptbench `run` per scene).  A batch holds many render
+ * jobs (each its own scene, acceleration structure, settings and film) and
+ * renders all of them, either one frame per launch per job ("plain") or in
+ * one persistent launch fed by a device work queue and replayed from a CUDA
+ * graph ("persistent").  Both give bit-identical films. */
+typedef struct vkptc_batch vkptc_batch;
+
+#define VKPTC_BATCH_PLAIN 0u
+#define VKPTC_BATCH_PERSISTENT 1u
+
+typedef struct vkptc_batch_tuning {
+  uint32_t pool_paths;       /* path slots of the persistent launch ("queue capacity"); 0 = default */
+  uint32_t block_size;       /* 0 = default */
+  uint32_t stack_depth;      /* traversal stack entries in shared memory; 0 = default */
+  uint32_t steps;            /* traversal steps between warp refills; 0 = default */
+  uint32_t sample_limit;     /* render at most this many samples per job (0 = each job's spp) */
+  uint32_t use_graph;        /* persistent mode: 1 = capture once, replay the CUDA graph */
+  uint32_t reserved[2];
+} vkptc_batch_tuning;
+
+typedef struct vkptc_batch_stats {
+  uint32_t jobs;
+  uint32_t graph_used;
+  uint64_t paths;            /* camera paths rendered by the last run */
+  uint64_t segments;         /* extension segments (finite samples) */
+  uint64_t shadow_rays;
+  uint64_t kernel_launches;  /* kernels launched by the last run */
+  double device_ms;          /* device time of the last run (CUDA events on the batch stream) */
+  uint32_t grid;
+  uint32_t block;
+  uint32_t pool_paths;
+  uint32_t stack_depth;
+  uint32_t steps;
+  uint32_t reserved;
+} vkptc_batch_stats;
+
+int32_t vkptc_batch_create(const vkptc_config* config, vkptc_batch** out_batch);
+int32_t vkptc_batch_destroy(vkptc_batch* batch);
+/* Adds one job: loads the scene and builds its acceleration structure (as
+ * configure + load_scene_snapshot + build_or_update_acceleration would). */
+int32_t vkptc_batch_add_job(vkptc_batch* batch, const vkptc_scene_view* scene, const vkptc_render_settings* settings,
+                            uint32_t* job_id);
+/* Clears every film, then renders samples [0, spp) (or sample_limit) of every job. */
+int32_t vkptc_batch_run(vkptc_batch* batch, uint32_t mode, const vkptc_batch_tuning* tuning);
+int32_t vkptc_batch_read_film(vkptc_batch* batch, uint32_t job_id, float* sum_rgb, uint32_t* count);
+int32_t vkptc_batch_get_stats(vkptc_batch* batch, vkptc_batch_stats* out);
+const char* vkptc_batch_last_error(vkptc_batch* batch);
+
 /* ---- allocation-free rendering -------------------------------------------
  * No counterpart in the reference: an extra entry point of this library.
  *

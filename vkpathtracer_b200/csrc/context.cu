@@ -19,6 +19,7 @@
 
 #include "../../include/vkptc.h"
 #include "bvh_host.h"
+#include "batch.cuh"
 #include "kernels.cuh"
 
 using namespace vkptc;
@@ -820,6 +821,395 @@ int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, u
   rc = check_device_error(ctx);
   if (rc == VKPTC_OK) ctx->last_error.clear();
   return rc;
+}
+
+}  // extern "C"
+
+// ================================================================== batches
+struct vkptc_batch {
+  vkptc_config config{};
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string last_error;
+  std::vector<vkptc_ctx*> jobs;
+  // persistent-mode device state
+  DevBuf<DevJob> d_jobs;
+  DevBuf<float4> staging;
+  DevBuf<uint32_t> p_job, p_local, p_depth, p_q0, p_q1, p_shq, p_fin, p_free, p_ctl;
+  DevBuf<uint64_t> p_rng;
+  DevBuf<float4> p_o, p_d, p_thr, p_rad, p_sh_o, p_sh_d, p_sh_c;
+  DevBuf<float2> p_hit;
+  DevBuf<int2> spill;
+  DevBuf<DevCounters> d_ctr;
+  DevBuf<uint32_t> d_err;
+  size_t smem_configured = 48 * 1024;
+  cudaGraphExec_t graph = nullptr;
+  std::string graph_key;
+  vkptc_batch_stats stats{};
+};
+
+namespace {
+
+int32_t bfail(vkptc_batch* b, int32_t code, const std::string& msg) {
+  if (b) b->last_error = msg;
+  return code;
+}
+
+int32_t bcuda(vkptc_batch* b, cudaError_t e, const char* what) {
+  const int32_t code = (e == cudaErrorMemoryAllocation) ? VKPTC_ALLOC_FAILED : VKPTC_INTERNAL_ERROR;
+  return bfail(b, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define VKPTC_BCUDA(b, call, what)                          \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return bcuda(b, e_, what);       \
+  } while (0)
+
+constexpr uint32_t kDefaultPoolPaths = 1u << 21;
+
+uint32_t job_samples(const vkptc_ctx* c, uint32_t limit) {
+  const uint32_t spp = std::max(1u, c->settings.spp);
+  return limit ? std::min(spp, limit) : spp;
+}
+
+void release_graph(vkptc_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_key.clear();
+}
+
+int32_t batch_clear_films(vkptc_batch* b) {
+  for (vkptc_ctx* c : b->jobs) {
+    VKPTC_BCUDA(b, cudaMemsetAsync(c->d_film_sum.ptr, 0, c->d_film_sum.bytes(), b->stream), "film clear");
+    VKPTC_BCUDA(b, cudaMemsetAsync(c->d_film_count.ptr, 0, c->d_film_count.bytes(), b->stream), "film clear");
+  }
+  return VKPTC_OK;
+}
+
+int32_t batch_run_plain(vkptc_batch* b, const vkptc_batch_tuning& t) {
+  uint64_t launches = 0;
+  for (vkptc_ctx* c : b->jobs) {
+    VKPTC_BCUDA(b, cudaMemsetAsync(c->d_ctr.ptr, 0, sizeof(DevCounters), b->stream), "counter clear");
+  }
+  VKPTC_BCUDA(b, cudaEventRecord(b->ev0, b->stream), "event");
+  int32_t rc = batch_clear_films(b);
+  if (rc != VKPTC_OK) return rc;
+  for (vkptc_ctx* c : b->jobs) {
+    cudaStream_t saved = c->stream;
+    const vkptc_config saved_cfg = c->config;
+    c->stream = b->stream;
+    if (t.block_size) c->config.block_size = t.block_size;
+    if (t.stack_depth) c->config.stack_depth = t.stack_depth;
+    if (t.steps) c->config.reserved[2] = t.steps;
+    const uint32_t spp = job_samples(c, t.sample_limit);
+    for (uint32_t sidx = 0; sidx < spp && rc == VKPTC_OK; ++sidx) {
+      // One frame per launch sequence: every sample is its own wave.
+      WaveTile wt{0u, 0u, c->settings.width, c->settings.height, sidx, 1u};
+      rc = run_wave(c, wt, 0u);
+      launches += 2u + (c->settings.enable_nee ? 3u : 2u) * c->settings.max_depth;
+    }
+    c->stream = saved;
+    c->config = saved_cfg;
+    if (rc != VKPTC_OK) return bfail(b, rc, std::string("plain batch run: ") + c->last_error);
+  }
+  VKPTC_BCUDA(b, cudaEventRecord(b->ev1, b->stream), "event");
+  VKPTC_BCUDA(b, cudaStreamSynchronize(b->stream), "batch sync");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  uint64_t segs = 0, shadow = 0;
+  for (vkptc_ctx* c : b->jobs) {
+    DevCounters dc{};
+    VKPTC_BCUDA(b, cudaMemcpy(&dc, c->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost), "counters");
+    segs += dc.rays;
+    shadow += dc.shadow_tests;
+    uint32_t err = 0;
+    VKPTC_BCUDA(b, cudaMemcpy(&err, c->d_err.ptr, sizeof(err), cudaMemcpyDeviceToHost), "error word");
+    if (err) return bfail(b, VKPTC_INTERNAL_ERROR, "device traversal stack overflow");
+  }
+  b->stats.segments = segs;
+  b->stats.shadow_rays = shadow;
+  b->stats.device_ms = ms;
+  b->stats.kernel_launches = launches;
+  b->stats.graph_used = 0;
+  return VKPTC_OK;
+}
+
+int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
+  const bool parity = b->config.math_mode == 0u;
+  // ---- jobs table and stagings
+  std::vector<DevJob> table(b->jobs.size());
+  unsigned long long total = 0, staging_px = 0;
+  int stack_cap = 1;
+  for (size_t k = 0; k < b->jobs.size(); ++k) {
+    vkptc_ctx* c = b->jobs[k];
+    DevJob& J = table[k];
+    J.scene = dev_scene(c);
+    J.settings = dev_settings(c, 0u);
+    J.path_base = total;
+    J.pixels = c->settings.width * c->settings.height;
+    J.spp = job_samples(c, t.sample_limit);
+    J.first_sample = 0u;
+    J.film = film_of(c);
+    total += static_cast<unsigned long long>(J.pixels) * J.spp;
+    staging_px += static_cast<unsigned long long>(J.pixels) * J.spp;
+    stack_cap = std::max(stack_cap, static_cast<int>(std::max<uint32_t>(1u, c->wide.stack_required)));
+  }
+  VKPTC_BCUDA(b, b->staging.alloc(std::max<unsigned long long>(1, staging_px)), "staging alloc");
+  unsigned long long off = 0;
+  for (DevJob& J : table) {
+    J.staging = b->staging.ptr + off;
+    off += static_cast<unsigned long long>(J.pixels) * J.spp;
+  }
+  VKPTC_BCUDA(b, b->d_jobs.alloc(table.size()), "job table alloc");
+  VKPTC_BCUDA(b, cudaMemcpy(b->d_jobs.ptr, table.data(), table.size() * sizeof(DevJob), cudaMemcpyHostToDevice),
+              "job table upload");
+  // ---- launch shape
+  BatchLaunch bl{};
+  bl.block = t.block_size ? static_cast<int>(std::min(256u, std::max(32u, (t.block_size + 31u) / 32u * 32u))) : 128;
+  bl.stack_cap = stack_cap;
+  bl.smem_entries = std::min(stack_cap, t.stack_depth ? static_cast<int>(t.stack_depth) : kDefaultSmemEntries);
+  bl.steps = t.steps ? static_cast<int>(t.steps) : kDefaultSteps;
+  bl.stream = b->stream;
+  bl.parity = parity;
+  const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
+  int max_optin = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
+  if (smem > static_cast<size_t>(max_optin)) return bfail(b, VKPTC_UNSUPPORTED, "stack does not fit in shared memory");
+  if (smem > b->smem_configured) {
+    VKPTC_BCUDA(b, ConfigureBatchSmem(smem), "shared memory limit");
+    b->smem_configured = smem;
+  }
+  const int per_sm = BatchBlocksPerSm(bl.block, smem, parity);
+  if (per_sm <= 0) return bfail(b, VKPTC_UNSUPPORTED, "persistent batch kernel does not fit on an SM with this block size");
+  bl.grid = per_sm * b->sm_count;
+  const size_t spill_entries =
+      bl.stack_cap > bl.smem_entries ? static_cast<size_t>(bl.grid) * bl.block * (bl.stack_cap - bl.smem_entries) : 0;
+  if (spill_entries) VKPTC_BCUDA(b, b->spill.alloc(spill_entries), "spill alloc");
+  bl.spill = spill_entries ? b->spill.ptr : nullptr;
+  // ---- pool
+  const uint32_t cap = std::max<uint32_t>(1024u, t.pool_paths ? t.pool_paths : kDefaultPoolPaths);
+  const size_t n = cap;
+  VKPTC_BCUDA(b, b->p_job.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_local.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_depth.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_q0.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_q1.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_shq.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_fin.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_free.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_ctl.alloc(kBatchCtlWords), "pool alloc");
+  VKPTC_BCUDA(b, b->p_rng.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_o.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_d.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_thr.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_rad.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_sh_o.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_sh_d.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_sh_c.alloc(n), "pool alloc");
+  VKPTC_BCUDA(b, b->p_hit.alloc(n), "pool alloc");
+  BatchPool P{};
+  P.capacity = cap;
+  P.job = b->p_job.ptr;
+  P.local = b->p_local.ptr;
+  P.depth = b->p_depth.ptr;
+  P.rng = b->p_rng.ptr;
+  P.ray_o = b->p_o.ptr;
+  P.ray_d = b->p_d.ptr;
+  P.thr = b->p_thr.ptr;
+  P.rad = b->p_rad.ptr;
+  P.hit = b->p_hit.ptr;
+  P.ext[0] = b->p_q0.ptr;
+  P.ext[1] = b->p_q1.ptr;
+  P.shq = b->p_shq.ptr;
+  P.sh_o = b->p_sh_o.ptr;
+  P.sh_d = b->p_sh_d.ptr;
+  P.sh_c = b->p_sh_c.ptr;
+  P.fin = b->p_fin.ptr;
+  P.freel = b->p_free.ptr;
+  P.ctl = b->p_ctl.ptr;
+
+  // ---- the run: film clear, pool reset, one persistent launch, in-order accumulation
+  auto enqueue = [&]() -> int32_t {
+    int32_t rc = batch_clear_films(b);
+    if (rc != VKPTC_OK) return rc;
+    VKPTC_BCUDA(b, cudaMemsetAsync(b->d_ctr.ptr, 0, sizeof(DevCounters), b->stream), "counter clear");
+    VKPTC_BCUDA(b, LaunchBatchInit(P, b->stream), "pool init");
+    VKPTC_BCUDA(b, LaunchBatchPersistent(b->d_jobs.ptr, static_cast<uint32_t>(table.size()), total, P, bl,
+                                          b->d_ctr.ptr, b->d_err.ptr),
+                "persistent launch");
+    VKPTC_BCUDA(b, LaunchStagingAccumulate(b->d_jobs.ptr, static_cast<uint32_t>(table.size()), staging_px,
+                                            b->stream, b->d_ctr.ptr),
+                "staging accumulate");
+    return VKPTC_OK;
+  };
+  VKPTC_BCUDA(b, cudaMemsetAsync(b->d_err.ptr, 0, sizeof(uint32_t), b->stream), "error clear");
+  bool graph_used = false;
+  if (t.use_graph) {
+    const std::string key = std::to_string(cap) + "/" + std::to_string(bl.block) + "/" + std::to_string(bl.smem_entries) +
+                            "/" + std::to_string(bl.steps) + "/" + std::to_string(t.sample_limit) + "/" +
+                            std::to_string(b->jobs.size()) + "/" +
+                            std::to_string(reinterpret_cast<uintptr_t>(b->staging.ptr)) + "/" +
+                            std::to_string(reinterpret_cast<uintptr_t>(b->p_job.ptr));
+    if (!b->graph || b->graph_key != key) {
+      release_graph(b);
+      VKPTC_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+      const int32_t rc = enqueue();
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+      if (rc != VKPTC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ec != cudaSuccess) return bcuda(b, ec, "graph capture");
+      const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) {
+        b->graph = nullptr;
+        return bcuda(b, ei, "graph instantiate");
+      }
+      b->graph_key = key;
+    }
+    VKPTC_BCUDA(b, cudaEventRecord(b->ev0, b->stream), "event");
+    VKPTC_BCUDA(b, cudaGraphLaunch(b->graph, b->stream), "graph launch");
+    VKPTC_BCUDA(b, cudaEventRecord(b->ev1, b->stream), "event");
+    graph_used = true;
+  } else {
+    VKPTC_BCUDA(b, cudaEventRecord(b->ev0, b->stream), "event");
+    const int32_t rc = enqueue();
+    if (rc != VKPTC_OK) return rc;
+    VKPTC_BCUDA(b, cudaEventRecord(b->ev1, b->stream), "event");
+  }
+  VKPTC_BCUDA(b, cudaStreamSynchronize(b->stream), "batch sync");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  uint32_t err = 0;
+  VKPTC_BCUDA(b, cudaMemcpy(&err, b->d_err.ptr, sizeof(err), cudaMemcpyDeviceToHost), "error word");
+  if (err & 2u) return bfail(b, VKPTC_TIMEOUT, "persistent batch: a grid barrier wait exceeded its bound");
+  if (err) return bfail(b, VKPTC_INTERNAL_ERROR, "device traversal stack overflow");
+  DevCounters dc{};
+  VKPTC_BCUDA(b, cudaMemcpy(&dc, b->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost), "counters");
+  b->stats.segments = dc.rays;
+  b->stats.shadow_rays = dc.shadow_tests;
+  b->stats.device_ms = ms;
+  b->stats.kernel_launches = 2u + static_cast<uint64_t>(table.size());   // init, persistent, accumulate per job
+  b->stats.graph_used = graph_used ? 1u : 0u;
+  b->stats.grid = static_cast<uint32_t>(bl.grid);
+  b->stats.block = static_cast<uint32_t>(bl.block);
+  b->stats.pool_paths = cap;
+  b->stats.stack_depth = static_cast<uint32_t>(bl.smem_entries);
+  b->stats.steps = static_cast<uint32_t>(bl.steps);
+  return VKPTC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vkptc_batch_create(const vkptc_config* config, vkptc_batch** out_batch) {
+  if (!out_batch) return VKPTC_INVALID_ARGUMENT;
+  *out_batch = nullptr;
+  auto* b = new (std::nothrow) vkptc_batch();
+  if (!b) return VKPTC_ALLOC_FAILED;
+  if (config) b->config = *config;
+  b->device = b->config.device;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    delete b;
+    return VKPTC_UNSUPPORTED;
+  }
+  if (b->device < 0 || b->device >= count) {
+    delete b;
+    return VKPTC_INVALID_ARGUMENT;
+  }
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+      b->d_ctr.alloc(1) != cudaSuccess || b->d_err.alloc(1) != cudaSuccess) {
+    delete b;
+    return VKPTC_INTERNAL_ERROR;
+  }
+  cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device);
+  *out_batch = b;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_batch_destroy(vkptc_batch* b) {
+  if (!b) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  release_graph(b);
+  for (vkptc_ctx* c : b->jobs) vkptc_destroy(c);
+  b->jobs.clear();
+  cudaStream_t st = b->stream;
+  cudaEvent_t e0 = b->ev0, e1 = b->ev1;
+  delete b;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  return VKPTC_OK;
+}
+
+int32_t vkptc_batch_add_job(vkptc_batch* b, const vkptc_scene_view* scene, const vkptc_render_settings* settings,
+                            uint32_t* job_id) {
+  if (!b) return VKPTC_INVALID_ARGUMENT;
+  if (!scene || !settings) return bfail(b, VKPTC_INVALID_ARGUMENT, "scene or settings is null");
+  cudaSetDevice(b->device);
+  vkptc_ctx* c = nullptr;
+  int32_t rc = vkptc_create(&b->config, &c);
+  if (rc != VKPTC_OK) return bfail(b, rc, "job context creation failed");
+  if ((rc = vkptc_configure(c, settings)) != VKPTC_OK || (rc = vkptc_load_scene(c, scene)) != VKPTC_OK ||
+      (rc = vkptc_build_acceleration(c)) != VKPTC_OK) {
+    b->last_error = std::string("job set-up failed: ") + c->last_error;
+    vkptc_destroy(c);
+    return rc;
+  }
+  if (c->has_transmissive) {
+    vkptc_destroy(c);
+    return bfail(b, VKPTC_UNSUPPORTED, "batched jobs with transmissive materials are not supported");
+  }
+  b->jobs.push_back(c);
+  release_graph(b);
+  if (job_id) *job_id = static_cast<uint32_t>(b->jobs.size() - 1);
+  b->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_batch_run(vkptc_batch* b, uint32_t mode, const vkptc_batch_tuning* tuning) {
+  if (!b) return VKPTC_INVALID_ARGUMENT;
+  if (b->jobs.empty()) return bfail(b, VKPTC_NOT_READY, "batch has no jobs");
+  if (mode > VKPTC_BATCH_PERSISTENT) return bfail(b, VKPTC_INVALID_ARGUMENT, "unknown batch mode");
+  cudaSetDevice(b->device);
+  vkptc_batch_tuning t{};
+  if (tuning) t = *tuning;
+  b->stats = vkptc_batch_stats{};
+  b->stats.jobs = static_cast<uint32_t>(b->jobs.size());
+  for (vkptc_ctx* c : b->jobs) {
+    b->stats.paths += static_cast<uint64_t>(c->settings.width) * c->settings.height * job_samples(c, t.sample_limit);
+  }
+  const int32_t rc = mode == VKPTC_BATCH_PLAIN ? batch_run_plain(b, t) : batch_run_persistent(b, t);
+  if (rc == VKPTC_OK) b->last_error.clear();
+  return rc;
+}
+
+int32_t vkptc_batch_read_film(vkptc_batch* b, uint32_t job_id, float* sum_rgb, uint32_t* count) {
+  if (!b) return VKPTC_INVALID_ARGUMENT;
+  if (job_id >= b->jobs.size()) return bfail(b, VKPTC_INVALID_ARGUMENT, "job id out of range");
+  const int32_t rc = vkptc_read_film(b->jobs[job_id], sum_rgb, count, nullptr);
+  if (rc != VKPTC_OK) b->last_error = b->jobs[job_id]->last_error;
+  return rc;
+}
+
+int32_t vkptc_batch_get_stats(vkptc_batch* b, vkptc_batch_stats* out) {
+  if (!b || !out) return VKPTC_INVALID_ARGUMENT;
+  *out = b->stats;
+  return VKPTC_OK;
+}
+
+const char* vkptc_batch_last_error(vkptc_batch* b) {
+  if (!b) return "null batch";
+  return b->last_error.c_str();
 }
 
 }  // extern "C"

@@ -381,7 +381,18 @@ struct TwoLevelStack {
   }
 };
 
+// Geometry a lane traverses (one launch may serve several scenes).
+struct GeoView {
+  const float4* nodes;
+  const float4* tris;
+  const float4* tie;
+  uint32_t prim_count;
+};
+
+__host__ __device__ __forceinline__ GeoView geo_of(const DevScene& s) { return GeoView{s.nodes, s.tris, s.tie, s.prim_count}; }
+
 struct LaneState {
+  GeoView g;
   RayPrep r;
   float t;          // closest: best distance so far; any: the query's upper bound
   uint32_t prim;    // closest: primitive; any: 1 when occluded
@@ -401,10 +412,9 @@ __device__ __forceinline__ void lane_begin(LaneState& L, V3 o, V3 d, float tmax,
 
 // Returns true when the query has finished.
 template <bool kAny, bool kStats>
-__device__ __forceinline__ bool lane_step(const DevScene& s, LaneState& L, const TwoLevelStack& stk,
-                                          TraceStats& st, uint32_t& err) {
+__device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk, TraceStats& st, uint32_t& err) {
   if (L.ref >= 0) {
-    const float4* np = s.nodes + 8 * L.ref;
+    const float4* np = L.g.nodes + 8 * L.ref;
     const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
     const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
     const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
@@ -451,7 +461,7 @@ __device__ __forceinline__ bool lane_step(const DevScene& s, LaneState& L, const
       st.tris += static_cast<uint32_t>(count);
     }
     for (int32_t i = 0; i < count; ++i) {
-      const float4* tp = s.tris + 3 * (first + i);
+      const float4* tp = L.g.tris + 3 * (first + i);
       const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
       const float th = mt_test(a, b, cc, L.r);
       if (th <= kEps) continue;
@@ -466,7 +476,7 @@ __device__ __forceinline__ bool lane_step(const DevScene& s, LaneState& L, const
         L.leaf = __float_as_uint(cc.z);
         L.lane = __float_as_uint(cc.w);
       } else if (th == L.t &&
-                 tie_candidate_wins(s.tie, L.r, L.leaf, L.lane, __float_as_uint(cc.z), __float_as_uint(cc.w))) {
+                 tie_candidate_wins(L.g.tie, L.r, L.leaf, L.lane, __float_as_uint(cc.z), __float_as_uint(cc.w))) {
         L.prim = __float_as_uint(cc.y);
         L.leaf = __float_as_uint(cc.z);
         L.lane = __float_as_uint(cc.w);
@@ -490,7 +500,7 @@ __device__ __forceinline__ bool lane_step(const DevScene& s, LaneState& L, const
 // query ids with one atomic (warp-aggregated) and refills them; lanes run up
 // to `steps` node/leaf steps between refills.
 template <class Src, bool kAny, bool kStats>
-__device__ __forceinline__ void persistent_traverse(const DevScene& s, const Src& src, uint32_t n, uint32_t* fetch,
+__device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, uint32_t* fetch,
                                                     TwoLevelStack stk, int steps, TraceStats& st, uint32_t& err) {
   const unsigned lane_id = threadIdx.x & 31u;
   LaneState L;
@@ -509,9 +519,9 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& s, const Src
         if (j < n && j >= base) {
           V3 o, d;
           float tmax;
-          src.load(j, o, d, tmax);
+          src.load(j, o, d, tmax, L.g);
           lane_begin(L, o, d, tmax, kAny);
-          if (s.prim_count == 0u || (kAny && !(tmax > kEps))) {
+          if (L.g.prim_count == 0u || (kAny && !(tmax > kEps))) {
             src.finish(j, L.t, L.prim);
             if (kStats) ++st.rays;
           } else {
@@ -524,7 +534,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& s, const Src
     if (!__any_sync(0xffffffffu, active)) break;
     if (active) {
       for (int k = 0; k < steps; ++k) {
-        if (lane_step<kAny, kStats>(s, L, stk, st, err)) {
+        if (lane_step<kAny, kStats>(L, stk, st, err)) {
           src.finish(tag, L.t, L.prim);
           if (kStats) ++st.rays;
           active = false;

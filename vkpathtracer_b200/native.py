@@ -84,6 +84,23 @@ class AccelInfo(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("pool_paths", ctypes.c_uint32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
+                ("steps", ctypes.c_uint32), ("sample_limit", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 2)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("jobs", ctypes.c_uint32), ("graph_used", ctypes.c_uint32), ("paths", ctypes.c_uint64),
+                ("segments", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64), ("device_ms", ctypes.c_double), ("grid", ctypes.c_uint32),
+                ("block", ctypes.c_uint32), ("pool_paths", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
+                ("steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
 P = ctypes.c_void_p
 U32, U64, I32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
 
@@ -114,7 +131,16 @@ SIGNATURES = {
     "vkptc_trace_rays": (I32, [P, P, P, U64, U32, P, P]),
     "vkptc_trace_rays_device": (I32, [P, P, P, U64, U32, P, P, P]),
     "vkptc_render_tile_noalloc": (I32, [P, ctypes.POINTER(Tile), U32, P, P, P]),
+    "vkptc_batch_create": (I32, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
+    "vkptc_batch_destroy": (I32, [P]),
+    "vkptc_batch_add_job": (I32, [P, ctypes.POINTER(SceneView), ctypes.POINTER(RenderSettingsC),
+                                  ctypes.POINTER(U32)]),
+    "vkptc_batch_run": (I32, [P, U32, ctypes.POINTER(BatchTuning)]),
+    "vkptc_batch_read_film": (I32, [P, U32, P, P]),
+    "vkptc_batch_get_stats": (I32, [P, ctypes.POINTER(BatchStats)]),
+    "vkptc_batch_last_error": (ctypes.c_char_p, [P]),
 }
+BATCH_PLAIN, BATCH_PERSISTENT = 0, 1
 NOALLOC_MAX_PATHS = 65536
 
 _LIB = None

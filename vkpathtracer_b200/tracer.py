@@ -64,6 +64,43 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
+def settings_c(settings: RenderSettings) -> "native.RenderSettingsC":
+    s = native.RenderSettingsC()
+    s.width, s.height, s.spp, s.max_depth = settings.width, settings.height, settings.spp, settings.max_depth
+    s.seed = settings.seed
+    s.enable_nee, s.enable_mis = int(settings.enable_nee), int(settings.enable_mis)
+    s.deterministic = int(settings.deterministic)
+    s.rr_start_depth = settings.russian_roulette_start_depth
+    s.rr_min_survival = settings.russian_roulette_min_survival
+    s.rr_max_survival = settings.russian_roulette_max_survival
+    s.camera_aperture_radius = settings.camera_aperture_radius
+    s.camera_focus_distance = settings.camera_focus_distance
+    s.firefly_clamp = settings.firefly_clamp
+    return s
+
+
+def scene_view(scene: Scene):
+    """POD view of a Scene; returns (view, arrays to keep alive during the call)."""
+    v = native.SceneView()
+    keep = (np.ascontiguousarray(scene.vertices, np.float32), np.ascontiguousarray(scene.indices, np.uint32),
+            np.ascontiguousarray(scene.instances, np.uint32), np.ascontiguousarray(scene.materials, np.float32),
+            np.ascontiguousarray(scene.lights, np.float32))
+    v.vertices, v.vertex_count = _ptr(keep[0]), keep[0].shape[0]
+    v.indices, v.index_count = _ptr(keep[1]), keep[1].size
+    v.instances, v.instance_count = _ptr(keep[2]), keep[2].shape[0]
+    v.materials, v.material_count = _ptr(keep[3]), keep[3].shape[0]
+    v.lights, v.light_count = (_ptr(keep[4]) if keep[4].size else None), keep[4].shape[0]
+    v.environment[:] = scene.environment
+    c = scene.camera
+    v.camera_position[:] = c.position
+    v.camera_target[:] = c.target
+    v.camera_up[:] = c.up
+    v.camera_fov_deg = c.fov_deg
+    v.camera_aperture_radius = c.aperture_radius
+    v.camera_focus_distance = c.focus_distance
+    return v, keep
+
+
 class CudaPathTracer:
     """One GPU render context.  Not re-entrant: drive it from one thread."""
 
@@ -120,40 +157,14 @@ class CudaPathTracer:
 
     # ------------------------------------------------------------ lifecycle
     def configure(self, settings: RenderSettings) -> Status:
-        s = native.RenderSettingsC()
-        s.width, s.height, s.spp, s.max_depth = settings.width, settings.height, settings.spp, settings.max_depth
-        s.seed = settings.seed
-        s.enable_nee, s.enable_mis = int(settings.enable_nee), int(settings.enable_mis)
-        s.deterministic = int(settings.deterministic)
-        s.rr_start_depth = settings.russian_roulette_start_depth
-        s.rr_min_survival = settings.russian_roulette_min_survival
-        s.rr_max_survival = settings.russian_roulette_max_survival
-        s.camera_aperture_radius = settings.camera_aperture_radius
-        s.camera_focus_distance = settings.camera_focus_distance
-        s.firefly_clamp = settings.firefly_clamp
+        s = settings_c(settings)
         st = self._status(self._lib.vkptc_configure(self._ctx, ctypes.byref(s)))
         if st.ok:
             self._settings = settings
         return st
 
     def load_scene_snapshot(self, scene: Scene) -> Status:
-        v = native.SceneView()
-        keep = (np.ascontiguousarray(scene.vertices, np.float32), np.ascontiguousarray(scene.indices, np.uint32),
-                np.ascontiguousarray(scene.instances, np.uint32), np.ascontiguousarray(scene.materials, np.float32),
-                np.ascontiguousarray(scene.lights, np.float32))
-        v.vertices, v.vertex_count = _ptr(keep[0]), keep[0].shape[0]
-        v.indices, v.index_count = _ptr(keep[1]), keep[1].size
-        v.instances, v.instance_count = _ptr(keep[2]), keep[2].shape[0]
-        v.materials, v.material_count = _ptr(keep[3]), keep[3].shape[0]
-        v.lights, v.light_count = (_ptr(keep[4]) if keep[4].size else None), keep[4].shape[0]
-        v.environment[:] = scene.environment
-        c = scene.camera
-        v.camera_position[:] = c.position
-        v.camera_target[:] = c.target
-        v.camera_up[:] = c.up
-        v.camera_fov_deg = c.fov_deg
-        v.camera_aperture_radius = c.aperture_radius
-        v.camera_focus_distance = c.focus_distance
+        v, keep = scene_view(scene)
         return self._status(self._lib.vkptc_load_scene(self._ctx, ctypes.byref(v)))
 
     def build_or_update_acceleration(self) -> Status:
@@ -285,3 +296,74 @@ class CudaPathTracer:
         """Device-pointer variant (e.g. torch tensors' data_ptr()); enqueued, not synchronised."""
         self._check(self._lib.vkptc_trace_rays_device(self._ctx, d_rays, d_tmax or None, n, mode, d_prim,
                                                       d_t or None, stream or None))
+
+
+class BatchRenderer:
+    """Many render jobs (scene + settings each) rendered together.
+
+    run("plain") renders every job one frame (sample) per launch sequence;
+    run("persistent") renders all of them in one persistent launch fed by a
+    device work queue, replayed from a CUDA graph.  Films are bit-identical.
+    """
+
+    def __init__(self, device: int = 0, math_mode: int = 0):
+        self._lib = native.load()
+        cfg = native.Config()
+        cfg.device = device
+        cfg.math_mode = math_mode
+        h = ctypes.c_void_p()
+        rc = self._lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != native.OK:
+            raise native.VkptcError(rc, "vkptc_batch_create failed")
+        self._b = h
+        self.settings = []
+
+    def _err(self):
+        return self._lib.vkptc_batch_last_error(self._b).decode()
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.vkptc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_job(self, scene: Scene, settings: RenderSettings) -> int:
+        v, keep = scene_view(scene)
+        s = settings_c(settings)
+        jid = ctypes.c_uint32()
+        rc = self._lib.vkptc_batch_add_job(self._b, ctypes.byref(v), ctypes.byref(s), ctypes.byref(jid))
+        if rc != native.OK:
+            raise native.VkptcError(rc, self._err())
+        self.settings.append(settings)
+        return int(jid.value)
+
+    def run(self, mode: str = "persistent", pool_paths: int = 0, block_size: int = 0, stack_depth: int = 0,
+            steps: int = 0, sample_limit: int = 0, use_graph: bool = True) -> dict:
+        t = native.BatchTuning(pool_paths, block_size, stack_depth, steps, sample_limit, int(use_graph))
+        m = native.BATCH_PERSISTENT if mode == "persistent" else native.BATCH_PLAIN
+        rc = self._lib.vkptc_batch_run(self._b, m, ctypes.byref(t))
+        if rc != native.OK:
+            raise native.VkptcError(rc, self._err())
+        st = native.BatchStats()
+        self._lib.vkptc_batch_get_stats(self._b, ctypes.byref(st))
+        return st.as_dict()
+
+    def film(self, job: int):
+        st = self.settings[job]
+        s = np.zeros((st.height, st.width, 3), np.float32)
+        c = np.zeros((st.height, st.width), np.uint32)
+        rc = self._lib.vkptc_batch_read_film(self._b, job, _ptr(s), _ptr(c))
+        if rc != native.OK:
+            raise native.VkptcError(rc, self._err())
+        return s, c
