@@ -1,17 +1,20 @@
 """Benchmark of the render hot path on B200 (one process per GPU).
 
-Workload (default): the full-frame scene -- a 64x64 grid of displaced
-spheres (2,064,418 triangles with ground and 16 quad lights; 50% Lambert,
-30% glossy, 20% mirror), 1920x1080, max depth 16, NEE+MIS, Russian roulette
-from depth 3, firefly clamp 10, FP32.  One step = one sample of every pixel
-(2,073,600 camera paths), rendered through the wavefront kernels with the
-scene and BVH resident in HBM.  metric = camera paths per second.
+Headline workload -- batched uneven jobs: 64 independent scenes, each a seeded
+displaced-sphere field with a triangle count log-uniform in [1K, 500K], a
+square resolution log-uniform in [128, 1024], spp in {4,8,16,32,64}, depth in
+{4,8,16}, the mixed material set (50% Lambert, 30% glossy, 20% mirror), quad
+lights, firefly clamp 10.  One step = rendering every sample of every job
+(~0.4 G camera paths) in ONE persistent launch fed by a device work queue and
+replayed from a CUDA graph, launch parameters picked by the autotuner.
+metric = camera paths per second.  The same line reports the plain mode (one
+frame per launch per job) on the same jobs, which produces bit-identical films.
 
-The line also carries: e2e (the same metric through the public C-ABI call
-with host buffers, film read back every step), the ray-query workload
-(8,388,608 rays on the 1,046,904-triangle sphere, Mrays/s), the traversal
-roofline of the dominant kernel, nvidia-smi clocks during the timed region,
-and the reference CPU tracer timed on this host (cpu_baseline).
+Also on the line: e2e (batch run through the C ABI + every film read back to
+host, each step), the full-frame scene (64x64 spheres, 2.06M triangles,
+1920x1080, 64 spp, depth 16), the ray-query workload (8,388,608 rays on the
+1,046,904-triangle sphere), the roofline of the persistent kernel, nvidia-smi
+clocks during the timed region, and the reference CPU tracer on this host.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -34,10 +37,9 @@ from vkpathtracer_b200 import scenes  # noqa: E402
 
 METRIC = "paths/s"
 UNIT = "paths/s"
-WORKLOAD = "sphere_grid_64x64_1080p_depth16"
-# Algorithmic bytes of one traversal step: a 128-byte wide node, a 48-byte
-# triangle record; each ray reads its 24-byte ray and writes an 8-byte hit.
-NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32
+WORKLOAD = "batch_64_uneven_jobs"
+NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
+PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
 
 
 def peaks():
@@ -89,6 +91,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
         sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
         mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        pw = [float(s[3]) for s in self.samples if len(s) > 3 and s[3].replace(".", "").isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for s in self.samples:
@@ -96,7 +99,7 @@ class ClockSampler:
                 if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "power_w_max": max(pw) if pw else None, "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
 def dist_init(args):
@@ -107,6 +110,9 @@ def dist_init(args):
         import datetime
         import torch.distributed as dist
         backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
@@ -117,44 +123,44 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(world, value, device=None):
+def reduce_over_ranks(world, value, op, device=None):
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
     t = torch.tensor([value], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
 
-def sum_over_ranks(world, value, device=None):
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+def make_jobs(count: int, seed: int = 5):
+    return scenes.batch_jobs(count=count, seed=seed)
 
 
 # ------------------------------------------------------------------ CPU side
-def cpu_sample_paths(scene, settings, seconds: float, threads: int, kind: str, seed: int = 0):
-    """Times the CPU oracle on a random pixel subset at 1 spp, grown until the
-    render takes about `seconds`.  Returns (paths/s, sample description)."""
+def cpu_sample(jobs, seconds: float, threads: int, kind: str, seed: int = 0, frac: float = 2e-3):
+    """Times the CPU oracle on a random pixel subset of every job at the job's
+    full spp; the subset grows until the render takes about `seconds`.
+    Returns (paths/s, description).  The reference has no firefly clamp, so the
+    reference kind renders the jobs unclamped (same work per path)."""
     import oracle
     o = oracle.load(kind)
-    npx = settings.width * settings.height
     rng = np.random.default_rng(seed)
-    n = 4096
     while True:
-        px = np.sort(rng.choice(npx, size=min(n, npx), replace=False)).astype(np.uint32)
-        r = o.render(scene, settings, first_sample=0, n_samples=1, threads=threads, pixels=px)
-        ms = r["counters"]["render_ms"]
-        if ms >= 1000.0 * seconds * 0.5 or n >= npx:
-            return px.size / (ms / 1e3), {"pixels": int(px.size), "render_ms": ms,
-                                          "segments": r["counters"]["rays"],
-                                          "shadow_rays": r["counters"]["shadow_tests"]}
-        n = int(min(npx, n * max(2.0, 1000.0 * seconds / max(ms, 1.0))))
+        paths, ms = 0, 0.0
+        for j in jobs:
+            st = j.settings
+            if kind == "reference":
+                st = scenes.RenderSettings(**{**st.__dict__, "firefly_clamp": 0.0})
+            npx = st.width * st.height
+            k = max(8, int(npx * frac))
+            px = np.sort(rng.choice(npx, size=min(k, npx), replace=False)).astype(np.uint32)
+            r = o.render(j.scene, st, first_sample=0, n_samples=st.spp, threads=threads, pixels=px)
+            paths += px.size * st.spp
+            ms += r["counters"]["render_ms"]
+        if ms >= 1000.0 * seconds * 0.5 or frac >= 1.0:
+            return paths / (ms / 1e3), {"pixel_fraction": frac, "paths": paths, "render_ms": ms}
+        frac = min(1.0, frac * max(2.0, 1000.0 * seconds / max(ms, 1.0)))
 
 
 def run_reference(args, world, rank):
@@ -163,185 +169,63 @@ def run_reference(args, world, rank):
     import oracle
     kind = "reference" if oracle.have_reference() else "port"
     threads = os.cpu_count() or 1
-    scene = scenes.sphere_grid()
-    settings = scenes.sphere_grid_settings(spp=1)
-    settings.firefly_clamp = 0.0 if kind == "reference" else settings.firefly_clamp
-    # size the per-step sample so the whole run stays within a few minutes
-    per_step_s = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
-    vals = []
-    sample = None
+    jobs = make_jobs(args.jobs)
+    per_step_s = max(1.5, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
+    vals, sample, frac = [], None, 2e-3
     for i in range(args.warmup + args.steps):
-        v, sample = cpu_sample_paths(scene, settings, per_step_s, threads, kind, seed=i)
+        v, sample = cpu_sample(jobs, per_step_s, threads, kind, seed=i, frac=frac)
+        frac = sample["pixel_fraction"]
         if i >= args.warmup:
             vals.append(v)
     value = float(np.mean(vals))
+    total_paths = sum(j.settings.width * j.settings.height * j.settings.spp for j in jobs)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * settings.width * settings.height / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_paths / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "width": 1920, "height": 1080, "spp_per_step": 1, "max_depth": 16,
-                       "triangles": scene.triangle_count, "parallelism": "cpu threads"},
+            "config": {"workload": WORKLOAD, "jobs": len(jobs), "paths": total_paths,
+                       "triangles": sum(j.scene.triangle_count for j in jobs), "parallelism": "cpu threads"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"random {sample['pixels']} of 2,073,600 pixels at 1 spp per step "
-                                       f"(TiledCpuPathTracer-equivalent scalar tracers over a shared accelerator)"},
+                             "sample": f"random {sample['pixel_fraction']:.4f} of every job's pixels at the job's "
+                                       f"spp per step ({sample['paths']} paths), scalar tracers over a shared "
+                                       f"accelerator on {threads} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ GPU side
-def run_ours(args, world, rank, local):
+def full_frame(device):
+    """The full-frame scene: 1920x1080, 64 spp, depth 16 as one persistent job,
+    plus one sample per launch through the wavefront path."""
     import torch
-    from vkpathtracer_b200.tracer import CudaPathTracer, RenderTile
-    torch.cuda.set_device(local)
-    hbm_peak, peak_kind = peaks()
-    scene = scenes.sphere_grid()
-    settings = scenes.sphere_grid_settings(spp=args.warmup + args.steps)
-    W, H = settings.width, settings.height
-    paths_per_step = W * H
-    stream = torch.cuda.Stream()
-    first = rank * (args.warmup + args.steps)   # each rank renders its own samples of the frame
-
-    # ---------------------------------------------------------- device-resident timing
-    t = CudaPathTracer(device=local)
-    assert t.configure(settings) and t.load_scene_snapshot(scene)
-    b0 = time.time()
-    assert t.build_or_update_acceleration()
-    build_ms = 1e3 * (time.time() - b0)
-    accel = t.accel_info()
-    t.set_stream(stream.cuda_stream)
-    assert t.reset_accumulation()
-    with torch.cuda.stream(stream):
-        for i in range(args.warmup):
-            t.render_frame(first + i, 1, sync=False)
-    torch.cuda.synchronize()
-    barrier(world)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            for i in range(args.steps):
-                t.render_frame(first + args.warmup + i, 1, sync=False)
-            e1.record(stream)
-        stream.synchronize()
-    torch.cuda.synchronize()
-    barrier(world)
-    ms = e0.elapsed_time(e1)
-    t.synchronize()
-    counters = t.read_counters()
-    ms_max = max_over_ranks(world, ms, device=torch.device("cuda", local))
-    total_paths = sum_over_ranks(world, paths_per_step * args.steps, device=torch.device("cuda", local))
-    value = total_paths / (ms_max / 1e3)
-    segs = counters["rays"]
-    shadow = counters["shadow_tests"]
-    mrays = (segs + shadow) / (ms / 1e3) / 1e6   # counters cover warm-up + timed steps: rescale
-    mrays *= args.steps / (args.warmup + args.steps)
-    t.close()
-
-    # ---------------------------------------------------------- end to end (host buffers)
-    e2e = None
-    with CudaPathTracer(device=local) as te:
-        assert te.configure(settings) and te.load_scene_snapshot(scene) and te.build_or_update_acceleration()
-        te.reset_accumulation()
-        hdr = np.empty((H, W, 3), np.float32)
-        for i in range(args.warmup):
-            te.render_tile(RenderTile(0, 0, W, H, first + i), 0)
-            hdr[:] = te.resolve_hdr()
-        barrier(world)
-        w0 = time.perf_counter()
-        for i in range(args.steps):
-            assert te.render_tile(RenderTile(0, 0, W, H, first + args.warmup + i), 0)
-            hdr[:] = te.resolve_hdr()
-        w1 = time.perf_counter()
-        e2e_ms = max_over_ranks(world, 1e3 * (w1 - w0), device=torch.device("cuda", local))
-        e2e = {"value": total_paths / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 28,
-               "d2h_bytes_per_step": W * H * 3 * 4,
-               "path": "vkptc_render(full-frame tile) + vkptc_resolve_hdr to host, every step"}
-
-    # ---------------------------------------------------------- roofline of the traversal kernel
-    roof = None
-    if rank == 0 and not args.no_roofline:
-        rsteps = min(args.steps, 4)
-        with CudaPathTracer(device=local, stage_timing=True) as tt:
-            tt.configure(settings)
-            tt.load_scene_snapshot(scene)
-            tt.build_or_update_acceleration()
-            tt.set_stream(stream.cuda_stream)
-            tt.reset_accumulation()
-            tt.render_frame(first, 1)
-            tt.read_stage_times()
-            tt.reset_accumulation()
-            tt.render_frame(first, rsteps)
-            stages = tt.read_stage_times()
-        ext_ms, ext_launches = stages["extend"]
-        ext = extension_stats(scene, settings, first, rsteps, local)
-        alg_bytes = NODE_BYTES * ext["nodes"] + TRI_BYTES * ext["tris"] + RAY_IO_BYTES * ext["rays"]
-        achieved = alg_bytes / (ext_ms / 1e3) / 1e9
-        traffic_path = os.path.join(ROOT, "profiles", "traffic_extend.json")
-        traffic = None
-        if os.path.exists(traffic_path):
-            try:
-                tr = json.load(open(traffic_path))
-                traffic = tr.get("bytes_per_launch_full_scale")
-            except Exception:
-                traffic = None
-        roof = {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": traffic,
-                "alg_bytes_per_launch": alg_bytes / max(1, ext_launches),
-                "avg_launch_ms": ext_ms / max(1, ext_launches), "launches": ext_launches,
-                "nodes_per_ray": ext["nodes"] / max(1, ext["rays"]),
-                "tris_per_ray": ext["tris"] / max(1, ext["rays"]),
-                "stage_ms": {k: v[0] for k, v in stages.items()}}
-
-    # ---------------------------------------------------------- ray-query workload
-    rq = None
-    if rank == 0 and not args.no_rayquery:
-        rq = ray_query(local)
-
-    # ---------------------------------------------------------- CPU baseline
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        import oracle
-        kind = "reference" if oracle.have_reference() else "port"
-        cs = scenes.sphere_grid_settings(spp=1)
-        cs.firefly_clamp = 0.0 if kind == "reference" else cs.firefly_clamp
-        threads = os.cpu_count() or 1
-        v, sample = cpu_sample_paths(scene, cs, 10.0, threads, kind)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"random {sample['pixels']} of {W * H} pixels of this frame at 1 spp, "
-                         f"{sample['render_ms']:.0f} ms render on {threads} threads"}
-
-    if rank == 0:
-        launches_per_step = 2 + 3 * settings.max_depth
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-                "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": 1,
-                           "max_depth": settings.max_depth, "triangles": scene.triangle_count,
-                           "wide_nodes": accel["wide_node_count"], "bvh_build_ms": build_ms,
-                           "l2": "inputs larger than L2 (BVH+triangles %.0f MB, wave state %.0f MB)" % (
-                               accel["device_bytes"] / 1e6, 140 * W * H / 1e6),
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-                "mrays_per_s": mrays, "segments_per_path": segs / max(1, counters["samples"]),
-                "reference_paths_per_sec_def": segs / max(1, counters["samples"]) * value,
-                "gpu_launches": launches_per_step * args.steps,
-                "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "ray_query": rq,
-                "cpu_baseline": cpu}
-        print(json.dumps(line), flush=True)
-
-
-def extension_stats(scene, settings, first, steps, device):
-    """Extension-ray traversal counts of the same samples (deterministic)."""
-    import ctypes
-    from vkpathtracer_b200.tracer import CudaPathTracer
-    with CudaPathTracer(device=device, collect_stats=True) as t:
-        t.configure(settings)
-        t.load_scene_snapshot(scene)
+    from vkpathtracer_b200.tracer import BatchRenderer, CudaPathTracer
+    sc = scenes.sphere_grid()
+    st = scenes.sphere_grid_settings()
+    out = {"workload": "sphere_grid_64x64_1080p_64spp_depth16", "triangles": sc.triangle_count}
+    with BatchRenderer(device=device) as b:
+        b.add_job(sc, st)
+        b.run("persistent")
+        runs = [b.run("persistent") for _ in range(2)]
+        ms = min(r["device_ms"] for r in runs)
+        r = runs[0]
+        out["paths_per_s"] = r["paths"] / (ms / 1e3)
+        out["mrays_per_s"] = (r["segments"] + r["shadow_rays"]) / (ms / 1e3) / 1e6
+        out["ms_per_frame_64spp"] = ms
+    with CudaPathTracer(device=device) as t:
+        t.configure(st)
+        t.load_scene_snapshot(sc)
         t.build_or_update_acceleration()
+        s = torch.cuda.Stream()
+        t.set_stream(s.cuda_stream)
         t.reset_accumulation()
-        t.render_frame(first, steps)
-        return t.extension_counters()
+        t.render_frame(0, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        t.render_frame(1, 8, sync=False)
+        e1.record(s)
+        s.synchronize()
+        out["wavefront_one_sample_per_launch_paths_per_s"] = 8 * st.width * st.height / (e0.elapsed_time(e1) / 1e3)
+    return out
 
 
 def ray_query(device):
@@ -369,23 +253,130 @@ def ray_query(device):
                     t.trace_rays_device(d_rays.data_ptr(), 0, n, mode, prim.data_ptr(), dist.data_ptr(), s.cuda_stream)
                 e1.record(s)
             s.synchronize()
-            ms = e0.elapsed_time(e1) / 10
-            out[f"{name}_mrays_per_s"] = n / ms / 1e3
-        # end to end through the host-buffer call
+            out[f"{name}_mrays_per_s"] = n / (e0.elapsed_time(e1) / 10) / 1e3
         t0 = time.perf_counter()
         t.trace_rays(rays)
         out["closest_e2e_mrays_per_s"] = n / (time.perf_counter() - t0) / 1e6
     return out
 
 
+def run_ours(args, world, rank, local):
+    import torch
+    from vkpathtracer_b200 import autotune
+    from vkpathtracer_b200.tracer import BatchRenderer
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    hbm_peak, peak_kind = peaks()
+    # Each rank renders its own replica of the job set (disjoint seeds).
+    jobs = make_jobs(args.jobs, seed=5 + 1000 * rank)
+    total_paths = sum(j.settings.width * j.settings.height * j.settings.spp for j in jobs)
+    b = BatchRenderer(device=local)
+    t0 = time.time()
+    for j in jobs:
+        b.add_job(j.scene, j.settings)
+    setup_s = time.time() - t0
+    key = autotune.workload_key((j.scene.triangle_count, j.settings.width, j.settings.spp, j.settings.max_depth)
+                                for j in jobs)
+    tune = autotune.tune_batch(b, key, use_cache=not args.retune)
+    tuning = {k: tune[k] for k in ("pool_paths", "block_size", "stack_depth", "steps")}
+
+    # ---------------------------------------------------------- plain mode (one frame per launch)
+    plain = b.run("plain")
+    plain_ps = plain["paths"] / (plain["device_ms"] / 1e3)
+
+    # ---------------------------------------------------------- timed persistent runs
+    for _ in range(args.warmup):
+        b.run("persistent", **tuning)
+    barrier(world)
+    torch.cuda.synchronize()
+    stats = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            stats.append(b.run("persistent", **tuning))
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_total = sum(s["device_ms"] for s in stats)
+    ms_max = reduce_over_ranks(world, ms_total, "max", dev)
+    all_paths = reduce_over_ranks(world, float(total_paths * args.steps), "sum", dev)
+    value = all_paths / (ms_max / 1e3)
+    st0 = stats[-1]
+    mrays = (st0["segments"] + st0["shadow_rays"]) / (st0["device_ms"] / 1e3) / 1e6
+
+    # ---------------------------------------------------------- end to end: C ABI + films to host
+    hostfilms = [np.empty((j.settings.height, j.settings.width, 3), np.float32) for j in jobs]
+    d2h = sum(j.settings.width * j.settings.height * 16 for j in jobs)
+    barrier(world)
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.run("persistent", **tuning)
+        for k in range(len(jobs)):
+            hostfilms[k][:] = b.film(k)[0]
+    e2e_ms = reduce_over_ranks(world, 1e3 * (time.perf_counter() - w0), "max", dev)
+    e2e = {"value": all_paths / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+           "path": "vkptc_batch_run (persistent, graph) + vkptc_batch_read_film of every job to host, every step; "
+                   "scenes and BVHs uploaded once before timing"}
+
+    roof = rq = ff = cpu = None
+    if rank == 0:
+        # ------------------------------------------------------ roofline of the persistent kernel
+        with BatchRenderer(device=local, collect_stats=True) as bs:
+            for j in jobs:
+                bs.add_job(j.scene, j.settings)
+            ss = bs.run("persistent", **tuning)
+        rays = ss["ext_rays"] + ss["shadow_queries"]
+        nodes = ss["ext_nodes"] + ss["shadow_nodes"]
+        tris = ss["ext_tris"] + ss["shadow_tris"]
+        alg = NODE_BYTES * nodes + TRI_BYTES * tris + RAY_IO_BYTES * rays + PATH_STATE_BYTES * ss["segments"] \
+            + 16 * ss["paths"]
+        kernel_ms = st0["device_ms"]
+        achieved = alg / (kernel_ms / 1e3) / 1e9
+        roof = {"kernel": "k_batch (persistent wavefront: regen, closest-hit, shade, any-hit, finish)",
+                "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": None,
+                "alg_bytes_per_launch": alg, "avg_launch_ms": kernel_ms, "launches": 1,
+                "nodes_per_ray": nodes / max(1, rays), "tris_per_ray": tris / max(1, rays),
+                "note": "one persistent launch per step; timing includes the pool reset and in-order film "
+                        "accumulation kernels of the same graph"}
+        if not args.no_rayquery:
+            rq = ray_query(local)
+        if not args.no_fullframe:
+            ff = full_frame(local)
+        if world == 1 and not args.no_cpu:
+            import oracle
+            kind = "reference" if oracle.have_reference() else "port"
+            threads = os.cpu_count() or 1
+            v, sample = cpu_sample(jobs, 15.0, threads, kind)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                   "sample": f"random {sample['pixel_fraction']:.4f} of every job's pixels at the job's spp "
+                             f"({sample['paths']} paths, {sample['render_ms']:.0f} ms on {threads} threads)"}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+                "config": {"workload": WORKLOAD, "jobs": len(jobs), "paths_per_step": total_paths,
+                           "triangles": sum(j.scene.triangle_count for j in jobs),
+                           "setup_s": setup_s, "tuning": tuning, "autotune": {k: tune.get(k) for k in
+                                                                              ("ms", "trials", "cached")},
+                           "l2": "inputs larger than L2 (all scenes, BVHs and the path pool resident in HBM)",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "mrays_per_s": mrays, "plain_paths_per_s": plain_ps, "speedup_vs_plain": value / world / plain_ps,
+                "plain_kernel_launches": plain["kernel_launches"],
+                "gpu_launches": sum(s["kernel_launches"] for s in stats),
+                "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--jobs", type=int, default=64)
+    ap.add_argument("--retune", action="store_true")
     ap.add_argument("--no-rayquery", action="store_true")
+    ap.add_argument("--no-fullframe", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -286,6 +286,9 @@ typedef struct vkptc_batch_stats {
   uint32_t stack_depth;
   uint32_t steps;
   uint32_t reserved;
+  /* traversal work (filled when vkptc_config.collect_stats = 1) */
+  uint64_t ext_rays, ext_nodes, ext_tris;
+  uint64_t shadow_queries, shadow_nodes, shadow_tris;
 } vkptc_batch_stats;
 
 int32_t vkptc_batch_create(const vkptc_config* config, vkptc_batch** out_batch);

@@ -1,0 +1,128 @@
+"""Autotuner for the persistent batched renderer and the wavefront renderer.
+
+Sweeps the launch parameters the kernels expose -- path-pool capacity (the
+device queue capacity), block size, traversal-stack entries kept in shared
+memory, and traversal steps between warp refills -- on a short run of the
+actual workload (one sample per job), keeps the fastest, and caches the
+choice in a JSON file keyed by GPU name and workload signature.  Films do not
+depend on these parameters (tests/test_gpu_batch.py), only speed does.
+"""
+from __future__ import annotations
+
+import hashlib
+import itertools
+import json
+import os
+import time
+from typing import Dict, Iterable, Optional
+
+DEFAULT_POOLS = (1 << 19, 1 << 20, 1 << 21, 1 << 22)
+DEFAULT_BLOCKS = (128, 256)
+DEFAULT_STACKS = (8, 16, 24)
+DEFAULT_STEPS = (4, 8)
+
+
+def cache_path() -> str:
+    base = os.environ.get("VKPTC_AUTOTUNE_CACHE")
+    if base:
+        return base
+    root = os.environ.get("XDG_CACHE_HOME", os.path.join(os.path.expanduser("~"), ".cache"))
+    return os.path.join(root, "vkpathtracer_b200", "autotune.json")
+
+
+def _gpu_name() -> str:
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.get_device_name(0)
+    except Exception:
+        pass
+    return "unknown"
+
+
+def workload_key(jobs_desc: Iterable) -> str:
+    h = hashlib.sha256()
+    for d in jobs_desc:
+        h.update(repr(d).encode())
+    return h.hexdigest()[:16]
+
+
+def _load_cache() -> Dict:
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _store_cache(data: Dict) -> None:
+    path = cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def tune_batch(batch, key: str, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS, stacks=DEFAULT_STACKS,
+               steps=DEFAULT_STEPS, sample_limit: int = 1, repeats: int = 2, use_cache: bool = True,
+               log: Optional[callable] = None) -> Dict:
+    """Returns {"pool_paths", "block_size", "stack_depth", "steps", "ms", "trials"} for `batch`."""
+    cache = _load_cache() if use_cache else {}
+    ckey = f"batch/{_gpu_name()}/{key}"
+    if use_cache and ckey in cache:
+        return dict(cache[ckey], cached=True)
+    best = None
+    trials = []
+    t0 = time.time()
+    for pool, block, stack, st in itertools.product(pools, blocks, stacks, steps):
+        try:
+            ms = min(batch.run("persistent", pool_paths=pool, block_size=block, stack_depth=stack, steps=st,
+                               sample_limit=sample_limit, use_graph=False)["device_ms"] for _ in range(repeats))
+        except Exception as e:   # a shape that does not fit (e.g. shared memory) is skipped
+            trials.append({"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st,
+                           "error": str(e)})
+            continue
+        trials.append({"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st, "ms": ms})
+        if log:
+            log(trials[-1])
+        if best is None or ms < best["ms"]:
+            best = {"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st, "ms": ms}
+    if best is None:
+        raise RuntimeError("autotune: no launch configuration ran")
+    best["trials"] = len(trials)
+    best["tune_seconds"] = time.time() - t0
+    if use_cache:
+        cache[ckey] = best
+        _store_cache(cache)
+    return dict(best, cached=False, all=trials)
+
+
+def tune_wavefront(make_tracer, render_samples: int = 1, blocks=DEFAULT_BLOCKS, stacks=DEFAULT_STACKS,
+                   steps=DEFAULT_STEPS, log: Optional[callable] = None) -> Dict:
+    """Sweeps block size, stack entries and steps of the wavefront renderer.
+    make_tracer(block_size, stack_depth, steps) must return a ready CudaPathTracer."""
+    import torch
+    best = None
+    for block, stack, st in itertools.product(blocks, stacks, steps):
+        t = make_tracer(block, stack, st)
+        s = torch.cuda.Stream()
+        t.set_stream(s.cuda_stream)
+        t.reset_accumulation()
+        t.render_frame(0, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        t.render_frame(1, render_samples, sync=False)
+        e1.record(s)
+        s.synchronize()
+        ms = e0.elapsed_time(e1) / render_samples
+        t.close()
+        rec = {"block_size": block, "stack_depth": stack, "steps": st, "ms": ms}
+        if log:
+            log(rec)
+        if best is None or ms < best["ms"]:
+            best = rec
+    return best

@@ -381,7 +381,7 @@ cudaError_t LaunchBatchPersistent(const DevJob* d_jobs, uint32_t job_count, unsi
   int scap = bl.smem_entries, tcap = bl.stack_cap, steps = bl.steps;
   int2* spill = bl.spill;
   void* args[] = {&jobs, &jc, &total, &P, &scap, &spill, &tcap, &steps, &ctr, &err};
-  const bool stats = false;
+  const bool stats = bl.stats;
   const void* fn = bl.parity ? (stats ? reinterpret_cast<const void*>(k_batch<true, true>)
                                       : reinterpret_cast<const void*>(k_batch<true, false>))
                              : (stats ? reinterpret_cast<const void*>(k_batch<false, true>)

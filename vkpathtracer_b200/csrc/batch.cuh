@@ -49,6 +49,7 @@ struct BatchLaunch {
   int2* spill;
   cudaStream_t stream;
   bool parity;
+  bool stats;   // count traversal work (node/leaf/triangle visits)
 };
 
 // Number of control words the pool needs.

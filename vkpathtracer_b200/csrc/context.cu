@@ -974,6 +974,7 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   bl.steps = t.steps ? static_cast<int>(t.steps) : kDefaultSteps;
   bl.stream = b->stream;
   bl.parity = parity;
+  bl.stats = b->config.collect_stats != 0u;
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
@@ -1093,6 +1094,12 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   VKPTC_BCUDA(b, cudaMemcpy(&dc, b->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost), "counters");
   b->stats.segments = dc.rays;
   b->stats.shadow_rays = dc.shadow_tests;
+  b->stats.ext_rays = dc.ext_rays;
+  b->stats.ext_nodes = dc.nodes;
+  b->stats.ext_tris = dc.tris;
+  b->stats.shadow_queries = dc.shadow_rays;
+  b->stats.shadow_nodes = dc.shadow_nodes;
+  b->stats.shadow_tris = dc.shadow_tris;
   b->stats.device_ms = ms;
   b->stats.kernel_launches = 2u + static_cast<uint64_t>(table.size());   // init, persistent, accumulate per job
   b->stats.graph_used = graph_used ? 1u : 0u;

@@ -95,7 +95,10 @@ class BatchStats(ctypes.Structure):
                 ("segments", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("device_ms", ctypes.c_double), ("grid", ctypes.c_uint32),
                 ("block", ctypes.c_uint32), ("pool_paths", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
-                ("steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("ext_rays", ctypes.c_uint64), ("ext_nodes", ctypes.c_uint64), ("ext_tris", ctypes.c_uint64),
+                ("shadow_queries", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64),
+                ("shadow_tris", ctypes.c_uint64)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}

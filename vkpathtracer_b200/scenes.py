@@ -494,6 +494,7 @@ def batch_jobs(count: int = 64, seed: int = 5, max_triangles: int = 500_000, max
         grid = max(1, int(round(math.sqrt(tris / per))))
         if grid * grid * per > max_triangles * 1.2:
             grid = max(1, grid - 1)
+        grid = max(grid, int(math.ceil(math.sqrt(min_triangles / per))))
         scene = sphere_field(grid, n_lat, n_lon, job_seed % 100000 + 7, n_lights=min(16, max(1, grid)),
                              light_size=max(1.0, 0.1 * grid * 3.0), light_height=max(4.0, 0.25 * grid * 3.0))
         settings = RenderSettings(width=side, height=side, spp=spp, max_depth=depth, seed=job_seed,

@@ -306,11 +306,12 @@ class BatchRenderer:
     device work queue, replayed from a CUDA graph.  Films are bit-identical.
     """
 
-    def __init__(self, device: int = 0, math_mode: int = 0):
+    def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
         cfg.math_mode = math_mode
+        cfg.collect_stats = int(collect_stats)
         h = ctypes.c_void_p()
         rc = self._lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != native.OK:
