@@ -278,7 +278,7 @@ def run_ours(args, world, rank, local):
     key = autotune.workload_key((j.scene.triangle_count, j.settings.width, j.settings.spp, j.settings.max_depth)
                                 for j in jobs)
     tune = autotune.tune_batch(b, key, use_cache=not args.retune)
-    tuning = {k: tune[k] for k in ("pool_paths", "block_size", "stack_depth", "steps")}
+    tuning = {k: tune[k] for k in ("pool_paths", "block_size", "stack_depth", "steps", "occupancy")}
 
     # ---------------------------------------------------------- plain mode (one frame per launch)
     plain = b.run("plain")

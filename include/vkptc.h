@@ -269,7 +269,9 @@ typedef struct vkptc_batch_tuning {
   uint32_t steps;            /* traversal steps between warp refills; 0 = default */
   uint32_t sample_limit;     /* render at most this many samples per job (0 = each job's spp) */
   uint32_t use_graph;        /* persistent mode: 1 = capture once, replay the CUDA graph */
-  uint32_t reserved[2];
+  uint32_t occupancy;        /* persistent kernel register variant: 0..3 = at least 1..4 resident
+                                256-thread blocks per SM (fewer registers, more warps) */
+  uint32_t reserved;
 } vkptc_batch_tuning;
 
 typedef struct vkptc_batch_stats {

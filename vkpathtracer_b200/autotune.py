@@ -20,6 +20,7 @@ DEFAULT_POOLS = (1 << 19, 1 << 20, 1 << 21, 1 << 22)
 DEFAULT_BLOCKS = (128, 256)
 DEFAULT_STACKS = (8, 16, 24)
 DEFAULT_STEPS = (4, 8)
+DEFAULT_OCCUPANCY = (0, 1, 2, 3)
 
 
 def cache_path() -> str:
@@ -68,9 +69,12 @@ def _store_cache(data: Dict) -> None:
 
 
 def tune_batch(batch, key: str, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS, stacks=DEFAULT_STACKS,
-               steps=DEFAULT_STEPS, sample_limit: int = 1, repeats: int = 2, use_cache: bool = True,
-               log: Optional[callable] = None) -> Dict:
-    """Returns {"pool_paths", "block_size", "stack_depth", "steps", "ms", "trials"} for `batch`."""
+               steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1, repeats: int = 2,
+               use_cache: bool = True, log: Optional[callable] = None) -> Dict:
+    """Returns {"pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials"}.
+
+    Coordinate search: the pool capacity first (other parameters at their
+    defaults), then block size x stack entries x steps x register variant."""
     cache = _load_cache() if use_cache else {}
     ckey = f"batch/{_gpu_name()}/{key}"
     if use_cache and ckey in cache:
@@ -78,19 +82,26 @@ def tune_batch(batch, key: str, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS, stac
     best = None
     trials = []
     t0 = time.time()
-    for pool, block, stack, st in itertools.product(pools, blocks, stacks, steps):
+
+    def trial(cfg):
+        nonlocal best
         try:
-            ms = min(batch.run("persistent", pool_paths=pool, block_size=block, stack_depth=stack, steps=st,
-                               sample_limit=sample_limit, use_graph=False)["device_ms"] for _ in range(repeats))
+            ms = min(batch.run("persistent", sample_limit=sample_limit, use_graph=False, **cfg)["device_ms"]
+                     for _ in range(repeats))
         except Exception as e:   # a shape that does not fit (e.g. shared memory) is skipped
-            trials.append({"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st,
-                           "error": str(e)})
-            continue
-        trials.append({"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st, "ms": ms})
+            trials.append(dict(cfg, error=str(e)))
+            return
+        trials.append(dict(cfg, ms=ms))
         if log:
             log(trials[-1])
         if best is None or ms < best["ms"]:
-            best = {"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st, "ms": ms}
+            best = dict(cfg, ms=ms)
+
+    for pool in pools:
+        trial({"pool_paths": pool, "block_size": 0, "stack_depth": 0, "steps": 0, "occupancy": 0})
+    pool = best["pool_paths"] if best else pools[0]
+    for block, stack, st, occ in itertools.product(blocks, stacks, steps, occupancy):
+        trial({"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st, "occupancy": occ})
     if best is None:
         raise RuntimeError("autotune: no launch configuration ran")
     best["trials"] = len(trials)

@@ -130,10 +130,13 @@ struct BatchShadowSource {
 
 }  // namespace
 
-template <bool kParity, bool kStats>
-__global__ void __launch_bounds__(256) k_batch(const DevJob* __restrict__ jobs, uint32_t job_count,
-                                               unsigned long long total, BatchPool P, int scap, int2* spill,
-                                               int total_cap, int steps, DevCounters* ctr, uint32_t* err) {
+// kMinBlocks: resident 256-thread blocks per SM the register allocation must
+// allow (0 = compiler's choice); the autotuner picks the occupancy/spill trade-off.
+template <bool kParity, bool kStats, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restrict__ jobs, uint32_t job_count,
+                                                           unsigned long long total, BatchPool P, int scap,
+                                                           int2* spill, int total_cap, int steps, DevCounters* ctr,
+                                                           uint32_t* err) {
   extern __shared__ int2 smem_stack[];
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gthreads = gridDim.x * blockDim.x;
@@ -353,21 +356,36 @@ cudaError_t set_smem_attr(K kernel, int bytes) {
 }
 }  // namespace
 
+// Kernel variant table: [parity][stats][occupancy variant].
+namespace {
+using BatchFn = void (*)(const DevJob*, uint32_t, unsigned long long, BatchPool, int, int2*, int, int, DevCounters*,
+                         uint32_t*);
+constexpr int kOccVariants = 4;   // minBlocks 1, 2, 3, 4
+BatchFn batch_fn(bool parity, bool stats, int occ) {
+  static const BatchFn table[2][2][kOccVariants] = {
+      {{k_batch<false, false, 1>, k_batch<false, false, 2>, k_batch<false, false, 3>, k_batch<false, false, 4>},
+       {k_batch<false, true, 1>, k_batch<false, true, 1>, k_batch<false, true, 1>, k_batch<false, true, 1>}},
+      {{k_batch<true, false, 1>, k_batch<true, false, 2>, k_batch<true, false, 3>, k_batch<true, false, 4>},
+       {k_batch<true, true, 1>, k_batch<true, true, 1>, k_batch<true, true, 1>, k_batch<true, true, 1>}}};
+  const int o = occ < 0 ? 0 : (occ >= kOccVariants ? kOccVariants - 1 : occ);
+  return table[parity ? 1 : 0][stats ? 1 : 0][o];
+}
+}  // namespace
+
 cudaError_t ConfigureBatchSmem(size_t bytes) {
   const int b = static_cast<int>(bytes);
-  cudaError_t e = set_smem_attr(k_batch<true, false>, b);
-  if (e == cudaSuccess) e = set_smem_attr(k_batch<true, true>, b);
-  if (e == cudaSuccess) e = set_smem_attr(k_batch<false, false>, b);
-  if (e == cudaSuccess) e = set_smem_attr(k_batch<false, true>, b);
+  cudaError_t e = cudaSuccess;
+  for (int p = 0; p < 2 && e == cudaSuccess; ++p)
+    for (int st = 0; st < 2 && e == cudaSuccess; ++st)
+      for (int o = 0; o < kOccVariants && e == cudaSuccess; ++o)
+        e = set_smem_attr(batch_fn(p != 0, st != 0, o), b);
   return e;
 }
 
-int BatchBlocksPerSm(int block, size_t smem, bool parity) {
+int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occ) {
   int blocks = 0;
-  const cudaError_t e = parity
-      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch<true, false>, block, smem)
-      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch<false, false>, block, smem);
-  if (e != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_fn(parity, stats, occ), block, smem) != cudaSuccess)
+    return 0;
   return blocks;
 }
 
@@ -381,11 +399,7 @@ cudaError_t LaunchBatchPersistent(const DevJob* d_jobs, uint32_t job_count, unsi
   int scap = bl.smem_entries, tcap = bl.stack_cap, steps = bl.steps;
   int2* spill = bl.spill;
   void* args[] = {&jobs, &jc, &total, &P, &scap, &spill, &tcap, &steps, &ctr, &err};
-  const bool stats = bl.stats;
-  const void* fn = bl.parity ? (stats ? reinterpret_cast<const void*>(k_batch<true, true>)
-                                      : reinterpret_cast<const void*>(k_batch<true, false>))
-                             : (stats ? reinterpret_cast<const void*>(k_batch<false, true>)
-                                      : reinterpret_cast<const void*>(k_batch<false, false>));
+  const void* fn = reinterpret_cast<const void*>(batch_fn(bl.parity, bl.stats, bl.occupancy));
   return cudaLaunchCooperativeKernel(fn, dim3(bl.grid), dim3(bl.block), args, smem, bl.stream);
 }
 

@@ -50,6 +50,7 @@ struct BatchLaunch {
   cudaStream_t stream;
   bool parity;
   bool stats;   // count traversal work (node/leaf/triangle visits)
+  int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
 };
 
 // Number of control words the pool needs.
@@ -68,7 +69,7 @@ cudaError_t LaunchStagingAccumulate(const DevJob* d_jobs, uint32_t job_count, un
 cudaError_t LaunchBatchInit(const BatchPool& pool, cudaStream_t stream);
 
 // Resident blocks per SM of the persistent batch kernel.
-int BatchBlocksPerSm(int block, size_t smem, bool parity);
+int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occupancy);
 cudaError_t ConfigureBatchSmem(size_t bytes);
 
 }  // namespace vkptc

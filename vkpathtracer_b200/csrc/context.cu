@@ -975,6 +975,7 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   bl.stream = b->stream;
   bl.parity = parity;
   bl.stats = b->config.collect_stats != 0u;
+  bl.occupancy = static_cast<int>(std::min(3u, t.occupancy));
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
@@ -983,7 +984,7 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
     VKPTC_BCUDA(b, ConfigureBatchSmem(smem), "shared memory limit");
     b->smem_configured = smem;
   }
-  const int per_sm = BatchBlocksPerSm(bl.block, smem, parity);
+  const int per_sm = BatchBlocksPerSm(bl.block, smem, parity, bl.stats, bl.occupancy);
   if (per_sm <= 0) return bfail(b, VKPTC_UNSUPPORTED, "persistent batch kernel does not fit on an SM with this block size");
   bl.grid = per_sm * b->sm_count;
   const size_t spill_entries =
@@ -1050,6 +1051,7 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   bool graph_used = false;
   if (t.use_graph) {
     const std::string key = std::to_string(cap) + "/" + std::to_string(bl.block) + "/" + std::to_string(bl.smem_entries) +
+                            "/o" + std::to_string(bl.occupancy) +
                             "/" + std::to_string(bl.steps) + "/" + std::to_string(t.sample_limit) + "/" +
                             std::to_string(b->jobs.size()) + "/" +
                             std::to_string(reinterpret_cast<uintptr_t>(b->staging.ptr)) + "/" +

@@ -87,7 +87,7 @@ class AccelInfo(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("pool_paths", ctypes.c_uint32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
                 ("steps", ctypes.c_uint32), ("sample_limit", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 2)]
+                ("occupancy", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class BatchStats(ctypes.Structure):

@@ -350,8 +350,8 @@ class BatchRenderer:
         return int(jid.value)
 
     def run(self, mode: str = "persistent", pool_paths: int = 0, block_size: int = 0, stack_depth: int = 0,
-            steps: int = 0, sample_limit: int = 0, use_graph: bool = True) -> dict:
-        t = native.BatchTuning(pool_paths, block_size, stack_depth, steps, sample_limit, int(use_graph))
+            steps: int = 0, sample_limit: int = 0, use_graph: bool = True, occupancy: int = 0) -> dict:
+        t = native.BatchTuning(pool_paths, block_size, stack_depth, steps, sample_limit, int(use_graph), occupancy)
         m = native.BATCH_PERSISTENT if mode == "persistent" else native.BATCH_PLAIN
         rc = self._lib.vkptc_batch_run(self._b, m, ctypes.byref(t))
         if rc != native.OK:
