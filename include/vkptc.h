@@ -62,10 +62,17 @@ typedef struct vkptc_config {
                                 spill to global memory); 0 = 16 */
   uint32_t math_mode;        /* 0 = parity (transcendentals in FP64, rounded once), 1 = fast FP32 */
   uint32_t collect_stats;    /* 1 = count node/leaf/triangle visits (device counters) */
-  /* reserved[0]: paths per wave (0 = 4 Mi); reserved[1]: 1 = per-stage CUDA-event timing;
-   * reserved[2]: traversal steps between warp refills (0 = 4) */
-  uint32_t reserved[3];
+  uint32_t wave_paths;       /* paths per wavefront wave (0 = 4 Mi) */
+  uint32_t stage_timing;     /* 1 = CUDA-event timing of every stage launch */
+  uint32_t steps;            /* traversal steps between warp refills (0 = 4) */
+  uint32_t bvh_mode;         /* traversal tree: VKPTC_BVH_REFERENCE (the reference builder's tree,
+                                flattened) or VKPTC_BVH_SAH (binned SAH); hit ids are the
+                                reference's in both (ties/parallel rule use the reference tree) */
+  uint32_t reserved[4];
 } vkptc_config;
+
+#define VKPTC_BVH_REFERENCE 0u
+#define VKPTC_BVH_SAH 1u
 
 /* Mirrors RenderSettings (src/pathtracer/PathTracer.h:134-178). */
 typedef struct vkptc_render_settings {

@@ -101,3 +101,16 @@ def test_each_job_matches_oracle_on_pixel_subset(batch):
         exact = np.mean(np.all(bits(got) == bits(ref), axis=1))
         rel = np.sqrt(np.mean((got - ref) ** 2)) / (np.mean(ref) + 1e-9)
         assert exact >= 0.95 and rel < 1e-3, (j, o.kind, exact, rel)
+
+
+def test_sah_batch_equals_reference_tree_batch(batch):
+    n = len(small_jobs())
+    batch.run("persistent")
+    ref = films(batch, n)
+    with BatchRenderer(bvh="sah") as b2:
+        for sc, st in small_jobs():
+            b2.add_job(sc, st)
+        b2.run("persistent")
+        for j in range(n):
+            f, c = b2.film(j)
+            assert np.array_equal(c, ref[j][1]) and np.array_equal(bits(f), bits(ref[j][0]))

@@ -27,7 +27,7 @@ def bits(a):
     return np.ascontiguousarray(a, np.float32).view(np.uint32)
 
 
-def make_tracer(scene, st, **kw):
+def make_tracer(scene, st, **kw):  # kw: CudaPathTracer options (bvh="sah" selects the SAH traversal tree)
     t = CudaPathTracer(**kw)
     assert t.configure(st)
     assert t.load_scene_snapshot(scene)
@@ -53,23 +53,28 @@ def film_report(gpu_sum, ref_sum, ref_samples, spp):
 
 
 # ------------------------------------------------------------------ hit ids
+BVHS = ["reference", "sah"]
+
+
+@pytest.mark.parametrize("bvh", BVHS)
 @pytest.mark.parametrize("name", ["box", "field", "sphere"])
-def test_closest_hit_ids_bit_exact_vs_reference_golden(name):
+def test_closest_hit_ids_bit_exact_vs_reference_golden(name, bvh):
     d = cases.load_fixture(name)
     sc = cases.scene_from_arrays(d)
     st = scenes.RenderSettings(width=8, height=8, spp=1)
-    with make_tracer(sc, st) as t:
+    with make_tracer(sc, st, bvh=bvh) as t:
         p, tt = t.trace_rays(d["rays"])
     assert np.array_equal(p, d["hit_prim"]), f"{np.sum(p != d['hit_prim'])} mismatching ids"
     assert np.array_equal(bits(tt), bits(d["hit_t"]))
 
 
-def test_closest_hit_ids_bit_exact_larger_sphere():
+@pytest.mark.parametrize("bvh", BVHS)
+def test_closest_hit_ids_bit_exact_larger_sphere(bvh):
     sc = scenes.displaced_sphere(resolution=256, seed=2)
     rays = scenes.ray_query_rays(sc, primary_side=256, random_count=65536, seed=4)
     o = oracle.load("auto")
     pr, tr, _, _ = o.intersect(sc, rays, threads=8)
-    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1), bvh=bvh) as t:
         p, tt = t.trace_rays(rays)
         info = t.accel_info()
     assert info["primitive_count"] == sc.triangle_count
@@ -77,20 +82,22 @@ def test_closest_hit_ids_bit_exact_larger_sphere():
     assert np.array_equal(bits(tt), bits(tr))
 
 
-def test_exact_ties_follow_reference_visit_order():
+@pytest.mark.parametrize("bvh", BVHS)
+def test_exact_ties_follow_reference_visit_order(bvh):
     """Rays through shared quad diagonals and box edges produce exact-t ties."""
     sc = scenes.cornell_box(seed=1)
     cam = sc.camera
     rays = scenes.primary_rays(cam, 512, 512)
     o = oracle.load("auto")
     pr, tr, _, _ = o.intersect(sc, rays, threads=8)
-    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1), bvh=bvh) as t:
         p, tt = t.trace_rays(rays)
     assert np.array_equal(p, pr)
     assert np.array_equal(bits(tt), bits(tr))
 
 
-def test_parallel_axis_rays_match_reference_rule():
+@pytest.mark.parametrize("bvh", BVHS)
+def test_parallel_axis_rays_match_reference_rule(bvh):
     sc = scenes.displaced_sphere(resolution=64, seed=5)
     rng = np.random.default_rng(7)
     n = 20000
@@ -101,12 +108,18 @@ def test_parallel_axis_rays_match_reference_rule():
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     rays = np.ascontiguousarray(np.concatenate([o, d.astype(np.float32)], 1), np.float32)
     pr, tr, _, _ = oracle.load("auto").intersect(sc, rays, threads=8)
-    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1), bvh=bvh) as t:
         p, tt = t.trace_rays(rays)
     assert np.array_equal(p, pr)
+    # any-hit must apply the same rule: occluded exactly when the closest hit lies before tmax
+    tmax = np.where(np.isfinite(tr), tr * np.float32(1.5), np.float32(100.0)).astype(np.float32)
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1), bvh=bvh) as t:
+        occ, _ = t.trace_rays(rays, mode=native.QUERY_ANY, tmax=tmax)
+    assert np.array_equal(occ.astype(bool), np.isfinite(tr) & (tr < tmax))
 
 
-def test_any_hit_equals_closest_hit_before_tmax():
+@pytest.mark.parametrize("bvh", BVHS)
+def test_any_hit_equals_closest_hit_before_tmax(bvh):
     d = cases.load_fixture("sphere")
     sc = cases.scene_from_arrays(d)
     rays = d["rays"]
@@ -115,7 +128,7 @@ def test_any_hit_equals_closest_hit_before_tmax():
     tmax = np.where(np.isfinite(tref), tref * rng.uniform(0.5, 1.5, tref.shape), rng.uniform(1, 80, tref.shape))
     tmax = tmax.astype(np.float32)
     tmax[:50] = tref[:50]          # t == tmax exactly: not occluded (strict)
-    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1)) as t:
+    with make_tracer(sc, scenes.RenderSettings(width=8, height=8, spp=1), bvh=bvh) as t:
         occ, _ = t.trace_rays(rays, mode=native.QUERY_ANY, tmax=tmax)
         occ_inf, _ = t.trace_rays(rays, mode=native.QUERY_ANY)
     expect = (tref < tmax) & np.isfinite(tref)
@@ -260,3 +273,18 @@ def test_fast_math_mode_is_statistically_equal():
     rep = film_report(g, ref["sum"], ref["samples"], st.spp)
     print(rep)
     assert rep["rmse_rel"] < 0.05
+
+
+def test_sah_traversal_tree_renders_identical_films():
+    """The SAH traversal tree changes only the visiting order: every hit (id, t)
+    is the reference's, so films are bit-identical to the reference tree's."""
+    cases_ = [(scenes.cornell_box(seed=1), scenes.cornell_settings(48, 40, 3)),
+              (scenes.sphere_field(8, 15, 18, seed=4, light_size=3.0, light_height=8.0),
+               scenes.RenderSettings(width=96, height=64, spp=3, max_depth=12, seed=7, firefly_clamp=10.0))]
+    for sc, st in cases_:
+        with make_tracer(sc, st) as a, make_tracer(sc, st, bvh="sah") as b:
+            a.render_frame(0, st.spp)
+            b.render_frame(0, st.spp)
+            fa, ca, _ = a.film()
+            fb, cb, _ = b.film()
+        assert np.array_equal(ca, cb) and np.array_equal(bits(fa), bits(fb))

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <functional>
 #include <limits>
 #include <numeric>
@@ -166,6 +167,157 @@ void BuildBinaryBvh(const SceneGeometry& geo, uint32_t leaf_threshold, std::vect
   nodes.resize(static_cast<size_t>(b.next_id));
 }
 
+namespace {
+
+struct SahBuilder {
+  const float* boxes;
+  std::vector<BinNode>* nodes;
+  uint32_t* base;
+  uint32_t max_leaf;
+  static constexpr int kBins = 32;
+
+  static float area(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+  }
+
+  int32_t build(uint32_t* idx, size_t n) {
+    const int32_t id = static_cast<int32_t>(nodes->size());
+    nodes->push_back(BinNode{});
+    float lo[3], hi[3], clo[3], chi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = clo[a] = std::numeric_limits<float>::max();
+      hi[a] = chi[a] = -std::numeric_limits<float>::max();
+    }
+    for (size_t i = 0; i < n; ++i) {
+      const float* b = boxes + 6 * idx[i];
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], b[a]);
+        hi[a] = std::max(hi[a], b[3 + a]);
+        const float c = 0.5f * (b[a] + b[3 + a]);
+        clo[a] = std::min(clo[a], c);
+        chi[a] = std::max(chi[a], c);
+      }
+    }
+    auto make_leaf = [&]() {
+      BinNode& nd = (*nodes)[static_cast<size_t>(id)];
+      std::memcpy(nd.lo, lo, sizeof(lo));
+      std::memcpy(nd.hi, hi, sizeof(hi));
+      nd.left = nd.right = -1;
+      nd.first = static_cast<int32_t>(idx - base);
+      nd.count = static_cast<int32_t>(n);
+      return id;
+    };
+    if (n <= max_leaf) return make_leaf();
+    // Best binned split over the three axes.
+    int best_axis = -1, best_bin = -1;
+    float best_cost = std::numeric_limits<float>::max();
+    for (int a = 0; a < 3; ++a) {
+      const float ext = chi[a] - clo[a];
+      if (!(ext > 0.0f)) continue;
+      const float scale = kBins / ext;
+      uint32_t cnt[kBins] = {};
+      float blo[kBins][3], bhi[kBins][3];
+      for (int k = 0; k < kBins; ++k)
+        for (int q = 0; q < 3; ++q) {
+          blo[k][q] = std::numeric_limits<float>::max();
+          bhi[k][q] = -std::numeric_limits<float>::max();
+        }
+      for (size_t i = 0; i < n; ++i) {
+        const float* b = boxes + 6 * idx[i];
+        const float c = 0.5f * (b[a] + b[3 + a]);
+        int k = static_cast<int>((c - clo[a]) * scale);
+        k = std::min(kBins - 1, std::max(0, k));
+        ++cnt[k];
+        for (int q = 0; q < 3; ++q) {
+          blo[k][q] = std::min(blo[k][q], b[q]);
+          bhi[k][q] = std::max(bhi[k][q], b[3 + q]);
+        }
+      }
+      // Sweep: right-side areas, then left.
+      float rarea[kBins];
+      uint32_t rcnt[kBins];
+      float rlo[3], rhi[3];
+      for (int q = 0; q < 3; ++q) {
+        rlo[q] = std::numeric_limits<float>::max();
+        rhi[q] = -std::numeric_limits<float>::max();
+      }
+      uint32_t rc = 0;
+      for (int k = kBins - 1; k > 0; --k) {
+        rc += cnt[k];
+        for (int q = 0; q < 3; ++q) {
+          rlo[q] = std::min(rlo[q], blo[k][q]);
+          rhi[q] = std::max(rhi[q], bhi[k][q]);
+        }
+        rcnt[k] = rc;
+        rarea[k] = rc ? area(rlo, rhi) : 0.0f;
+      }
+      float llo[3], lhi[3];
+      for (int q = 0; q < 3; ++q) {
+        llo[q] = std::numeric_limits<float>::max();
+        lhi[q] = -std::numeric_limits<float>::max();
+      }
+      uint32_t lc = 0;
+      for (int k = 0; k < kBins - 1; ++k) {
+        lc += cnt[k];
+        for (int q = 0; q < 3; ++q) {
+          llo[q] = std::min(llo[q], blo[k][q]);
+          lhi[q] = std::max(lhi[q], bhi[k][q]);
+        }
+        if (lc == 0 || rcnt[k + 1] == 0) continue;
+        const float cost = area(llo, lhi) * static_cast<float>(lc) + rarea[k + 1] * static_cast<float>(rcnt[k + 1]);
+        if (cost < best_cost) {
+          best_cost = cost;
+          best_axis = a;
+          best_bin = k;
+        }
+      }
+    }
+    uint32_t* mid;
+    if (best_axis < 0) {
+      // All centroids coincide: split the list in half.
+      mid = idx + n / 2;
+    } else {
+      const float scale = kBins / (chi[best_axis] - clo[best_axis]);
+      const float c0 = clo[best_axis];
+      mid = std::partition(idx, idx + n, [&](uint32_t p) {
+        const float* b = boxes + 6 * p;
+        const float c = 0.5f * (b[best_axis] + b[3 + best_axis]);
+        int k = static_cast<int>((c - c0) * scale);
+        k = std::min(kBins - 1, std::max(0, k));
+        return k <= best_bin;
+      });
+      if (mid == idx || mid == idx + n) mid = idx + n / 2;
+    }
+    const size_t nl = static_cast<size_t>(mid - idx);
+    const int32_t l = build(idx, nl);
+    const int32_t r = build(mid, n - nl);
+    BinNode& nd = (*nodes)[static_cast<size_t>(id)];
+    std::memcpy(nd.lo, lo, sizeof(lo));
+    std::memcpy(nd.hi, hi, sizeof(hi));
+    nd.left = l;
+    nd.right = r;
+    nd.first = -1;
+    nd.count = 0;
+    return id;
+  }
+};
+
+}  // namespace
+
+void BuildSahBvh(const SceneGeometry& geo, uint32_t max_leaf, std::vector<BinNode>& nodes,
+                 std::vector<uint32_t>& prim_indices) {
+  const size_t n = geo.prims.size();
+  nodes.clear();
+  prim_indices.clear();
+  if (n == 0) return;
+  nodes.reserve(2 * n);
+  prim_indices.resize(n);
+  std::iota(prim_indices.begin(), prim_indices.end(), 0u);
+  SahBuilder b{geo.boxes.data(), &nodes, prim_indices.data(), std::max(1u, std::min(8u, max_leaf))};
+  b.build(prim_indices.data(), n);
+}
+
 bool ValidateBinaryBvh(const std::vector<BinNode>& nodes, const std::vector<uint32_t>& prim_indices,
                        size_t prim_count, std::string& error) {
   if (nodes.empty()) {
@@ -209,21 +361,32 @@ bool ValidateBinaryBvh(const std::vector<BinNode>& nodes, const std::vector<uint
 }
 
 void CollapseToWide(const SceneGeometry& geo, const std::vector<BinNode>& bin,
-                    const std::vector<uint32_t>& prim_indices, WideBvh& out) {
+                    const std::vector<uint32_t>& prim_indices, const std::vector<BinNode>& ref,
+                    const std::vector<uint32_t>& ref_prims, WideBvh& out) {
   out = WideBvh{};
-  if (bin.empty()) return;
-  out.binary_nodes = static_cast<uint32_t>(bin.size());
-  // Tie records: bounds, parent and depth of every binary node.
-  out.tie_nodes.resize(bin.size());
-  std::vector<int32_t> parent(bin.size(), -1), depth(bin.size(), 0);
+  if (bin.empty() || ref.empty()) return;
+  out.binary_nodes = static_cast<uint32_t>(ref.size());
+  out.reference_topology = (&bin == &ref) ||
+                           (bin.size() == ref.size() && prim_indices == ref_prims &&
+                            std::memcmp(bin.data(), ref.data(), bin.size() * sizeof(BinNode)) == 0);
+  // Tie records: bounds, parent and depth of every reference binary node, and
+  // for every primitive its reference leaf and lane.
+  out.tie_nodes.resize(ref.size());
+  std::vector<int32_t> parent(ref.size(), -1), depth(ref.size(), 0);
+  std::vector<uint32_t> ref_leaf(geo.prims.size(), 0u), ref_lane(geo.prims.size(), 0u);
   {
     std::vector<int32_t> st{0};
     while (!st.empty()) {
       const int32_t id = st.back();
       st.pop_back();
-      const BinNode& nd = bin[static_cast<size_t>(id)];
+      const BinNode& nd = ref[static_cast<size_t>(id)];
       if (nd.count > 0) {
         ++out.binary_leaves;
+        for (int32_t i = 0; i < nd.count; ++i) {
+          const uint32_t p = ref_prims[static_cast<size_t>(nd.first + i)];
+          ref_leaf[p] = static_cast<uint32_t>(id);
+          ref_lane[p] = static_cast<uint32_t>(i);
+        }
         continue;
       }
       for (int32_t c : {nd.left, nd.right}) {
@@ -233,14 +396,14 @@ void CollapseToWide(const SceneGeometry& geo, const std::vector<BinNode>& bin,
       }
     }
   }
-  for (size_t i = 0; i < bin.size(); ++i) {
+  for (size_t i = 0; i < ref.size(); ++i) {
     TieNode& t = out.tie_nodes[i];
-    t.lox = bin[i].lo[0];
-    t.loy = bin[i].lo[1];
-    t.loz = bin[i].lo[2];
-    t.hix = bin[i].hi[0];
-    t.hiy = bin[i].hi[1];
-    t.hiz = bin[i].hi[2];
+    t.lox = ref[i].lo[0];
+    t.loy = ref[i].lo[1];
+    t.loz = ref[i].lo[2];
+    t.hix = ref[i].hi[0];
+    t.hiy = ref[i].hi[1];
+    t.hiz = ref[i].hi[2];
     t.parent = parent[i];
     t.depth = depth[i];
   }
@@ -262,8 +425,8 @@ void CollapseToWide(const SceneGeometry& geo, const std::vector<BinNode>& bin,
       r.e2y = hp.e2[1];
       r.e2z = hp.e2[2];
       r.prim = p;
-      r.leaf = static_cast<uint32_t>(leaf_id);
-      r.lane = static_cast<uint32_t>(i);
+      r.leaf = ref_leaf[p];
+      r.lane = ref_lane[p];
       out.tris.push_back(r);
     }
     return ~static_cast<int32_t>((first << 3) | static_cast<uint32_t>(lf.count - 1));

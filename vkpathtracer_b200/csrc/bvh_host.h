@@ -65,6 +65,7 @@ struct WideBvh {
   uint32_t binary_leaves = 0;
   uint32_t depth = 0;
   uint32_t stack_required = 0;
+  bool reference_topology = true;   // traversal tree == reference tree
 };
 
 // Flattens instances x triangles in the accelerator's order, skipping
@@ -79,13 +80,25 @@ bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* 
 void BuildBinaryBvh(const SceneGeometry& geo, uint32_t leaf_threshold, std::vector<BinNode>& nodes,
                     std::vector<uint32_t>& prim_indices);
 
+// Binned-SAH binary BVH over the same padded primitive boxes (32 bins per
+// axis, leaves of <= max_leaf primitives).  Used only as the traversal tree:
+// hit ids stay the reference's because ties and the parallel-axis rule are
+// resolved against the reference tree (see CollapseToWide).
+void BuildSahBvh(const SceneGeometry& geo, uint32_t max_leaf, std::vector<BinNode>& nodes,
+                 std::vector<uint32_t>& prim_indices);
+
 // Validates an externally supplied binary BVH against the primitive count.
 bool ValidateBinaryBvh(const std::vector<BinNode>& nodes, const std::vector<uint32_t>& prim_indices,
                        size_t prim_count, std::string& error);
 
-// Collapses the binary tree into the wide layout.  Each wide child slot is a
-// binary node with its exact float bounds; leaves stay whole binary leaves.
+// Collapses a binary traversal tree into the wide layout.  Each wide child
+// slot is a binary node with its exact float bounds; leaves stay whole binary
+// leaves.  Triangle records and tie nodes come from the REFERENCE tree
+// (ref_nodes / ref_prims): each triangle carries its reference leaf and lane,
+// so exact-distance ties and the parallel-axis rule follow the reference even
+// when the traversal tree is a different one.
 void CollapseToWide(const SceneGeometry& geo, const std::vector<BinNode>& nodes,
-                    const std::vector<uint32_t>& prim_indices, WideBvh& out);
+                    const std::vector<uint32_t>& prim_indices, const std::vector<BinNode>& ref_nodes,
+                    const std::vector<uint32_t>& ref_prims, WideBvh& out);
 
 }  // namespace vkptc

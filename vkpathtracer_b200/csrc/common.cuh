@@ -134,6 +134,7 @@ struct DevScene {
   float tan_half_fov;
   float aperture, focus;
   uint32_t stack_required;
+  uint32_t reference_tree;   // 1: the traversal tree is the reference's own tree
 };
 
 // Render-wide integrator settings.

@@ -165,6 +165,7 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.aperture = c->cam.aperture > 0.0f ? c->cam.aperture : c->settings.camera_aperture_radius;
   s.focus = c->cam.focus > 0.0f ? c->cam.focus : c->settings.camera_focus_distance;
   s.stack_required = c->wide.stack_required;
+  s.reference_tree = c->wide.reference_topology ? 1u : 0u;
   return s;
 }
 
@@ -208,7 +209,7 @@ int32_t launch_shape(vkptc_ctx* c, cudaStream_t stream, LaunchShape& ls, bool al
   ls.stack_cap = stack_cap(c);
   const int asked = c->config.stack_depth ? static_cast<int>(c->config.stack_depth) : kDefaultSmemEntries;
   ls.smem_entries = allow_spill ? std::min(ls.stack_cap, std::max(1, asked)) : ls.stack_cap;
-  ls.steps = c->config.reserved[2] ? static_cast<int>(c->config.reserved[2]) : kDefaultSteps;
+  ls.steps = c->config.steps ? static_cast<int>(c->config.steps) : kDefaultSteps;
   ls.stream = stream;
   ls.spill = nullptr;
   const int32_t rc = ensure_stack_smem(c, ls);
@@ -300,7 +301,18 @@ int32_t check_device_error(vkptc_ctx* c) {
 
 int32_t upload_accel(vkptc_ctx* c, const std::vector<BinNode>& bin, const std::vector<uint32_t>& prim_indices,
                      double build_ms) {
-  CollapseToWide(c->geo, bin, prim_indices, c->wide);
+  // The reference tree always supplies tie order and the parallel-axis rule;
+  // the traversal tree is either that same tree or a binned-SAH tree.
+  if (c->config.bvh_mode == VKPTC_BVH_SAH) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<BinNode> sah;
+    std::vector<uint32_t> sah_prims;
+    BuildSahBvh(c->geo, 4u, sah, sah_prims);
+    CollapseToWide(c->geo, sah, sah_prims, bin, prim_indices, c->wide);
+    build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  } else {
+    CollapseToWide(c->geo, bin, prim_indices, bin, prim_indices, c->wide);
+  }
   const WideBvh& w = c->wide;
   VKPTC_CUDA(c, c->d_nodes.alloc(std::max<size_t>(1, w.nodes.size() * 8)), "bvh alloc");
   VKPTC_CUDA(c, c->d_tris.alloc(std::max<size_t>(1, w.tris.size() * 3)), "bvh alloc");
@@ -342,7 +354,7 @@ int32_t run_wave(vkptc_ctx* c, const WaveTile& tile, uint32_t frame) {
   if (rc != VKPTC_OK) return rc;
   const DevScene s = dev_scene(c);
   const DevSettings st = dev_settings(c, frame);
-  StageTimer* timer = c->config.reserved[1] ? &c->timer : nullptr;
+  StageTimer* timer = c->config.stage_timing ? &c->timer : nullptr;
   VKPTC_CUDA(c, LaunchWave(s, st, wave_state(c), tile, film_of(c), c->config.math_mode == 0u,
                            c->config.collect_stats != 0u, ls, c->d_ctr.ptr, c->d_err.ptr, timer),
              "wave launch");
@@ -363,7 +375,7 @@ int32_t run_wave(vkptc_ctx* c, const WaveTile& tile, uint32_t frame) {
 constexpr uint32_t kDefaultWavePaths = 1u << 22;
 
 uint32_t wave_paths(const vkptc_ctx* c) {
-  return c->config.reserved[0] ? c->config.reserved[0] : kDefaultWavePaths;
+  return c->config.wave_paths ? c->config.wave_paths : kDefaultWavePaths;
 }
 
 }  // namespace
@@ -392,7 +404,7 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
     return VKPTC_INTERNAL_ERROR;
   }
   c->stream = c->own_stream;
-  if (c->config.reserved[1]) {
+  if (c->config.stage_timing) {
     c->timer_events.resize(2 * 4096);
     for (auto& e : c->timer_events) cudaEventCreate(&e);
     c->timer.events = c->timer_events.data();
@@ -659,7 +671,7 @@ int32_t vkptc_set_stream(vkptc_ctx* ctx, void* stream) {
 
 int32_t vkptc_read_stage_times(vkptc_ctx* ctx, double* ms_out, uint64_t* launches_out) {
   if (!ctx || !ms_out) return VKPTC_INVALID_ARGUMENT;
-  if (!ctx->config.reserved[1]) return fail(ctx, VKPTC_UNSUPPORTED, "stage timing not enabled in vkptc_config");
+  if (!ctx->config.stage_timing) return fail(ctx, VKPTC_UNSUPPORTED, "stage timing not enabled in vkptc_config");
   for (int k = 0; k < StageTimer::kStages; ++k) {
     ms_out[k] = ctx->stage_ms[k];
     if (launches_out) launches_out[k] = ctx->stage_launches[k];
@@ -903,7 +915,7 @@ int32_t batch_run_plain(vkptc_batch* b, const vkptc_batch_tuning& t) {
     c->stream = b->stream;
     if (t.block_size) c->config.block_size = t.block_size;
     if (t.stack_depth) c->config.stack_depth = t.stack_depth;
-    if (t.steps) c->config.reserved[2] = t.steps;
+    if (t.steps) c->config.steps = t.steps;
     const uint32_t spp = job_samples(c, t.sample_limit);
     for (uint32_t sidx = 0; sidx < spp && rc == VKPTC_OK; ++sidx) {
       // One frame per launch sequence: every sample is its own wave.

@@ -290,13 +290,13 @@ __global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveSta
       float remain = o4.w;
       bool visible = true;
       if (!s.has_transmissive) {
-        const RayPrep r = prep_ray(so, sd);
+        const RayPrep r = prep_ray(so, sd, s.reference_tree != 0u);
         visible = !trace_any<kStats>(s, r, remain, stk, st, local_err);
       } else {
         // Closest-hit loop that steps through up to 8 transmissive occluders
         // (src/pathtracer/ScalarCpuPathTracer.cpp:1067-1087).
         for (uint32_t skips = 0; skips < 8u && remain > 0.004f; ++skips) {
-          const RayPrep r = prep_ray(so, sd);
+          const RayPrep r = prep_ray(so, sd, s.reference_tree != 0u);
           float t;
           uint32_t prim;
           trace_closest<kStats>(s, r, stk, t, prim, st, local_err);

@@ -32,23 +32,49 @@ namespace vkptc {
 
 struct RayPrep {
   float ox, oy, oz, dx, dy, dz;
-  float ix, iy, iz;      // 1/d, 0 on parallel axes
+  float ix, iy, iz;      // 1/d (0 on axes the node test treats with the inside rule)
   float nix, niy, niz;   // -o/d (for the fused node test)
-  uint32_t par;          // bit k: axis k is parallel
+  uint32_t par;          // bit k: |d_k| <= 1e-4, the reference's "parallel" axis
+  uint32_t node_par;     // axes the node test handles with the origin-inside-slab rule
+  uint32_t leaf_par;     // axes whose reference rule is applied at the leaf (reference leaf box)
 };
 
-__device__ __forceinline__ RayPrep prep_ray(V3 o, V3 d) {
+// reference_tree: the traversal tree is the reference's own tree, so the
+// reference's parallel-axis rule is applied exactly in every node test (it is
+// monotone under box inclusion).  Otherwise nodes are tested geometrically
+// (an exactly-zero component uses the inside rule, which is then exact) and
+// the rule is applied where it decides the result: a hit on a triangle counts
+// only if the origin lies inside its REFERENCE leaf's slab on those axes.
+__device__ __forceinline__ RayPrep prep_ray(V3 o, V3 d, bool reference_tree = true) {
   RayPrep r;
   r.ox = o.x; r.oy = o.y; r.oz = o.z;
   r.dx = d.x; r.dy = d.y; r.dz = d.z;
   r.par = (fabsf(d.x) <= kEps ? 1u : 0u) | (fabsf(d.y) <= kEps ? 2u : 0u) | (fabsf(d.z) <= kEps ? 4u : 0u);
-  r.ix = (r.par & 1u) ? 0.0f : __fdiv_rn(1.0f, d.x);
-  r.iy = (r.par & 2u) ? 0.0f : __fdiv_rn(1.0f, d.y);
-  r.iz = (r.par & 4u) ? 0.0f : __fdiv_rn(1.0f, d.z);
+  if (reference_tree) {
+    r.node_par = r.par;
+    r.leaf_par = 0u;
+  } else {
+    r.node_par = (fabsf(d.x) < 1e-20f ? 1u : 0u) | (fabsf(d.y) < 1e-20f ? 2u : 0u) | (fabsf(d.z) < 1e-20f ? 4u : 0u);
+    r.leaf_par = r.par;
+  }
+  r.ix = (r.node_par & 1u) ? 0.0f : __fdiv_rn(1.0f, d.x);
+  r.iy = (r.node_par & 2u) ? 0.0f : __fdiv_rn(1.0f, d.y);
+  r.iz = (r.node_par & 4u) ? 0.0f : __fdiv_rn(1.0f, d.z);
   r.nix = -(o.x * r.ix);
   r.niy = -(o.y * r.iy);
   r.niz = -(o.z * r.iz);
   return r;
+}
+
+// The reference's parallel-axis rule for a hit in reference leaf `leaf`.
+__device__ __forceinline__ bool leaf_rule_ok(const float4* tie, uint32_t leaf, const RayPrep& r) {
+  if (r.leaf_par == 0u) return true;
+  const float4 a = __ldg(tie + 2 * leaf);
+  const float4 b = __ldg(tie + 2 * leaf + 1);
+  if ((r.leaf_par & 1u) && (r.ox < a.x || r.ox > b.x)) return false;
+  if ((r.leaf_par & 2u) && (r.oy < a.y || r.oy > b.y)) return false;
+  if ((r.leaf_par & 4u) && (r.oz < a.z || r.oz > b.z)) return false;
+  return true;
 }
 
 // The reference's slab test verbatim (no fusion); returns the entry distance.
@@ -87,18 +113,18 @@ __device__ __forceinline__ bool node_slab(float lx, float hx, float ly, float hy
   float nx = fminf(ax0, ax1), fx = fmaxf(ax0, ax1);
   float ny = fminf(ay0, ay1), fy = fmaxf(ay0, ay1);
   float nz = fminf(az0, az1), fz = fmaxf(az0, az1);
-  if (r.par) {
-    if (r.par & 1u) {
+  if (r.node_par) {
+    if (r.node_par & 1u) {
       const bool in = !(r.ox < lx || r.ox > hx);
       nx = in ? -kInf : kInf;
       fx = kInf;
     }
-    if (r.par & 2u) {
+    if (r.node_par & 2u) {
       const bool in = !(r.oy < ly || r.oy > hy);
       ny = in ? -kInf : kInf;
       fy = kInf;
     }
-    if (r.par & 4u) {
+    if (r.node_par & 4u) {
       const bool in = !(r.oz < lz || r.oz > hz);
       nz = in ? -kInf : kInf;
       fz = kInf;
@@ -268,6 +294,7 @@ __device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& 
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
         const float th = mt_test(a, b, cc, r);
         if (th <= kEps) continue;   // also rejects the -1 miss code
+        if (r.leaf_par != 0u && !leaf_rule_ok(s.tie, __float_as_uint(cc.z), r)) continue;
         if (th < best_t) {
           best_t = th;
           best_prim = __float_as_uint(cc.y);
@@ -346,8 +373,9 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, f
       }
       for (int32_t i = 0; i < count; ++i) {
         const float4* tp = s.tris + 3 * (first + i);
-        const float th = mt_test(__ldg(tp), __ldg(tp + 1), __ldg(tp + 2), r);
-        if (th > kEps && th < tmax) return true;
+        const float4 tc = __ldg(tp + 2);
+        const float th = mt_test(__ldg(tp), __ldg(tp + 1), tc, r);
+        if (th > kEps && th < tmax && (r.leaf_par == 0u || leaf_rule_ok(s.tie, __float_as_uint(tc.z), r))) return true;
       }
     }
     if (sp == 0) break;
@@ -387,9 +415,12 @@ struct GeoView {
   const float4* tris;
   const float4* tie;
   uint32_t prim_count;
+  uint32_t reference_tree;   // 1: traversal tree is the reference tree
 };
 
-__host__ __device__ __forceinline__ GeoView geo_of(const DevScene& s) { return GeoView{s.nodes, s.tris, s.tie, s.prim_count}; }
+__host__ __device__ __forceinline__ GeoView geo_of(const DevScene& s) {
+  return GeoView{s.nodes, s.tris, s.tie, s.prim_count, s.reference_tree};
+}
 
 struct LaneState {
   GeoView g;
@@ -402,7 +433,7 @@ struct LaneState {
 };
 
 __device__ __forceinline__ void lane_begin(LaneState& L, V3 o, V3 d, float tmax, bool any) {
-  L.r = prep_ray(o, d);
+  L.r = prep_ray(o, d, L.g.reference_tree != 0u);
   L.t = any ? tmax : kInf;
   L.prim = any ? 0u : kMiss;
   L.leaf = L.lane = 0u;
@@ -465,6 +496,7 @@ __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk
       const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
       const float th = mt_test(a, b, cc, L.r);
       if (th <= kEps) continue;
+      if (L.r.leaf_par != 0u && !leaf_rule_ok(L.g.tie, __float_as_uint(cc.z), L.r)) continue;
       if (kAny) {
         if (th < L.t) {
           L.prim = 1u;

@@ -21,8 +21,12 @@ QUERY_CLOSEST, QUERY_ANY = 0, 1
 
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
-                ("math_mode", ctypes.c_uint32), ("collect_stats", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 3)]
+                ("math_mode", ctypes.c_uint32), ("collect_stats", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
+                ("stage_timing", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("bvh_mode", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 4)]
+
+
+BVH_REFERENCE, BVH_SAH = 0, 1
 
 
 class RenderSettingsC(ctypes.Structure):

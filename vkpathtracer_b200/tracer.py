@@ -108,7 +108,7 @@ class CudaPathTracer:
 
     def __init__(self, device: int = 0, block_size: int = 0, stack_depth: int = 0, math_mode: int = 0,
                  collect_stats: bool = False, wave_paths: int = 0, stage_timing: bool = False,
-                 steps: int = 0):
+                 steps: int = 0, bvh: str = "reference"):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -116,9 +116,10 @@ class CudaPathTracer:
         cfg.stack_depth = stack_depth
         cfg.math_mode = math_mode
         cfg.collect_stats = int(collect_stats)
-        cfg.reserved[0] = wave_paths
-        cfg.reserved[1] = int(stage_timing)
-        cfg.reserved[2] = steps
+        cfg.wave_paths = wave_paths
+        cfg.stage_timing = int(stage_timing)
+        cfg.steps = steps
+        cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
         handle = ctypes.c_void_p()
         rc = self._lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle))
         if rc != native.OK:
@@ -306,12 +307,13 @@ class BatchRenderer:
     device work queue, replayed from a CUDA graph.  Films are bit-identical.
     """
 
-    def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False):
+    def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False, bvh: str = "reference"):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
         cfg.math_mode = math_mode
         cfg.collect_stats = int(collect_stats)
+        cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
         h = ctypes.c_void_p()
         rc = self._lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != native.OK:
