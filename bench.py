@@ -202,7 +202,7 @@ def full_frame(device):
     sc = scenes.sphere_grid()
     st = scenes.sphere_grid_settings()
     out = {"workload": "sphere_grid_64x64_1080p_64spp_depth16", "triangles": sc.triangle_count}
-    with BatchRenderer(device=device) as b:
+    with BatchRenderer(device=device, bvh="sah") as b:
         b.add_job(sc, st)
         b.run("persistent")
         runs = [b.run("persistent") for _ in range(2)]
@@ -211,7 +211,7 @@ def full_frame(device):
         out["paths_per_s"] = r["paths"] / (ms / 1e3)
         out["mrays_per_s"] = (r["segments"] + r["shadow_rays"]) / (ms / 1e3) / 1e6
         out["ms_per_frame_64spp"] = ms
-    with CudaPathTracer(device=device) as t:
+    with CudaPathTracer(device=device, bvh="sah") as t:
         t.configure(st)
         t.load_scene_snapshot(sc)
         t.build_or_update_acceleration()
@@ -236,7 +236,7 @@ def ray_query(device):
     n = rays.shape[0]
     out = {"workload": "displaced_sphere_1046904_tris_8388608_rays"}
     s = torch.cuda.Stream()
-    with CudaPathTracer(device=device) as t:
+    with CudaPathTracer(device=device, bvh="sah") as t:
         t.configure(scenes.RenderSettings(width=8, height=8, spp=1))
         t.load_scene_snapshot(sc)
         t.build_or_update_acceleration()
@@ -270,7 +270,7 @@ def run_ours(args, world, rank, local):
     # Each rank renders its own replica of the job set (disjoint seeds).
     jobs = make_jobs(args.jobs, seed=5 + 1000 * rank)
     total_paths = sum(j.settings.width * j.settings.height * j.settings.spp for j in jobs)
-    b = BatchRenderer(device=local)
+    b = BatchRenderer(device=local, bvh="sah")
     t0 = time.time()
     for j in jobs:
         b.add_job(j.scene, j.settings)
@@ -319,7 +319,7 @@ def run_ours(args, world, rank, local):
     roof = rq = ff = cpu = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the persistent kernel
-        with BatchRenderer(device=local, collect_stats=True) as bs:
+        with BatchRenderer(device=local, collect_stats=True, bvh="sah") as bs:
             for j in jobs:
                 bs.add_job(j.scene, j.settings)
             ss = bs.run("persistent", **tuning)
@@ -354,7 +354,8 @@ def run_ours(args, world, rank, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
                 "config": {"workload": WORKLOAD, "jobs": len(jobs), "paths_per_step": total_paths,
                            "triangles": sum(j.scene.triangle_count for j in jobs),
-                           "setup_s": setup_s, "tuning": tuning, "autotune": {k: tune.get(k) for k in
+                           "setup_s": setup_s, "bvh": "sah traversal tree (hit ids exact: ties and parallel-axis "
+                                                    "rule through the reference tree)", "tuning": tuning, "autotune": {k: tune.get(k) for k in
                                                                               ("ms", "trials", "cached")},
                            "l2": "inputs larger than L2 (all scenes, BVHs and the path pool resident in HBM)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
