@@ -342,6 +342,74 @@ const char* vkptc_batch_last_error(vkptc_batch* batch);
 int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* tile, uint32_t frame, float* d_film_sum,
                                   uint32_t* d_film_count, void* stream);
 
+/* ---- differentiable rendering (forward / backward pair) -------------------
+ * No counterpart in the reference: its tracer has no derivative path.
+ *
+ * Parameters are VKPTC_ADJ_PARAMS_PER_MATERIAL floats per scene material, in
+ * material order: albedo r, g, b, roughness, emission r, g, b.  They replace
+ * those words of the loaded materials for the forward and backward only (the
+ * context's own renderer keeps the loaded scene).
+ *
+ * vkptc_forward renders desc->spp samples (from desc->first_sample, RNG frame
+ * desc->frame) of every pixel, one path per thread, forms the image exactly
+ * as the film does (sample order, non-finite samples dropped) and returns
+ * the loss L = mean over pixels and channels of (image - target)^2, reduced
+ * in FP64.  rr_params (NULL = params) are the parameters whose throughput
+ * sets the Russian-roulette probabilities and decisions: passing the
+ * unperturbed vector makes a finite difference use the same roulette as
+ * the derivative.  image_rgb (W*H*3, optional) receives the image.
+ *
+ * vkptc_backward returns dL/dparams for the last forward: every path is
+ * replayed from its RNG key and swept in reverse.  The estimator
+ * differentiated: Phong-lobe directions are reparameterized (they move with
+ * roughness and with the incoming direction), the roulette probability is
+ * held constant, and every discrete decision (hits, visibility, lobe
+ * fallbacks) is the forward's, so visibility-boundary terms are excluded.
+ * Emission gradients are meaningful for emissive materials (and for
+ * surfaces seen directly by the camera).
+ *
+ * Supported: materials of models 0, 1 and 3 with metallic <= 0.65,
+ * transmission <= 0.05, clearcoat <= 0.05 and roughness > 0.001 (Lambertian
+ * and Phong-lobe glossy, optionally emissive), at most
+ * VKPTC_ADJ_MAX_MATERIALS materials, max_depth <= VKPTC_ADJ_MAX_DEPTH;
+ * anything else returns VKPTC_UNSUPPORTED.  All three calls are synchronous
+ * on the context's stream. */
+#define VKPTC_ADJ_PARAMS_PER_MATERIAL 7u
+#define VKPTC_ADJ_MAX_MATERIALS 64u
+#define VKPTC_ADJ_MAX_DEPTH 8u
+typedef struct vkptc_adjoint_desc {
+  uint32_t spp;
+  uint32_t first_sample;
+  uint32_t frame;
+  uint32_t reserved[5];
+} vkptc_adjoint_desc;
+
+typedef struct vkptc_adjoint_stats {
+  uint64_t paths;           /* paths per forward (= per backward) */
+  uint64_t forwards, backwards;
+  double forward_ms;        /* device time of the last forward (render + loss) */
+  double backward_ms;       /* device time of the last backward (replay + sweep + reduction) */
+  uint32_t forward_grid, backward_grid, block, reserved;
+} vkptc_adjoint_stats;
+
+/* target_rgb: W*H*3 floats (NULL: no target; the loss is 0 and so is the gradient). */
+int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, const float* target_rgb,
+                            uint64_t target_floats);
+int32_t vkptc_forward(vkptc_ctx* ctx, const float* params, uint32_t param_count, const float* rr_params,
+                      double* loss, float* image_rgb);
+int32_t vkptc_backward(vkptc_ctx* ctx, float* grad, uint32_t param_count);
+/* As vkptc_backward with each path's adjoint scaled by path_weight[path]
+ * (paths in the order of vkptc_adjoint_read_samples; NULL = all 1). */
+int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float* grad, uint32_t param_count);
+/* Per-path results of the last forward, path = sample_offset * W*H + y*W + x:
+ * rgb (paths*3 floats, optional) the radiance; signature (paths, optional) a
+ * 32-bit hash of the path's discrete decisions (hit primitives, visibility,
+ * lobe fallbacks, termination): equal hashes under two parameter vectors mean
+ * the path took the same branches, which finite-difference checks use to
+ * leave out paths that crossed a discontinuity. */
+int32_t vkptc_adjoint_read_samples(vkptc_ctx* ctx, float* rgb, uint32_t* signature);
+int32_t vkptc_adjoint_get_stats(vkptc_ctx* ctx, vkptc_adjoint_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

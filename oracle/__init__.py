@@ -4,6 +4,10 @@ Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl
 reference legs may import this package, and only as the checker or the CPU
 baseline.  The product package (vkpathtracer_b200) never imports it.
 
+The FP64 adjoint (oracle/adjoint.cpp -> oracle/_build/libvkptadj.so,
+oracle/vkpt_adjoint.h) is the checker of the GPU forward/backward pair;
+load_adjoint() returns it.
+
 Two interchangeable implementations of oracle/vkpt_oracle.h:
   "reference"  oracle/_ref/libvkptref.so   -- the reference's own CPU tracer,
                compiled from its unmodified sources by oracle/Makefile.
@@ -22,6 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libvkptref.so")
 PORT_LIB = os.path.join(HERE, "_build", "libvkptport.so")
+ADJ_LIB = os.path.join(HERE, "_build", "libvkptadj.so")
 REFERENCE_SRC = "/root/reference/src"
 
 
@@ -220,3 +225,83 @@ def load(kind: str = "auto") -> Oracle:
 
 def have_reference() -> bool:
     return os.path.exists(REF_LIB)
+
+
+def build_adjoint(quiet: bool = True) -> str:
+    """Compile the FP64 adjoint with g++ (no reference sources needed)."""
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    deps = [os.path.join(HERE, f) for f in ("adjoint.cpp", "vkpt_adjoint.h", "vkpt_oracle.h")]
+    if (not os.path.exists(ADJ_LIB)) or os.path.getmtime(ADJ_LIB) < max(os.path.getmtime(d) for d in deps):
+        cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-o", ADJ_LIB, deps[0], "-lpthread"]
+        subprocess.run(cmd, check=True, capture_output=quiet)
+    return ADJ_LIB
+
+
+class VkoAdjointRequest(ctypes.Structure):
+    _fields_ = [("params", ctypes.c_void_p), ("param_count", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("first_sample", ctypes.c_uint32), ("frame", ctypes.c_uint32), ("target", ctypes.c_void_p),
+                ("grad_index", ctypes.c_void_p), ("grad_count", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+                ("rr_params", ctypes.c_void_p)]
+
+
+class AdjointOracle:
+    """FP64 forward-mode adjoint of the render path (checker only)."""
+
+    def __init__(self, path: str):
+        self.lib = ctypes.CDLL(path)
+        self.lib.vko_adjoint.restype = ctypes.c_int
+        self.lib.vko_adjoint.argtypes = [ctypes.POINTER(VkoScene), ctypes.POINTER(VkoSettings),
+                                         ctypes.POINTER(VkoAdjointRequest), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.c_void_p, ctypes.c_void_p]
+        self.lib.vko_adjoint_last_error.restype = ctypes.c_char_p
+        self.lib.vko_adjoint_fd.restype = ctypes.c_int
+        self.lib.vko_adjoint_fd.argtypes = [ctypes.POINTER(VkoScene), ctypes.POINTER(VkoSettings),
+                                            ctypes.POINTER(VkoAdjointRequest), ctypes.c_double, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+
+    def finite_difference(self, scene, settings, params: np.ndarray, target: np.ndarray, spp: int, grad_index,
+                          h: float = 1e-3, threads: int = 1, frame: int = 0, first_sample: int = 0):
+        """Flip-excluding central differences (see vko_adjoint_fd): returns (fd, flips)."""
+        sc, keep = Oracle.make_scene(scene)
+        st = Oracle.make_settings(settings)
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        tg = np.ascontiguousarray(target, np.float32).reshape(-1)
+        gi = np.ascontiguousarray(grad_index, np.uint32).reshape(-1)
+        fd = np.zeros(max(1, gi.size), np.float64)
+        flips = np.zeros(max(1, gi.size), np.uint64)
+        rq = VkoAdjointRequest(_ptr(p), p.size, spp, first_sample, frame, _ptr(tg), _ptr(gi), gi.size, threads, None)
+        rc = self.lib.vko_adjoint_fd(ctypes.byref(sc), ctypes.byref(st), ctypes.byref(rq), h, _ptr(fd), _ptr(flips))
+        del keep
+        if rc != 0:
+            raise RuntimeError(f"adjoint oracle failed: {self.lib.vko_adjoint_last_error().decode()}")
+        return fd[:gi.size], flips[:gi.size]
+
+    def run(self, scene, settings, params: np.ndarray, target: Optional[np.ndarray], spp: int,
+            grad_index, threads: int = 1, frame: int = 0, first_sample: int = 0,
+            rr_params: Optional[np.ndarray] = None):
+        """Returns (loss, grad[len(grad_index)], image (H, W, 3) float64)."""
+        sc, keep = Oracle.make_scene(scene)
+        st = Oracle.make_settings(settings)
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        tg = None if target is None else np.ascontiguousarray(target, np.float32).reshape(-1)
+        gi = np.ascontiguousarray(grad_index, np.uint32).reshape(-1)
+        grad = np.zeros(max(1, gi.size), np.float64)
+        img = np.zeros((settings.height, settings.width, 3), np.float64)
+        rp = None if rr_params is None else np.ascontiguousarray(rr_params, np.float32).reshape(-1)
+        if rp is not None and rp.size != p.size:
+            raise ValueError("rr_params must have the shape of params")
+        rq = VkoAdjointRequest(_ptr(p), p.size, spp, first_sample, frame, _ptr(tg), _ptr(gi) if gi.size else None,
+                               gi.size, threads, _ptr(rp))
+        loss = ctypes.c_double(0.0)
+        rc = self.lib.vko_adjoint(ctypes.byref(sc), ctypes.byref(st), ctypes.byref(rq), ctypes.byref(loss),
+                                  _ptr(grad), _ptr(img))
+        del keep
+        if rc != 0:
+            raise RuntimeError(f"adjoint oracle failed: {self.lib.vko_adjoint_last_error().decode()}")
+        return loss.value, grad[:gi.size], img
+
+
+def load_adjoint() -> AdjointOracle:
+    if "adjoint" not in _CACHE:
+        _CACHE["adjoint"] = AdjointOracle(build_adjoint())
+    return _CACHE["adjoint"]

@@ -1,0 +1,47 @@
+// adjoint_launch.h -- launch interface of the differentiable-rendering kernels
+// (adjoint.cu).  One forward renders `spp` samples of every pixel with one
+// path per thread and keeps each sample's radiance; the loss kernel forms the
+// image, the mean-squared-error loss (FP64 reduction) and the per-pixel
+// adjoint; the backward replays every path from its RNG key and runs the
+// reverse sweep over its vertices.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace vkptc {
+
+struct AdjLaunch {
+  int grid, block;
+  int stack_cap;          // traversal stack entries per thread (all in shared memory)
+  uint32_t spp, first_sample;
+  bool parity;
+  cudaStream_t stream;
+};
+
+// Path radiance of every (sample, pixel): rad[s * W*H + y*W + x] = rgb, and
+// in w the bits of a 32-bit hash of the path's discrete decisions.
+// mat0 (16 floats per material) drives the Russian-roulette probabilities
+// and decisions; pass the scene's own table for the ordinary estimator.
+cudaError_t LaunchAdjForward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
+                             float4* rad, uint32_t* err);
+
+// Image (sample-order accumulation exactly as the film does), loss partials
+// per block, and the per-pixel adjoint dL/d(sample radiance) (0 without a target).
+cudaError_t LaunchAdjLoss(const DevSettings& st, uint32_t spp, const float4* rad, const float* target, float* image,
+                          float4* adj, double* loss_part, double* loss, int grid, cudaStream_t stream);
+
+// Reverse sweep: per-block gradient partials grad_part[block][7 * materials],
+// then the fixed-order reduction into grad (7 floats per material).
+// path_weight (optional, one per path) scales each path's adjoint.
+cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
+                              const float4* rad, const float4* adj, const float* path_weight, float* grad_part,
+                              float* grad, uint32_t* err);
+
+size_t AdjBackwardSmem(int block, int stack_cap, uint32_t materials);
+size_t AdjForwardSmem(int block, int stack_cap);
+int AdjBlocksPerSm(bool backward, int block, size_t smem, bool parity);
+cudaError_t ConfigureAdjSmem(size_t bytes);
+
+}  // namespace vkptc

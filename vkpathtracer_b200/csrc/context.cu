@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/vkptc.h"
+#include "adjoint_launch.h"
 #include "bvh_host.h"
 #include "batch.cuh"
 #include "kernels.cuh"
@@ -51,6 +52,28 @@ struct DevBuf {
 struct HostCamera {
   float pos[3], target[3], up[3];
   float fov, aperture, focus;
+};
+
+// Differentiable-rendering state of a context (vkptc_forward / vkptc_backward).
+struct AdjointState {
+  bool setup = false, forward_done = false, has_target = false;
+  vkptc_adjoint_desc desc{};
+  uint32_t width = 0, height = 0;
+  std::vector<float> host_mat, host_mat0;   // 16 floats per material: params / roulette params applied
+  DevBuf<float> mat, mat0;                 // device copies of the two tables
+  DevBuf<float4> rad;                      // per-sample radiance of the last forward
+  DevBuf<float4> adj;                      // per-pixel adjoint of a sample's radiance
+  DevBuf<float> target, image;
+  DevBuf<double> loss_part, loss;
+  DevBuf<float> grad_part, grad;
+  DevBuf<float> path_weight;
+  int loss_grid = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  vkptc_adjoint_stats stats{};
+  ~AdjointState() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 }  // namespace
@@ -107,6 +130,8 @@ struct vkptc_ctx {
   // ray-query scratch for host-buffer calls
   DevBuf<float> q_rays, q_tmax, q_t;
   DevBuf<uint32_t> q_prim;
+
+  AdjointState adj;
 };
 
 namespace {
@@ -451,6 +476,7 @@ int32_t vkptc_configure(vkptc_ctx* ctx, const vkptc_render_settings* settings) {
   ctx->configured = true;
   ctx->has_scene = false;
   ctx->accel_valid = false;
+  ctx->adj.setup = false;
   ctx->current_sample = 0;
   ctx->accumulation_gen = 0;
   ctx->last_error.clear();
@@ -469,6 +495,7 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
     const uint32_t effect = static_cast<uint32_t>(scene->materials[16 * i + 15] + 0.5f) & 1023u;
     if (effect != 0u) return fail(ctx, VKPTC_UNSUPPORTED, "procedural material effects (effect != 0) are not supported");
   }
+  ctx->adj.setup = false;
   cudaSetDevice(ctx->device);
   std::string err;
   SceneGeometry geo;
@@ -600,6 +627,7 @@ int32_t vkptc_shutdown(vkptc_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->configured = ctx->has_scene = ctx->accel_valid = false;
+  ctx->adj.setup = false;
   ctx->geo = SceneGeometry{};
   ctx->wide = WideBvh{};
   ctx->d_nodes.release();
@@ -1332,3 +1360,258 @@ extern "C" int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* t
   ctx->last_error.clear();
   return VKPTC_OK;
 }
+
+// ============================================================ adjoint
+namespace {
+
+// The supported material subset (Lambertian / Phong-lobe glossy, optionally
+// emissive); returns an empty string when material m qualifies.
+std::string adjoint_material_issue(const float* m, size_t i) {
+  const uint32_t model = static_cast<uint32_t>(m[7] + 0.5f);
+  const float rough = std::isfinite(m[6]) ? std::min(1.0f, std::max(0.0f, m[6])) : 0.0f;
+  std::string why;
+  if (model != 0u && model != 1u && model != 3u) why = "model " + std::to_string(model);
+  else if (m[8] > 0.65f) why = "metallic";
+  else if (m[10] > 0.05f) why = "transmissive";
+  else if (m[11] > 0.05f) why = "clear coat";
+  else if (rough <= 0.001f) why = "mirror (roughness <= 0.001)";
+  if (why.empty()) return why;
+  return "material " + std::to_string(i) + " is " + why + "; the adjoint supports Lambertian and Phong-lobe glossy "
+         "materials (models 0, 1, 3) only";
+}
+
+// Material table with the 7 parameters of each material substituted.
+void apply_params(const std::vector<float>& base, const float* params, std::vector<float>& out) {
+  out = base;
+  const size_t n = base.size() / 16;
+  for (size_t i = 0; i < n; ++i) {
+    const float* p = params + VKPTC_ADJ_PARAMS_PER_MATERIAL * i;
+    float* m = &out[16 * i];
+    m[0] = p[0];
+    m[1] = p[1];
+    m[2] = p[2];
+    m[6] = p[3];
+    m[3] = p[4];
+    m[4] = p[5];
+    m[5] = p[6];
+  }
+}
+
+AdjLaunch adj_launch(vkptc_ctx* c, bool backward, int32_t& rc) {
+  AdjLaunch l{};
+  rc = VKPTC_OK;
+  l.block = 128;
+  l.stack_cap = stack_cap(c);
+  l.spp = c->adj.desc.spp;
+  l.first_sample = c->adj.desc.first_sample;
+  l.parity = c->config.math_mode == 0u;
+  l.stream = c->stream;
+  const uint32_t mats = static_cast<uint32_t>(c->materials.size() / 16);
+  const size_t smem = backward ? AdjBackwardSmem(l.block, l.stack_cap, mats) : AdjForwardSmem(l.block, l.stack_cap);
+  int max_optin = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if (smem > static_cast<size_t>(max_optin)) {
+    rc = fail(c, VKPTC_UNSUPPORTED, "adjoint: traversal stack and gradient slots do not fit in shared memory");
+    return l;
+  }
+  if (smem > 48 * 1024) {
+    const cudaError_t e = ConfigureAdjSmem(smem);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(c, e, "adjoint shared memory limit");
+      return l;
+    }
+  }
+  l.grid = c->sm_count * AdjBlocksPerSm(backward, l.block, smem, l.parity);
+  return l;
+}
+
+DevScene adj_scene(vkptc_ctx* c) {
+  DevScene s = dev_scene(c);
+  s.materials = c->adj.mat.ptr;
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, const float* target_rgb,
+                            uint64_t target_floats) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!desc) return fail(ctx, VKPTC_INVALID_ARGUMENT, "desc is null");
+  if (!ctx->configured || !ctx->has_scene || !ctx->accel_valid) {
+    return fail(ctx, VKPTC_NOT_READY, "adjoint requires a configured tracer with a scene and a built acceleration structure");
+  }
+  if (desc->spp == 0u) return fail(ctx, VKPTC_INVALID_ARGUMENT, "spp must be positive");
+  if (ctx->settings.max_depth > VKPTC_ADJ_MAX_DEPTH) {
+    return fail(ctx, VKPTC_UNSUPPORTED, "adjoint supports max_depth <= " + std::to_string(VKPTC_ADJ_MAX_DEPTH));
+  }
+  const size_t mats = ctx->materials.size() / 16;
+  if (mats > VKPTC_ADJ_MAX_MATERIALS) {
+    return fail(ctx, VKPTC_UNSUPPORTED, "adjoint supports at most " + std::to_string(VKPTC_ADJ_MAX_MATERIALS) + " materials");
+  }
+  for (size_t i = 0; i < mats; ++i) {
+    const std::string why = adjoint_material_issue(&ctx->materials[16 * i], i);
+    if (!why.empty()) return fail(ctx, VKPTC_UNSUPPORTED, why);
+  }
+  if (ctx->has_transmissive) return fail(ctx, VKPTC_UNSUPPORTED, "adjoint: transmissive materials are not supported");
+  const uint64_t npx = static_cast<uint64_t>(ctx->settings.width) * ctx->settings.height;
+  if (npx == 0) return fail(ctx, VKPTC_INVALID_ARGUMENT, "empty film");
+  if (target_rgb && target_floats != 3 * npx) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "target must hold W*H*3 floats");
+  }
+  const uint64_t paths = npx * desc->spp;
+  if (paths > (1ull << 31)) return fail(ctx, VKPTC_INVALID_ARGUMENT, "more than 2^31 paths per forward");
+  cudaSetDevice(ctx->device);
+  AdjointState& a = ctx->adj;
+  VKPTC_CUDA(ctx, a.rad.alloc(paths), "adjoint radiance alloc");
+  VKPTC_CUDA(ctx, a.adj.alloc(npx), "adjoint alloc");
+  VKPTC_CUDA(ctx, a.image.alloc(3 * npx), "adjoint image alloc");
+  VKPTC_CUDA(ctx, a.mat.alloc(ctx->materials.size()), "adjoint material alloc");
+  VKPTC_CUDA(ctx, a.mat0.alloc(ctx->materials.size()), "adjoint material alloc");
+  a.loss_grid = static_cast<int>(std::min<uint64_t>(1024, (npx + 255) / 256));
+  VKPTC_CUDA(ctx, a.loss_part.alloc(a.loss_grid), "adjoint loss alloc");
+  VKPTC_CUDA(ctx, a.loss.alloc(1), "adjoint loss alloc");
+  if (target_rgb) {
+    VKPTC_CUDA(ctx, a.target.alloc(3 * npx), "adjoint target alloc");
+    VKPTC_CUDA(ctx, cudaMemcpy(a.target.ptr, target_rgb, 3 * npx * sizeof(float), cudaMemcpyHostToDevice), "target upload");
+  }
+  for (auto& e : a.ev)
+    if (!e) VKPTC_CUDA(ctx, cudaEventCreate(&e), "adjoint events");
+  a.desc = *desc;
+  a.width = ctx->settings.width;
+  a.height = ctx->settings.height;
+  a.has_target = target_rgb != nullptr;
+  a.setup = true;
+  a.forward_done = false;
+  a.stats = vkptc_adjoint_stats{};
+  a.stats.paths = paths;
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_forward(vkptc_ctx* ctx, const float* params, uint32_t param_count, const float* rr_params, double* loss,
+                      float* image_rgb) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  AdjointState& a = ctx->adj;
+  if (!a.setup || a.width != ctx->settings.width || a.height != ctx->settings.height || !ctx->accel_valid) {
+    return fail(ctx, VKPTC_NOT_READY, "vkptc_adjoint_setup must run (again) before vkptc_forward");
+  }
+  const size_t mats = ctx->materials.size() / 16;
+  if (!params || param_count != VKPTC_ADJ_PARAMS_PER_MATERIAL * mats) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "params must hold 7 floats per material (" +
+                                                 std::to_string(VKPTC_ADJ_PARAMS_PER_MATERIAL * mats) + ")");
+  }
+  apply_params(ctx->materials, params, a.host_mat);
+  apply_params(ctx->materials, rr_params ? rr_params : params, a.host_mat0);
+  for (size_t i = 0; i < mats; ++i) {
+    const std::string why = adjoint_material_issue(&a.host_mat[16 * i], i);
+    if (!why.empty()) return fail(ctx, VKPTC_UNSUPPORTED, why);
+  }
+  cudaSetDevice(ctx->device);
+  const size_t bytes = a.host_mat.size() * sizeof(float);
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(a.mat.ptr, a.host_mat.data(), bytes, cudaMemcpyHostToDevice, ctx->stream), "params upload");
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(a.mat0.ptr, a.host_mat0.data(), bytes, cudaMemcpyHostToDevice, ctx->stream), "params upload");
+  int32_t rc = VKPTC_OK;
+  const AdjLaunch l = adj_launch(ctx, false, rc);
+  if (rc != VKPTC_OK) return rc;
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_err.ptr, 0, sizeof(uint32_t), ctx->stream), "error clear");
+  const DevSettings st = dev_settings(ctx, a.desc.frame);
+  VKPTC_CUDA(ctx, cudaEventRecord(a.ev[0], ctx->stream), "event");
+  VKPTC_CUDA(ctx, LaunchAdjForward(adj_scene(ctx), st, a.mat0.ptr, l, a.rad.ptr, ctx->d_err.ptr), "adjoint forward launch");
+  VKPTC_CUDA(ctx, LaunchAdjLoss(st, a.desc.spp, a.rad.ptr, a.has_target ? a.target.ptr : nullptr, a.image.ptr, a.adj.ptr,
+                                a.loss_part.ptr, a.loss.ptr, a.loss_grid, ctx->stream),
+             "adjoint loss launch");
+  VKPTC_CUDA(ctx, cudaEventRecord(a.ev[1], ctx->stream), "event");
+  double host_loss = 0.0;
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(&host_loss, a.loss.ptr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "loss readback");
+  if (image_rgb) {
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(image_rgb, a.image.ptr, a.image.count * sizeof(float), cudaMemcpyDeviceToHost,
+                                    ctx->stream), "image readback");
+  }
+  rc = check_device_error(ctx);
+  if (rc != VKPTC_OK) return rc;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, a.ev[0], a.ev[1]);
+  a.stats.forward_ms = ms;
+  a.stats.forwards++;
+  a.stats.forward_grid = static_cast<uint32_t>(l.grid);
+  a.stats.block = static_cast<uint32_t>(l.block);
+  if (loss) *loss = host_loss;
+  a.forward_done = true;
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_backward(vkptc_ctx* ctx, float* grad, uint32_t param_count) {
+  return vkptc_backward_weighted(ctx, nullptr, grad, param_count);
+}
+
+int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float* grad, uint32_t param_count) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  AdjointState& a = ctx->adj;
+  if (!a.setup || !a.forward_done || !ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "vkptc_backward needs a vkptc_forward first");
+  const size_t mats = ctx->materials.size() / 16;
+  const size_t stride = VKPTC_ADJ_PARAMS_PER_MATERIAL * mats;
+  if (!grad || param_count != stride) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "grad must hold 7 floats per material (" + std::to_string(stride) + ")");
+  }
+  cudaSetDevice(ctx->device);
+  int32_t rc = VKPTC_OK;
+  const AdjLaunch l = adj_launch(ctx, true, rc);
+  if (rc != VKPTC_OK) return rc;
+  VKPTC_CUDA(ctx, a.grad_part.alloc(static_cast<size_t>(l.grid) * stride), "gradient partials alloc");
+  VKPTC_CUDA(ctx, a.grad.alloc(stride), "gradient alloc");
+  if (path_weight) {
+    VKPTC_CUDA(ctx, a.path_weight.alloc(a.stats.paths), "path weight alloc");
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(a.path_weight.ptr, path_weight, a.stats.paths * sizeof(float), cudaMemcpyHostToDevice,
+                                    ctx->stream), "path weight upload");
+  }
+  VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_err.ptr, 0, sizeof(uint32_t), ctx->stream), "error clear");
+  VKPTC_CUDA(ctx, cudaEventRecord(a.ev[2], ctx->stream), "event");
+  VKPTC_CUDA(ctx, LaunchAdjBackward(adj_scene(ctx), dev_settings(ctx, a.desc.frame), a.mat0.ptr, l, a.rad.ptr, a.adj.ptr,
+                                    path_weight ? a.path_weight.ptr : nullptr, a.grad_part.ptr, a.grad.ptr,
+                                    ctx->d_err.ptr),
+             "adjoint backward launch");
+  VKPTC_CUDA(ctx, cudaEventRecord(a.ev[3], ctx->stream), "event");
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(grad, a.grad.ptr, stride * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
+             "gradient readback");
+  rc = check_device_error(ctx);
+  if (rc != VKPTC_OK) return rc;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, a.ev[2], a.ev[3]);
+  a.stats.backward_ms = ms;
+  a.stats.backwards++;
+  a.stats.backward_grid = static_cast<uint32_t>(l.grid);
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_adjoint_read_samples(vkptc_ctx* ctx, float* rgb, uint32_t* signature) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  AdjointState& a = ctx->adj;
+  if (!a.setup || !a.forward_done) return fail(ctx, VKPTC_NOT_READY, "no forward to read");
+  if (!rgb && !signature) return VKPTC_OK;
+  cudaSetDevice(ctx->device);
+  std::vector<float4> host(a.stats.paths);
+  VKPTC_CUDA(ctx, cudaMemcpy(host.data(), a.rad.ptr, host.size() * sizeof(float4), cudaMemcpyDeviceToHost),
+             "sample readback");
+  for (size_t j = 0; j < host.size(); ++j) {
+    if (rgb) {
+      rgb[3 * j + 0] = host[j].x;
+      rgb[3 * j + 1] = host[j].y;
+      rgb[3 * j + 2] = host[j].z;
+    }
+    if (signature) std::memcpy(&signature[j], &host[j].w, sizeof(uint32_t));
+  }
+  return VKPTC_OK;
+}
+
+int32_t vkptc_adjoint_get_stats(vkptc_ctx* ctx, vkptc_adjoint_stats* out) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!out) return fail(ctx, VKPTC_INVALID_ARGUMENT, "out is null");
+  *out = ctx->adj.stats;
+  return VKPTC_OK;
+}
+
+}  // extern "C"

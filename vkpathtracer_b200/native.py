@@ -108,6 +108,25 @@ class BatchStats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
 
 
+class AdjointDesc(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_uint32), ("first_sample", ctypes.c_uint32), ("frame", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 5)]
+
+
+class AdjointStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_uint64), ("forwards", ctypes.c_uint64), ("backwards", ctypes.c_uint64),
+                ("forward_ms", ctypes.c_double), ("backward_ms", ctypes.c_double),
+                ("forward_grid", ctypes.c_uint32), ("backward_grid", ctypes.c_uint32), ("block", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
+ADJ_PARAMS_PER_MATERIAL = 7
+ADJ_MAX_MATERIALS = 64
+ADJ_MAX_DEPTH = 8
+
 P = ctypes.c_void_p
 U32, U64, I32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
 
@@ -146,6 +165,12 @@ SIGNATURES = {
     "vkptc_batch_read_film": (I32, [P, U32, P, P]),
     "vkptc_batch_get_stats": (I32, [P, ctypes.POINTER(BatchStats)]),
     "vkptc_batch_last_error": (ctypes.c_char_p, [P]),
+    "vkptc_adjoint_setup": (I32, [P, ctypes.POINTER(AdjointDesc), P, U64]),
+    "vkptc_forward": (I32, [P, P, U32, P, ctypes.POINTER(ctypes.c_double), P]),
+    "vkptc_backward": (I32, [P, P, U32]),
+    "vkptc_backward_weighted": (I32, [P, P, P, U32]),
+    "vkptc_adjoint_read_samples": (I32, [P, P, P]),
+    "vkptc_adjoint_get_stats": (I32, [P, ctypes.POINTER(AdjointStats)]),
 }
 BATCH_PLAIN, BATCH_PERSISTENT = 0, 1
 NOALLOC_MAX_PATHS = 65536

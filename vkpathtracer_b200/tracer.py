@@ -127,6 +127,7 @@ class CudaPathTracer:
         self._ctx = handle
         self._settings: Optional[RenderSettings] = None
         self._keep = None
+        self._material_count = 0
 
     # ------------------------------------------------------------ plumbing
     def _err(self) -> str:
@@ -166,7 +167,10 @@ class CudaPathTracer:
 
     def load_scene_snapshot(self, scene: Scene) -> Status:
         v, keep = scene_view(scene)
-        return self._status(self._lib.vkptc_load_scene(self._ctx, ctypes.byref(v)))
+        st = self._status(self._lib.vkptc_load_scene(self._ctx, ctypes.byref(v)))
+        if st.ok:
+            self._material_count = max(1, int(np.asarray(scene.materials).reshape(-1, 16).shape[0]))
+        return st
 
     def build_or_update_acceleration(self) -> Status:
         return self._status(self._lib.vkptc_build_acceleration(self._ctx))
@@ -297,6 +301,63 @@ class CudaPathTracer:
         """Device-pointer variant (e.g. torch tensors' data_ptr()); enqueued, not synchronised."""
         self._check(self._lib.vkptc_trace_rays_device(self._ctx, d_rays, d_tmax or None, n, mode, d_prim,
                                                       d_t or None, stream or None))
+
+
+    # ------------------------------------------------ differentiable rendering
+    def adjoint_setup(self, spp: int, target: Optional[np.ndarray] = None, frame: int = 0, first_sample: int = 0):
+        """Prepares vkptc_forward / vkptc_backward: spp samples per pixel, MSE
+        loss against target (H, W, 3) float32, or no target."""
+        d = native.AdjointDesc()
+        d.spp, d.first_sample, d.frame = spp, first_sample, frame
+        tg = None if target is None else np.ascontiguousarray(target, np.float32).reshape(-1)
+        self._check(self._lib.vkptc_adjoint_setup(self._ctx, ctypes.byref(d), _ptr(tg), 0 if tg is None else tg.size))
+        self._adj_spp = spp
+
+    def forward(self, params: np.ndarray, rr_params: Optional[np.ndarray] = None, image: bool = False):
+        """params: (materials, 7) albedo rgb, roughness, emission rgb.  Returns
+        the loss (FP64), and the (H, W, 3) image when image=True."""
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        rp = None if rr_params is None else np.ascontiguousarray(rr_params, np.float32).reshape(-1)
+        if rp is not None and rp.size != p.size:
+            raise ValueError("rr_params must have the shape of params")
+        loss = ctypes.c_double(0.0)
+        img = np.zeros((self._settings.height, self._settings.width, 3), np.float32) if image else None
+        self._check(self._lib.vkptc_forward(self._ctx, _ptr(p), p.size, _ptr(rp), ctypes.byref(loss), _ptr(img)))
+        return (loss.value, img) if image else loss.value
+
+    def backward(self, path_weight: Optional[np.ndarray] = None) -> np.ndarray:
+        """dL/dparams of the last forward, shape (materials, 7).  path_weight
+        (optional, one float per path) scales each path's contribution."""
+        n = self._material_count * native.ADJ_PARAMS_PER_MATERIAL
+        g = np.zeros(n, np.float32)
+        if path_weight is None:
+            self._check(self._lib.vkptc_backward(self._ctx, _ptr(g), n))
+        else:
+            pw = np.ascontiguousarray(path_weight, np.float32).reshape(-1)
+            if pw.size != self._settings.width * self._settings.height * self._adj_spp:
+                raise ValueError("path_weight must hold one float per path")
+            self._check(self._lib.vkptc_backward_weighted(self._ctx, _ptr(pw), _ptr(g), n))
+        return g.reshape(-1, native.ADJ_PARAMS_PER_MATERIAL)
+
+    def adjoint_samples(self):
+        """(rgb (spp, H, W, 3), signature (spp, H, W) uint32) of the last forward."""
+        W, H, n = self._settings.width, self._settings.height, self._adj_spp
+        rgb = np.zeros((n, H, W, 3), np.float32)
+        sig = np.zeros((n, H, W), np.uint32)
+        self._check(self._lib.vkptc_adjoint_read_samples(self._ctx, _ptr(rgb), _ptr(sig)))
+        return rgb, sig
+
+    def adjoint_stats(self) -> dict:
+        st = native.AdjointStats()
+        self._check(self._lib.vkptc_adjoint_get_stats(self._ctx, ctypes.byref(st)))
+        return st.as_dict()
+
+
+def material_params(materials: np.ndarray) -> np.ndarray:
+    """The 7 differentiable parameters of each material row (16 floats):
+    albedo rgb, roughness, emission rgb."""
+    m = np.asarray(materials, np.float32).reshape(-1, 16)
+    return np.ascontiguousarray(np.concatenate([m[:, 0:3], m[:, 6:7], m[:, 3:6]], axis=1))
 
 
 class BatchRenderer:
