@@ -260,6 +260,101 @@ def ray_query(device):
     return out
 
 
+def inverse_rendering(device, gd_steps: int = 200):
+    """Inverse rendering: the box room with 16 boxes, 64 parameters (per-box RGB
+    albedo and roughness), 128x128, 32 spp, depth 6, MSE loss.  grads/s = full
+    forward+backward passes per second through the C ABI (parameters uploaded,
+    loss and the gradient read back every pass).  Then 200 Adam steps from a
+    seeded start towards a 1024-spp target rendered with the held-out
+    parameters: fresh samples every step, the backward on samples independent
+    of the forward's (decorrelated), firefly clamp 10 on every image; the loss
+    of the 512-spp image is reported at the first and last parameters."""
+    from vkpathtracer_b200.tracer import CudaPathTracer, material_params
+    sc = scenes.inverse_box_scene()
+    st = scenes.inverse_settings()
+    out = {"workload": "inverse_box_16_objects_64_params_128x128_32spp_depth6", "params": 64,
+           "paths_per_pass": st.width * st.height * st.spp}
+    p_true = material_params(sc.materials)
+    rs = np.random.RandomState(11)
+    p0 = p_true.copy()
+    p0[5:21, :3] = rs.uniform(0.1, 0.8, (16, 3))
+    p0[5:21, 3] = rs.uniform(0.1, 0.8, 16)
+    with CudaPathTracer(device=device, bvh="sah") as t:
+        t.configure(st)
+        t.load_scene_snapshot(sc)
+        t.build_or_update_acceleration()
+        t.adjoint_setup(st.spp)
+        _, target = t.forward(p_true, image=True)
+        t.adjoint_setup(st.spp, target)
+        for _ in range(3):
+            t.forward(p0)
+            t.backward()
+        n = 20
+        fwd_ms = bwd_ms = 0.0
+        t0 = time.perf_counter()
+        for _ in range(n):
+            t.forward(p0)
+            t.backward()
+            s = t.adjoint_stats()
+            fwd_ms += s["forward_ms"]
+            bwd_ms += s["backward_ms"]
+        wall = time.perf_counter() - t0
+        out["grads_per_s"] = n / wall
+        out["device_grads_per_s"] = n / ((fwd_ms + bwd_ms) / 1e3)
+        out["forward_ms"] = fwd_ms / n
+        out["backward_ms"] = bwd_ms / n
+        out["forward_paths_per_s"] = out["paths_per_pass"] / (out["forward_ms"] / 1e3)
+        out["backward_paths_per_s"] = out["paths_per_pass"] / (out["backward_ms"] / 1e3)
+        out["e2e"] = {"h2d_bytes_per_pass": 7 * 4 * 2 * len(p_true), "d2h_bytes_per_pass": 8 + 7 * 4 * len(p_true)}
+
+    # gradient descent (Adam) on the 64 box parameters
+    gst = scenes.inverse_settings()
+    gst.firefly_clamp = 10.0
+    with CudaPathTracer(device=device, bvh="sah") as t:
+        t.configure(gst)
+        t.load_scene_snapshot(sc)
+        t.build_or_update_acceleration()
+        t.adjoint_setup(1024)
+        _, target = t.forward(p_true, image=True)
+
+        def converged_loss(q):
+            t.adjoint_setup(512, target, frame=7777)
+            return t.forward(q)
+        mask = np.zeros_like(p0, bool)
+        mask[5:21, :4] = True
+        conv0 = converged_loss(p0)
+        t.adjoint_setup(gst.spp, target, decorrelated=True)
+        p = p0.copy()
+        m = np.zeros_like(p)
+        v = np.zeros_like(p)
+        losses = []
+        t0 = time.perf_counter()
+        for k in range(1, gd_steps + 1):
+            t.adjoint_frames(k, 1_000_000 + k)
+            losses.append(t.forward(p))
+            g = t.backward()
+            m = 0.9 * m + 0.1 * g
+            v = 0.999 * v + 0.001 * g * g
+            step = 0.01 * (m / (1 - 0.9 ** k)) / (np.sqrt(v / (1 - 0.999 ** k)) + 1e-8)
+            p = np.where(mask, np.clip(p - step, 0.02, 1.0), p)
+        gd_s = time.perf_counter() - t0
+        conv1 = converged_loss(p)
+        conv_true = converged_loss(p_true)
+
+    def rmse(q, cols):
+        mm = np.zeros_like(mask)
+        mm[5:21, cols] = True
+        return float(np.sqrt(np.mean((q[mm] - p_true[mm]) ** 2)))
+    out["gradient_descent"] = {
+        "steps": gd_steps, "optimizer": "adam lr 0.01, parameters clipped to [0.02, 1]",
+        "setup": "fresh samples each step, decorrelated backward, 1024-spp target, firefly clamp 10",
+        "loss_32spp_first": losses[0], "loss_32spp_last": losses[-1],
+        "loss_512spp_first": conv0, "loss_512spp_last": conv1, "loss_512spp_at_true_params": conv_true,
+        "albedo_rmse_first": rmse(p0, [0, 1, 2]), "albedo_rmse_last": rmse(p, [0, 1, 2]),
+        "roughness_rmse_first": rmse(p0, [3]), "roughness_rmse_last": rmse(p, [3]), "seconds": gd_s}
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     from vkpathtracer_b200 import autotune
@@ -316,7 +411,7 @@ def run_ours(args, world, rank, local):
            "path": "vkptc_batch_run (persistent, graph) + vkptc_batch_read_film of every job to host, every step; "
                    "scenes and BVHs uploaded once before timing"}
 
-    roof = rq = ff = cpu = None
+    roof = rq = ff = cpu = inv = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the persistent kernel
         with BatchRenderer(device=local, collect_stats=True, bvh="sah") as bs:
@@ -341,6 +436,7 @@ def run_ours(args, world, rank, local):
             rq = ray_query(local)
         if not args.no_fullframe:
             ff = full_frame(local)
+        inv = None if args.no_adjoint else inverse_rendering(local)
         if world == 1 and not args.no_cpu:
             import oracle
             kind = "reference" if oracle.have_reference() else "port"
@@ -363,7 +459,7 @@ def run_ours(args, world, rank, local):
                 "plain_kernel_launches": plain["kernel_launches"],
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
-                "cpu_baseline": cpu}
+                "inverse_rendering": inv, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     b.close()
 
@@ -379,6 +475,7 @@ def main():
     ap.add_argument("--no-rayquery", action="store_true")
     ap.add_argument("--no-fullframe", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

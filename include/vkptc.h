@@ -377,11 +377,20 @@ int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* tile, uint32
 #define VKPTC_ADJ_PARAMS_PER_MATERIAL 7u
 #define VKPTC_ADJ_MAX_MATERIALS 64u
 #define VKPTC_ADJ_MAX_DEPTH 8u
+/* flags: VKPTC_ADJ_DECORRELATED makes vkptc_backward replay the paths of
+ * backward_frame (independent samples of the same pixels) instead of the
+ * forward's: the residual and the path derivatives then share no samples, so
+ * the gradient is unbiased for the loss of the expected image (with shared
+ * samples it also carries their covariance, which pulls low-spp
+ * optimisations towards darker, smoother images). */
+#define VKPTC_ADJ_DECORRELATED 1u
 typedef struct vkptc_adjoint_desc {
   uint32_t spp;
   uint32_t first_sample;
-  uint32_t frame;
-  uint32_t reserved[5];
+  uint32_t frame;            /* RNG frame of the forward's paths */
+  uint32_t backward_frame;   /* RNG frame the backward replays under VKPTC_ADJ_DECORRELATED */
+  uint32_t flags;
+  uint32_t reserved[3];
 } vkptc_adjoint_desc;
 
 typedef struct vkptc_adjoint_stats {
@@ -398,6 +407,9 @@ int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, cons
 int32_t vkptc_forward(vkptc_ctx* ctx, const float* params, uint32_t param_count, const float* rr_params,
                       double* loss, float* image_rgb);
 int32_t vkptc_backward(vkptc_ctx* ctx, float* grad, uint32_t param_count);
+/* Changes desc.frame / desc.backward_frame (e.g. fresh samples every
+ * optimisation step); the next call must be a vkptc_forward. */
+int32_t vkptc_adjoint_set_frames(vkptc_ctx* ctx, uint32_t frame, uint32_t backward_frame);
 /* As vkptc_backward with each path's adjoint scaled by path_weight[path]
  * (paths in the order of vkptc_adjoint_read_samples; NULL = all 1). */
 int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float* grad, uint32_t param_count);

@@ -107,6 +107,25 @@ def test_backward_matches_fp64_adjoint(problem):
     assert e_all <= GRAD_REL_TOL
 
 
+def test_full_size_backward_matches_fp64_adjoint():
+    """128x128, 32 spp, depth 6, all 64 box parameters (the inverse-rendering workload)."""
+    import os
+    t, sc, st = setup(128, 128, 32)
+    t.adjoint_setup(32)
+    _, target = t.forward(material_params(sc.materials), image=True)
+    t.adjoint_setup(32, target)
+    p = start_params(sc, seed=11)
+    loss = t.forward(p)
+    g = t.backward().reshape(-1)[param_index()]
+    o_loss, o_grad, _ = oracle.load_adjoint().run(sc, st, p, target, 32, param_index(),
+                                                  threads=os.cpu_count() or 1)
+    e = rel_err(g, o_grad)
+    print(f"full size: loss {loss:.6e} (fp64 {o_loss:.6e}), gradient rel err {e:.2e}")
+    assert abs(loss - o_loss) <= 1e-3 * o_loss
+    assert e <= GRAD_REL_TOL
+    t.close()
+
+
 def fd_check(t, p, spp, idx):
     """Central differences through the GPU forward with the roulette of p,
     linearised loss, flipped paths left out; returns (fd, adjoint on the same
@@ -161,6 +180,24 @@ def test_backward_is_deterministic(problem):
     g2 = t.backward()
     assert np.array_equal(g1, g2)
     assert np.array_equal(g1, grad)
+
+
+def test_decorrelated_backward_replays_the_chosen_frame(problem):
+    t, sc, st, target, p, loss, grad = problem
+    # replaying the forward's own frame reproduces the ordinary backward exactly
+    t.adjoint_setup(8, target, frame=0, decorrelated=True, backward_frame=0)
+    assert t.forward(p) == loss
+    assert np.array_equal(t.backward(), grad)
+    # another frame: independent samples (the shared-sample covariance term
+    # of the ordinary gradient is absent, so the two differ)
+    t.adjoint_frames(0, 12345)
+    t.forward(p)
+    g2 = t.backward()
+    assert np.all(np.isfinite(g2))
+    assert not np.array_equal(g2, grad)
+    assert np.abs(g2.reshape(-1)[param_index()]).max() > 0
+    t.adjoint_setup(8, target)
+    t.forward(p)
 
 
 def test_gradient_descent_lowers_loss():

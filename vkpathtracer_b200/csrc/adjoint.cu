@@ -334,9 +334,8 @@ __device__ __forceinline__ void adj_reverse(const DevScene& s, const DevSettings
 
 template <bool kParity>
 __global__ void __launch_bounds__(128) k_adj_backward(DevScene s, DevSettings st, const float* mat0, uint32_t spp,
-                                                      uint32_t first_sample, int cap, const float4* rad,
-                                                      const float4* adj, const float* path_weight, float* grad_part,
-                                                      uint32_t* err) {
+                                                      uint32_t first_sample, int cap, const float4* adj,
+                                                      const float* path_weight, float* grad_part, uint32_t* err) {
   extern __shared__ int2 smem_dyn[];
   const int warps = blockDim.x >> 5;
   const uint32_t stride = s.material_count * kAdjParams;
@@ -357,21 +356,22 @@ __global__ void __launch_bounds__(128) k_adj_backward(DevScene s, DevSettings st
     uint32_t nrec = 0u;
     if (on) {
       const uint32_t sl = static_cast<uint32_t>(j / npx), p = static_cast<uint32_t>(j % npx);
-      const float4 rv = rad[j];
       float4 a = adj[p];
       if (path_weight) {
         const float pw = path_weight[j];
         a = make_float4(a.x * pw, a.y * pw, a.z * pw, 0.0f);
       }
-      on = isfinite(rv.x) && isfinite(rv.y) && isfinite(rv.z);
+      on = a.x != 0.0f || a.y != 0.0f || a.z != 0.0f;
       if (on) {
+        // The replayed radiance decides what the film would have dropped or
+        // clamped (the replay may use other samples than the forward's).
+        const float4 rv = adj_primal<kParity, true>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk,
+                                                    local_err, rec, nrec);
         const float fc = st.firefly_clamp;
         g = mk((fc > 0.0f && rv.x > fc) ? 0.0f : a.x, (fc > 0.0f && rv.y > fc) ? 0.0f : a.y,
                (fc > 0.0f && rv.z > fc) ? 0.0f : a.z);
-        on = g.x != 0.0f || g.y != 0.0f || g.z != 0.0f;
+        on = isfinite(rv.x) && isfinite(rv.y) && isfinite(rv.z);
       }
-      if (on) adj_primal<kParity, true>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk, local_err,
-                                        rec, nrec);
     }
     adj_reverse<kParity>(s, st, rec, nrec, on, g, warp_grad);
   }
@@ -440,15 +440,15 @@ cudaError_t LaunchAdjLoss(const DevSettings& st, uint32_t spp, const float4* rad
 }
 
 cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
-                              const float4* rad, const float4* adj, const float* path_weight, float* grad_part,
-                              float* grad, uint32_t* err) {
+                              const float4* adj, const float* path_weight, float* grad_part, float* grad,
+                              uint32_t* err) {
   const size_t smem = AdjBackwardSmem(l.block, l.stack_cap, s.material_count);
   if (l.parity)
-    k_adj_backward<true><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, rad,
-                                                              adj, path_weight, grad_part, err);
+    k_adj_backward<true><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, adj,
+                                                              path_weight, grad_part, err);
   else
-    k_adj_backward<false><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, rad,
-                                                               adj, path_weight, grad_part, err);
+    k_adj_backward<false><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, adj,
+                                                               path_weight, grad_part, err);
   const uint32_t stride = s.material_count * kAdjParams;
   k_adj_grad_reduce<<<(stride + 127) / 128, 128, 0, l.stream>>>(grad_part, l.grid, stride, grad);
   return cudaGetLastError();

@@ -34,10 +34,11 @@ cudaError_t LaunchAdjLoss(const DevSettings& st, uint32_t spp, const float4* rad
 
 // Reverse sweep: per-block gradient partials grad_part[block][7 * materials],
 // then the fixed-order reduction into grad (7 floats per material).
-// path_weight (optional, one per path) scales each path's adjoint.
+// path_weight (optional, one per path) scales each path's adjoint.  The
+// paths replayed are those of st.frame (the forward's, or independent ones).
 cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
-                              const float4* rad, const float4* adj, const float* path_weight, float* grad_part,
-                              float* grad, uint32_t* err);
+                              const float4* adj, const float* path_weight, float* grad_part, float* grad,
+                              uint32_t* err);
 
 size_t AdjBackwardSmem(int block, int stack_cap, uint32_t materials);
 size_t AdjForwardSmem(int block, int stack_cap);

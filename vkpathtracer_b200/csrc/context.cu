@@ -1569,7 +1569,8 @@ int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float*
   }
   VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_err.ptr, 0, sizeof(uint32_t), ctx->stream), "error clear");
   VKPTC_CUDA(ctx, cudaEventRecord(a.ev[2], ctx->stream), "event");
-  VKPTC_CUDA(ctx, LaunchAdjBackward(adj_scene(ctx), dev_settings(ctx, a.desc.frame), a.mat0.ptr, l, a.rad.ptr, a.adj.ptr,
+  const uint32_t replay_frame = (a.desc.flags & VKPTC_ADJ_DECORRELATED) ? a.desc.backward_frame : a.desc.frame;
+  VKPTC_CUDA(ctx, LaunchAdjBackward(adj_scene(ctx), dev_settings(ctx, replay_frame), a.mat0.ptr, l, a.adj.ptr,
                                     path_weight ? a.path_weight.ptr : nullptr, a.grad_part.ptr, a.grad.ptr,
                                     ctx->d_err.ptr),
              "adjoint backward launch");
@@ -1584,6 +1585,15 @@ int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float*
   a.stats.backwards++;
   a.stats.backward_grid = static_cast<uint32_t>(l.grid);
   ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_adjoint_set_frames(vkptc_ctx* ctx, uint32_t frame, uint32_t backward_frame) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->adj.setup) return fail(ctx, VKPTC_NOT_READY, "vkptc_adjoint_setup must run first");
+  ctx->adj.desc.frame = frame;
+  ctx->adj.desc.backward_frame = backward_frame;
+  ctx->adj.forward_done = false;
   return VKPTC_OK;
 }
 

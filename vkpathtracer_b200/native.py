@@ -110,7 +110,10 @@ class BatchStats(ctypes.Structure):
 
 class AdjointDesc(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_uint32), ("first_sample", ctypes.c_uint32), ("frame", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 5)]
+                ("backward_frame", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
+
+
+ADJ_DECORRELATED = 1
 
 
 class AdjointStats(ctypes.Structure):
@@ -169,6 +172,7 @@ SIGNATURES = {
     "vkptc_forward": (I32, [P, P, U32, P, ctypes.POINTER(ctypes.c_double), P]),
     "vkptc_backward": (I32, [P, P, U32]),
     "vkptc_backward_weighted": (I32, [P, P, P, U32]),
+    "vkptc_adjoint_set_frames": (I32, [P, U32, U32]),
     "vkptc_adjoint_read_samples": (I32, [P, P, P]),
     "vkptc_adjoint_get_stats": (I32, [P, ctypes.POINTER(AdjointStats)]),
 }

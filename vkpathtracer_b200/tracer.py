@@ -304,11 +304,16 @@ class CudaPathTracer:
 
 
     # ------------------------------------------------ differentiable rendering
-    def adjoint_setup(self, spp: int, target: Optional[np.ndarray] = None, frame: int = 0, first_sample: int = 0):
+    def adjoint_setup(self, spp: int, target: Optional[np.ndarray] = None, frame: int = 0, first_sample: int = 0,
+                      decorrelated: bool = False, backward_frame: int = 0):
         """Prepares vkptc_forward / vkptc_backward: spp samples per pixel, MSE
-        loss against target (H, W, 3) float32, or no target."""
+        loss against target (H, W, 3) float32, or no target.  decorrelated:
+        the backward replays the paths of backward_frame instead of the
+        forward's (an unbiased gradient of the expected image's loss)."""
         d = native.AdjointDesc()
         d.spp, d.first_sample, d.frame = spp, first_sample, frame
+        d.backward_frame = backward_frame
+        d.flags = native.ADJ_DECORRELATED if decorrelated else 0
         tg = None if target is None else np.ascontiguousarray(target, np.float32).reshape(-1)
         self._check(self._lib.vkptc_adjoint_setup(self._ctx, ctypes.byref(d), _ptr(tg), 0 if tg is None else tg.size))
         self._adj_spp = spp
@@ -338,6 +343,10 @@ class CudaPathTracer:
                 raise ValueError("path_weight must hold one float per path")
             self._check(self._lib.vkptc_backward_weighted(self._ctx, _ptr(pw), _ptr(g), n))
         return g.reshape(-1, native.ADJ_PARAMS_PER_MATERIAL)
+
+    def adjoint_frames(self, frame: int, backward_frame: int = 0):
+        """New RNG frames for the next forward (and a decorrelated backward)."""
+        self._check(self._lib.vkptc_adjoint_set_frames(self._ctx, frame, backward_frame))
 
     def adjoint_samples(self):
         """(rgb (spp, H, W, 3), signature (spp, H, W) uint32) of the last forward."""
