@@ -133,6 +133,14 @@ def reduce_over_ranks(world, value, op, device=None):
     return float(t.item())
 
 
+def aggregate_throughput(world, units_local, ms_local, device=None):
+    """Whole-job throughput of N replicas: the units all ranks processed over
+    the slowest rank's device time.  Returns (units/s, max ms, total units)."""
+    ms_max = reduce_over_ranks(world, float(ms_local), "max", device)
+    units = reduce_over_ranks(world, float(units_local), "sum", device)
+    return units / (ms_max / 1e3), ms_max, units
+
+
 def make_jobs(count: int, seed: int = 5):
     return scenes.batch_jobs(count=count, seed=seed)
 
@@ -170,7 +178,7 @@ def run_reference(args, world, rank):
     kind = "reference" if oracle.have_reference() else "port"
     threads = os.cpu_count() or 1
     jobs = make_jobs(args.jobs)
-    per_step_s = max(1.5, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
+    per_step_s = args.cpu_step_seconds or max(1.5, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
     vals, sample, frac = [], None, 2e-3
     for i in range(args.warmup + args.steps):
         v, sample = cpu_sample(jobs, per_step_s, threads, kind, seed=i, frac=frac)
@@ -391,9 +399,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     ms_total = sum(s["device_ms"] for s in stats)
-    ms_max = reduce_over_ranks(world, ms_total, "max", dev)
-    all_paths = reduce_over_ranks(world, float(total_paths * args.steps), "sum", dev)
-    value = all_paths / (ms_max / 1e3)
+    value, ms_max, all_paths = aggregate_throughput(world, total_paths * args.steps, ms_total, dev)
     st0 = stats[-1]
     mrays = (st0["segments"] + st0["shadow_rays"]) / (st0["device_ms"] / 1e3) / 1e6
 
@@ -476,6 +482,8 @@ def main():
     ap.add_argument("--no-fullframe", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--cpu-step-seconds", type=float, default=0.0,
+                    help="CPU work per reference-arm step (0 = about a minute over all steps)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
