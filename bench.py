@@ -40,6 +40,9 @@ UNIT = "paths/s"
 WORKLOAD = "batch_64_uneven_jobs"
 NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
 PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
+# DRAM bytes (read + write) per extension ray of k_loop_extend, from one ncu
+# capture of the 4-job case (profiles/k_loop_extend_batch_4_jobs.md).
+TRAFFIC_BYTES_PER_EXT_RAY = 0.0
 
 
 def peaks():
@@ -202,23 +205,28 @@ def run_reference(args, world, rank):
 
 
 # ------------------------------------------------------------------ GPU side
-def full_frame(device):
-    """The full-frame scene: 1920x1080, 64 spp, depth 16 as one persistent job,
-    plus one sample per launch through the wavefront path."""
+def full_frame(device, tunings=None):
+    """The full-frame scene: 1920x1080, 64 spp, depth 16 as one batched job
+    (both drivers, with the batch workload's tuning), plus one sample per
+    launch through the wavefront path."""
     import torch
     from vkpathtracer_b200.tracer import BatchRenderer, CudaPathTracer
     sc = scenes.sphere_grid()
     st = scenes.sphere_grid_settings()
     out = {"workload": "sphere_grid_64x64_1080p_64spp_depth16", "triangles": sc.triangle_count}
+    tunings = tunings or {"loop": {}, "persistent": {}}
     with BatchRenderer(device=device, bvh="sah") as b:
         b.add_job(sc, st)
-        b.run("persistent")
-        runs = [b.run("persistent") for _ in range(2)]
-        ms = min(r["device_ms"] for r in runs)
-        r = runs[0]
-        out["paths_per_s"] = r["paths"] / (ms / 1e3)
-        out["mrays_per_s"] = (r["segments"] + r["shadow_rays"]) / (ms / 1e3) / 1e6
-        out["ms_per_frame_64spp"] = ms
+        for m, cfg in tunings.items():
+            b.run(m, **cfg)
+            runs = [b.run(m, **cfg) for _ in range(2)]
+            ms = min(r["device_ms"] for r in runs)
+            r = runs[0]
+            out[m] = {"paths_per_s": r["paths"] / (ms / 1e3),
+                      "mrays_per_s": (r["segments"] + r["shadow_rays"]) / (ms / 1e3) / 1e6,
+                      "ms_per_frame_64spp": ms}
+        best = max(out[m]["paths_per_s"] for m in tunings)
+        out["paths_per_s"] = best
     with CudaPathTracer(device=device, bvh="sah") as t:
         t.configure(st)
         t.load_scene_snapshot(sc)
@@ -363,6 +371,27 @@ def inverse_rendering(device, gd_steps: int = 200):
     return out
 
 
+def profile_run(args, local):
+    """Small fixed run for profilers: the job set rendered by one driver
+    without a CUDA graph (every stage a plain launch), with the tuning from
+    the autotuner's cache when there is one.  Prints the run's stats."""
+    from vkpathtracer_b200 import autotune
+    from vkpathtracer_b200.tracer import BatchRenderer
+    jobs = make_jobs(args.jobs)
+    key = autotune.workload_key((j.scene.triangle_count, j.settings.width, j.settings.spp, j.settings.max_depth)
+                                for j in jobs)
+    cached = autotune._load_cache().get(f"batch/{autotune._gpu_name()}/loop+persistent/{key}", {})
+    cfg = cached.get("per_mode", {}).get(args.profile_run, {})
+    tuning = {k: cfg[k] for k in ("pool_paths", "block_size", "stack_depth", "steps", "occupancy") if k in cfg}
+    with BatchRenderer(device=local, bvh="sah") as b:
+        for j in jobs:
+            b.add_job(j.scene, j.settings)
+        for _ in range(2):
+            r = b.run(args.profile_run, use_graph=False, **tuning)
+    print(json.dumps({"profile_run": args.profile_run, "jobs": len(jobs), "tuning": tuning,
+                      "iterations": r["iterations"], "device_ms": r["device_ms"], "paths": r["paths"]}), flush=True)
+
+
 def run_ours(args, world, rank, local):
     import torch
     from vkpathtracer_b200 import autotune
@@ -381,7 +410,9 @@ def run_ours(args, world, rank, local):
     key = autotune.workload_key((j.scene.triangle_count, j.settings.width, j.settings.spp, j.settings.max_depth)
                                 for j in jobs)
     tune = autotune.tune_batch(b, key, use_cache=not args.retune)
-    tuning = {k: tune[k] for k in ("pool_paths", "block_size", "stack_depth", "steps", "occupancy")}
+    keys = ("pool_paths", "block_size", "stack_depth", "steps", "occupancy")
+    mode = tune["mode"]
+    tuning = {k: tune[k] for k in keys}
 
     # ---------------------------------------------------------- plain mode (one frame per launch)
     plain = b.run("plain")
@@ -389,13 +420,13 @@ def run_ours(args, world, rank, local):
 
     # ---------------------------------------------------------- timed persistent runs
     for _ in range(args.warmup):
-        b.run("persistent", **tuning)
+        b.run(mode, **tuning)
     barrier(world)
     torch.cuda.synchronize()
     stats = []
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
-            stats.append(b.run("persistent", **tuning))
+            stats.append(b.run(mode, **tuning))
     torch.cuda.synchronize()
     barrier(world)
     ms_total = sum(s["device_ms"] for s in stats)
@@ -409,39 +440,68 @@ def run_ours(args, world, rank, local):
     barrier(world)
     w0 = time.perf_counter()
     for _ in range(args.steps):
-        b.run("persistent", **tuning)
+        b.run(mode, **tuning)
         for k in range(len(jobs)):
             hostfilms[k][:] = b.film(k)[0]
     e2e_ms = reduce_over_ranks(world, 1e3 * (time.perf_counter() - w0), "max", dev)
     e2e = {"value": all_paths / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
-           "path": "vkptc_batch_run (persistent, graph) + vkptc_batch_read_film of every job to host, every step; "
-                   "scenes and BVHs uploaded once before timing"}
+           "path": f"vkptc_batch_run ({mode} driver, graph) + vkptc_batch_read_film of every job to host, every "
+                   "step; scenes and BVHs uploaded once before timing"}
+    # both drivers, each with its own best tuning, on the same jobs
+    drivers = {}
+    for m, cfg in tune.get("per_mode", {}).items():
+        mt = {k: cfg[k] for k in keys}
+        b.run(m, **mt)
+        ms = min(b.run(m, **mt)["device_ms"] for _ in range(2))
+        drivers[m] = {"paths_per_s": total_paths / (ms / 1e3), "tuning": mt}
 
     roof = rq = ff = cpu = inv = None
     if rank == 0:
-        # ------------------------------------------------------ roofline of the persistent kernel
+        # ------------------------------------------------------ roofline of the dominant kernel
+        # traversal work counted in a stats run (same rays: the traversal is deterministic)
         with BatchRenderer(device=local, collect_stats=True, bvh="sah") as bs:
             for j in jobs:
                 bs.add_job(j.scene, j.settings)
-            ss = bs.run("persistent", **tuning)
+            ss = bs.run(mode, **tuning)
         rays = ss["ext_rays"] + ss["shadow_queries"]
         nodes = ss["ext_nodes"] + ss["shadow_nodes"]
         tris = ss["ext_tris"] + ss["shadow_tris"]
-        alg = NODE_BYTES * nodes + TRI_BYTES * tris + RAY_IO_BYTES * rays + PATH_STATE_BYTES * ss["segments"] \
-            + 16 * ss["paths"]
-        kernel_ms = st0["device_ms"]
-        achieved = alg / (kernel_ms / 1e3) / 1e9
-        roof = {"kernel": "k_batch (persistent wavefront: regen, closest-hit, shade, any-hit, finish)",
-                "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": None,
-                "alg_bytes_per_launch": alg, "avg_launch_ms": kernel_ms, "launches": 1,
-                "nodes_per_ray": nodes / max(1, rays), "tris_per_ray": tris / max(1, rays),
-                "note": "one persistent launch per step; timing includes the pool reset and in-order film "
-                        "accumulation kernels of the same graph"}
+        if mode == "loop":
+            # per-stage CUDA events (host-driven iterations of the same stage kernels)
+            with BatchRenderer(device=local, stage_timing=True, bvh="sah") as bt:
+                for j in jobs:
+                    bt.add_job(j.scene, j.settings)
+                tt = bt.run("loop", use_graph=False, **tuning)
+            stage = tt["stage_ms"]
+            alg = NODE_BYTES * ss["ext_nodes"] + TRI_BYTES * ss["ext_tris"] + RAY_IO_BYTES * ss["ext_rays"]
+            iters = max(1, tt["iterations"])
+            achieved = alg / (stage["extend"] / 1e3) / 1e9
+            traffic = TRAFFIC_BYTES_PER_EXT_RAY * ss["ext_rays"] / iters
+            roof = {"kernel": "k_loop_extend (closest-hit traversal stage of the loop driver)", "bound": "hbm",
+                    "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                    "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": traffic,
+                    "traffic_note": "per launch: DRAM bytes per extension ray from the ncu capture of the 4-job "
+                                    "case (profiles/k_loop_extend_batch_4_jobs.md) x extension rays per launch",
+                    "alg_bytes_per_launch": alg / iters, "avg_launch_ms": stage["extend"] / iters,
+                    "launches": iters, "stage_ms": stage,
+                    "stage_share": {k: v / max(1e-9, sum(stage.values())) for k, v in stage.items()},
+                    "shadow_stage_achieved_gbs": (NODE_BYTES * ss["shadow_nodes"] + TRI_BYTES * ss["shadow_tris"]
+                                                  + RAY_IO_BYTES * ss["shadow_queries"]) / (stage["shadow"] / 1e3) / 1e9,
+                    "nodes_per_ray": nodes / max(1, rays), "tris_per_ray": tris / max(1, rays)}
+        else:
+            alg = NODE_BYTES * nodes + TRI_BYTES * tris + RAY_IO_BYTES * rays + PATH_STATE_BYTES * ss["segments"] \
+                + 16 * ss["paths"]
+            kernel_ms = st0["device_ms"]
+            achieved = alg / (kernel_ms / 1e3) / 1e9
+            roof = {"kernel": "k_batch (persistent wavefront: regen, closest-hit, shade, any-hit, finish)",
+                    "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                    "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": None,
+                    "alg_bytes_per_launch": alg, "avg_launch_ms": kernel_ms, "launches": 1,
+                    "nodes_per_ray": nodes / max(1, rays), "tris_per_ray": tris / max(1, rays)}
         if not args.no_rayquery:
             rq = ray_query(local)
         if not args.no_fullframe:
-            ff = full_frame(local)
+            ff = full_frame(local, {m: d["tuning"] for m, d in drivers.items()} or None)
         inv = None if args.no_adjoint else inverse_rendering(local)
         if world == 1 and not args.no_cpu:
             import oracle
@@ -457,11 +517,13 @@ def run_ours(args, world, rank, local):
                 "config": {"workload": WORKLOAD, "jobs": len(jobs), "paths_per_step": total_paths,
                            "triangles": sum(j.scene.triangle_count for j in jobs),
                            "setup_s": setup_s, "bvh": "sah traversal tree (hit ids exact: ties and parallel-axis "
-                                                    "rule through the reference tree)", "tuning": tuning, "autotune": {k: tune.get(k) for k in
-                                                                              ("ms", "trials", "cached")},
+                                                    "rule through the reference tree)",
+                           "driver": mode, "tuning": tuning,
+                           "autotune": {k: tune.get(k) for k in ("ms", "trials", "cached")},
                            "l2": "inputs larger than L2 (all scenes, BVHs and the path pool resident in HBM)",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
                 "mrays_per_s": mrays, "plain_paths_per_s": plain_ps, "speedup_vs_plain": value / world / plain_ps,
+                "drivers": drivers,
                 "plain_kernel_launches": plain["kernel_launches"],
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
@@ -482,6 +544,8 @@ def main():
     ap.add_argument("--no-fullframe", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--profile-run", choices=["loop", "persistent"], default=None,
+                    help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
     ap.add_argument("--cpu-step-seconds", type=float, default=0.0,
                     help="CPU work per reference-arm step (0 = about a minute over all steps)")
     args = ap.parse_args()
@@ -489,7 +553,9 @@ def main():
         args.warmup = 3
     world, rank, local = dist_init(args)
     try:
-        if args.impl == "reference":
+        if args.profile_run:
+            profile_run(args, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

@@ -268,6 +268,12 @@ typedef struct vkptc_batch vkptc_batch;
 
 #define VKPTC_BATCH_PLAIN 0u
 #define VKPTC_BATCH_PERSISTENT 1u
+/* The same pool, work queue and stages as VKPTC_BATCH_PERSISTENT, but one
+ * kernel per stage (each with its own register budget and occupancy) inside a
+ * CUDA graph while-node that the device keeps iterating until the work queue
+ * is empty: one graph launch per run, no grid barrier.  Films are identical
+ * to the other modes. */
+#define VKPTC_BATCH_LOOP 2u
 
 typedef struct vkptc_batch_tuning {
   uint32_t pool_paths;       /* path slots of the persistent launch ("queue capacity"); 0 = default */
@@ -275,7 +281,8 @@ typedef struct vkptc_batch_tuning {
   uint32_t stack_depth;      /* traversal stack entries in shared memory; 0 = default */
   uint32_t steps;            /* traversal steps between warp refills; 0 = default */
   uint32_t sample_limit;     /* render at most this many samples per job (0 = each job's spp) */
-  uint32_t use_graph;        /* persistent mode: 1 = capture once, replay the CUDA graph */
+  uint32_t use_graph;        /* persistent/loop modes: 1 = capture once, replay the CUDA graph
+                                (loop mode without a graph runs one host round trip per iteration) */
   uint32_t occupancy;        /* persistent kernel register variant: 0..3 = at least 1..4 resident
                                 256-thread blocks per SM (fewer registers, more warps) */
   uint32_t reserved;
@@ -294,10 +301,14 @@ typedef struct vkptc_batch_stats {
   uint32_t pool_paths;
   uint32_t stack_depth;
   uint32_t steps;
-  uint32_t reserved;
+  uint32_t iterations;       /* pool iterations (stage rounds) of the last persistent/loop run */
   /* traversal work (filled when vkptc_config.collect_stats = 1) */
   uint64_t ext_rays, ext_nodes, ext_tris;
   uint64_t shadow_queries, shadow_nodes, shadow_tris;
+  /* loop driver without a graph and vkptc_config.stage_timing = 1: device
+   * time of each stage summed over the iterations (regen, extend, shade,
+   * shadow, finish; CUDA events around every stage launch) */
+  double stage_ms[5];
 } vkptc_batch_stats;
 
 int32_t vkptc_batch_create(const vkptc_config* config, vkptc_batch** out_batch);

@@ -63,12 +63,32 @@ def test_persistent_equals_plain_bitwise(batch):
     assert s_pers["kernel_launches"] < s_plain["kernel_launches"]
 
 
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_loop_mode_equals_plain_bitwise(batch, use_graph):
+    """One kernel per stage in a CUDA graph while-node (or host-driven)."""
+    n = len(small_jobs())
+    s_plain = batch.run("plain")
+    plain = films(batch, n)
+    s_loop = batch.run("loop", use_graph=use_graph)
+    assert s_loop["graph_used"] == int(use_graph)
+    assert s_loop["iterations"] > 0
+    assert s_loop["kernel_launches"] == 1 + 5 * s_loop["iterations"] + n
+    for (a, ca), (b, cb) in zip(plain, films(batch, n)):
+        assert np.array_equal(ca, cb) and np.array_equal(bits(a), bits(b))
+    assert s_loop["segments"] == s_plain["segments"]
+    assert s_loop["shadow_rays"] == s_plain["shadow_rays"]
+    # the persistent driver runs the same number of pool iterations
+    s_pers = batch.run("persistent", use_graph=use_graph)
+    assert s_pers["iterations"] == s_loop["iterations"]
+
+
+@pytest.mark.parametrize("mode", ["persistent", "loop"])
 @pytest.mark.parametrize("pool,block,stack,steps", [(1024, 64, 4, 1), (4096, 256, 8, 16), (1 << 18, 128, 32, 4)])
-def test_tuning_does_not_change_films(batch, pool, block, stack, steps):
+def test_tuning_does_not_change_films(batch, mode, pool, block, stack, steps):
     n = len(small_jobs())
     batch.run("plain")
     ref = films(batch, n)
-    batch.run("persistent", pool_paths=pool, block_size=block, stack_depth=stack, steps=steps)
+    batch.run(mode, pool_paths=pool, block_size=block, stack_depth=stack, steps=steps)
     got = films(batch, n)
     for (a, ca), (b, cb) in zip(ref, got):
         assert np.array_equal(ca, cb) and np.array_equal(bits(a), bits(b))

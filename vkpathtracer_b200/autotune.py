@@ -1,11 +1,13 @@
-"""Autotuner for the persistent batched renderer and the wavefront renderer.
+"""Autotuner for the batched renderer and the wavefront renderer.
 
-Sweeps the launch parameters the kernels expose -- path-pool capacity (the
-device queue capacity), block size, traversal-stack entries kept in shared
-memory, and traversal steps between warp refills -- on a short run of the
-actual workload (one sample per job), keeps the fastest, and caches the
-choice in a JSON file keyed by GPU name and workload signature.  Films do not
-depend on these parameters (tests/test_gpu_batch.py), only speed does.
+Sweeps the launch parameters the kernels expose -- the driver (the
+cooperative persistent kernel or the device-driven stage loop), path-pool
+capacity (the device queue capacity), block size, traversal-stack entries
+kept in shared memory, traversal steps between warp refills and the register
+variant -- on a short run of the actual workload (one sample per job), keeps
+the fastest, and caches the choice in a JSON file keyed by GPU name and
+workload signature.  Films do not depend on these parameters
+(tests/test_gpu_batch.py), only speed does.
 """
 from __future__ import annotations
 
@@ -68,15 +70,20 @@ def _store_cache(data: Dict) -> None:
         pass
 
 
-def tune_batch(batch, key: str, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS, stacks=DEFAULT_STACKS,
-               steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1, repeats: int = 2,
-               use_cache: bool = True, log: Optional[callable] = None) -> Dict:
-    """Returns {"pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials"}.
+DEFAULT_MODES = ("loop", "persistent")
 
-    Coordinate search: the pool capacity first (other parameters at their
-    defaults), then block size x stack entries x steps x register variant."""
+
+def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS,
+               stacks=DEFAULT_STACKS, steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1,
+               repeats: int = 2, use_cache: bool = True, log: Optional[callable] = None) -> Dict:
+    """Returns {"mode", "pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials"}.
+
+    Coordinate search per driver: the pool capacity first (other parameters
+    at their defaults), then block size x stack entries x steps x register
+    variant; the fastest over both drivers wins.  Trials replay a CUDA graph
+    (the way the runs are timed), so the loop driver is measured as it runs."""
     cache = _load_cache() if use_cache else {}
-    ckey = f"batch/{_gpu_name()}/{key}"
+    ckey = f"batch/{_gpu_name()}/{'+'.join(modes)}/{key}"
     if use_cache and ckey in cache:
         return dict(cache[ckey], cached=True)
     best = None
@@ -86,24 +93,39 @@ def tune_batch(batch, key: str, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS, stac
     def trial(cfg):
         nonlocal best
         try:
-            ms = min(batch.run("persistent", sample_limit=sample_limit, use_graph=False, **cfg)["device_ms"]
+            mode = cfg["mode"]
+            args = {k: v for k, v in cfg.items() if k != "mode"}
+            batch.run(mode, sample_limit=sample_limit, use_graph=True, **args)   # capture
+            ms = min(batch.run(mode, sample_limit=sample_limit, use_graph=True, **args)["device_ms"]
                      for _ in range(repeats))
         except Exception as e:   # a shape that does not fit (e.g. shared memory) is skipped
             trials.append(dict(cfg, error=str(e)))
-            return
+            return None
         trials.append(dict(cfg, ms=ms))
         if log:
             log(trials[-1])
         if best is None or ms < best["ms"]:
             best = dict(cfg, ms=ms)
+        return ms
 
-    for pool in pools:
-        trial({"pool_paths": pool, "block_size": 0, "stack_depth": 0, "steps": 0, "occupancy": 0})
-    pool = best["pool_paths"] if best else pools[0]
-    for block, stack, st, occ in itertools.product(blocks, stacks, steps, occupancy):
-        trial({"pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st, "occupancy": occ})
+    for mode in modes:
+        mode_best = None
+        for pool in pools:
+            cfg = {"mode": mode, "pool_paths": pool, "block_size": 0, "stack_depth": 0, "steps": 0, "occupancy": 0}
+            ms = trial(cfg)
+            if ms is not None and (mode_best is None or ms < mode_best[1]):
+                mode_best = (pool, ms)
+        pool = mode_best[0] if mode_best else pools[0]
+        for block, stack, st, occ in itertools.product(blocks, stacks, steps, occupancy):
+            trial({"mode": mode, "pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st,
+                   "occupancy": occ})
     if best is None:
         raise RuntimeError("autotune: no launch configuration ran")
+    per_mode = {}
+    for tr in trials:
+        if "ms" in tr and (tr["mode"] not in per_mode or tr["ms"] < per_mode[tr["mode"]]["ms"]):
+            per_mode[tr["mode"]] = dict(tr)
+    best["per_mode"] = per_mode
     best["trials"] = len(trials)
     best["tune_seconds"] = time.time() - t0
     if use_cache:

@@ -35,6 +35,7 @@ constexpr int kCtlExt0 = 0, kCtlExt1 = 1, kCtlShadow = 2, kCtlFin = 3, kCtlFree 
 constexpr int kCtlFetchExt = 5, kCtlFetchShadow = 6;
 constexpr int kCtlWork = 8;      // 64-bit path counter (words 8, 9)
 constexpr int kCtlBarCount = 12, kCtlBarGen = 13, kCtlAbort = 15;
+constexpr int kCtlCur = 16, kCtlMore = kBatchCtlMore, kCtlIter = kBatchCtlIterations;   // loop driver words
 constexpr unsigned kBarrierSpinLimit = 1u << 26;   // x ~128 ns sleeps: ~8.6 s
 
 __device__ __forceinline__ bool grid_barrier(uint32_t* ctl) {
@@ -128,8 +129,154 @@ struct BatchShadowSource {
   }
 };
 
+// ------------------------------------------------------------------ phases
+// The five stages of one iteration over the pool.  Both drivers run them:
+// the cooperative persistent kernel (grid barriers between stages) and the
+// device-driven loop (one kernel per stage, a CUDA graph while-node around
+// them).  Each is grid-stride over a device-side count.
+
+// REGEN: free slots take the next path ids of the work queue, generate the
+// camera ray and append to the extension queue `cur`.
+template <bool kParity>
+__device__ __forceinline__ void phase_regen(const DevJob* __restrict__ jobs, uint32_t job_count,
+                                            unsigned long long total, const BatchPool& P, uint32_t cur) {
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  const unsigned lane = threadIdx.x & 31u;
+  unsigned long long* work_next = reinterpret_cast<unsigned long long*>(P.ctl + kCtlWork);
+  const uint32_t nfree = P.ctl[kCtlFree];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < nfree; base += gthreads) {
+    const uint32_t j = base + threadIdx.x;
+    const bool want = j < nfree;
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    unsigned long long g0 = 0ull;
+    const int lead = __ffs(mask) - 1;
+    if (mask != 0u && static_cast<int>(lane) == lead) g0 = atomicAdd(work_next, static_cast<unsigned long long>(__popc(mask)));
+    g0 = __shfl_sync(0xffffffffu, g0, lead < 0 ? 0 : lead);
+    const unsigned long long g = g0 + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u)));
+    const bool ok = want && g < total;
+    uint32_t slot = 0u;
+    if (ok) {
+      slot = P.freel[j];
+      const uint32_t jb = find_job(jobs, job_count, g);
+      const DevJob& J = jobs[jb];
+      const uint32_t local = static_cast<uint32_t>(g - J.path_base);
+      const uint32_t sl = local / J.pixels, px = local - sl * J.pixels;
+      const uint32_t W = J.settings.width;
+      V3 o, d;
+      uint64_t rng;
+      camera_path<kParity>(J.scene, J.settings, px % W, px / W, J.first_sample + sl, o, d, rng);
+      P.job[slot] = jb;
+      P.local[slot] = local;
+      P.depth[slot] = 0u;
+      P.rng[slot] = rng;
+      P.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+      P.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
+      P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+      P.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    const uint32_t qi = warp_append(&P.ctl[cur], ok);
+    if (ok) P.ext[cur][qi] = slot;
+  }
+}
+
+// SHADE: one bounce of the integrator for every path of extension queue
+// `cur`; appends to the next extension queue, the shadow queue, or the
+// finished list.  Returns this thread's shadow-test count.
+template <bool kParity>
+__device__ __forceinline__ uint32_t phase_shade(const DevJob* __restrict__ jobs, const BatchPool& P, uint32_t cur,
+                                                uint32_t n_ext) {
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  uint32_t shadow_tests = 0u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n_ext; base += gthreads) {
+    const uint32_t j = base + threadIdx.x;
+    bool next = false, shadow = false, fin = false;
+    uint32_t slot = 0u;
+    ShadeOut R;
+    if (j < n_ext) {
+      slot = P.ext[cur][j];
+      const DevJob& J = jobs[P.job[slot]];
+      const uint32_t depth = P.depth[slot];
+      const float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot], t4 = P.thr[slot], r4 = P.rad[slot];
+      const float2 h2 = P.hit[slot];
+      PathRegs pr;
+      pr.o = mk(o4.x, o4.y, o4.z);
+      pr.d = mk(d4.x, d4.y, d4.z);
+      pr.thr = mk(t4.x, t4.y, t4.z);
+      pr.rad = mk(r4.x, r4.y, r4.z);
+      pr.segs = r4.w;
+      pr.rng = P.rng[slot];
+      R = shade_bounce<kParity>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y));
+      if (R.next) {
+        P.ray_o[slot] = make_float4(pr.o.x, pr.o.y, pr.o.z, 0.0f);
+        P.ray_d[slot] = make_float4(pr.d.x, pr.d.y, pr.d.z, 0.0f);
+        P.thr[slot] = make_float4(pr.thr.x, pr.thr.y, pr.thr.z, 0.0f);
+        P.rng[slot] = pr.rng;
+        P.depth[slot] = depth + 1u;
+      }
+      P.rad[slot] = make_float4(pr.rad.x, pr.rad.y, pr.rad.z, pr.segs);
+      next = R.next;
+      fin = !R.next;
+      shadow = R.shadow;
+      shadow_tests += R.shadow_tests;
+    }
+    const uint32_t qn = warp_append(&P.ctl[cur ^ 1u], next);
+    if (next) P.ext[cur ^ 1u][qn] = slot;
+    const uint32_t qf = warp_append(&P.ctl[kCtlFin], fin);
+    if (fin) P.fin[qf] = slot;
+    const uint32_t qs = warp_append(&P.ctl[kCtlShadow], shadow);
+    if (shadow) {
+      P.shq[qs] = slot;
+      P.sh_o[qs] = make_float4(R.sh_o.x, R.sh_o.y, R.sh_o.z, R.sh_t);
+      P.sh_d[qs] = make_float4(R.sh_d.x, R.sh_d.y, R.sh_d.z, 0.0f);
+      P.sh_c[qs] = make_float4(R.sh_c.x, R.sh_c.y, R.sh_c.z, 0.0f);
+    }
+  }
+  return shadow_tests;
+}
+
+// FINISH: finished paths write their radiance to the job's staging slot and
+// return their slot to the free list.
+__device__ __forceinline__ void phase_finish(const DevJob* __restrict__ jobs, const BatchPool& P) {
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  const uint32_t n_fin = P.ctl[kCtlFin];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n_fin; base += gthreads) {
+    const uint32_t j = base + threadIdx.x;
+    const bool ok = j < n_fin;
+    uint32_t slot = 0u;
+    if (ok) {
+      slot = P.fin[j];
+      const DevJob& J = jobs[P.job[slot]];
+      J.staging[P.local[slot]] = P.rad[slot];
+    }
+    const uint32_t qi = warp_append(&P.ctl[kCtlFree], ok);
+    if (ok) P.freel[qi] = slot;
+  }
+}
+
+__device__ __forceinline__ TwoLevelStack batch_stack(int2* smem_stack, int scap, int2* spill, int total_cap) {
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  return TwoLevelStack{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), scap,
+                       spill ? spill + gtid : nullptr, static_cast<int>(gthreads), total_cap};
+}
+
+template <bool kStats>
+__device__ __forceinline__ void flush_traversal_stats(DevCounters* ctr, const TraceStats& st_e, const TraceStats& st_s) {
+  if (kStats) {
+    warp_count(&ctr->nodes, st_e.nodes);
+    warp_count(&ctr->leaves, st_e.leaves);
+    warp_count(&ctr->tris, st_e.tris);
+    warp_count(&ctr->ext_rays, st_e.rays);
+    warp_count(&ctr->shadow_nodes, st_s.nodes);
+    warp_count(&ctr->shadow_leaves, st_s.leaves);
+    warp_count(&ctr->shadow_tris, st_s.tris);
+    warp_count(&ctr->shadow_rays, st_s.rays);
+  }
+}
+
 }  // namespace
 
+// ------------------------------------------------------- persistent driver
 // kMinBlocks: resident 256-thread blocks per SM the register allocation must
 // allow (0 = compiler's choice); the autotuner picks the occupancy/spill trade-off.
 template <bool kParity, bool kStats, int kMinBlocks>
@@ -138,12 +285,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
                                                            int2* spill, int total_cap, int steps, DevCounters* ctr,
                                                            uint32_t* err) {
   extern __shared__ int2 smem_stack[];
-  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t gthreads = gridDim.x * blockDim.x;
-  const TwoLevelStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), scap,
-                          spill ? spill + gtid : nullptr, static_cast<int>(gthreads), total_cap};
-  const unsigned lane = threadIdx.x & 31u;
-  unsigned long long* work_next = reinterpret_cast<unsigned long long*>(P.ctl + kCtlWork);
+  const TwoLevelStack stk = batch_stack(smem_stack, scap, spill, total_cap);
   TraceStats st_e, st_s;
   uint32_t lerr = 0u;
   uint32_t shadow_tests = 0u;
@@ -151,47 +293,10 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
 
   while (true) {
-    // ------------------------------------------------------------- REGEN
     if (leader) P.ctl[kCtlFetchExt] = 0u;
-    {
-      const uint32_t nfree = P.ctl[kCtlFree];
-      for (uint32_t base = blockIdx.x * blockDim.x; base < nfree; base += gthreads) {
-        const uint32_t j = base + threadIdx.x;
-        const bool want = j < nfree;
-        const unsigned mask = __ballot_sync(0xffffffffu, want);
-        unsigned long long g0 = 0ull;
-        const int lead = __ffs(mask) - 1;
-        if (mask != 0u && static_cast<int>(lane) == lead) g0 = atomicAdd(work_next, static_cast<unsigned long long>(__popc(mask)));
-        g0 = __shfl_sync(0xffffffffu, g0, lead < 0 ? 0 : lead);
-        const unsigned long long g = g0 + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u)));
-        const bool ok = want && g < total;
-        uint32_t slot = 0u;
-        if (ok) {
-          slot = P.freel[j];
-          const uint32_t jb = find_job(jobs, job_count, g);
-          const DevJob& J = jobs[jb];
-          const uint32_t local = static_cast<uint32_t>(g - J.path_base);
-          const uint32_t sl = local / J.pixels, px = local - sl * J.pixels;
-          const uint32_t W = J.settings.width;
-          V3 o, d;
-          uint64_t rng;
-          camera_path<kParity>(J.scene, J.settings, px % W, px / W, J.first_sample + sl, o, d, rng);
-          P.job[slot] = jb;
-          P.local[slot] = local;
-          P.depth[slot] = 0u;
-          P.rng[slot] = rng;
-          P.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
-          P.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
-          P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-          P.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        const uint32_t qi = warp_append(&P.ctl[cur], ok);
-        if (ok) P.ext[cur][qi] = slot;
-      }
-    }
+    phase_regen<kParity>(jobs, job_count, total, P, cur);
     if (!grid_barrier(P.ctl)) break;
 
-    // ------------------------------------------------------------- EXTEND
     const uint32_t n_ext = P.ctl[cur];
     if (n_ext == 0u) break;   // no live path and no work left (same value in every block)
     if (leader) {
@@ -207,54 +312,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
     }
     if (!grid_barrier(P.ctl)) break;
 
-    // ------------------------------------------------------------- SHADE
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n_ext; base += gthreads) {
-      const uint32_t j = base + threadIdx.x;
-      bool next = false, shadow = false, fin = false;
-      uint32_t slot = 0u;
-      ShadeOut R;
-      if (j < n_ext) {
-        slot = P.ext[cur][j];
-        const DevJob& J = jobs[P.job[slot]];
-        const uint32_t depth = P.depth[slot];
-        const float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot], t4 = P.thr[slot], r4 = P.rad[slot];
-        const float2 h2 = P.hit[slot];
-        PathRegs pr;
-        pr.o = mk(o4.x, o4.y, o4.z);
-        pr.d = mk(d4.x, d4.y, d4.z);
-        pr.thr = mk(t4.x, t4.y, t4.z);
-        pr.rad = mk(r4.x, r4.y, r4.z);
-        pr.segs = r4.w;
-        pr.rng = P.rng[slot];
-        R = shade_bounce<kParity>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y));
-        if (R.next) {
-          P.ray_o[slot] = make_float4(pr.o.x, pr.o.y, pr.o.z, 0.0f);
-          P.ray_d[slot] = make_float4(pr.d.x, pr.d.y, pr.d.z, 0.0f);
-          P.thr[slot] = make_float4(pr.thr.x, pr.thr.y, pr.thr.z, 0.0f);
-          P.rng[slot] = pr.rng;
-          P.depth[slot] = depth + 1u;
-        }
-        P.rad[slot] = make_float4(pr.rad.x, pr.rad.y, pr.rad.z, pr.segs);
-        next = R.next;
-        fin = !R.next;
-        shadow = R.shadow;
-        shadow_tests += R.shadow_tests;
-      }
-      const uint32_t qn = warp_append(&P.ctl[cur ^ 1u], next);
-      if (next) P.ext[cur ^ 1u][qn] = slot;
-      const uint32_t qf = warp_append(&P.ctl[kCtlFin], fin);
-      if (fin) P.fin[qf] = slot;
-      const uint32_t qs = warp_append(&P.ctl[kCtlShadow], shadow);
-      if (shadow) {
-        P.shq[qs] = slot;
-        P.sh_o[qs] = make_float4(R.sh_o.x, R.sh_o.y, R.sh_o.z, R.sh_t);
-        P.sh_d[qs] = make_float4(R.sh_d.x, R.sh_d.y, R.sh_d.z, 0.0f);
-        P.sh_c[qs] = make_float4(R.sh_c.x, R.sh_c.y, R.sh_c.z, 0.0f);
-      }
-    }
+    shadow_tests += phase_shade<kParity>(jobs, P, cur, n_ext);
     if (!grid_barrier(P.ctl)) break;
 
-    // ------------------------------------------------------------- SHADOW
     {
       const uint32_t n_sh = P.ctl[kCtlShadow];
       const BatchShadowSource src{jobs, P.shq, P.job, P.sh_o, P.sh_d, P.sh_c, P.rad};
@@ -262,41 +322,99 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
     }
     if (!grid_barrier(P.ctl)) break;
 
-    // ------------------------------------------------------------- FINISH
-    {
-      const uint32_t n_fin = P.ctl[kCtlFin];
-      for (uint32_t base = blockIdx.x * blockDim.x; base < n_fin; base += gthreads) {
-        const uint32_t j = base + threadIdx.x;
-        const bool ok = j < n_fin;
-        uint32_t slot = 0u;
-        if (ok) {
-          slot = P.fin[j];
-          const DevJob& J = jobs[P.job[slot]];
-          J.staging[P.local[slot]] = P.rad[slot];
-        }
-        const uint32_t qi = warp_append(&P.ctl[kCtlFree], ok);
-        if (ok) P.freel[qi] = slot;
-      }
-    }
+    phase_finish(jobs, P);
+    if (leader) P.ctl[kCtlIter] += 1u;
     if (!grid_barrier(P.ctl)) break;
     cur ^= 1u;
   }
 
   warp_count(&ctr->shadow_tests, shadow_tests);
-  if (kStats) {
-    warp_count(&ctr->nodes, st_e.nodes);
-    warp_count(&ctr->leaves, st_e.leaves);
-    warp_count(&ctr->tris, st_e.tris);
-    warp_count(&ctr->ext_rays, st_e.rays);
-    warp_count(&ctr->shadow_nodes, st_s.nodes);
-    warp_count(&ctr->shadow_leaves, st_s.leaves);
-    warp_count(&ctr->shadow_tris, st_s.tris);
-    warp_count(&ctr->shadow_rays, st_s.rays);
-  }
+  flush_traversal_stats<kStats>(ctr, st_e, st_s);
   if (lerr) atomicOr(err, lerr);
   if (threadIdx.x == 0 && blockIdx.x == 0 && *reinterpret_cast<volatile uint32_t*>(P.ctl + kCtlAbort) != 0u) {
     atomicOr(err, 2u);   // barrier timeout
   }
+}
+
+// ------------------------------------------------------- device-driven loop
+// One kernel per stage; the stage boundary is the kernel boundary, so no
+// kernel waits on another and each stage gets its own register budget and
+// occupancy.  The extension queue index lives in ctl[kCtlCur]; the finish
+// stage flips it, decides whether another iteration is needed and sets the
+// graph's while-condition (or ctl[kCtlMore] for a host-driven loop).
+namespace {
+__device__ __forceinline__ bool block_leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
+}  // namespace
+
+template <bool kParity>
+__global__ void __launch_bounds__(256) k_loop_regen(const DevJob* __restrict__ jobs, uint32_t job_count,
+                                                    unsigned long long total, BatchPool P) {
+  const uint32_t cur = P.ctl[kCtlCur];
+  if (block_leader()) P.ctl[kCtlFetchExt] = 0u;
+  phase_regen<kParity>(jobs, job_count, total, P, cur);
+}
+
+template <bool kStats, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_loop_extend(const DevJob* __restrict__ jobs, BatchPool P, int scap,
+                                                     int2* spill, int total_cap, int steps, DevCounters* ctr,
+                                                     uint32_t* err) {
+  extern __shared__ int2 smem_stack[];
+  const uint32_t cur = P.ctl[kCtlCur];
+  const uint32_t n_ext = P.ctl[cur];
+  if (block_leader()) {
+    P.ctl[cur ^ 1u] = 0u;
+    P.ctl[kCtlShadow] = 0u;
+    P.ctl[kCtlFin] = 0u;
+    P.ctl[kCtlFree] = 0u;
+    P.ctl[kCtlFetchShadow] = 0u;
+  }
+  if (n_ext == 0u) return;
+  const TwoLevelStack stk = batch_stack(smem_stack, scap, spill, total_cap);
+  TraceStats st_e, st_s;
+  uint32_t lerr = 0u;
+  const BatchExtendSource src{jobs, P.ext[cur], P.job, P.ray_o, P.ray_d, P.hit};
+  persistent_traverse<BatchExtendSource, false, kStats>(src, n_ext, &P.ctl[kCtlFetchExt], stk, steps, st_e, lerr);
+  flush_traversal_stats<kStats>(ctr, st_e, st_s);
+  if (lerr) atomicOr(err, lerr);
+}
+
+template <bool kParity>
+__global__ void __launch_bounds__(256) k_loop_shade(const DevJob* __restrict__ jobs, BatchPool P, DevCounters* ctr) {
+  const uint32_t cur = P.ctl[kCtlCur];
+  const uint32_t n_ext = P.ctl[cur];
+  const uint32_t shadow_tests = phase_shade<kParity>(jobs, P, cur, n_ext);
+  warp_count(&ctr->shadow_tests, shadow_tests);
+}
+
+template <bool kStats, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_loop_shadow(const DevJob* __restrict__ jobs, BatchPool P, int scap,
+                                                     int2* spill, int total_cap, int steps, DevCounters* ctr,
+                                                     uint32_t* err) {
+  extern __shared__ int2 smem_stack[];
+  const uint32_t n_sh = P.ctl[kCtlShadow];
+  if (n_sh == 0u) return;
+  const TwoLevelStack stk = batch_stack(smem_stack, scap, spill, total_cap);
+  TraceStats st_e, st_s;
+  uint32_t lerr = 0u;
+  const BatchShadowSource src{jobs, P.shq, P.job, P.sh_o, P.sh_d, P.sh_c, P.rad};
+  persistent_traverse<BatchShadowSource, true, kStats>(src, n_sh, &P.ctl[kCtlFetchShadow], stk, steps, st_s, lerr);
+  flush_traversal_stats<kStats>(ctr, st_e, st_s);
+  if (lerr) atomicOr(err, lerr);
+}
+
+__global__ void __launch_bounds__(256) k_loop_finish(const DevJob* __restrict__ jobs, unsigned long long total,
+                                                     BatchPool P, cudaGraphConditionalHandle handle) {
+  if (block_leader()) {
+    // Everything this decision reads was written by earlier stages.
+    const uint32_t cur = P.ctl[kCtlCur];
+    const unsigned long long work = *reinterpret_cast<const unsigned long long*>(P.ctl + kCtlWork);
+    const uint32_t more = (P.ctl[cur ^ 1u] > 0u || work < total) ? 1u : 0u;
+    P.ctl[kCtlMore] = more;
+    P.ctl[kCtlCur] = cur ^ 1u;
+    P.ctl[kCtlIter] += 1u;
+    if (handle) cudaGraphSetConditional(handle, more);
+  }
+  phase_finish(jobs, P);
 }
 
 // Adds one job's stagings to its film, sample by sample (the reference's order).
@@ -408,6 +526,84 @@ cudaError_t LaunchStagingAccumulate(const DevJob* d_jobs, uint32_t job_count, un
   for (uint32_t j = 0; j < job_count; ++j) {
     k_staging_accumulate<<<296, 256, 0, stream>>>(d_jobs, j, ctr);
   }
+  return cudaGetLastError();
+}
+
+}  // namespace vkptc
+
+namespace vkptc {
+
+namespace {
+template <typename K>
+int blocks_per_sm(K kernel, int block, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem) != cudaSuccess) return 0;
+  return n;
+}
+
+// Traversal stage variants: [stats][occupancy variant] (at least 1..4
+// resident 256-thread blocks per SM; stats runs use the unconstrained one).
+using LoopTraceFn = void (*)(const DevJob*, BatchPool, int, int2*, int, int, DevCounters*, uint32_t*);
+LoopTraceFn loop_extend_fn(bool stats, int occ) {
+  static const LoopTraceFn t[2][4] = {
+      {k_loop_extend<false, 1>, k_loop_extend<false, 2>, k_loop_extend<false, 3>, k_loop_extend<false, 4>},
+      {k_loop_extend<true, 1>, k_loop_extend<true, 1>, k_loop_extend<true, 1>, k_loop_extend<true, 1>}};
+  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+}
+LoopTraceFn loop_shadow_fn(bool stats, int occ) {
+  static const LoopTraceFn t[2][4] = {
+      {k_loop_shadow<false, 1>, k_loop_shadow<false, 2>, k_loop_shadow<false, 3>, k_loop_shadow<false, 4>},
+      {k_loop_shadow<true, 1>, k_loop_shadow<true, 1>, k_loop_shadow<true, 1>, k_loop_shadow<true, 1>}};
+  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+}
+
+}  // namespace
+
+LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count) {
+  LoopGrids g{};
+  g.regen = sm_count * (parity ? blocks_per_sm(k_loop_regen<true>, block, 0) : blocks_per_sm(k_loop_regen<false>, block, 0));
+  g.extend = sm_count * blocks_per_sm(loop_extend_fn(stats, occupancy), block, smem);
+  g.shade = sm_count * (parity ? blocks_per_sm(k_loop_shade<true>, block, 0) : blocks_per_sm(k_loop_shade<false>, block, 0));
+  g.shadow = sm_count * blocks_per_sm(loop_shadow_fn(stats, occupancy), block, smem);
+  g.finish = sm_count * blocks_per_sm(k_loop_finish, block, 0);
+  return g;
+}
+
+cudaError_t ConfigureBatchLoopSmem(size_t bytes) {
+  const int b = static_cast<int>(bytes);
+  cudaError_t e = cudaSuccess;
+  for (int st = 0; st < 2 && e == cudaSuccess; ++st)
+    for (int o = 0; o < 4 && e == cudaSuccess; ++o) {
+      e = set_smem_attr(loop_extend_fn(st != 0, o), b);
+      if (e == cudaSuccess) e = set_smem_attr(loop_shadow_fn(st != 0, o), b);
+    }
+  return e;
+}
+
+cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
+                                     const BatchPool& P, const BatchLaunch& bl, const LoopGrids& g,
+                                     cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
+                                     cudaEvent_t* marks) {
+  const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
+  cudaStream_t s = bl.stream;
+  auto mark = [&](int i) {
+    if (marks) cudaEventRecord(marks[i], s);
+  };
+  mark(0);
+  if (bl.parity) k_loop_regen<true><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
+  else k_loop_regen<false><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
+  mark(1);
+  loop_extend_fn(bl.stats, bl.occupancy)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill,
+                                                                           bl.stack_cap, bl.steps, ctr, err);
+  mark(2);
+  if (bl.parity) k_loop_shade<true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  else k_loop_shade<false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  mark(3);
+  loop_shadow_fn(bl.stats, bl.occupancy)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill,
+                                                                           bl.stack_cap, bl.steps, ctr, err);
+  mark(4);
+  k_loop_finish<<<g.finish, bl.block, 0, s>>>(jobs, total, P, handle);
+  mark(5);
   return cudaGetLastError();
 }
 

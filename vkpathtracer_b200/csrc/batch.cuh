@@ -51,6 +51,7 @@ struct BatchLaunch {
   bool parity;
   bool stats;   // count traversal work (node/leaf/triangle visits)
   int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
+                  // (the persistent kernel; in the loop driver, its two traversal stages)
 };
 
 // Number of control words the pool needs.
@@ -71,5 +72,24 @@ cudaError_t LaunchBatchInit(const BatchPool& pool, cudaStream_t stream);
 // Resident blocks per SM of the persistent batch kernel.
 int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occupancy);
 cudaError_t ConfigureBatchSmem(size_t bytes);
+
+// Device-driven loop: the same five stages as separate kernels (each with its
+// own register budget and occupancy), one iteration enqueued per call; the
+// finish stage sets `handle` (a graph while-condition; 0 outside a graph) and
+// the pool's "iterate again" word.  Grids are resident blocks x SMs.
+struct LoopGrids {
+  int regen, extend, shade, shadow, finish;
+};
+LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count);
+cudaError_t ConfigureBatchLoopSmem(size_t bytes);
+// marks (optional, outside a graph): 6 events recorded around the five stages.
+cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
+                                     const BatchPool& pool, const BatchLaunch& bl, const LoopGrids& grids,
+                                     cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
+                                     cudaEvent_t* marks = nullptr);
+// Words of BatchPool::ctl: "iterate again" (set by the loop's finish stage)
+// and the iteration count of the last run (both drivers).
+constexpr int kBatchCtlMore = 17;
+constexpr int kBatchCtlIterations = 18;
 
 }  // namespace vkptc

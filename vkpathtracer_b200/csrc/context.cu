@@ -887,6 +887,9 @@ struct vkptc_batch {
   size_t smem_configured = 48 * 1024;
   cudaGraphExec_t graph = nullptr;
   std::string graph_key;
+  cudaStream_t body_stream = nullptr;   // captures the device-driven loop's body
+  cudaEvent_t marks[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // stage timing
+  size_t loop_smem_configured = 48 * 1024;
   vkptc_batch_stats stats{};
 };
 
@@ -977,8 +980,13 @@ int32_t batch_run_plain(vkptc_batch* b, const vkptc_batch_tuning& t) {
   return VKPTC_OK;
 }
 
-int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
+// The pool-based modes: VKPTC_BATCH_PERSISTENT (one cooperative kernel, grid
+// barriers between stages) and VKPTC_BATCH_LOOP (one kernel per stage inside
+// a CUDA graph while-node; host-driven iterations without a graph).
+int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mode) {
   const bool parity = b->config.math_mode == 0u;
+  const bool loop = mode == VKPTC_BATCH_LOOP;
+  for (double& v : b->stats.stage_ms) v = 0.0;
   // ---- jobs table and stagings
   std::vector<DevJob> table(b->jobs.size());
   unsigned long long total = 0, staging_px = 0;
@@ -1020,13 +1028,26 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
   if (smem > static_cast<size_t>(max_optin)) return bfail(b, VKPTC_UNSUPPORTED, "stack does not fit in shared memory");
-  if (smem > b->smem_configured) {
-    VKPTC_BCUDA(b, ConfigureBatchSmem(smem), "shared memory limit");
-    b->smem_configured = smem;
+  LoopGrids lg{};
+  if (loop) {
+    if (smem > b->loop_smem_configured) {
+      VKPTC_BCUDA(b, ConfigureBatchLoopSmem(smem), "shared memory limit");
+      b->loop_smem_configured = smem;
+    }
+    lg = BatchLoopGrids(bl.block, smem, parity, bl.stats, bl.occupancy, b->sm_count);
+    if (lg.regen <= 0 || lg.extend <= 0 || lg.shade <= 0 || lg.shadow <= 0 || lg.finish <= 0) {
+      return bfail(b, VKPTC_UNSUPPORTED, "a batch stage kernel does not fit on an SM with this block size");
+    }
+    bl.grid = std::max(lg.extend, lg.shadow);   // the traversal stages own the spill area
+  } else {
+    if (smem > b->smem_configured) {
+      VKPTC_BCUDA(b, ConfigureBatchSmem(smem), "shared memory limit");
+      b->smem_configured = smem;
+    }
+    const int per_sm = BatchBlocksPerSm(bl.block, smem, parity, bl.stats, bl.occupancy);
+    if (per_sm <= 0) return bfail(b, VKPTC_UNSUPPORTED, "persistent batch kernel does not fit on an SM with this block size");
+    bl.grid = per_sm * b->sm_count;
   }
-  const int per_sm = BatchBlocksPerSm(bl.block, smem, parity, bl.stats, bl.occupancy);
-  if (per_sm <= 0) return bfail(b, VKPTC_UNSUPPORTED, "persistent batch kernel does not fit on an SM with this block size");
-  bl.grid = per_sm * b->sm_count;
   const size_t spill_entries =
       bl.stack_cap > bl.smem_entries ? static_cast<size_t>(bl.grid) * bl.block * (bl.stack_cap - bl.smem_entries) : 0;
   if (spill_entries) VKPTC_BCUDA(b, b->spill.alloc(spill_entries), "spill alloc");
@@ -1073,24 +1094,66 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   P.freel = b->p_free.ptr;
   P.ctl = b->p_ctl.ptr;
 
-  // ---- the run: film clear, pool reset, one persistent launch, in-order accumulation
-  auto enqueue = [&]() -> int32_t {
+  // ---- the run: film clear, pool reset, the pool iterations, in-order accumulation
+  const uint32_t njobs = static_cast<uint32_t>(table.size());
+  auto prologue = [&]() -> int32_t {
     int32_t rc = batch_clear_films(b);
     if (rc != VKPTC_OK) return rc;
     VKPTC_BCUDA(b, cudaMemsetAsync(b->d_ctr.ptr, 0, sizeof(DevCounters), b->stream), "counter clear");
     VKPTC_BCUDA(b, LaunchBatchInit(P, b->stream), "pool init");
-    VKPTC_BCUDA(b, LaunchBatchPersistent(b->d_jobs.ptr, static_cast<uint32_t>(table.size()), total, P, bl,
-                                          b->d_ctr.ptr, b->d_err.ptr),
-                "persistent launch");
-    VKPTC_BCUDA(b, LaunchStagingAccumulate(b->d_jobs.ptr, static_cast<uint32_t>(table.size()), staging_px,
-                                            b->stream, b->d_ctr.ptr),
+    return VKPTC_OK;
+  };
+  auto epilogue = [&]() -> int32_t {
+    VKPTC_BCUDA(b, LaunchStagingAccumulate(b->d_jobs.ptr, njobs, staging_px, b->stream, b->d_ctr.ptr),
                 "staging accumulate");
     return VKPTC_OK;
+  };
+  // Everything but a host-driven loop is one stream sequence (capturable).
+  auto enqueue = [&]() -> int32_t {
+    int32_t rc = prologue();
+    if (rc != VKPTC_OK) return rc;
+    if (!loop) {
+      VKPTC_BCUDA(b, LaunchBatchPersistent(b->d_jobs.ptr, njobs, total, P, bl, b->d_ctr.ptr, b->d_err.ptr),
+                  "persistent launch");
+    } else {
+      // Inside a capture: a while-node whose body is one iteration of the stages.
+      cudaStreamCaptureStatus status;
+      cudaGraph_t cg = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      VKPTC_BCUDA(b, cudaStreamGetCaptureInfo(b->stream, &status, nullptr, &cg, &deps, &ndeps), "capture info");
+      if (status != cudaStreamCaptureStatusActive) return bfail(b, VKPTC_INTERNAL_ERROR, "loop mode needs a capture");
+      cudaGraphConditionalHandle handle;
+      VKPTC_BCUDA(b, cudaGraphConditionalHandleCreate(&handle, cg, 1u, cudaGraphCondAssignDefault), "conditional handle");
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cnode;
+      VKPTC_BCUDA(b, cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp), "while node");
+      VKPTC_BCUDA(b, cudaStreamUpdateCaptureDependencies(b->stream, &cnode, 1, cudaStreamSetCaptureDependencies),
+                  "capture dependencies");
+      if (!b->body_stream) VKPTC_BCUDA(b, cudaStreamCreateWithFlags(&b->body_stream, cudaStreamNonBlocking), "stream");
+      VKPTC_BCUDA(b, cudaStreamBeginCaptureToGraph(b->body_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeRelaxed),
+                  "body capture");
+      BatchLaunch bb = bl;
+      bb.stream = b->body_stream;
+      const cudaError_t el = LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, P, bb, lg, handle, b->d_ctr.ptr,
+                                                      b->d_err.ptr);
+      cudaGraph_t body = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(b->body_stream, &body);
+      if (el != cudaSuccess) return bcuda(b, el, "loop body");
+      if (ee != cudaSuccess) return bcuda(b, ee, "body capture");
+    }
+    return epilogue();
   };
   VKPTC_BCUDA(b, cudaMemsetAsync(b->d_err.ptr, 0, sizeof(uint32_t), b->stream), "error clear");
   bool graph_used = false;
   if (t.use_graph) {
-    const std::string key = std::to_string(cap) + "/" + std::to_string(bl.block) + "/" + std::to_string(bl.smem_entries) +
+    const std::string key = std::string(loop ? "loop/" : "persistent/") + std::to_string(cap) + "/" +
+                            std::to_string(bl.block) + "/" + std::to_string(bl.smem_entries) +
                             "/o" + std::to_string(bl.occupancy) +
                             "/" + std::to_string(bl.steps) + "/" + std::to_string(t.sample_limit) + "/" +
                             std::to_string(b->jobs.size()) + "/" +
@@ -1119,9 +1182,41 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
     VKPTC_BCUDA(b, cudaGraphLaunch(b->graph, b->stream), "graph launch");
     VKPTC_BCUDA(b, cudaEventRecord(b->ev1, b->stream), "event");
     graph_used = true;
-  } else {
+  } else if (!loop) {
     VKPTC_BCUDA(b, cudaEventRecord(b->ev0, b->stream), "event");
     const int32_t rc = enqueue();
+    if (rc != VKPTC_OK) return rc;
+    VKPTC_BCUDA(b, cudaEventRecord(b->ev1, b->stream), "event");
+  } else {
+    // Host-driven loop (no graph): one iteration per round trip; with
+    // stage_timing, CUDA events around every stage launch.
+    const bool timing = b->config.stage_timing != 0u;
+    if (timing && !b->marks[0]) {
+      for (auto& e : b->marks) VKPTC_BCUDA(b, cudaEventCreate(&e), "stage events");
+    }
+    double stage_ms[5] = {0, 0, 0, 0, 0};
+    VKPTC_BCUDA(b, cudaEventRecord(b->ev0, b->stream), "event");
+    int32_t rc = prologue();
+    if (rc != VKPTC_OK) return rc;
+    for (;;) {
+      VKPTC_BCUDA(b, LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, P, bl, lg, 0, b->d_ctr.ptr, b->d_err.ptr,
+                                              timing ? b->marks : nullptr),
+                  "loop iteration");
+      uint32_t more = 0;
+      VKPTC_BCUDA(b, cudaMemcpyAsync(&more, P.ctl + kBatchCtlMore, sizeof(more), cudaMemcpyDeviceToHost, b->stream),
+                  "loop condition");
+      VKPTC_BCUDA(b, cudaStreamSynchronize(b->stream), "loop sync");
+      if (timing) {
+        for (int i = 0; i < 5; ++i) {
+          float m = 0.0f;
+          cudaEventElapsedTime(&m, b->marks[i], b->marks[i + 1]);
+          stage_ms[i] += m;
+        }
+      }
+      if (!more) break;
+    }
+    for (int i = 0; i < 5; ++i) b->stats.stage_ms[i] = stage_ms[i];
+    rc = epilogue();
     if (rc != VKPTC_OK) return rc;
     VKPTC_BCUDA(b, cudaEventRecord(b->ev1, b->stream), "event");
   }
@@ -1134,6 +1229,9 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   if (err) return bfail(b, VKPTC_INTERNAL_ERROR, "device traversal stack overflow");
   DevCounters dc{};
   VKPTC_BCUDA(b, cudaMemcpy(&dc, b->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost), "counters");
+  uint32_t iterations = 0;
+  VKPTC_BCUDA(b, cudaMemcpy(&iterations, P.ctl + kBatchCtlIterations, sizeof(iterations), cudaMemcpyDeviceToHost),
+              "iterations");
   b->stats.segments = dc.rays;
   b->stats.shadow_rays = dc.shadow_tests;
   b->stats.ext_rays = dc.ext_rays;
@@ -1143,7 +1241,9 @@ int32_t batch_run_persistent(vkptc_batch* b, const vkptc_batch_tuning& t) {
   b->stats.shadow_nodes = dc.shadow_nodes;
   b->stats.shadow_tris = dc.shadow_tris;
   b->stats.device_ms = ms;
-  b->stats.kernel_launches = 2u + static_cast<uint64_t>(table.size());   // init, persistent, accumulate per job
+  // init, then one persistent kernel or five stage kernels per iteration, then accumulate per job
+  b->stats.kernel_launches = 1u + (loop ? 5ull * iterations : 1ull) + static_cast<uint64_t>(table.size());
+  b->stats.iterations = iterations;
   b->stats.graph_used = graph_used ? 1u : 0u;
   b->stats.grid = static_cast<uint32_t>(bl.grid);
   b->stats.block = static_cast<uint32_t>(bl.block);
@@ -1191,12 +1291,17 @@ int32_t vkptc_batch_destroy(vkptc_batch* b) {
   release_graph(b);
   for (vkptc_ctx* c : b->jobs) vkptc_destroy(c);
   b->jobs.clear();
-  cudaStream_t st = b->stream;
+  cudaStream_t st = b->stream, bs = b->body_stream;
+  cudaEvent_t marks[6];
+  std::copy(std::begin(b->marks), std::end(b->marks), marks);
   cudaEvent_t e0 = b->ev0, e1 = b->ev1;
   delete b;
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   if (st) cudaStreamDestroy(st);
+  if (bs) cudaStreamDestroy(bs);
+  for (cudaEvent_t e : marks)
+    if (e) cudaEventDestroy(e);
   return VKPTC_OK;
 }
 
@@ -1228,7 +1333,7 @@ int32_t vkptc_batch_add_job(vkptc_batch* b, const vkptc_scene_view* scene, const
 int32_t vkptc_batch_run(vkptc_batch* b, uint32_t mode, const vkptc_batch_tuning* tuning) {
   if (!b) return VKPTC_INVALID_ARGUMENT;
   if (b->jobs.empty()) return bfail(b, VKPTC_NOT_READY, "batch has no jobs");
-  if (mode > VKPTC_BATCH_PERSISTENT) return bfail(b, VKPTC_INVALID_ARGUMENT, "unknown batch mode");
+  if (mode > VKPTC_BATCH_LOOP) return bfail(b, VKPTC_INVALID_ARGUMENT, "unknown batch mode");
   cudaSetDevice(b->device);
   vkptc_batch_tuning t{};
   if (tuning) t = *tuning;
@@ -1237,7 +1342,7 @@ int32_t vkptc_batch_run(vkptc_batch* b, uint32_t mode, const vkptc_batch_tuning*
   for (vkptc_ctx* c : b->jobs) {
     b->stats.paths += static_cast<uint64_t>(c->settings.width) * c->settings.height * job_samples(c, t.sample_limit);
   }
-  const int32_t rc = mode == VKPTC_BATCH_PLAIN ? batch_run_plain(b, t) : batch_run_persistent(b, t);
+  const int32_t rc = mode == VKPTC_BATCH_PLAIN ? batch_run_plain(b, t) : batch_run_pool(b, t, mode);
   if (rc == VKPTC_OK) b->last_error.clear();
   return rc;
 }

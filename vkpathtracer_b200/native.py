@@ -99,13 +99,15 @@ class BatchStats(ctypes.Structure):
                 ("segments", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("device_ms", ctypes.c_double), ("grid", ctypes.c_uint32),
                 ("block", ctypes.c_uint32), ("pool_paths", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
-                ("steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("steps", ctypes.c_uint32), ("iterations", ctypes.c_uint32),
                 ("ext_rays", ctypes.c_uint64), ("ext_nodes", ctypes.c_uint64), ("ext_tris", ctypes.c_uint64),
                 ("shadow_queries", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64),
-                ("shadow_tris", ctypes.c_uint64)]
+                ("shadow_tris", ctypes.c_uint64), ("stage_ms", ctypes.c_double * 5)]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+        d = {n: getattr(self, n) for n, _ in self._fields_ if n not in ("reserved", "stage_ms")}
+        d["stage_ms"] = dict(zip(("regen", "extend", "shade", "shadow", "finish"), list(self.stage_ms)))
+        return d
 
 
 class AdjointDesc(ctypes.Structure):
@@ -176,7 +178,7 @@ SIGNATURES = {
     "vkptc_adjoint_read_samples": (I32, [P, P, P]),
     "vkptc_adjoint_get_stats": (I32, [P, ctypes.POINTER(AdjointStats)]),
 }
-BATCH_PLAIN, BATCH_PERSISTENT = 0, 1
+BATCH_PLAIN, BATCH_PERSISTENT, BATCH_LOOP = 0, 1, 2
 NOALLOC_MAX_PATHS = 65536
 
 _LIB = None

@@ -377,12 +377,14 @@ class BatchRenderer:
     device work queue, replayed from a CUDA graph.  Films are bit-identical.
     """
 
-    def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False, bvh: str = "reference"):
+    def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False, bvh: str = "reference",
+                 stage_timing: bool = False):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
         cfg.math_mode = math_mode
         cfg.collect_stats = int(collect_stats)
+        cfg.stage_timing = int(stage_timing)
         cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
         h = ctypes.c_void_p()
         rc = self._lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(h))
@@ -424,7 +426,10 @@ class BatchRenderer:
     def run(self, mode: str = "persistent", pool_paths: int = 0, block_size: int = 0, stack_depth: int = 0,
             steps: int = 0, sample_limit: int = 0, use_graph: bool = True, occupancy: int = 0) -> dict:
         t = native.BatchTuning(pool_paths, block_size, stack_depth, steps, sample_limit, int(use_graph), occupancy)
-        m = native.BATCH_PERSISTENT if mode == "persistent" else native.BATCH_PLAIN
+        modes = {"plain": native.BATCH_PLAIN, "persistent": native.BATCH_PERSISTENT, "loop": native.BATCH_LOOP}
+        if mode not in modes:
+            raise ValueError(f"mode must be one of {sorted(modes)}")
+        m = modes[mode]
         rc = self._lib.vkptc_batch_run(self._b, m, ctypes.byref(t))
         if rc != native.OK:
             raise native.VkptcError(rc, self._err())
