@@ -41,7 +41,7 @@ WORKLOAD = "batch_64_uneven_jobs"
 NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
 PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
 # DRAM bytes (read + write) per extension ray of k_loop_extend, from one ncu
-# capture of the 4-job case (profiles/k_loop_extend_batch_4_jobs.md).
+# capture of the 4-job case (profiles/k_lp_extend_batch_4_jobs.md).
 TRAFFIC_BYTES_PER_EXT_RAY = 0.0
 
 
@@ -477,11 +477,11 @@ def run_ours(args, world, rank, local):
             iters = max(1, tt["iterations"])
             achieved = alg / (stage["extend"] / 1e3) / 1e9
             traffic = TRAFFIC_BYTES_PER_EXT_RAY * ss["ext_rays"] / iters
-            roof = {"kernel": "k_loop_extend (closest-hit traversal stage of the loop driver)", "bound": "hbm",
+            roof = {"kernel": "k_lp_extend (closest-hit traversal stage of the loop driver)", "bound": "hbm",
                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                     "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": traffic,
                     "traffic_note": "per launch: DRAM bytes per extension ray from the ncu capture of the 4-job "
-                                    "case (profiles/k_loop_extend_batch_4_jobs.md) x extension rays per launch",
+                                    "case (profiles/k_lp_extend_batch_4_jobs.md) x extension rays per launch",
                     "alg_bytes_per_launch": alg / iters, "avg_launch_ms": stage["extend"] / iters,
                     "launches": iters, "stage_ms": stage,
                     "stage_share": {k: v / max(1e-9, sum(stage.values())) for k, v in stage.items()},

@@ -18,11 +18,11 @@ import os
 import time
 from typing import Dict, Iterable, Optional
 
-DEFAULT_POOLS = (1 << 19, 1 << 20, 1 << 21, 1 << 22)
+DEFAULT_POOLS = (1 << 20, 1 << 21, 1 << 22, 1 << 23)
 DEFAULT_BLOCKS = (128, 256)
-DEFAULT_STACKS = (8, 16, 24)
-DEFAULT_STEPS = (4, 8)
-DEFAULT_OCCUPANCY = (0, 1, 2, 3)
+DEFAULT_STACKS = (8, 16)
+DEFAULT_STEPS = (8, 16)
+DEFAULT_OCCUPANCY = (1, 2, 3)
 
 
 def cache_path() -> str:

@@ -35,7 +35,7 @@ constexpr int kCtlExt0 = 0, kCtlExt1 = 1, kCtlShadow = 2, kCtlFin = 3, kCtlFree 
 constexpr int kCtlFetchExt = 5, kCtlFetchShadow = 6;
 constexpr int kCtlWork = 8;      // 64-bit path counter (words 8, 9)
 constexpr int kCtlBarCount = 12, kCtlBarGen = 13, kCtlAbort = 15;
-constexpr int kCtlCur = 16, kCtlMore = kBatchCtlMore, kCtlIter = kBatchCtlIterations;   // loop driver words
+constexpr int kCtlIter = kBatchCtlIterations;
 constexpr unsigned kBarrierSpinLimit = 1u << 26;   // x ~128 ns sleeps: ~8.6 s
 
 __device__ __forceinline__ bool grid_barrier(uint32_t* ctl) {
@@ -66,20 +66,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* ctl) {
   return *reinterpret_cast<volatile uint32_t*>(ctl + kCtlAbort) == 0u;
 }
 
-__device__ __forceinline__ uint32_t find_job(const DevJob* jobs, uint32_t count, unsigned long long g) {
-  uint32_t lo = 0u, hi = count;
-  while (hi - lo > 1u) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (jobs[mid].path_base <= g) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ GeoView job_geo(const DevJob* jobs, uint32_t j) {
-  const DevScene& s = jobs[j].scene;
-  return GeoView{s.nodes, s.tris, s.tie, s.prim_count};
-}
+__device__ __forceinline__ GeoView job_geo(const DevJob* jobs, uint32_t j) { return geo_of(jobs[j].scene); }
 
 struct BatchExtendSource {
   const DevJob* jobs;
@@ -130,10 +117,9 @@ struct BatchShadowSource {
 };
 
 // ------------------------------------------------------------------ phases
-// The five stages of one iteration over the pool.  Both drivers run them:
-// the cooperative persistent kernel (grid barriers between stages) and the
-// device-driven loop (one kernel per stage, a CUDA graph while-node around
-// them).  Each is grid-stride over a device-side count.
+// The five stages of one iteration over the pool, separated by grid
+// barriers in the persistent kernel.  Each is grid-stride over a device-side
+// count.
 
 // REGEN: free slots take the next path ids of the work queue, generate the
 // camera ray and append to the extension queue `cur`.
@@ -336,87 +322,6 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
   }
 }
 
-// ------------------------------------------------------- device-driven loop
-// One kernel per stage; the stage boundary is the kernel boundary, so no
-// kernel waits on another and each stage gets its own register budget and
-// occupancy.  The extension queue index lives in ctl[kCtlCur]; the finish
-// stage flips it, decides whether another iteration is needed and sets the
-// graph's while-condition (or ctl[kCtlMore] for a host-driven loop).
-namespace {
-__device__ __forceinline__ bool block_leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
-}  // namespace
-
-template <bool kParity>
-__global__ void __launch_bounds__(256) k_loop_regen(const DevJob* __restrict__ jobs, uint32_t job_count,
-                                                    unsigned long long total, BatchPool P) {
-  const uint32_t cur = P.ctl[kCtlCur];
-  if (block_leader()) P.ctl[kCtlFetchExt] = 0u;
-  phase_regen<kParity>(jobs, job_count, total, P, cur);
-}
-
-template <bool kStats, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) k_loop_extend(const DevJob* __restrict__ jobs, BatchPool P, int scap,
-                                                     int2* spill, int total_cap, int steps, DevCounters* ctr,
-                                                     uint32_t* err) {
-  extern __shared__ int2 smem_stack[];
-  const uint32_t cur = P.ctl[kCtlCur];
-  const uint32_t n_ext = P.ctl[cur];
-  if (block_leader()) {
-    P.ctl[cur ^ 1u] = 0u;
-    P.ctl[kCtlShadow] = 0u;
-    P.ctl[kCtlFin] = 0u;
-    P.ctl[kCtlFree] = 0u;
-    P.ctl[kCtlFetchShadow] = 0u;
-  }
-  if (n_ext == 0u) return;
-  const TwoLevelStack stk = batch_stack(smem_stack, scap, spill, total_cap);
-  TraceStats st_e, st_s;
-  uint32_t lerr = 0u;
-  const BatchExtendSource src{jobs, P.ext[cur], P.job, P.ray_o, P.ray_d, P.hit};
-  persistent_traverse<BatchExtendSource, false, kStats>(src, n_ext, &P.ctl[kCtlFetchExt], stk, steps, st_e, lerr);
-  flush_traversal_stats<kStats>(ctr, st_e, st_s);
-  if (lerr) atomicOr(err, lerr);
-}
-
-template <bool kParity>
-__global__ void __launch_bounds__(256) k_loop_shade(const DevJob* __restrict__ jobs, BatchPool P, DevCounters* ctr) {
-  const uint32_t cur = P.ctl[kCtlCur];
-  const uint32_t n_ext = P.ctl[cur];
-  const uint32_t shadow_tests = phase_shade<kParity>(jobs, P, cur, n_ext);
-  warp_count(&ctr->shadow_tests, shadow_tests);
-}
-
-template <bool kStats, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) k_loop_shadow(const DevJob* __restrict__ jobs, BatchPool P, int scap,
-                                                     int2* spill, int total_cap, int steps, DevCounters* ctr,
-                                                     uint32_t* err) {
-  extern __shared__ int2 smem_stack[];
-  const uint32_t n_sh = P.ctl[kCtlShadow];
-  if (n_sh == 0u) return;
-  const TwoLevelStack stk = batch_stack(smem_stack, scap, spill, total_cap);
-  TraceStats st_e, st_s;
-  uint32_t lerr = 0u;
-  const BatchShadowSource src{jobs, P.shq, P.job, P.sh_o, P.sh_d, P.sh_c, P.rad};
-  persistent_traverse<BatchShadowSource, true, kStats>(src, n_sh, &P.ctl[kCtlFetchShadow], stk, steps, st_s, lerr);
-  flush_traversal_stats<kStats>(ctr, st_e, st_s);
-  if (lerr) atomicOr(err, lerr);
-}
-
-__global__ void __launch_bounds__(256) k_loop_finish(const DevJob* __restrict__ jobs, unsigned long long total,
-                                                     BatchPool P, cudaGraphConditionalHandle handle) {
-  if (block_leader()) {
-    // Everything this decision reads was written by earlier stages.
-    const uint32_t cur = P.ctl[kCtlCur];
-    const unsigned long long work = *reinterpret_cast<const unsigned long long*>(P.ctl + kCtlWork);
-    const uint32_t more = (P.ctl[cur ^ 1u] > 0u || work < total) ? 1u : 0u;
-    P.ctl[kCtlMore] = more;
-    P.ctl[kCtlCur] = cur ^ 1u;
-    P.ctl[kCtlIter] += 1u;
-    if (handle) cudaGraphSetConditional(handle, more);
-  }
-  phase_finish(jobs, P);
-}
-
 // Adds one job's stagings to its film, sample by sample (the reference's order).
 __global__ void __launch_bounds__(256) k_staging_accumulate(const DevJob* jobs, uint32_t jb, DevCounters* ctr) {
   const DevJob& J = jobs[jb];
@@ -531,80 +436,3 @@ cudaError_t LaunchStagingAccumulate(const DevJob* d_jobs, uint32_t job_count, un
 
 }  // namespace vkptc
 
-namespace vkptc {
-
-namespace {
-template <typename K>
-int blocks_per_sm(K kernel, int block, size_t smem) {
-  int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem) != cudaSuccess) return 0;
-  return n;
-}
-
-// Traversal stage variants: [stats][occupancy variant] (at least 1..4
-// resident 256-thread blocks per SM; stats runs use the unconstrained one).
-using LoopTraceFn = void (*)(const DevJob*, BatchPool, int, int2*, int, int, DevCounters*, uint32_t*);
-LoopTraceFn loop_extend_fn(bool stats, int occ) {
-  static const LoopTraceFn t[2][4] = {
-      {k_loop_extend<false, 1>, k_loop_extend<false, 2>, k_loop_extend<false, 3>, k_loop_extend<false, 4>},
-      {k_loop_extend<true, 1>, k_loop_extend<true, 1>, k_loop_extend<true, 1>, k_loop_extend<true, 1>}};
-  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
-}
-LoopTraceFn loop_shadow_fn(bool stats, int occ) {
-  static const LoopTraceFn t[2][4] = {
-      {k_loop_shadow<false, 1>, k_loop_shadow<false, 2>, k_loop_shadow<false, 3>, k_loop_shadow<false, 4>},
-      {k_loop_shadow<true, 1>, k_loop_shadow<true, 1>, k_loop_shadow<true, 1>, k_loop_shadow<true, 1>}};
-  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
-}
-
-}  // namespace
-
-LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count) {
-  LoopGrids g{};
-  g.regen = sm_count * (parity ? blocks_per_sm(k_loop_regen<true>, block, 0) : blocks_per_sm(k_loop_regen<false>, block, 0));
-  g.extend = sm_count * blocks_per_sm(loop_extend_fn(stats, occupancy), block, smem);
-  g.shade = sm_count * (parity ? blocks_per_sm(k_loop_shade<true>, block, 0) : blocks_per_sm(k_loop_shade<false>, block, 0));
-  g.shadow = sm_count * blocks_per_sm(loop_shadow_fn(stats, occupancy), block, smem);
-  g.finish = sm_count * blocks_per_sm(k_loop_finish, block, 0);
-  return g;
-}
-
-cudaError_t ConfigureBatchLoopSmem(size_t bytes) {
-  const int b = static_cast<int>(bytes);
-  cudaError_t e = cudaSuccess;
-  for (int st = 0; st < 2 && e == cudaSuccess; ++st)
-    for (int o = 0; o < 4 && e == cudaSuccess; ++o) {
-      e = set_smem_attr(loop_extend_fn(st != 0, o), b);
-      if (e == cudaSuccess) e = set_smem_attr(loop_shadow_fn(st != 0, o), b);
-    }
-  return e;
-}
-
-cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
-                                     const BatchPool& P, const BatchLaunch& bl, const LoopGrids& g,
-                                     cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
-                                     cudaEvent_t* marks) {
-  const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
-  cudaStream_t s = bl.stream;
-  auto mark = [&](int i) {
-    if (marks) cudaEventRecord(marks[i], s);
-  };
-  mark(0);
-  if (bl.parity) k_loop_regen<true><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
-  else k_loop_regen<false><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
-  mark(1);
-  loop_extend_fn(bl.stats, bl.occupancy)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill,
-                                                                           bl.stack_cap, bl.steps, ctr, err);
-  mark(2);
-  if (bl.parity) k_loop_shade<true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
-  else k_loop_shade<false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
-  mark(3);
-  loop_shadow_fn(bl.stats, bl.occupancy)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill,
-                                                                           bl.stack_cap, bl.steps, ctr, err);
-  mark(4);
-  k_loop_finish<<<g.finish, bl.block, 0, s>>>(jobs, total, P, handle);
-  mark(5);
-  return cudaGetLastError();
-}
-
-}  // namespace vkptc

@@ -54,8 +54,23 @@ struct BatchLaunch {
                   // (the persistent kernel; in the loop driver, its two traversal stages)
 };
 
-// Number of control words the pool needs.
+// Number of control words the pool needs; word kBatchCtlIterations holds the
+// iteration count of the last run.
 constexpr int kBatchCtlWords = 32;
+constexpr int kBatchCtlIterations = 18;
+
+#ifdef __CUDACC__
+// Job of global path id g (jobs sorted by path_base).
+__device__ __forceinline__ uint32_t find_job(const DevJob* jobs, uint32_t count, unsigned long long g) {
+  uint32_t lo = 0u, hi = count;
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].path_base <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+#endif
 
 // Runs every job to completion in one cooperative launch (fills the stagings),
 // then accumulates each job's stagings into its film in sample order.
@@ -73,23 +88,57 @@ cudaError_t LaunchBatchInit(const BatchPool& pool, cudaStream_t stream);
 int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occupancy);
 cudaError_t ConfigureBatchSmem(size_t bytes);
 
-// Device-driven loop: the same five stages as separate kernels (each with its
-// own register budget and occupancy), one iteration enqueued per call; the
-// finish stage sets `handle` (a graph while-condition; 0 outside a graph) and
-// the pool's "iterate again" word.  Grids are resident blocks x SMs.
+// ------------------------------------------------------------ loop driver
+// The same five stages as separate kernels (each with its own register
+// budget and occupancy) in a CUDA graph while-node that the device keeps
+// iterating until the work queue is empty (batch_loop.cu).  Path state lives
+// in two compacted generations: the extension stage reads generation `cur`
+// by position, shading appends surviving paths to the other generation,
+// shadow queries to a queue that names their destination, and finished paths
+// to a list the finish stage moves into the stagings -- every access is by
+// queue position, so loads and stores coalesce.
+struct PathSoA {
+  uint32_t* job;
+  uint32_t* local;                // sample_local * pixels + pixel
+  uint32_t* depth;
+  uint64_t* rng;
+  float4* o;
+  float4* d;
+  float4* thr;
+  float4* rad;                    // w = segments
+};
+
+struct LoopPool {
+  uint32_t capacity;              // paths per generation ("queue capacity")
+  PathSoA gen[2];
+  float2* hit;                    // per position of the current generation
+  float4* sh_o;                   // origin, max distance
+  float4* sh_d;                   // direction, job (bits)
+  float4* sh_c;                   // contribution when visible
+  uint32_t* sh_dst;               // position in the next generation, or kLoopFinBit | finished-list position
+  float4* fin_rad;
+  uint32_t* fin_job;
+  uint32_t* fin_local;
+  uint32_t* ctl;                  // control words (kLoopCtl*)
+};
+
+constexpr uint32_t kLoopFinBit = 0x80000000u;
+constexpr int kLoopCtlWords = 32;
+constexpr int kLoopCtlMore = 17;        // 1 while another iteration is needed
+constexpr int kLoopCtlIterations = 18;  // iterations of the last run
+
 struct LoopGrids {
   int regen, extend, shade, shadow, finish;
 };
 LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count);
 cudaError_t ConfigureBatchLoopSmem(size_t bytes);
-// marks (optional, outside a graph): 6 events recorded around the five stages.
+cudaError_t LaunchBatchLoopInit(const LoopPool& pool, cudaStream_t stream);
+// One iteration of the five stages; the finish stage sets `handle` (the
+// graph's while-condition; 0 outside a graph) and ctl[kLoopCtlMore].
+// marks (optional, outside a graph): 6 events recorded around the stages.
 cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
-                                     const BatchPool& pool, const BatchLaunch& bl, const LoopGrids& grids,
+                                     const LoopPool& pool, const BatchLaunch& bl, const LoopGrids& grids,
                                      cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
                                      cudaEvent_t* marks = nullptr);
-// Words of BatchPool::ctl: "iterate again" (set by the loop's finish stage)
-// and the iteration count of the last run (both drivers).
-constexpr int kBatchCtlMore = 17;
-constexpr int kBatchCtlIterations = 18;
 
 }  // namespace vkptc

@@ -1,0 +1,362 @@
+// batch_loop.cu -- the loop driver of the batched renderer.
+//
+// The persistent driver (batch.cu) runs the five stages of an iteration in
+// one cooperative kernel with grid barriers between them.  This driver runs
+// each stage as its own kernel, so a stage gets the register budget and
+// occupancy it needs (the traversal stages run at 64-80 registers, shading at
+// ~94), and the iterations are driven by the device: the stages form the body
+// of a CUDA graph while-node whose condition the finish stage sets.  One
+// graph launch renders every job; no kernel ever waits on another.
+//
+// Path state is kept in two compacted generations (structure of arrays).
+// Each iteration:
+//   REGEN   new camera paths from the 64-bit work counter are appended to
+//           generation `cur` until it holds `capacity` paths
+//   EXTEND  closest-hit traversal of generation `cur`, hit by position
+//   SHADE   one bounce per path: survivors appended to generation cur^1,
+//           NEE queries to the shadow queue (with their destination), ended
+//           paths to the finished list
+//   SHADOW  any-hit traversal; a visible query adds its term at its destination
+//   FINISH  finished paths' radiance to the job's staging slot; cur ^= 1
+// Positions are warp-aggregated appends, so every access coalesces.  The
+// stagings are added to the films in sample order afterwards (as in the
+// persistent driver), so films are bit-identical across drivers.
+#include "batch.cuh"
+#include "integrator.cuh"
+#include "traverse.cuh"
+
+namespace vkptc {
+
+namespace {
+
+constexpr int kLCur = 0;            // current generation
+constexpr int kLCount0 = 1;         // paths in generation 0 / 1: words 1, 2
+constexpr int kLShadow = 3, kLFin = 4;
+constexpr int kLFetchExt = 5, kLFetchShadow = 6;
+constexpr int kLWork = 8;           // 64-bit path counter (words 8, 9)
+constexpr int kLBase = 10;          // paths in generation `cur` when its REGEN starts
+constexpr int kLMore = kLoopCtlMore, kLIter = kLoopCtlIterations;
+
+__device__ __forceinline__ bool block_leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
+
+__device__ __forceinline__ GeoView job_geo(const DevJob* jobs, uint32_t j) { return geo_of(jobs[j].scene); }
+
+struct LoopExtendSource {
+  const DevJob* jobs;
+  PathSoA A;
+  float2* hit;
+  __device__ __forceinline__ void load(uint32_t j, V3& o, V3& d, float& tm, GeoView& g) const {
+    g = job_geo(jobs, A.job[j]);
+    const float4 a = A.o[j], b = A.d[j];
+    o = mk(a.x, a.y, a.z);
+    d = mk(b.x, b.y, b.z);
+    tm = kInf;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, float t, uint32_t prim) const {
+    hit[j] = make_float2(t, __uint_as_float(prim));
+  }
+};
+
+struct LoopShadowSource {
+  const DevJob* jobs;
+  LoopPool P;
+  PathSoA B;   // the next generation (destinations of surviving paths)
+  __device__ __forceinline__ void load(uint32_t j, V3& o, V3& d, float& tm, GeoView& g) const {
+    const float4 a = P.sh_o[j], b = P.sh_d[j];
+    g = job_geo(jobs, __float_as_uint(b.w));
+    o = mk(a.x, a.y, a.z);
+    d = mk(b.x, b.y, b.z);
+    tm = a.w;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, float, uint32_t occluded) const {
+    if (occluded) return;
+    const uint32_t dst = P.sh_dst[j];
+    const float4 c = P.sh_c[j];
+    float4* r = (dst & kLoopFinBit) ? P.fin_rad + (dst & ~kLoopFinBit) : B.rad + dst;
+    float4 v = *r;
+    v.x = v.x + c.x;
+    v.y = v.y + c.y;
+    v.z = v.z + c.z;
+    *r = v;
+  }
+};
+
+__device__ __forceinline__ TwoLevelStack loop_stack(int2* smem_stack, int scap, int2* spill, int total_cap) {
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  return TwoLevelStack{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), scap,
+                       spill ? spill + gtid : nullptr, static_cast<int>(gthreads), total_cap};
+}
+
+template <bool kStats>
+__device__ __forceinline__ void flush_stats(DevCounters* ctr, const TraceStats& st, bool shadow) {
+  if (!kStats) return;
+  if (shadow) {
+    warp_count(&ctr->shadow_nodes, st.nodes);
+    warp_count(&ctr->shadow_leaves, st.leaves);
+    warp_count(&ctr->shadow_tris, st.tris);
+    warp_count(&ctr->shadow_rays, st.rays);
+  } else {
+    warp_count(&ctr->nodes, st.nodes);
+    warp_count(&ctr->leaves, st.leaves);
+    warp_count(&ctr->tris, st.tris);
+    warp_count(&ctr->ext_rays, st.rays);
+  }
+}
+
+// ---------------------------------------------------------------- stages
+__global__ void k_lp_init(uint32_t* ctl) {
+  const uint32_t i = threadIdx.x;
+  if (i < static_cast<uint32_t>(kLoopCtlWords)) ctl[i] = 0u;
+}
+
+template <bool kParity>
+__global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ jobs, uint32_t job_count,
+                                                  unsigned long long total, LoopPool P) {
+  const uint32_t cur = P.ctl[kLCur];
+  uint32_t* count = P.ctl + kLCount0 + cur;
+  // The count itself grows while this kernel appends; every block sizes its
+  // share from the value the previous finish stage recorded.
+  const uint32_t room = P.capacity - P.ctl[kLBase];
+  if (block_leader()) P.ctl[kLFetchExt] = 0u;
+  const PathSoA A = P.gen[cur];
+  unsigned long long* work_next = reinterpret_cast<unsigned long long*>(P.ctl + kLWork);
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < room; base += gthreads) {
+    const uint32_t j = base + threadIdx.x;
+    const bool want = j < room;
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    unsigned long long g0 = 0ull;
+    const int lead = __ffs(mask) - 1;
+    if (mask != 0u && static_cast<int>(lane) == lead) g0 = atomicAdd(work_next, static_cast<unsigned long long>(__popc(mask)));
+    g0 = __shfl_sync(0xffffffffu, g0, lead < 0 ? 0 : lead);
+    const unsigned long long g = g0 + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u)));
+    const bool ok = want && g < total;
+    const uint32_t q = warp_append(count, ok);
+    if (ok) {
+      const uint32_t jb = find_job(jobs, job_count, g);
+      const DevJob& J = jobs[jb];
+      const uint32_t local = static_cast<uint32_t>(g - J.path_base);
+      const uint32_t sl = local / J.pixels, px = local - sl * J.pixels;
+      const uint32_t W = J.settings.width;
+      V3 o, d;
+      uint64_t rng;
+      camera_path<kParity>(J.scene, J.settings, px % W, px / W, J.first_sample + sl, o, d, rng);
+      A.job[q] = jb;
+      A.local[q] = local;
+      A.depth[q] = 0u;
+      A.rng[q] = rng;
+      A.o[q] = make_float4(o.x, o.y, o.z, 0.0f);
+      A.d[q] = make_float4(d.x, d.y, d.z, 0.0f);
+      A.thr[q] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+      A.rad[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+  }
+}
+
+template <bool kStats, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __restrict__ jobs, LoopPool P, int scap,
+                                                               int2* spill, int total_cap, int steps, DevCounters* ctr,
+                                                               uint32_t* err) {
+  extern __shared__ int2 smem_stack[];
+  const uint32_t cur = P.ctl[kLCur];
+  const uint32_t n = P.ctl[kLCount0 + cur];
+  if (block_leader()) {
+    P.ctl[kLCount0 + (cur ^ 1u)] = 0u;
+    P.ctl[kLShadow] = 0u;
+    P.ctl[kLFin] = 0u;
+    P.ctl[kLFetchShadow] = 0u;
+  }
+  if (n == 0u) return;
+  const TwoLevelStack stk = loop_stack(smem_stack, scap, spill, total_cap);
+  TraceStats st;
+  uint32_t lerr = 0u;
+  const LoopExtendSource src{jobs, P.gen[cur], P.hit};
+  persistent_traverse<LoopExtendSource, false, kStats>(src, n, &P.ctl[kLFetchExt], stk, steps, st, lerr);
+  flush_stats<kStats>(ctr, st, false);
+  if (lerr) atomicOr(err, lerr);
+}
+
+template <bool kParity>
+__global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr) {
+  const uint32_t cur = P.ctl[kLCur];
+  const uint32_t n = P.ctl[kLCount0 + cur];
+  const PathSoA A = P.gen[cur], B = P.gen[cur ^ 1u];
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  uint32_t shadow_tests = 0u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gthreads) {
+    const uint32_t j = base + threadIdx.x;
+    bool next = false, shadow = false, fin = false;
+    uint32_t jb = 0u, local = 0u, depth = 0u;
+    PathRegs pr;
+    ShadeOut R;
+    if (j < n) {
+      jb = A.job[j];
+      local = A.local[j];
+      depth = A.depth[j];
+      const DevJob& J = jobs[jb];
+      const float4 o4 = A.o[j], d4 = A.d[j], t4 = A.thr[j], r4 = A.rad[j];
+      const float2 h2 = P.hit[j];
+      pr.o = mk(o4.x, o4.y, o4.z);
+      pr.d = mk(d4.x, d4.y, d4.z);
+      pr.thr = mk(t4.x, t4.y, t4.z);
+      pr.rad = mk(r4.x, r4.y, r4.z);
+      pr.segs = r4.w;
+      pr.rng = A.rng[j];
+      R = shade_bounce<kParity>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y));
+      next = R.next;
+      fin = !R.next;
+      shadow = R.shadow;
+      shadow_tests += R.shadow_tests;
+    }
+    const uint32_t qn = warp_append(&P.ctl[kLCount0 + (cur ^ 1u)], next);
+    if (next) {
+      B.job[qn] = jb;
+      B.local[qn] = local;
+      B.depth[qn] = depth + 1u;
+      B.rng[qn] = pr.rng;
+      B.o[qn] = make_float4(pr.o.x, pr.o.y, pr.o.z, 0.0f);
+      B.d[qn] = make_float4(pr.d.x, pr.d.y, pr.d.z, 0.0f);
+      B.thr[qn] = make_float4(pr.thr.x, pr.thr.y, pr.thr.z, 0.0f);
+      B.rad[qn] = make_float4(pr.rad.x, pr.rad.y, pr.rad.z, pr.segs);
+    }
+    const uint32_t qf = warp_append(&P.ctl[kLFin], fin);
+    if (fin) {
+      P.fin_rad[qf] = make_float4(pr.rad.x, pr.rad.y, pr.rad.z, pr.segs);
+      P.fin_job[qf] = jb;
+      P.fin_local[qf] = local;
+    }
+    const uint32_t qs = warp_append(&P.ctl[kLShadow], shadow);
+    if (shadow) {
+      P.sh_o[qs] = make_float4(R.sh_o.x, R.sh_o.y, R.sh_o.z, R.sh_t);
+      P.sh_d[qs] = make_float4(R.sh_d.x, R.sh_d.y, R.sh_d.z, __uint_as_float(jb));
+      P.sh_c[qs] = make_float4(R.sh_c.x, R.sh_c.y, R.sh_c.z, 0.0f);
+      P.sh_dst[qs] = next ? qn : (qf | kLoopFinBit);
+    }
+  }
+  warp_count(&ctr->shadow_tests, shadow_tests);
+}
+
+template <bool kStats, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_lp_shadow(const DevJob* __restrict__ jobs, LoopPool P, int scap,
+                                                               int2* spill, int total_cap, int steps, DevCounters* ctr,
+                                                               uint32_t* err) {
+  extern __shared__ int2 smem_stack[];
+  const uint32_t n = P.ctl[kLShadow];
+  if (n == 0u) return;
+  const uint32_t cur = P.ctl[kLCur];
+  const TwoLevelStack stk = loop_stack(smem_stack, scap, spill, total_cap);
+  TraceStats st;
+  uint32_t lerr = 0u;
+  const LoopShadowSource src{jobs, P, P.gen[cur ^ 1u]};
+  persistent_traverse<LoopShadowSource, true, kStats>(src, n, &P.ctl[kLFetchShadow], stk, steps, st, lerr);
+  flush_stats<kStats>(ctr, st, true);
+  if (lerr) atomicOr(err, lerr);
+}
+
+__global__ void __launch_bounds__(256) k_lp_finish(const DevJob* __restrict__ jobs, unsigned long long total,
+                                                   LoopPool P, cudaGraphConditionalHandle handle) {
+  const uint32_t cur = P.ctl[kLCur];
+  if (block_leader()) {
+    // Everything this decision reads was final before this kernel started.
+    const unsigned long long work = *reinterpret_cast<const unsigned long long*>(P.ctl + kLWork);
+    const uint32_t survivors = P.ctl[kLCount0 + (cur ^ 1u)];
+    const uint32_t more = (survivors > 0u || work < total) ? 1u : 0u;
+    P.ctl[kLMore] = more;
+    P.ctl[kLBase] = survivors;
+    P.ctl[kLCur] = cur ^ 1u;
+    P.ctl[kLIter] += 1u;
+    if (handle) cudaGraphSetConditional(handle, more);
+  }
+  const uint32_t n = P.ctl[kLFin];
+  for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
+    const DevJob& J = jobs[P.fin_job[f]];
+    J.staging[P.fin_local[f]] = P.fin_rad[f];
+  }
+}
+
+template <typename K>
+int blocks_per_sm(K kernel, int block, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem) != cudaSuccess) return 0;
+  return n;
+}
+
+template <typename K>
+cudaError_t set_smem_attr(K kernel, int bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// Traversal stage variants: [stats][register variant] (at least 1..4
+// resident 256-thread blocks per SM; stats runs use the unconstrained one).
+using LoopTraceFn = void (*)(const DevJob*, LoopPool, int, int2*, int, int, DevCounters*, uint32_t*);
+LoopTraceFn extend_fn(bool stats, int occ) {
+  static const LoopTraceFn t[2][4] = {
+      {k_lp_extend<false, 1>, k_lp_extend<false, 2>, k_lp_extend<false, 3>, k_lp_extend<false, 4>},
+      {k_lp_extend<true, 1>, k_lp_extend<true, 1>, k_lp_extend<true, 1>, k_lp_extend<true, 1>}};
+  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+}
+LoopTraceFn shadow_fn(bool stats, int occ) {
+  static const LoopTraceFn t[2][4] = {
+      {k_lp_shadow<false, 1>, k_lp_shadow<false, 2>, k_lp_shadow<false, 3>, k_lp_shadow<false, 4>},
+      {k_lp_shadow<true, 1>, k_lp_shadow<true, 1>, k_lp_shadow<true, 1>, k_lp_shadow<true, 1>}};
+  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+}
+
+}  // namespace
+
+LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count) {
+  LoopGrids g{};
+  g.regen = sm_count * (parity ? blocks_per_sm(k_lp_regen<true>, block, 0) : blocks_per_sm(k_lp_regen<false>, block, 0));
+  g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy), block, smem);
+  g.shade = sm_count * (parity ? blocks_per_sm(k_lp_shade<true>, block, 0) : blocks_per_sm(k_lp_shade<false>, block, 0));
+  g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy), block, smem);
+  g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
+  return g;
+}
+
+cudaError_t ConfigureBatchLoopSmem(size_t bytes) {
+  const int b = static_cast<int>(bytes);
+  cudaError_t e = cudaSuccess;
+  for (int st = 0; st < 2 && e == cudaSuccess; ++st)
+    for (int o = 0; o < 4 && e == cudaSuccess; ++o) {
+      e = set_smem_attr(extend_fn(st != 0, o), b);
+      if (e == cudaSuccess) e = set_smem_attr(shadow_fn(st != 0, o), b);
+    }
+  return e;
+}
+
+cudaError_t LaunchBatchLoopInit(const LoopPool& pool, cudaStream_t stream) {
+  k_lp_init<<<1, kLoopCtlWords, 0, stream>>>(pool.ctl);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
+                                     const LoopPool& P, const BatchLaunch& bl, const LoopGrids& g,
+                                     cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
+                                     cudaEvent_t* marks) {
+  const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
+  cudaStream_t s = bl.stream;
+  auto mark = [&](int i) {
+    if (marks) cudaEventRecord(marks[i], s);
+  };
+  mark(0);
+  if (bl.parity) k_lp_regen<true><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
+  else k_lp_regen<false><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
+  mark(1);
+  extend_fn(bl.stats, bl.occupancy)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
+                                                                      bl.steps, ctr, err);
+  mark(2);
+  if (bl.parity) k_lp_shade<true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  else k_lp_shade<false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  mark(3);
+  shadow_fn(bl.stats, bl.occupancy)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
+                                                                      bl.steps, ctr, err);
+  mark(4);
+  k_lp_finish<<<g.finish, bl.block, 0, s>>>(jobs, total, P, handle);
+  mark(5);
+  return cudaGetLastError();
+}
+
+}  // namespace vkptc

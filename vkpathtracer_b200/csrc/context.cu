@@ -882,6 +882,13 @@ struct vkptc_batch {
   DevBuf<float4> p_o, p_d, p_thr, p_rad, p_sh_o, p_sh_d, p_sh_c;
   DevBuf<float2> p_hit;
   DevBuf<int2> spill;
+  // loop-driver state: two compacted path generations, shadow queue, finished list
+  DevBuf<uint32_t> l_job[2], l_local[2], l_depth[2];
+  DevBuf<uint64_t> l_rng[2];
+  DevBuf<float4> l_o[2], l_d[2], l_thr[2], l_rad[2];
+  DevBuf<float2> l_hit;
+  DevBuf<float4> l_sh_o, l_sh_d, l_sh_c, l_fin_rad;
+  DevBuf<uint32_t> l_sh_dst, l_fin_job, l_fin_local, l_ctl;
   DevBuf<DevCounters> d_ctr;
   DevBuf<uint32_t> d_err;
   size_t smem_configured = 48 * 1024;
@@ -1055,6 +1062,41 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   // ---- pool
   const uint32_t cap = std::max<uint32_t>(1024u, t.pool_paths ? t.pool_paths : kDefaultPoolPaths);
   const size_t n = cap;
+  BatchPool P{};
+  LoopPool LP{};
+  if (loop) {
+    for (int g = 0; g < 2; ++g) {
+      VKPTC_BCUDA(b, b->l_job[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_local[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_depth[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_rng[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_o[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_d[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_thr[g].alloc(n), "pool alloc");
+      VKPTC_BCUDA(b, b->l_rad[g].alloc(n), "pool alloc");
+      LP.gen[g] = PathSoA{b->l_job[g].ptr, b->l_local[g].ptr, b->l_depth[g].ptr, b->l_rng[g].ptr,
+                          b->l_o[g].ptr,   b->l_d[g].ptr,     b->l_thr[g].ptr,   b->l_rad[g].ptr};
+    }
+    VKPTC_BCUDA(b, b->l_hit.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_sh_o.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_sh_d.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_sh_c.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_sh_dst.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_fin_rad.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_fin_job.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_fin_local.alloc(n), "pool alloc");
+    VKPTC_BCUDA(b, b->l_ctl.alloc(kLoopCtlWords), "pool alloc");
+    LP.capacity = cap;
+    LP.hit = b->l_hit.ptr;
+    LP.sh_o = b->l_sh_o.ptr;
+    LP.sh_d = b->l_sh_d.ptr;
+    LP.sh_c = b->l_sh_c.ptr;
+    LP.sh_dst = b->l_sh_dst.ptr;
+    LP.fin_rad = b->l_fin_rad.ptr;
+    LP.fin_job = b->l_fin_job.ptr;
+    LP.fin_local = b->l_fin_local.ptr;
+    LP.ctl = b->l_ctl.ptr;
+  } else {
   VKPTC_BCUDA(b, b->p_job.alloc(n), "pool alloc");
   VKPTC_BCUDA(b, b->p_local.alloc(n), "pool alloc");
   VKPTC_BCUDA(b, b->p_depth.alloc(n), "pool alloc");
@@ -1073,7 +1115,6 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   VKPTC_BCUDA(b, b->p_sh_d.alloc(n), "pool alloc");
   VKPTC_BCUDA(b, b->p_sh_c.alloc(n), "pool alloc");
   VKPTC_BCUDA(b, b->p_hit.alloc(n), "pool alloc");
-  BatchPool P{};
   P.capacity = cap;
   P.job = b->p_job.ptr;
   P.local = b->p_local.ptr;
@@ -1093,6 +1134,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   P.fin = b->p_fin.ptr;
   P.freel = b->p_free.ptr;
   P.ctl = b->p_ctl.ptr;
+  }
 
   // ---- the run: film clear, pool reset, the pool iterations, in-order accumulation
   const uint32_t njobs = static_cast<uint32_t>(table.size());
@@ -1100,7 +1142,8 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
     int32_t rc = batch_clear_films(b);
     if (rc != VKPTC_OK) return rc;
     VKPTC_BCUDA(b, cudaMemsetAsync(b->d_ctr.ptr, 0, sizeof(DevCounters), b->stream), "counter clear");
-    VKPTC_BCUDA(b, LaunchBatchInit(P, b->stream), "pool init");
+    if (loop) VKPTC_BCUDA(b, LaunchBatchLoopInit(LP, b->stream), "pool init");
+    else VKPTC_BCUDA(b, LaunchBatchInit(P, b->stream), "pool init");
     return VKPTC_OK;
   };
   auto epilogue = [&]() -> int32_t {
@@ -1140,7 +1183,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
                   "body capture");
       BatchLaunch bb = bl;
       bb.stream = b->body_stream;
-      const cudaError_t el = LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, P, bb, lg, handle, b->d_ctr.ptr,
+      const cudaError_t el = LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, LP, bb, lg, handle, b->d_ctr.ptr,
                                                       b->d_err.ptr);
       cudaGraph_t body = nullptr;
       const cudaError_t ee = cudaStreamEndCapture(b->body_stream, &body);
@@ -1158,7 +1201,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
                             "/" + std::to_string(bl.steps) + "/" + std::to_string(t.sample_limit) + "/" +
                             std::to_string(b->jobs.size()) + "/" +
                             std::to_string(reinterpret_cast<uintptr_t>(b->staging.ptr)) + "/" +
-                            std::to_string(reinterpret_cast<uintptr_t>(b->p_job.ptr));
+                            std::to_string(reinterpret_cast<uintptr_t>(loop ? b->l_job[0].ptr : b->p_job.ptr));
     if (!b->graph || b->graph_key != key) {
       release_graph(b);
       VKPTC_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
@@ -1199,11 +1242,11 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
     int32_t rc = prologue();
     if (rc != VKPTC_OK) return rc;
     for (;;) {
-      VKPTC_BCUDA(b, LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, P, bl, lg, 0, b->d_ctr.ptr, b->d_err.ptr,
+      VKPTC_BCUDA(b, LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, LP, bl, lg, 0, b->d_ctr.ptr, b->d_err.ptr,
                                               timing ? b->marks : nullptr),
                   "loop iteration");
       uint32_t more = 0;
-      VKPTC_BCUDA(b, cudaMemcpyAsync(&more, P.ctl + kBatchCtlMore, sizeof(more), cudaMemcpyDeviceToHost, b->stream),
+      VKPTC_BCUDA(b, cudaMemcpyAsync(&more, LP.ctl + kLoopCtlMore, sizeof(more), cudaMemcpyDeviceToHost, b->stream),
                   "loop condition");
       VKPTC_BCUDA(b, cudaStreamSynchronize(b->stream), "loop sync");
       if (timing) {
@@ -1230,7 +1273,8 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   DevCounters dc{};
   VKPTC_BCUDA(b, cudaMemcpy(&dc, b->d_ctr.ptr, sizeof(dc), cudaMemcpyDeviceToHost), "counters");
   uint32_t iterations = 0;
-  VKPTC_BCUDA(b, cudaMemcpy(&iterations, P.ctl + kBatchCtlIterations, sizeof(iterations), cudaMemcpyDeviceToHost),
+  VKPTC_BCUDA(b, cudaMemcpy(&iterations, loop ? LP.ctl + kLoopCtlIterations : P.ctl + kBatchCtlIterations,
+                            sizeof(iterations), cudaMemcpyDeviceToHost),
               "iterations");
   b->stats.segments = dc.rays;
   b->stats.shadow_rays = dc.shadow_tests;
