@@ -40,9 +40,10 @@ UNIT = "paths/s"
 WORKLOAD = "batch_64_uneven_jobs"
 NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
 PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
-# DRAM bytes (read + write) per extension ray of k_loop_extend, from one ncu
-# capture of the 4-job case (profiles/k_lp_extend_batch_4_jobs.md).
-TRAFFIC_BYTES_PER_EXT_RAY = 0.0
+# DRAM bytes (read + write) per extension ray of k_lp_extend, from one ncu
+# capture of the 4-job case (profiles/k_lp_extend_batch_4_jobs.md: 62.79 MB
+# for a launch of 1,048,576 rays).
+TRAFFIC_BYTES_PER_EXT_RAY = 62789632 / 1048576
 
 
 def peaks():
