@@ -209,6 +209,15 @@ __device__ __forceinline__ Dual dot(const DV3& a, const DV3& b) { return a.x * b
 __device__ __forceinline__ DV3 cross(const DV3& a, const DV3& b) {
   return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
+// Mixed constant/dual forms: a constant operand contributes no tangent, so
+// these skip the zero-tangent arithmetic the all-dual forms would execute
+// (IEEE rules keep the compiler from folding x * 0 away).
+__device__ __forceinline__ DV3 sub(V3 a, const DV3& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ Dual dot(V3 a, const DV3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ Dual dot(const DV3& a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ DV3 cross(V3 a, const DV3& b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
 __device__ __forceinline__ DV3 unit(const DV3& v) {
   const Dual l = gsqrt(dot(v, v));
   if (l.v <= kEps) return lift<DV3>(mk(0.0f, 1.0f, 0.0f));
@@ -224,7 +233,7 @@ __device__ __forceinline__ S adj_light_pdf(const DevScene& s, const float* light
   if (s.light_count == 0u) return total;
   const float inv_n = 1.0f / static_cast<float>(s.light_count);
   for (uint32_t k = 0; k < s.light_count; ++k) {
-    const VT tl = sub(lift<VT>(ld3(lights + 16u * k)), p);
+    const VT tl = sub(ld3(lights + 16u * k), p);
     const S dist = gsqrt(dot(tl, tl));
     if (val(dist) < kEps) continue;
     if (val(dot(divs(tl, dist), dir)) > 0.9999f) total = total + inv_n / (dist * dist + kEps);
@@ -243,7 +252,7 @@ template <class S, class VT>
 __device__ __forceinline__ S adj_spot(const float* L, const VT& from_light) {
   const float inner = L[11], outer = L[12];
   if (inner <= -0.999f) return lift_s(1.0f, S{});
-  const S cone = dot(unit(from_light), lift<VT>(unit(ld3(L + 8))));
+  const S cone = dot(unit(from_light), unit(ld3(L + 8)));
   if (val(cone) <= outer) return lift_s(0.0f, S{});
   if (val(cone) >= inner || inner <= outer) return lift_s(1.0f, S{});
   const S t = sclamp((cone - outer) / (inner - outer), 0.0f, 1.0f);
@@ -261,7 +270,7 @@ struct AdjNee {
 };
 
 template <class S, class VT, bool kParity, bool kReplay>
-__device__ __forceinline__ bool adj_nee(const DevScene& s, const float* lights, const VT& p, const VT& n,
+__device__ __forceinline__ bool adj_nee(const DevScene& s, const float* lights, const VT& p, V3 n,
                                         const MaterialRec& m, const S& rough, const VT& view, uint64_t& rng,
                                         uint32_t& flags, AdjNee<S, VT>& q) {
   const uint32_t nl = s.light_count;
@@ -277,7 +286,7 @@ __device__ __forceinline__ bool adj_nee(const DevScene& s, const float* lights, 
     const float phi = 6.28318530718f * next01(rng);
     lp = add(lp, mul(mk(r * t_cos<kParity>(phi), uz, r * t_sin<kParity>(phi)), radius));
   }
-  const VT tl = sub(lift<VT>(lp), p);
+  const VT tl = sub(lp, p);
   const S d2 = dot(tl, tl);
   const S dist = gsqrt(d2);
   if (kReplay) {
@@ -291,10 +300,10 @@ __device__ __forceinline__ bool adj_nee(const DevScene& s, const float* lights, 
   const S sf = adj_spot<S, VT>(L, neg(ldir));
   if (!kReplay && val(sf) <= 0.0f) return false;
   const V3 alb = albedo_effect0(m);
-  const VT irr = mul(lift<VT>(ld3(L + 3)), (L[6] * sf) / (d2 + kEps));
+  const VT irr = mul(ld3(L + 3), (L[6] * sf) / (d2 + kEps));
   const float fnl = static_cast<float>(nl);
   // Diffuse term (no mirror or transmissive material reaches here).
-  VT acc = mul(mul(mulv(lift<VT>(mul(alb, kInvPi)), irr), cth), fnl);
+  VT acc = mul(mul(mulv(mul(alb, kInvPi), irr), cth), fnl);
   S spec_w = lift_s(0.0f, rough);
   if (val(rough) < 0.65f) {
     const VT hv = unit(add(ldir, unit(view)));
@@ -305,7 +314,7 @@ __device__ __forceinline__ bool adj_nee(const DevScene& s, const float* lights, 
     const S ss = clamp01((1.0f - rough) * 0.8f + m.metallic * 0.45f + m.clearcoat * 0.35f + 0.0f + 0.0f);
     const V3 tint = add(mul(mk(1.0f, 1.0f, 1.0f), 0.88f), mul(alb, 0.12f));
     spec_w = spec * cth * fnl * smax(0.15f, ss);
-    acc = add(acc, mul(mulv(lift<VT>(tint), irr), spec_w));
+    acc = add(acc, mul(mulv(tint, irr), spec_w));
   }
   flags |= kVfNeeValid;
   q.radiance = acc;
@@ -332,19 +341,18 @@ __device__ __forceinline__ VT adj_phong(uint64_t& rng, const VT& refl, const S& 
   else alt = !(fabsf(val(refl.z)) < 0.999f);
   if (alt) flags |= kVfFrameAlt;
   const V3 ref = alt ? mk(0.0f, 1.0f, 0.0f) : mk(0.0f, 0.0f, 1.0f);
-  const VT t = unit(cross(lift<VT>(ref), refl));
+  const VT t = unit(cross(ref, refl));
   const VT b = cross(refl, t);
   VT out = unit(add(add(mul(t, sn * t_cos<kParity>(phi)), mul(b, sn * t_sin<kParity>(phi))), mul(refl, ct)));
-  const VT nn = lift<VT>(n);
   bool reflected;
   if (kReplay) reflected = (flags & kVfReflected) != 0u;
-  else reflected = val(dot(out, nn)) <= 0.0f;
+  else reflected = val(dot(out, n)) <= 0.0f;
   if (reflected) {
     flags |= kVfReflected;
-    out = sub(out, mul(nn, 2.0f * dot(out, nn)));
+    out = sub(out, mul(n, 2.0f * dot(out, n)));
     bool hemi;
     if (kReplay) hemi = (flags & kVfHemi) != 0u;
-    else hemi = val(dot(out, nn)) <= 0.0f;
+    else hemi = val(dot(out, n)) <= 0.0f;
     if (hemi) {
       flags |= kVfHemi;
       return lift<VT>(sample_hemisphere<kParity>(rng, n));
@@ -376,10 +384,9 @@ __device__ __forceinline__ void adj_vertex(const DevScene& s, const DevSettings&
   R.hp = add(o, mul(d, ht));
   bool entering;
   if (kReplay) entering = (flags & kVfEntering) != 0u;
-  else entering = val(dot(d, lift<VT>(gn))) < 0.0f;
+  else entering = val(dot(d, gn)) < 0.0f;
   if (entering) flags |= kVfEntering;
   const V3 nv = entering ? gn : neg(gn);
-  const VT nrm = lift<VT>(nv);
   const bool emissive_any = m.emissive.x > 0.0f || m.emissive.y > 0.0f || m.emissive.z > 0.0f;
   const bool emissive_model = m.model == 1u || emissive_any;
   const bool diffuse = val(rough) >= 0.999f;
@@ -387,7 +394,7 @@ __device__ __forceinline__ void adj_vertex(const DevScene& s, const DevSettings&
   if (!st.enable_nee || depth == 0u) {
     R.w_e = lift_s(1.0f, rough);
   } else if (st.enable_mis && emissive_model) {
-    const S bp = smax(0.0f, dot(nrm, neg(d))) * kInvPi;
+    const S bp = smax(0.0f, dot(nv, neg(d))) * kInvPi;
     const S lpdf = adj_light_pdf<S, VT>(s, lights, o, d);
     R.w_e = adj_mis(bp, lpdf);
   } else {
@@ -396,12 +403,12 @@ __device__ __forceinline__ void adj_vertex(const DevScene& s, const DevSettings&
 
   R.nee = false;
   if (st.enable_nee && depth < st.max_depth - 1u) {
-    R.nee = adj_nee<S, VT, kParity, kReplay>(s, lights, R.hp, nrm, m, rough, neg(d), rng, flags, R.q);
+    R.nee = adj_nee<S, VT, kParity, kReplay>(s, lights, R.hp, nv, m, rough, neg(d), rng, flags, R.q);
     if (R.nee) {
       if (st.enable_mis) {
-        const VT tl = sub(lift<VT>(ld3(lights)), R.hp);
+        const VT tl = sub(ld3(lights), R.hp);
         const VT ld = unit(tl);
-        const S bp = smax(0.0f, dot(nrm, ld)) * kInvPi;
+        const S bp = smax(0.0f, dot(nv, ld)) * kInvPi;
         const float lpdf = 1.0f / static_cast<float>(s.light_count);
         R.w_n = adj_mis(lift_s(lpdf, rough), bp);
       } else {
@@ -410,7 +417,7 @@ __device__ __forceinline__ void adj_vertex(const DevScene& s, const DevSettings&
     }
   }
 
-  const VT refl = sub(d, mul(nrm, 2.0f * dot(nrm, d)));
+  const VT refl = sub(d, mul(nv, 2.0f * dot(nv, d)));
   if (diffuse) {
     R.out = lift<VT>(sample_hemisphere<kParity>(rng, nv));
   } else {
@@ -419,7 +426,7 @@ __device__ __forceinline__ void adj_vertex(const DevScene& s, const DevSettings&
     const S ex = smax(0.0f, 2.0f / (a2 * a2) - 2.0f);
     R.out = adj_phong<S, VT, kParity, kReplay>(rng, refl, ex, nv, flags);
   }
-  R.scattered = !(val(dot(R.out, nrm)) <= 0.0f);
+  R.scattered = !(val(dot(R.out, nv)) <= 0.0f);
 }
 
 }  // namespace vkptc
