@@ -58,19 +58,27 @@ __device__ __forceinline__ V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
 // Transcendentals.  Parity mode evaluates in FP64 and rounds once, which
 // lands on the correctly rounded float result (as glibc's sinf/cosf/powf do
 // to within their sub-ulp error); fast mode uses the FP32 library calls.
+// The FP64 routines are long, so each is one out-of-line function shared by
+// all call sites of a kernel: the shading code stays small enough for the
+// instruction cache.
+static __device__ __noinline__ float parity_sin(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
+static __device__ __noinline__ float parity_cos(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
+static __device__ __noinline__ float parity_pow(float x, float y) {
+  return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
+}
 template <bool kParity>
 __device__ __forceinline__ float t_sin(float x) {
-  if constexpr (kParity) return static_cast<float>(sin(static_cast<double>(x)));
+  if constexpr (kParity) return parity_sin(x);
   else return sinf(x);
 }
 template <bool kParity>
 __device__ __forceinline__ float t_cos(float x) {
-  if constexpr (kParity) return static_cast<float>(cos(static_cast<double>(x)));
+  if constexpr (kParity) return parity_cos(x);
   else return cosf(x);
 }
 template <bool kParity>
 __device__ __forceinline__ float t_pow(float x, float y) {
-  if constexpr (kParity) return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
+  if constexpr (kParity) return parity_pow(x, y);
   else return powf(x, y);
 }
 
