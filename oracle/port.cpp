@@ -16,7 +16,7 @@
 //   sample_direct_light             src/pathtracer/ScalarCpuPathTracer.cpp:1022-1118
 //   light_pdf_for_direction, Mis    src/pathtracer/ScalarCpuPathTracer.cpp:1120-1146
 //   sample_hemisphere / phong lobe  src/pathtracer/ScalarCpuPathTracer.cpp:978-1020
-//   apply_material_effect (0 only)  src/pathtracer/ScalarCpuPathTracer.cpp:264-355
+//   apply_material_effect           src/pathtracer/ScalarCpuPathTracer.cpp:186-355
 //   schlick_fresnel, refract_dir    src/pathtracer/ScalarCpuPathTracer.cpp:357-377
 //   accelerator build / intersect   src/pathtracer/CpuBvhAccelerator.cpp:84-154, 161-263, 360-477
 //   midpoint BVH builder            src/cpu/ParallelBvhBuilder.cpp:13-257
@@ -67,6 +67,62 @@ inline float clamp01(float v) {
   return fmin_std(1.0f, fmax_std(0.0f, v));
 }
 inline float pow5(float v) { const float v2 = v * v; return v2 * v2 * v; }
+
+// ---- procedural material effects (ScalarCpuPathTracer.cpp:186-355) ----------
+// hash01: fract(sin(dot(p, k) + seed * k4) * 43758.5453).
+inline float fx_hash(float x, float y, float z, float seed) {
+  const float v = std::sin(x * 12.9898f + y * 78.233f + z * 37.719f + seed * 19.19f) * 43758.5453f;
+  return v - std::floor(v);
+}
+inline float fx_smooth(float e0, float e1, float x) {
+  const float t = clamp01((x - e0) / fmax_std(1.0e-6f, e1 - e0));
+  return t * t * (3.0f - 2.0f * t);
+}
+inline V3 fx_lin(V3 a, float sa, V3 b, float sb) { return add(mul(a, sa), mul(b, sb)); }
+
+// Wood species 16..19 (16 plain, 17 parquet, 18 walnut, 19 sandalwood).
+inline V3 fx_wood(V3 base, V3 p, float roughness, float clearcoat, uint32_t style) {
+  const float rough = clamp01(roughness), coat = clamp01(clearcoat);
+  const float polish = clamp01(coat * (1.25f - rough * 0.75f));
+  const float par = style == 17u ? 1.0f : 0.0f, wal = style == 18u ? 1.0f : 0.0f, san = style == 19u ? 1.0f : 0.0f;
+  const float pw = 0.40f + 0.16f * par + 0.08f * polish - 0.18f * wal;
+  const float pl = 1.15f + 0.85f * par + 0.55f * polish - 0.55f * wal;
+  const float u = (p.x + san * p.y * 0.35f) / fmax_std(0.12f, pw);
+  const float v = (p.z + wal * p.y * 0.70f + san * p.x * 0.22f) / fmax_std(0.30f, pl);
+  const float cu = std::floor(u), cv = std::floor(v);
+  const float lu = u - cu, lv = v - cv;
+  const float seed = fx_hash(cu, cv, 0.0f, 16.0f);
+  const float macro = fx_hash(std::floor(p.x * 3.7f), std::floor(p.y * 3.7f), std::floor(p.z * 3.7f),
+                              31.0f + static_cast<float>(style));
+  const float micro = fx_hash(std::floor(p.x * 34.0f), std::floor(p.y * 34.0f), std::floor(p.z * 34.0f),
+                              47.0f + static_cast<float>(style));
+  const bool rot = par > 0.5f && std::fmod(cu + cv, 2.0f) >= 1.0f;
+  const float along = rot ? lv : lu, across = rot ? lu : lv;
+  const float wobble = (macro - 0.5f) * (0.06f + rough * 0.12f + wal * 0.08f + san * 0.04f);
+  const float wa = along + wobble + std::sin(across * 6.0f + seed * 5.0f) * 0.018f;
+  const float freq = 12.0f + rough * 8.0f + wal * 22.0f + san * 36.0f;
+  const float wave = std::sin((wa * freq + seed * 6.2831853f) +
+                              std::sin(across * (6.0f + rough * 8.0f) + seed * 4.0f) *
+                                  (0.25f + rough * 0.45f + wal * 0.45f));
+  const float fine = std::sin(wa * (55.0f + rough * 55.0f + san * 110.0f) + across * (9.0f + wal * 25.0f) +
+                              seed * 12.0f);
+  const float fw = 0.10f + rough * 0.18f + wal * 0.18f + san * 0.22f;
+  const float ring = fx_smooth(-0.35f + polish * 0.18f, 0.82f, wave) * (1.0f - fw) + (0.5f + 0.5f * fine) * fw;
+  const float su = fmin_std(lu, 1.0f - lu), sv = fmin_std(lv, 1.0f - lv);
+  const float seam = (1.0f - san) * (1.0f - fx_smooth(0.0f, 0.028f + polish * 0.018f, fmin_std(su, sv)));
+  const V3 dark = mul(base, 0.46f - rough * 0.10f - wal * 0.18f);
+  const V3 amber = add(mul(base, 1.14f + coat * 0.22f + san * 0.18f),
+                       V3{0.08f + san * 0.18f, 0.055f + san * 0.06f, 0.025f});
+  V3 wood = fx_lin(dark, 1.0f - ring, amber, ring);
+  const float tint = 0.92f + (0.08f + wal * 0.12f + san * 0.06f) * seed + (macro - 0.5f) * (0.08f + rough * 0.06f);
+  const float pores = fx_smooth(0.74f - wal * 0.08f, 1.0f, micro) *
+                      (0.025f + rough * 0.055f + wal * 0.055f + san * 0.018f);
+  wood = mul(wood, tint);
+  wood = mul(wood, 1.0f - pores);
+  wood = mul(wood, 1.0f - seam * (0.10f + rough * 0.35f + par * 0.18f) * (1.0f - coat * 0.45f));
+  const float mix = 0.30f + rough * 0.34f - polish * 0.14f + wal * 0.26f + san * 0.18f;
+  return fx_lin(base, 1.0f - mix, wood, mix);
+}
 inline V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
 
 uint64_t mix64(uint64_t x) {
@@ -386,9 +442,76 @@ struct Integrator {
   const World& w;
   const vko_settings& cfg;
 
-  V3 albedo_of(const Material& m) const {
-    // Effect 0 (the only one these scenes use): albedo clamped to [0, 1.5].
-    const V3 c = m.albedo;
+  // The material's albedo after its procedural effect at point p (normal n,
+  // ray direction `in`), clamped to [0, 1.5].
+  V3 albedo_of(const Material& m, V3 p, V3 n, V3 in) const {
+    V3 c = m.albedo;
+    const uint32_t fx = m.effect;
+    if (fx != 0u) {
+      const float h = fx_hash(p.x, p.y, p.z, static_cast<float>(fx));
+      const float facing = dot(n, neg(in));
+      switch (fx) {
+        case 1u: {
+          const float g = fmax_std(0.0f, 1.0f - std::fabs(facing));
+          c = fx_lin(c, 0.65f + 0.25f * h, V3{0.25f, 0.22f, 0.28f}, g * g * (0.4f + m.sheen));
+          break;
+        }
+        case 2u:
+          c = mul(c, 0.45f + 0.55f * (0.5f + 0.5f * std::sin(p.x * 7.0f + p.z * 5.0f + h * 6.0f)));
+          break;
+        case 3u:
+          c = mul(c, h > 0.72f ? 0.18f : 1.0f);
+          break;
+        case 4u: {
+          const float vein = 0.5f + 0.5f * std::sin((p.x + p.y * 0.4f + p.z * 0.7f) * 9.0f + h * 3.0f);
+          c = fx_lin(c, 0.55f + 0.45f * vein, V3{0.18f, 0.20f, 0.23f}, 1.0f - vein);
+          break;
+        }
+        case 5u:
+          c = fx_lin(c, 0.55f + 0.35f * h, V3{0.45f, 0.16f, 0.04f}, 0.25f + 0.25f * h);
+          break;
+        case 6u:
+          c = mul(c, 0.65f + 0.35f * h);
+          break;
+        case 7u:
+          c = fx_lin(c, 0.78f, V3{1.0f, 0.62f, 0.42f}, 0.16f);
+          break;
+        case 8u:
+          c = fx_lin(c, 0.55f, V3{0.35f + 0.45f * h, 0.25f + 0.35f * (1.0f - h), 0.85f}, 0.45f);
+          break;
+        case 9u:
+          c = mul(c, std::fmod(std::floor(p.x * 4.0f) + std::floor(p.z * 4.0f), 2.0f) < 0.5f ? 1.0f : 0.28f);
+          break;
+        case 10u:
+          c = fx_lin(c, 0.45f, V3{1.0f, 0.35f + 0.3f * h, 0.08f}, 0.55f);
+          break;
+        case 11u:
+          c = mul(c, 0.55f + 0.45f * (0.5f + 0.5f * std::sin(p.y * 18.0f + h * 5.0f)));
+          break;
+        case 12u: {
+          const float f2 = fmax_std(0.0f, facing) * fmax_std(0.0f, facing);
+          c = add(c, mul(V3{0.55f, 0.65f, 0.95f}, f2 * f2 * f2));
+          break;
+        }
+        case 13u:
+          c = mul(c, 0.65f + 0.35f * std::fabs(std::sin(p.x * 10.0f) * std::cos(p.z * 10.0f)));
+          break;
+        case 14u:
+          c = mul(V3{0.15f, 0.75f, 1.0f}, 0.2f + 0.8f * std::pow(fmax_std(0.0f, 1.0f - std::fabs(facing)), 0.8f));
+          break;
+        case 15u: {
+          const float bands = 0.5f + 0.5f * std::sin(p.y * 11.0f + p.x * 3.0f + h * 7.0f);
+          const float rim = std::pow(fmax_std(0.0f, 1.0f - std::fabs(facing)), 1.5f);
+          c = fx_lin(c, 0.25f + 0.45f * bands, V3{0.48f, 0.56f, 0.68f}, 0.18f + 0.32f * rim);
+          break;
+        }
+        case 16u: case 17u: case 18u: case 19u:
+          c = fx_wood(c, p, m.roughness, m.clearcoat, fx);
+          break;
+        default:
+          break;
+      }
+    }
     return {fmin_std(1.5f, fmax_std(0.0f, c.x)), fmin_std(1.5f, fmax_std(0.0f, c.y)),
             fmin_std(1.5f, fmax_std(0.0f, c.z))};
   }
@@ -471,7 +594,7 @@ struct Integrator {
       so = add(so, mul(ldir, adv));
       remain -= adv;
     }
-    const V3 alb = albedo_of(m);
+    const V3 alb = albedo_of(m, h.p, h.n, neg(ldir));
     const V3 irr = mul(L.color, (L.intensity * sf) / (d2 + kEps));
     V3 acc{0.0f, 0.0f, 0.0f};
     if (!mirror && !trans) {
@@ -544,7 +667,7 @@ struct Integrator {
       const bool entering = dot(d, h.n) < 0.0f;
       const V3 n = entering ? h.n : neg(h.n);
       const Material& m = w.mat(h.mat);
-      const V3 alb = albedo_of(m);
+      const V3 alb = albedo_of(m, h.p, n, d);
       const float rough = clamp01(m.roughness);
       const bool emissive_model = m.model == 1u || m.emissive_any();
       const bool mirror = m.model == 2u || rough <= 0.001f;
@@ -688,10 +811,6 @@ int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t fi
                float* film_sum, uint32_t* film_count, float* film_invalid, float* per_sample,
                vko_counters* counters) {
   if (!scene || !settings) return fail("null scene or settings");
-  for (uint32_t i = 0; i < scene->material_count; ++i) {
-    const uint32_t effect = static_cast<uint32_t>(scene->materials[16 * i + 15] + 0.5f) & 1023u;
-    if (effect != 0u) return fail("port oracle implements material effect 0 only");
-  }
   World w;
   w.load(*scene);
   Integrator it{w, *settings};

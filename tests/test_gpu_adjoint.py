@@ -236,6 +236,16 @@ def test_unsupported_material_is_rejected():
     t.close()
 
 
+def test_procedural_effect_is_rejected():
+    sc = scenes.inverse_box_scene()
+    sc.materials[7, 15] = 4.0     # veined box
+    t, _, _ = setup(16, 16, 1, scene=sc)
+    with pytest.raises(native.VkptcError) as e:
+        t.adjoint_setup(1)
+    assert e.value.code == native.UNSUPPORTED
+    t.close()
+
+
 def test_backward_before_forward_is_not_ready():
     t, sc, st = setup(16, 16, 1)
     t.adjoint_setup(1)

@@ -104,6 +104,21 @@ def test_port_matches_live_reference_material_zoo(port, nee, mis):
 
 
 @pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
+@pytest.mark.parametrize("nee,mis", [(True, True), (False, False)])
+def test_port_matches_live_reference_material_effects(port, nee, mis):
+    """Procedural material effects 1..19 (apply_material_effect) in the trace
+    loop and in next-event estimation."""
+    ref = oracle.load("reference")
+    sc = scenes.effect_gallery()
+    st = scenes.RenderSettings(width=48, height=40, spp=2, max_depth=6, seed=5, enable_nee=nee, enable_mis=mis)
+    a = ref.render(sc, st)
+    b = port.render(sc, st)
+    assert np.array_equal(bits(a["sum"]), bits(b["sum"]))
+    assert np.array_equal(a["count"], b["count"])
+    assert a["counters"]["rays"] == b["counters"]["rays"]
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
 def test_port_matches_live_reference_pixel_list_and_threads(port):
     ref = oracle.load("reference")
     sc = scenes.cornell_box(seed=3)

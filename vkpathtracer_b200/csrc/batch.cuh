@@ -50,6 +50,7 @@ struct BatchLaunch {
   cudaStream_t stream;
   bool parity;
   bool stats;   // count traversal work (node/leaf/triangle visits)
+  bool effects; // some job has a material with a procedural effect (loop driver: shading variant)
   int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
                   // (the persistent kernel; in the loop driver, its two traversal stages)
 };

@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __r
   if (lerr) atomicOr(err, lerr);
 }
 
-template <bool kParity>
+template <bool kParity, bool kEffects>
 __global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr) {
   const uint32_t cur = P.ctl[kLCur];
   const uint32_t n = P.ctl[kLCount0 + cur];
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ job
       pr.rad = mk(r4.x, r4.y, r4.z);
       pr.segs = r4.w;
       pr.rng = A.rng[j];
-      R = shade_bounce<kParity>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y));
+      R = shade_bounce<kParity, kEffects>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y));
       next = R.next;
       fin = !R.next;
       shadow = R.shadow;
@@ -310,7 +310,8 @@ LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int oc
   LoopGrids g{};
   g.regen = sm_count * (parity ? blocks_per_sm(k_lp_regen<true>, block, 0) : blocks_per_sm(k_lp_regen<false>, block, 0));
   g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy), block, smem);
-  g.shade = sm_count * (parity ? blocks_per_sm(k_lp_shade<true>, block, 0) : blocks_per_sm(k_lp_shade<false>, block, 0));
+  g.shade = sm_count * (parity ? blocks_per_sm(k_lp_shade<true, true>, block, 0)
+                               : blocks_per_sm(k_lp_shade<false, true>, block, 0));
   g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy), block, smem);
   g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
   return g;
@@ -348,8 +349,13 @@ cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, uns
   extend_fn(bl.stats, bl.occupancy)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
                                                                       bl.steps, ctr, err);
   mark(2);
-  if (bl.parity) k_lp_shade<true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
-  else k_lp_shade<false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  if (bl.effects) {
+    if (bl.parity) k_lp_shade<true, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+    else k_lp_shade<false, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  } else {
+    if (bl.parity) k_lp_shade<true, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+    else k_lp_shade<false, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+  }
   mark(3);
   shadow_fn(bl.stats, bl.occupancy)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
                                                                       bl.steps, ctr, err);

@@ -137,6 +137,7 @@ struct DevScene {
   uint32_t light_count;
   uint32_t prim_count;
   uint32_t has_transmissive;
+  uint32_t has_effects;       // some material has a procedural effect (1..19)
   V3 env;
   V3 cam_pos, cam_fwd, cam_right, cam_up;
   float tan_half_fov;

@@ -101,6 +101,7 @@ struct vkptc_ctx {
   float env[3] = {0, 0, 0};
   HostCamera cam{};
   bool has_transmissive = false;
+  bool has_effects = false;
 
   // device scene
   DevBuf<float4> d_nodes, d_tris, d_shade, d_tie;
@@ -182,6 +183,7 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.light_count = static_cast<uint32_t>(c->lights.size() / 16);
   s.prim_count = static_cast<uint32_t>(c->geo.prims.size());
   s.has_transmissive = c->has_transmissive ? 1u : 0u;
+  s.has_effects = c->has_effects ? 1u : 0u;
   s.env = mk(c->env[0], c->env[1], c->env[2]);
   s.cam_pos = mk(c->cam.pos[0], c->cam.pos[1], c->cam.pos[2]);
   camera_basis(c->cam, s.cam_fwd, s.cam_right, s.cam_up);
@@ -491,10 +493,6 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
       (scene->material_count && !scene->materials) || (scene->light_count && !scene->lights)) {
     return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene array pointer is null");
   }
-  for (uint32_t i = 0; i < scene->material_count; ++i) {
-    const uint32_t effect = static_cast<uint32_t>(scene->materials[16 * i + 15] + 0.5f) & 1023u;
-    if (effect != 0u) return fail(ctx, VKPTC_UNSUPPORTED, "procedural material effects (effect != 0) are not supported");
-  }
   ctx->adj.setup = false;
   cudaSetDevice(ctx->device);
   std::string err;
@@ -513,9 +511,11 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   ctx->lights.assign(scene->lights, scene->lights + 16 * static_cast<size_t>(scene->light_count));
   for (size_t i = 0; i < ctx->lights.size() / 16; ++i) ctx->lights[16 * i + 7] = std::max(0.0f, ctx->lights[16 * i + 7]);
   ctx->has_transmissive = false;
+  ctx->has_effects = false;
   for (size_t i = 0; i < ctx->materials.size() / 16; ++i) {
     const float* m = &ctx->materials[16 * i];
     if (static_cast<uint32_t>(m[7] + 0.5f) == 5u || m[10] > 0.05f) ctx->has_transmissive = true;
+    if ((static_cast<uint32_t>(m[15] + 0.5f) & 1023u) != 0u) ctx->has_effects = true;
   }
   std::memcpy(ctx->env, scene->environment, sizeof(ctx->env));
   std::memcpy(ctx->cam.pos, scene->camera_position, 12);
@@ -1030,6 +1030,8 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   bl.stream = b->stream;
   bl.parity = parity;
   bl.stats = b->config.collect_stats != 0u;
+  bl.effects = false;
+  for (vkptc_ctx* c : b->jobs) bl.effects = bl.effects || c->has_effects;
   bl.occupancy = static_cast<int>(std::min(3u, t.occupancy));
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
   int max_optin = 0;
@@ -1524,9 +1526,10 @@ std::string adjoint_material_issue(const float* m, size_t i) {
   else if (m[10] > 0.05f) why = "transmissive";
   else if (m[11] > 0.05f) why = "clear coat";
   else if (rough <= 0.001f) why = "mirror (roughness <= 0.001)";
+  else if ((static_cast<uint32_t>(m[15] + 0.5f) & 1023u) != 0u) why = "a procedural effect";
   if (why.empty()) return why;
   return "material " + std::to_string(i) + " is " + why + "; the adjoint supports Lambertian and Phong-lobe glossy "
-         "materials (models 0, 1, 3) only";
+         "materials (models 0, 1, 3) without procedural effects only";
 }
 
 // Material table with the 7 parameters of each material substituted.

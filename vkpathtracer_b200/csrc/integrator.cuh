@@ -38,8 +38,152 @@ __device__ __forceinline__ V3 albedo_effect0(const MaterialRec& m) {
           smin(1.5f, smax(0.0f, m.albedo.z))};
 }
 
-// sample_direct_light without the visibility loop (which the shadow stage runs).
+// ---------------------------------------------------- procedural effects
+// apply_material_effect (src/pathtracer/ScalarCpuPathTracer.cpp:186-355):
+// the albedo a surface shows at point p (shading normal n, ray direction
+// `in`), then clamped to [0, 1.5].  Effect 0 is the plain clamped albedo;
+// 1..19 are the reference's procedural looks (fibres, cells, cracks, veins,
+// oxidation, grain, subsurface tint, thin film, check mask, hot surface,
+// streaks, retro sparkle, wave normal hint, x-ray rim, smoke bands and four
+// wood species), evaluated in the reference's operation order.
 template <bool kParity>
+__device__ __forceinline__ float fx_hash(float x, float y, float z, float seed) {
+  const float v = t_sin<kParity>(x * 12.9898f + y * 78.233f + z * 37.719f + seed * 19.19f) * 43758.5453f;
+  return v - floorf(v);
+}
+__device__ __forceinline__ float fx_smooth(float e0, float e1, float x) {
+  const float t = clamp01((x - e0) / smax(1.0e-6f, e1 - e0));
+  return t * t * (3.0f - 2.0f * t);
+}
+__device__ __forceinline__ V3 fx_lin(V3 a, float sa, V3 b, float sb) { return add(mul(a, sa), mul(b, sb)); }
+
+template <bool kParity>
+__device__ __noinline__ V3 fx_wood(V3 base, V3 p, float roughness, float clearcoat, uint32_t style) {
+  const float rough = clamp01(roughness), coat = clamp01(clearcoat);
+  const float polish = clamp01(coat * (1.25f - rough * 0.75f));
+  const float par = style == 17u ? 1.0f : 0.0f, wal = style == 18u ? 1.0f : 0.0f, san = style == 19u ? 1.0f : 0.0f;
+  const float pw = 0.40f + 0.16f * par + 0.08f * polish - 0.18f * wal;
+  const float pl = 1.15f + 0.85f * par + 0.55f * polish - 0.55f * wal;
+  const float u = (p.x + san * p.y * 0.35f) / smax(0.12f, pw);
+  const float v = (p.z + wal * p.y * 0.70f + san * p.x * 0.22f) / smax(0.30f, pl);
+  const float cu = floorf(u), cv = floorf(v);
+  const float lu = u - cu, lv = v - cv;
+  const float seed = fx_hash<kParity>(cu, cv, 0.0f, 16.0f);
+  const float macro = fx_hash<kParity>(floorf(p.x * 3.7f), floorf(p.y * 3.7f), floorf(p.z * 3.7f),
+                                       31.0f + static_cast<float>(style));
+  const float micro = fx_hash<kParity>(floorf(p.x * 34.0f), floorf(p.y * 34.0f), floorf(p.z * 34.0f),
+                                       47.0f + static_cast<float>(style));
+  const bool rot = par > 0.5f && fmodf(cu + cv, 2.0f) >= 1.0f;
+  const float along = rot ? lv : lu, across = rot ? lu : lv;
+  const float wobble = (macro - 0.5f) * (0.06f + rough * 0.12f + wal * 0.08f + san * 0.04f);
+  const float wa = along + wobble + t_sin<kParity>(across * 6.0f + seed * 5.0f) * 0.018f;
+  const float freq = 12.0f + rough * 8.0f + wal * 22.0f + san * 36.0f;
+  const float wave = t_sin<kParity>((wa * freq + seed * 6.2831853f) +
+                                    t_sin<kParity>(across * (6.0f + rough * 8.0f) + seed * 4.0f) *
+                                        (0.25f + rough * 0.45f + wal * 0.45f));
+  const float fine = t_sin<kParity>(wa * (55.0f + rough * 55.0f + san * 110.0f) + across * (9.0f + wal * 25.0f) +
+                                    seed * 12.0f);
+  const float fw = 0.10f + rough * 0.18f + wal * 0.18f + san * 0.22f;
+  const float ring = fx_smooth(-0.35f + polish * 0.18f, 0.82f, wave) * (1.0f - fw) + (0.5f + 0.5f * fine) * fw;
+  const float su = smin(lu, 1.0f - lu), sv = smin(lv, 1.0f - lv);
+  const float seam = (1.0f - san) * (1.0f - fx_smooth(0.0f, 0.028f + polish * 0.018f, smin(su, sv)));
+  const V3 dark = mul(base, 0.46f - rough * 0.10f - wal * 0.18f);
+  const V3 amber = add(mul(base, 1.14f + coat * 0.22f + san * 0.18f),
+                       mk(0.08f + san * 0.18f, 0.055f + san * 0.06f, 0.025f));
+  V3 wood = fx_lin(dark, 1.0f - ring, amber, ring);
+  const float tint = 0.92f + (0.08f + wal * 0.12f + san * 0.06f) * seed + (macro - 0.5f) * (0.08f + rough * 0.06f);
+  const float pores = fx_smooth(0.74f - wal * 0.08f, 1.0f, micro) *
+                      (0.025f + rough * 0.055f + wal * 0.055f + san * 0.018f);
+  wood = mul(wood, tint);
+  wood = mul(wood, 1.0f - pores);
+  wood = mul(wood, 1.0f - seam * (0.10f + rough * 0.35f + par * 0.18f) * (1.0f - coat * 0.45f));
+  const float mix = 0.30f + rough * 0.34f - polish * 0.14f + wal * 0.26f + san * 0.18f;
+  return fx_lin(base, 1.0f - mix, wood, mix);
+}
+
+template <bool kParity>
+__device__ __noinline__ V3 fx_albedo(const MaterialRec& m, V3 p, V3 n, V3 in) {
+  V3 c = m.albedo;
+  const uint32_t fx = m.effect;
+  const float h = fx_hash<kParity>(p.x, p.y, p.z, static_cast<float>(fx));
+  const float facing = dot(n, neg(in));
+  switch (fx) {
+    case 1u: {
+      const float g = smax(0.0f, 1.0f - fabsf(facing));
+      c = fx_lin(c, 0.65f + 0.25f * h, mk(0.25f, 0.22f, 0.28f), g * g * (0.4f + m.sheen));
+      break;
+    }
+    case 2u:
+      c = mul(c, 0.45f + 0.55f * (0.5f + 0.5f * t_sin<kParity>(p.x * 7.0f + p.z * 5.0f + h * 6.0f)));
+      break;
+    case 3u:
+      c = mul(c, h > 0.72f ? 0.18f : 1.0f);
+      break;
+    case 4u: {
+      const float vein = 0.5f + 0.5f * t_sin<kParity>((p.x + p.y * 0.4f + p.z * 0.7f) * 9.0f + h * 3.0f);
+      c = fx_lin(c, 0.55f + 0.45f * vein, mk(0.18f, 0.20f, 0.23f), 1.0f - vein);
+      break;
+    }
+    case 5u:
+      c = fx_lin(c, 0.55f + 0.35f * h, mk(0.45f, 0.16f, 0.04f), 0.25f + 0.25f * h);
+      break;
+    case 6u:
+      c = mul(c, 0.65f + 0.35f * h);
+      break;
+    case 7u:
+      c = fx_lin(c, 0.78f, mk(1.0f, 0.62f, 0.42f), 0.16f);
+      break;
+    case 8u:
+      c = fx_lin(c, 0.55f, mk(0.35f + 0.45f * h, 0.25f + 0.35f * (1.0f - h), 0.85f), 0.45f);
+      break;
+    case 9u:
+      c = mul(c, fmodf(floorf(p.x * 4.0f) + floorf(p.z * 4.0f), 2.0f) < 0.5f ? 1.0f : 0.28f);
+      break;
+    case 10u:
+      c = fx_lin(c, 0.45f, mk(1.0f, 0.35f + 0.3f * h, 0.08f), 0.55f);
+      break;
+    case 11u:
+      c = mul(c, 0.55f + 0.45f * (0.5f + 0.5f * t_sin<kParity>(p.y * 18.0f + h * 5.0f)));
+      break;
+    case 12u: {
+      const float f2 = smax(0.0f, facing) * smax(0.0f, facing);
+      c = add(c, mul(mk(0.55f, 0.65f, 0.95f), f2 * f2 * f2));
+      break;
+    }
+    case 13u:
+      c = mul(c, 0.65f + 0.35f * fabsf(t_sin<kParity>(p.x * 10.0f) * t_cos<kParity>(p.z * 10.0f)));
+      break;
+    case 14u:
+      c = mul(mk(0.15f, 0.75f, 1.0f), 0.2f + 0.8f * t_pow<kParity>(smax(0.0f, 1.0f - fabsf(facing)), 0.8f));
+      break;
+    case 15u: {
+      const float bands = 0.5f + 0.5f * t_sin<kParity>(p.y * 11.0f + p.x * 3.0f + h * 7.0f);
+      const float rim = t_pow<kParity>(smax(0.0f, 1.0f - fabsf(facing)), 1.5f);
+      c = fx_lin(c, 0.25f + 0.45f * bands, mk(0.48f, 0.56f, 0.68f), 0.18f + 0.32f * rim);
+      break;
+    }
+    case 16u:
+    case 17u:
+    case 18u:
+    case 19u:
+      c = fx_wood<kParity>(c, p, m.roughness, m.clearcoat, fx);
+      break;
+    default:
+      break;
+  }
+  return mk(smin(1.5f, smax(0.0f, c.x)), smin(1.5f, smax(0.0f, c.y)), smin(1.5f, smax(0.0f, c.z)));
+}
+
+// kEffects = false compiles shading for scenes without procedural effects
+// (every material's effect is 0), which keeps that code small.
+template <bool kParity, bool kEffects>
+__device__ __forceinline__ V3 surface_albedo(const MaterialRec& m, V3 p, V3 n, V3 in) {
+  if constexpr (kEffects) return m.effect == 0u ? albedo_effect0(m) : fx_albedo<kParity>(m, p, n, in);
+  else return albedo_effect0(m);
+}
+
+// sample_direct_light without the visibility loop (which the shadow stage runs).
+template <bool kParity, bool kEffects = true>
 __device__ __forceinline__ NeeQuery nee_setup(const DevScene& s, const float* lights, V3 p, V3 n, uint32_t mat_index,
                                               V3 view, uint64_t& rng) {
   NeeQuery q;
@@ -73,7 +217,7 @@ __device__ __forceinline__ NeeQuery nee_setup(const DevScene& s, const float* li
   const bool metal = m.model == 4u || m.metallic > 0.65f;
   const bool trans = m.model == 5u || m.transmission > 0.05f;
   const bool coat = m.model == 7u || m.clearcoat > 0.05f;
-  const V3 alb = albedo_effect0(m);
+  const V3 alb = surface_albedo<kParity, kEffects>(m, p, n, neg(ldir));
   const V3 irr = mul(ld3(L + 3), (L[6] * sf) / (d2 + kEps));
   V3 acc = mk(0.0f, 0.0f, 0.0f);
   const float fnl = static_cast<float>(nl);
@@ -201,7 +345,7 @@ struct ShadeOut {
 
 // One bounce of the reference's trace loop for a path whose extension ray
 // (P.o, P.d) hit primitive `prim` at distance `ht` (prim == kMiss: no hit).
-template <bool kParity>
+template <bool kParity, bool kEffects = true>
 __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSettings& st, const float* lights,
                                                uint32_t depth, PathRegs& P, float ht, uint32_t prim) {
   ShadeOut R;
@@ -225,7 +369,7 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
     const V3 nrm = entering ? gn : neg(gn);
     const uint32_t mi = mat_index < s.material_count - 1u ? mat_index : s.material_count - 1u;
     const MaterialRec m = load_material(s.materials + 16u * mi);
-    const V3 alb = albedo_effect0(m);
+    const V3 alb = surface_albedo<kParity, kEffects>(m, hp, nrm, d);
     const float rough = clamp01(m.roughness);
     const bool emissive_any = m.emissive.x > 0.0f || m.emissive.y > 0.0f || m.emissive.z > 0.0f;
     const bool emissive_model = m.model == 1u || emissive_any;
@@ -246,7 +390,7 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
     }
 
     if (st.enable_nee && depth < st.max_depth - 1u) {
-      const NeeQuery nq = nee_setup<kParity>(s, lights, hp, nrm, mat_index, neg(d), rng);
+      const NeeQuery nq = nee_setup<kParity, kEffects>(s, lights, hp, nrm, mat_index, neg(d), rng);
       if (nq.valid) {
         R.shadow_tests = 1u;
         V3 c;

@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_
 
 constexpr uint32_t kSmemLights = 64;   // lights staged in shared memory by the shade stage
 
-template <bool kParity>
+template <bool kParity, bool kEffects>
 __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveState w, uint32_t cur,
                                                uint32_t depth, DevCounters* ctr) {
   __shared__ float sm_lights[16 * kSmemLights];
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveS
       P.rad = mk(r4.x, r4.y, r4.z);
       P.segs = r4.w;
       P.rng = w.rng[p];
-      const ShadeOut R = shade_bounce<kParity>(s, st, lights, depth, P, h2.x, __float_as_uint(h2.y));
+      const ShadeOut R = shade_bounce<kParity, kEffects>(s, st, lights, depth, P, h2.x, __float_as_uint(h2.y));
       if (R.next) {
         w.ray_o[p] = make_float4(P.o.x, P.o.y, P.o.z, 0.0f);
         w.ray_d[p] = make_float4(P.d.x, P.d.y, P.d.z, 0.0f);
@@ -396,8 +396,13 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
                                                              ls.steps, ctr, err);
     tm.end(ls.stream);
     tm.begin(2, ls.stream);
-    if (parity) k_shade<true><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
-    else k_shade<false><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
+    if (s.has_effects) {
+      if (parity) k_shade<true, true><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
+      else k_shade<false, true><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
+    } else {
+      if (parity) k_shade<true, false><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
+      else k_shade<false, false><<<ls.grid, ls.block, 0, ls.stream>>>(s, st, w, cur, depth, ctr);
+    }
     tm.end(ls.stream);
     if (st.enable_nee) {
       tm.begin(3, ls.stream);

@@ -11,6 +11,7 @@ benchmark configurations:
   sphere_grid()          64x64 displaced spheres (~2M triangles), 1920x1080, 64 spp, depth 16
   batch_jobs()           64 uneven render jobs for the persistent batched renderer
   inverse_box_scene()    the box room with 16 boxes and a 64-parameter material vector
+  effect_gallery()       the box room with one box per procedural material effect (1..19)
 
 Scene records use the reference's standard GPU word maps
 (src/gpu/VulkanGpuPathTracer.cpp:323-338 for materials, :381-396 for lights),
@@ -257,6 +258,34 @@ def cornell_box(seed: int = 1) -> Scene:
     v, t, inst = b.arrays()
     cam = Camera(position=(0.0, 0.5, 1.9), target=(0.0, 0.5, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0)
     return Scene(v, t, inst, np.array(mats), np.array(lights), (0.0, 0.0, 0.0), cam, "cornell_box").contiguous()
+
+
+def effect_gallery(seed: int = 11) -> Scene:
+    """The closed box with every procedural material effect (1..19): 19 small
+    boxes on the floor, one per effect, with varied roughness, clear coat and
+    sheen (the wood species read both); parquet floor and checker back wall."""
+    st = Stream(seed)
+    b = _Builder()
+    mats: list = []
+    lights: list = []
+    _room(b, mats, st)
+    mats[0][M_EFFECT] = 17.0   # floor: parquet
+    mats[2][M_EFFECT] = 9.0    # back wall: check pattern
+    for k in range(19):
+        gx, gz = k % 5, k // 5
+        cx, cz = -0.36 + 0.18 * gx, -0.33 + 0.18 * gz
+        hy = st.uniform(0.03, 0.09)
+        alb = tuple(st.uniform(0.2, 0.9) for _ in range(3))
+        rough = (0.2, 0.5, 0.8, 1.0)[k % 4]
+        model = (0, 3, 6, 7)[k % 4]
+        mats.append(material(albedo=alb, roughness=rough, model=model, clearcoat=0.5 if model == 7 else 0.0,
+                             sheen=0.7 if model == 6 else 0.0, effect=k + 1))
+        v, t = _box((cx, hy, cz), (0.06, hy, 0.06), st.uniform(-30.0, 30.0))
+        b.add(v, t, len(mats) - 1)
+    _ceiling_light(b, mats, lights)
+    v, t, inst = b.arrays()
+    cam = Camera(position=(0.0, 0.5, 1.9), target=(0.0, 0.3, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0)
+    return Scene(v, t, inst, np.array(mats), np.array(lights), (0.02, 0.02, 0.03), cam, "effect_gallery").contiguous()
 
 
 def cornell_settings(width=256, height=256, spp=16) -> RenderSettings:
