@@ -108,6 +108,15 @@ typedef struct vkptc_scene_view {
   float camera_fov_deg;
   float camera_aperture_radius;
   float camera_focus_distance;
+  /* Optional equirectangular environment map (PathTracerSceneSnapshot's
+   * environment_map, sampled as SampleSceneEnvironment does,
+   * src/pathtracer/PathTracer.cpp:213-272): width*height rgb texels, row-major,
+   * row 0 toward +y; scale multiplies the texels (all <= 1e-6: 1).  NULL or a
+   * zero size: the constant environment above. */
+  const float* environment_map;
+  uint32_t environment_map_width;
+  uint32_t environment_map_height;
+  float environment_map_scale[3];
 } vkptc_scene_view;
 
 /* Binary BVH as ParallelBvhBuilder returns it (src/cpu/ParallelBvhBuilder.h:22-39):

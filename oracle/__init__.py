@@ -44,6 +44,10 @@ class VkoScene(ctypes.Structure):
         ("camera_fov_deg", ctypes.c_float),
         ("camera_aperture_radius", ctypes.c_float),
         ("camera_focus_distance", ctypes.c_float),
+        ("environment_map", ctypes.c_void_p),
+        ("environment_map_width", ctypes.c_uint32),
+        ("environment_map_height", ctypes.c_uint32),
+        ("environment_map_scale", ctypes.c_float * 3),
     ]
 
 
@@ -135,6 +139,13 @@ class Oracle:
         s.camera_fov_deg = c.fov_deg
         s.camera_aperture_radius = c.aperture_radius
         s.camera_focus_distance = c.focus_distance
+        env = getattr(scene, "env_map", None)
+        if env is not None:
+            env = np.ascontiguousarray(env, np.float32)
+            keep = keep + (env,)
+            s.environment_map = _ptr(env)
+            s.environment_map_height, s.environment_map_width = env.shape[0], env.shape[1]
+            s.environment_map_scale[:] = scene.env_scale
         return s, keep
 
     @staticmethod

@@ -241,7 +241,36 @@ struct World {
   std::vector<Material> mats;
   std::vector<Light> lights;
   V3 env{};
+  std::vector<V3> env_map;   // equirectangular texels, row-major (empty: constant environment)
+  uint32_t env_w = 0, env_h = 0;
+  V3 env_scale{1.0f, 1.0f, 1.0f};
   V3 cam_pos{}, cam_fwd{}, cam_right{}, cam_up{};
+
+  // SampleSceneEnvironment (src/pathtracer/PathTracer.cpp:213-272).
+  V3 environment(V3 d) const {
+    if (env_map.empty()) return env;
+    const float len_sq = d.x * d.x + d.y * d.y + d.z * d.z;
+    if (len_sq <= 1.0e-12f) return env;
+    const float inv_len = 1.0f / std::sqrt(len_sq);
+    const V3 dir{d.x * inv_len, d.y * inv_len, d.z * inv_len};
+    float u = 0.5f + std::atan2(dir.z, dir.x) * 0.15915494309189533577f;
+    u -= std::floor(u);
+    const float v = std::acos(clampf(dir.y, -1.0f, 1.0f)) * 0.31830988618379067154f;
+    const float x = u * static_cast<float>(env_w);
+    const float y = clampf(v, 0.0f, 1.0f) * static_cast<float>(env_h - 1u);
+    const uint32_t x0 = static_cast<uint32_t>(std::floor(x)) % env_w, x1 = (x0 + 1u) % env_w;
+    const uint32_t y0 = static_cast<uint32_t>(std::floor(y)), y1 = std::min(y0 + 1u, env_h - 1u);
+    const float tx = x - std::floor(x), ty = y - std::floor(y);
+    auto at = [&](uint32_t px, uint32_t py) { return env_map[static_cast<size_t>(py) * env_w + px]; };
+    const V3 c00 = at(x0, y0), c10 = at(x1, y0), c01 = at(x0, y1), c11 = at(x1, y1);
+    const V3 top{c00.x + (c10.x - c00.x) * tx, c00.y + (c10.y - c00.y) * tx, c00.z + (c10.z - c00.z) * tx};
+    const V3 bot{c01.x + (c11.x - c01.x) * tx, c01.y + (c11.y - c01.y) * tx, c01.z + (c11.z - c01.z) * tx};
+    V3 c{top.x + (bot.x - top.x) * ty, top.y + (bot.y - top.y) * ty, top.z + (bot.z - top.z) * ty};
+    c.x *= env_scale.x;
+    c.y *= env_scale.y;
+    c.z *= env_scale.z;
+    return c;
+  }
   float fov = 60.0f;
   float aperture = 0.0f, focus = 0.0f;
 
@@ -313,6 +342,14 @@ struct World {
       lights.push_back(Light{ld3(l), ld3(l + 3), ld3(l + 8), l[6], l[7], l[11], l[12]});
     }
     env = ld3(s.environment);
+    if (s.environment_map && s.environment_map_width && s.environment_map_height) {
+      env_w = s.environment_map_width;
+      env_h = s.environment_map_height;
+      env_map.resize(static_cast<size_t>(env_w) * env_h);
+      for (size_t i = 0; i < env_map.size(); ++i) env_map[i] = ld3(s.environment_map + 3 * i);
+      env_scale = ld3(s.environment_map_scale);
+      if (fmax_std(fmax_std(env_scale.x, env_scale.y), env_scale.z) <= 1.0e-6f) env_scale = {1.0f, 1.0f, 1.0f};
+    }
     cam_pos = ld3(s.camera_position);
     fov = s.camera_fov_deg;
     aperture = s.camera_aperture_radius;
@@ -661,7 +698,7 @@ struct Integrator {
       ++segs;
       World::Hit h;
       if (!w.intersect(o, d, h, st)) {
-        rad = add(rad, mulv(thr, w.env));
+        rad = add(rad, mulv(thr, w.environment(d)));
         break;
       }
       const bool entering = dot(d, h.n) < 0.0f;

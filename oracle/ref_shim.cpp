@@ -91,6 +91,14 @@ pt::PathTracerSceneSnapshot to_snapshot(const vko_scene& s) {
     r.spot_outer_cos = l[12];
   }
   out.environment_color = v3(s.environment);
+  if (s.environment_map && s.environment_map_width && s.environment_map_height) {
+    const size_t n = static_cast<size_t>(s.environment_map_width) * s.environment_map_height;
+    out.environment_map.resize(n);
+    for (size_t i = 0; i < n; ++i) out.environment_map[i] = v3(s.environment_map + 3 * i);
+    out.environment_map_width = s.environment_map_width;
+    out.environment_map_height = s.environment_map_height;
+    out.environment_map_scale = v3(s.environment_map_scale);
+  }
   out.camera_position = v3(s.camera_position);
   out.camera_target = v3(s.camera_target);
   out.camera_up = v3(s.camera_up);

@@ -51,6 +51,10 @@ typedef struct vko_scene {
   float camera_fov_deg;
   float camera_aperture_radius;
   float camera_focus_distance;
+  const float* environment_map;      /* optional: width*height rgb texels (NULL = constant environment) */
+  uint32_t environment_map_width;
+  uint32_t environment_map_height;
+  float environment_map_scale[3];
 } vko_scene;
 
 typedef struct vko_settings {

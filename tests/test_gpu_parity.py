@@ -22,7 +22,9 @@ RMSE_REL_TOL = 1e-3        # RMSE(gpu - oracle) / mean(oracle)
 SIGMA3_FAIL_FRAC = 0.003   # fraction of pixel channels allowed outside 3 sigma
 BIT_EXACT_FRAC = 0.97      # fraction of pixels expected bit-identical in parity math mode
 EFFECT_BIT_EXACT_FRAC = 0.93  # the same with procedural effects (their hash magnifies sin's last bit)
-EFFECT_NOISE_FRAC = 0.35      # RMSE bound as a fraction of the reference's seed-to-seed RMSE
+EFFECT_FAR_FRAC = 0.05        # with effects: pixels allowed to differ by more than 1 %
+EFFECT_BIAS = 0.02            # with effects: relative difference of the image means
+ENV_BIT_EXACT_FRAC = 0.85     # with an environment map: every sky pixel runs atan2/acos
 
 
 def bits(a):
@@ -190,24 +192,42 @@ def test_film_matches_oracle_material_effects(nee):
     wall), evaluated in the trace loop and in next-event estimation."""
     sc = scenes.effect_gallery()
     st = scenes.RenderSettings(width=96, height=80, spp=4, max_depth=6, seed=21, enable_nee=nee, enable_mis=nee)
-    o = oracle.load("auto")
-    ref = o.render(sc, st, threads=8, per_sample=True)
+    ref = oracle.load("auto").render(sc, st, threads=8, per_sample=True)
     with make_tracer(sc, st) as t:
         t.render_frame(0, st.spp)
         g, cnt, _ = t.film()
     rep = film_report(g, ref["sum"], ref["samples"], st.spp)
     # The effects' hash, fract(sin(.) * 43758.5), magnifies a last-bit
     # difference of sin into a visibly different value, so a few paths take
-    # other roulette decisions and become independent samples.  The bound on
-    # the RMSE is therefore relative to the reference's own sampling noise:
-    # the RMSE between two reference renders that differ only in the seed.
-    other = o.render(sc, scenes.RenderSettings(**{**st.__dict__, "seed": st.seed + 1}), threads=8)
-    noise = float(np.sqrt(np.mean((other["sum"] - ref["sum"]) ** 2)) / st.spp / (np.mean(ref["sum"]) / st.spp))
-    print(rep, "seed-to-seed noise", noise)
+    # other roulette decisions and become independent samples: those pixels
+    # differ by sampling noise (the 3-sigma test), the rest agree exactly or
+    # nearly, and the image has no bias.
+    rel = np.abs(g - ref["sum"]) / np.maximum(np.abs(ref["sum"]), 1e-3)
+    far = float(np.mean(np.any(rel > 1e-2, axis=-1)))
+    bias = abs(float(np.mean(g)) - float(np.mean(ref["sum"]))) / float(np.mean(ref["sum"]))
+    print(rep, "pixels off by > 1%:", far, "mean bias:", bias)
     assert np.array_equal(cnt, ref["count"])
-    assert rep["rmse_rel"] < EFFECT_NOISE_FRAC * noise
     assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
     assert rep["bit_exact"] >= EFFECT_BIT_EXACT_FRAC
+    assert far < EFFECT_FAR_FRAC
+    assert bias < EFFECT_BIAS
+
+
+def test_film_matches_oracle_environment_map():
+    """Escaping paths sample an equirectangular sky map; the lookup's atan2 and
+    acos are the only new transcendentals, and they touch no path decision."""
+    sc = scenes.sky_scene()
+    st = scenes.RenderSettings(width=96, height=64, spp=4, max_depth=8, seed=17)
+    ref = oracle.load("auto").render(sc, st, threads=8, per_sample=True)
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp)
+        g, cnt, _ = t.film()
+    rep = film_report(g, ref["sum"], ref["samples"], st.spp)
+    print(rep)
+    assert np.array_equal(cnt, ref["count"])
+    assert rep["rmse_rel"] < RMSE_REL_TOL
+    assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
+    assert rep["bit_exact"] >= ENV_BIT_EXACT_FRAC
 
 
 def test_render_frame_batches_equal_per_tile_calls():

@@ -119,6 +119,21 @@ def test_port_matches_live_reference_material_effects(port, nee, mis):
 
 
 @pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
+def test_port_matches_live_reference_environment_map(port):
+    """Escaping paths sample the equirectangular map (SampleSceneEnvironment)."""
+    ref = oracle.load("reference")
+    sc = scenes.sky_scene()
+    st = scenes.RenderSettings(width=48, height=32, spp=2, max_depth=5, seed=3)
+    a = ref.render(sc, st)
+    b = port.render(sc, st)
+    assert np.array_equal(bits(a["sum"]), bits(b["sum"]))
+    plain = scenes.sky_scene()
+    plain.env_map = None
+    c = ref.render(plain, st)
+    assert not np.array_equal(a["sum"], c["sum"])   # the map is actually used
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
 def test_port_matches_live_reference_pixel_list_and_threads(port):
     ref = oracle.load("reference")
     sc = scenes.cornell_box(seed=3)

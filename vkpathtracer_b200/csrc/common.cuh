@@ -66,6 +66,20 @@ static __device__ __noinline__ float parity_cos(float x) { return static_cast<fl
 static __device__ __noinline__ float parity_pow(float x, float y) {
   return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
 }
+static __device__ __noinline__ float parity_atan2(float y, float x) {
+  return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
+}
+static __device__ __noinline__ float parity_acos(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
+template <bool kParity>
+__device__ __forceinline__ float t_atan2(float y, float x) {
+  if constexpr (kParity) return parity_atan2(y, x);
+  else return atan2f(y, x);
+}
+template <bool kParity>
+__device__ __forceinline__ float t_acos(float x) {
+  if constexpr (kParity) return parity_acos(x);
+  else return acosf(x);
+}
 template <bool kParity>
 __device__ __forceinline__ float t_sin(float x) {
   if constexpr (kParity) return parity_sin(x);
@@ -139,6 +153,9 @@ struct DevScene {
   uint32_t has_transmissive;
   uint32_t has_effects;       // some material has a procedural effect (1..19)
   V3 env;
+  const float4* env_map;      // equirectangular texels (rgb, w unused), or null
+  uint32_t env_w, env_h;
+  V3 env_scale;
   V3 cam_pos, cam_fwd, cam_right, cam_up;
   float tan_half_fov;
   float aperture, focus;

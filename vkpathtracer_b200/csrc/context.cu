@@ -99,6 +99,9 @@ struct vkptc_ctx {
   SceneGeometry geo;
   std::vector<float> materials, lights;
   float env[3] = {0, 0, 0};
+  uint32_t env_w = 0, env_h = 0;          // environment map size (0: constant environment)
+  float env_scale[3] = {1, 1, 1};
+  DevBuf<float4> d_env;
   HostCamera cam{};
   bool has_transmissive = false;
   bool has_effects = false;
@@ -185,6 +188,10 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.has_transmissive = c->has_transmissive ? 1u : 0u;
   s.has_effects = c->has_effects ? 1u : 0u;
   s.env = mk(c->env[0], c->env[1], c->env[2]);
+  s.env_map = c->env_w ? c->d_env.ptr : nullptr;
+  s.env_w = c->env_w;
+  s.env_h = c->env_h;
+  s.env_scale = mk(c->env_scale[0], c->env_scale[1], c->env_scale[2]);
   s.cam_pos = mk(c->cam.pos[0], c->cam.pos[1], c->cam.pos[2]);
   camera_basis(c->cam, s.cam_fwd, s.cam_right, s.cam_up);
   const float radians = c->cam.fov * (kPi / 180.0f);
@@ -518,6 +525,25 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
     if ((static_cast<uint32_t>(m[15] + 0.5f) & 1023u) != 0u) ctx->has_effects = true;
   }
   std::memcpy(ctx->env, scene->environment, sizeof(ctx->env));
+  // Environment map: used when it holds width*height texels (as the reference checks).
+  const uint64_t env_texels = static_cast<uint64_t>(scene->environment_map_width) * scene->environment_map_height;
+  ctx->env_w = ctx->env_h = 0u;
+  if (scene->environment_map && env_texels > 0) {
+    if (env_texels > (1ull << 28)) return fail(ctx, VKPTC_INVALID_ARGUMENT, "environment map above 2^28 texels");
+    std::vector<float4> texels(env_texels);
+    for (uint64_t i = 0; i < env_texels; ++i) {
+      const float* t = scene->environment_map + 3 * i;
+      texels[i] = make_float4(t[0], t[1], t[2], 0.0f);
+    }
+    VKPTC_CUDA(ctx, ctx->d_env.alloc(env_texels), "environment alloc");
+    VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_env.ptr, texels.data(), env_texels * sizeof(float4), cudaMemcpyHostToDevice),
+               "environment upload");
+    ctx->env_w = scene->environment_map_width;
+    ctx->env_h = scene->environment_map_height;
+    const float* sc = scene->environment_map_scale;
+    const bool unit_scale = std::max({sc[0], sc[1], sc[2]}) <= 1.0e-6f;
+    for (int a = 0; a < 3; ++a) ctx->env_scale[a] = unit_scale ? 1.0f : sc[a];
+  }
   std::memcpy(ctx->cam.pos, scene->camera_position, 12);
   std::memcpy(ctx->cam.target, scene->camera_target, 12);
   std::memcpy(ctx->cam.up, scene->camera_up, 12);
@@ -1607,6 +1633,7 @@ int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, cons
     if (!why.empty()) return fail(ctx, VKPTC_UNSUPPORTED, why);
   }
   if (ctx->has_transmissive) return fail(ctx, VKPTC_UNSUPPORTED, "adjoint: transmissive materials are not supported");
+  if (ctx->env_w) return fail(ctx, VKPTC_UNSUPPORTED, "adjoint: environment maps are not supported");
   const uint64_t npx = static_cast<uint64_t>(ctx->settings.width) * ctx->settings.height;
   if (npx == 0) return fail(ctx, VKPTC_INVALID_ARGUMENT, "empty film");
   if (target_rgb && target_floats != 3 * npx) {

@@ -182,6 +182,43 @@ __device__ __forceinline__ V3 surface_albedo(const MaterialRec& m, V3 p, V3 n, V
   else return albedo_effect0(m);
 }
 
+// ---------------------------------------------------- environment
+// SampleSceneEnvironment (src/pathtracer/PathTracer.cpp:213-272): the constant
+// environment colour, or a bilinear lookup in the equirectangular map
+// (u from atan2(z, x), v from acos(y), texel grid wrapped in u and clamped
+// in v), scaled.
+template <bool kParity>
+__device__ __forceinline__ V3 environment(const DevScene& s, V3 dir_in) {
+  if (s.env_map == nullptr) return s.env;
+  const float len_sq = dir_in.x * dir_in.x + dir_in.y * dir_in.y + dir_in.z * dir_in.z;
+  if (len_sq <= 1.0e-12f) return s.env;
+  const float inv_len = 1.0f / sqrtf(len_sq);
+  const V3 dir = mk(dir_in.x * inv_len, dir_in.y * inv_len, dir_in.z * inv_len);
+  float u = 0.5f + t_atan2<kParity>(dir.z, dir.x) * 0.15915494309189533577f;
+  u -= floorf(u);
+  const float v = t_acos<kParity>(sclamp(dir.y, -1.0f, 1.0f)) * 0.31830988618379067154f;
+  const uint32_t W = s.env_w, H = s.env_h;
+  const float x = u * static_cast<float>(W);
+  const float y = sclamp(v, 0.0f, 1.0f) * static_cast<float>(H - 1u);
+  const uint32_t x0 = static_cast<uint32_t>(floorf(x)) % W;
+  const uint32_t x1 = (x0 + 1u) % W;
+  const uint32_t y0 = static_cast<uint32_t>(floorf(y));
+  const uint32_t y1 = y0 + 1u < H - 1u ? y0 + 1u : H - 1u;
+  const float tx = x - floorf(x);
+  const float ty = y - floorf(y);
+  const float4 c00 = __ldg(s.env_map + static_cast<size_t>(y0) * W + x0);
+  const float4 c10 = __ldg(s.env_map + static_cast<size_t>(y0) * W + x1);
+  const float4 c01 = __ldg(s.env_map + static_cast<size_t>(y1) * W + x0);
+  const float4 c11 = __ldg(s.env_map + static_cast<size_t>(y1) * W + x1);
+  const V3 top = mk(c00.x + (c10.x - c00.x) * tx, c00.y + (c10.y - c00.y) * tx, c00.z + (c10.z - c00.z) * tx);
+  const V3 bot = mk(c01.x + (c11.x - c01.x) * tx, c01.y + (c11.y - c01.y) * tx, c01.z + (c11.z - c01.z) * tx);
+  V3 c = mk(top.x + (bot.x - top.x) * ty, top.y + (bot.y - top.y) * ty, top.z + (bot.z - top.z) * ty);
+  c.x *= s.env_scale.x;
+  c.y *= s.env_scale.y;
+  c.z *= s.env_scale.z;
+  return c;
+}
+
 // sample_direct_light without the visibility loop (which the shadow stage runs).
 template <bool kParity, bool kEffects = true>
 __device__ __forceinline__ NeeQuery nee_setup(const DevScene& s, const float* lights, V3 p, V3 n, uint32_t mat_index,
@@ -359,7 +396,7 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
   uint64_t rng = P.rng;
   P.segs = P.segs + 1.0f;
   if (prim == kMiss) {
-    rad = add(rad, mulv(thr, s.env));
+    rad = add(rad, mulv(thr, environment<kParity>(s, d)));
   } else {
     const V3 hp = add(o, mul(d, ht));
     const float4 sh = __ldg(s.shade + prim);

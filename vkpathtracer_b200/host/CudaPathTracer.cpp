@@ -73,8 +73,8 @@ Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
 
 Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& scene) {
   if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
-  if (!scene.sdf_primitives.empty() || !scene.environment_map.empty()) {
-    fail("the cuda backend renders triangle scenes with a constant environment (no SDF primitives, no environment map)");
+  if (!scene.sdf_primitives.empty()) {
+    fail("the cuda backend renders triangle scenes (no SDF primitives)");
     return Status::error(StatusCode::Unsupported, m_last_error);
   }
   for (const auto& inst : scene.instances) {
@@ -137,6 +137,16 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
   v.camera_fov_deg = scene.camera_fov_deg;
   v.camera_aperture_radius = scene.camera_aperture_radius;
   v.camera_focus_distance = scene.camera_focus_distance;
+  // The reference samples the map only when it holds width*height texels.
+  const size_t env_texels = static_cast<size_t>(scene.environment_map_width) * scene.environment_map_height;
+  if (env_texels > 0 && scene.environment_map.size() >= env_texels) {
+    v.environment_map = reinterpret_cast<const float*>(scene.environment_map.data());   // packed Vec3
+    v.environment_map_width = scene.environment_map_width;
+    v.environment_map_height = scene.environment_map_height;
+    v.environment_map_scale[0] = scene.environment_map_scale.x;
+    v.environment_map_scale[1] = scene.environment_map_scale.y;
+    v.environment_map_scale[2] = scene.environment_map_scale.z;
+  }
   const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
   if (st) m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
   return st;

@@ -48,7 +48,9 @@ class SceneView(ctypes.Structure):
                 ("environment", ctypes.c_float * 3), ("camera_position", ctypes.c_float * 3),
                 ("camera_target", ctypes.c_float * 3), ("camera_up", ctypes.c_float * 3),
                 ("camera_fov_deg", ctypes.c_float), ("camera_aperture_radius", ctypes.c_float),
-                ("camera_focus_distance", ctypes.c_float)]
+                ("camera_focus_distance", ctypes.c_float), ("environment_map", ctypes.c_void_p),
+                ("environment_map_width", ctypes.c_uint32), ("environment_map_height", ctypes.c_uint32),
+                ("environment_map_scale", ctypes.c_float * 3)]
 
 
 class BvhView(ctypes.Structure):

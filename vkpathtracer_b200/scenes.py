@@ -12,6 +12,7 @@ benchmark configurations:
   batch_jobs()           64 uneven render jobs for the persistent batched renderer
   inverse_box_scene()    the box room with 16 boxes and a 64-parameter material vector
   effect_gallery()       the box room with one box per procedural material effect (1..19)
+  sky_scene()            displaced spheres under an equirectangular sky map
 
 Scene records use the reference's standard GPU word maps
 (src/gpu/VulkanGpuPathTracer.cpp:323-338 for materials, :381-396 for lights),
@@ -98,6 +99,8 @@ class Scene:
     environment: tuple = (0.0, 0.0, 0.0)
     camera: Camera = dataclasses.field(default_factory=Camera)
     name: str = "scene"
+    env_map: Optional[np.ndarray] = None   # (H, W, 3) float32 equirectangular map, row 0 toward +y
+    env_scale: tuple = (0.0, 0.0, 0.0)     # texel multiplier (all <= 1e-6 means 1)
 
     @property
     def triangle_count(self) -> int:
@@ -480,6 +483,44 @@ def sphere_field(grid: int, n_lat: int, n_lon: int, seed: int, spacing: float = 
                  fov_deg=50.0)
     return Scene(v, t, inst, np.array(mats), np.array(lights),
                  (environment, environment, environment), cam, f"sphere_field_{grid}").contiguous()
+
+
+def sky_map(width: int = 128, height: int = 64, seed: int = 2, sun_dir=(0.4, 0.55, -0.73),
+            sun_radiance: float = 40.0) -> np.ndarray:
+    """Equirectangular sky, (height, width, 3) float32, row 0 toward +y, in the
+    reference's mapping (u = 0.5 + atan2(z, x) / 2pi, v = acos(y) / pi): a blue
+    gradient, a warm horizon, a darker ground, seeded value-noise clouds and a
+    small bright sun."""
+    v = (np.arange(height, dtype=np.float64) + 0.5) / height
+    u = (np.arange(width, dtype=np.float64) + 0.5) / width
+    theta = v[:, None] * math.pi
+    phi = (u[None, :] - 0.5) * 2.0 * math.pi
+    y = np.cos(theta) * np.ones_like(phi)
+    x = np.sin(theta) * np.cos(phi)
+    z = np.sin(theta) * np.sin(phi)
+    up = np.clip(y, 0.0, 1.0)[..., None]
+    sky = (1.0 - up) * np.array([1.0, 0.75, 0.5]) + up * np.array([0.25, 0.45, 0.95])
+    ground = np.array([0.18, 0.15, 0.12]) * np.ones_like(sky)
+    img = np.where((y >= 0.0)[..., None], sky, ground)
+    pts = np.stack([x, y, z], axis=-1).reshape(-1, 3) * 3.0
+    cloud = value_noise(pts, 4, seed).reshape(height, width)
+    cloud = np.clip((cloud - 0.55) * 3.0, 0.0, 1.0) * (y > 0.05)
+    img = img * (1.0 - 0.6 * cloud[..., None]) + 0.9 * cloud[..., None]
+    sd = np.asarray(sun_dir, np.float64)
+    sd = sd / np.linalg.norm(sd)
+    cosang = x * sd[0] + y * sd[1] + z * sd[2]
+    img = img + (cosang > 0.995)[..., None] * sun_radiance * np.array([1.0, 0.9, 0.7])
+    return np.ascontiguousarray(img, np.float32)
+
+
+def sky_scene(seed: int = 3, grid: int = 4) -> Scene:
+    """Displaced spheres (Lambert, glossy, mirror) on a ground plane under the
+    sky map, one sun-like point light for next-event estimation."""
+    sc = sphere_field(grid, 14, 18, seed=seed, n_lights=1, light_size=0.5, light_height=12.0)
+    sc.env_map = sky_map(seed=seed)
+    sc.env_scale = (1.0, 1.0, 1.0)
+    sc.name = "sky_scene"
+    return sc
 
 
 def sphere_grid(seed: int = 4, grid: int = 64) -> Scene:

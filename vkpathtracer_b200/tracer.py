@@ -98,6 +98,12 @@ def scene_view(scene: Scene):
     v.camera_fov_deg = c.fov_deg
     v.camera_aperture_radius = c.aperture_radius
     v.camera_focus_distance = c.focus_distance
+    if scene.env_map is not None:
+        env = np.ascontiguousarray(scene.env_map, np.float32)
+        keep = keep + (env,)
+        v.environment_map = _ptr(env)
+        v.environment_map_height, v.environment_map_width = env.shape[0], env.shape[1]
+        v.environment_map_scale[:] = scene.env_scale
     return v, keep
 
 
