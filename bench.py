@@ -245,6 +245,52 @@ def full_frame(device, tunings=None):
     return out
 
 
+def sdf_scene(device, cpu_seconds: float = 0.0):
+    """SDF primitives next to the triangle BVH (the SDF gallery: analytic
+    ellipsoid, five sphere-traced shapes, a triangle ground) at 1280x720,
+    16 spp, depth 8, as one job of the loop driver; per-stage times from a
+    host-driven run; SDF work from one counted sample through the wavefront
+    path; optionally the CPU oracle on a bounded pixel sample of the same job."""
+    from vkpathtracer_b200.tracer import BatchRenderer, CudaPathTracer
+    sc = scenes.sdf_gallery()
+    st = scenes.RenderSettings(width=1280, height=720, spp=16, max_depth=8, seed=1234)
+    paths = st.width * st.height * st.spp
+    out = {"workload": "sdf_gallery_720p_16spp_depth8", "sdf_primitives": int(sc.sdf.shape[0]),
+           "triangles": sc.triangle_count}
+    with BatchRenderer(device=device) as b:
+        b.add_job(sc, st)
+        b.run("loop")
+        ms = min(b.run("loop")["device_ms"] for _ in range(2))
+        out["paths_per_s"] = paths / (ms / 1e3)
+        out["ms_per_frame"] = ms
+    with BatchRenderer(device=device, stage_timing=True) as b:
+        b.add_job(sc, st)
+        stage = b.run("loop", use_graph=False)["stage_ms"]
+        out["stage_share"] = {k: v / max(1e-9, sum(stage.values())) for k, v in stage.items()}
+    with CudaPathTracer(device=device) as t:
+        one = scenes.RenderSettings(**{**st.__dict__, "spp": 1})
+        t.configure(one)
+        t.load_scene_snapshot(sc)
+        t.build_or_update_acceleration()
+        t.reset_accumulation()
+        t.render_frame(0, 1)
+        c = t.read_counters()
+        out["per_path"] = {"segments": c["rays"] / (st.width * st.height),
+                           "sdf_tests": c["sdf_tests"] / (st.width * st.height),
+                           "sdf_steps": c["sdf_steps"] / (st.width * st.height)}
+        out["sdf_steps_per_s"] = out["per_path"]["sdf_steps"] * out["paths_per_s"]
+    if cpu_seconds > 0.0:
+        import oracle
+        kind = "reference" if oracle.have_reference() else "port"
+        threads = os.cpu_count() or 1
+        v, sample = cpu_sample([scenes.Job(sc, st, 0)], cpu_seconds, threads, kind)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                               "sample": f"random {sample['pixel_fraction']:.4f} of the pixels at 16 spp "
+                                         f"({sample['paths']} paths)"}
+        out["speedup_vs_cpu"] = out["paths_per_s"] / v
+    return out
+
+
 def ray_query(device):
     import torch
     from vkpathtracer_b200.tracer import CudaPathTracer
@@ -393,6 +439,20 @@ def profile_run(args, local):
                       "iterations": r["iterations"], "device_ms": r["device_ms"], "paths": r["paths"]}), flush=True)
 
 
+def profile_sdf(local):
+    """Small fixed run for profilers: the SDF gallery (640x360, 4 spp, depth 8)
+    rendered twice by the loop driver without a CUDA graph."""
+    from vkpathtracer_b200.tracer import BatchRenderer
+    sc = scenes.sdf_gallery()
+    st = scenes.RenderSettings(width=640, height=360, spp=4, max_depth=8, seed=1234)
+    with BatchRenderer(device=local) as b:
+        b.add_job(sc, st)
+        for _ in range(2):
+            r = b.run("loop", use_graph=False)
+    print(json.dumps({"profile_sdf": sc.name, "iterations": r["iterations"], "device_ms": r["device_ms"],
+                      "paths": r["paths"]}), flush=True)
+
+
 def run_ours(args, world, rank, local):
     import torch
     from vkpathtracer_b200 import autotune
@@ -456,7 +516,7 @@ def run_ours(args, world, rank, local):
         ms = min(b.run(m, **mt)["device_ms"] for _ in range(2))
         drivers[m] = {"paths_per_s": total_paths / (ms / 1e3), "tuning": mt}
 
-    roof = rq = ff = cpu = inv = None
+    roof = rq = ff = cpu = inv = sdf = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the dominant kernel
         # traversal work counted in a stats run (same rays: the traversal is deterministic)
@@ -504,6 +564,7 @@ def run_ours(args, world, rank, local):
         if not args.no_fullframe:
             ff = full_frame(local, {m: d["tuning"] for m, d in drivers.items()} or None)
         inv = None if args.no_adjoint else inverse_rendering(local)
+        sdf = None if args.no_sdf else sdf_scene(local, 0.0 if (args.no_cpu or world > 1) else 5.0)
         if world == 1 and not args.no_cpu:
             import oracle
             kind = "reference" if oracle.have_reference() else "port"
@@ -528,7 +589,7 @@ def run_ours(args, world, rank, local):
                 "plain_kernel_launches": plain["kernel_launches"],
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
-                "inverse_rendering": inv, "cpu_baseline": cpu}
+                "inverse_rendering": inv, "sdf_scene": sdf, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     b.close()
 
@@ -545,8 +606,11 @@ def main():
     ap.add_argument("--no-fullframe", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-sdf", action="store_true")
     ap.add_argument("--profile-run", choices=["loop", "persistent"], default=None,
                     help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
+    ap.add_argument("--profile-sdf", action="store_true",
+                    help="profiling aid: render the SDF gallery twice with the loop driver, no CUDA graph, and exit")
     ap.add_argument("--cpu-step-seconds", type=float, default=0.0,
                     help="CPU work per reference-arm step (0 = about a minute over all steps)")
     args = ap.parse_args()
@@ -554,7 +618,9 @@ def main():
         args.warmup = 3
     world, rank, local = dist_init(args)
     try:
-        if args.profile_run:
+        if args.profile_sdf:
+            profile_sdf(local)
+        elif args.profile_run:
             profile_run(args, local)
         elif args.impl == "reference":
             run_reference(args, world, rank)

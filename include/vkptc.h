@@ -117,7 +117,27 @@ typedef struct vkptc_scene_view {
   uint32_t environment_map_width;
   uint32_t environment_map_height;
   float environment_map_scale[3];
+  /* Optional SDF primitives (PathTracerSceneSnapshot::sdf_primitives, the
+   * RTSdfPrimitive records of src/pathtracer/PathTracer.h:330-339), tested
+   * after the triangles for every extension and shadow ray with the nearest
+   * surface kept, as ScalarCpuPathTracer::intersect_scene does
+   * (src/pathtracer/ScalarCpuPathTracer.Intersect.cpp:91-129).  16 floats
+   * each: shape (vkptc_sdf_shape), position xyz, scale xyz, rotation xyz
+   * (Euler angles, radians), material index, radius, param_a, param_b, 0, 0.
+   * Shapes outside vkptc_sdf_shape never hit (the reference's switch default). */
+  const float* sdf_primitives;
+  uint32_t sdf_count;
 } vkptc_scene_view;
+
+/* SdfShape (src/pathtracer/PathTracer.h:232-240). */
+typedef enum vkptc_sdf_shape {
+  VKPTC_SDF_SPHERE = 0,
+  VKPTC_SDF_BOX = 1,
+  VKPTC_SDF_ROUNDED_BOX = 2,
+  VKPTC_SDF_PLANE = 3,
+  VKPTC_SDF_TORUS = 4,
+  VKPTC_SDF_CAPSULE = 5
+} vkptc_sdf_shape;
 
 /* Binary BVH as ParallelBvhBuilder returns it (src/cpu/ParallelBvhBuilder.h:22-39):
  * per node min3, max3 (f32) then left, right, first_prim, prim_count (i32). */

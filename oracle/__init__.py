@@ -48,6 +48,8 @@ class VkoScene(ctypes.Structure):
         ("environment_map_width", ctypes.c_uint32),
         ("environment_map_height", ctypes.c_uint32),
         ("environment_map_scale", ctypes.c_float * 3),
+        ("sdf_primitives", ctypes.c_void_p),
+        ("sdf_count", ctypes.c_uint32),
     ]
 
 
@@ -66,6 +68,8 @@ class VkoCounters(ctypes.Structure):
         ("triangle_hits", ctypes.c_uint64), ("bvh_node_visits", ctypes.c_uint64),
         ("bvh_leaf_visits", ctypes.c_uint64), ("shadow_tests", ctypes.c_uint64),
         ("render_ms", ctypes.c_double),
+        ("sdf_tests", ctypes.c_uint64), ("sdf_steps", ctypes.c_uint64), ("sdf_hits", ctypes.c_uint64),
+        ("sdf_misses", ctypes.c_uint64),
     ]
 
     def as_dict(self):
@@ -146,6 +150,11 @@ class Oracle:
             s.environment_map = _ptr(env)
             s.environment_map_height, s.environment_map_width = env.shape[0], env.shape[1]
             s.environment_map_scale[:] = scene.env_scale
+        sdf = getattr(scene, "sdf", None)
+        if sdf is not None and len(sdf):
+            sdf = np.ascontiguousarray(sdf, np.float32).reshape(-1, 16)
+            keep = keep + (sdf,)
+            s.sdf_primitives, s.sdf_count = _ptr(sdf), sdf.shape[0]
         return s, keep
 
     @staticmethod

@@ -22,6 +22,11 @@
 //   midpoint BVH builder            src/cpu/ParallelBvhBuilder.cpp:13-257
 //   leaf triangle batch             src/cpu/BvhTriangleIntersector.cpp:25-74, 186-209
 //   FilmBuffer::add_sample          src/pathtracer/FilmBuffer.cpp:80-91
+//   SDF primitives: rotate_x/y/z, rotate_euler(_inv), divide_by_scale
+//                                   src/pathtracer/ScalarCpuPathTracer.cpp:113-159
+//     sdf_distance, sdf_normal      src/pathtracer/ScalarCpuPathTracer.cpp:808-853
+//     intersect_sphere, the march   src/pathtracer/ScalarCpuPathTracer.cpp:855-930
+//     nearest-hit reduction         src/pathtracer/ScalarCpuPathTracer.Intersect.cpp:91-129
 
 #include "vkpt_oracle.h"
 
@@ -166,7 +171,103 @@ struct Prim {
 struct Box { float lo[3], hi[3]; };
 struct Node { Box box; int32_t left, right, first, count; };
 
-struct Stats { uint64_t tri_tests = 0, tri_hits = 0, nodes = 0, leaves = 0, shadow = 0; };
+struct Stats {
+  uint64_t tri_tests = 0, tri_hits = 0, nodes = 0, leaves = 0, shadow = 0;
+  uint64_t sdf_tests = 0, sdf_steps = 0, sdf_hits = 0, sdf_misses = 0;
+};
+
+// ------------------------------------------------------------ SDF primitives
+struct Sdf {
+  uint32_t shape, material;   // shape 0..5 (sphere, box, rounded box, plane, torus, capsule)
+  V3 pos, scale, rot;
+  float radius, pa, pb;
+};
+
+// Rotation about one axis by `a` radians, the sine and cosine taken per call.
+inline V3 turn_x(V3 v, float a) { const float s = std::sin(a), c = std::cos(a); return {v.x, c * v.y - s * v.z, s * v.y + c * v.z}; }
+inline V3 turn_y(V3 v, float a) { const float s = std::sin(a), c = std::cos(a); return {c * v.x + s * v.z, v.y, -s * v.x + c * v.z}; }
+inline V3 turn_z(V3 v, float a) { const float s = std::sin(a), c = std::cos(a); return {c * v.x - s * v.y, s * v.x + c * v.y, v.z}; }
+inline V3 unscale(V3 v, V3 s) {
+  return {v.x / (s.x != 0.0f ? s.x : 1.0f), v.y / (s.y != 0.0f ? s.y : 1.0f), v.z / (s.z != 0.0f ? s.z : 1.0f)};
+}
+// World vector -> primitive space: inverse Euler rotation (x, y, z order), then 1/scale.
+inline V3 sdf_local(const Sdf& p, V3 v) {
+  return unscale(turn_z(turn_y(turn_x(v, -p.rot.x), -p.rot.y), -p.rot.z), p.scale);
+}
+inline float vlen(V3 v) { return std::sqrt(dot(v, v)); }
+
+float sdf_value(const Sdf& p, V3 w) {
+  const V3 l = sdf_local(p, sub(w, p.pos));
+  switch (p.shape) {
+    case 0: return vlen(l) - p.radius;
+    case 1: {
+      const V3 q{std::fabs(l.x) - p.scale.x, std::fabs(l.y) - p.scale.y, std::fabs(l.z) - p.scale.z};
+      const V3 m{fmax_std(0.0f, q.x), fmax_std(0.0f, q.y), fmax_std(0.0f, q.z)};
+      return vlen(m) + fmin_std(fmax_std(q.x, fmax_std(q.y, q.z)), 0.0f);
+    }
+    case 2: {
+      const V3 q{std::fabs(l.x) - p.scale.x + p.pa, std::fabs(l.y) - p.scale.y + p.pa, std::fabs(l.z) - p.scale.z + p.pa};
+      const V3 m{fmax_std(0.0f, q.x), fmax_std(0.0f, q.y), fmax_std(0.0f, q.z)};
+      return vlen(m) + fmin_std(fmax_std(q.x, fmax_std(q.y, q.z)), 0.0f) - p.pa;
+    }
+    case 3: return l.y + p.pb;
+    case 4: {
+      const float ring = fmax_std(0.05f, p.pa), tube = fmax_std(0.02f, p.radius);
+      const float qx = vlen(V3{l.x, 0.0f, l.z}) - ring;
+      return vlen(V3{qx, l.y, 0.0f}) - tube;
+    }
+    default: {
+      const V3 a{0.0f, -p.pa, 0.0f}, b{0.0f, p.pa, 0.0f};
+      const V3 ab = sub(b, a);
+      const float s = dot(sub(l, a), ab) / fmax_std(kEps, dot(ab, ab));
+      const float c = fmax_std(0.0f, fmin_std(1.0f, s));
+      return vlen(sub(l, add(a, mul(ab, c)))) - p.radius;
+    }
+  }
+}
+
+// Closest intersection of one primitive; t is the caller's (0 on entry).
+bool sdf_hit(const Sdf& p, V3 o, V3 d, float& t, V3& n, Stats& st) {
+  ++st.sdf_tests;
+  if (p.shape == 0u) {   // analytic sphere
+    ++st.sdf_steps;
+    const float r = fmax_std(0.01f, p.radius);
+    const V3 lo = sdf_local(p, sub(o, p.pos)), ld = sdf_local(p, d);
+    const float a = dot(ld, ld);
+    if (a <= kEps * kEps) { ++st.sdf_misses; return false; }
+    const float hb = dot(lo, ld);
+    const float c = dot(lo, lo) - r * r;
+    const float disc = hb * hb - a * c;
+    if (disc < 0.0f) { ++st.sdf_misses; return false; }
+    const float root = std::sqrt(disc);
+    float cand = (-hb - root) / a;
+    if (cand <= kEps) cand = (-hb + root) / a;
+    if (cand <= kEps || !std::isfinite(cand)) { ++st.sdf_misses; return false; }
+    t = cand;
+    const V3 ln = unscale(unit(add(lo, mul(ld, t))), p.scale);
+    n = unit(turn_x(turn_y(turn_z(ln, p.rot.z), p.rot.y), p.rot.x));
+    ++st.sdf_hits;
+    return true;
+  }
+  for (uint32_t i = 0; i < 192u; ++i) {   // sphere tracing
+    ++st.sdf_steps;
+    const V3 x = add(o, mul(d, t));
+    const float dist = sdf_value(p, x);
+    if (dist <= kEps) {
+      const float e = 0.0005f;
+      const float gx = sdf_value(p, add(x, V3{e, 0.0f, 0.0f})) - sdf_value(p, sub(x, V3{e, 0.0f, 0.0f}));
+      const float gy = sdf_value(p, add(x, V3{0.0f, e, 0.0f})) - sdf_value(p, sub(x, V3{0.0f, e, 0.0f}));
+      const float gz = sdf_value(p, add(x, V3{0.0f, 0.0f, e})) - sdf_value(p, sub(x, V3{0.0f, 0.0f, e}));
+      n = unit(mul(V3{gx, gy, gz}, 0.5f));
+      ++st.sdf_hits;
+      return true;
+    }
+    t += fmax_std(1.0e-3f, dist);
+    if (t > 10000.0f) break;
+  }
+  ++st.sdf_misses;
+  return false;
+}
 
 // ----------------------------------------------------------------- BVH build
 struct Builder {
@@ -244,6 +345,7 @@ struct World {
   std::vector<V3> env_map;   // equirectangular texels, row-major (empty: constant environment)
   uint32_t env_w = 0, env_h = 0;
   V3 env_scale{1.0f, 1.0f, 1.0f};
+  std::vector<Sdf> sdfs;
   V3 cam_pos{}, cam_fwd{}, cam_right{}, cam_up{};
 
   // SampleSceneEnvironment (src/pathtracer/PathTracer.cpp:213-272).
@@ -349,6 +451,20 @@ struct World {
       for (size_t i = 0; i < env_map.size(); ++i) env_map[i] = ld3(s.environment_map + 3 * i);
       env_scale = ld3(s.environment_map_scale);
       if (fmax_std(fmax_std(env_scale.x, env_scale.y), env_scale.z) <= 1.0e-6f) env_scale = {1.0f, 1.0f, 1.0f};
+    }
+    for (uint32_t i = 0; i < s.sdf_count; ++i) {
+      const float* q = s.sdf_primitives + 16 * static_cast<size_t>(i);
+      if (!(q[0] >= 0.0f && q[0] < 5.5f)) continue;   // unknown shape: never hits, counts nothing
+      Sdf p;
+      p.shape = static_cast<uint32_t>(q[0] + 0.5f);
+      p.pos = ld3(q + 1);
+      p.scale = ld3(q + 4);
+      p.rot = ld3(q + 7);
+      p.material = q[10] >= 0.0f ? static_cast<uint32_t>(q[10] + 0.5f) : 0u;
+      p.radius = q[11];
+      p.pa = q[12];
+      p.pb = q[13];
+      sdfs.push_back(p);
     }
     cam_pos = ld3(s.camera_position);
     fov = s.camera_fov_deg;
@@ -460,15 +576,29 @@ struct World {
   bool intersect(V3 o, V3 d, Hit& h, Stats& st) const {
     h = Hit{false, 0.0f, {}, {}, 0};
     float t = 0.0f;
+    float best = std::numeric_limits<float>::infinity();
     const int64_t k = closest(o, d, t, st);
-    if (k < 0) return false;
-    const Prim& p = prims[static_cast<size_t>(k)];
-    h.hit = true;
-    h.t = t;
-    h.p = add(o, mul(d, t));
-    h.n = p.n;
-    h.mat = p.material;
-    return true;
+    if (k >= 0) {
+      const Prim& p = prims[static_cast<size_t>(k)];
+      h.hit = true;
+      h.t = t;
+      h.p = add(o, mul(d, t));
+      h.n = p.n;
+      h.mat = p.material;
+      best = t;
+    }
+    for (const Sdf& p : sdfs) {
+      float ts = 0.0f;
+      V3 n{};
+      if (!sdf_hit(p, o, d, ts, n, st) || ts >= best) continue;
+      best = ts;
+      h.hit = true;
+      h.t = ts;
+      h.p = add(o, mul(d, ts));
+      h.n = unit(n);
+      h.mat = p.material;
+    }
+    return h.hit;
   }
 
   const Material& mat(uint32_t i) const { return mats[std::min<size_t>(i, mats.size() - 1)]; }
@@ -913,6 +1043,10 @@ int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t fi
       counters->bvh_node_visits += stats[t].nodes;
       counters->bvh_leaf_visits += stats[t].leaves;
       counters->shadow_tests += stats[t].shadow;
+      counters->sdf_tests += stats[t].sdf_tests;
+      counters->sdf_steps += stats[t].sdf_steps;
+      counters->sdf_hits += stats[t].sdf_hits;
+      counters->sdf_misses += stats[t].sdf_misses;
     }
     counters->render_ms = ms;
   }

@@ -99,6 +99,20 @@ pt::PathTracerSceneSnapshot to_snapshot(const vko_scene& s) {
     out.environment_map_height = s.environment_map_height;
     out.environment_map_scale = v3(s.environment_map_scale);
   }
+  for (uint32_t i = 0; i < s.sdf_count; ++i) {
+    const float* q = s.sdf_primitives + 16 * static_cast<size_t>(i);
+    pt::RTSdfPrimitive r;
+    const bool known = q[0] >= 0.0f && q[0] < 5.5f;
+    r.shape = known ? static_cast<pt::SdfShape>(static_cast<uint32_t>(q[0] + 0.5f)) : pt::SdfShape::Unknown;
+    r.position = v3(q + 1);
+    r.scale = v3(q + 4);
+    r.rotation = v3(q + 7);
+    r.material_index = q[10] >= 0.0f ? static_cast<uint32_t>(q[10] + 0.5f) : 0u;
+    r.radius = q[11];
+    r.param_a = q[12];
+    r.param_b = q[13];
+    out.sdf_primitives.push_back(r);
+  }
   out.camera_position = v3(s.camera_position);
   out.camera_target = v3(s.camera_target);
   out.camera_up = v3(s.camera_up);
@@ -147,6 +161,10 @@ void add_counters(vko_counters* out, const pt::SampleCounters& c) {
   out->bvh_node_visits += c.bvh_node_visits;
   out->bvh_leaf_visits += c.bvh_leaf_visits;
   out->shadow_tests += c.shadow_tests;
+  out->sdf_tests += c.sdf_tests;
+  out->sdf_steps += c.sdf_steps;
+  out->sdf_hits += c.sdf_hits;
+  out->sdf_misses += c.sdf_misses;
 }
 
 double ms_since(std::chrono::steady_clock::time_point t0) {

@@ -55,6 +55,12 @@ typedef struct vko_scene {
   uint32_t environment_map_width;
   uint32_t environment_map_height;
   float environment_map_scale[3];
+  /* optional SDF primitives, 16 floats each: shape (0 sphere, 1 box,
+   * 2 rounded box, 3 plane, 4 torus, 5 capsule; others never hit), position3,
+   * scale3, rotation3 (Euler radians), material index, radius, param_a,
+   * param_b, 0, 0 (RTSdfPrimitive, src/pathtracer/PathTracer.h:330-339) */
+  const float* sdf_primitives;
+  uint32_t sdf_count;
 } vko_scene;
 
 typedef struct vko_settings {
@@ -83,6 +89,10 @@ typedef struct vko_counters {
   uint64_t bvh_leaf_visits;
   uint64_t shadow_tests;
   double render_ms;         /* wall time of the sample loop only */
+  uint64_t sdf_tests;
+  uint64_t sdf_steps;
+  uint64_t sdf_hits;
+  uint64_t sdf_misses;
 } vko_counters;
 
 /* Renders samples [first_sample, first_sample + n_samples) of frame 0.

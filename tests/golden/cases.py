@@ -43,23 +43,35 @@ def _sphere_rays(scene):
     return scenes.ray_query_rays(scene, primary_side=48, random_count=4096, scale=16.0, seed=3)
 
 
+def _sdf():
+    return scenes.sdf_gallery()
+
+
+def _sdf_settings():
+    return scenes.RenderSettings(width=48, height=36, spp=2, max_depth=6, seed=4321, enable_nee=True, enable_mis=True)
+
+
 CASES = {
     "box": (_box, _box_settings, _box_rays),
     "field": (_field, _field_settings, _field_rays),
     "sphere": (_sphere, None, _sphere_rays),
+    "sdf": (_sdf, _sdf_settings, None),
 }
 
 
 # ---- fixture (de)serialisation: the fixtures carry their exact inputs
 def scene_to_arrays(scene):
     c = scene.camera
-    return {
+    out = {
         "vertices": scene.vertices, "indices": scene.indices, "instances": scene.instances,
         "materials": scene.materials, "lights": scene.lights,
         "environment": np.array(scene.environment, np.float32),
         "camera": np.array(list(c.position) + list(c.target) + list(c.up) +
                            [c.fov_deg, c.aperture_radius, c.focus_distance], np.float32),
     }
+    if scene.sdf is not None:
+        out["sdf"] = np.ascontiguousarray(scene.sdf, np.float32)
+    return out
 
 
 def scene_from_arrays(d):
@@ -67,7 +79,8 @@ def scene_from_arrays(d):
     camera = scenes.Camera(tuple(cam[0:3]), tuple(cam[3:6]), tuple(cam[6:9]), float(cam[9]), float(cam[10]),
                            float(cam[11]))
     return scenes.Scene(d["vertices"], d["indices"], d["instances"], d["materials"], d["lights"],
-                        tuple(float(x) for x in d["environment"]), camera, "fixture").contiguous()
+                        tuple(float(x) for x in d["environment"]), camera, "fixture",
+                        sdf=d.get("sdf")).contiguous()
 
 
 def settings_to_arrays(st):

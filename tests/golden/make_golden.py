@@ -3,7 +3,7 @@
 Run in a container that has the reference sources (the reference oracle
 oracle/_ref/libvkptref.so is built from them by oracle/Makefile):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]     (default: every case)
 
 Each fixture is a small .npz: the inputs are regenerated from the seeded
 scene generators at test time, the outputs come from the reference's own
@@ -25,7 +25,10 @@ from tests.golden import cases  # noqa: E402
 def main():
     oracle.build_ref()
     ref = oracle.load("reference")
+    only = set(sys.argv[1:])
     for name, (scene_fn, settings_fn, rays_fn) in cases.CASES.items():
+        if only and name not in only:
+            continue
         scene = scene_fn()
         out = cases.scene_to_arrays(scene)
         nodes, prim = ref.build_bvh(scene)
@@ -41,6 +44,9 @@ def main():
             c = r["counters"]
             out["counters"] = np.array([c["samples"], c["rays"], c["triangle_tests"], c["triangle_hits"],
                                         c["bvh_node_visits"], c["bvh_leaf_visits"], c["shadow_tests"]], np.uint64)
+            if scene.sdf is not None:
+                out["sdf_counters"] = np.array([c["sdf_tests"], c["sdf_steps"], c["sdf_hits"], c["sdf_misses"]],
+                                               np.uint64)
         if rays_fn is not None:
             rays = rays_fn(scene)
             out["rays"] = rays

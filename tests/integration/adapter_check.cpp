@@ -97,6 +97,25 @@ bool load(const char* path, pt::PathTracerSceneSnapshot& s, pt::RenderSettings& 
   st.seed = seed;
   st.russian_roulette_min_survival = rr[0];
   st.russian_roulette_max_survival = rr[1];
+  // optional trailer: SDF primitive count, then 16 floats each
+  uint32_t n_sdf = 0;
+  std::vector<float> sdf;
+  if (f.read(reinterpret_cast<char*>(&n_sdf), 4) && n_sdf > 0) {
+    if (!read_vec(f, sdf, 16 * static_cast<size_t>(n_sdf))) return false;
+    for (uint32_t i = 0; i < n_sdf; ++i) {
+      const float* q = &sdf[16 * i];
+      pt::RTSdfPrimitive r;
+      r.shape = static_cast<pt::SdfShape>(static_cast<uint32_t>(q[0] + 0.5f));
+      r.position = {q[1], q[2], q[3]};
+      r.scale = {q[4], q[5], q[6]};
+      r.rotation = {q[7], q[8], q[9]};
+      r.material_index = static_cast<uint32_t>(q[10] + 0.5f);
+      r.radius = q[11];
+      r.param_a = q[12];
+      r.param_b = q[13];
+      s.sdf_primitives.push_back(r);
+    }
+  }
   return true;
 }
 

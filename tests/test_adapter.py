@@ -35,6 +35,9 @@ def write_scene(path, sc, st):
                   st.russian_roulette_start_depth], np.uint32).tofile(f)
         np.array([st.seed], np.uint64).tofile(f)
         np.array([st.russian_roulette_min_survival, st.russian_roulette_max_survival], np.float32).tofile(f)
+        if sc.sdf is not None:
+            np.array([sc.sdf.shape[0]], np.uint32).tofile(f)
+            sc.sdf.astype(np.float32).tofile(f)
 
 
 @needs_bin
@@ -46,10 +49,12 @@ def test_adapter_without_device_reports_unsupported():
 
 @needs_bin
 @pytest.mark.gpu
-@pytest.mark.parametrize("which", ["box", "field"])
+@pytest.mark.parametrize("which", ["box", "field", "sdf"])
 def test_adapter_matches_reference_through_ipathtracer(tmp_path, which):
     if which == "box":
         sc, st = scenes.cornell_box(seed=1), scenes.cornell_settings(64, 48, 3)
+    elif which == "sdf":
+        sc, st = scenes.sdf_gallery(), scenes.RenderSettings(width=64, height=48, spp=2, max_depth=6, seed=8)
     else:
         sc = scenes.sphere_field(4, 12, 14, seed=5, n_lights=4, light_size=2.0, light_height=6.0)
         st = scenes.RenderSettings(width=64, height=40, spp=2, max_depth=8, seed=31)

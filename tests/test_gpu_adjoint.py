@@ -246,6 +246,16 @@ def test_procedural_effect_is_rejected():
     t.close()
 
 
+def test_sdf_scene_is_rejected():
+    sc = scenes.inverse_box_scene()
+    sc.sdf = scenes.sdf_primitive("sphere", (0.0, 0.3, 0.0), (0.1, 0.1, 0.1), material=6, radius=1.0)[None]
+    t, _, _ = setup(16, 16, 1, scene=sc)
+    with pytest.raises(native.VkptcError) as e:
+        t.adjoint_setup(1)
+    assert e.value.code == native.UNSUPPORTED
+    t.close()
+
+
 def test_backward_before_forward_is_not_ready():
     t, sc, st = setup(16, 16, 1)
     t.adjoint_setup(1)

@@ -134,3 +134,32 @@ def test_sah_batch_equals_reference_tree_batch(batch):
         for j in range(n):
             f, c = b2.film(j)
             assert np.array_equal(c, ref[j][1]) and np.array_equal(bits(f), bits(ref[j][0]))
+
+
+def test_sdf_jobs_equal_across_drivers_and_match_oracle():
+    """Jobs with SDF primitives (one without triangles) in the batched
+    drivers: loop and persistent films equal the plain ones bit for bit, and
+    each job matches the oracle on a pixel subset."""
+    jobs = [(scenes.sdf_gallery(), scenes.RenderSettings(width=48, height=40, spp=3, max_depth=6, seed=2)),
+            (scenes.cornell_box(seed=2), scenes.cornell_settings(32, 24, 2)),
+            (scenes.sdf_complexity(), scenes.RenderSettings(width=40, height=30, spp=2, max_depth=5, seed=6))]
+    with BatchRenderer() as b:
+        for sc, st in jobs:
+            b.add_job(sc, st)
+        b.run("plain")
+        plain = films(b, len(jobs))
+        for mode in ("loop", "persistent"):
+            b.run(mode)
+            for (f, c), (pf, pc) in zip(films(b, len(jobs)), plain):
+                assert np.array_equal(c, pc) and np.array_equal(bits(f), bits(pf)), mode
+    o = oracle.load("auto")
+    rng = np.random.default_rng(1)
+    for (sc, st), (g, gc) in zip(jobs, plain):
+        npx = st.width * st.height
+        px = np.sort(rng.choice(npx, size=npx // 4, replace=False)).astype(np.uint32)
+        r = o.render(sc, st, pixels=px, threads=8)
+        ref, got = r["sum"].reshape(-1, 3)[px], g.reshape(-1, 3)[px]
+        assert np.array_equal(gc.reshape(-1)[px], r["count"].reshape(-1)[px])
+        exact = np.mean(np.all(bits(got) == bits(ref), axis=1))
+        rel = np.sqrt(np.mean((got - ref) ** 2)) / (np.mean(ref) + 1e-9)
+        assert exact >= 0.95 and rel < 1e-3, (sc.name, exact, rel)

@@ -154,7 +154,7 @@ def test_external_bvh_gives_same_hits():
 
 
 # ------------------------------------------------------------------ films
-@pytest.mark.parametrize("name", ["box", "field"])
+@pytest.mark.parametrize("name", ["box", "field", "sdf"])
 def test_film_matches_reference_golden(name):
     d = cases.load_fixture(name)
     sc, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
@@ -228,6 +228,55 @@ def test_film_matches_oracle_environment_map():
     assert rep["rmse_rel"] < RMSE_REL_TOL
     assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
     assert rep["bit_exact"] >= ENV_BIT_EXACT_FRAC
+
+
+@pytest.mark.parametrize("variant", ["gallery", "glass", "complexity"])
+def test_film_matches_oracle_sdf_primitives(variant):
+    """SDF primitives next to the triangle BVH: analytic ellipsoid, marched
+    box / rounded box / torus / capsule / plane; "glass" makes the ellipsoid
+    transmissive (the shadow loop steps through it), "complexity" has no
+    triangles at all."""
+    sc = {"gallery": scenes.sdf_gallery, "glass": lambda: scenes.sdf_gallery(glass=True),
+          "complexity": scenes.sdf_complexity}[variant]()
+    st = scenes.RenderSettings(width=96, height=72, spp=4, max_depth=8, seed=23)
+    ref = oracle.load("auto").render(sc, st, threads=8, per_sample=True)
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp)
+        g, cnt, _ = t.film()
+        c = t.read_counters()
+    rep = film_report(g, ref["sum"], ref["samples"], st.spp)
+    print(variant, rep, {k: c[k] for k in ("sdf_tests", "sdf_steps", "sdf_hits", "sdf_misses")},
+          {k: ref["counters"][k] for k in ("sdf_tests", "sdf_hits")})
+    assert np.array_equal(cnt, ref["count"])
+    assert rep["rmse_rel"] < RMSE_REL_TOL
+    assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
+    assert rep["bit_exact"] >= BIT_EXACT_FRAC
+    # every extension ray tests every primitive; shadow rays stop at the first occluder
+    assert c["sdf_tests"] >= c["rays"] * sc.sdf.shape[0]
+    assert 0 < c["sdf_hits"] <= c["sdf_tests"] and c["sdf_misses"] == c["sdf_tests"] - c["sdf_hits"]
+
+
+def test_unknown_sdf_shape_never_hits():
+    """A shape code outside the six (SdfShape::Unknown) is skipped, as the
+    reference's switch default does: the film equals the scene without it."""
+    sc = scenes.sdf_gallery()
+    st = scenes.RenderSettings(width=48, height=36, spp=2, max_depth=6, seed=3)
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp)
+        a, _, _ = t.film()
+    bad = sc.sdf.copy()
+    bad[0, 0] = 6.0
+    sc2 = scenes.sdf_gallery()
+    sc2.sdf = np.concatenate([bad[:1], sc.sdf[1:]])
+    sc3 = scenes.sdf_gallery()
+    sc3.sdf = np.ascontiguousarray(sc.sdf[1:])
+    with make_tracer(sc2, st) as t:
+        t.render_frame(0, st.spp)
+        b, _, _ = t.film()
+    with make_tracer(sc3, st) as t:
+        t.render_frame(0, st.spp)
+        c, _, _ = t.film()
+    assert np.array_equal(b, c) and not np.array_equal(a, b)
 
 
 def test_render_frame_batches_equal_per_tile_calls():

@@ -24,7 +24,7 @@ def port():
     return oracle.load("port")
 
 
-@pytest.mark.parametrize("name", ["box", "field"])
+@pytest.mark.parametrize("name", ["box", "field", "sdf"])
 def test_port_film_matches_reference_golden(port, name):
     d = cases.load_fixture(name)
     scene, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
@@ -36,6 +36,9 @@ def test_port_film_matches_reference_golden(port, name):
     got = np.array([c["samples"], c["rays"], c["triangle_tests"], c["triangle_hits"], c["bvh_node_visits"],
                     c["bvh_leaf_visits"], c["shadow_tests"]], np.uint64)
     assert np.array_equal(got, d["counters"])
+    if "sdf_counters" in d:
+        sdf = np.array([c["sdf_tests"], c["sdf_steps"], c["sdf_hits"], c["sdf_misses"]], np.uint64)
+        assert np.array_equal(sdf, d["sdf_counters"])
 
 
 @pytest.mark.parametrize("name", ["box", "field", "sphere"])
@@ -116,6 +119,31 @@ def test_port_matches_live_reference_material_effects(port, nee, mis):
     assert np.array_equal(bits(a["sum"]), bits(b["sum"]))
     assert np.array_equal(a["count"], b["count"])
     assert a["counters"]["rays"] == b["counters"]["rays"]
+
+
+SDF_SCENES = {"gallery": lambda: scenes.sdf_gallery(), "glass": lambda: scenes.sdf_gallery(glass=True),
+              "complexity": lambda: scenes.sdf_complexity()}
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
+@pytest.mark.parametrize("variant", list(SDF_SCENES))
+@pytest.mark.parametrize("nee,mis", [(True, True), (False, False)])
+def test_port_matches_live_reference_sdf_primitives(port, variant, nee, mis):
+    """SDF primitives (intersect_scene's loop after the triangles): analytic
+    sphere, sphere-traced box / rounded box / plane / torus / capsule with
+    rotations and scales, a transmissive SDF in the shadow loop, and a scene
+    with no triangles."""
+    ref = oracle.load("reference")
+    sc = SDF_SCENES[variant]()
+    st = scenes.RenderSettings(width=48, height=36, spp=2, max_depth=6, seed=9, enable_nee=nee, enable_mis=mis)
+    a = ref.render(sc, st)
+    b = port.render(sc, st)
+    assert np.array_equal(bits(a["sum"]), bits(b["sum"]))
+    assert np.array_equal(a["count"], b["count"])
+    for k in ("samples", "rays", "shadow_tests", "sdf_tests", "sdf_steps", "sdf_hits", "sdf_misses",
+              "triangle_tests", "bvh_node_visits"):
+        assert a["counters"][k] == b["counters"][k], k
+    assert a["counters"]["sdf_hits"] > 0
 
 
 @pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")

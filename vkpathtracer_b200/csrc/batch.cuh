@@ -51,6 +51,7 @@ struct BatchLaunch {
   bool parity;
   bool stats;   // count traversal work (node/leaf/triangle visits)
   bool effects; // some job has a material with a procedural effect (loop driver: shading variant)
+  bool sdf;     // some job has SDF primitives (loop driver: the two SDF stages run)
   int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
                   // (the persistent kernel; in the loop driver, its two traversal stages)
 };
@@ -124,12 +125,13 @@ struct LoopPool {
 };
 
 constexpr uint32_t kLoopFinBit = 0x80000000u;
+constexpr uint32_t kLoopDropDst = 0xFFFFFFFFu;   // shadow query an SDF occludes
 constexpr int kLoopCtlWords = 32;
 constexpr int kLoopCtlMore = 17;        // 1 while another iteration is needed
 constexpr int kLoopCtlIterations = 18;  // iterations of the last run
 
 struct LoopGrids {
-  int regen, extend, shade, shadow, finish;
+  int regen, extend, shade, shadow, finish, sdf;
 };
 LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count);
 cudaError_t ConfigureBatchLoopSmem(size_t bytes);

@@ -18,9 +18,15 @@
 //           paths to the finished list
 //   SHADOW  any-hit traversal; a visible query adds its term at its destination
 //   FINISH  finished paths' radiance to the job's staging slot; cur ^= 1
+// With SDF primitives in some job, two load-balanced stages join them: after
+// EXTEND the SDF closest-hit test folds SDF hits into the hit buffer, and
+// before SHADOW the SDF occlusion test drops the queries an SDF occludes (one
+// march step per lane and call, lanes refilled as their queries finish).
 // Positions are warp-aggregated appends, so every access coalesces.  The
 // stagings are added to the films in sample order afterwards (as in the
 // persistent driver), so films are bit-identical across drivers.
+#include <algorithm>
+
 #include "batch.cuh"
 #include "integrator.cuh"
 #include "traverse.cuh"
@@ -33,6 +39,7 @@ constexpr int kLCur = 0;            // current generation
 constexpr int kLCount0 = 1;         // paths in generation 0 / 1: words 1, 2
 constexpr int kLShadow = 3, kLFin = 4;
 constexpr int kLFetchExt = 5, kLFetchShadow = 6;
+constexpr int kLFetchSdf = 7, kLFetchSdfShadow = 11;
 constexpr int kLWork = 8;           // 64-bit path counter (words 8, 9)
 constexpr int kLBase = 10;          // paths in generation `cur` when its REGEN starts
 constexpr int kLMore = kLoopCtlMore, kLIter = kLoopCtlIterations;
@@ -71,6 +78,7 @@ struct LoopShadowSource {
   __device__ __forceinline__ void finish(uint32_t j, float, uint32_t occluded) const {
     if (occluded) return;
     const uint32_t dst = P.sh_dst[j];
+    if (dst == kLoopDropDst) return;
     const float4 c = P.sh_c[j];
     float4* r = (dst & kLoopFinBit) ? P.fin_rad + (dst & ~kLoopFinBit) : B.rad + dst;
     float4 v = *r;
@@ -80,6 +88,58 @@ struct LoopShadowSource {
     *r = v;
   }
 };
+
+// SDF closest-hit of the current generation: folds into the triangle hit.
+struct LoopSdfExtSource {
+  const DevJob* jobs;
+  PathSoA A;
+  float2* hit;
+  __device__ __forceinline__ void load(uint32_t j, SdfLane& L) const {
+    const DevScene& s = jobs[A.job[j]].scene;
+    L.sdf = s.sdf;
+    L.count = s.sdf_count;
+    if (L.count == 0u) return;
+    const float4 a = A.o[j], b = A.d[j];
+    L.o = mk(a.x, a.y, a.z);
+    L.d = mk(b.x, b.y, b.z);
+    const float2 h = hit[j];
+    L.best = h.x;
+    L.prim = __float_as_uint(h.y);
+  }
+  __device__ __forceinline__ void finish(uint32_t j, const SdfLane& L) const {
+    if (L.count != 0u) hit[j] = make_float2(L.best, __uint_as_float(L.prim));
+  }
+};
+
+// SDF occlusion of the shadow queue: an occluded query is dropped (its bound
+// set to 0 so the triangle any-hit does no work for it either).
+struct LoopSdfShadowSource {
+  const DevJob* jobs;
+  LoopPool P;
+  __device__ __forceinline__ void load(uint32_t j, SdfLane& L) const {
+    const float4 a = P.sh_o[j], b = P.sh_d[j];
+    const DevScene& s = jobs[__float_as_uint(b.w)].scene;
+    L.sdf = s.sdf;
+    L.count = s.sdf_count;
+    L.o = mk(a.x, a.y, a.z);
+    L.d = mk(b.x, b.y, b.z);
+    L.best = a.w;
+    L.prim = 0u;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, const SdfLane& L) const {
+    if (L.prim == 0u) return;
+    P.sh_dst[j] = kLoopDropDst;
+    P.sh_o[j].w = 0.0f;
+  }
+};
+
+constexpr int kSdfStepsPerRefill = 8;
+
+__device__ __forceinline__ void flush_sdf(DevCounters* ctr, const SdfCount& c) {
+  warp_count(&ctr->sdf_tests, c.tests);
+  warp_count(&ctr->sdf_steps, c.steps);
+  warp_count(&ctr->sdf_hits, c.hits);
+}
 
 __device__ __forceinline__ TwoLevelStack loop_stack(int2* smem_stack, int scap, int2* spill, int total_cap) {
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -167,6 +227,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __r
     P.ctl[kLShadow] = 0u;
     P.ctl[kLFin] = 0u;
     P.ctl[kLFetchShadow] = 0u;
+    P.ctl[kLFetchSdf] = 0u;
+    P.ctl[kLFetchSdfShadow] = 0u;
   }
   if (n == 0u) return;
   const TwoLevelStack stk = loop_stack(smem_stack, scap, spill, total_cap);
@@ -178,8 +240,28 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __r
   if (lerr) atomicOr(err, lerr);
 }
 
+__global__ void __launch_bounds__(256) k_lp_sdf(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr) {
+  const uint32_t cur = P.ctl[kLCur];
+  const uint32_t n = P.ctl[kLCount0 + cur];
+  if (n == 0u) return;
+  SdfCount c;
+  const LoopSdfExtSource src{jobs, P.gen[cur], P.hit};
+  sdf_persistent<LoopSdfExtSource, false>(src, n, &P.ctl[kLFetchSdf], kSdfStepsPerRefill, c);
+  flush_sdf(ctr, c);
+}
+
+__global__ void __launch_bounds__(256) k_lp_sdf_shadow(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr) {
+  const uint32_t n = P.ctl[kLShadow];
+  if (n == 0u) return;
+  SdfCount c;
+  const LoopSdfShadowSource src{jobs, P};
+  sdf_persistent<LoopSdfShadowSource, true>(src, n, &P.ctl[kLFetchSdfShadow], kSdfStepsPerRefill, c);
+  flush_sdf(ctr, c);
+}
+
 template <bool kParity, bool kEffects>
-__global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr) {
+__global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr,
+                                                  uint32_t sdf_staged) {
   const uint32_t cur = P.ctl[kLCur];
   const uint32_t n = P.ctl[kLCount0 + cur];
   const PathSoA A = P.gen[cur], B = P.gen[cur ^ 1u];
@@ -204,7 +286,8 @@ __global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ job
       pr.rad = mk(r4.x, r4.y, r4.z);
       pr.segs = r4.w;
       pr.rng = A.rng[j];
-      R = shade_bounce<kParity, kEffects>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y));
+      R = shade_bounce<kParity, kEffects>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y),
+                                          sdf_staged != 0u);
       next = R.next;
       fin = !R.next;
       shadow = R.shadow;
@@ -314,6 +397,7 @@ LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int oc
                                : blocks_per_sm(k_lp_shade<false, true>, block, 0));
   g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy), block, smem);
   g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
+  g.sdf = sm_count * std::min(blocks_per_sm(k_lp_sdf, block, 0), blocks_per_sm(k_lp_sdf_shadow, block, 0));
   return g;
 }
 
@@ -348,15 +432,18 @@ cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, uns
   mark(1);
   extend_fn(bl.stats, bl.occupancy)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
                                                                       bl.steps, ctr, err);
+  if (bl.sdf) k_lp_sdf<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
   mark(2);
+  const uint32_t staged = bl.sdf ? 1u : 0u;
   if (bl.effects) {
-    if (bl.parity) k_lp_shade<true, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
-    else k_lp_shade<false, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+    if (bl.parity) k_lp_shade<true, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
+    else k_lp_shade<false, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
   } else {
-    if (bl.parity) k_lp_shade<true, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
-    else k_lp_shade<false, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr);
+    if (bl.parity) k_lp_shade<true, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
+    else k_lp_shade<false, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
   }
   mark(3);
+  if (bl.sdf) k_lp_sdf_shadow<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
   shadow_fn(bl.stats, bl.occupancy)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
                                                                       bl.steps, ctr, err);
   mark(4);

@@ -161,6 +161,8 @@ struct DevScene {
   float aperture, focus;
   uint32_t stack_required;
   uint32_t reference_tree;   // 1: the traversal tree is the reference's own tree
+  const float4* sdf;         // SDF primitive records (sdf.cuh), tested after the triangles
+  uint32_t sdf_count;
 };
 
 // Render-wide integrator settings.

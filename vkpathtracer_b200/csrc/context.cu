@@ -22,6 +22,7 @@
 #include "bvh_host.h"
 #include "batch.cuh"
 #include "kernels.cuh"
+#include "sdf.cuh"
 
 using namespace vkptc;
 
@@ -102,6 +103,8 @@ struct vkptc_ctx {
   uint32_t env_w = 0, env_h = 0;          // environment map size (0: constant environment)
   float env_scale[3] = {1, 1, 1};
   DevBuf<float4> d_env;
+  uint32_t sdf_count = 0;                 // SDF primitives (records of kSdfWords float4)
+  DevBuf<float4> d_sdf;
   HostCamera cam{};
   bool has_transmissive = false;
   bool has_effects = false;
@@ -200,6 +203,8 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.focus = c->cam.focus > 0.0f ? c->cam.focus : c->settings.camera_focus_distance;
   s.stack_required = c->wide.stack_required;
   s.reference_tree = c->wide.reference_topology ? 1u : 0u;
+  s.sdf = c->sdf_count ? c->d_sdf.ptr : nullptr;
+  s.sdf_count = c->sdf_count;
   return s;
 }
 
@@ -544,6 +549,65 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
     const bool unit_scale = std::max({sc[0], sc[1], sc[2]}) <= 1.0e-6f;
     for (int a = 0; a < 3; ++a) ctx->env_scale[a] = unit_scale ? 1.0f : sc[a];
   }
+  // SDF primitives: one record of kSdfWords float4 each (sdf.cuh), with the
+  // sines and cosines of the rotation angles taken once here, by the same
+  // float sin/cos calls the reference makes per evaluation.
+  ctx->sdf_count = 0u;
+  if (scene->sdf_count) {
+    if (!scene->sdf_primitives) return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene array pointer is null");
+    std::vector<float4> rec;
+    for (uint32_t i = 0; i < scene->sdf_count; ++i) {
+      const float* q = scene->sdf_primitives + 16 * static_cast<size_t>(i);
+      if (!(q[0] >= 0.0f && q[0] < 5.5f)) continue;   // Unknown shape: never hits
+      const uint32_t shape = static_cast<uint32_t>(q[0] + 0.5f);
+      const float mat = q[10] >= 0.0f ? q[10] : 0.0f;
+      const uint32_t material = mat < 4294967040.0f ? static_cast<uint32_t>(mat + 0.5f) : 0xFFFFFFFFu;
+      const float rx = q[7], ry = q[8], rz = q[9];
+      auto div = [](float v) { return v != 0.0f ? v : 1.0f; };
+      auto bits = [](uint32_t v) {
+        float f;
+        std::memcpy(&f, &v, 4);
+        return f;
+      };
+      rec.push_back(make_float4(q[1], q[2], q[3], bits(shape)));
+      rec.push_back(make_float4(q[4], q[5], q[6], bits(material)));
+      rec.push_back(make_float4(div(q[4]), div(q[5]), div(q[6]), q[11]));
+      const bool unit_scale = div(q[4]) == 1.0f && div(q[5]) == 1.0f && div(q[6]) == 1.0f;
+      const bool no_rotation = rx == 0.0f && ry == 0.0f && rz == 0.0f;
+      rec.push_back(make_float4(q[12], q[13], bits((unit_scale ? 1u : 0u) | (no_rotation ? 2u : 0u)), 0.0f));
+      rec.push_back(make_float4(std::sin(-rx), std::cos(-rx), std::sin(-ry), std::cos(-ry)));
+      rec.push_back(make_float4(std::sin(-rz), std::cos(-rz), std::sin(rz), std::cos(rz)));
+      rec.push_back(make_float4(std::sin(ry), std::cos(ry), std::sin(rx), std::cos(rx)));
+      // Cull sphere of a marched shape: a bound on |local point| over the set
+      // {distance <= 1e-4}, times the largest divisor (local = R^-1 (w - pos) / div).
+      const double e = 1e-4, pa = q[12], rad = q[11];
+      const double sx = std::fabs(q[4]), sy = std::fabs(q[5]), sz = std::fabs(q[6]);
+      double rl = 0.0;   // 0: never culled
+      if (shape == kSdfBox) rl = std::sqrt((sx + e) * (sx + e) + (sy + e) * (sy + e) + (sz + e) * (sz + e));
+      if (shape == kSdfRoundedBox) {
+        const double a = std::fabs(pa) + e;
+        rl = std::sqrt((sx + a) * (sx + a) + (sy + a) * (sy + a) + (sz + a) * (sz + a));
+      }
+      if (shape == kSdfTorus) {
+        const double ring = std::max(0.05, pa), tube = std::max(0.02, rad);
+        rl = std::sqrt((ring + tube + e) * (ring + tube + e) + (tube + e) * (tube + e));
+      }
+      if (shape == kSdfCapsule) rl = std::fabs(pa) + std::max(0.0, rad + e);
+      const double dmax = std::max({std::fabs(div(q[4])), std::fabs(div(q[5])), std::fabs(div(q[6]))});
+      const double dmin = std::min({std::fabs(div(q[4])), std::fabs(div(q[5])), std::fabs(div(q[6]))});
+      double cull_r = rl * dmax * (1.0 + 1e-5), cull_k = dmax / dmin;
+      bool finite = std::isfinite(cull_r) && std::isfinite(cull_k) && cull_r < 1e30;
+      for (int w = 1; w <= 13; ++w) finite = finite && std::isfinite(q[w]);
+      if (!finite || rl == 0.0) cull_r = cull_k = 0.0;
+      rec.push_back(make_float4(static_cast<float>(cull_r), static_cast<float>(cull_k), 0.0f, 0.0f));
+    }
+    if (!rec.empty()) {
+      VKPTC_CUDA(ctx, ctx->d_sdf.alloc(rec.size()), "sdf alloc");
+      VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_sdf.ptr, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice),
+                 "sdf upload");
+      ctx->sdf_count = static_cast<uint32_t>(rec.size() / kSdfWords);
+    }
+  }
   std::memcpy(ctx->cam.pos, scene->camera_position, 12);
   std::memcpy(ctx->cam.target, scene->camera_target, 12);
   std::memcpy(ctx->cam.up, scene->camera_up, 12);
@@ -806,6 +870,10 @@ int32_t vkptc_read_counters(vkptc_ctx* ctx, vkptc_counters* out) {
   out->triangle_tests = dc.tris + dc.shadow_tris;
   out->bvh_node_visits = dc.nodes + dc.shadow_nodes;
   out->bvh_leaf_visits = dc.leaves + dc.shadow_leaves;
+  out->sdf_tests = dc.sdf_tests;
+  out->sdf_steps = dc.sdf_steps;
+  out->sdf_hits = dc.sdf_hits;
+  out->sdf_misses = dc.sdf_tests - dc.sdf_hits;
   return VKPTC_OK;
 }
 
@@ -1057,7 +1125,11 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   bl.parity = parity;
   bl.stats = b->config.collect_stats != 0u;
   bl.effects = false;
-  for (vkptc_ctx* c : b->jobs) bl.effects = bl.effects || c->has_effects;
+  bl.sdf = false;
+  for (vkptc_ctx* c : b->jobs) {
+    bl.effects = bl.effects || c->has_effects;
+    bl.sdf = bl.sdf || c->sdf_count != 0u;
+  }
   bl.occupancy = static_cast<int>(std::min(3u, t.occupancy));
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
   int max_optin = 0;
@@ -1634,6 +1706,7 @@ int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, cons
   }
   if (ctx->has_transmissive) return fail(ctx, VKPTC_UNSUPPORTED, "adjoint: transmissive materials are not supported");
   if (ctx->env_w) return fail(ctx, VKPTC_UNSUPPORTED, "adjoint: environment maps are not supported");
+  if (ctx->sdf_count) return fail(ctx, VKPTC_UNSUPPORTED, "adjoint: SDF primitives are not supported");
   const uint64_t npx = static_cast<uint64_t>(ctx->settings.width) * ctx->settings.height;
   if (npx == 0) return fail(ctx, VKPTC_INVALID_ARGUMENT, "empty film");
   if (target_rgb && target_floats != 3 * npx) {

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "sdf.cuh"
 
 namespace vkptc {
 
@@ -378,14 +379,23 @@ struct ShadeOut {
   uint32_t shadow_tests;
   V3 sh_o, sh_d, sh_c;
   float sh_t;
+  SdfCount sdf;       // SDF primitive tests of this bounce (extension and shadow)
 };
 
 // One bounce of the reference's trace loop for a path whose extension ray
-// (P.o, P.d) hit primitive `prim` at distance `ht` (prim == kMiss: no hit).
+// (P.o, P.d) hit triangle `prim` at distance `ht` (prim == kMiss: no triangle
+// hit).  The scene's SDF primitives are tested here, after the triangles, as
+// intersect_scene does; an SDF hit becomes prim = kSdfTag | index.  In a
+// scene without transmissive materials the shadow query's SDF test runs here
+// too: a query an SDF occludes is never queued for the triangle any-hit.
+// sdf_staged: a load-balanced stage has already folded the SDF hits into
+// (ht, prim) and tests the shadow queries itself (the loop driver).
 template <bool kParity, bool kEffects = true>
 __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSettings& st, const float* lights,
-                                               uint32_t depth, PathRegs& P, float ht, uint32_t prim) {
+                                               uint32_t depth, PathRegs& P, float ht, uint32_t prim,
+                                               bool sdf_staged = false) {
   ShadeOut R;
+  if (s.sdf_count != 0u && !sdf_staged) sdf_closest(s.sdf, s.sdf_count, P.o, P.d, ht, prim, R.sdf);
   R.next = false;
   R.shadow = false;
   R.shadow_tests = 0u;
@@ -399,9 +409,16 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
     rad = add(rad, mulv(thr, environment<kParity>(s, d)));
   } else {
     const V3 hp = add(o, mul(d, ht));
-    const float4 sh = __ldg(s.shade + prim);
-    const V3 gn = mk(sh.x, sh.y, sh.z);
-    const uint32_t mat_index = __float_as_uint(sh.w);
+    V3 gn;
+    uint32_t mat_index;
+    if (prim & kSdfTag) {
+      gn = sdf_hit_normal(s.sdf, prim & ~kSdfTag, o, d, ht);
+      mat_index = sdf_material(s.sdf, prim & ~kSdfTag);
+    } else {
+      const float4 sh = __ldg(s.shade + prim);
+      gn = mk(sh.x, sh.y, sh.z);
+      mat_index = __float_as_uint(sh.w);
+    }
     const bool entering = dot(d, gn) < 0.0f;
     const V3 nrm = entering ? gn : neg(gn);
     const uint32_t mi = mat_index < s.material_count - 1u ? mat_index : s.material_count - 1u;
@@ -441,7 +458,8 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
           c = mulv(thr, nq.radiance);
         }
         if (nq.remain > 0.004f) {
-          R.shadow = true;
+          R.shadow = !(s.sdf_count != 0u && !s.has_transmissive && !sdf_staged &&
+                       sdf_any(s.sdf, s.sdf_count, nq.origin, nq.dir, nq.remain, R.sdf));
           R.sh_o = nq.origin;
           R.sh_d = nq.dir;
           R.sh_t = nq.remain;

@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveS
     bool emit_next = false, emit_shadow = false;
     uint32_t p = 0u;
     uint32_t shadow_tests = 0u;
+    SdfCount sdf_n;
     // shadow query payload
     V3 sh_o = mk(0, 0, 0), sh_d = mk(0, 0, 0), sh_c = mk(0, 0, 0);
     float sh_t = 0.0f;
@@ -241,6 +242,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveS
       emit_next = R.next;
       emit_shadow = R.shadow;
       shadow_tests = R.shadow_tests;
+      sdf_n = R.sdf;
       sh_o = R.sh_o;
       sh_d = R.sh_d;
       sh_c = R.sh_c;
@@ -257,6 +259,11 @@ __global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveS
       w.sh_c[slot_s] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
     }
     warp_count(&ctr->shadow_tests, shadow_tests);
+    if (s.sdf_count != 0u) {
+      warp_count(&ctr->sdf_tests, sdf_n.tests);
+      warp_count(&ctr->sdf_steps, sdf_n.steps);
+      warp_count(&ctr->sdf_hits, sdf_n.hits);
+    }
   }
 }
 
@@ -283,6 +290,7 @@ __global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveSta
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     const uint32_t j = base + threadIdx.x;
     TraceStats st;
+    SdfCount sdf_n;
     if (j < n) {
       const float4 o4 = w.sh_o[j], d4 = w.sh_d[j];
       V3 so = mk(o4.x, o4.y, o4.z);
@@ -300,8 +308,10 @@ __global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveSta
           float t;
           uint32_t prim;
           trace_closest<kStats>(s, r, stk, t, prim, st, local_err);
+          if (s.sdf_count != 0u) sdf_closest(s.sdf, s.sdf_count, so, sd, t, prim, sdf_n);
           if (prim == kMiss || t >= remain) break;
-          const uint32_t mat_index = __float_as_uint(__ldg(s.shade + prim).w);
+          const uint32_t mat_index = (prim & kSdfTag) ? sdf_material(s.sdf, prim & ~kSdfTag)
+                                                      : __float_as_uint(__ldg(s.shade + prim).w);
           const uint32_t mi = mat_index < s.material_count - 1u ? mat_index : s.material_count - 1u;
           const float* mm = s.materials + 16u * mi;
           const bool tr = static_cast<uint32_t>(mm[7] + 0.5f) == 5u || mm[10] > 0.05f;
@@ -329,6 +339,11 @@ __global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveSta
       warp_count(&ctr->shadow_leaves, st.leaves);
       warp_count(&ctr->shadow_tris, st.tris);
       warp_count(&ctr->shadow_rays, j < n ? 1u : 0u);
+    }
+    if (s.sdf_count != 0u) {
+      warp_count(&ctr->sdf_tests, sdf_n.tests);
+      warp_count(&ctr->sdf_steps, sdf_n.steps);
+      warp_count(&ctr->sdf_hits, sdf_n.hits);
     }
   }
   if (local_err) atomicOr(err, local_err);

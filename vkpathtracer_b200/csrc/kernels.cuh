@@ -47,6 +47,7 @@ struct DevCounters {
   unsigned long long nodes, leaves, tris;
   unsigned long long shadow_nodes, shadow_leaves, shadow_tris;
   unsigned long long ext_rays, shadow_rays;   // traversal queries issued (stats mode)
+  unsigned long long sdf_tests, sdf_steps, sdf_hits;
 };
 
 struct LaunchShape {

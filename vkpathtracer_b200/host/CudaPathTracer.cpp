@@ -73,10 +73,6 @@ Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
 
 Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& scene) {
   if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
-  if (!scene.sdf_primitives.empty()) {
-    fail("the cuda backend renders triangle scenes (no SDF primitives)");
-    return Status::error(StatusCode::Unsupported, m_last_error);
-  }
   for (const auto& inst : scene.instances) {
     if (inst.has_flag(pt::kRTInstanceFlagDynamicTransform) && inst.local_vertex_count > 0u &&
         inst.local_index_count > 0u) {
@@ -147,6 +143,21 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
     v.environment_map_scale[1] = scene.environment_map_scale.y;
     v.environment_map_scale[2] = scene.environment_map_scale.z;
   }
+  // SDF primitives: 16-float records (RTSdfPrimitive field order); a shape
+  // outside the known six (SdfShape::Unknown) never hits, as in the reference.
+  std::vector<float> sdf(16 * scene.sdf_primitives.size(), 0.0f);
+  for (size_t i = 0; i < scene.sdf_primitives.size(); ++i) {
+    const pt::RTSdfPrimitive& p = scene.sdf_primitives[i];
+    float* w = &sdf[16 * i];
+    w[0] = static_cast<float>(static_cast<uint32_t>(p.shape));
+    w[1] = p.position.x; w[2] = p.position.y; w[3] = p.position.z;
+    w[4] = p.scale.x; w[5] = p.scale.y; w[6] = p.scale.z;
+    w[7] = p.rotation.x; w[8] = p.rotation.y; w[9] = p.rotation.z;
+    w[10] = static_cast<float>(p.material_index);
+    w[11] = p.radius; w[12] = p.param_a; w[13] = p.param_b;
+  }
+  v.sdf_primitives = sdf.empty() ? nullptr : sdf.data();
+  v.sdf_count = static_cast<uint32_t>(scene.sdf_primitives.size());
   const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
   if (st) m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
   return st;
@@ -245,6 +256,10 @@ pt::SampleCounters CudaPathTracer::read_counters() const {
     out.bvh_node_visits = c.bvh_node_visits;
     out.bvh_leaf_visits = c.bvh_leaf_visits;
     out.shadow_tests = c.shadow_tests;
+    out.sdf_tests = c.sdf_tests;
+    out.sdf_steps = c.sdf_steps;
+    out.sdf_hits = c.sdf_hits;
+    out.sdf_misses = c.sdf_misses;
   }
   return out;
 }

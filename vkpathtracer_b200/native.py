@@ -50,7 +50,11 @@ class SceneView(ctypes.Structure):
                 ("camera_fov_deg", ctypes.c_float), ("camera_aperture_radius", ctypes.c_float),
                 ("camera_focus_distance", ctypes.c_float), ("environment_map", ctypes.c_void_p),
                 ("environment_map_width", ctypes.c_uint32), ("environment_map_height", ctypes.c_uint32),
-                ("environment_map_scale", ctypes.c_float * 3)]
+                ("environment_map_scale", ctypes.c_float * 3),
+                ("sdf_primitives", ctypes.c_void_p), ("sdf_count", ctypes.c_uint32)]
+
+# vkptc_sdf_shape
+SDF_SPHERE, SDF_BOX, SDF_ROUNDED_BOX, SDF_PLANE, SDF_TORUS, SDF_CAPSULE = range(6)
 
 
 class BvhView(ctypes.Structure):

@@ -101,6 +101,7 @@ class Scene:
     name: str = "scene"
     env_map: Optional[np.ndarray] = None   # (H, W, 3) float32 equirectangular map, row 0 toward +y
     env_scale: tuple = (0.0, 0.0, 0.0)     # texel multiplier (all <= 1e-6 means 1)
+    sdf: Optional[np.ndarray] = None       # (N, 16) float32 SDF primitive records (sdf_primitive)
 
     @property
     def triangle_count(self) -> int:
@@ -289,6 +290,87 @@ def effect_gallery(seed: int = 11) -> Scene:
     v, t, inst = b.arrays()
     cam = Camera(position=(0.0, 0.5, 1.9), target=(0.0, 0.3, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0)
     return Scene(v, t, inst, np.array(mats), np.array(lights), (0.02, 0.02, 0.03), cam, "effect_gallery").contiguous()
+
+
+SDF_SHAPES = {"sphere": 0, "box": 1, "rounded_box": 2, "plane": 3, "torus": 4, "capsule": 5}
+
+
+def sdf_primitive(shape: str, position, scale=(1.0, 1.0, 1.0), rotation=(0.0, 0.0, 0.0), material: int = 0,
+                  radius: float = 0.5, param_a: float = 0.0, param_b: float = 0.0) -> np.ndarray:
+    """One RTSdfPrimitive record (src/pathtracer/PathTracer.h:330-339) as 16
+    floats: shape, position3, scale3, rotation3 (Euler radians), material,
+    radius, param_a, param_b, 0, 0.  The reference measures a box's and a
+    rounded box's half extents in primitive space (world / scale), so their
+    world half extents are scale * scale."""
+    r = np.zeros(16, np.float32)
+    r[0] = SDF_SHAPES[shape]
+    r[1:4], r[4:7], r[7:10] = position, scale, rotation
+    r[10], r[11], r[12], r[13] = material, radius, param_a, param_b
+    return r
+
+
+def sdf_gallery(seed: int = 7, glass: bool = False) -> Scene:
+    """One SDF primitive of every shape on a triangle ground with two triangle
+    boxes: a scaled, rotated ellipsoid (analytic sphere test), a box, a rounded
+    box, a torus (scaled) and a capsule (sphere-traced), and a vertical SDF
+    plane as the back wall.  The marched shapes keep scale ~1: the reference
+    marches by primitive-space distance (world / scale), which overshoots thin
+    shapes at small scales.  Materials span Lambert, glossy, metal, mirror and
+    sheen; glass=True makes the ellipsoid transmissive (the shadow test then
+    steps through it).  One point light and a constant sky."""
+    st = Stream(seed)
+    b = _Builder()
+    mats: list = [material(albedo=(0.55, 0.55, 0.5), roughness=1.0)]
+    v, t = _quad((-8.0, 0.0, -8.0), (-8.0, 0.0, 8.0), (8.0, 0.0, 8.0), (8.0, 0.0, -8.0))
+    b.add(v, t, 0)
+    for k in range(2):
+        mats.append(material(albedo=tuple(st.uniform(0.3, 0.8) for _ in range(3)), roughness=1.0))
+        v, t = _box((-3.2 + 6.0 * k, 0.4, 2.6 - 5.0 * k), (0.4, 0.4, 0.4), st.uniform(-30.0, 30.0))
+        b.add(v, t, len(mats) - 1)
+    lights = [point_light((3.0, 8.0, 5.0), (1.0, 0.95, 0.9), 120.0)]
+    base = len(mats)
+    mats.append(material(albedo=(0.9, 0.9, 0.95), roughness=0.0, model=5, ior=1.5, transmission=0.9) if glass
+                else material(albedo=(0.8, 0.3, 0.2), roughness=0.35, model=3))
+    mats.append(material(albedo=(0.3, 0.6, 0.8), roughness=1.0))
+    mats.append(material(albedo=(0.9, 0.75, 0.4), roughness=0.3, metallic=0.9, model=4))
+    mats.append(material(albedo=(0.95, 0.95, 0.95), roughness=0.0, model=2))
+    mats.append(material(albedo=(0.5, 0.8, 0.4), roughness=0.7, model=6, sheen=0.6))
+    mats.append(material(albedo=(0.7, 0.62, 0.55), roughness=1.0))
+    sdf = np.stack([
+        sdf_primitive("sphere", (-3.0, 1.0, 0.0), (1.2, 1.0, 0.9), (0.3, 0.5, 0.0), base + 0, radius=1.0),
+        sdf_primitive("box", (0.0, 1.0, -1.5), (1.0, 1.0, 1.0), (0.0, 0.6, 0.0), base + 1),
+        sdf_primitive("rounded_box", (3.0, 1.0, -0.5), (1.0, 1.0, 1.0), (0.2, -0.4, 0.1), base + 2, param_a=0.3),
+        sdf_primitive("torus", (-1.3, 0.9, 2.2), (0.8, 0.8, 0.8), (1.1, 0.3, 0.0), base + 3, radius=0.3,
+                      param_a=1.0),
+        sdf_primitive("capsule", (1.8, 1.4, 2.0), (1.0, 1.0, 1.0), (0.0, 0.0, 0.7), base + 4, radius=0.5,
+                      param_a=0.8),
+        sdf_primitive("plane", (0.0, 0.0, -6.0), (1.0, 1.0, 1.0), (1.5707964, 0.0, 0.0), base + 5),
+    ])
+    v, t, inst = b.arrays()
+    cam = Camera(position=(0.0, 4.5, 10.0), target=(0.0, 0.8, 0.0), up=(0.0, 1.0, 0.0), fov_deg=45.0)
+    return Scene(v, t, inst, np.array(mats), np.array(lights), (0.25, 0.3, 0.4), cam,
+                 "sdf_glass" if glass else "sdf_gallery", sdf=sdf).contiguous()
+
+
+def sdf_complexity() -> Scene:
+    """SDF primitives only (no triangles), after the reference's SDF
+    complexity scene (assets/scenes/sdf_complexity.json): a sphere of scale
+    0.8 at (0, 1, 0) and a box of scale (0.4, 0.6, 0.4) at (1.2, 0.5, 0) in
+    one matte material, on an SDF ground plane, lit by one point light and a
+    constant sky."""
+    mats = np.array([material(albedo=(0.72, 0.72, 0.88), roughness=1.0),
+                     material(albedo=(0.5, 0.5, 0.45), roughness=1.0)])
+    lights = np.array([point_light((2.0, 4.0, 3.0), (0.85, 0.9, 1.0), 14.0)])
+    sdf = np.stack([
+        sdf_primitive("sphere", (0.0, 1.0, 0.0), (0.8, 0.8, 0.8), material=0, radius=0.8),
+        sdf_primitive("box", (1.2, 0.5, 0.0), (0.4, 0.6, 0.4), material=0, radius=1.0, param_a=0.4),
+        sdf_primitive("plane", (0.0, 0.0, 0.0), material=1),
+    ])
+    cam = Camera(position=(0.6, 1.4, 4.2), target=(0.5, 0.6, 0.0), up=(0.0, 1.0, 0.0), fov_deg=58.0)
+    empty_v = np.zeros((0, 3), np.float32)
+    empty_t = np.zeros((0, 3), np.uint32)
+    return Scene(empty_v, empty_t, np.zeros((0, 3), np.uint32), mats, lights, (0.35, 0.4, 0.5), cam,
+                 "sdf_complexity", sdf=sdf).contiguous()
 
 
 def cornell_settings(width=256, height=256, spp=16) -> RenderSettings:

@@ -104,6 +104,10 @@ def scene_view(scene: Scene):
         v.environment_map = _ptr(env)
         v.environment_map_height, v.environment_map_width = env.shape[0], env.shape[1]
         v.environment_map_scale[:] = scene.env_scale
+    if scene.sdf is not None and len(scene.sdf):
+        sdf = np.ascontiguousarray(scene.sdf, np.float32).reshape(-1, 16)
+        keep = keep + (sdf,)
+        v.sdf_primitives, v.sdf_count = _ptr(sdf), sdf.shape[0]
     return v, keep
 
 
