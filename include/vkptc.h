@@ -68,11 +68,17 @@ typedef struct vkptc_config {
   uint32_t bvh_mode;         /* traversal tree: VKPTC_BVH_REFERENCE (the reference builder's tree,
                                 flattened) or VKPTC_BVH_SAH (binned SAH); hit ids are the
                                 reference's in both (ties/parallel rule use the reference tree) */
-  uint32_t reserved[4];
+  uint32_t build_mode;       /* where vkptc_build_acceleration builds: VKPTC_BUILD_DEVICE (default;
+                                the same reference tree, bit for bit, plus the traversal tree,
+                                built by CUDA kernels) or VKPTC_BUILD_HOST (the host restatement of
+                                ParallelBvhBuilder, kept as the parity mode) */
+  uint32_t reserved[3];
 } vkptc_config;
 
 #define VKPTC_BVH_REFERENCE 0u
 #define VKPTC_BVH_SAH 1u
+#define VKPTC_BUILD_DEVICE 0u
+#define VKPTC_BUILD_HOST 1u
 
 /* Mirrors RenderSettings (src/pathtracer/PathTracer.h:134-178). */
 typedef struct vkptc_render_settings {
@@ -215,6 +221,17 @@ int32_t vkptc_build_acceleration(vkptc_ctx* ctx);
  * output over the accelerator's primitive order, CpuBvhAccelerator.cpp:247-256). */
 int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh);
 int32_t vkptc_get_accel_info(vkptc_ctx* ctx, vkptc_accel_info* out);
+/* Extension (no reference counterpart): copies one device array of the built
+ * accelerator to host memory, for inspection and for checking the device
+ * build against the host build.  what: VKPTC_ACCEL_WIDE_NODES (128 B each),
+ * VKPTC_ACCEL_TRIANGLES (48 B each, leaf order), VKPTC_ACCEL_TIE_NODES (32 B
+ * each, the reference binary tree), VKPTC_ACCEL_SHADING (16 B per primitive).
+ * *bytes receives the array's size; out may be NULL to query it. */
+int32_t vkptc_read_accel(vkptc_ctx* ctx, uint32_t what, void* out, uint64_t capacity, uint64_t* bytes);
+#define VKPTC_ACCEL_WIDE_NODES 0u
+#define VKPTC_ACCEL_TRIANGLES 1u
+#define VKPTC_ACCEL_TIE_NODES 2u
+#define VKPTC_ACCEL_SHADING 3u
 /* Host-only (no device needed): the binary BVH vkptc_build_acceleration
  * builds, in ParallelBvhBuilder's layout, for callers that keep a CPU copy.
  * replaces ParallelBvhBuilder::build (src/cpu/ParallelBvhBuilder.cpp:165-257)

@@ -1,0 +1,1220 @@
+// bvh_build.cu -- the acceleration structure built on the device.
+//
+// Steps (all on the stream given; the host only sizes launches between the
+// levels of the top-down build):
+//   1. flatten: one thread per candidate triangle of every instance, invalid
+//      ones dropped by a scan (FlattenScene's order and arithmetic);
+//   2. the reference's midpoint tree (ParallelBvhBuilder, deterministic mode,
+//      src/cpu/ParallelBvhBuilder.cpp:61-257), top-down:
+//        nodes above kSmallNode primitives, level by level over all nodes of
+//        the level at once: centroid bounds by a segmented warp reduction
+//        plus one atomic per run, the widest axis and its midpoint, a flag per
+//        primitive, an exclusive scan, and a stable scatter (left flags first,
+//        in order; count/2 when one side is empty, order unchanged);
+//        smaller subtrees by one thread each, sequentially, the same steps;
+//      then node bounds by a bottom-up refit (union of children; min/max are
+//      exact, so the result equals the top-down bounds of the reference) and
+//      the reference's node ids: the reference allocates the two children of
+//      the k-th internal node of its depth-first pre-order as 2k+1, 2k+2, and
+//      k is found by walking up from each node, adding 1 per ancestor and the
+//      internal-node count of the left subtree when coming from the right;
+//   3. optionally a binned-SAH traversal tree (32 bins per axis) with the same
+//      machinery;
+//   4. the wide collapse of the traversal tree (CollapseToWide's greedy
+//      largest-area opening, wide nodes in depth-first pre-order, found the
+//      same way), triangle records in leaf order and the tie records of the
+//      reference tree.
+// Every array equals the host path's bit for bit (tested).  A non-finite
+// vertex, edge or bound sends the build back to the host path (min/max of NaN
+// depends on operand order, and NaN payloads differ between x86 and the GPU).
+#include "bvh_build.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+namespace vkptc {
+namespace {
+
+constexpr float kPadB = 1e-4f;
+constexpr uint32_t kSmallNode = 64;   // subtrees of at most this many primitives: one thread each
+constexpr uint32_t kLeafMax = 4;      // ParallelBvhBuilder's leaf threshold
+constexpr int kScanThreads = 512;
+constexpr uint32_t kScanBlock = 2 * kScanThreads;
+constexpr int kThreads = 256;
+constexpr int kSahBins = 32;
+
+inline unsigned grid_for(uint64_t n, int threads = kThreads) {
+  return static_cast<unsigned>(std::max<uint64_t>(1, (n + threads - 1) / threads));
+}
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ float bmin(float a, float b) { return (b < a) ? b : a; }   // std::min order
+__device__ __forceinline__ float bmax(float a, float b) { return (a < b) ? b : a; }   // std::max order
+// Order-preserving map of floats to unsigned keys (atomicMin/Max on floats).
+__device__ __forceinline__ uint32_t fkey(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fval(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+struct TNode {          // binary node under construction (temporary ids)
+  int32_t begin, count, left, right, parent;
+};
+
+// ---------------------------------------------------------------- scan
+// Exclusive scan of n+1 elements (element n reads as 0), so out[n] = total.
+__global__ void __launch_bounds__(kScanThreads) k_scan_blocks(const uint32_t* __restrict__ in, uint32_t n,
+                                                              uint32_t* __restrict__ out, uint32_t m,
+                                                              uint32_t* __restrict__ sums) {
+  __shared__ uint32_t warp_tot[kScanThreads / 32];
+  const uint32_t i0 = blockIdx.x * kScanBlock + 2u * threadIdx.x, i1 = i0 + 1u;
+  const uint32_t a = i0 < n ? in[i0] : 0u, b = i1 < n ? in[i1] : 0u;
+  const uint32_t s = a + b;
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t x = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (static_cast<int>(lane) >= o) x += y;
+  }
+  if (lane == 31u) warp_tot[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = lane < kScanThreads / 32 ? warp_tot[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (static_cast<int>(lane) >= o) t += y;
+    }
+    if (lane < kScanThreads / 32) warp_tot[lane] = t;
+  }
+  __syncthreads();
+  const uint32_t off = warp ? warp_tot[warp - 1] : 0u;
+  const uint32_t excl = off + x - s;
+  if (i0 < m) out[i0] = excl;
+  if (i1 < m) out[i1] = excl + a;
+  if (threadIdx.x == kScanThreads - 1) sums[blockIdx.x] = off + x;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(uint32_t* __restrict__ out, uint32_t m,
+                                                           const uint32_t* __restrict__ offs) {
+  const uint32_t i0 = blockIdx.x * kScanBlock + 2u * threadIdx.x;
+  const uint32_t add = offs[blockIdx.x];
+  if (i0 < m) out[i0] += add;
+  if (i0 + 1u < m) out[i0 + 1u] += add;
+}
+
+// Stream-ordered scratch allocations, released on destruction.
+struct Scratch {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  cudaError_t err = cudaSuccess;
+  template <class T>
+  T* get(size_t n) {
+    void* p = nullptr;
+    if (err != cudaSuccess) return nullptr;
+    err = cudaMallocAsync(&p, std::max<size_t>(1, n) * sizeof(T), s);
+    if (err != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  ~Scratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+  }
+};
+
+// out: n+1 entries.
+cudaError_t exclusive_scan(const uint32_t* in, uint32_t n, uint32_t* out, Scratch& sc) {
+  const uint32_t m = n + 1u;
+  const uint32_t blocks = (m + kScanBlock - 1u) / kScanBlock;
+  uint32_t* sums = sc.get<uint32_t>(blocks);
+  if (!sums) return sc.err;
+  k_scan_blocks<<<blocks, kScanThreads, 0, sc.s>>>(in, n, out, m, sums);
+  if (blocks > 1u) {
+    uint32_t* offs = sc.get<uint32_t>(blocks + 1u);
+    if (!offs) return sc.err;
+    cudaError_t e = exclusive_scan(sums, blocks, offs, sc);
+    if (e != cudaSuccess) return e;
+    k_scan_add<<<blocks, kScanThreads, 0, sc.s>>>(out, m, offs);
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- flatten
+__device__ __forceinline__ uint32_t find_instance(const unsigned long long* prefix, uint32_t count,
+                                                  unsigned long long c) {
+  uint32_t lo = 0u, hi = count;   // prefix[lo] <= c < prefix[hi]
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (prefix[mid] <= c) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+struct FlatIn {
+  const float* v;
+  uint32_t nv;
+  const uint32_t* idx;
+  uint32_t ni;
+  const uint32_t* inst;
+  const unsigned long long* prefix;
+  uint32_t ninst;
+  uint32_t candidates;
+};
+
+__global__ void k_flat_valid(FlatIn f, uint32_t* __restrict__ flag) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= f.candidates) return;
+  const uint32_t i = find_instance(f.prefix, f.ninst, c);
+  const unsigned long long k = c - f.prefix[i];
+  const unsigned long long base = (static_cast<unsigned long long>(f.inst[3 * i]) + k) * 3ull;
+  bool ok = base + 2ull < f.ni;
+  if (ok) ok = f.idx[base] < f.nv && f.idx[base + 1] < f.nv && f.idx[base + 2] < f.nv;
+  flag[c] = ok ? 1u : 0u;
+}
+
+__device__ __forceinline__ float min3(float a, float b, float c) {   // std::min({a, b, c})
+  float m = a;
+  if (b < m) m = b;
+  if (c < m) m = c;
+  return m;
+}
+__device__ __forceinline__ float max3(float a, float b, float c) {   // std::max({a, b, c})
+  float m = a;
+  if (m < b) m = b;
+  if (m < c) m = c;
+  return m;
+}
+
+__global__ void k_flat_write(FlatIn f, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                             float4* __restrict__ pv, float4* __restrict__ shade, float4* __restrict__ blo,
+                             float4* __restrict__ bhi, uint32_t* __restrict__ nonfinite) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= f.candidates || !flag[c]) return;
+  const uint32_t i = find_instance(f.prefix, f.ninst, c);
+  const unsigned long long k = c - f.prefix[i];
+  const unsigned long long base = (static_cast<unsigned long long>(f.inst[3 * i]) + k) * 3ull;
+  const uint32_t mat = f.inst[3 * i + 2];
+  const float* a = f.v + 3ull * f.idx[base];
+  const float* b = f.v + 3ull * f.idx[base + 1];
+  const float* cc = f.v + 3ull * f.idx[base + 2];
+  const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+  const float e2x = cc[0] - a[0], e2y = cc[1] - a[1], e2z = cc[2] - a[2];
+  const float nx = e1y * e2z - e1z * e2y;
+  const float ny = e1z * e2x - e1x * e2z;
+  const float nz = e1x * e2y - e1y * e2x;
+  const float l2 = nx * nx + ny * ny + nz * nz;
+  float4 n;
+  if (l2 <= kPadB * kPadB) {
+    n = make_float4(0.0f, 1.0f, 0.0f, __uint_as_float(mat));
+  } else {
+    const float inv = 1.0f / sqrtf(l2);
+    n = make_float4(nx * inv, ny * inv, nz * inv, __uint_as_float(mat));
+  }
+  const uint32_t p = pos[c];
+  pv[3 * p + 0] = make_float4(a[0], a[1], a[2], e1x);
+  pv[3 * p + 1] = make_float4(e1y, e1z, e2x, e2y);
+  pv[3 * p + 2] = make_float4(e2z, 0.0f, 0.0f, 0.0f);
+  shade[p] = n;
+  const float4 lo = make_float4(min3(a[0], b[0], cc[0]) - kPadB, min3(a[1], b[1], cc[1]) - kPadB,
+                                min3(a[2], b[2], cc[2]) - kPadB, 0.0f);
+  const float4 hi = make_float4(max3(a[0], b[0], cc[0]) + kPadB, max3(a[1], b[1], cc[1]) + kPadB,
+                                max3(a[2], b[2], cc[2]) + kPadB, 0.0f);
+  blo[p] = lo;
+  bhi[p] = hi;
+  // Any non-finite vertex coordinate, edge or bound: the host path builds this scene (NaN
+  // propagation through min/max and subtraction is operand-order and platform dependent).
+  bool fin = isfinite(lo.x) && isfinite(lo.y) && isfinite(lo.z) && isfinite(hi.x) && isfinite(hi.y) &&
+             isfinite(hi.z) && isfinite(0.5f * (lo.x + hi.x)) && isfinite(0.5f * (lo.y + hi.y)) &&
+             isfinite(0.5f * (lo.z + hi.z));
+  for (int q = 0; q < 3; ++q) fin = fin && isfinite(a[q]) && isfinite(b[q]) && isfinite(cc[q]);
+  fin = fin && isfinite(e1x) && isfinite(e1y) && isfinite(e1z) && isfinite(e2x) && isfinite(e2y) && isfinite(e2z);
+  if (!fin) atomicOr(nonfinite, 1u);
+}
+
+// ---------------------------------------------------------------- top-down build
+__device__ __forceinline__ float centroid(const float4* blo, const float4* bhi, uint32_t p, int axis) {
+  const float4 lo = blo[p], hi = bhi[p];
+  const float l = axis == 0 ? lo.x : (axis == 1 ? lo.y : lo.z);
+  const float h = axis == 0 ? hi.x : (axis == 1 ? hi.y : hi.z);
+  return 0.5f * (l + h);
+}
+
+struct BuildArrays {
+  const float4* blo;
+  const float4* bhi;
+  TNode* nodes;
+  int32_t* slot_of;        // per temporary node: slot in this level's active list, or -1
+  uint32_t* cb;            // per slot: 6 keys (centroid lo xyz, hi xyz)
+  int32_t* axis;           // per slot (-1: all centroids coincide, SAH)
+  float* split;            // per slot (midpoint) / best bin (SAH, as bits)
+  uint32_t* nl;            // per slot
+  uint32_t* ident;         // per slot: 1 = order unchanged, count/2 split
+  uint32_t* counter;       // [0] next temporary node id, [1] next-level active count, [2] small count
+};
+
+__global__ void k_level_init(BuildArrays A, const uint32_t* __restrict__ act, uint32_t n_act) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_act) return;
+  A.slot_of[act[s]] = static_cast<int32_t>(s);
+  uint32_t* k = A.cb + 6 * s;
+  k[0] = k[1] = k[2] = 0xffffffffu;   // min keys
+  k[3] = k[4] = k[5] = 0u;            // max keys
+}
+
+__global__ void k_level_done(BuildArrays A, const uint32_t* __restrict__ act, uint32_t n_act) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n_act) A.slot_of[act[s]] = -1;
+}
+
+// Centroid bounds of every active node: segmented warp reduction over runs of
+// positions of the same node, then one atomic per run and key.
+__global__ void k_centroid_bounds(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
+                                  uint32_t n) {
+  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31u;
+  int32_t s = -1;
+  uint32_t kmin[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, kmax[3] = {0u, 0u, 0u};
+  if (pos < n) {
+    s = A.slot_of[node_of[pos]];
+    if (s >= 0) {
+      const uint32_t p = idx[pos];
+      for (int a = 0; a < 3; ++a) kmin[a] = kmax[a] = fkey(centroid(A.blo, A.bhi, p, a));
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t so = __shfl_down_sync(0xffffffffu, s, o);
+    uint32_t omin[3], omax[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      omin[a] = __shfl_down_sync(0xffffffffu, kmin[a], o);
+      omax[a] = __shfl_down_sync(0xffffffffu, kmax[a], o);
+    }
+    if (static_cast<int>(lane) + o < 32 && so == s) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        kmin[a] = min(kmin[a], omin[a]);
+        kmax[a] = max(kmax[a], omax[a]);
+      }
+    }
+  }
+  const int32_t sp = __shfl_up_sync(0xffffffffu, s, 1);
+  const bool head = s >= 0 && (lane == 0u || sp != s);
+  if (head) {
+    uint32_t* k = A.cb + 6 * s;
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(k + a, kmin[a]);
+      atomicMax(k + 3 + a, kmax[a]);
+    }
+  }
+}
+
+// Widest centroid axis and its midpoint (BuildBinaryBvh's split).
+__global__ void k_midpoint_split(BuildArrays A, uint32_t n_act) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_act) return;
+  const uint32_t* k = A.cb + 6 * s;
+  float clo[3], chi[3];
+  for (int a = 0; a < 3; ++a) {
+    clo[a] = fval(k[a]);
+    chi[a] = fval(k[3 + a]);
+  }
+  int axis = 0;
+  float widest = chi[0] - clo[0];
+  for (int a = 1; a < 3; ++a) {
+    const float e = chi[a] - clo[a];
+    if (e > widest) {
+      widest = e;
+      axis = a;
+    }
+  }
+  A.axis[s] = axis;
+  A.split[s] = 0.5f * (clo[axis] + chi[axis]);
+}
+
+__device__ __forceinline__ bool goes_left(const BuildArrays& A, uint32_t p, int32_t s, bool sah) {
+  const int axis = A.axis[s];
+  if (!sah) return centroid(A.blo, A.bhi, p, axis) < A.split[s];
+  if (axis < 0) return false;
+  const uint32_t* k = A.cb + 6 * s;
+  const float c0 = fval(k[axis]);
+  const float scale = static_cast<float>(kSahBins) / (fval(k[3 + axis]) - c0);
+  int bin = static_cast<int>((centroid(A.blo, A.bhi, p, axis) - c0) * scale);
+  bin = bin < 0 ? 0 : (bin > kSahBins - 1 ? kSahBins - 1 : bin);
+  return bin <= static_cast<int>(__float_as_uint(A.split[s]));
+}
+
+__global__ void k_flags(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
+                        uint32_t n, uint32_t* __restrict__ flag, bool sah) {
+  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= n) return;
+  const int32_t s = A.slot_of[node_of[pos]];
+  flag[pos] = (s >= 0 && goes_left(A, idx[pos], s, sah)) ? 1u : 0u;
+}
+
+// Children of every active node; big ones go to the next level's list, small
+// ones to the per-thread list, leaves nowhere.
+__global__ void k_children(BuildArrays A, const uint32_t* __restrict__ act, uint32_t n_act, uint32_t base,
+                           const uint32_t* __restrict__ excl, uint32_t* __restrict__ next_act,
+                           uint32_t* __restrict__ small) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_act) return;
+  const uint32_t nd = act[s];
+  TNode& t = A.nodes[nd];
+  const uint32_t b = static_cast<uint32_t>(t.begin), n = static_cast<uint32_t>(t.count);
+  uint32_t nl = excl[b + n] - excl[b];
+  const bool ident = nl == 0u || nl == n;
+  if (ident) nl = n / 2u;
+  A.nl[s] = nl;
+  A.ident[s] = ident ? 1u : 0u;
+  const uint32_t l = base + 2u * s, r = l + 1u;
+  t.left = static_cast<int32_t>(l);
+  t.right = static_cast<int32_t>(r);
+  const uint32_t cnt[2] = {nl, n - nl};
+  const uint32_t id[2] = {l, r};
+  for (int c = 0; c < 2; ++c) {
+    A.nodes[id[c]] = TNode{static_cast<int32_t>(c == 0 ? b : b + nl), static_cast<int32_t>(cnt[c]), -1, -1,
+                           static_cast<int32_t>(nd)};
+    A.slot_of[id[c]] = -1;
+    if (cnt[c] > kSmallNode) next_act[atomicAdd(&A.counter[1], 1u)] = id[c];
+    else if (cnt[c] > kLeafMax) small[atomicAdd(&A.counter[2], 1u)] = id[c];
+  }
+}
+
+__global__ void k_scatter(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
+                          uint32_t n, const uint32_t* __restrict__ excl, uint32_t* __restrict__ idx2,
+                          uint32_t* __restrict__ node2) {
+  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= n) return;
+  const uint32_t nd = node_of[pos];
+  const int32_t s = A.slot_of[nd];
+  if (s < 0) {
+    idx2[pos] = idx[pos];
+    node2[pos] = nd;
+    return;
+  }
+  const TNode t = A.nodes[nd];
+  const uint32_t b = static_cast<uint32_t>(t.begin);
+  const uint32_t nl = A.nl[s];
+  const uint32_t i = pos - b;
+  uint32_t dst;
+  bool left;
+  if (A.ident[s]) {
+    dst = pos;
+    left = i < nl;
+  } else {
+    const uint32_t rk = excl[pos] - excl[b];
+    left = excl[pos + 1] != excl[pos];
+    dst = left ? b + rk : b + nl + (i - rk);
+  }
+  idx2[dst] = idx[pos];
+  node2[dst] = static_cast<uint32_t>(left ? t.left : t.right);
+}
+
+// Sequential build of one small subtree per thread (same split rules).
+template <bool kSah>
+__global__ void k_small(BuildArrays A, const uint32_t* __restrict__ small, uint32_t n_small, uint32_t* __restrict__ idx) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_small) return;
+  uint32_t stack[64];
+  uint32_t tmp[kSmallNode];
+  int sp = 0;
+  stack[sp++] = small[w];
+  while (sp > 0) {
+    const uint32_t nd = stack[--sp];
+    const TNode t = A.nodes[nd];
+    const uint32_t b = static_cast<uint32_t>(t.begin), n = static_cast<uint32_t>(t.count);
+    if (n <= kLeafMax) continue;
+    float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t p = idx[b + i];
+      for (int a = 0; a < 3; ++a) {
+        const float c = centroid(A.blo, A.bhi, p, a);
+        clo[a] = bmin(clo[a], c);
+        chi[a] = bmax(chi[a], c);
+      }
+    }
+    uint32_t nl = 0u;
+    bool ident;
+    if (!kSah) {
+      int axis = 0;
+      float widest = chi[0] - clo[0];
+      for (int a = 1; a < 3; ++a) {
+        const float e = chi[a] - clo[a];
+        if (e > widest) {
+          widest = e;
+          axis = a;
+        }
+      }
+      const float split = 0.5f * (clo[axis] + chi[axis]);
+      uint32_t nr = 0u;
+      for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t p = idx[b + i];
+        if (centroid(A.blo, A.bhi, p, axis) < split) idx[b + nl++] = p;
+        else tmp[nr++] = p;
+      }
+      for (uint32_t i = 0; i < nr; ++i) idx[b + nl + i] = tmp[i];
+      ident = nl == 0u || nl == n;
+    } else {
+      // Binned SAH over the three axes (32 bins), counts and bounds per bin.
+      int best_axis = -1, best_bin = -1;
+      float best_cost = FLT_MAX;
+      for (int a = 0; a < 3; ++a) {
+        const float ext = chi[a] - clo[a];
+        if (!(ext > 0.0f)) continue;
+        const float scale = static_cast<float>(kSahBins) / ext;
+        uint32_t cnt[kSahBins];
+        float blo[kSahBins][3], bhi[kSahBins][3];
+        for (int k = 0; k < kSahBins; ++k) {
+          cnt[k] = 0u;
+          for (int q = 0; q < 3; ++q) {
+            blo[k][q] = FLT_MAX;
+            bhi[k][q] = -FLT_MAX;
+          }
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+          const uint32_t p = idx[b + i];
+          int k = static_cast<int>((centroid(A.blo, A.bhi, p, a) - clo[a]) * scale);
+          k = k < 0 ? 0 : (k > kSahBins - 1 ? kSahBins - 1 : k);
+          ++cnt[k];
+          const float4 lo = A.blo[p], hi = A.bhi[p];
+          blo[k][0] = bmin(blo[k][0], lo.x);
+          blo[k][1] = bmin(blo[k][1], lo.y);
+          blo[k][2] = bmin(blo[k][2], lo.z);
+          bhi[k][0] = bmax(bhi[k][0], hi.x);
+          bhi[k][1] = bmax(bhi[k][1], hi.y);
+          bhi[k][2] = bmax(bhi[k][2], hi.z);
+        }
+        float rarea[kSahBins];
+        uint32_t rcnt[kSahBins];
+        float rlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        uint32_t rc = 0u;
+        for (int k = kSahBins - 1; k > 0; --k) {
+          rc += cnt[k];
+          for (int q = 0; q < 3; ++q) {
+            rlo[q] = bmin(rlo[q], blo[k][q]);
+            rhi[q] = bmax(rhi[q], bhi[k][q]);
+          }
+          rcnt[k] = rc;
+          const float dx = rhi[0] - rlo[0], dy = rhi[1] - rlo[1], dz = rhi[2] - rlo[2];
+          rarea[k] = rc ? dx * dy + dy * dz + dz * dx : 0.0f;
+        }
+        float llo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, lhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        uint32_t lc = 0u;
+        for (int k = 0; k < kSahBins - 1; ++k) {
+          lc += cnt[k];
+          for (int q = 0; q < 3; ++q) {
+            llo[q] = bmin(llo[q], blo[k][q]);
+            lhi[q] = bmax(lhi[q], bhi[k][q]);
+          }
+          if (lc == 0u || rcnt[k + 1] == 0u) continue;
+          const float dx = lhi[0] - llo[0], dy = lhi[1] - llo[1], dz = lhi[2] - llo[2];
+          const float cost = (dx * dy + dy * dz + dz * dx) * static_cast<float>(lc) +
+                             rarea[k + 1] * static_cast<float>(rcnt[k + 1]);
+          if (cost < best_cost) {
+            best_cost = cost;
+            best_axis = a;
+            best_bin = k;
+          }
+        }
+      }
+      if (best_axis >= 0) {
+        const float c0 = clo[best_axis];
+        const float scale = static_cast<float>(kSahBins) / (chi[best_axis] - c0);
+        uint32_t nr = 0u;
+        for (uint32_t i = 0; i < n; ++i) {
+          const uint32_t p = idx[b + i];
+          int k = static_cast<int>((centroid(A.blo, A.bhi, p, best_axis) - c0) * scale);
+          k = k < 0 ? 0 : (k > kSahBins - 1 ? kSahBins - 1 : k);
+          if (k <= best_bin) idx[b + nl++] = p;
+          else tmp[nr++] = p;
+        }
+        for (uint32_t i = 0; i < nr; ++i) idx[b + nl + i] = tmp[i];
+      }
+      ident = nl == 0u || nl == n;
+    }
+    if (ident) nl = n / 2u;
+    const uint32_t l = atomicAdd(&A.counter[0], 2u), r = l + 1u;
+    A.nodes[nd].left = static_cast<int32_t>(l);
+    A.nodes[nd].right = static_cast<int32_t>(r);
+    A.nodes[l] = TNode{static_cast<int32_t>(b), static_cast<int32_t>(nl), -1, -1, static_cast<int32_t>(nd)};
+    A.nodes[r] = TNode{static_cast<int32_t>(b + nl), static_cast<int32_t>(n - nl), -1, -1, static_cast<int32_t>(nd)};
+    if (sp + 2 <= 64) {
+      stack[sp++] = r;
+      stack[sp++] = l;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- SAH binning of large nodes
+// Per active slot: 3 axes x 32 bins x (count, 6 bound keys).
+constexpr int kBinWords = 7;
+__global__ void k_sah_bin_init(uint32_t* __restrict__ bins, uint32_t n_act) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_act * 3u * kSahBins) return;
+  uint32_t* w = bins + kBinWords * i;
+  w[0] = 0u;
+  w[1] = w[2] = w[3] = 0xffffffffu;
+  w[4] = w[5] = w[6] = 0u;
+}
+
+__global__ void k_sah_bin(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
+                          uint32_t n, uint32_t* __restrict__ bins) {
+  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  int32_t s = -1;
+  uint32_t p = 0u;
+  if (pos < n) {
+    s = A.slot_of[node_of[pos]];
+    if (s >= 0) p = idx[pos];
+  }
+  const unsigned active = __ballot_sync(0xffffffffu, s >= 0);
+  if (s < 0) return;
+  const uint32_t* k = A.cb + 6 * s;
+  const float4 lo = A.blo[p], hi = A.bhi[p];
+  const uint32_t klo[3] = {fkey(lo.x), fkey(lo.y), fkey(lo.z)};
+  const uint32_t khi[3] = {fkey(hi.x), fkey(hi.y), fkey(hi.z)};
+  for (int a = 0; a < 3; ++a) {
+    const float c0 = fval(k[a]), ext = fval(k[3 + a]) - c0;
+    int bin = 0;
+    if (ext > 0.0f) {
+      bin = static_cast<int>((centroid(A.blo, A.bhi, p, a) - c0) * (static_cast<float>(kSahBins) / ext));
+      bin = bin < 0 ? 0 : (bin > kSahBins - 1 ? kSahBins - 1 : bin);
+    }
+    const uint32_t key = (static_cast<uint32_t>(s) * 3u + static_cast<uint32_t>(a)) * kSahBins + static_cast<uint32_t>(bin);
+    const unsigned grp = __match_any_sync(active, key);
+    const int leader = __ffs(grp) - 1;
+    const uint32_t mlo0 = __reduce_min_sync(grp, klo[0]), mlo1 = __reduce_min_sync(grp, klo[1]),
+                   mlo2 = __reduce_min_sync(grp, klo[2]);
+    const uint32_t mhi0 = __reduce_max_sync(grp, khi[0]), mhi1 = __reduce_max_sync(grp, khi[1]),
+                   mhi2 = __reduce_max_sync(grp, khi[2]);
+    if (static_cast<int>(threadIdx.x & 31u) == leader) {
+      uint32_t* w = bins + kBinWords * key;
+      atomicAdd(w, static_cast<uint32_t>(__popc(grp)));
+      atomicMin(w + 1, mlo0);
+      atomicMin(w + 2, mlo1);
+      atomicMin(w + 3, mlo2);
+      atomicMax(w + 4, mhi0);
+      atomicMax(w + 5, mhi1);
+      atomicMax(w + 6, mhi2);
+    }
+  }
+}
+
+// Best binned split of each large node (same sweep as the host SAH builder).
+__global__ void k_sah_split(BuildArrays A, const uint32_t* __restrict__ bins, uint32_t n_act) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_act) return;
+  const uint32_t* k = A.cb + 6 * s;
+  int best_axis = -1, best_bin = -1;
+  float best_cost = FLT_MAX;
+  for (int a = 0; a < 3; ++a) {
+    const float ext = fval(k[3 + a]) - fval(k[a]);
+    if (!(ext > 0.0f)) continue;
+    const uint32_t* bw = bins + kBinWords * ((s * 3u + static_cast<uint32_t>(a)) * kSahBins);
+    float rarea[kSahBins];
+    uint32_t rcnt[kSahBins];
+    float rlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    uint32_t rc = 0u;
+    for (int b = kSahBins - 1; b > 0; --b) {
+      const uint32_t* w = bw + kBinWords * b;
+      rc += w[0];
+      if (w[0]) {
+        for (int q = 0; q < 3; ++q) {
+          rlo[q] = bmin(rlo[q], fval(w[1 + q]));
+          rhi[q] = bmax(rhi[q], fval(w[4 + q]));
+        }
+      }
+      rcnt[b] = rc;
+      const float dx = rhi[0] - rlo[0], dy = rhi[1] - rlo[1], dz = rhi[2] - rlo[2];
+      rarea[b] = rc ? dx * dy + dy * dz + dz * dx : 0.0f;
+    }
+    float llo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, lhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    uint32_t lc = 0u;
+    for (int b = 0; b < kSahBins - 1; ++b) {
+      const uint32_t* w = bw + kBinWords * b;
+      lc += w[0];
+      if (w[0]) {
+        for (int q = 0; q < 3; ++q) {
+          llo[q] = bmin(llo[q], fval(w[1 + q]));
+          lhi[q] = bmax(lhi[q], fval(w[4 + q]));
+        }
+      }
+      if (lc == 0u || rcnt[b + 1] == 0u) continue;
+      const float dx = lhi[0] - llo[0], dy = lhi[1] - llo[1], dz = lhi[2] - llo[2];
+      const float cost = (dx * dy + dy * dz + dz * dx) * static_cast<float>(lc) +
+                         rarea[b + 1] * static_cast<float>(rcnt[b + 1]);
+      if (cost < best_cost) {
+        best_cost = cost;
+        best_axis = a;
+        best_bin = b;
+      }
+    }
+  }
+  A.axis[s] = best_axis;
+  A.split[s] = __uint_as_float(static_cast<uint32_t>(best_bin < 0 ? 0 : best_bin));
+}
+
+// ---------------------------------------------------------------- refit, ids, outputs
+struct Finish {
+  const TNode* nodes;
+  const float4* blo;
+  const float4* bhi;
+  const uint32_t* idx;
+  float4* nlo;       // per temporary node
+  float4* nhi;
+  uint32_t* visits;
+  int32_t* icount;   // internal nodes in the subtree
+  int32_t* rank;     // internal: depth-first pre-order rank among internal nodes
+  int32_t* depth;
+  int32_t* final_id;
+};
+
+__global__ void k_refit(Finish F, uint32_t n_nodes) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes || F.nodes[x].left >= 0) return;
+  const TNode t = F.nodes[x];
+  float4 lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.0f), hi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.0f);
+  for (int32_t i = 0; i < t.count; ++i) {
+    const uint32_t p = F.idx[t.begin + i];
+    const float4 a = F.blo[p], b = F.bhi[p];
+    lo = make_float4(bmin(lo.x, a.x), bmin(lo.y, a.y), bmin(lo.z, a.z), 0.0f);
+    hi = make_float4(bmax(hi.x, b.x), bmax(hi.y, b.y), bmax(hi.z, b.z), 0.0f);
+  }
+  F.nlo[x] = lo;
+  F.nhi[x] = hi;
+  F.icount[x] = 0;
+  while (true) {
+    __threadfence();
+    const int32_t p = F.nodes[x].parent;
+    if (p < 0) break;
+    if (atomicAdd(&F.visits[p], 1u) == 0u) break;   // the sibling finishes the parent
+    const TNode pt = F.nodes[p];
+    const float4 l0 = __ldcg(F.nlo + pt.left), l1 = __ldcg(F.nhi + pt.left);
+    const float4 r0 = __ldcg(F.nlo + pt.right), r1 = __ldcg(F.nhi + pt.right);
+    F.nlo[p] = make_float4(bmin(l0.x, r0.x), bmin(l0.y, r0.y), bmin(l0.z, r0.z), 0.0f);
+    F.nhi[p] = make_float4(bmax(l1.x, r1.x), bmax(l1.y, r1.y), bmax(l1.z, r1.z), 0.0f);
+    F.icount[p] = 1 + __ldcg(F.icount + pt.left) + __ldcg(F.icount + pt.right);
+    x = static_cast<uint32_t>(p);
+  }
+}
+
+__global__ void k_ranks(Finish F, uint32_t n_nodes) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes) return;
+  int32_t r = 0, d = 0;
+  int32_t y = static_cast<int32_t>(x);
+  while (F.nodes[y].parent >= 0) {
+    const int32_t p = F.nodes[y].parent;
+    r += 1;
+    if (F.nodes[p].right == y) r += F.icount[F.nodes[p].left];
+    y = p;
+    ++d;
+  }
+  F.rank[x] = r;
+  F.depth[x] = d;
+}
+
+__global__ void k_final_ids(Finish F, uint32_t n_nodes) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes) return;
+  if (x == 0u) F.final_id[0] = 0;
+  const TNode t = F.nodes[x];
+  if (t.left < 0) return;
+  F.final_id[t.left] = 2 * F.rank[x] + 1;
+  F.final_id[t.right] = 2 * F.rank[x] + 2;
+}
+
+// BinNode array in final ids (and the tie records when tie != null).
+__global__ void k_write_bin(Finish F, uint32_t n_nodes, BinNode* __restrict__ out, TieNode* __restrict__ tie) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes) return;
+  const TNode t = F.nodes[x];
+  const int32_t f = F.final_id[x];
+  const float4 lo = F.nlo[x], hi = F.nhi[x];
+  BinNode b;
+  b.lo[0] = lo.x;
+  b.lo[1] = lo.y;
+  b.lo[2] = lo.z;
+  b.hi[0] = hi.x;
+  b.hi[1] = hi.y;
+  b.hi[2] = hi.z;
+  if (t.left >= 0) {
+    b.left = F.final_id[t.left];
+    b.right = F.final_id[t.right];
+    b.first = -1;
+    b.count = 0;
+  } else {
+    b.left = b.right = -1;
+    b.first = t.begin;
+    b.count = t.count;
+  }
+  out[f] = b;
+  if (tie) {
+    TieNode r;
+    r.lox = lo.x;
+    r.loy = lo.y;
+    r.loz = lo.z;
+    r.parent = t.parent >= 0 ? F.final_id[t.parent] : -1;
+    r.hix = hi.x;
+    r.hiy = hi.y;
+    r.hiz = hi.z;
+    r.depth = F.depth[x];
+    tie[f] = r;
+  }
+}
+
+__global__ void k_ref_leaf(Finish F, uint32_t n_nodes, uint32_t* __restrict__ ref_leaf, uint32_t* __restrict__ ref_lane) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes) return;
+  const TNode t = F.nodes[x];
+  if (t.left >= 0) return;
+  for (int32_t i = 0; i < t.count; ++i) {
+    const uint32_t p = F.idx[t.begin + i];
+    ref_leaf[p] = static_cast<uint32_t>(F.final_id[x]);
+    ref_lane[p] = static_cast<uint32_t>(i);
+  }
+}
+
+// ---------------------------------------------------------------- wide collapse
+struct WTemp {          // wide node under construction
+  int32_t slot[4];      // binary node per slot
+  int32_t child[4];     // wide temporary id of an internal slot, -1 for a leaf slot
+  int32_t nslots, parent, stack_here;
+};
+
+struct WideArrays {
+  const BinNode* bin;
+  WTemp* w;
+  uint32_t* counter;    // [0] next temporary wide id, [1] next-level count, [2] max depth, [3] max stack
+  uint32_t* size;       // subtree sizes
+  uint32_t* visits;
+  int32_t* final_id;
+};
+
+__device__ __forceinline__ float bin_area(const BinNode& n) {
+  const float dx = n.hi[0] - n.lo[0], dy = n.hi[1] - n.lo[1], dz = n.hi[2] - n.lo[2];
+  return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_wide_expand(WideArrays W, const uint32_t* __restrict__ cur, uint32_t n_cur, uint32_t level,
+                              uint32_t* __restrict__ next) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_cur) return;
+  const uint32_t wid = cur[i];
+  WTemp& w = W.w[wid];
+  const int32_t root = w.slot[0];
+  int32_t slots[4];
+  int ns = 0;
+  const BinNode r = W.bin[root];
+  if (r.count > 0) {
+    slots[ns++] = root;
+  } else {
+    slots[ns++] = r.left;
+    slots[ns++] = r.right;
+    while (ns < 4) {
+      int best = -1;
+      float best_area = -1.0f;
+      for (int s = 0; s < ns; ++s) {
+        const BinNode c = W.bin[slots[s]];
+        if (c.count > 0) continue;
+        const float a = bin_area(c);
+        if (a > best_area) {
+          best_area = a;
+          best = s;
+        }
+      }
+      if (best < 0) break;
+      const BinNode c = W.bin[slots[best]];
+      for (int s = ns; s > best + 1; --s) slots[s] = slots[s - 1];
+      slots[best] = c.left;
+      slots[best + 1] = c.right;
+      ++ns;
+    }
+  }
+  const int32_t stack_here = w.stack_here + ns - 1;
+  w.nslots = ns;
+  w.stack_here = stack_here;
+  atomicMax(&W.counter[2], level + 1u);
+  atomicMax(&W.counter[3], static_cast<uint32_t>(stack_here));
+  for (int s = 0; s < 4; ++s) {
+    w.slot[s] = s < ns ? slots[s] : -1;
+    w.child[s] = -1;
+    if (s < ns && W.bin[slots[s]].count == 0) {
+      const uint32_t c = atomicAdd(&W.counter[0], 1u);
+      W.w[c].slot[0] = slots[s];
+      W.w[c].parent = static_cast<int32_t>(wid);
+      W.w[c].stack_here = stack_here;   // the child's stack on entry
+      w.child[s] = static_cast<int32_t>(c);
+      next[atomicAdd(&W.counter[1], 1u)] = c;
+    }
+  }
+  W.visits[wid] = 0u;
+}
+
+__global__ void k_wide_sizes(WideArrays W, uint32_t n_wide) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_wide) return;
+  const WTemp w0 = W.w[x];
+  for (int s = 0; s < w0.nslots; ++s)
+    if (w0.child[s] >= 0) return;   // not a bottom node
+  W.size[x] = 1u;
+  while (true) {
+    __threadfence();
+    const int32_t p = W.w[x].parent;
+    if (p < 0) break;
+    const WTemp pw = W.w[p];
+    int need = 0;
+    for (int s = 0; s < pw.nslots; ++s) need += pw.child[s] >= 0 ? 1 : 0;
+    if (atomicAdd(&W.visits[p], 1u) + 1u < static_cast<uint32_t>(need)) break;
+    uint32_t sz = 1u;
+    for (int s = 0; s < pw.nslots; ++s)
+      if (pw.child[s] >= 0) sz += __ldcg(W.size + pw.child[s]);
+    W.size[p] = sz;
+    x = static_cast<uint32_t>(p);
+  }
+}
+
+__global__ void k_wide_ids(WideArrays W, uint32_t n_wide) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_wide) return;
+  int32_t id = 0;
+  int32_t y = static_cast<int32_t>(x);
+  while (W.w[y].parent >= 0) {
+    const int32_t p = W.w[y].parent;
+    const WTemp pw = W.w[p];
+    id += 1;
+    for (int s = 0; s < pw.nslots && pw.child[s] != y; ++s)
+      if (pw.child[s] >= 0) id += static_cast<int32_t>(W.size[pw.child[s]]);
+    y = p;
+  }
+  W.final_id[x] = id;
+}
+
+__global__ void k_wide_write(WideArrays W, uint32_t n_wide, WideNode* __restrict__ out) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_wide) return;
+  const WTemp w = W.w[x];
+  WideNode n;
+  for (int k = 0; k < 4; ++k) {
+    n.lox[k] = n.loy[k] = n.loz[k] = 1.0f;
+    n.hix[k] = n.hiy[k] = n.hiz[k] = -1.0f;
+    n.child[k] = 0;
+    n.meta[k] = 0;
+  }
+  n.meta[0] = w.nslots;
+  for (int k = 0; k < w.nslots; ++k) {
+    const BinNode c = W.bin[w.slot[k]];
+    n.lox[k] = c.lo[0];
+    n.loy[k] = c.lo[1];
+    n.loz[k] = c.lo[2];
+    n.hix[k] = c.hi[0];
+    n.hiy[k] = c.hi[1];
+    n.hiz[k] = c.hi[2];
+    n.child[k] = c.count > 0 ? ~static_cast<int32_t>((static_cast<uint32_t>(c.first) << 3) |
+                                                     static_cast<uint32_t>(c.count - 1))
+                             : W.final_id[w.child[k]];
+  }
+  out[W.final_id[x]] = n;
+}
+
+__global__ void k_tri_records(const uint32_t* __restrict__ order, uint32_t n, const float4* __restrict__ pv,
+                              const uint32_t* __restrict__ ref_leaf, const uint32_t* __restrict__ ref_lane,
+                              TriRecord* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t p = order[i];
+  const float4 a = pv[3 * p], b = pv[3 * p + 1], c = pv[3 * p + 2];
+  TriRecord r;
+  r.v0x = a.x;
+  r.v0y = a.y;
+  r.v0z = a.z;
+  r.e1x = a.w;
+  r.e1y = b.x;
+  r.e1z = b.y;
+  r.e2x = b.z;
+  r.e2y = b.w;
+  r.e2z = c.x;
+  r.prim = p;
+  r.leaf = ref_leaf[p];
+  r.lane = ref_lane[p];
+  out[i] = r;
+}
+
+__global__ void k_iota(uint32_t* __restrict__ a, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+__global__ void k_fill_u32(uint32_t* __restrict__ a, uint32_t n, uint32_t v) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+__global__ void k_root(TNode* nodes, uint32_t n, int32_t* slot_of) {
+  nodes[0] = TNode{0, static_cast<int32_t>(n), -1, -1, -1};
+  slot_of[0] = -1;
+}
+
+#define BB_TRY(x)                        \
+  do {                                   \
+    cudaError_t e_ = (x);                \
+    if (e_ != cudaSuccess) return e_;    \
+  } while (0)
+
+template <class T>
+cudaError_t read_scalar(const T* d, T& h, cudaStream_t s) {
+  BB_TRY(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
+  return cudaStreamSynchronize(s);
+}
+
+// Top-down build of one binary tree over `order` (iota on entry, the tree's
+// primitive order on return).  Returns the temporary node count.
+cudaError_t build_tree(const float4* blo, const float4* bhi, uint32_t n, bool sah, uint32_t* order, TNode* nodes,
+                       uint32_t& n_nodes, Scratch& sc) {
+  cudaStream_t s = sc.s;
+  const uint32_t cap_nodes = 2u * n;
+  int32_t* slot_of = sc.get<int32_t>(cap_nodes);
+  uint32_t* node_of = sc.get<uint32_t>(n);
+  uint32_t* idx2 = sc.get<uint32_t>(n);
+  uint32_t* node2 = sc.get<uint32_t>(n);
+  uint32_t* flag = sc.get<uint32_t>(n);
+  uint32_t* excl = sc.get<uint32_t>(n + 1u);
+  // Nodes of one level above kSmallNode primitives are disjoint: at most n / 65 of them;
+  // small subtree roots (5..64 primitives) are disjoint too.
+  const uint32_t max_act = n / (kSmallNode + 1u) + 2u;
+  uint32_t* act = sc.get<uint32_t>(max_act);
+  uint32_t* next = sc.get<uint32_t>(max_act);
+  uint32_t* small = sc.get<uint32_t>(n / (kLeafMax + 1u) + 2u);
+  uint32_t* counter = sc.get<uint32_t>(4);
+  uint32_t* cb = sc.get<uint32_t>(6ull * max_act);
+  int32_t* axis = sc.get<int32_t>(max_act);
+  float* split = sc.get<float>(max_act);
+  uint32_t* nl = sc.get<uint32_t>(max_act);
+  uint32_t* ident = sc.get<uint32_t>(max_act);
+  uint32_t* bins = sah ? sc.get<uint32_t>(static_cast<size_t>(kBinWords) * 3u * kSahBins * max_act) : nullptr;
+  if (sc.err != cudaSuccess) return sc.err;
+  BuildArrays A{blo, bhi, nodes, slot_of, cb, axis, split, nl, ident, counter};
+  k_fill_u32<<<grid_for(cap_nodes), kThreads, 0, s>>>(reinterpret_cast<uint32_t*>(slot_of), cap_nodes, 0xffffffffu);
+  k_fill_u32<<<grid_for(n), kThreads, 0, s>>>(node_of, n, 0u);
+  k_root<<<1, 1, 0, s>>>(nodes, n, slot_of);
+  const uint32_t init[4] = {1u, 0u, 0u, 0u};
+  BB_TRY(cudaMemcpyAsync(counter, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  uint32_t n_act = 0u, n_small = 0u;
+  if (n > kSmallNode) {
+    const uint32_t zero = 0u;
+    BB_TRY(cudaMemcpyAsync(act, &zero, 4, cudaMemcpyHostToDevice, s));
+    n_act = 1u;
+  } else if (n > kLeafMax) {
+    const uint32_t zero = 0u;
+    BB_TRY(cudaMemcpyAsync(small, &zero, 4, cudaMemcpyHostToDevice, s));
+    n_small = 1u;
+    BB_TRY(cudaMemcpyAsync(counter + 2, &n_small, 4, cudaMemcpyHostToDevice, s));
+  }
+  uint32_t* idx = order;
+  uint32_t base = 1u;
+  while (n_act > 0u) {
+    k_level_init<<<grid_for(n_act), kThreads, 0, s>>>(A, act, n_act);
+    k_centroid_bounds<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n);
+    if (sah) {
+      k_sah_bin_init<<<grid_for(static_cast<uint64_t>(n_act) * 3u * kSahBins), kThreads, 0, s>>>(bins, n_act);
+      k_sah_bin<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, bins);
+      k_sah_split<<<grid_for(n_act, 64), 64, 0, s>>>(A, bins, n_act);
+    } else {
+      k_midpoint_split<<<grid_for(n_act), kThreads, 0, s>>>(A, n_act);
+    }
+    k_flags<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, flag, sah);
+    BB_TRY(exclusive_scan(flag, n, excl, sc));
+    BB_TRY(cudaMemsetAsync(counter + 1, 0, 4, s));
+    k_children<<<grid_for(n_act), kThreads, 0, s>>>(A, act, n_act, base, excl, next, small);
+    k_scatter<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, excl, idx2, node2);
+    k_level_done<<<grid_for(n_act), kThreads, 0, s>>>(A, act, n_act);
+    BB_TRY(cudaGetLastError());
+    // the scattered order becomes the current one (the caller's buffer keeps the final order)
+    BB_TRY(cudaMemcpyAsync(idx, idx2, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    std::swap(node_of, node2);
+    std::swap(act, next);
+    base += 2u * n_act;
+    uint32_t cnt[3];
+    BB_TRY(cudaMemcpyAsync(cnt, counter, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+    BB_TRY(cudaStreamSynchronize(s));
+    n_act = cnt[1];
+    n_small = cnt[2];
+  }
+  BB_TRY(cudaMemcpyAsync(counter, &base, 4, cudaMemcpyHostToDevice, s));
+  if (n_small > 0u) {
+    if (sah) k_small<true><<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
+    else k_small<false><<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
+  }
+  BB_TRY(cudaGetLastError());
+  return read_scalar(counter, n_nodes, s);
+}
+
+// Node bounds, reference ids and BinNode array of a built tree.
+cudaError_t finish_tree(const float4* blo, const float4* bhi, const uint32_t* order, const TNode* nodes,
+                        uint32_t n_nodes, BinNode* out, TieNode* tie, uint32_t* ref_leaf, uint32_t* ref_lane,
+                        Scratch& sc) {
+  cudaStream_t s = sc.s;
+  Finish F{nodes, blo, bhi, order, sc.get<float4>(n_nodes), sc.get<float4>(n_nodes), sc.get<uint32_t>(n_nodes),
+           sc.get<int32_t>(n_nodes), sc.get<int32_t>(n_nodes), sc.get<int32_t>(n_nodes), sc.get<int32_t>(n_nodes)};
+  if (sc.err != cudaSuccess) return sc.err;
+  BB_TRY(cudaMemsetAsync(F.visits, 0, n_nodes * sizeof(uint32_t), s));
+  k_refit<<<grid_for(n_nodes), kThreads, 0, s>>>(F, n_nodes);
+  k_ranks<<<grid_for(n_nodes), kThreads, 0, s>>>(F, n_nodes);
+  k_final_ids<<<grid_for(n_nodes), kThreads, 0, s>>>(F, n_nodes);
+  k_write_bin<<<grid_for(n_nodes), kThreads, 0, s>>>(F, n_nodes, out, tie);
+  if (ref_leaf) k_ref_leaf<<<grid_for(n_nodes), kThreads, 0, s>>>(F, n_nodes, ref_leaf, ref_lane);
+  return cudaGetLastError();
+}
+
+cudaError_t collapse(const BinNode* bin, uint32_t n_bin, WideNode* out, uint32_t& n_wide, uint32_t& depth,
+                     uint32_t& stack_required, Scratch& sc) {
+  cudaStream_t s = sc.s;
+  const uint32_t cap = n_bin;   // wide nodes <= binary internal nodes + 1
+  WideArrays W{bin, sc.get<WTemp>(cap), sc.get<uint32_t>(4), sc.get<uint32_t>(cap), sc.get<uint32_t>(cap),
+               sc.get<int32_t>(cap)};
+  uint32_t* cur = sc.get<uint32_t>(cap);
+  uint32_t* next = sc.get<uint32_t>(cap);
+  if (sc.err != cudaSuccess) return sc.err;
+  WTemp root{};
+  root.slot[0] = 0;
+  root.parent = -1;
+  root.stack_here = 0;
+  BB_TRY(cudaMemcpyAsync(W.w, &root, sizeof(root), cudaMemcpyHostToDevice, s));
+  const uint32_t init[4] = {1u, 0u, 0u, 0u};
+  BB_TRY(cudaMemcpyAsync(W.counter, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  const uint32_t zero = 0u;
+  BB_TRY(cudaMemcpyAsync(cur, &zero, 4, cudaMemcpyHostToDevice, s));
+  uint32_t n_cur = 1u, level = 0u;
+  while (n_cur > 0u) {
+    BB_TRY(cudaMemsetAsync(W.counter + 1, 0, 4, s));
+    k_wide_expand<<<grid_for(n_cur), kThreads, 0, s>>>(W, cur, n_cur, level, next);
+    BB_TRY(cudaGetLastError());
+    std::swap(cur, next);
+    BB_TRY(read_scalar(W.counter + 1, n_cur, s));
+    ++level;
+  }
+  uint32_t cnt[4];
+  BB_TRY(cudaMemcpyAsync(cnt, W.counter, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+  BB_TRY(cudaStreamSynchronize(s));
+  n_wide = cnt[0];
+  depth = cnt[2];
+  stack_required = cnt[3] + 1u;
+  k_wide_sizes<<<grid_for(n_wide), kThreads, 0, s>>>(W, n_wide);
+  k_wide_ids<<<grid_for(n_wide), kThreads, 0, s>>>(W, n_wide);
+  k_wide_write<<<grid_for(n_wide), kThreads, 0, s>>>(W, n_wide, out);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t dmalloc(T*& p, size_t n) {
+  return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(1, n) * sizeof(T));
+}
+
+}  // namespace
+
+void FreeDeviceAccel(DeviceAccelOut& out) {
+  cudaFree(out.nodes);
+  cudaFree(out.tris);
+  cudaFree(out.tie);
+  cudaFree(out.shade);
+  cudaFree(out.ref_nodes);
+  cudaFree(out.ref_order);
+  out = DeviceAccelOut{};
+}
+
+cudaError_t BuildAccelOnDevice(const float* vertices, uint32_t vertex_count, const uint32_t* indices,
+                               uint32_t index_count, const uint32_t* instances, uint32_t instance_count, bool sah,
+                               cudaStream_t stream, DeviceAccelOut& out) {
+  out = DeviceAccelOut{};
+  // Candidate triangles of every instance (the host path's loop bounds).
+  std::vector<unsigned long long> prefix(instance_count + 1u, 0ull);
+  for (uint32_t i = 0; i < instance_count; ++i) prefix[i + 1] = prefix[i] + instances[3 * i + 1];
+  const unsigned long long candidates = prefix[instance_count];
+  if (candidates >= (1ull << 31)) return cudaErrorInvalidValue;
+  Scratch sc{stream};
+  float* d_v = sc.get<float>(3ull * vertex_count);
+  uint32_t* d_i = sc.get<uint32_t>(index_count);
+  uint32_t* d_inst = sc.get<uint32_t>(3ull * instance_count);
+  unsigned long long* d_prefix = sc.get<unsigned long long>(instance_count + 1u);
+  const uint32_t nc = static_cast<uint32_t>(candidates);
+  uint32_t* flag = sc.get<uint32_t>(nc);
+  uint32_t* pos = sc.get<uint32_t>(nc + 1u);
+  uint32_t* nonfinite = sc.get<uint32_t>(1);
+  if (sc.err != cudaSuccess) return sc.err;
+  if (vertex_count) BB_TRY(cudaMemcpyAsync(d_v, vertices, 12ull * vertex_count, cudaMemcpyHostToDevice, stream));
+  if (index_count) BB_TRY(cudaMemcpyAsync(d_i, indices, 4ull * index_count, cudaMemcpyHostToDevice, stream));
+  if (instance_count) BB_TRY(cudaMemcpyAsync(d_inst, instances, 12ull * instance_count, cudaMemcpyHostToDevice, stream));
+  BB_TRY(cudaMemcpyAsync(d_prefix, prefix.data(), 8ull * (instance_count + 1u), cudaMemcpyHostToDevice, stream));
+  BB_TRY(cudaMemsetAsync(nonfinite, 0, 4, stream));
+  const FlatIn f{d_v, vertex_count, d_i, index_count, d_inst, d_prefix, instance_count, nc};
+  if (nc) k_flat_valid<<<grid_for(nc), kThreads, 0, stream>>>(f, flag);
+  BB_TRY(exclusive_scan(flag, nc, pos, sc));
+  uint32_t n = 0u;
+  BB_TRY(read_scalar(pos + nc, n, stream));
+  out.prim_count = n;
+  float4* pv = sc.get<float4>(3ull * n);
+  float4* blo = sc.get<float4>(n);
+  float4* bhi = sc.get<float4>(n);
+  if (sc.err != cudaSuccess) return sc.err;
+  BB_TRY(dmalloc(out.shade, n));
+  if (nc) k_flat_write<<<grid_for(nc), kThreads, 0, stream>>>(f, flag, pos, pv, out.shade, blo, bhi, nonfinite);
+  uint32_t bad = 0u;
+  BB_TRY(read_scalar(nonfinite, bad, stream));
+  if (bad) {
+    FreeDeviceAccel(out);
+    out.fallback = true;
+    return cudaSuccess;
+  }
+  if (n == 0u) return cudaSuccess;
+
+  // Reference tree.
+  TNode* tn = sc.get<TNode>(2ull * n);
+  uint32_t* ref_leaf = sc.get<uint32_t>(n);
+  uint32_t* ref_lane = sc.get<uint32_t>(n);
+  if (sc.err != cudaSuccess) return sc.err;
+  BB_TRY(dmalloc(out.ref_order, n));
+  k_iota<<<grid_for(n), kThreads, 0, stream>>>(out.ref_order, n);
+  uint32_t n_ref = 0u;
+  BB_TRY(build_tree(blo, bhi, n, false, out.ref_order, tn, n_ref, sc));
+  BB_TRY(dmalloc(out.ref_nodes, n_ref));
+  TieNode* tie = nullptr;
+  BB_TRY(dmalloc(tie, n_ref));
+  out.tie = reinterpret_cast<float4*>(tie);
+  BB_TRY(finish_tree(blo, bhi, out.ref_order, tn, n_ref, out.ref_nodes, tie, ref_leaf, ref_lane, sc));
+  out.binary_nodes = n_ref;
+  out.binary_leaves = (n_ref + 1u) / 2u;
+
+  // Traversal tree: the reference tree itself, or a binned-SAH tree.
+  const BinNode* trav = out.ref_nodes;
+  const uint32_t* trav_order = out.ref_order;
+  uint32_t n_trav = n_ref;
+  if (sah) {
+    uint32_t* sah_order = sc.get<uint32_t>(n);
+    TNode* sn = sc.get<TNode>(2ull * n);
+    if (sc.err != cudaSuccess) return sc.err;
+    k_iota<<<grid_for(n), kThreads, 0, stream>>>(sah_order, n);
+    BB_TRY(build_tree(blo, bhi, n, true, sah_order, sn, n_trav, sc));
+    BinNode* sah_nodes = sc.get<BinNode>(n_trav);
+    if (sc.err != cudaSuccess) return sc.err;
+    BB_TRY(finish_tree(blo, bhi, sah_order, sn, n_trav, sah_nodes, nullptr, nullptr, nullptr, sc));
+    trav = sah_nodes;
+    trav_order = sah_order;
+    out.reference_topology = false;
+  }
+  WideNode* wide = nullptr;
+  BB_TRY(dmalloc(wide, n_trav));
+  out.nodes = reinterpret_cast<float4*>(wide);
+  BB_TRY(collapse(trav, n_trav, wide, out.wide_nodes, out.depth, out.stack_required, sc));
+  TriRecord* tris = nullptr;
+  BB_TRY(dmalloc(tris, n));
+  out.tris = reinterpret_cast<float4*>(tris);
+  k_tri_records<<<grid_for(n), kThreads, 0, stream>>>(trav_order, n, pv, ref_leaf, ref_lane, tris);
+  BB_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(stream);
+}
+
+}  // namespace vkptc

@@ -19,6 +19,7 @@
 
 #include "../../include/vkptc.h"
 #include "adjoint_launch.h"
+#include "bvh_build.h"
 #include "bvh_host.h"
 #include "batch.cuh"
 #include "kernels.cuh"
@@ -48,6 +49,11 @@ struct DevBuf {
     return e;
   }
   size_t bytes() const { return count * sizeof(T); }
+  void adopt(T* p, size_t n) {
+    release();
+    ptr = p;
+    count = p ? n : 0;
+  }
 };
 
 struct HostCamera {
@@ -97,7 +103,11 @@ struct vkptc_ctx {
   vkptc_render_settings settings{};
 
   // scene (host copies needed to rebuild)
-  SceneGeometry geo;
+  SceneGeometry geo;                      // flattened on the host (host build, external BVHs)
+  bool geo_ready = false;
+  std::vector<float> raw_vertices;        // the scene's arrays, for the device build
+  std::vector<uint32_t> raw_indices, raw_instances;
+  uint32_t prim_count = 0;                // flattened primitives of the built accelerator
   std::vector<float> materials, lights;
   float env[3] = {0, 0, 0};
   uint32_t env_w = 0, env_h = 0;          // environment map size (0: constant environment)
@@ -187,7 +197,7 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.lights = c->d_lights.ptr;
   s.material_count = static_cast<uint32_t>(c->materials.size() / 16);
   s.light_count = static_cast<uint32_t>(c->lights.size() / 16);
-  s.prim_count = static_cast<uint32_t>(c->geo.prims.size());
+  s.prim_count = c->prim_count;
   s.has_transmissive = c->has_transmissive ? 1u : 0u;
   s.has_effects = c->has_effects ? 1u : 0u;
   s.env = mk(c->env[0], c->env[1], c->env[2]);
@@ -371,6 +381,7 @@ int32_t upload_accel(vkptc_ctx* c, const std::vector<BinNode>& bin, const std::v
   }
   if (!shade.empty())
     VKPTC_CUDA(c, cudaMemcpy(c->d_shade.ptr, shade.data(), shade.size() * sizeof(float4), cudaMemcpyHostToDevice), "bvh upload");
+  c->prim_count = static_cast<uint32_t>(c->geo.prims.size());
   c->accel = vkptc_accel_info{};
   c->accel.primitive_count = static_cast<uint32_t>(c->geo.prims.size());
   c->accel.binary_node_count = w.binary_nodes;
@@ -507,13 +518,28 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   }
   ctx->adj.setup = false;
   cudaSetDevice(ctx->device);
-  std::string err;
-  SceneGeometry geo;
-  if (!FlattenScene(scene->vertices, scene->vertex_count, scene->indices, scene->index_count, scene->instances,
-                    scene->instance_count, geo, err)) {
-    return fail(ctx, VKPTC_INVALID_ARGUMENT, err);
+  if (scene->instance_count > 0 && scene->instances == nullptr)
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "instances pointer is null");
+  if (ctx->config.build_mode == VKPTC_BUILD_HOST) {
+    std::string err;
+    SceneGeometry geo;
+    if (!FlattenScene(scene->vertices, scene->vertex_count, scene->indices, scene->index_count, scene->instances,
+                      scene->instance_count, geo, err)) {
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, err);
+    }
+    ctx->geo = std::move(geo);
+    ctx->geo_ready = true;
+    ctx->raw_vertices.clear();
+    ctx->raw_indices.clear();
+    ctx->raw_instances.clear();
+  } else {
+    // Flattened on the device by the build (or on the host for an external BVH).
+    ctx->raw_vertices.assign(scene->vertices, scene->vertices + 3 * static_cast<size_t>(scene->vertex_count));
+    ctx->raw_indices.assign(scene->indices, scene->indices + scene->index_count);
+    ctx->raw_instances.assign(scene->instances, scene->instances + 3 * static_cast<size_t>(scene->instance_count));
+    ctx->geo = SceneGeometry{};
+    ctx->geo_ready = false;
   }
-  ctx->geo = std::move(geo);
   ctx->materials.assign(scene->materials, scene->materials + 16 * static_cast<size_t>(scene->material_count));
   if (ctx->materials.empty()) {
     // The reference substitutes one default RTMaterial (ScalarCpuPathTracer.cpp:468-470).
@@ -627,10 +653,86 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   return VKPTC_OK;
 }
 
+// Host flattening of the scene for the host build and external BVHs.
+int32_t ensure_geo(vkptc_ctx* c) {
+  if (c->geo_ready) return VKPTC_OK;
+  std::string err;
+  SceneGeometry geo;
+  if (!FlattenScene(c->raw_vertices.data(), static_cast<uint32_t>(c->raw_vertices.size() / 3), c->raw_indices.data(),
+                    static_cast<uint32_t>(c->raw_indices.size()), c->raw_instances.data(),
+                    static_cast<uint32_t>(c->raw_instances.size() / 3), geo, err)) {
+    return fail(c, VKPTC_INVALID_ARGUMENT, err);
+  }
+  c->geo = std::move(geo);
+  c->geo_ready = true;
+  return VKPTC_OK;
+}
+
+// Device build: every array the traversal reads, produced by CUDA kernels
+// (bvh_build.cu).  Returns VKPTC_OK with *done = false when the scene needs
+// the host path (non-finite primitive bounds).
+int32_t build_on_device(vkptc_ctx* c, bool* done) {
+  *done = false;
+  const auto t0 = std::chrono::steady_clock::now();
+  DeviceAccelOut out;
+  const cudaError_t e = BuildAccelOnDevice(
+      c->raw_vertices.data(), static_cast<uint32_t>(c->raw_vertices.size() / 3), c->raw_indices.data(),
+      static_cast<uint32_t>(c->raw_indices.size()), c->raw_instances.data(),
+      static_cast<uint32_t>(c->raw_instances.size() / 3), c->config.bvh_mode == VKPTC_BVH_SAH, c->stream, out);
+  if (e != cudaSuccess) {
+    FreeDeviceAccel(out);
+    return cuda_fail(c, e, "device BVH build");
+  }
+  if (out.fallback) return VKPTC_OK;
+  const uint32_t n = out.prim_count;
+  c->d_shade.adopt(out.shade, std::max<uint32_t>(1, n));
+  if (n == 0u) {
+    VKPTC_CUDA(c, c->d_nodes.alloc(1), "bvh alloc");
+    VKPTC_CUDA(c, c->d_tris.alloc(1), "bvh alloc");
+    VKPTC_CUDA(c, c->d_tie.alloc(1), "bvh alloc");
+  } else {
+    c->d_nodes.adopt(out.nodes, 8ull * out.wide_nodes);
+    c->d_tris.adopt(out.tris, 3ull * n);
+    c->d_tie.adopt(out.tie, 2ull * out.binary_nodes);
+  }
+  cudaFree(out.ref_nodes);
+  cudaFree(out.ref_order);
+  c->wide = WideBvh{};
+  c->wide.binary_nodes = out.binary_nodes;
+  c->wide.binary_leaves = out.binary_leaves;
+  c->wide.depth = out.depth;
+  c->wide.stack_required = out.stack_required;
+  c->wide.reference_topology = out.reference_topology;
+  c->prim_count = n;
+  c->accel = vkptc_accel_info{};
+  c->accel.primitive_count = n;
+  c->accel.binary_node_count = out.binary_nodes;
+  c->accel.binary_leaf_count = out.binary_leaves;
+  c->accel.wide_node_count = out.wide_nodes;
+  c->accel.wide_depth = out.depth;
+  c->accel.stack_required = out.stack_required;
+  c->accel.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  c->accel.device_bytes = static_cast<uint64_t>(out.wide_nodes) * sizeof(WideNode) + static_cast<uint64_t>(n) * sizeof(TriRecord);
+  c->accel_valid = true;
+  *done = true;
+  return VKPTC_OK;
+}
+
 int32_t vkptc_build_acceleration(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "build_or_update_acceleration called before load_scene_snapshot");
   cudaSetDevice(ctx->device);
+  if (ctx->config.build_mode != VKPTC_BUILD_HOST) {
+    bool done = false;
+    const int32_t rc = build_on_device(ctx, &done);
+    if (rc != VKPTC_OK) return rc;
+    if (done) {
+      ctx->last_error.clear();
+      return VKPTC_OK;
+    }
+  }
+  int32_t grc = ensure_geo(ctx);
+  if (grc != VKPTC_OK) return grc;
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<BinNode> bin;
   std::vector<uint32_t> order;
@@ -657,6 +759,8 @@ int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh) {
     std::memcpy(&bin[i].count, w + 9, 4);
   }
   std::vector<uint32_t> order(bvh->prim_indices, bvh->prim_indices + bvh->prim_count);
+  const int32_t grc = ensure_geo(ctx);
+  if (grc != VKPTC_OK) return grc;
   std::string err;
   if (!ValidateBinaryBvh(bin, order, ctx->geo.prims.size(), err)) return fail(ctx, VKPTC_INVALID_ARGUMENT, err);
   const int32_t rc = upload_accel(ctx, bin, order, 0.0);
@@ -698,6 +802,40 @@ int32_t vkptc_get_accel_info(vkptc_ctx* ctx, vkptc_accel_info* out) {
   return VKPTC_OK;
 }
 
+int32_t vkptc_read_accel(vkptc_ctx* ctx, uint32_t what, void* out, uint64_t capacity, uint64_t* bytes) {
+  if (!ctx || !bytes) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "acceleration structure not built");
+  const void* src = nullptr;
+  uint64_t n = 0;
+  switch (what) {
+    case VKPTC_ACCEL_WIDE_NODES:
+      src = ctx->d_nodes.ptr;
+      n = static_cast<uint64_t>(ctx->accel.wide_node_count) * sizeof(WideNode);
+      break;
+    case VKPTC_ACCEL_TRIANGLES:
+      src = ctx->d_tris.ptr;
+      n = static_cast<uint64_t>(ctx->prim_count) * sizeof(TriRecord);
+      break;
+    case VKPTC_ACCEL_TIE_NODES:
+      src = ctx->d_tie.ptr;
+      n = ctx->prim_count ? static_cast<uint64_t>(ctx->accel.binary_node_count) * sizeof(TieNode) : 0u;
+      break;
+    case VKPTC_ACCEL_SHADING:
+      src = ctx->d_shade.ptr;
+      n = static_cast<uint64_t>(ctx->prim_count) * sizeof(float4);
+      break;
+    default:
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, "unknown accelerator array");
+  }
+  *bytes = n;
+  if (!out || n == 0) return VKPTC_OK;
+  if (capacity < n) return fail(ctx, VKPTC_INVALID_ARGUMENT, "output buffer too small");
+  cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(out, src, n, cudaMemcpyDeviceToHost, ctx->stream), "accel read");
+  VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "accel read");
+  return VKPTC_OK;
+}
+
 int32_t vkptc_reset(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "reset_accumulation called before configure");
@@ -719,6 +857,11 @@ int32_t vkptc_shutdown(vkptc_ctx* ctx) {
   ctx->configured = ctx->has_scene = ctx->accel_valid = false;
   ctx->adj.setup = false;
   ctx->geo = SceneGeometry{};
+  ctx->geo_ready = false;
+  ctx->raw_vertices.clear();
+  ctx->raw_indices.clear();
+  ctx->raw_instances.clear();
+  ctx->prim_count = 0;
   ctx->wide = WideBvh{};
   ctx->d_nodes.release();
   ctx->d_tris.release();

@@ -23,10 +23,12 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
                 ("math_mode", ctypes.c_uint32), ("collect_stats", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
                 ("stage_timing", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("bvh_mode", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 4)]
+                ("build_mode", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
 
 
 BVH_REFERENCE, BVH_SAH = 0, 1
+BUILD_DEVICE, BUILD_HOST = 0, 1
+ACCEL_WIDE_NODES, ACCEL_TRIANGLES, ACCEL_TIE_NODES, ACCEL_SHADING = range(4)
 
 
 class RenderSettingsC(ctypes.Structure):
@@ -150,6 +152,7 @@ SIGNATURES = {
     "vkptc_build_acceleration": (I32, [P]),
     "vkptc_load_bvh": (I32, [P, ctypes.POINTER(BvhView)]),
     "vkptc_get_accel_info": (I32, [P, ctypes.POINTER(AccelInfo)]),
+    "vkptc_read_accel": (I32, [P, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),
     "vkptc_reset": (I32, [P]),
     "vkptc_shutdown": (I32, [P]),

@@ -118,7 +118,7 @@ class CudaPathTracer:
 
     def __init__(self, device: int = 0, block_size: int = 0, stack_depth: int = 0, math_mode: int = 0,
                  collect_stats: bool = False, wave_paths: int = 0, stage_timing: bool = False,
-                 steps: int = 0, bvh: str = "reference"):
+                 steps: int = 0, bvh: str = "reference", build: str = "device"):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -130,6 +130,7 @@ class CudaPathTracer:
         cfg.stage_timing = int(stage_timing)
         cfg.steps = steps
         cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
+        cfg.build_mode = native.BUILD_HOST if build == "host" else native.BUILD_DEVICE
         handle = ctypes.c_void_p()
         rc = self._lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle))
         if rc != native.OK:
@@ -196,6 +197,16 @@ class CudaPathTracer:
         a = native.AccelInfo()
         self._check(self._lib.vkptc_get_accel_info(self._ctx, ctypes.byref(a)))
         return a.as_dict()
+
+    def read_accel(self, what: int) -> np.ndarray:
+        """One device array of the accelerator (native.ACCEL_*) as raw uint32 words."""
+        n = ctypes.c_uint64(0)
+        self._check(self._lib.vkptc_read_accel(self._ctx, what, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value // 4, np.uint32)
+        if n.value:
+            self._check(self._lib.vkptc_read_accel(self._ctx, what, out.ctypes.data_as(ctypes.c_void_p), n.value,
+                                                   ctypes.byref(n)))
+        return out
 
     def reset_accumulation(self) -> bool:
         return self._lib.vkptc_reset(self._ctx) == native.OK
@@ -388,7 +399,7 @@ class BatchRenderer:
     """
 
     def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False, bvh: str = "reference",
-                 stage_timing: bool = False):
+                 stage_timing: bool = False, build: str = "device"):
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -396,6 +407,7 @@ class BatchRenderer:
         cfg.collect_stats = int(collect_stats)
         cfg.stage_timing = int(stage_timing)
         cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
+        cfg.build_mode = native.BUILD_HOST if build == "host" else native.BUILD_DEVICE
         h = ctypes.c_void_p()
         rc = self._lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != native.OK:
