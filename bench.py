@@ -291,6 +291,43 @@ def sdf_scene(device, cpu_seconds: float = 0.0):
     return out
 
 
+def bvh_build(device, cpu: bool = True):
+    """Acceleration-structure build of the 2,064,418-triangle sphere grid:
+    the device build (reference tree alone, and with the SAH traversal tree)
+    and the host build (the parity mode), each through
+    vkptc_build_acceleration from the scene already loaded; and the
+    reference's own CPU builder (ParallelBvhBuilder) on the same triangles."""
+    from vkpathtracer_b200.tracer import CudaPathTracer
+    sc = scenes.sphere_grid()
+    st = scenes.RenderSettings(width=64, height=64, spp=1)
+    n = sc.triangle_count
+    out = {"workload": "sphere_grid_64x64_2064418_triangles", "triangles": n}
+    for build, bvh, reps in (("device", "reference", 6), ("device", "sah", 6), ("host", "reference", 1)):
+        with CudaPathTracer(device=device, bvh=bvh, build=build) as t:
+            t.configure(st)
+            t.load_scene_snapshot(sc)
+            ms = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                t.build_or_update_acceleration()
+                ms.append(1e3 * (time.perf_counter() - t0))
+            out[f"{build}_{bvh}_ms"] = min(ms)
+    out["device_sah_triangles_per_s"] = n / (out["device_sah_ms"] / 1e3)
+    out["speedup_device_vs_host_reference_tree"] = out["host_reference_ms"] / out["device_reference_ms"]
+    if cpu:
+        import oracle
+        kind = "reference" if oracle.have_reference() else "port"
+        o = oracle.load(kind)
+        t0 = time.perf_counter()
+        o.build_bvh(sc)
+        ms = 1e3 * (time.perf_counter() - t0)
+        out["cpu_baseline"] = {"value": ms, "unit": "ms", "cores": 1, "kind": kind,
+                               "sample": "ParallelBvhBuilder (deterministic, leaf threshold 4) on the full scene, "
+                                         "primitive bounds included"}
+        out["speedup_device_vs_reference_builder"] = ms / out["device_reference_ms"]
+    return out
+
+
 def ray_query(device):
     import torch
     from vkpathtracer_b200.tracer import CudaPathTracer
@@ -516,7 +553,7 @@ def run_ours(args, world, rank, local):
         ms = min(b.run(m, **mt)["device_ms"] for _ in range(2))
         drivers[m] = {"paths_per_s": total_paths / (ms / 1e3), "tuning": mt}
 
-    roof = rq = ff = cpu = inv = sdf = None
+    roof = rq = ff = cpu = inv = sdf = bb = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the dominant kernel
         # traversal work counted in a stats run (same rays: the traversal is deterministic)
@@ -565,6 +602,7 @@ def run_ours(args, world, rank, local):
             ff = full_frame(local, {m: d["tuning"] for m, d in drivers.items()} or None)
         inv = None if args.no_adjoint else inverse_rendering(local)
         sdf = None if args.no_sdf else sdf_scene(local, 0.0 if (args.no_cpu or world > 1) else 5.0)
+        bb = None if args.no_build else bvh_build(local, cpu=not args.no_cpu and world == 1)
         if world == 1 and not args.no_cpu:
             import oracle
             kind = "reference" if oracle.have_reference() else "port"
@@ -589,7 +627,7 @@ def run_ours(args, world, rank, local):
                 "plain_kernel_launches": plain["kernel_launches"],
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
-                "inverse_rendering": inv, "sdf_scene": sdf, "cpu_baseline": cpu}
+                "inverse_rendering": inv, "sdf_scene": sdf, "bvh_build": bb, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     b.close()
 
@@ -607,6 +645,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-sdf", action="store_true")
+    ap.add_argument("--no-build", action="store_true")
     ap.add_argument("--profile-run", choices=["loop", "persistent"], default=None,
                     help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
     ap.add_argument("--profile-sdf", action="store_true",

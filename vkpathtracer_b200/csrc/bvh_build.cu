@@ -108,16 +108,38 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(uint32_t* __restrict_
   if (i0 + 1u < m) out[i0 + 1u] += add;
 }
 
+// The builder's memory pool on the current device: freed scratch stays mapped
+// (up to 1 GiB) for the next build instead of going back to the driver.
+cudaMemPool_t build_pool() {
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = 1ull << 30;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 // Stream-ordered scratch allocations, released on destruction.
 struct Scratch {
   cudaStream_t s;
   std::vector<void*> ptrs;
   cudaError_t err = cudaSuccess;
+  cudaMemPool_t pool = build_pool();
   template <class T>
   T* get(size_t n) {
     void* p = nullptr;
     if (err != cudaSuccess) return nullptr;
-    err = cudaMallocAsync(&p, std::max<size_t>(1, n) * sizeof(T), s);
+    const size_t bytes = std::max<size_t>(1, n) * sizeof(T);
+    err = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, s) : cudaMallocAsync(&p, bytes, s);
     if (err != cudaSuccess) return nullptr;
     ptrs.push_back(p);
     return static_cast<T*>(p);
@@ -303,6 +325,31 @@ __global__ void k_centroid_bounds(BuildArrays A, const uint32_t* __restrict__ id
         kmax[a] = max(kmax[a], omax[a]);
       }
     }
+  }
+  // A block whose positions all belong to one node (the common case in the
+  // upper levels) combines its warps in shared memory: one atomic per key.
+  __shared__ uint32_t blk[kThreads / 32][6];
+  __shared__ int32_t s0;
+  if (threadIdx.x == 0) s0 = s;
+  __syncthreads();
+  const bool uniform = __syncthreads_and(s == s0) && s0 >= 0;
+  if (uniform) {
+    if (lane == 0u) {
+      for (int a = 0; a < 3; ++a) {
+        blk[threadIdx.x >> 5][a] = kmin[a];
+        blk[threadIdx.x >> 5][3 + a] = kmax[a];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6u) {
+      uint32_t v = blk[0][threadIdx.x];
+      for (int w = 1; w < kThreads / 32; ++w)
+        v = threadIdx.x < 3u ? min(v, blk[w][threadIdx.x]) : max(v, blk[w][threadIdx.x]);
+      uint32_t* k = A.cb + 6 * s0 + threadIdx.x;
+      if (threadIdx.x < 3u) atomicMin(k, v);
+      else atomicMax(k, v);
+    }
+    return;
   }
   const int32_t sp = __shfl_up_sync(0xffffffffu, s, 1);
   const bool head = s >= 0 && (lane == 0u || sp != s);
@@ -606,58 +653,94 @@ __global__ void k_sah_bin(BuildArrays A, const uint32_t* __restrict__ idx, const
   }
 }
 
-// Best binned split of each large node (same sweep as the host SAH builder).
+// Best binned split of each large node (the host SAH builder's sweep), one
+// warp per node: lane b holds bin b; suffix and prefix counts and bounds by
+// shuffle scans, the cheapest plane by a warp argmin (lowest axis, then bin,
+// on equal cost, as the sequential sweep keeps the first minimum).
 __global__ void k_sah_split(BuildArrays A, const uint32_t* __restrict__ bins, uint32_t n_act) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = static_cast<int>(threadIdx.x & 31u);
   if (s >= n_act) return;
   const uint32_t* k = A.cb + 6 * s;
-  int best_axis = -1, best_bin = -1;
   float best_cost = FLT_MAX;
+  int best_axis = -1, best_bin = -1;
   for (int a = 0; a < 3; ++a) {
     const float ext = fval(k[3 + a]) - fval(k[a]);
     if (!(ext > 0.0f)) continue;
-    const uint32_t* bw = bins + kBinWords * ((s * 3u + static_cast<uint32_t>(a)) * kSahBins);
-    float rarea[kSahBins];
-    uint32_t rcnt[kSahBins];
-    float rlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-    uint32_t rc = 0u;
-    for (int b = kSahBins - 1; b > 0; --b) {
-      const uint32_t* w = bw + kBinWords * b;
-      rc += w[0];
-      if (w[0]) {
-        for (int q = 0; q < 3; ++q) {
-          rlo[q] = bmin(rlo[q], fval(w[1 + q]));
-          rhi[q] = bmax(rhi[q], fval(w[4 + q]));
-        }
-      }
-      rcnt[b] = rc;
-      const float dx = rhi[0] - rlo[0], dy = rhi[1] - rlo[1], dz = rhi[2] - rlo[2];
-      rarea[b] = rc ? dx * dy + dy * dz + dz * dx : 0.0f;
+    const uint32_t* w = bins + kBinWords * ((s * 3u + static_cast<uint32_t>(a)) * kSahBins + static_cast<uint32_t>(lane));
+    const uint32_t cnt = w[0];
+    float lo[3], hi[3];
+    for (int q = 0; q < 3; ++q) {
+      lo[q] = cnt ? fval(w[1 + q]) : FLT_MAX;
+      hi[q] = cnt ? fval(w[4 + q]) : -FLT_MAX;
     }
-    float llo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, lhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-    uint32_t lc = 0u;
-    for (int b = 0; b < kSahBins - 1; ++b) {
-      const uint32_t* w = bw + kBinWords * b;
-      lc += w[0];
-      if (w[0]) {
+    // prefix over bins 0..lane (left side of the plane after this bin)
+    uint32_t lc = cnt;
+    float llo[3] = {lo[0], lo[1], lo[2]}, lhi[3] = {hi[0], hi[1], hi[2]};
+    // suffix over bins lane..31 (right side of the plane before this bin)
+    uint32_t rc = cnt;
+    float rlo[3] = {lo[0], lo[1], lo[2]}, rhi[3] = {hi[0], hi[1], hi[2]};
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t lcu = __shfl_up_sync(0xffffffffu, lc, o);
+      const uint32_t rcd = __shfl_down_sync(0xffffffffu, rc, o);
+      float lu[6], rd[6];
+      for (int q = 0; q < 3; ++q) {
+        lu[q] = __shfl_up_sync(0xffffffffu, llo[q], o);
+        lu[3 + q] = __shfl_up_sync(0xffffffffu, lhi[q], o);
+        rd[q] = __shfl_down_sync(0xffffffffu, rlo[q], o);
+        rd[3 + q] = __shfl_down_sync(0xffffffffu, rhi[q], o);
+      }
+      if (lane >= o) {
+        lc += lcu;
         for (int q = 0; q < 3; ++q) {
-          llo[q] = bmin(llo[q], fval(w[1 + q]));
-          lhi[q] = bmax(lhi[q], fval(w[4 + q]));
+          llo[q] = bmin(llo[q], lu[q]);
+          lhi[q] = bmax(lhi[q], lu[3 + q]);
         }
       }
-      if (lc == 0u || rcnt[b + 1] == 0u) continue;
-      const float dx = lhi[0] - llo[0], dy = lhi[1] - llo[1], dz = lhi[2] - llo[2];
-      const float cost = (dx * dy + dy * dz + dz * dx) * static_cast<float>(lc) +
-                         rarea[b + 1] * static_cast<float>(rcnt[b + 1]);
-      if (cost < best_cost) {
-        best_cost = cost;
-        best_axis = a;
-        best_bin = b;
+      if (lane + o < 32) {
+        rc += rcd;
+        for (int q = 0; q < 3; ++q) {
+          rlo[q] = bmin(rlo[q], rd[q]);
+          rhi[q] = bmax(rhi[q], rd[3 + q]);
+        }
       }
+    }
+    // the plane after bin `lane`: left = prefix(lane), right = suffix(lane + 1)
+    const uint32_t rcn = __shfl_down_sync(0xffffffffu, rc, 1);
+    float rn[6];
+    for (int q = 0; q < 3; ++q) {
+      rn[q] = __shfl_down_sync(0xffffffffu, rlo[q], 1);
+      rn[3 + q] = __shfl_down_sync(0xffffffffu, rhi[q], 1);
+    }
+    float cost = FLT_MAX;
+    if (lane < 31 && lc != 0u && rcn != 0u) {
+      const float dx = lhi[0] - llo[0], dy = lhi[1] - llo[1], dz = lhi[2] - llo[2];
+      const float ex = rn[3] - rn[0], ey = rn[4] - rn[1], ez = rn[5] - rn[2];
+      cost = (dx * dy + dy * dz + dz * dx) * static_cast<float>(lc) + (ex * ey + ey * ez + ez * ex) * static_cast<float>(rcn);
+    }
+    // warp argmin, lowest bin first on equal cost
+    float c = cost;
+    int b = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float co = __shfl_xor_sync(0xffffffffu, c, o);
+      const int bo = __shfl_xor_sync(0xffffffffu, b, o);
+      if (co < c || (co == c && bo < b)) {
+        c = co;
+        b = bo;
+      }
+    }
+    if (c < best_cost) {
+      best_cost = c;
+      best_axis = a;
+      best_bin = b;
     }
   }
-  A.axis[s] = best_axis;
-  A.split[s] = __uint_as_float(static_cast<uint32_t>(best_bin < 0 ? 0 : best_bin));
+  if (lane == 0) {
+    A.axis[s] = best_axis;
+    A.split[s] = __uint_as_float(static_cast<uint32_t>(best_bin < 0 ? 0 : best_bin));
+  }
 }
 
 // ---------------------------------------------------------------- refit, ids, outputs
@@ -1022,7 +1105,7 @@ cudaError_t build_tree(const float4* blo, const float4* bhi, uint32_t n, bool sa
     if (sah) {
       k_sah_bin_init<<<grid_for(static_cast<uint64_t>(n_act) * 3u * kSahBins), kThreads, 0, s>>>(bins, n_act);
       k_sah_bin<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, bins);
-      k_sah_split<<<grid_for(n_act, 64), 64, 0, s>>>(A, bins, n_act);
+      k_sah_split<<<grid_for(static_cast<uint64_t>(n_act) * 32u, 128), 128, 0, s>>>(A, bins, n_act);
     } else {
       k_midpoint_split<<<grid_for(n_act), kThreads, 0, s>>>(A, n_act);
     }
@@ -1126,7 +1209,7 @@ void FreeDeviceAccel(DeviceAccelOut& out) {
   out = DeviceAccelOut{};
 }
 
-cudaError_t BuildAccelOnDevice(const float* vertices, uint32_t vertex_count, const uint32_t* indices,
+cudaError_t BuildAccelOnDevice(const float* d_vertices, uint32_t vertex_count, const uint32_t* d_indices,
                                uint32_t index_count, const uint32_t* instances, uint32_t instance_count, bool sah,
                                cudaStream_t stream, DeviceAccelOut& out) {
   out = DeviceAccelOut{};
@@ -1136,8 +1219,6 @@ cudaError_t BuildAccelOnDevice(const float* vertices, uint32_t vertex_count, con
   const unsigned long long candidates = prefix[instance_count];
   if (candidates >= (1ull << 31)) return cudaErrorInvalidValue;
   Scratch sc{stream};
-  float* d_v = sc.get<float>(3ull * vertex_count);
-  uint32_t* d_i = sc.get<uint32_t>(index_count);
   uint32_t* d_inst = sc.get<uint32_t>(3ull * instance_count);
   unsigned long long* d_prefix = sc.get<unsigned long long>(instance_count + 1u);
   const uint32_t nc = static_cast<uint32_t>(candidates);
@@ -1145,12 +1226,10 @@ cudaError_t BuildAccelOnDevice(const float* vertices, uint32_t vertex_count, con
   uint32_t* pos = sc.get<uint32_t>(nc + 1u);
   uint32_t* nonfinite = sc.get<uint32_t>(1);
   if (sc.err != cudaSuccess) return sc.err;
-  if (vertex_count) BB_TRY(cudaMemcpyAsync(d_v, vertices, 12ull * vertex_count, cudaMemcpyHostToDevice, stream));
-  if (index_count) BB_TRY(cudaMemcpyAsync(d_i, indices, 4ull * index_count, cudaMemcpyHostToDevice, stream));
   if (instance_count) BB_TRY(cudaMemcpyAsync(d_inst, instances, 12ull * instance_count, cudaMemcpyHostToDevice, stream));
   BB_TRY(cudaMemcpyAsync(d_prefix, prefix.data(), 8ull * (instance_count + 1u), cudaMemcpyHostToDevice, stream));
   BB_TRY(cudaMemsetAsync(nonfinite, 0, 4, stream));
-  const FlatIn f{d_v, vertex_count, d_i, index_count, d_inst, d_prefix, instance_count, nc};
+  const FlatIn f{d_vertices, vertex_count, d_indices, index_count, d_inst, d_prefix, instance_count, nc};
   if (nc) k_flat_valid<<<grid_for(nc), kThreads, 0, stream>>>(f, flag);
   BB_TRY(exclusive_scan(flag, nc, pos, sc));
   uint32_t n = 0u;

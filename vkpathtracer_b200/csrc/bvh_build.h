@@ -30,10 +30,11 @@ struct DeviceAccelOut {
   bool fallback = false;       // non-finite primitive bounds: use the host builder instead
 };
 
-// Builds everything from the scene arrays (host pointers; copied to the
-// device).  sah: the traversal tree is a binned-SAH tree instead of the
+// Builds everything from the scene arrays: vertices and indices in device
+// memory, the instance table (first_triangle, triangle_count, material) on
+// the host.  sah: the traversal tree is a binned-SAH tree instead of the
 // reference tree.  Returns a CUDA error; on fallback, nothing is allocated.
-cudaError_t BuildAccelOnDevice(const float* vertices, uint32_t vertex_count, const uint32_t* indices,
+cudaError_t BuildAccelOnDevice(const float* d_vertices, uint32_t vertex_count, const uint32_t* d_indices,
                                uint32_t index_count, const uint32_t* instances, uint32_t instance_count, bool sah,
                                cudaStream_t stream, DeviceAccelOut& out);
 

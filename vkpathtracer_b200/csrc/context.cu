@@ -105,8 +105,10 @@ struct vkptc_ctx {
   // scene (host copies needed to rebuild)
   SceneGeometry geo;                      // flattened on the host (host build, external BVHs)
   bool geo_ready = false;
-  std::vector<float> raw_vertices;        // the scene's arrays, for the device build
-  std::vector<uint32_t> raw_indices, raw_instances;
+  DevBuf<float> d_raw_vertices;           // the scene's arrays, for the device build
+  DevBuf<uint32_t> d_raw_indices;
+  uint32_t raw_vertex_count = 0, raw_index_count = 0;
+  std::vector<uint32_t> raw_instances;
   uint32_t prim_count = 0;                // flattened primitives of the built accelerator
   std::vector<float> materials, lights;
   float env[3] = {0, 0, 0};
@@ -529,13 +531,21 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
     }
     ctx->geo = std::move(geo);
     ctx->geo_ready = true;
-    ctx->raw_vertices.clear();
-    ctx->raw_indices.clear();
+    ctx->d_raw_vertices.release();
+    ctx->d_raw_indices.release();
     ctx->raw_instances.clear();
   } else {
     // Flattened on the device by the build (or on the host for an external BVH).
-    ctx->raw_vertices.assign(scene->vertices, scene->vertices + 3 * static_cast<size_t>(scene->vertex_count));
-    ctx->raw_indices.assign(scene->indices, scene->indices + scene->index_count);
+    ctx->raw_vertex_count = scene->vertex_count;
+    ctx->raw_index_count = scene->index_count;
+    VKPTC_CUDA(ctx, ctx->d_raw_vertices.alloc(std::max<size_t>(1, 3ull * scene->vertex_count)), "scene alloc");
+    VKPTC_CUDA(ctx, ctx->d_raw_indices.alloc(std::max<size_t>(1, scene->index_count)), "scene alloc");
+    if (scene->vertex_count)
+      VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_raw_vertices.ptr, scene->vertices, 12ull * scene->vertex_count,
+                                 cudaMemcpyHostToDevice), "scene upload");
+    if (scene->index_count)
+      VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_raw_indices.ptr, scene->indices, 4ull * scene->index_count,
+                                 cudaMemcpyHostToDevice), "scene upload");
     ctx->raw_instances.assign(scene->instances, scene->instances + 3 * static_cast<size_t>(scene->instance_count));
     ctx->geo = SceneGeometry{};
     ctx->geo_ready = false;
@@ -656,10 +666,15 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
 // Host flattening of the scene for the host build and external BVHs.
 int32_t ensure_geo(vkptc_ctx* c) {
   if (c->geo_ready) return VKPTC_OK;
+  std::vector<float> v(3ull * c->raw_vertex_count);
+  std::vector<uint32_t> idx(c->raw_index_count);
+  if (!v.empty())
+    VKPTC_CUDA(c, cudaMemcpy(v.data(), c->d_raw_vertices.ptr, v.size() * 4, cudaMemcpyDeviceToHost), "scene read");
+  if (!idx.empty())
+    VKPTC_CUDA(c, cudaMemcpy(idx.data(), c->d_raw_indices.ptr, idx.size() * 4, cudaMemcpyDeviceToHost), "scene read");
   std::string err;
   SceneGeometry geo;
-  if (!FlattenScene(c->raw_vertices.data(), static_cast<uint32_t>(c->raw_vertices.size() / 3), c->raw_indices.data(),
-                    static_cast<uint32_t>(c->raw_indices.size()), c->raw_instances.data(),
+  if (!FlattenScene(v.data(), c->raw_vertex_count, idx.data(), c->raw_index_count, c->raw_instances.data(),
                     static_cast<uint32_t>(c->raw_instances.size() / 3), geo, err)) {
     return fail(c, VKPTC_INVALID_ARGUMENT, err);
   }
@@ -676,8 +691,7 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
   const auto t0 = std::chrono::steady_clock::now();
   DeviceAccelOut out;
   const cudaError_t e = BuildAccelOnDevice(
-      c->raw_vertices.data(), static_cast<uint32_t>(c->raw_vertices.size() / 3), c->raw_indices.data(),
-      static_cast<uint32_t>(c->raw_indices.size()), c->raw_instances.data(),
+      c->d_raw_vertices.ptr, c->raw_vertex_count, c->d_raw_indices.ptr, c->raw_index_count, c->raw_instances.data(),
       static_cast<uint32_t>(c->raw_instances.size() / 3), c->config.bvh_mode == VKPTC_BVH_SAH, c->stream, out);
   if (e != cudaSuccess) {
     FreeDeviceAccel(out);
@@ -858,8 +872,8 @@ int32_t vkptc_shutdown(vkptc_ctx* ctx) {
   ctx->adj.setup = false;
   ctx->geo = SceneGeometry{};
   ctx->geo_ready = false;
-  ctx->raw_vertices.clear();
-  ctx->raw_indices.clear();
+  ctx->d_raw_vertices.release();
+  ctx->d_raw_indices.release();
   ctx->raw_instances.clear();
   ctx->prim_count = 0;
   ctx->wide = WideBvh{};
