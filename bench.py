@@ -476,6 +476,20 @@ def profile_run(args, local):
                       "iterations": r["iterations"], "device_ms": r["device_ms"], "paths": r["paths"]}), flush=True)
 
 
+def profile_build(local):
+    """Small fixed run for profilers: the 2,064,418-triangle sphere grid built
+    twice on the device with each traversal tree (reference, SAH)."""
+    from vkpathtracer_b200.tracer import CudaPathTracer
+    sc = scenes.sphere_grid()
+    for bvh in ("reference", "sah"):
+        with CudaPathTracer(device=local, bvh=bvh) as t:
+            t.configure(scenes.RenderSettings(width=64, height=64, spp=1))
+            t.load_scene_snapshot(sc)
+            for _ in range(2):
+                t.build_or_update_acceleration()
+            print(json.dumps({"profile_build": bvh, "build_ms": t.accel_info()["build_ms"]}), flush=True)
+
+
 def profile_sdf(local):
     """Small fixed run for profilers: the SDF gallery (640x360, 4 spp, depth 8)
     rendered twice by the loop driver without a CUDA graph."""
@@ -648,6 +662,8 @@ def main():
     ap.add_argument("--no-build", action="store_true")
     ap.add_argument("--profile-run", choices=["loop", "persistent"], default=None,
                     help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
+    ap.add_argument("--profile-build", action="store_true",
+                    help="profiling aid: build the 2M-triangle sphere grid twice per traversal tree and exit")
     ap.add_argument("--profile-sdf", action="store_true",
                     help="profiling aid: render the SDF gallery twice with the loop driver, no CUDA graph, and exit")
     ap.add_argument("--cpu-step-seconds", type=float, default=0.0,
@@ -657,7 +673,9 @@ def main():
         args.warmup = 3
     world, rank, local = dist_init(args)
     try:
-        if args.profile_sdf:
+        if args.profile_build:
+            profile_build(local)
+        elif args.profile_sdf:
             profile_sdf(local)
         elif args.profile_run:
             profile_run(args, local)

@@ -214,8 +214,11 @@ int32_t vkptc_configure(vkptc_ctx* ctx, const vkptc_render_settings* settings);
 /* replaces IPathTracer::load_scene_snapshot (src/pathtracer/PathTracer.h:1088) */
 int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene);
 /* replaces IPathTracer::build_or_update_acceleration (src/pathtracer/PathTracer.h:1092):
- * builds the binary midpoint BVH on the host exactly as ParallelBvhBuilder
- * does (deterministic mode) and flattens it into the wide HBM layout. */
+ * builds the binary midpoint BVH exactly as ParallelBvhBuilder does
+ * (deterministic mode), optionally a binned-SAH traversal tree, and flattens
+ * the traversal tree into the wide HBM layout -- on the device by default
+ * (VKPTC_BUILD_DEVICE), on the host with VKPTC_BUILD_HOST; the arrays are the
+ * same either way. */
 int32_t vkptc_build_acceleration(vkptc_ctx* ctx);
 /* Same, from an externally built binary BVH (the reference's ParallelBvhBuilder
  * output over the accelerator's primitive order, CpuBvhAccelerator.cpp:247-256). */
