@@ -133,6 +133,21 @@ typedef struct vkptc_scene_view {
    * Shapes outside vkptc_sdf_shape never hit (the reference's switch default). */
   const float* sdf_primitives;
   uint32_t sdf_count;
+  /* Optional dynamic-transform instances (RTInstance, src/pathtracer/PathTracer.h:276-296),
+   * flattened as CpuBvhAccelerator::build does (src/pathtracer/CpuBvhAccelerator.cpp:173-247):
+   * instance_local holds 5 words per instance (flags, local_first_vertex, local_vertex_count,
+   * local_first_index, local_index_count) and instance_transforms 10 floats per instance
+   * (translation xyz, rotation quaternion xyzw, scale xyz).  An instance with flag bit 0
+   * (kRTInstanceFlagDynamicTransform) and local vertices and indices takes each triangle from
+   * local_vertices / local_indices, scaled, rotated and translated to world space, falling back
+   * to the global arrays for a triangle whose local indices are out of range.  NULL arrays:
+   * every instance uses the global arrays. */
+  const uint32_t* instance_local;
+  const float* instance_transforms;
+  const float* local_vertices;
+  uint32_t local_vertex_count;
+  const uint32_t* local_indices;
+  uint32_t local_index_count;
 } vkptc_scene_view;
 
 /* SdfShape (src/pathtracer/PathTracer.h:232-240). */

@@ -50,6 +50,12 @@ class VkoScene(ctypes.Structure):
         ("environment_map_scale", ctypes.c_float * 3),
         ("sdf_primitives", ctypes.c_void_p),
         ("sdf_count", ctypes.c_uint32),
+        ("instance_local", ctypes.c_void_p),
+        ("instance_transforms", ctypes.c_void_p),
+        ("local_vertices", ctypes.c_void_p),
+        ("local_vertex_count", ctypes.c_uint32),
+        ("local_indices", ctypes.c_void_p),
+        ("local_index_count", ctypes.c_uint32),
     ]
 
 
@@ -155,6 +161,15 @@ class Oracle:
             sdf = np.ascontiguousarray(sdf, np.float32).reshape(-1, 16)
             keep = keep + (sdf,)
             s.sdf_primitives, s.sdf_count = _ptr(sdf), sdf.shape[0]
+        if getattr(scene, "instance_local", None) is not None:
+            il = np.ascontiguousarray(scene.instance_local, np.uint32).reshape(-1, 5)
+            it = np.ascontiguousarray(scene.instance_transforms, np.float32).reshape(-1, 10)
+            lv = np.ascontiguousarray(scene.local_vertices, np.float32).reshape(-1, 3)
+            li = np.ascontiguousarray(scene.local_indices, np.uint32).reshape(-1)
+            keep = keep + (il, it, lv, li)
+            s.instance_local, s.instance_transforms = _ptr(il), _ptr(it)
+            s.local_vertices, s.local_vertex_count = (_ptr(lv) if lv.size else None), lv.shape[0]
+            s.local_indices, s.local_index_count = (_ptr(li) if li.size else None), li.size
         return s, keep
 
     @staticmethod
@@ -193,6 +208,20 @@ class Oracle:
         self._check(rc)
         return {"sum": film, "count": count, "invalid": invalid, "samples": samples,
                 "counters": ctr.as_dict()}
+
+    def convert_scene_json(self, path: str):
+        """Reference only: a scene document converted by the reference's own
+        SceneDocument loader and BuildSceneDataFromDocument, as a Scene."""
+        import tempfile
+        from vkpathtracer_b200 import scenes
+        if self.kind != "reference":
+            raise RuntimeError("scene documents are converted by the reference oracle only")
+        self.lib.vko_convert_scene_json.restype = ctypes.c_int
+        self.lib.vko_convert_scene_json.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "snapshot.bin")
+            self._check(self.lib.vko_convert_scene_json(path.encode(), out.encode()))
+            return scenes.load_snapshot_dump(out, os.path.splitext(os.path.basename(path))[0])
 
     def build_bvh(self, scene, leaf_threshold: int = 4, deterministic: bool = True):
         sc, keep = self.make_scene(scene)

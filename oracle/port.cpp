@@ -27,6 +27,7 @@
 //     sdf_distance, sdf_normal      src/pathtracer/ScalarCpuPathTracer.cpp:808-853
 //     intersect_sphere, the march   src/pathtracer/ScalarCpuPathTracer.cpp:855-930
 //     nearest-hit reduction         src/pathtracer/ScalarCpuPathTracer.Intersect.cpp:91-129
+//   dynamic-instance flattening     src/pathtracer/CpuBvhAccelerator.cpp:47-74, 173-247
 
 #include "vkpt_oracle.h"
 
@@ -376,15 +377,54 @@ struct World {
   float fov = 60.0f;
   float aperture = 0.0f, focus = 0.0f;
 
+  // transform_instance_vertex: scale, rotate by the normalized quaternion, translate.
+  static V3 instance_vertex(V3 l, const float* t) {
+    const V3 sc{l.x * t[7], l.y * t[8], l.z * t[9]};
+    const float len_sq = t[3] * t[3] + t[4] * t[4] + t[5] * t[5] + t[6] * t[6];
+    V3 r = sc;
+    if (!(len_sq <= kEps * kEps)) {
+      const float inv = 1.0f / std::sqrt(len_sq);
+      const V3 q{t[3] * inv, t[4] * inv, t[5] * inv};
+      const float qw = t[6] * inv;
+      const V3 tt = mul(cross(q, sc), 2.0f);
+      r = add(add(sc, mul(tt, qw)), cross(q, tt));
+    }
+    return add(r, V3{t[0], t[1], t[2]});
+  }
+
   void load(const vko_scene& s, bool stable = true, size_t leaf = 4) {
+    const bool dyn = s.instance_local && s.instance_transforms;
     for (uint32_t i = 0; i < s.instance_count; ++i) {
       const uint32_t first = s.instances[3 * i], count = s.instances[3 * i + 1], mat = s.instances[3 * i + 2];
+      const uint32_t* loc = dyn ? s.instance_local + 5 * i : nullptr;
+      const bool use_local = loc && (loc[0] & 1u) && loc[2] > 0u && loc[4] > 0u;
       for (uint32_t k = 0; k < count; ++k) {
-        const uint32_t base = (first + k) * 3u;
-        if (base + 2u >= s.index_count) continue;
-        const uint32_t a = s.indices[base], b = s.indices[base + 1], c = s.indices[base + 2];
-        if (a >= s.vertex_count || b >= s.vertex_count || c >= s.vertex_count) continue;
-        const V3 v0 = ld3(s.vertices + 3 * a), v1 = ld3(s.vertices + 3 * b), v2 = ld3(s.vertices + 3 * c);
+        V3 v0{}, v1{}, v2{};
+        bool loaded = false;
+        if (use_local) {
+          const uint32_t lb = loc[3] + k * 3u, le = loc[1] + loc[2];
+          if (lb < 0xFFFFFFFEu && lb + 2u < s.local_index_count) {
+            const uint32_t a = loc[1] + s.local_indices[lb], b = loc[1] + s.local_indices[lb + 1],
+                           c = loc[1] + s.local_indices[lb + 2];
+            if (a < le && b < le && c < le && a < s.local_vertex_count && b < s.local_vertex_count &&
+                c < s.local_vertex_count) {
+              const float* t = s.instance_transforms + 10 * i;
+              v0 = instance_vertex(ld3(s.local_vertices + 3 * a), t);
+              v1 = instance_vertex(ld3(s.local_vertices + 3 * b), t);
+              v2 = instance_vertex(ld3(s.local_vertices + 3 * c), t);
+              loaded = true;
+            }
+          }
+        }
+        if (!loaded) {
+          const uint32_t base = (first + k) * 3u;
+          if (base >= 0xFFFFFFFEu || base + 2u >= s.index_count) continue;
+          const uint32_t a = s.indices[base], b = s.indices[base + 1], c = s.indices[base + 2];
+          if (a >= s.vertex_count || b >= s.vertex_count || c >= s.vertex_count) continue;
+          v0 = ld3(s.vertices + 3 * a);
+          v1 = ld3(s.vertices + 3 * b);
+          v2 = ld3(s.vertices + 3 * c);
+        }
         Box bx;
         bx.lo[0] = std::min({v0.x, v1.x, v2.x}) - kEps;
         bx.lo[1] = std::min({v0.y, v1.y, v2.y}) - kEps;

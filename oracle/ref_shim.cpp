@@ -16,6 +16,7 @@
 
 #include "core/Logging.h"
 #include "cpu/ParallelBvhBuilder.h"
+#include "scene/Scene.h"
 #include "cpu/TiledCpuPathTracer.h"
 #include "pathtracer/PathTracer.h"
 
@@ -23,6 +24,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -58,6 +60,24 @@ pt::PathTracerSceneSnapshot to_snapshot(const vko_scene& s) {
     out.instances[i].first_triangle = s.instances[3 * i + 0];
     out.instances[i].triangle_count = s.instances[3 * i + 1];
     out.instances[i].material_index = s.instances[3 * i + 2];
+    if (s.instance_local && s.instance_transforms) {
+      const uint32_t* l = s.instance_local + 5 * i;
+      const float* t = s.instance_transforms + 10 * i;
+      pt::RTInstance& r = out.instances[i];
+      r.flags = l[0];
+      r.local_first_vertex = l[1];
+      r.local_vertex_count = l[2];
+      r.local_first_index = l[3];
+      r.local_index_count = l[4];
+      r.translation = pt::Vec3{t[0], t[1], t[2]};
+      r.rotation = pt::Quat4{t[3], t[4], t[5], t[6]};
+      r.scale = pt::Vec3{t[7], t[8], t[9]};
+    }
+  }
+  if (s.instance_local && s.instance_transforms) {
+    out.local_vertices.resize(s.local_vertex_count);
+    for (uint32_t i = 0; i < s.local_vertex_count; ++i) out.local_vertices[i] = v3(s.local_vertices + 3 * i);
+    out.local_indices.assign(s.local_indices, s.local_indices + s.local_index_count);
   }
   out.materials.resize(s.material_count);
   for (uint32_t i = 0; i < s.material_count; ++i) {
@@ -228,6 +248,104 @@ int render_full(pt::IPathTracer& tracer, const vko_settings& st, uint32_t first,
 extern "C" {
 
 const char* vko_last_error(void) { return g_error.c_str(); }
+
+// Snapshot dump of a converted scene document, little-endian:
+//   char[4] "VKSJ", u32 version (1)
+//   u32 nv, ni, ninst, nmat, nlight, nsdf, nlv, nli, env_w, env_h
+//   f32 vertices[3 nv]; u32 indices[ni]; u32 instances[3 ninst];
+//   u32 instance_local[5 ninst]; f32 instance_transforms[10 ninst];
+//   f32 materials[16 nmat]; f32 lights[16 nlight]; f32 sdf[16 nsdf];
+//   f32 local_vertices[3 nlv]; u32 local_indices[nli];
+//   f32 environment[3]; f32 camera[12] (position3, target3, up3, fov, aperture, focus);
+//   f32 environment_map_scale[3]; f32 environment_map[3 env_w env_h]
+// Record layouts as in vkpt_oracle.h (material and light word maps, SDF records).
+int vko_convert_scene_json(const char* path, const char* out_path) {
+  quiet_logs();
+  if (!path || !out_path) return fail("null path");
+  auto doc = vkpt::scene::SceneDocument::load_from_file(path);
+  if (!doc) return fail(std::string("scene document failed to load: ") + path);
+  std::vector<std::string> issues;
+  if (!doc.value().validate(&issues)) return fail("scene document failed validation");
+  auto conv = pt::BuildSceneDataFromDocument(doc.value());
+  if (!conv) return fail("BuildSceneDataFromDocument failed");
+  const pt::PathTracerSceneSnapshot& s = conv.value();
+  std::vector<float> f32;
+  std::vector<uint32_t> u32;
+  FILE* fp = std::fopen(out_path, "wb");
+  if (!fp) return fail("cannot open output");
+  auto wu = [&](const std::vector<uint32_t>& v) { if (!v.empty()) std::fwrite(v.data(), 4, v.size(), fp); };
+  auto wf = [&](const std::vector<float>& v) { if (!v.empty()) std::fwrite(v.data(), 4, v.size(), fp); };
+  std::fwrite("VKSJ", 1, 4, fp);
+  const uint32_t head[11] = {1u,
+                             static_cast<uint32_t>(s.vertices.size()),
+                             static_cast<uint32_t>(s.indices.size()),
+                             static_cast<uint32_t>(s.instances.size()),
+                             static_cast<uint32_t>(s.materials.size()),
+                             static_cast<uint32_t>(s.lights.size()),
+                             static_cast<uint32_t>(s.sdf_primitives.size()),
+                             static_cast<uint32_t>(s.local_vertices.size()),
+                             static_cast<uint32_t>(s.local_indices.size()),
+                             s.environment_map_width,
+                             s.environment_map_height};
+  std::fwrite(head, 4, 11, fp);
+  f32.clear();
+  for (const auto& v : s.vertices) f32.insert(f32.end(), {v.x, v.y, v.z});
+  wf(f32);
+  wu(s.indices);
+  u32.clear();
+  for (const auto& i : s.instances) u32.insert(u32.end(), {i.first_triangle, i.triangle_count, i.material_index});
+  wu(u32);
+  u32.clear();
+  for (const auto& i : s.instances)
+    u32.insert(u32.end(), {i.flags, i.local_first_vertex, i.local_vertex_count, i.local_first_index, i.local_index_count});
+  wu(u32);
+  f32.clear();
+  for (const auto& i : s.instances)
+    f32.insert(f32.end(), {i.translation.x, i.translation.y, i.translation.z, i.rotation.x, i.rotation.y, i.rotation.z,
+                           i.rotation.w, i.scale.x, i.scale.y, i.scale.z});
+  wf(f32);
+  f32.clear();
+  for (const auto& m : s.materials) {
+    const uint32_t packed = (m.material_effect & 1023u) | ((m.material_flags & 1u) ? 1024u : 0u);
+    f32.insert(f32.end(), {m.albedo.x, m.albedo.y, m.albedo.z, m.emissive.x, m.emissive.y, m.emissive.z, m.roughness,
+                           static_cast<float>(m.material_model), m.metallic, m.ior, m.transmission, m.clearcoat,
+                           m.sheen, m.anisotropy, m.alpha, static_cast<float>(packed)});
+  }
+  wf(f32);
+  f32.clear();
+  for (const auto& l : s.lights)
+    f32.insert(f32.end(), {l.position.x, l.position.y, l.position.z, l.color.x, l.color.y, l.color.z, l.intensity,
+                           l.radius, l.direction.x, l.direction.y, l.direction.z, l.spot_inner_cos, l.spot_outer_cos,
+                           0.0f, 0.0f, 0.0f});
+  wf(f32);
+  f32.clear();
+  for (const auto& p : s.sdf_primitives)
+    f32.insert(f32.end(), {static_cast<float>(static_cast<uint32_t>(p.shape)), p.position.x, p.position.y, p.position.z,
+                           p.scale.x, p.scale.y, p.scale.z, p.rotation.x, p.rotation.y, p.rotation.z,
+                           static_cast<float>(p.material_index), p.radius, p.param_a, p.param_b, 0.0f, 0.0f});
+  wf(f32);
+  f32.clear();
+  for (const auto& v : s.local_vertices) f32.insert(f32.end(), {v.x, v.y, v.z});
+  wf(f32);
+  wu(s.local_indices);
+  f32 = {s.environment_color.x, s.environment_color.y, s.environment_color.z};
+  wf(f32);
+  f32 = {s.camera_position.x, s.camera_position.y, s.camera_position.z, s.camera_target.x, s.camera_target.y,
+         s.camera_target.z, s.camera_up.x, s.camera_up.y, s.camera_up.z, s.camera_fov_deg, s.camera_aperture_radius,
+         s.camera_focus_distance};
+  wf(f32);
+  f32 = {s.environment_map_scale.x, s.environment_map_scale.y, s.environment_map_scale.z};
+  wf(f32);
+  f32.clear();
+  const size_t texels = static_cast<size_t>(s.environment_map_width) * s.environment_map_height;
+  for (size_t i = 0; i < texels && i < s.environment_map.size(); ++i)
+    f32.insert(f32.end(), {s.environment_map[i].x, s.environment_map[i].y, s.environment_map[i].z});
+  f32.resize(3 * texels, 0.0f);
+  wf(f32);
+  std::fclose(fp);
+  return 0;
+}
+
 const char* vko_impl_name(void) { return "reference"; }
 
 int vko_render(const vko_scene* scene, const vko_settings* settings,

@@ -61,6 +61,16 @@ typedef struct vko_scene {
    * param_b, 0, 0 (RTSdfPrimitive, src/pathtracer/PathTracer.h:330-339) */
   const float* sdf_primitives;
   uint32_t sdf_count;
+  /* optional dynamic-transform instances (RTInstance): 5 words per instance
+   * (flags, local_first_vertex, local_vertex_count, local_first_index,
+   * local_index_count), 10 floats per instance (translation3, quaternion xyzw,
+   * scale3), and the local vertex / index arrays; NULL: none */
+  const uint32_t* instance_local;
+  const float* instance_transforms;
+  const float* local_vertices;
+  uint32_t local_vertex_count;
+  const uint32_t* local_indices;
+  uint32_t local_index_count;
 } vko_scene;
 
 typedef struct vko_settings {
@@ -126,6 +136,13 @@ int vko_build_bvh(const vko_scene* scene, uint32_t leaf_threshold, int determini
 int vko_intersect(const vko_scene* scene, const float* rays, uint64_t ray_count,
                   uint32_t threads, uint32_t* prim_out, float* t_out,
                   uint64_t* stats, double* elapsed_ms);
+
+/* Reference only (oracle/_ref): loads a scene document (SceneDocument::
+ * load_from_file, validate) and converts it with BuildSceneDataFromDocument
+ * (src/pathtracer/SceneConversion.cpp), then writes the snapshot's arrays to
+ * out_path in the little-endian layout documented in ref_shim.cpp.  Returns
+ * 0 on success. */
+int vko_convert_scene_json(const char* path, const char* out_path);
 
 const char* vko_last_error(void);
 const char* vko_impl_name(void);

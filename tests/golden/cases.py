@@ -71,6 +71,14 @@ def scene_to_arrays(scene):
     }
     if scene.sdf is not None:
         out["sdf"] = np.ascontiguousarray(scene.sdf, np.float32)
+    if scene.instance_local is not None:
+        out["instance_local"] = np.ascontiguousarray(scene.instance_local, np.uint32)
+        out["instance_transforms"] = np.ascontiguousarray(scene.instance_transforms, np.float32)
+        out["local_vertices"] = np.ascontiguousarray(scene.local_vertices, np.float32)
+        out["local_indices"] = np.ascontiguousarray(scene.local_indices, np.uint32)
+    if scene.env_map is not None:
+        out["env_map"] = np.ascontiguousarray(scene.env_map, np.float32)
+        out["env_scale"] = np.array(scene.env_scale, np.float32)
     return out
 
 
@@ -80,7 +88,11 @@ def scene_from_arrays(d):
                            float(cam[11]))
     return scenes.Scene(d["vertices"], d["indices"], d["instances"], d["materials"], d["lights"],
                         tuple(float(x) for x in d["environment"]), camera, "fixture",
-                        sdf=d.get("sdf")).contiguous()
+                        env_map=d.get("env_map"),
+                        env_scale=tuple(float(x) for x in d["env_scale"]) if "env_scale" in d else (0.0, 0.0, 0.0),
+                        sdf=d.get("sdf"), instance_local=d.get("instance_local"),
+                        instance_transforms=d.get("instance_transforms"), local_vertices=d.get("local_vertices"),
+                        local_indices=d.get("local_indices")).contiguous()
 
 
 def settings_to_arrays(st):
@@ -101,4 +113,21 @@ def settings_from_arrays(d):
 def load_fixture(name):
     import os
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"{name}.npz")
+    return dict(np.load(path))
+
+
+# ---- the reference's own scene documents, converted by its SceneDocument loader and
+# BuildSceneDataFromDocument (tests/golden/make_scene_fixtures.py)
+SCENE_DOCUMENTS = ["cornell_native", "glass_lab", "material_gauntlet", "mirror_room", "neon_room", "shadow_study",
+                   "sdf_complexity", "tessellation_sphere_levels", "ecs_lifecycle_scripting_demo",
+                   "particle_benchmark_simple", "material_shader_physics_showcase"]
+
+
+def scene_document_settings():
+    return scenes.RenderSettings(width=64, height=48, spp=4, max_depth=8, seed=4321, enable_nee=True, enable_mis=True)
+
+
+def load_scene_fixture(name):
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "scenes", f"{name}.npz")
     return dict(np.load(path))

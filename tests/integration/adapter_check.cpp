@@ -5,7 +5,12 @@
 //
 // usage: adapter_check nodevice            (expects no CUDA device)
 //        adapter_check <scene.bin>         (scene + settings written by tests/test_adapter.py)
+//        adapter_check json <scene.json> <width> <height> <spp> <max_depth>
+//            (the scene document loaded and converted by the reference's own
+//             SceneDocument::load_from_file and BuildSceneDataFromDocument, as
+//             ptbench does, src/benchmark/BenchmarkRuntime.cpp:491-596)
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -16,6 +21,7 @@
 #include "CudaPathTracer.h"
 #include "core/Logging.h"
 #include "pathtracer/PathTracer.h"
+#include "scene/Scene.h"
 
 namespace pt = vkpt::pathtracer;
 
@@ -116,6 +122,30 @@ bool load(const char* path, pt::PathTracerSceneSnapshot& s, pt::RenderSettings& 
       s.sdf_primitives.push_back(r);
     }
   }
+  // optional trailer: dynamic-transform instances (instance count, local vertex
+  // and index counts; 5 words and 10 floats per instance; local arrays)
+  uint32_t dyn[3] = {0, 0, 0};
+  if (f.read(reinterpret_cast<char*>(dyn), sizeof(dyn)) && dyn[0] == c[2]) {
+    std::vector<uint32_t> loc, lidx;
+    std::vector<float> tr, lv;
+    if (!read_vec(f, loc, 5ull * dyn[0]) || !read_vec(f, tr, 10ull * dyn[0]) || !read_vec(f, lv, 3ull * dyn[1]) ||
+        !read_vec(f, lidx, dyn[2]))
+      return false;
+    for (uint32_t i = 0; i < dyn[0]; ++i) {
+      pt::RTInstance& r = s.instances[i];
+      r.flags = loc[5 * i];
+      r.local_first_vertex = loc[5 * i + 1];
+      r.local_vertex_count = loc[5 * i + 2];
+      r.local_first_index = loc[5 * i + 3];
+      r.local_index_count = loc[5 * i + 4];
+      const float* t = &tr[10 * i];
+      r.translation = {t[0], t[1], t[2]};
+      r.rotation = {t[3], t[4], t[5], t[6]};
+      r.scale = {t[7], t[8], t[9]};
+    }
+    for (uint32_t i = 0; i < dyn[1]; ++i) s.local_vertices.push_back(pt::Vec3{lv[3 * i], lv[3 * i + 1], lv[3 * i + 2]});
+    s.local_indices = lidx;
+  }
   return true;
 }
 
@@ -154,7 +184,28 @@ int main(int argc, char** argv) {
   }
   pt::PathTracerSceneSnapshot scene;
   pt::RenderSettings st;
-  if (!load(argv[1], scene, st)) {
+  if (std::strcmp(argv[1], "json") == 0) {
+    if (argc < 7) return 2;
+    auto doc = vkpt::scene::SceneDocument::load_from_file(argv[2]);
+    std::vector<std::string> issues;
+    if (!doc || !doc.value().validate(&issues)) {
+      std::printf("FAIL cannot load scene document %s\n", argv[2]);
+      return 2;
+    }
+    auto conv = pt::BuildSceneDataFromDocument(doc.value());
+    if (!conv) {
+      std::printf("FAIL scene conversion %s\n", argv[2]);
+      return 2;
+    }
+    scene = conv.value();
+    st.width = static_cast<uint32_t>(std::atoi(argv[3]));
+    st.height = static_cast<uint32_t>(std::atoi(argv[4]));
+    st.spp = static_cast<uint32_t>(std::atoi(argv[5]));
+    st.max_depth = static_cast<uint32_t>(std::atoi(argv[6]));
+    st.seed = 1234u;
+    std::printf("scene %s: %zu triangles, %zu instances, %zu sdf, %zu lights\n", argv[2], scene.indices.size() / 3,
+                scene.instances.size(), scene.sdf_primitives.size(), scene.lights.size());
+  } else if (!load(argv[1], scene, st)) {
     std::printf("FAIL cannot read %s\n", argv[1]);
     return 2;
   }

@@ -35,9 +35,17 @@ def write_scene(path, sc, st):
                   st.russian_roulette_start_depth], np.uint32).tofile(f)
         np.array([st.seed], np.uint64).tofile(f)
         np.array([st.russian_roulette_min_survival, st.russian_roulette_max_survival], np.float32).tofile(f)
-        if sc.sdf is not None:
-            np.array([sc.sdf.shape[0]], np.uint32).tofile(f)
-            sc.sdf.astype(np.float32).tofile(f)
+        sdf = sc.sdf if sc.sdf is not None else np.zeros((0, 16), np.float32)
+        np.array([sdf.shape[0]], np.uint32).tofile(f)
+        sdf.astype(np.float32).tofile(f)
+        if sc.instance_local is not None:   # dynamic-transform instances
+            lv = np.asarray(sc.local_vertices, np.float32).reshape(-1, 3)
+            li = np.asarray(sc.local_indices, np.uint32).reshape(-1)
+            np.array([sc.instances.shape[0], lv.shape[0], li.size], np.uint32).tofile(f)
+            np.asarray(sc.instance_local, np.uint32).tofile(f)
+            np.asarray(sc.instance_transforms, np.float32).tofile(f)
+            lv.tofile(f)
+            li.tofile(f)
 
 
 @needs_bin
@@ -58,6 +66,31 @@ def test_adapter_matches_reference_through_ipathtracer(tmp_path, which):
     else:
         sc = scenes.sphere_field(4, 12, 14, seed=5, n_lights=4, light_size=2.0, light_height=6.0)
         st = scenes.RenderSettings(width=64, height=40, spp=2, max_depth=8, seed=31)
+    path = os.path.join(tmp_path, "scene.bin")
+    write_scene(path, sc, st)
+    r = subprocess.run([BIN, path], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+
+REFERENCE_SCENES = ["cornell_native", "glass_lab", "tessellation_sphere_levels", "material_shader_physics_showcase",
+                    "sdf_complexity", "mirror_room"]
+
+
+@needs_bin
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", REFERENCE_SCENES)
+def test_adapter_renders_reference_scene_documents(tmp_path, name):
+    """The reference's own scene files as its SceneDocument loader and
+    BuildSceneDataFromDocument convert them (fixtures made by
+    tests/golden/make_scene_fixtures.py), dynamic-transform instances and SDF
+    primitives included, rendered through IPathTracer by both tracers: the
+    snapshot ptbench's `run --scene <file>.json` hands the cuda backend."""
+    from tests.golden import cases
+    d = cases.load_scene_fixture(name)
+    sc = cases.scene_from_arrays(d)
+    st = scenes.RenderSettings(width=64, height=48, spp=2, max_depth=8, seed=1234)
     path = os.path.join(tmp_path, "scene.bin")
     write_scene(path, sc, st)
     r = subprocess.run([BIN, path], capture_output=True, text=True, timeout=300)

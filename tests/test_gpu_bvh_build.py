@@ -61,6 +61,9 @@ def scene_cases():
     bad = tiny_scene(200, seed=3, extra_instances=[(190, 20, 0), (5000, 3, 0), (10, 0, 0)])
     bad.indices[7] = (0, 1, 10 ** 6)
     yield "invalid_and_empty_instances", bad
+    # the reference's own scene documents: dynamic-transform instances with local geometry
+    for name in ("cornell_native", "tessellation_sphere_levels", "material_shader_physics_showcase"):
+        yield name, cases.scene_from_arrays(cases.load_scene_fixture(name))
 
 
 @pytest.mark.parametrize("name,sc", list(scene_cases()))

@@ -230,6 +230,26 @@ def test_film_matches_oracle_environment_map():
     assert rep["bit_exact"] >= ENV_BIT_EXACT_FRAC
 
 
+@pytest.mark.parametrize("name", cases.SCENE_DOCUMENTS)
+def test_film_matches_reference_scene_documents(name):
+    """The reference's own scene files as its converter produces them
+    (dynamic-transform instances, SDF primitives, transmissive materials),
+    against the reference CPU tracer's film of the same snapshot."""
+    d = cases.load_scene_fixture(name)
+    sc, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp)
+        g, cnt, _ = t.film()
+        c = t.read_counters()
+    rep = film_report(g, d["film_sum"], d["samples"], st.spp)
+    print(name, rep)
+    assert np.array_equal(cnt, d["film_count"])
+    assert c["samples"] == int(d["counters"][0])
+    assert rep["rmse_rel"] < RMSE_REL_TOL
+    assert rep["sigma3_fail"] < SIGMA3_FAIL_FRAC
+    assert rep["bit_exact"] >= BIT_EXACT_FRAC
+
+
 @pytest.mark.parametrize("variant", ["gallery", "glass", "complexity"])
 def test_film_matches_oracle_sdf_primitives(variant):
     """SDF primitives next to the triangle BVH: analytic ellipsoid, marched

@@ -193,3 +193,24 @@ def test_port_matches_live_reference_ray_query_with_parallel_axes(port):
     assert np.array_equal(pa, pb)
     assert np.array_equal(bits(ta), bits(tb))
     assert np.array_equal(sa, sb)
+
+
+@pytest.mark.parametrize("name", cases.SCENE_DOCUMENTS)
+def test_port_film_matches_reference_scene_documents(port, name):
+    """The reference's own scene files (converted by its SceneDocument loader
+    and BuildSceneDataFromDocument): dynamic-transform instances flattened
+    through their local geometry and transforms, SDF primitives, transmissive
+    and emissive materials; films, per-sample radiance and counters equal the
+    reference's."""
+    d = cases.load_scene_fixture(name)
+    scene, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
+    r = port.render(scene, st, per_sample=True, threads=4)
+    assert np.array_equal(bits(r["sum"]), bits(d["film_sum"]))
+    assert np.array_equal(r["count"], d["film_count"])
+    assert np.array_equal(bits(r["samples"]), bits(d["samples"]))
+    c = r["counters"]
+    got = np.array([c["samples"], c["rays"], c["triangle_tests"], c["triangle_hits"], c["bvh_node_visits"],
+                    c["bvh_leaf_visits"], c["shadow_tests"]], np.uint64)
+    assert np.array_equal(got, d["counters"])
+    sdf = np.array([c["sdf_tests"], c["sdf_steps"], c["sdf_hits"], c["sdf_misses"]], np.uint64)
+    assert np.array_equal(sdf, d["sdf_counters"])

@@ -183,21 +183,86 @@ struct FlatIn {
   uint32_t nv;
   const uint32_t* idx;
   uint32_t ni;
+  const float* lv;            // local (dynamic-instance) vertices
+  uint32_t nlv;
+  const uint32_t* lidx;
+  uint32_t nli;
   const uint32_t* inst;
+  const uint32_t* inst_local;   // 5 per instance, or null
+  const float* inst_tr;         // 10 per instance, or null
   const unsigned long long* prefix;
   uint32_t ninst;
   uint32_t candidates;
 };
 
+// transform_instance_vertex (the host's TransformInstanceVertex, same operations).
+__device__ __forceinline__ void instance_vertex(const float* l, const float* tr, float out[3]) {
+  const float sx = l[0] * tr[7], sy = l[1] * tr[8], sz = l[2] * tr[9];
+  float rx = sx, ry = sy, rz = sz;
+  const float len_sq = tr[3] * tr[3] + tr[4] * tr[4] + tr[5] * tr[5] + tr[6] * tr[6];
+  if (!(len_sq <= kPadB * kPadB)) {
+    const float inv_len = 1.0f / sqrtf(len_sq);
+    const float qx = tr[3] * inv_len, qy = tr[4] * inv_len, qz = tr[5] * inv_len;
+    const float qw = tr[6] * inv_len;
+    const float tx = (qy * sz - qz * sy) * 2.0f;
+    const float ty = (qz * sx - qx * sz) * 2.0f;
+    const float tz = (qx * sy - qy * sx) * 2.0f;
+    const float cx = qy * tz - qz * ty;
+    const float cy = qz * tx - qx * tz;
+    const float cz = qx * ty - qy * tx;
+    rx = (sx + tx * qw) + cx;
+    ry = (sy + ty * qw) + cy;
+    rz = (sz + tz * qw) + cz;
+  }
+  out[0] = rx + tr[0];
+  out[1] = ry + tr[1];
+  out[2] = rz + tr[2];
+}
+
+// The three world-space vertices of candidate c, or false when the triangle
+// is skipped (CpuBvhAccelerator::build's checks, 32-bit index arithmetic).
+__device__ __forceinline__ bool flat_triangle(const FlatIn& f, uint32_t c, uint32_t& inst, float a[3], float b[3],
+                                              float cc[3]) {
+  const uint32_t i = find_instance(f.prefix, f.ninst, c);
+  inst = i;
+  const uint32_t k = static_cast<uint32_t>(c - f.prefix[i]);
+  if (f.inst_local) {
+    const uint32_t* loc = f.inst_local + 5 * i;
+    if ((loc[0] & 1u) != 0u && loc[2] > 0u && loc[4] > 0u) {
+      const uint32_t local_base = loc[3] + k * 3u;
+      const uint32_t local_end = loc[1] + loc[2];
+      // (a wrapped local_base + 2 would make the reference read out of range: skipped here)
+      if (local_base < 0xFFFFFFFEu && local_base + 2u < f.nli) {
+        const uint32_t v0 = loc[1] + f.lidx[local_base], v1 = loc[1] + f.lidx[local_base + 1u],
+                       v2 = loc[1] + f.lidx[local_base + 2u];
+        if (v0 < local_end && v1 < local_end && v2 < local_end && v0 < f.nlv && v1 < f.nlv && v2 < f.nlv) {
+          const float* tr = f.inst_tr + 10 * i;
+          instance_vertex(f.lv + 3ull * v0, tr, a);
+          instance_vertex(f.lv + 3ull * v1, tr, b);
+          instance_vertex(f.lv + 3ull * v2, tr, cc);
+          return true;
+        }
+      }
+    }
+  }
+  const uint32_t base = (f.inst[3 * i] + k) * 3u;
+  if (base >= 0xFFFFFFFEu || base + 2u >= f.ni) return false;
+  const uint32_t ia = f.idx[base], ib = f.idx[base + 1u], ic = f.idx[base + 2u];
+  if (ia >= f.nv || ib >= f.nv || ic >= f.nv) return false;
+  for (int q = 0; q < 3; ++q) {
+    a[q] = f.v[3ull * ia + q];
+    b[q] = f.v[3ull * ib + q];
+    cc[q] = f.v[3ull * ic + q];
+  }
+  return true;
+}
+
 __global__ void k_flat_valid(FlatIn f, uint32_t* __restrict__ flag) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= f.candidates) return;
-  const uint32_t i = find_instance(f.prefix, f.ninst, c);
-  const unsigned long long k = c - f.prefix[i];
-  const unsigned long long base = (static_cast<unsigned long long>(f.inst[3 * i]) + k) * 3ull;
-  bool ok = base + 2ull < f.ni;
-  if (ok) ok = f.idx[base] < f.nv && f.idx[base + 1] < f.nv && f.idx[base + 2] < f.nv;
-  flag[c] = ok ? 1u : 0u;
+  uint32_t inst;
+  float a[3], b[3], cc[3];
+  flag[c] = flat_triangle(f, c, inst, a, b, cc) ? 1u : 0u;
 }
 
 __device__ __forceinline__ float min3(float a, float b, float c) {   // std::min({a, b, c})
@@ -218,13 +283,10 @@ __global__ void k_flat_write(FlatIn f, const uint32_t* __restrict__ flag, const 
                              float4* __restrict__ bhi, uint32_t* __restrict__ nonfinite) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= f.candidates || !flag[c]) return;
-  const uint32_t i = find_instance(f.prefix, f.ninst, c);
-  const unsigned long long k = c - f.prefix[i];
-  const unsigned long long base = (static_cast<unsigned long long>(f.inst[3 * i]) + k) * 3ull;
+  uint32_t i;
+  float a[3], b[3], cc[3];
+  flat_triangle(f, c, i, a, b, cc);
   const uint32_t mat = f.inst[3 * i + 2];
-  const float* a = f.v + 3ull * f.idx[base];
-  const float* b = f.v + 3ull * f.idx[base + 1];
-  const float* cc = f.v + 3ull * f.idx[base + 2];
   const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
   const float e2x = cc[0] - a[0], e2y = cc[1] - a[1], e2z = cc[2] - a[2];
   const float nx = e1y * e2z - e1z * e2y;
@@ -1209,10 +1271,11 @@ void FreeDeviceAccel(DeviceAccelOut& out) {
   out = DeviceAccelOut{};
 }
 
-cudaError_t BuildAccelOnDevice(const float* d_vertices, uint32_t vertex_count, const uint32_t* d_indices,
-                               uint32_t index_count, const uint32_t* instances, uint32_t instance_count, bool sah,
-                               cudaStream_t stream, DeviceAccelOut& out) {
+cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStream_t stream, DeviceAccelOut& out) {
   out = DeviceAccelOut{};
+  const uint32_t* instances = sc_in.instances;
+  const uint32_t instance_count = sc_in.instance_count;
+  const bool dyn = sc_in.instance_local && sc_in.instance_transforms;
   // Candidate triangles of every instance (the host path's loop bounds).
   std::vector<unsigned long long> prefix(instance_count + 1u, 0ull);
   for (uint32_t i = 0; i < instance_count; ++i) prefix[i + 1] = prefix[i] + instances[3 * i + 1];
@@ -1220,6 +1283,8 @@ cudaError_t BuildAccelOnDevice(const float* d_vertices, uint32_t vertex_count, c
   if (candidates >= (1ull << 31)) return cudaErrorInvalidValue;
   Scratch sc{stream};
   uint32_t* d_inst = sc.get<uint32_t>(3ull * instance_count);
+  uint32_t* d_inst_local = dyn ? sc.get<uint32_t>(5ull * instance_count) : nullptr;
+  float* d_inst_tr = dyn ? sc.get<float>(10ull * instance_count) : nullptr;
   unsigned long long* d_prefix = sc.get<unsigned long long>(instance_count + 1u);
   const uint32_t nc = static_cast<uint32_t>(candidates);
   uint32_t* flag = sc.get<uint32_t>(nc);
@@ -1227,9 +1292,16 @@ cudaError_t BuildAccelOnDevice(const float* d_vertices, uint32_t vertex_count, c
   uint32_t* nonfinite = sc.get<uint32_t>(1);
   if (sc.err != cudaSuccess) return sc.err;
   if (instance_count) BB_TRY(cudaMemcpyAsync(d_inst, instances, 12ull * instance_count, cudaMemcpyHostToDevice, stream));
+  if (dyn && instance_count) {
+    BB_TRY(cudaMemcpyAsync(d_inst_local, sc_in.instance_local, 20ull * instance_count, cudaMemcpyHostToDevice, stream));
+    BB_TRY(cudaMemcpyAsync(d_inst_tr, sc_in.instance_transforms, 40ull * instance_count, cudaMemcpyHostToDevice, stream));
+  }
   BB_TRY(cudaMemcpyAsync(d_prefix, prefix.data(), 8ull * (instance_count + 1u), cudaMemcpyHostToDevice, stream));
   BB_TRY(cudaMemsetAsync(nonfinite, 0, 4, stream));
-  const FlatIn f{d_vertices, vertex_count, d_indices, index_count, d_inst, d_prefix, instance_count, nc};
+  const FlatIn f{sc_in.vertices, sc_in.vertex_count, sc_in.indices, sc_in.index_count,
+                 sc_in.local_vertices, dyn ? sc_in.local_vertex_count : 0u,
+                 sc_in.local_indices, dyn ? sc_in.local_index_count : 0u,
+                 d_inst, d_inst_local, d_inst_tr, d_prefix, instance_count, nc};
   if (nc) k_flat_valid<<<grid_for(nc), kThreads, 0, stream>>>(f, flag);
   BB_TRY(exclusive_scan(flag, nc, pos, sc));
   uint32_t n = 0u;

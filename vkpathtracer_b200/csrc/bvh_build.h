@@ -30,13 +30,27 @@ struct DeviceAccelOut {
   bool fallback = false;       // non-finite primitive bounds: use the host builder instead
 };
 
-// Builds everything from the scene arrays: vertices and indices in device
-// memory, the instance table (first_triangle, triangle_count, material) on
-// the host.  sah: the traversal tree is a binned-SAH tree instead of the
-// reference tree.  Returns a CUDA error; on fallback, nothing is allocated.
-cudaError_t BuildAccelOnDevice(const float* d_vertices, uint32_t vertex_count, const uint32_t* d_indices,
-                               uint32_t index_count, const uint32_t* instances, uint32_t instance_count, bool sah,
-                               cudaStream_t stream, DeviceAccelOut& out);
+// The scene's geometry arrays: vertex and index arrays (global and local) in
+// device memory, the per-instance tables on the host.
+struct DeviceSceneArrays {
+  const float* vertices = nullptr;
+  uint32_t vertex_count = 0;
+  const uint32_t* indices = nullptr;
+  uint32_t index_count = 0;
+  const float* local_vertices = nullptr;      // dynamic instances (may be null)
+  uint32_t local_vertex_count = 0;
+  const uint32_t* local_indices = nullptr;
+  uint32_t local_index_count = 0;
+  const uint32_t* instances = nullptr;        // host: first_triangle, triangle_count, material
+  uint32_t instance_count = 0;
+  const uint32_t* instance_local = nullptr;   // host, 5 per instance (see InstanceGeometry), or null
+  const float* instance_transforms = nullptr; // host, 10 per instance, or null
+};
+
+// Builds everything from the scene arrays.  sah: the traversal tree is a
+// binned-SAH tree instead of the reference tree.  Returns a CUDA error; on
+// fallback, nothing is allocated.
+cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& scene, bool sah, cudaStream_t stream, DeviceAccelOut& out);
 
 void FreeDeviceAccel(DeviceAccelOut& out);
 

@@ -100,8 +100,33 @@ float surface_area(const BinNode& n) {
 
 }  // namespace
 
+void TransformInstanceVertex(const float* local, const float* tr, float out[3]) {
+  const float sx = local[0] * tr[7], sy = local[1] * tr[8], sz = local[2] * tr[9];
+  float rx = sx, ry = sy, rz = sz;
+  const float len_sq = tr[3] * tr[3] + tr[4] * tr[4] + tr[5] * tr[5] + tr[6] * tr[6];
+  if (!(len_sq <= kPad * kPad)) {
+    const float inv_len = 1.0f / std::sqrt(len_sq);
+    const float qx = tr[3] * inv_len, qy = tr[4] * inv_len, qz = tr[5] * inv_len;
+    const float qw = tr[6] * inv_len;
+    // t = 2 * cross(q, v); v + t * qw + cross(q, t)
+    const float tx = (qy * sz - qz * sy) * 2.0f;
+    const float ty = (qz * sx - qx * sz) * 2.0f;
+    const float tz = (qx * sy - qy * sx) * 2.0f;
+    const float cx = qy * tz - qz * ty;
+    const float cy = qz * tx - qx * tz;
+    const float cz = qx * ty - qy * tx;
+    rx = (sx + tx * qw) + cx;
+    ry = (sy + ty * qw) + cy;
+    rz = (sz + tz * qw) + cz;
+  }
+  out[0] = rx + tr[0];
+  out[1] = ry + tr[1];
+  out[2] = rz + tr[2];
+}
+
 bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* indices, uint32_t index_count,
-                  const uint32_t* instances, uint32_t instance_count, SceneGeometry& out, std::string& error) {
+                  const uint32_t* instances, uint32_t instance_count, SceneGeometry& out, std::string& error,
+                  const InstanceGeometry* dyn) {
   out.prims.clear();
   out.boxes.clear();
   if (instance_count > 0 && instances == nullptr) {
@@ -112,16 +137,44 @@ bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* 
   for (uint32_t i = 0; i < instance_count; ++i) capacity += instances[3 * i + 1];
   out.prims.reserve(capacity);
   out.boxes.reserve(6 * capacity);
+  const bool has_dyn = dyn && dyn->instance_local && dyn->instance_transforms;
   for (uint32_t i = 0; i < instance_count; ++i) {
     const uint32_t first = instances[3 * i], count = instances[3 * i + 1], mat = instances[3 * i + 2];
+    const uint32_t* loc = has_dyn ? dyn->instance_local + 5 * static_cast<size_t>(i) : nullptr;
+    const bool use_local = loc && (loc[0] & 1u) != 0u && loc[2] > 0u && loc[4] > 0u;
     for (uint32_t k = 0; k < count; ++k) {
-      const uint64_t base = (static_cast<uint64_t>(first) + k) * 3u;
-      if (base + 2u >= index_count) continue;
-      const uint32_t ia = indices[base], ib = indices[base + 1], ic = indices[base + 2];
-      if (ia >= vertex_count || ib >= vertex_count || ic >= vertex_count) continue;
-      const float* a = vertices + 3 * static_cast<size_t>(ia);
-      const float* b = vertices + 3 * static_cast<size_t>(ib);
-      const float* c = vertices + 3 * static_cast<size_t>(ic);
+      float la[3], lb[3], lc[3];
+      const float *a = nullptr, *b = nullptr, *c = nullptr;
+      if (use_local) {
+        // 32-bit index arithmetic, as the accelerator's
+        const uint32_t local_base = loc[3] + k * 3u;
+        const uint32_t local_end = loc[1] + loc[2];
+        // (a wrapped local_base + 2 would make the reference read out of range: skipped here)
+        if (local_base < 0xFFFFFFFEu && local_base + 2u < dyn->local_index_count) {
+          const uint32_t l0 = dyn->local_indices[local_base], l1 = dyn->local_indices[local_base + 1u],
+                         l2 = dyn->local_indices[local_base + 2u];
+          const uint32_t v0 = loc[1] + l0, v1 = loc[1] + l1, v2 = loc[1] + l2;
+          if (v0 < local_end && v1 < local_end && v2 < local_end && v0 < dyn->local_vertex_count &&
+              v1 < dyn->local_vertex_count && v2 < dyn->local_vertex_count) {
+            const float* tr = dyn->instance_transforms + 10 * static_cast<size_t>(i);
+            TransformInstanceVertex(dyn->local_vertices + 3 * static_cast<size_t>(v0), tr, la);
+            TransformInstanceVertex(dyn->local_vertices + 3 * static_cast<size_t>(v1), tr, lb);
+            TransformInstanceVertex(dyn->local_vertices + 3 * static_cast<size_t>(v2), tr, lc);
+            a = la;
+            b = lb;
+            c = lc;
+          }
+        }
+      }
+      if (!a) {
+        const uint32_t base = (first + k) * 3u;   // 32-bit, as the accelerator's
+        if (base >= 0xFFFFFFFEu || base + 2u >= index_count) continue;
+        const uint32_t ia = indices[base], ib = indices[base + 1u], ic = indices[base + 2u];
+        if (ia >= vertex_count || ib >= vertex_count || ic >= vertex_count) continue;
+        a = vertices + 3 * static_cast<size_t>(ia);
+        b = vertices + 3 * static_cast<size_t>(ib);
+        c = vertices + 3 * static_cast<size_t>(ic);
+      }
       HostPrim p;
       for (int ax = 0; ax < 3; ++ax) {
         p.v0[ax] = a[ax];

@@ -68,11 +68,27 @@ struct WideBvh {
   bool reference_topology = true;   // traversal tree == reference tree
 };
 
+// Dynamic-transform instances: local geometry and per-instance transforms
+// (all null when the scene has none).
+struct InstanceGeometry {
+  const uint32_t* instance_local = nullptr;       // 5 per instance: flags, local first/count vertex, first/count index
+  const float* instance_transforms = nullptr;     // 10 per instance: translation3, quaternion xyzw, scale3
+  const float* local_vertices = nullptr;
+  uint32_t local_vertex_count = 0;
+  const uint32_t* local_indices = nullptr;
+  uint32_t local_index_count = 0;
+};
+
+// A world-space vertex of a dynamic instance: scale, normalized-quaternion
+// rotation, translation (transform_instance_vertex and rotate_quat,
+// src/pathtracer/CpuBvhAccelerator.cpp:47-74).
+void TransformInstanceVertex(const float* local, const float* transform, float out[3]);
+
 // Flattens instances x triangles in the accelerator's order, skipping
 // triangles with out-of-range indices (src/pathtracer/CpuBvhAccelerator.cpp:173-247).
 bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* indices,
                   uint32_t index_count, const uint32_t* instances, uint32_t instance_count,
-                  SceneGeometry& out, std::string& error);
+                  SceneGeometry& out, std::string& error, const InstanceGeometry* dyn = nullptr);
 
 // Binary BVH: widest-centroid-axis midpoint split, stable partition,
 // count/2 fallback, leaves of <= leaf_threshold primitives, child ids

@@ -109,6 +109,11 @@ struct vkptc_ctx {
   DevBuf<uint32_t> d_raw_indices;
   uint32_t raw_vertex_count = 0, raw_index_count = 0;
   std::vector<uint32_t> raw_instances;
+  DevBuf<float> d_raw_local_vertices;     // dynamic instances (empty without)
+  DevBuf<uint32_t> d_raw_local_indices;
+  uint32_t raw_local_vertex_count = 0, raw_local_index_count = 0;
+  std::vector<uint32_t> raw_instance_local;
+  std::vector<float> raw_instance_transforms;
   uint32_t prim_count = 0;                // flattened primitives of the built accelerator
   std::vector<float> materials, lights;
   float env[3] = {0, 0, 0};
@@ -522,11 +527,24 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   cudaSetDevice(ctx->device);
   if (scene->instance_count > 0 && scene->instances == nullptr)
     return fail(ctx, VKPTC_INVALID_ARGUMENT, "instances pointer is null");
+  const bool dyn = scene->instance_local != nullptr && scene->instance_transforms != nullptr;
+  if ((scene->instance_local != nullptr) != (scene->instance_transforms != nullptr) ||
+      (dyn && ((scene->local_vertex_count && !scene->local_vertices) || (scene->local_index_count && !scene->local_indices))))
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "dynamic-instance array pointer is null");
+  InstanceGeometry ig;
+  if (dyn) {
+    ig.instance_local = scene->instance_local;
+    ig.instance_transforms = scene->instance_transforms;
+    ig.local_vertices = scene->local_vertices;
+    ig.local_vertex_count = scene->local_vertex_count;
+    ig.local_indices = scene->local_indices;
+    ig.local_index_count = scene->local_index_count;
+  }
   if (ctx->config.build_mode == VKPTC_BUILD_HOST) {
     std::string err;
     SceneGeometry geo;
     if (!FlattenScene(scene->vertices, scene->vertex_count, scene->indices, scene->index_count, scene->instances,
-                      scene->instance_count, geo, err)) {
+                      scene->instance_count, geo, err, dyn ? &ig : nullptr)) {
       return fail(ctx, VKPTC_INVALID_ARGUMENT, err);
     }
     ctx->geo = std::move(geo);
@@ -547,6 +565,26 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
       VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_raw_indices.ptr, scene->indices, 4ull * scene->index_count,
                                  cudaMemcpyHostToDevice), "scene upload");
     ctx->raw_instances.assign(scene->instances, scene->instances + 3 * static_cast<size_t>(scene->instance_count));
+    ctx->raw_instance_local.clear();
+    ctx->raw_instance_transforms.clear();
+    ctx->raw_local_vertex_count = ctx->raw_local_index_count = 0u;
+    ctx->d_raw_local_vertices.release();
+    ctx->d_raw_local_indices.release();
+    if (dyn) {
+      ctx->raw_instance_local.assign(scene->instance_local, scene->instance_local + 5 * static_cast<size_t>(scene->instance_count));
+      ctx->raw_instance_transforms.assign(scene->instance_transforms,
+                                          scene->instance_transforms + 10 * static_cast<size_t>(scene->instance_count));
+      ctx->raw_local_vertex_count = scene->local_vertex_count;
+      ctx->raw_local_index_count = scene->local_index_count;
+      VKPTC_CUDA(ctx, ctx->d_raw_local_vertices.alloc(std::max<size_t>(1, 3ull * scene->local_vertex_count)), "scene alloc");
+      VKPTC_CUDA(ctx, ctx->d_raw_local_indices.alloc(std::max<size_t>(1, scene->local_index_count)), "scene alloc");
+      if (scene->local_vertex_count)
+        VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_raw_local_vertices.ptr, scene->local_vertices, 12ull * scene->local_vertex_count,
+                                   cudaMemcpyHostToDevice), "scene upload");
+      if (scene->local_index_count)
+        VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_raw_local_indices.ptr, scene->local_indices, 4ull * scene->local_index_count,
+                                   cudaMemcpyHostToDevice), "scene upload");
+    }
     ctx->geo = SceneGeometry{};
     ctx->geo_ready = false;
   }
@@ -672,10 +710,26 @@ int32_t ensure_geo(vkptc_ctx* c) {
     VKPTC_CUDA(c, cudaMemcpy(v.data(), c->d_raw_vertices.ptr, v.size() * 4, cudaMemcpyDeviceToHost), "scene read");
   if (!idx.empty())
     VKPTC_CUDA(c, cudaMemcpy(idx.data(), c->d_raw_indices.ptr, idx.size() * 4, cudaMemcpyDeviceToHost), "scene read");
+  std::vector<float> lv(3ull * c->raw_local_vertex_count);
+  std::vector<uint32_t> li(c->raw_local_index_count);
+  if (!lv.empty())
+    VKPTC_CUDA(c, cudaMemcpy(lv.data(), c->d_raw_local_vertices.ptr, lv.size() * 4, cudaMemcpyDeviceToHost), "scene read");
+  if (!li.empty())
+    VKPTC_CUDA(c, cudaMemcpy(li.data(), c->d_raw_local_indices.ptr, li.size() * 4, cudaMemcpyDeviceToHost), "scene read");
+  InstanceGeometry ig;
+  const bool dyn = !c->raw_instance_local.empty();
+  if (dyn) {
+    ig.instance_local = c->raw_instance_local.data();
+    ig.instance_transforms = c->raw_instance_transforms.data();
+    ig.local_vertices = lv.data();
+    ig.local_vertex_count = c->raw_local_vertex_count;
+    ig.local_indices = li.data();
+    ig.local_index_count = c->raw_local_index_count;
+  }
   std::string err;
   SceneGeometry geo;
   if (!FlattenScene(v.data(), c->raw_vertex_count, idx.data(), c->raw_index_count, c->raw_instances.data(),
-                    static_cast<uint32_t>(c->raw_instances.size() / 3), geo, err)) {
+                    static_cast<uint32_t>(c->raw_instances.size() / 3), geo, err, dyn ? &ig : nullptr)) {
     return fail(c, VKPTC_INVALID_ARGUMENT, err);
   }
   c->geo = std::move(geo);
@@ -690,9 +744,22 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
   *done = false;
   const auto t0 = std::chrono::steady_clock::now();
   DeviceAccelOut out;
-  const cudaError_t e = BuildAccelOnDevice(
-      c->d_raw_vertices.ptr, c->raw_vertex_count, c->d_raw_indices.ptr, c->raw_index_count, c->raw_instances.data(),
-      static_cast<uint32_t>(c->raw_instances.size() / 3), c->config.bvh_mode == VKPTC_BVH_SAH, c->stream, out);
+  DeviceSceneArrays a;
+  a.vertices = c->d_raw_vertices.ptr;
+  a.vertex_count = c->raw_vertex_count;
+  a.indices = c->d_raw_indices.ptr;
+  a.index_count = c->raw_index_count;
+  a.instances = c->raw_instances.data();
+  a.instance_count = static_cast<uint32_t>(c->raw_instances.size() / 3);
+  if (!c->raw_instance_local.empty()) {
+    a.local_vertices = c->d_raw_local_vertices.ptr;
+    a.local_vertex_count = c->raw_local_vertex_count;
+    a.local_indices = c->d_raw_local_indices.ptr;
+    a.local_index_count = c->raw_local_index_count;
+    a.instance_local = c->raw_instance_local.data();
+    a.instance_transforms = c->raw_instance_transforms.data();
+  }
+  const cudaError_t e = BuildAccelOnDevice(a, c->config.bvh_mode == VKPTC_BVH_SAH, c->stream, out);
   if (e != cudaSuccess) {
     FreeDeviceAccel(out);
     return cuda_fail(c, e, "device BVH build");
@@ -787,8 +854,18 @@ int32_t vkptc_build_binary_bvh(const vkptc_scene_view* scene, uint32_t* nodes_ou
   if (!scene || !nodes_out || !node_count || !prim_out || !prim_count) return VKPTC_INVALID_ARGUMENT;
   SceneGeometry geo;
   std::string err;
+  InstanceGeometry ig;
+  const bool dyn = scene->instance_local != nullptr && scene->instance_transforms != nullptr;
+  if (dyn) {
+    ig.instance_local = scene->instance_local;
+    ig.instance_transforms = scene->instance_transforms;
+    ig.local_vertices = scene->local_vertices;
+    ig.local_vertex_count = scene->local_vertex_count;
+    ig.local_indices = scene->local_indices;
+    ig.local_index_count = scene->local_index_count;
+  }
   if (!FlattenScene(scene->vertices, scene->vertex_count, scene->indices, scene->index_count, scene->instances,
-                    scene->instance_count, geo, err)) {
+                    scene->instance_count, geo, err, dyn ? &ig : nullptr)) {
     return VKPTC_INVALID_ARGUMENT;
   }
   std::vector<BinNode> bin;
@@ -875,6 +952,10 @@ int32_t vkptc_shutdown(vkptc_ctx* ctx) {
   ctx->d_raw_vertices.release();
   ctx->d_raw_indices.release();
   ctx->raw_instances.clear();
+  ctx->d_raw_local_vertices.release();
+  ctx->d_raw_local_indices.release();
+  ctx->raw_instance_local.clear();
+  ctx->raw_instance_transforms.clear();
   ctx->prim_count = 0;
   ctx->wide = WideBvh{};
   ctx->d_nodes.release();

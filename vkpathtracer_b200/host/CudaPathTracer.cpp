@@ -73,13 +73,6 @@ Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
 
 Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& scene) {
   if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
-  for (const auto& inst : scene.instances) {
-    if (inst.has_flag(pt::kRTInstanceFlagDynamicTransform) && inst.local_vertex_count > 0u &&
-        inst.local_index_count > 0u) {
-      fail("dynamic-transform instances with local geometry are not supported by the cuda backend yet");
-      return Status::error(StatusCode::Unsupported, m_last_error);
-    }
-  }
   // Standard GPU word maps (src/gpu/VulkanGpuPathTracer.cpp:323-338, 381-396).
   std::vector<float> mats(16 * scene.materials.size(), 0.0f);
   for (size_t i = 0; i < scene.materials.size(); ++i) {
@@ -104,10 +97,22 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
     w[11] = l.spot_inner_cos; w[12] = l.spot_outer_cos;
   }
   std::vector<uint32_t> inst(3 * scene.instances.size());
+  std::vector<uint32_t> inst_local(5 * scene.instances.size());
+  std::vector<float> inst_tr(10 * scene.instances.size());
+  bool dynamic = false;
   for (size_t i = 0; i < scene.instances.size(); ++i) {
-    inst[3 * i + 0] = scene.instances[i].first_triangle;
-    inst[3 * i + 1] = scene.instances[i].triangle_count;
-    inst[3 * i + 2] = scene.instances[i].material_index;
+    const pt::RTInstance& r = scene.instances[i];
+    inst[3 * i + 0] = r.first_triangle;
+    inst[3 * i + 1] = r.triangle_count;
+    inst[3 * i + 2] = r.material_index;
+    // dynamic-transform instances: local geometry and transform (RTInstance field order)
+    const uint32_t l[5] = {r.flags, r.local_first_vertex, r.local_vertex_count, r.local_first_index,
+                           r.local_index_count};
+    const float t[10] = {r.translation.x, r.translation.y, r.translation.z, r.rotation.x, r.rotation.y,
+                         r.rotation.z, r.rotation.w, r.scale.x, r.scale.y, r.scale.z};
+    std::copy(l, l + 5, inst_local.begin() + 5 * i);
+    std::copy(t, t + 10, inst_tr.begin() + 10 * i);
+    dynamic = dynamic || r.has_flag(pt::kRTInstanceFlagDynamicTransform);
   }
   vkptc_scene_view v{};
   v.vertices = reinterpret_cast<const float*>(scene.vertices.data());   // Vec3 is three packed floats
@@ -158,6 +163,14 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
   }
   v.sdf_primitives = sdf.empty() ? nullptr : sdf.data();
   v.sdf_count = static_cast<uint32_t>(scene.sdf_primitives.size());
+  if (dynamic) {
+    v.instance_local = inst_local.data();
+    v.instance_transforms = inst_tr.data();
+    v.local_vertices = reinterpret_cast<const float*>(scene.local_vertices.data());   // packed Vec3
+    v.local_vertex_count = static_cast<uint32_t>(scene.local_vertices.size());
+    v.local_indices = scene.local_indices.data();
+    v.local_index_count = static_cast<uint32_t>(scene.local_indices.size());
+  }
   const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
   if (st) m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
   return st;

@@ -53,7 +53,10 @@ class SceneView(ctypes.Structure):
                 ("camera_focus_distance", ctypes.c_float), ("environment_map", ctypes.c_void_p),
                 ("environment_map_width", ctypes.c_uint32), ("environment_map_height", ctypes.c_uint32),
                 ("environment_map_scale", ctypes.c_float * 3),
-                ("sdf_primitives", ctypes.c_void_p), ("sdf_count", ctypes.c_uint32)]
+                ("sdf_primitives", ctypes.c_void_p), ("sdf_count", ctypes.c_uint32),
+                ("instance_local", ctypes.c_void_p), ("instance_transforms", ctypes.c_void_p),
+                ("local_vertices", ctypes.c_void_p), ("local_vertex_count", ctypes.c_uint32),
+                ("local_indices", ctypes.c_void_p), ("local_index_count", ctypes.c_uint32)]
 
 # vkptc_sdf_shape
 SDF_SPHERE, SDF_BOX, SDF_ROUNDED_BOX, SDF_PLANE, SDF_TORUS, SDF_CAPSULE = range(6)

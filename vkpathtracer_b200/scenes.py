@@ -102,6 +102,11 @@ class Scene:
     env_map: Optional[np.ndarray] = None   # (H, W, 3) float32 equirectangular map, row 0 toward +y
     env_scale: tuple = (0.0, 0.0, 0.0)     # texel multiplier (all <= 1e-6 means 1)
     sdf: Optional[np.ndarray] = None       # (N, 16) float32 SDF primitive records (sdf_primitive)
+    # dynamic-transform instances (all None when the scene has none)
+    instance_local: Optional[np.ndarray] = None        # (I, 5) uint32: flags, local first/count vertex, first/count index
+    instance_transforms: Optional[np.ndarray] = None   # (I, 10) float32: translation3, quaternion xyzw, scale3
+    local_vertices: Optional[np.ndarray] = None        # (V', 3) float32
+    local_indices: Optional[np.ndarray] = None         # (K,) uint32
 
     @property
     def triangle_count(self) -> int:
@@ -290,6 +295,49 @@ def effect_gallery(seed: int = 11) -> Scene:
     v, t, inst = b.arrays()
     cam = Camera(position=(0.0, 0.5, 1.9), target=(0.0, 0.3, 0.0), up=(0.0, 1.0, 0.0), fov_deg=40.0)
     return Scene(v, t, inst, np.array(mats), np.array(lights), (0.02, 0.02, 0.03), cam, "effect_gallery").contiguous()
+
+
+def load_snapshot_dump(path: str, name: str = "") -> Scene:
+    """A PathTracerSceneSnapshot written by the reference oracle's scene
+    converter (vko_convert_scene_json: SceneDocument -> BuildSceneDataFromDocument),
+    layout documented in oracle/ref_shim.cpp."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:4] != b"VKSJ":
+        raise ValueError("not a snapshot dump")
+    head = np.frombuffer(data, np.uint32, 11, 4)
+    if int(head[0]) != 1:
+        raise ValueError("unknown snapshot dump version")
+    nv, ni, ninst, nmat, nlight, nsdf, nlv, nli, ew, eh = (int(x) for x in head[1:])
+    off = 48
+
+    def take(dtype, n):
+        nonlocal off
+        a = np.frombuffer(data, dtype, n, off).copy()
+        off += 4 * n
+        return a
+
+    vertices = take(np.float32, 3 * nv).reshape(-1, 3)
+    indices = take(np.uint32, ni)
+    instances = take(np.uint32, 3 * ninst).reshape(-1, 3)
+    instance_local = take(np.uint32, 5 * ninst).reshape(-1, 5)
+    instance_transforms = take(np.float32, 10 * ninst).reshape(-1, 10)
+    materials = take(np.float32, 16 * nmat).reshape(-1, 16)
+    lights = take(np.float32, 16 * nlight).reshape(-1, 16)
+    sdf = take(np.float32, 16 * nsdf).reshape(-1, 16)
+    local_vertices = take(np.float32, 3 * nlv).reshape(-1, 3)
+    local_indices = take(np.uint32, nli)
+    env = take(np.float32, 3)
+    cam = take(np.float32, 12).astype(np.float64)
+    env_scale = take(np.float32, 3)
+    env_map = take(np.float32, 3 * ew * eh).reshape(eh, ew, 3) if ew * eh else None
+    camera = Camera(tuple(cam[0:3]), tuple(cam[3:6]), tuple(cam[6:9]), float(cam[9]), float(cam[10]), float(cam[11]))
+    # trailing partial triangles are ignored by the accelerator (index checks), so keep the flat array
+    return Scene(vertices, indices.reshape(-1, 3) if ni % 3 == 0 else indices, instances, materials, lights,
+                 tuple(float(x) for x in env), camera, name or "snapshot", env_map=env_map,
+                 env_scale=tuple(float(x) for x in env_scale), sdf=sdf if nsdf else None,
+                 instance_local=instance_local, instance_transforms=instance_transforms,
+                 local_vertices=local_vertices, local_indices=local_indices).contiguous()
 
 
 SDF_SHAPES = {"sphere": 0, "box": 1, "rounded_box": 2, "plane": 3, "torus": 4, "capsule": 5}

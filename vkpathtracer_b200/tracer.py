@@ -108,6 +108,15 @@ def scene_view(scene: Scene):
         sdf = np.ascontiguousarray(scene.sdf, np.float32).reshape(-1, 16)
         keep = keep + (sdf,)
         v.sdf_primitives, v.sdf_count = _ptr(sdf), sdf.shape[0]
+    if scene.instance_local is not None:
+        il = np.ascontiguousarray(scene.instance_local, np.uint32).reshape(-1, 5)
+        it = np.ascontiguousarray(scene.instance_transforms, np.float32).reshape(-1, 10)
+        lv = np.ascontiguousarray(scene.local_vertices, np.float32).reshape(-1, 3)
+        li = np.ascontiguousarray(scene.local_indices, np.uint32).reshape(-1)
+        keep = keep + (il, it, lv, li)
+        v.instance_local, v.instance_transforms = _ptr(il), _ptr(it)
+        v.local_vertices, v.local_vertex_count = (_ptr(lv) if lv.size else None), lv.shape[0]
+        v.local_indices, v.local_index_count = (_ptr(li) if li.size else None), li.size
     return v, keep
 
 
