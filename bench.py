@@ -328,6 +328,39 @@ def bvh_build(device, cpu: bool = True):
     return out
 
 
+def film_resolve(device, cpu: bool = True):
+    """LDR resolve of a 1920x1080 film (ACES, gamma): the device resolve with
+    the image read back to the host (what IPathTracer::resolve_ldr returns),
+    against the reference's ApplyFilmResolve of the same HDR film on one
+    host thread."""
+    from vkpathtracer_b200.tracer import CudaPathTracer
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.RenderSettings(width=1920, height=1080, spp=2, max_depth=6, seed=3)
+    out = {"workload": "film_1920x1080_aces_gamma"}
+    with CudaPathTracer(device=device) as t:
+        t.configure(st)
+        t.load_scene_snapshot(sc)
+        t.build_or_update_acceleration()
+        t.render_frame(0, st.spp)
+        t.resolve_ldr(tone_map="aces")
+        ms = []
+        for _ in range(10):
+            t0 = time.perf_counter()
+            t.resolve_ldr(tone_map="aces")
+            ms.append(1e3 * (time.perf_counter() - t0))
+        out["device_resolve_ldr_ms"] = float(np.median(ms))
+        if cpu:
+            import oracle
+            kind = "reference" if oracle.have_reference() else "port"
+            hdr = t.resolve_hdr().reshape(st.height, st.width, 3)
+            o = oracle.load(kind)
+            t0 = time.perf_counter()
+            o.apply_film_resolve(hdr, tone_map="aces")
+            out["cpu_baseline"] = {"value": 1e3 * (time.perf_counter() - t0), "unit": "ms", "cores": 1, "kind": kind,
+                                   "sample": "ApplyFilmResolve of the full film (HDR already on the host)"}
+    return out
+
+
 def ray_query(device):
     import torch
     from vkpathtracer_b200.tracer import CudaPathTracer
@@ -567,7 +600,7 @@ def run_ours(args, world, rank, local):
         ms = min(b.run(m, **mt)["device_ms"] for _ in range(2))
         drivers[m] = {"paths_per_s": total_paths / (ms / 1e3), "tuning": mt}
 
-    roof = rq = ff = cpu = inv = sdf = bb = None
+    roof = rq = ff = cpu = inv = sdf = bb = fr = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the dominant kernel
         # traversal work counted in a stats run (same rays: the traversal is deterministic)
@@ -617,6 +650,7 @@ def run_ours(args, world, rank, local):
         inv = None if args.no_adjoint else inverse_rendering(local)
         sdf = None if args.no_sdf else sdf_scene(local, 0.0 if (args.no_cpu or world > 1) else 5.0)
         bb = None if args.no_build else bvh_build(local, cpu=not args.no_cpu and world == 1)
+        fr = film_resolve(local, cpu=not args.no_cpu and world == 1)
         if world == 1 and not args.no_cpu:
             import oracle
             kind = "reference" if oracle.have_reference() else "port"
@@ -641,7 +675,8 @@ def run_ours(args, world, rank, local):
                 "plain_kernel_launches": plain["kernel_launches"],
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
-                "inverse_rendering": inv, "sdf_scene": sdf, "bvh_build": bb, "cpu_baseline": cpu}
+                "inverse_rendering": inv, "sdf_scene": sdf, "bvh_build": bb, "film_resolve": fr,
+                "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     b.close()
 

@@ -292,6 +292,44 @@ int32_t vkptc_read_stage_times(vkptc_ctx* ctx, double* ms_out, uint64_t* launche
 int32_t vkptc_read_film(vkptc_ctx* ctx, float* sum_rgb, uint32_t* count, float* invalid);
 /* replaces IPathTracer::resolve_hdr / FilmBuffer::resolve_hdr (src/pathtracer/FilmBuffer.cpp:160-214) */
 int32_t vkptc_resolve_hdr(vkptc_ctx* ctx, float* rgb);
+
+/* Mirrors FilmResolveSettings (src/pathtracer/PathTracer.h:55-74), with the
+ * camera's exposure controls already folded into exposure as
+ * CameraAdjustedFilmResolveSettings does (src/pathtracer/FilmBuffer.cpp:226-251). */
+typedef struct vkptc_film_resolve {
+  float exposure;
+  float white_balance_kelvin;  /* 6500: no change */
+  uint32_t tone_map;           /* vkptc_tone_map */
+  uint32_t output_transform;   /* vkptc_output_transform */
+  float gamma;
+  uint32_t clamp_output;
+} vkptc_film_resolve;
+typedef enum vkptc_tone_map {
+  VKPTC_TONEMAP_LINEAR = 0,
+  VKPTC_TONEMAP_REINHARD = 1,
+  VKPTC_TONEMAP_FILMIC = 2,
+  VKPTC_TONEMAP_ACES = 3
+} vkptc_tone_map;
+typedef enum vkptc_output_transform { VKPTC_OUTPUT_GAMMA = 0, VKPTC_OUTPUT_LINEAR = 1 } vkptc_output_transform;
+typedef enum vkptc_readback_state {
+  VKPTC_READBACK_INVALID = 0,
+  VKPTC_READBACK_PENDING = 1,
+  VKPTC_READBACK_READY = 2,
+  VKPTC_READBACK_FAILED = 3
+} vkptc_readback_state;
+
+/* replaces IPathTracer::resolve_ldr, i.e. ApplyFilmResolve(resolve_hdr())
+ * (src/pathtracer/FilmBuffer.cpp:253-325), computed on the device: per-pixel
+ * mean, exposure, white balance, tone map, gamma, clamp, 8-bit quantization.
+ * rgba: 4*W*H bytes (alpha 255). */
+int32_t vkptc_resolve_ldr(vkptc_ctx* ctx, const vkptc_film_resolve* settings, uint8_t* rgba);
+/* replaces IPathTracer::request_film_readback (src/pathtracer/PathTracer.h:1173): enqueues the
+ * LDR resolve of the film as it stands after the work already submitted and a copy to
+ * pinned host memory on the context's stream; *token identifies it (the latest only). */
+int32_t vkptc_request_ldr_readback(vkptc_ctx* ctx, const vkptc_film_resolve* settings, uint64_t* token);
+/* replaces IPathTracer::poll_film (src/pathtracer/PathTracer.h:1174): *state receives a
+ * vkptc_readback_state; READY copies the image into rgba (4*W*H bytes). Never blocks. */
+int32_t vkptc_poll_ldr_readback(vkptc_ctx* ctx, uint64_t token, uint8_t* rgba, uint32_t* state);
 /* replaces IPathTracer::replace_film_history (src/pathtracer/PathTracer.h:1099):
  * loads a saved film (resume = reload the film, continue at the next sample). */
 int32_t vkptc_write_film(vkptc_ctx* ctx, const float* sum_rgb, const uint32_t* count, const float* invalid);

@@ -209,6 +209,24 @@ class Oracle:
         return {"sum": film, "count": count, "invalid": invalid, "samples": samples,
                 "counters": ctr.as_dict()}
 
+    def apply_film_resolve(self, hdr: np.ndarray, exposure: float = 1.0, white_balance_kelvin: float = 6500.0,
+                           tone_map: str = "linear", output_transform: str = "gamma", gamma: float = 2.2,
+                           clamp_output: bool = True) -> np.ndarray:
+        """ApplyFilmResolve of an (H, W, 3) HDR film -> (H, W, 4) uint8."""
+        hdr = np.ascontiguousarray(hdr, np.float32)
+        h, w = hdr.shape[0], hdr.shape[1]
+
+        class Resolve(ctypes.Structure):
+            _fields_ = [("exposure", ctypes.c_float), ("white_balance_kelvin", ctypes.c_float),
+                        ("tone_map", ctypes.c_uint32), ("output_transform", ctypes.c_uint32),
+                        ("gamma", ctypes.c_float), ("clamp_output", ctypes.c_uint32)]
+        rs = Resolve(exposure, white_balance_kelvin, {"linear": 0, "reinhard": 1, "filmic": 2, "aces": 3}[tone_map],
+                     {"gamma": 0, "linear": 1}[output_transform], gamma, int(clamp_output))
+        out = np.zeros((h, w, 4), np.uint8)
+        self.lib.vko_apply_film_resolve.restype = ctypes.c_int
+        self._check(self.lib.vko_apply_film_resolve(_ptr(hdr), w, h, ctypes.byref(rs), _ptr(out)))
+        return out
+
     def convert_scene_json(self, path: str):
         """Reference only: a scene document converted by the reference's own
         SceneDocument loader and BuildSceneDataFromDocument, as a Scene."""

@@ -28,6 +28,8 @@
 //     intersect_sphere, the march   src/pathtracer/ScalarCpuPathTracer.cpp:855-930
 //     nearest-hit reduction         src/pathtracer/ScalarCpuPathTracer.Intersect.cpp:91-129
 //   dynamic-instance flattening     src/pathtracer/CpuBvhAccelerator.cpp:47-74, 173-247
+//   ApplyFilmResolve, WhiteBalanceScale, ColorTemperatureToRgb
+//                                   src/pathtracer/FilmBuffer.cpp:30-49, 216-224, 253-325
 
 #include "vkpt_oracle.h"
 
@@ -1089,6 +1091,56 @@ int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t fi
       counters->sdf_misses += stats[t].sdf_misses;
     }
     counters->render_ms = ms;
+  }
+  return 0;
+}
+
+static void temperature_rgb(float kelvin, float rgb[3]) {
+  const float t = std::clamp(kelvin, 1000.0f, 40000.0f) / 100.0f;
+  if (t <= 66.0f) {
+    rgb[0] = 1.0f;
+    rgb[1] = std::clamp(0.39008158f * std::log(std::max(1.0f, t)) - 0.63184144f, 0.0f, 1.0f);
+    rgb[2] = t <= 19.0f ? 0.0f
+                        : std::clamp(0.5432068f * std::log(std::max(1.0f, t - 10.0f)) - 1.1962541f, 0.0f, 1.0f);
+  } else {
+    rgb[0] = std::clamp(1.2929362f * std::pow(t - 60.0f, -0.13320476f), 0.0f, 1.0f);
+    rgb[1] = std::clamp(1.1298909f * std::pow(t - 60.0f, -0.075514846f), 0.0f, 1.0f);
+    rgb[2] = 1.0f;
+  }
+}
+
+int vko_apply_film_resolve(const float* hdr, uint32_t width, uint32_t height, const vko_resolve* s, uint8_t* rgba) {
+  if (!hdr || !s || !rgba) return fail("null argument");
+  float d65[3], target[3], wb[3];
+  temperature_rgb(6500.0f, d65);
+  temperature_rgb(s->white_balance_kelvin, target);
+  for (int k = 0; k < 3; ++k) wb[k] = d65[k] / std::max(1.0e-3f, target[k]);
+  const float inv_gamma = 1.0f / std::max(0.01f, s->gamma);
+  auto tonemap = [&](float x) -> float {
+    switch (s->tone_map) {
+      case 1u: return x / (1.0f + x);
+      case 2u: {
+        auto F = [](float v) {
+          const float A = 0.15f, B = 0.50f, C = 0.10f, D = 0.20f, E = 0.02f, Fc = 0.30f;
+          return ((v * (A * v + C * B) + D * E) / (v * (A * v + B) + D * Fc)) - E / Fc;
+        };
+        return F(x) / F(11.2f);
+      }
+      case 3u: return (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+      default: return x;
+    }
+  };
+  const size_t n = static_cast<size_t>(width) * height;
+  for (size_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      float x = hdr[3 * i + k] * s->exposure * wb[k];
+      if (!std::isfinite(x)) x = 0.0f;
+      x = tonemap(x);
+      if (s->output_transform == 0u) x = std::pow(std::max(0.0f, x), inv_gamma);
+      if (s->clamp_output) x = std::min(1.0f, std::max(0.0f, x));
+      rgba[4 * i + k] = static_cast<uint8_t>(x * 255.0f + 0.5f);
+    }
+    rgba[4 * i + 3] = 255u;
   }
   return 0;
 }

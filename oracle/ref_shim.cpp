@@ -249,6 +249,26 @@ extern "C" {
 
 const char* vko_last_error(void) { return g_error.c_str(); }
 
+int vko_apply_film_resolve(const float* hdr_rgb, uint32_t width, uint32_t height, const vko_resolve* s,
+                           uint8_t* rgba) {
+  if (!hdr_rgb || !s || !rgba) return fail("null argument");
+  pt::FilmHdr hdr;
+  hdr.width = width;
+  hdr.height = height;
+  hdr.rgbf.assign(hdr_rgb, hdr_rgb + 3ull * width * height);
+  pt::FilmResolveSettings rs;
+  rs.exposure = s->exposure;
+  rs.white_balance_kelvin = s->white_balance_kelvin;
+  rs.tone_map = static_cast<pt::ToneMapMode>(s->tone_map);
+  rs.output_transform = static_cast<pt::OutputTransformMode>(s->output_transform);
+  rs.gamma = s->gamma;
+  rs.clamp_output = s->clamp_output != 0;
+  const pt::FilmLdr ldr = pt::ApplyFilmResolve(hdr, rs);
+  if (ldr.rgba8.size() != 4ull * width * height) return fail("resolve size");
+  std::memcpy(rgba, ldr.rgba8.data(), ldr.rgba8.size());
+  return 0;
+}
+
 // Snapshot dump of a converted scene document, little-endian:
 //   char[4] "VKSJ", u32 version (1)
 //   u32 nv, ni, ninst, nmat, nlight, nsdf, nlv, nli, env_w, env_h

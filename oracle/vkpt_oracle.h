@@ -137,6 +137,21 @@ int vko_intersect(const vko_scene* scene, const float* rays, uint64_t ray_count,
                   uint32_t threads, uint32_t* prim_out, float* t_out,
                   uint64_t* stats, double* elapsed_ms);
 
+/* FilmResolveSettings (src/pathtracer/PathTracer.h:55-74). */
+typedef struct vko_resolve {
+  float exposure;
+  float white_balance_kelvin;
+  uint32_t tone_map;          /* 0 linear, 1 reinhard, 2 filmic approx, 3 aces approx */
+  uint32_t output_transform;  /* 0 gamma, 1 linear */
+  float gamma;
+  uint32_t clamp_output;
+} vko_resolve;
+
+/* ApplyFilmResolve (src/pathtracer/FilmBuffer.cpp:253-325) of an HDR film
+ * (3*W*H floats) into rgba (4*W*H bytes). */
+int vko_apply_film_resolve(const float* hdr_rgb, uint32_t width, uint32_t height, const vko_resolve* settings,
+                           uint8_t* rgba);
+
 /* Reference only (oracle/_ref): loads a scene document (SceneDocument::
  * load_from_file, validate) and converts it with BuildSceneDataFromDocument
  * (src/pathtracer/SceneConversion.cpp), then writes the snapshot's arrays to

@@ -9,6 +9,7 @@
 //            (the scene document loaded and converted by the reference's own
 //             SceneDocument::load_from_file and BuildSceneDataFromDocument, as
 //             ptbench does, src/benchmark/BenchmarkRuntime.cpp:491-596)
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -245,7 +246,30 @@ int main(int argc, char** argv) {
   const auto hdr_a = ref.resolve_hdr(), hdr_b = gpu.resolve_hdr();
   check(hdr_a.width == hdr_b.width && hdr_a.rgbf.size() == hdr_b.rgbf.size(), "resolve_hdr shape");
   const auto ldr = gpu.resolve_ldr();
-  check(ldr.rgba8.size() == 4u * st.width * st.height, "resolve_ldr through the reference's ApplyFilmResolve");
+  check(ldr.rgba8.size() == 4u * st.width * st.height, "resolve_ldr size");
+  // the device tone map against the reference's ApplyFilmResolve of the same HDR film
+  const auto ref_ldr = pt::ApplyFilmResolve(gpu.resolve_hdr(), gpu.film().resolve_settings());
+  size_t ldr_same = 0, ldr_max = 0;
+  for (size_t i = 0; i < ldr.rgba8.size() && i < ref_ldr.rgba8.size(); ++i) {
+    const int d = std::abs(static_cast<int>(ldr.rgba8[i]) - static_cast<int>(ref_ldr.rgba8[i]));
+    ldr_same += d == 0 ? 1u : 0u;
+    ldr_max = std::max<size_t>(ldr_max, static_cast<size_t>(d));
+  }
+  std::printf("ldr bytes identical %.5f max step %zu\n", double(ldr_same) / std::max<size_t>(1, ldr.rgba8.size()), ldr_max);
+  check(ref_ldr.rgba8.size() == ldr.rgba8.size() && ldr_max <= 1u && ldr_same * 1000u >= 999u * ldr.rgba8.size(),
+        "device resolve_ldr equals ApplyFilmResolve of the device HDR film (<= 1 step on < 0.1 % of bytes)");
+  // split film readback: request, then poll until ready (bounded)
+  const auto token = gpu.request_film_readback();
+  check(static_cast<bool>(token), "request_film_readback");
+  pt::FilmReadbackResult rb;
+  for (int k = 0; k < 1000000; ++k) {
+    rb = gpu.poll_film(token);
+    if (rb.state != pt::FilmReadbackState::Pending) break;
+  }
+  check(rb.ready() && rb.ldr.rgba8 == ldr.rgba8, "poll_film returns the resolved film");
+  pt::FilmReadbackToken stale = token;
+  stale.id += 1000;
+  check(gpu.poll_film(stale).state == pt::FilmReadbackState::Invalid, "poll_film rejects an unknown token");
   // reset keeps the acceleration structure; the film starts over
   check(gpu.reset_accumulation() && gpu.status().accel_valid && gpu.read_counters().samples == 0, "reset is film-only");
   // tiles = full frame (CheckScalarRenderTilePrimitive, tests/snapshot_bus_smoke.cpp:1368-1435)

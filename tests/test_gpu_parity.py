@@ -405,3 +405,45 @@ def test_sah_traversal_tree_renders_identical_films():
             fa, ca, _ = a.film()
             fb, cb, _ = b.film()
         assert np.array_equal(ca, cb) and np.array_equal(bits(fa), bits(fb))
+
+
+RESOLVES = [dict(), dict(tone_map="reinhard", exposure=1.7), dict(tone_map="filmic", white_balance_kelvin=3200.0),
+            dict(tone_map="aces", output_transform="linear"), dict(tone_map="linear", clamp_output=False, gamma=1.8,
+                                                                   white_balance_kelvin=9000.0)]
+
+
+def test_device_ldr_resolve_matches_apply_film_resolve():
+    """resolve_ldr on the device against the reference's ApplyFilmResolve of
+    the same HDR film (the film's per-pixel mean): equal bytes except where
+    gamma's pow lands on a rounding boundary (at most one step)."""
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(96, 64, 3)
+    o = oracle.load("auto")
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp)
+        hdr = t.resolve_hdr().reshape(st.height, st.width, 3)
+        for kw in RESOLVES:
+            g = t.resolve_ldr(**kw)
+            r = o.apply_film_resolve(hdr, **kw)
+            d = np.abs(g.astype(np.int32) - r.astype(np.int32))
+            print(kw, "identical", float(np.mean(d == 0)), "max", int(d.max()))
+            assert d.max() <= 1 and np.mean(d == 0) >= 0.999, kw
+
+
+def test_split_film_readback():
+    """request_film_readback / poll_film: pending until the GPU work behind the
+    token is done, then the resolved image; an unknown token is invalid."""
+    import time
+    sc = scenes.cornell_box(seed=1)
+    st = scenes.cornell_settings(256, 192, 8)
+    with make_tracer(sc, st) as t:
+        t.render_frame(0, st.spp, sync=False)
+        tok = t.request_film_readback(tone_map="aces")
+        deadline = time.time() + 30.0
+        state, img = t.poll_film(tok)
+        while state == native.READBACK_PENDING and time.time() < deadline:
+            time.sleep(0.001)
+            state, img = t.poll_film(tok)
+        assert state == native.READBACK_READY
+        assert np.array_equal(img, t.resolve_ldr(tone_map="aces"))
+        assert t.poll_film(tok + 7)[0] == native.READBACK_INVALID

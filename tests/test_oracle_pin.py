@@ -214,3 +214,21 @@ def test_port_film_matches_reference_scene_documents(port, name):
     assert np.array_equal(got, d["counters"])
     sdf = np.array([c["sdf_tests"], c["sdf_steps"], c["sdf_hits"], c["sdf_misses"]], np.uint64)
     assert np.array_equal(sdf, d["sdf_counters"])
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
+def test_port_film_resolve_matches_reference(port):
+    """ApplyFilmResolve: exposure, white balance (ColorTemperatureToRgb), every
+    tone map, gamma and linear output, with and without the clamp; NaN and
+    infinite pixels."""
+    ref = oracle.load("reference")
+    rs = np.random.RandomState(0)
+    hdr = (rs.exponential(0.7, (48, 64, 3)) * (rs.rand(48, 64, 1) < 0.98)).astype(np.float32)
+    hdr[3, 5, 1], hdr[7, 9, 0] = np.nan, np.inf
+    for tm in ("linear", "reinhard", "filmic", "aces"):
+        for ot in ("gamma", "linear"):
+            for kelvin in (6500.0, 3200.0, 9000.0):
+                for clamp in (True, False):
+                    kw = dict(exposure=1.3, white_balance_kelvin=kelvin, tone_map=tm, output_transform=ot,
+                              gamma=2.2, clamp_output=clamp)
+                    assert np.array_equal(ref.apply_film_resolve(hdr, **kw), port.apply_film_resolve(hdr, **kw)), kw

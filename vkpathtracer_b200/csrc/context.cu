@@ -132,6 +132,14 @@ struct vkptc_ctx {
   WideBvh wide;
   vkptc_accel_info accel{};
 
+  // split LDR readback (request / poll)
+  DevBuf<uint8_t> d_ldr;
+  uint8_t* h_ldr = nullptr;               // pinned, 4 bytes per pixel
+  size_t h_ldr_bytes = 0;
+  cudaEvent_t ldr_event = nullptr;
+  uint64_t ldr_token = 0, ldr_next_token = 1;
+  uint32_t ldr_width = 0, ldr_height = 0;
+
   // film
   DevBuf<float4> d_film_sum;
   DevBuf<uint32_t> d_film_count;
@@ -485,6 +493,8 @@ int32_t vkptc_destroy(vkptc_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   cudaStream_t s = ctx->own_stream;
   for (auto& e : ctx->timer_events) cudaEventDestroy(e);
+  if (ctx->ldr_event) cudaEventDestroy(ctx->ldr_event);
+  if (ctx->h_ldr) cudaFreeHost(ctx->h_ldr);
   delete ctx;
   if (s) cudaStreamDestroy(s);
   return VKPTC_OK;
@@ -1092,6 +1102,104 @@ int32_t vkptc_resolve_hdr(vkptc_ctx* ctx, float* rgb) {
   cudaFreeAsync(d_rgb, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "resolve");
+  return VKPTC_OK;
+}
+
+namespace {
+
+// ColorTemperatureToRgb and WhiteBalanceScale (src/pathtracer/FilmBuffer.cpp:30-49, 216-224),
+// with the same float functions, so the scale equals the reference's.
+void temperature_rgb(float kelvin, float rgb[3]) {
+  const float t = std::clamp(kelvin, 1000.0f, 40000.0f) / 100.0f;
+  if (t <= 66.0f) {
+    rgb[0] = 1.0f;
+    rgb[1] = std::clamp(0.39008158f * std::log(std::max(1.0f, t)) - 0.63184144f, 0.0f, 1.0f);
+    rgb[2] = t <= 19.0f ? 0.0f
+                        : std::clamp(0.5432068f * std::log(std::max(1.0f, t - 10.0f)) - 1.1962541f, 0.0f, 1.0f);
+  } else {
+    rgb[0] = std::clamp(1.2929362f * std::pow(t - 60.0f, -0.13320476f), 0.0f, 1.0f);
+    rgb[1] = std::clamp(1.1298909f * std::pow(t - 60.0f, -0.075514846f), 0.0f, 1.0f);
+    rgb[2] = 1.0f;
+  }
+}
+
+LdrResolve ldr_settings(const vkptc_film_resolve& s) {
+  LdrResolve r{};
+  r.exposure = s.exposure;
+  float d65[3], target[3];
+  temperature_rgb(6500.0f, d65);
+  temperature_rgb(s.white_balance_kelvin, target);
+  for (int k = 0; k < 3; ++k) r.wb[k] = d65[k] / std::max(1.0e-3f, target[k]);
+  r.gamma = s.gamma;
+  r.tone_map = s.tone_map;
+  r.output_transform = s.output_transform;
+  r.clamp_output = s.clamp_output;
+  return r;
+}
+
+}  // namespace
+
+int32_t vkptc_resolve_ldr(vkptc_ctx* ctx, const vkptc_film_resolve* settings, uint8_t* rgba) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "film not configured");
+  if (!settings || !rgba) return fail(ctx, VKPTC_INVALID_ARGUMENT, "resolve argument is null");
+  cudaSetDevice(ctx->device);
+  const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
+  VKPTC_CUDA(ctx, ctx->d_ldr.alloc(std::max<size_t>(4, 4 * px)), "resolve alloc");
+  VKPTC_CUDA(ctx, LaunchResolveLdr(film_of(ctx), ldr_settings(*settings), ctx->config.math_mode == 0u, ctx->d_ldr.ptr,
+                                   ctx->stream), "resolve");
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(rgba, ctx->d_ldr.ptr, 4 * px, cudaMemcpyDeviceToHost, ctx->stream), "resolve read");
+  VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "resolve read");
+  return VKPTC_OK;
+}
+
+int32_t vkptc_request_ldr_readback(vkptc_ctx* ctx, const vkptc_film_resolve* settings, uint64_t* token) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!settings || !token) return fail(ctx, VKPTC_INVALID_ARGUMENT, "readback argument is null");
+  *token = 0;
+  if (!ctx->configured || !ctx->has_scene || !ctx->accel_valid)
+    return fail(ctx, VKPTC_NOT_READY, "film readback requested before the backend is ready");
+  cudaSetDevice(ctx->device);
+  const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
+  VKPTC_CUDA(ctx, ctx->d_ldr.alloc(std::max<size_t>(4, 4 * px)), "readback alloc");
+  if (ctx->h_ldr_bytes < 4 * px) {
+    if (ctx->h_ldr) cudaFreeHost(ctx->h_ldr);
+    ctx->h_ldr = nullptr;
+    ctx->h_ldr_bytes = 0;
+    VKPTC_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_ldr), std::max<size_t>(4, 4 * px)), "readback alloc");
+    ctx->h_ldr_bytes = std::max<size_t>(4, 4 * px);
+  }
+  if (!ctx->ldr_event) VKPTC_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ldr_event, cudaEventDisableTiming), "readback event");
+  VKPTC_CUDA(ctx, LaunchResolveLdr(film_of(ctx), ldr_settings(*settings), ctx->config.math_mode == 0u, ctx->d_ldr.ptr,
+                                   ctx->stream), "readback resolve");
+  VKPTC_CUDA(ctx, cudaMemcpyAsync(ctx->h_ldr, ctx->d_ldr.ptr, 4 * px, cudaMemcpyDeviceToHost, ctx->stream), "readback copy");
+  VKPTC_CUDA(ctx, cudaEventRecord(ctx->ldr_event, ctx->stream), "readback event");
+  ctx->ldr_token = ctx->ldr_next_token++;
+  ctx->ldr_width = ctx->settings.width;
+  ctx->ldr_height = ctx->settings.height;
+  *token = ctx->ldr_token;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_poll_ldr_readback(vkptc_ctx* ctx, uint64_t token, uint8_t* rgba, uint32_t* state) {
+  if (!ctx || !state) return VKPTC_INVALID_ARGUMENT;
+  *state = VKPTC_READBACK_INVALID;
+  if (token == 0 || token != ctx->ldr_token || ctx->ldr_width != ctx->settings.width ||
+      ctx->ldr_height != ctx->settings.height)
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "invalid film readback token");
+  cudaSetDevice(ctx->device);
+  const cudaError_t q = cudaEventQuery(ctx->ldr_event);
+  if (q == cudaErrorNotReady) {
+    *state = VKPTC_READBACK_PENDING;
+    return VKPTC_OK;
+  }
+  if (q != cudaSuccess) {
+    *state = VKPTC_READBACK_FAILED;
+    return cuda_fail(ctx, q, "film readback");
+  }
+  if (!rgba) return fail(ctx, VKPTC_INVALID_ARGUMENT, "rgba is null");
+  std::memcpy(rgba, ctx->h_ldr, 4ull * ctx->ldr_width * ctx->ldr_height);
+  *state = VKPTC_READBACK_READY;
   return VKPTC_OK;
 }
 

@@ -16,6 +16,8 @@
 // wavefront reordering does not change any random number a path draws, and
 // the stages add radiance terms in the reference's order (emission, then the
 // NEE term of the same bounce, then the next bounce).
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "integrator.cuh"
 #include "traverse.cuh"
@@ -454,6 +456,66 @@ __global__ void k_resolve_hdr(Film film, float* out) {
     out[3 * i + 1] = v.y * inv;
     out[3 * i + 2] = v.z * inv;
   }
+}
+
+// ApplyFilmResolve (src/pathtracer/FilmBuffer.cpp:253-325) per pixel, on the
+// film's per-pixel mean: exposure then white balance, non-finite to 0, tone
+// map, gamma (pow, FP64 rounded once in parity mode), clamp, and the x86
+// float -> uint8 conversion (truncate to int32, keep the low byte).
+__device__ __forceinline__ float ldr_tonemap(float x, uint32_t mode) {
+  switch (mode) {
+    case 1u:
+      return x / (1.0f + x);
+    case 2u: {
+      const float A = 0.15f, B = 0.50f, C = 0.10f, D = 0.20f, E = 0.02f, F = 0.30f;
+      const float W = 11.2f;
+      const float fx = ((x * (A * x + C * B) + D * E) / (x * (A * x + B) + D * F)) - E / F;
+      const float fw = ((W * (A * W + C * B) + D * E) / (W * (A * W + B) + D * F)) - E / F;
+      return fx / fw;
+    }
+    case 3u:
+      return (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+    default:
+      return x;
+  }
+}
+
+template <bool kParity>
+__global__ void k_resolve_ldr(Film film, LdrResolve rs, uint8_t* __restrict__ out) {
+  const size_t npx = static_cast<size_t>(film.width) * film.height;
+  const float inv_gamma = 1.0f / smax(0.01f, rs.gamma);
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npx;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const uint32_t c = film.count[i];
+    const float inv = 1.0f / static_cast<float>(c > 1u ? c : 1u);
+    const float4 v = film.sum[i];
+    float ch[3] = {v.x * inv * rs.exposure * rs.wb[0], v.y * inv * rs.exposure * rs.wb[1],
+                   v.z * inv * rs.exposure * rs.wb[2]};
+    uint32_t word = 0xFF000000u;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float x = ch[k];
+      if (!isfinite(x)) x = 0.0f;
+      x = ldr_tonemap(x, rs.tone_map);
+      if (rs.output_transform == 0u) {
+        const float b = smax(0.0f, x);
+        x = kParity ? parity_pow(b, inv_gamma) : powf(b, inv_gamma);
+      }
+      if (rs.clamp_output) x = smin(1.0f, smax(0.0f, x));
+      const int32_t q = __float2int_rz(x * 255.0f + 0.5f);
+      word |= (static_cast<uint32_t>(q) & 0xFFu) << (8 * k);
+    }
+    reinterpret_cast<uint32_t*>(out)[i] = word;
+  }
+}
+
+cudaError_t LaunchResolveLdr(const Film& film, const LdrResolve& rs, bool parity, uint8_t* rgba_out,
+                             cudaStream_t stream) {
+  const size_t npx = static_cast<size_t>(film.width) * film.height;
+  const int grid = static_cast<int>(std::min<size_t>(4096, std::max<size_t>(1, (npx + 255) / 256)));
+  if (parity) k_resolve_ldr<true><<<grid, 256, 0, stream>>>(film, rs, rgba_out);
+  else k_resolve_ldr<false><<<grid, 256, 0, stream>>>(film, rs, rgba_out);
+  return cudaGetLastError();
 }
 
 template <typename K>

@@ -101,4 +101,12 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
 // Film helpers.
 cudaError_t LaunchResolveHdr(const Film& film, float* rgb_out, cudaStream_t stream);
 
+// ApplyFilmResolve on the device; wb: the white-balance scale (host-computed).
+struct LdrResolve {
+  float exposure, wb[3], gamma;
+  uint32_t tone_map, output_transform, clamp_output;
+};
+cudaError_t LaunchResolveLdr(const Film& film, const LdrResolve& rs, bool parity, uint8_t* rgba_out,
+                             cudaStream_t stream);
+
 }  // namespace vkptc

@@ -253,9 +253,66 @@ pt::FilmHdr CudaPathTracer::resolve_hdr() const {
   return out;
 }
 
+namespace {
+
+vkptc_film_resolve to_resolve(const pt::FilmResolveSettings& s) {
+  vkptc_film_resolve r{};
+  r.exposure = s.exposure;
+  r.white_balance_kelvin = s.white_balance_kelvin;
+  r.tone_map = static_cast<uint32_t>(s.tone_map);
+  r.output_transform = static_cast<uint32_t>(s.output_transform);
+  r.gamma = s.gamma;
+  r.clamp_output = s.clamp_output ? 1u : 0u;
+  return r;
+}
+
+}  // namespace
+
 pt::FilmLdr CudaPathTracer::resolve_ldr() const {
-  // Tone mapping stays the reference's own host code (ApplyFilmResolve); only HDR comes from the device.
-  return pt::ApplyFilmResolve(resolve_hdr(), m_film.resolve_settings());
+  // ApplyFilmResolve on the device with the camera-adjusted resolve settings.
+  pt::FilmLdr out;
+  if (!m_ctx) return out;
+  out.width = m_settings.width;
+  out.height = m_settings.height;
+  out.rgba8.resize(4 * static_cast<size_t>(out.width) * out.height);
+  const vkptc_film_resolve rs = to_resolve(m_film.resolve_settings());
+  if (vkptc_resolve_ldr(m_ctx, &rs, out.rgba8.data()) != VKPTC_OK) {
+    m_last_error = vkptc_last_error(m_ctx);
+    return pt::FilmLdr{};
+  }
+  return out;
+}
+
+pt::FilmReadbackToken CudaPathTracer::request_film_readback() {
+  pt::FilmReadbackToken token;
+  if (!m_ctx) return token;
+  const vkptc_film_resolve rs = to_resolve(m_film.resolve_settings());
+  uint64_t id = 0;
+  if (vkptc_request_ldr_readback(m_ctx, &rs, &id) != VKPTC_OK) {
+    m_last_error = vkptc_last_error(m_ctx);
+    return token;
+  }
+  token.id = id;
+  token.fence_value = id;
+  token.width = m_settings.width;
+  token.height = m_settings.height;
+  return token;
+}
+
+pt::FilmReadbackResult CudaPathTracer::poll_film(pt::FilmReadbackToken token) {
+  if (!m_ctx || !token || token.width != m_settings.width || token.height != m_settings.height)
+    return {pt::FilmReadbackState::Invalid, {}, "invalid cuda film readback token"};
+  pt::FilmLdr ldr;
+  ldr.width = token.width;
+  ldr.height = token.height;
+  ldr.rgba8.resize(4 * static_cast<size_t>(ldr.width) * ldr.height);
+  uint32_t state = VKPTC_READBACK_INVALID;
+  const int32_t rc = vkptc_poll_ldr_readback(m_ctx, token.id, ldr.rgba8.data(), &state);
+  if (state == VKPTC_READBACK_PENDING) return {pt::FilmReadbackState::Pending, {}, {}};
+  if (state == VKPTC_READBACK_READY) return {pt::FilmReadbackState::Ready, std::move(ldr), {}};
+  m_last_error = rc == VKPTC_OK ? "film readback failed" : vkptc_last_error(m_ctx);
+  return {state == VKPTC_READBACK_INVALID ? pt::FilmReadbackState::Invalid : pt::FilmReadbackState::Failed, {},
+          m_last_error};
 }
 
 pt::SampleCounters CudaPathTracer::read_counters() const {

@@ -50,6 +50,8 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   bool supports_tile_rendering() const override { return true; }
   bool supports_tile_batching() const override { return true; }
   vkpt::pathtracer::FilmLdr resolve_ldr() const override;
+  vkpt::pathtracer::FilmReadbackToken request_film_readback() override;
+  vkpt::pathtracer::FilmReadbackResult poll_film(vkpt::pathtracer::FilmReadbackToken token) override;
   vkpt::pathtracer::FilmHdr resolve_hdr() const override;
   vkpt::pathtracer::SampleCounters read_counters() const override;
   vkpt::pathtracer::PathTracerStatus status() const override;

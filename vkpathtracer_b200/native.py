@@ -62,6 +62,16 @@ class SceneView(ctypes.Structure):
 SDF_SPHERE, SDF_BOX, SDF_ROUNDED_BOX, SDF_PLANE, SDF_TORUS, SDF_CAPSULE = range(6)
 
 
+class FilmResolve(ctypes.Structure):
+    _fields_ = [("exposure", ctypes.c_float), ("white_balance_kelvin", ctypes.c_float), ("tone_map", ctypes.c_uint32),
+                ("output_transform", ctypes.c_uint32), ("gamma", ctypes.c_float), ("clamp_output", ctypes.c_uint32)]
+
+
+TONE_MAPS = {"linear": 0, "reinhard": 1, "filmic": 2, "aces": 3}
+OUTPUT_TRANSFORMS = {"gamma": 0, "linear": 1}
+READBACK_INVALID, READBACK_PENDING, READBACK_READY, READBACK_FAILED = range(4)
+
+
 class BvhView(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_void_p), ("node_count", ctypes.c_uint32),
                 ("prim_indices", ctypes.c_void_p), ("prim_count", ctypes.c_uint32)]
@@ -156,6 +166,9 @@ SIGNATURES = {
     "vkptc_load_bvh": (I32, [P, ctypes.POINTER(BvhView)]),
     "vkptc_get_accel_info": (I32, [P, ctypes.POINTER(AccelInfo)]),
     "vkptc_read_accel": (I32, [P, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "vkptc_resolve_ldr": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.c_void_p]),
+    "vkptc_request_ldr_readback": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.POINTER(ctypes.c_uint64)]),
+    "vkptc_poll_ldr_readback": (I32, [P, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),
     "vkptc_reset": (I32, [P]),
     "vkptc_shutdown": (I32, [P]),

@@ -207,6 +207,38 @@ class CudaPathTracer:
         self._check(self._lib.vkptc_get_accel_info(self._ctx, ctypes.byref(a)))
         return a.as_dict()
 
+    @staticmethod
+    def film_resolve(exposure: float = 1.0, white_balance_kelvin: float = 6500.0, tone_map: str = "linear",
+                     output_transform: str = "gamma", gamma: float = 2.2, clamp_output: bool = True):
+        """FilmResolveSettings (the reference's defaults)."""
+        r = native.FilmResolve()
+        r.exposure, r.white_balance_kelvin = exposure, white_balance_kelvin
+        r.tone_map, r.output_transform = native.TONE_MAPS[tone_map], native.OUTPUT_TRANSFORMS[output_transform]
+        r.gamma, r.clamp_output = gamma, int(clamp_output)
+        return r
+
+    def resolve_ldr(self, **settings) -> np.ndarray:
+        """ApplyFilmResolve(resolve_hdr()) on the device: (H, W, 4) uint8."""
+        st = self._settings
+        out = np.zeros((st.height, st.width, 4), np.uint8)
+        rs = self.film_resolve(**settings)
+        self._check(self._lib.vkptc_resolve_ldr(self._ctx, ctypes.byref(rs), out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def request_film_readback(self, **settings) -> int:
+        tok = ctypes.c_uint64(0)
+        rs = self.film_resolve(**settings)
+        self._check(self._lib.vkptc_request_ldr_readback(self._ctx, ctypes.byref(rs), ctypes.byref(tok)))
+        return int(tok.value)
+
+    def poll_film(self, token: int):
+        """(state, image or None); state is native.READBACK_*; never blocks."""
+        st = self._settings
+        out = np.zeros((st.height, st.width, 4), np.uint8)
+        state = ctypes.c_uint32(0)
+        self._lib.vkptc_poll_ldr_readback(self._ctx, token, out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(state))
+        return int(state.value), (out if state.value == native.READBACK_READY else None)
+
     def read_accel(self, what: int) -> np.ndarray:
         """One device array of the accelerator (native.ACCEL_*) as raw uint32 words."""
         n = ctypes.c_uint64(0)
