@@ -239,6 +239,25 @@ int32_t vkptc_build_acceleration(vkptc_ctx* ctx);
  * output over the accelerator's primitive order, CpuBvhAccelerator.cpp:247-256). */
 int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh);
 int32_t vkptc_get_accel_info(vkptc_ctx* ctx, vkptc_accel_info* out);
+
+/* RTInstanceTransformUpdate (src/pathtracer/PathTracer.h:298-306), resolved to an instance index. */
+typedef struct vkptc_instance_update {
+  uint32_t instance_index;
+  uint32_t flags;              /* OR-ed into the instance's flags */
+  float translation[3];
+  float rotation[4];           /* quaternion xyzw */
+  float scale[3];
+} vkptc_instance_update;
+/* replaces IPathTracer::apply_instance_transform_update (src/pathtracer/PathTracer.h:1123-1135) as the
+ * CPU accelerator implements it (src/pathtracer/CpuBvhAccelerator.cpp:265-358, 527-606): every updated
+ * instance must be a dynamic-transform instance with local geometry (else VKPTC_UNSUPPORTED, the
+ * reference's BlockedNeedsFullStaticAccelRebuild); its primitives are recomputed with the new
+ * transform and both trees are refitted with their topology unchanged (no rebuild), on the device.
+ * All updates are checked before any is applied.  The film is not reset (vkptc_reset does that). */
+int32_t vkptc_update_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_update* updates, uint32_t count);
+/* replaces IPathTracer::plan_instance_transform_update (src/pathtracer/PathTracer.h:1115-1122): the
+ * same checks and return codes as vkptc_update_instance_transforms, nothing applied. */
+int32_t vkptc_check_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_update* updates, uint32_t count);
 /* Extension (no reference counterpart): copies one device array of the built
  * accelerator to host memory, for inspection and for checking the device
  * build against the host build.  what: VKPTC_ACCEL_WIDE_NODES (128 B each),

@@ -82,6 +82,23 @@ class VkoCounters(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class VkoInstanceUpdate(ctypes.Structure):
+    _fields_ = [("instance_index", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("translation", ctypes.c_float * 3),
+                ("rotation", ctypes.c_float * 4), ("scale", ctypes.c_float * 3)]
+
+
+def instance_updates(updates, struct=VkoInstanceUpdate):
+    """[{"instance", "translation", "rotation", "scale", "flags"}] -> ctypes array."""
+    arr = (struct * max(1, len(updates)))()
+    for k, u in enumerate(updates):
+        arr[k].instance_index = u["instance"]
+        arr[k].flags = u.get("flags", 0)
+        arr[k].translation[:] = u.get("translation", (0.0, 0.0, 0.0))
+        arr[k].rotation[:] = u.get("rotation", (0.0, 0.0, 0.0, 1.0))
+        arr[k].scale[:] = u.get("scale", (1.0, 1.0, 1.0))
+    return arr
+
+
 def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
@@ -189,8 +206,10 @@ class Oracle:
 
     # -- API
     def render(self, scene, settings, first_sample: int = 0, n_samples: Optional[int] = None,
-               threads: int = 1, pixels: Optional[np.ndarray] = None, per_sample: bool = False):
-        """Returns dict(sum=(H,W,3), count=(H,W), invalid=(H,W), samples=(n,H,W,3)|None, counters)."""
+               threads: int = 1, pixels: Optional[np.ndarray] = None, per_sample: bool = False,
+               updates=None):
+        """Returns dict(sum=(H,W,3), count=(H,W), invalid=(H,W), samples=(n,H,W,3)|None, counters).
+        updates: instance transform updates applied after the build (one tracer, full frame)."""
         n = settings.spp if n_samples is None else n_samples
         W, H = settings.width, settings.height
         sc, keep = self.make_scene(scene)
@@ -201,9 +220,16 @@ class Oracle:
         samples = np.zeros((n, H, W, 3), np.float32) if per_sample else None
         px = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint32)
         ctr = VkoCounters()
-        rc = self.lib.vko_render(ctypes.byref(sc), ctypes.byref(st), first_sample, n, threads,
-                                 _ptr(px), 0 if px is None else px.size, _ptr(film), _ptr(count),
-                                 _ptr(invalid), _ptr(samples), ctypes.byref(ctr))
+        if updates:
+            ups = instance_updates(updates)
+            self.lib.vko_set_instance_updates(ups, len(updates))
+        try:
+            rc = self.lib.vko_render(ctypes.byref(sc), ctypes.byref(st), first_sample, n, threads,
+                                     _ptr(px), 0 if px is None else px.size, _ptr(film), _ptr(count),
+                                     _ptr(invalid), _ptr(samples), ctypes.byref(ctr))
+        finally:
+            if updates:
+                self.lib.vko_set_instance_updates(None, 0)
         del keep
         self._check(rc)
         return {"sum": film, "count": count, "invalid": invalid, "samples": samples,

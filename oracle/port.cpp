@@ -28,6 +28,7 @@
 //     intersect_sphere, the march   src/pathtracer/ScalarCpuPathTracer.cpp:855-930
 //     nearest-hit reduction         src/pathtracer/ScalarCpuPathTracer.Intersect.cpp:91-129
 //   dynamic-instance flattening     src/pathtracer/CpuBvhAccelerator.cpp:47-74, 173-247
+//   instance transform refit        src/pathtracer/CpuBvhAccelerator.cpp:265-358, 527-606
 //   ApplyFilmResolve, WhiteBalanceScale, ColorTemperatureToRgb
 //                                   src/pathtracer/FilmBuffer.cpp:30-49, 216-224, 253-325
 
@@ -46,6 +47,7 @@
 namespace {
 
 thread_local std::string g_error;
+thread_local std::vector<vko_instance_update> g_updates;
 int fail(const std::string& m) { g_error = m; return 1; }
 
 constexpr float kPi = 3.14159265358979323846f;
@@ -394,9 +396,14 @@ struct World {
     return add(r, V3{t[0], t[1], t[2]});
   }
 
+  const vko_scene* src = nullptr;
+  std::vector<uint32_t> inst_first, inst_count;   // flattened primitive range per instance
+
   void load(const vko_scene& s, bool stable = true, size_t leaf = 4) {
+    src = &s;
     const bool dyn = s.instance_local && s.instance_transforms;
     for (uint32_t i = 0; i < s.instance_count; ++i) {
+      inst_first.push_back(static_cast<uint32_t>(prims.size()));
       const uint32_t first = s.instances[3 * i], count = s.instances[3 * i + 1], mat = s.instances[3 * i + 2];
       const uint32_t* loc = dyn ? s.instance_local + 5 * i : nullptr;
       const bool use_local = loc && (loc[0] & 1u) && loc[2] > 0u && loc[4] > 0u;
@@ -447,6 +454,7 @@ struct World {
         prims.push_back(p);
         boxes.push_back(bx);
       }
+      inst_count.push_back(static_cast<uint32_t>(prims.size()) - inst_first.back());
     }
     if (!prims.empty()) {
       nodes.assign(2 * prims.size() - 1, Node{});
@@ -641,6 +649,79 @@ struct World {
       h.mat = p.material;
     }
     return h.hit;
+  }
+
+  // apply_instance_transform_update of the CPU accelerator: every update checked
+  // (dynamic instance with local geometry, complete primitive range, local
+  // indices in range), the primitives recomputed with the new transform, then
+  // refit_node(0) over the unchanged topology.
+  bool apply_updates(const std::vector<vko_instance_update>& ups, std::string& why) {
+    const vko_scene& s = *src;
+    for (const auto& u : ups) {
+      const uint32_t i = u.instance_index;
+      if (i >= s.instance_count) { why = "unknown instance"; return false; }
+      const uint32_t* loc = (s.instance_local && s.instance_transforms) ? s.instance_local + 5 * i : nullptr;
+      if (!loc || !(loc[0] & 1u) || loc[2] == 0u || loc[4] == 0u) { why = "needs dynamic local geometry"; return false; }
+    }
+    for (const auto& u : ups) {
+      const uint32_t i = u.instance_index;
+      const uint32_t* loc = s.instance_local + 5 * i;
+      const uint32_t count = s.instances[3 * i + 1], mat = s.instances[3 * i + 2];
+      if (inst_count[i] != count) { why = "primitive range"; return false; }
+      const float t[10] = {u.translation[0], u.translation[1], u.translation[2], u.rotation[0], u.rotation[1],
+                           u.rotation[2], u.rotation[3], u.scale[0], u.scale[1], u.scale[2]};
+      for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t lb = loc[3] + k * 3u, le = loc[1] + loc[2];
+        if (lb >= 0xFFFFFFFEu || lb + 2u >= s.local_index_count) { why = "local indices"; return false; }
+        V3 v[3];
+        for (int j = 0; j < 3; ++j) {
+          const uint32_t a = loc[1] + s.local_indices[lb + j];
+          if (a >= le || a >= s.local_vertex_count) { why = "local vertices"; return false; }
+          v[j] = instance_vertex(ld3(s.local_vertices + 3 * a), t);
+        }
+        Prim& p = prims[inst_first[i] + k];
+        p.material = mat;
+        p.v0 = v[0];
+        p.e1 = sub(v[1], v[0]);
+        p.e2 = sub(v[2], v[0]);
+        const V3 cr = cross(p.e1, p.e2);
+        const float l2 = dot(cr, cr);
+        p.n = (l2 <= kEps * kEps) ? V3{0.0f, 1.0f, 0.0f} : mul(cr, 1.0f / std::sqrt(l2));
+        Box& bx = boxes[inst_first[i] + k];
+        bx.lo[0] = std::min({v[0].x, v[1].x, v[2].x}) - kEps;
+        bx.lo[1] = std::min({v[0].y, v[1].y, v[2].y}) - kEps;
+        bx.lo[2] = std::min({v[0].z, v[1].z, v[2].z}) - kEps;
+        bx.hi[0] = std::max({v[0].x, v[1].x, v[2].x}) + kEps;
+        bx.hi[1] = std::max({v[0].y, v[1].y, v[2].y}) + kEps;
+        bx.hi[2] = std::max({v[0].z, v[1].z, v[2].z}) + kEps;
+      }
+    }
+    if (!nodes.empty()) refit(0);
+    return true;
+  }
+
+  Box refit(int32_t id) {
+    Node& nd = nodes[static_cast<size_t>(id)];
+    if (nd.count > 0) {
+      Box b = boxes[order[static_cast<size_t>(nd.first)]];
+      for (int32_t k = 1; k < nd.count; ++k) {
+        const Box& o = boxes[order[static_cast<size_t>(nd.first + k)]];
+        for (int a = 0; a < 3; ++a) {
+          b.lo[a] = fmin_std(b.lo[a], o.lo[a]);
+          b.hi[a] = fmax_std(b.hi[a], o.hi[a]);
+        }
+      }
+      nd.box = b;
+      return b;
+    }
+    const Box l = refit(nd.left), r = refit(nd.right);
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+      b.lo[a] = fmin_std(l.lo[a], r.lo[a]);
+      b.hi[a] = fmax_std(l.hi[a], r.hi[a]);
+    }
+    nodes[static_cast<size_t>(id)].box = b;
+    return b;
   }
 
   const Material& mat(uint32_t i) const { return mats[std::min<size_t>(i, mats.size() - 1)]; }
@@ -1015,6 +1096,11 @@ extern "C" {
 const char* vko_last_error(void) { return g_error.c_str(); }
 const char* vko_impl_name(void) { return "port"; }
 
+int vko_set_instance_updates(const vko_instance_update* updates, uint32_t count) {
+  g_updates.assign(updates, updates + count);
+  return 0;
+}
+
 int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t first_sample,
                uint32_t n_samples, uint32_t threads, const uint32_t* pixels, uint32_t pixel_count,
                float* film_sum, uint32_t* film_count, float* film_invalid, float* per_sample,
@@ -1022,6 +1108,10 @@ int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t fi
   if (!scene || !settings) return fail("null scene or settings");
   World w;
   w.load(*scene);
+  if (!g_updates.empty()) {
+    std::string why;
+    if (!w.apply_updates(g_updates, why)) return fail("transform update rejected: " + why);
+  }
   Integrator it{w, *settings};
   const uint32_t W = settings->width, H = settings->height;
   const size_t npx = static_cast<size_t>(W) * H;

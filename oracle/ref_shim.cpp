@@ -193,6 +193,8 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 // Full-frame render through one IPathTracer, one render_tile per sample, as
 // ptbench's `run` loop does (src/benchmark/BenchmarkRuntime.cpp:682-693).
+thread_local std::vector<pt::RTInstanceTransformUpdate> g_updates;
+
 int render_full(pt::IPathTracer& tracer, const vko_settings& st, uint32_t first, uint32_t n,
                 float* film_sum, uint32_t* film_count, float* film_invalid, float* per_sample,
                 vko_counters* counters) {
@@ -248,6 +250,20 @@ int render_full(pt::IPathTracer& tracer, const vko_settings& st, uint32_t first,
 extern "C" {
 
 const char* vko_last_error(void) { return g_error.c_str(); }
+
+int vko_set_instance_updates(const vko_instance_update* updates, uint32_t count) {
+  g_updates.clear();
+  for (uint32_t i = 0; i < count; ++i) {
+    pt::RTInstanceTransformUpdate u;
+    u.instance_index = updates[i].instance_index;
+    u.flags = updates[i].flags;
+    u.translation = pt::Vec3{updates[i].translation[0], updates[i].translation[1], updates[i].translation[2]};
+    u.rotation = pt::Quat4{updates[i].rotation[0], updates[i].rotation[1], updates[i].rotation[2], updates[i].rotation[3]};
+    u.scale = pt::Vec3{updates[i].scale[0], updates[i].scale[1], updates[i].scale[2]};
+    g_updates.push_back(u);
+  }
+  return 0;
+}
 
 int vko_apply_film_resolve(const float* hdr_rgb, uint32_t width, uint32_t height, const vko_resolve* s,
                            uint8_t* rgba) {
@@ -381,12 +397,16 @@ int vko_render(const vko_scene* scene, const vko_settings* settings,
   const auto rs = to_settings(*settings, first_sample + n_samples);
   const std::size_t npx = static_cast<std::size_t>(settings->width) * settings->height;
 
-  if (pixels == nullptr) {
-    if (threads <= 1u) {
+  if (pixels == nullptr || !g_updates.empty()) {
+    if (threads <= 1u || !g_updates.empty()) {
       pt::ScalarCpuPathTracer tracer;
       if (!tracer.configure(rs) || !tracer.load_scene_snapshot(snap) ||
           !tracer.build_or_update_acceleration() || !tracer.reset_accumulation()) {
         return fail("scalar tracer setup failed: " + tracer.status().last_error);
+      }
+      if (!g_updates.empty()) {
+        const auto r = tracer.apply_instance_transform_update(g_updates, pt::InstanceTransformUpdateOptions{});
+        if (!r.applied()) return fail(std::string("transform update rejected: ") + (r.message ? r.message : ""));
       }
       return render_full(tracer, *settings, first_sample, n_samples, film_sum, film_count,
                          film_invalid, per_sample, counters);

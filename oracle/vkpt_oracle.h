@@ -137,6 +137,22 @@ int vko_intersect(const vko_scene* scene, const float* rays, uint64_t ray_count,
                   uint32_t threads, uint32_t* prim_out, float* t_out,
                   uint64_t* stats, double* elapsed_ms);
 
+/* RTInstanceTransformUpdate (src/pathtracer/PathTracer.h:298-306) by instance index. */
+typedef struct vko_instance_update {
+  uint32_t instance_index;
+  uint32_t flags;
+  float translation[3];
+  float rotation[4];   /* quaternion xyzw */
+  float scale[3];
+} vko_instance_update;
+
+/* Instance transform updates (IPathTracer::apply_instance_transform_update)
+ * applied by the calling thread's next vko_render calls after the
+ * accelerator is built and before rendering; count 0 clears them.  A render
+ * with updates is a full-frame render on one tracer (threads, pixel lists
+ * ignored).  The render fails when the reference rejects the updates. */
+int vko_set_instance_updates(const vko_instance_update* updates, uint32_t count);
+
 /* FilmResolveSettings (src/pathtracer/PathTracer.h:55-74). */
 typedef struct vko_resolve {
   float exposure;

@@ -131,3 +131,18 @@ def load_scene_fixture(name):
     import os
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "scenes", f"{name}.npz")
     return dict(np.load(path))
+
+
+def transform_updates(scene, step=1.0, count=3):
+    """Instance transform updates for the first `count` dynamic-transform
+    instances with local geometry: a shift, a rotation about y, a 5 % scale."""
+    import math
+    il = scene.instance_local
+    dyn = [i for i in range(scene.instances.shape[0]) if il[i, 0] & 1 and il[i, 2] and il[i, 4]]
+    ups = []
+    for k, i in enumerate(dyn[:count]):
+        t = scene.instance_transforms[i]
+        a = (0.3 + 0.2 * k) * step
+        ups.append({"instance": i, "translation": (t[0] + 0.05 * (k + 1) * step, t[1] + 0.02 * step, t[2] - 0.03),
+                    "rotation": (0.0, math.sin(a / 2), 0.0, math.cos(a / 2)), "scale": tuple(t[7:10] * 1.05)})
+    return ups

@@ -232,3 +232,19 @@ def test_port_film_resolve_matches_reference(port):
                     kw = dict(exposure=1.3, white_balance_kelvin=kelvin, tone_map=tm, output_transform=ot,
                               gamma=2.2, clamp_output=clamp)
                     assert np.array_equal(ref.apply_film_resolve(hdr, **kw), port.apply_film_resolve(hdr, **kw)), kw
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
+@pytest.mark.parametrize("name", ["cornell_native", "tessellation_sphere_levels", "material_shader_physics_showcase"])
+def test_port_instance_refit_matches_reference(port, name):
+    """apply_instance_transform_update of the CPU accelerator after the build:
+    the port's refit gives the reference's film."""
+    ref = oracle.load("reference")
+    d = cases.load_scene_fixture(name)
+    scene, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
+    ups = cases.transform_updates(scene)
+    a = ref.render(scene, st, updates=ups)
+    b = port.render(scene, st, updates=ups)
+    assert np.array_equal(bits(a["sum"]), bits(b["sum"]))
+    assert a["counters"]["rays"] == b["counters"]["rays"]
+    assert not np.array_equal(bits(a["sum"]), bits(d["film_sum"]))

@@ -940,6 +940,7 @@ struct WideArrays {
   uint32_t* size;       // subtree sizes
   uint32_t* visits;
   int32_t* final_id;
+  int32_t* slot_bin;    // optional: binary node per wide slot (refit)
 };
 
 __device__ __forceinline__ float bin_area(const BinNode& n) {
@@ -1053,6 +1054,8 @@ __global__ void k_wide_write(WideArrays W, uint32_t n_wide, WideNode* __restrict
     n.meta[k] = 0;
   }
   n.meta[0] = w.nslots;
+  if (W.slot_bin)
+    for (int k = 0; k < 4; ++k) W.slot_bin[4 * W.final_id[x] + k] = k < w.nslots ? w.slot[k] : -1;
   for (int k = 0; k < w.nslots; ++k) {
     const BinNode c = W.bin[w.slot[k]];
     n.lox[k] = c.lo[0];
@@ -1216,11 +1219,11 @@ cudaError_t finish_tree(const float4* blo, const float4* bhi, const uint32_t* or
 }
 
 cudaError_t collapse(const BinNode* bin, uint32_t n_bin, WideNode* out, uint32_t& n_wide, uint32_t& depth,
-                     uint32_t& stack_required, Scratch& sc) {
+                     uint32_t& stack_required, Scratch& sc, int32_t* slot_bin = nullptr) {
   cudaStream_t s = sc.s;
   const uint32_t cap = n_bin;   // wide nodes <= binary internal nodes + 1
   WideArrays W{bin, sc.get<WTemp>(cap), sc.get<uint32_t>(4), sc.get<uint32_t>(cap), sc.get<uint32_t>(cap),
-               sc.get<int32_t>(cap)};
+               sc.get<int32_t>(cap), slot_bin};
   uint32_t* cur = sc.get<uint32_t>(cap);
   uint32_t* next = sc.get<uint32_t>(cap);
   if (sc.err != cudaSuccess) return sc.err;
@@ -1259,9 +1262,201 @@ cudaError_t dmalloc(T*& p, size_t n) {
   return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(1, n) * sizeof(T));
 }
 
+__global__ void k_inst_first(const uint32_t* __restrict__ pos, const unsigned long long* __restrict__ prefix,
+                             uint32_t ninst, uint32_t* __restrict__ first) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= ninst) first[i] = pos[prefix[i]];
+}
+
+__global__ void k_tri_pos(const uint32_t* __restrict__ order, uint32_t n, uint32_t* __restrict__ tri_pos) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) tri_pos[order[i]] = i;
+}
+
+__global__ void k_parents(const BinNode* __restrict__ nodes, uint32_t n, int32_t* __restrict__ parent) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  if (x == 0u) parent[0] = -1;
+  const BinNode b = nodes[x];
+  if (b.count == 0) {
+    parent[b.left] = static_cast<int32_t>(x);
+    parent[b.right] = static_cast<int32_t>(x);
+  }
+}
+
+// ---------------------------------------------------------------- refit after transform updates
+struct RefitTri {
+  const RefitUpdate* up;
+  const uint32_t* offset;   // per update: first triangle of the launch (update count + 1 entries)
+  uint32_t n_up;
+  const float* lv;
+  const uint32_t* li;
+};
+
+__global__ void k_refit_prims(RefitTri R, uint32_t total, const uint32_t* __restrict__ tri_pos, TriRecord* __restrict__ tris,
+                              float4* __restrict__ shade, float4* __restrict__ blo, float4* __restrict__ bhi) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  uint32_t lo = 0u, hi = R.n_up;   // offset[lo] <= g < offset[hi]
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (R.offset[mid] <= g) lo = mid;
+    else hi = mid;
+  }
+  const RefitUpdate& u = R.up[lo];
+  const uint32_t k = g - R.offset[lo];
+  const uint32_t base = u.local_first_index + k * 3u;
+  float a[3], b[3], c[3];
+  instance_vertex(R.lv + 3ull * (u.local_first_vertex + R.li[base]), u.transform, a);
+  instance_vertex(R.lv + 3ull * (u.local_first_vertex + R.li[base + 1u]), u.transform, b);
+  instance_vertex(R.lv + 3ull * (u.local_first_vertex + R.li[base + 2u]), u.transform, c);
+  const uint32_t p = u.prim_first + k;
+  const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+  const float e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
+  const float nx = e1y * e2z - e1z * e2y;
+  const float ny = e1z * e2x - e1x * e2z;
+  const float nz = e1x * e2y - e1y * e2x;
+  const float l2 = nx * nx + ny * ny + nz * nz;
+  if (l2 <= kPadB * kPadB) {
+    shade[p] = make_float4(0.0f, 1.0f, 0.0f, __uint_as_float(u.material));
+  } else {
+    const float inv = 1.0f / sqrtf(l2);
+    shade[p] = make_float4(nx * inv, ny * inv, nz * inv, __uint_as_float(u.material));
+  }
+  TriRecord& r = tris[tri_pos[p]];
+  r.v0x = a[0];
+  r.v0y = a[1];
+  r.v0z = a[2];
+  r.e1x = e1x;
+  r.e1y = e1y;
+  r.e1z = e1z;
+  r.e2x = e2x;
+  r.e2y = e2y;
+  r.e2z = e2z;
+  blo[p] = make_float4(min3(a[0], b[0], c[0]) - kPadB, min3(a[1], b[1], c[1]) - kPadB, min3(a[2], b[2], c[2]) - kPadB, 0.0f);
+  bhi[p] = make_float4(max3(a[0], b[0], c[0]) + kPadB, max3(a[1], b[1], c[1]) + kPadB, max3(a[2], b[2], c[2]) + kPadB, 0.0f);
+}
+
+// refit_node over a whole binary tree, bottom-up by walks from the leaves
+// (leaf: union of its primitives' boxes; internal: union of its children).
+__global__ void k_refit_tree(BinNode* __restrict__ nodes, const int32_t* __restrict__ parent, const uint32_t* __restrict__ order,
+                             uint32_t n_nodes, const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                             uint32_t* __restrict__ visits, TieNode* __restrict__ tie) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes || nodes[x].count == 0) return;
+  const BinNode leaf = nodes[x];
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int32_t i = 0; i < leaf.count; ++i) {
+    const uint32_t p = order[leaf.first + i];
+    const float4 a = blo[p], b = bhi[p];
+    lo[0] = bmin(lo[0], a.x);
+    lo[1] = bmin(lo[1], a.y);
+    lo[2] = bmin(lo[2], a.z);
+    hi[0] = bmax(hi[0], b.x);
+    hi[1] = bmax(hi[1], b.y);
+    hi[2] = bmax(hi[2], b.z);
+  }
+  while (true) {
+    for (int q = 0; q < 3; ++q) {
+      nodes[x].lo[q] = lo[q];
+      nodes[x].hi[q] = hi[q];
+    }
+    if (tie) {
+      tie[x].lox = lo[0];
+      tie[x].loy = lo[1];
+      tie[x].loz = lo[2];
+      tie[x].hix = hi[0];
+      tie[x].hiy = hi[1];
+      tie[x].hiz = hi[2];
+    }
+    __threadfence();
+    const int32_t p = parent[x];
+    if (p < 0) break;
+    if (atomicAdd(&visits[p], 1u) == 0u) break;
+    const BinNode pn = nodes[p];
+    const int32_t sib = pn.left == static_cast<int32_t>(x) ? pn.right : pn.left;
+    for (int q = 0; q < 3; ++q) {
+      lo[q] = bmin(lo[q], __ldcg(&nodes[sib].lo[q]));
+      hi[q] = bmax(hi[q], __ldcg(&nodes[sib].hi[q]));
+    }
+    x = static_cast<uint32_t>(p);
+  }
+}
+
+__global__ void k_refit_wide(WideNode* __restrict__ wide, uint32_t n_wide, const int32_t* __restrict__ slot_bin,
+                             const BinNode* __restrict__ bin) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_wide) return;
+  for (int k = 0; k < 4; ++k) {
+    const int32_t b = slot_bin[4 * w + k];
+    if (b < 0) continue;
+    const BinNode c = bin[b];
+    wide[w].lox[k] = c.lo[0];
+    wide[w].loy[k] = c.lo[1];
+    wide[w].loz[k] = c.lo[2];
+    wide[w].hix[k] = c.hi[0];
+    wide[w].hiy[k] = c.hi[1];
+    wide[w].hiz[k] = c.hi[2];
+  }
+}
+
 }  // namespace
 
+void FreeRefitState(DeviceRefitState*& st) {
+  if (!st) return;
+  cudaFree(st->blo);
+  cudaFree(st->bhi);
+  cudaFree(st->tri_pos);
+  cudaFree(st->trav_nodes);
+  cudaFree(st->trav_order);
+  cudaFree(st->trav_parent);
+  cudaFree(st->slot_bin);
+  cudaFree(st->inst_first);
+  delete st;
+  st = nullptr;
+}
+
+cudaError_t RefitOnDevice(DeviceRefitState& st, const std::vector<RefitUpdate>& updates, const float* local_vertices,
+                          const uint32_t* local_indices, BinNode* ref_nodes, const uint32_t* ref_order,
+                          uint32_t ref_count, float4* nodes, uint32_t wide_count, float4* tris, float4* tie,
+                          float4* shade, cudaStream_t stream) {
+  if (updates.empty()) return cudaSuccess;
+  Scratch sc{stream};
+  std::vector<uint32_t> offset(updates.size() + 1, 0u);
+  for (size_t i = 0; i < updates.size(); ++i) offset[i + 1] = offset[i] + updates[i].prim_count;
+  RefitUpdate* d_up = sc.get<RefitUpdate>(updates.size());
+  uint32_t* d_off = sc.get<uint32_t>(offset.size());
+  int32_t* ref_parent = sc.get<int32_t>(ref_count);
+  uint32_t* visits = sc.get<uint32_t>(std::max(ref_count, st.trav_count));
+  if (sc.err != cudaSuccess) return sc.err;
+  BB_TRY(cudaMemcpyAsync(d_up, updates.data(), updates.size() * sizeof(RefitUpdate), cudaMemcpyHostToDevice, stream));
+  BB_TRY(cudaMemcpyAsync(d_off, offset.data(), offset.size() * 4, cudaMemcpyHostToDevice, stream));
+  const uint32_t total = offset.back();
+  const RefitTri R{d_up, d_off, static_cast<uint32_t>(updates.size()), local_vertices, local_indices};
+  if (total)
+    k_refit_prims<<<grid_for(total), kThreads, 0, stream>>>(R, total, st.tri_pos, reinterpret_cast<TriRecord*>(tris),
+                                                            shade, st.blo, st.bhi);
+  // the reference tree (tie records) ...
+  k_parents<<<grid_for(ref_count), kThreads, 0, stream>>>(ref_nodes, ref_count, ref_parent);
+  BB_TRY(cudaMemsetAsync(visits, 0, ref_count * sizeof(uint32_t), stream));
+  k_refit_tree<<<grid_for(ref_count), kThreads, 0, stream>>>(ref_nodes, ref_parent, ref_order, ref_count, st.blo,
+                                                             st.bhi, visits, reinterpret_cast<TieNode*>(tie));
+  // ... the traversal tree when it is a different one, then the wide slots
+  const BinNode* trav = ref_nodes;
+  if (st.trav_nodes) {
+    BB_TRY(cudaMemsetAsync(visits, 0, st.trav_count * sizeof(uint32_t), stream));
+    k_refit_tree<<<grid_for(st.trav_count), kThreads, 0, stream>>>(st.trav_nodes, st.trav_parent, st.trav_order,
+                                                                   st.trav_count, st.blo, st.bhi, visits, nullptr);
+    trav = st.trav_nodes;
+  }
+  k_refit_wide<<<grid_for(wide_count), kThreads, 0, stream>>>(reinterpret_cast<WideNode*>(nodes), wide_count,
+                                                              st.slot_bin, trav);
+  BB_TRY(cudaGetLastError());
+  return cudaStreamSynchronize(stream);
+}
+
 void FreeDeviceAccel(DeviceAccelOut& out) {
+  FreeRefitState(out.refit);
   cudaFree(out.nodes);
   cudaFree(out.tris);
   cudaFree(out.tie);
@@ -1276,6 +1471,12 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   const uint32_t* instances = sc_in.instances;
   const uint32_t instance_count = sc_in.instance_count;
   const bool dyn = sc_in.instance_local && sc_in.instance_transforms;
+  // Keep what a refit needs when some instance can take transform updates.
+  bool keep_refit = false;
+  for (uint32_t i = 0; dyn && i < instance_count; ++i) {
+    const uint32_t* l = sc_in.instance_local + 5 * i;
+    keep_refit = keep_refit || ((l[0] & 1u) != 0u && l[2] > 0u && l[4] > 0u);
+  }
   // Candidate triangles of every instance (the host path's loop bounds).
   std::vector<unsigned long long> prefix(instance_count + 1u, 0ull);
   for (uint32_t i = 0; i < instance_count; ++i) prefix[i + 1] = prefix[i] + instances[3 * i + 1];
@@ -1308,13 +1509,34 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   BB_TRY(read_scalar(pos + nc, n, stream));
   out.prim_count = n;
   float4* pv = sc.get<float4>(3ull * n);
-  float4* blo = sc.get<float4>(n);
-  float4* bhi = sc.get<float4>(n);
+  float4* blo = nullptr;
+  float4* bhi = nullptr;
+  if (keep_refit) {
+    out.refit = new DeviceRefitState();
+    BB_TRY(dmalloc(out.refit->blo, n));
+    BB_TRY(dmalloc(out.refit->bhi, n));
+    BB_TRY(dmalloc(out.refit->inst_first, instance_count + 1u));
+    blo = out.refit->blo;
+    bhi = out.refit->bhi;
+  } else {
+    blo = sc.get<float4>(n);
+    bhi = sc.get<float4>(n);
+  }
   if (sc.err != cudaSuccess) return sc.err;
   BB_TRY(dmalloc(out.shade, n));
   if (nc) k_flat_write<<<grid_for(nc), kThreads, 0, stream>>>(f, flag, pos, pv, out.shade, blo, bhi, nonfinite);
   uint32_t bad = 0u;
   BB_TRY(read_scalar(nonfinite, bad, stream));
+  if (keep_refit && !bad) {
+    k_inst_first<<<grid_for(instance_count + 1u), kThreads, 0, stream>>>(pos, d_prefix, instance_count,
+                                                                          out.refit->inst_first);
+    std::vector<uint32_t> first(instance_count + 1u);
+    BB_TRY(cudaMemcpyAsync(first.data(), out.refit->inst_first, 4ull * first.size(), cudaMemcpyDeviceToHost, stream));
+    BB_TRY(cudaStreamSynchronize(stream));
+    out.refit->host_inst_first.assign(first.begin(), first.end() - 1);
+    out.refit->host_inst_count.resize(instance_count);
+    for (uint32_t i = 0; i < instance_count; ++i) out.refit->host_inst_count[i] = first[i + 1] - first[i];
+  }
   if (bad) {
     FreeDeviceAccel(out);
     out.fallback = true;
@@ -1344,14 +1566,25 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   const uint32_t* trav_order = out.ref_order;
   uint32_t n_trav = n_ref;
   if (sah) {
-    uint32_t* sah_order = sc.get<uint32_t>(n);
+    uint32_t* sah_order = nullptr;
+    if (keep_refit) BB_TRY(dmalloc(out.refit->trav_order, n));
+    sah_order = keep_refit ? out.refit->trav_order : sc.get<uint32_t>(n);
     TNode* sn = sc.get<TNode>(2ull * n);
     if (sc.err != cudaSuccess) return sc.err;
     k_iota<<<grid_for(n), kThreads, 0, stream>>>(sah_order, n);
     BB_TRY(build_tree(blo, bhi, n, true, sah_order, sn, n_trav, sc));
-    BinNode* sah_nodes = sc.get<BinNode>(n_trav);
+    BinNode* sah_nodes = nullptr;
+    if (keep_refit) {
+      BB_TRY(dmalloc(out.refit->trav_nodes, n_trav));
+      BB_TRY(dmalloc(out.refit->trav_parent, n_trav));
+      out.refit->trav_count = n_trav;
+      sah_nodes = out.refit->trav_nodes;
+    } else {
+      sah_nodes = sc.get<BinNode>(n_trav);
+    }
     if (sc.err != cudaSuccess) return sc.err;
     BB_TRY(finish_tree(blo, bhi, sah_order, sn, n_trav, sah_nodes, nullptr, nullptr, nullptr, sc));
+    if (keep_refit) k_parents<<<grid_for(n_trav), kThreads, 0, stream>>>(sah_nodes, n_trav, out.refit->trav_parent);
     trav = sah_nodes;
     trav_order = sah_order;
     out.reference_topology = false;
@@ -1359,11 +1592,17 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   WideNode* wide = nullptr;
   BB_TRY(dmalloc(wide, n_trav));
   out.nodes = reinterpret_cast<float4*>(wide);
-  BB_TRY(collapse(trav, n_trav, wide, out.wide_nodes, out.depth, out.stack_required, sc));
+  if (keep_refit) BB_TRY(dmalloc(out.refit->slot_bin, 4ull * n_trav));
+  BB_TRY(collapse(trav, n_trav, wide, out.wide_nodes, out.depth, out.stack_required, sc,
+                  keep_refit ? out.refit->slot_bin : nullptr));
   TriRecord* tris = nullptr;
   BB_TRY(dmalloc(tris, n));
   out.tris = reinterpret_cast<float4*>(tris);
   k_tri_records<<<grid_for(n), kThreads, 0, stream>>>(trav_order, n, pv, ref_leaf, ref_lane, tris);
+  if (keep_refit) {
+    BB_TRY(dmalloc(out.refit->tri_pos, n));
+    k_tri_pos<<<grid_for(n), kThreads, 0, stream>>>(trav_order, n, out.refit->tri_pos);
+  }
   BB_TRY(cudaGetLastError());
   return cudaStreamSynchronize(stream);
 }

@@ -15,6 +15,21 @@
 
 namespace vkptc {
 
+// What a refit after instance transform updates needs, kept on the device
+// when the scene has dynamic-transform instances with local geometry.
+struct DeviceRefitState {
+  float4* blo = nullptr;            // per primitive: padded box
+  float4* bhi = nullptr;
+  uint32_t* tri_pos = nullptr;      // per primitive: its triangle record
+  BinNode* trav_nodes = nullptr;    // the traversal tree when it is not the reference tree (SAH)
+  uint32_t* trav_order = nullptr;
+  int32_t* trav_parent = nullptr;
+  uint32_t trav_count = 0;
+  int32_t* slot_bin = nullptr;      // per wide node: the binary node of each slot (-1 unused)
+  uint32_t* inst_first = nullptr;   // per instance: first flattened primitive (host copy below)
+  std::vector<uint32_t> host_inst_first, host_inst_count;   // per instance: primitive range
+};
+
 struct DeviceAccelOut {
   // Device arrays allocated by the builder with cudaMalloc (caller frees).
   float4* nodes = nullptr;     // WideNode, 8 float4 each
@@ -28,6 +43,7 @@ struct DeviceAccelOut {
   uint32_t wide_nodes = 0, depth = 0, stack_required = 0;
   bool reference_topology = true;
   bool fallback = false;       // non-finite primitive bounds: use the host builder instead
+  DeviceRefitState* refit = nullptr;   // kept for dynamic-instance scenes (owned; FreeDeviceAccel frees)
 };
 
 // The scene's geometry arrays: vertex and index arrays (global and local) in
@@ -53,5 +69,25 @@ struct DeviceSceneArrays {
 cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& scene, bool sah, cudaStream_t stream, DeviceAccelOut& out);
 
 void FreeDeviceAccel(DeviceAccelOut& out);
+void FreeRefitState(DeviceRefitState*& state);
+
+// One instance transform update, resolved to an instance of the scene.
+struct RefitUpdate {
+  uint32_t instance;
+  uint32_t prim_first, prim_count;             // its flattened primitives
+  uint32_t local_first_vertex, local_first_index, material;
+  float transform[10];                         // translation3, quaternion xyzw, scale3
+};
+
+// The refit of CpuBvhAccelerator::apply_instance_transform_update
+// (src/pathtracer/CpuBvhAccelerator.cpp:308-358, 527-606): the updated
+// instances' primitives recomputed from their local geometry, then every node
+// of the reference tree (and of the traversal tree when it differs) refitted
+// bottom-up with its topology unchanged, and the wide nodes' slot bounds and
+// tie records rewritten.  nodes/tris/tie/shade: the accelerator's arrays.
+cudaError_t RefitOnDevice(DeviceRefitState& state, const std::vector<RefitUpdate>& updates, const float* local_vertices,
+                          const uint32_t* local_indices, BinNode* ref_nodes, const uint32_t* ref_order,
+                          uint32_t ref_count, float4* nodes, uint32_t wide_count, float4* tris, float4* tie,
+                          float4* shade, cudaStream_t stream);
 
 }  // namespace vkptc

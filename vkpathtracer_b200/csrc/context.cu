@@ -114,6 +114,11 @@ struct vkptc_ctx {
   uint32_t raw_local_vertex_count = 0, raw_local_index_count = 0;
   std::vector<uint32_t> raw_instance_local;
   std::vector<float> raw_instance_transforms;
+  std::vector<uint32_t> raw_local_indices_host;   // for checking transform updates
+  DeviceRefitState* refit = nullptr;      // device build of a scene with dynamic local geometry
+  BinNode* d_ref_nodes = nullptr;         // its reference tree, kept for refits
+  uint32_t* d_ref_order = nullptr;
+  uint32_t ref_count = 0;
   uint32_t prim_count = 0;                // flattened primitives of the built accelerator
   std::vector<float> materials, lights;
   float env[3] = {0, 0, 0};
@@ -487,6 +492,8 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
   return VKPTC_OK;
 }
 
+void release_refit(vkptc_ctx* c);
+
 int32_t vkptc_destroy(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
@@ -495,6 +502,7 @@ int32_t vkptc_destroy(vkptc_ctx* ctx) {
   for (auto& e : ctx->timer_events) cudaEventDestroy(e);
   if (ctx->ldr_event) cudaEventDestroy(ctx->ldr_event);
   if (ctx->h_ldr) cudaFreeHost(ctx->h_ldr);
+  release_refit(ctx);
   delete ctx;
   if (s) cudaStreamDestroy(s);
   return VKPTC_OK;
@@ -577,6 +585,7 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
     ctx->raw_instances.assign(scene->instances, scene->instances + 3 * static_cast<size_t>(scene->instance_count));
     ctx->raw_instance_local.clear();
     ctx->raw_instance_transforms.clear();
+    ctx->raw_local_indices_host.clear();
     ctx->raw_local_vertex_count = ctx->raw_local_index_count = 0u;
     ctx->d_raw_local_vertices.release();
     ctx->d_raw_local_indices.release();
@@ -594,6 +603,7 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
       if (scene->local_index_count)
         VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_raw_local_indices.ptr, scene->local_indices, 4ull * scene->local_index_count,
                                    cudaMemcpyHostToDevice), "scene upload");
+      ctx->raw_local_indices_host.assign(scene->local_indices, scene->local_indices + scene->local_index_count);
     }
     ctx->geo = SceneGeometry{};
     ctx->geo_ready = false;
@@ -747,6 +757,15 @@ int32_t ensure_geo(vkptc_ctx* c) {
   return VKPTC_OK;
 }
 
+void release_refit(vkptc_ctx* c) {
+  FreeRefitState(c->refit);
+  cudaFree(c->d_ref_nodes);
+  cudaFree(c->d_ref_order);
+  c->d_ref_nodes = nullptr;
+  c->d_ref_order = nullptr;
+  c->ref_count = 0;
+}
+
 // Device build: every array the traversal reads, produced by CUDA kernels
 // (bvh_build.cu).  Returns VKPTC_OK with *done = false when the scene needs
 // the host path (non-finite primitive bounds).
@@ -786,8 +805,17 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
     c->d_tris.adopt(out.tris, 3ull * n);
     c->d_tie.adopt(out.tie, 2ull * out.binary_nodes);
   }
-  cudaFree(out.ref_nodes);
-  cudaFree(out.ref_order);
+  release_refit(c);
+  if (out.refit) {
+    c->refit = out.refit;
+    c->d_ref_nodes = out.ref_nodes;
+    c->d_ref_order = out.ref_order;
+    c->ref_count = out.binary_nodes;
+    out.refit = nullptr;
+  } else {
+    cudaFree(out.ref_nodes);
+    cudaFree(out.ref_order);
+  }
   c->wide = WideBvh{};
   c->wide.binary_nodes = out.binary_nodes;
   c->wide.binary_leaves = out.binary_leaves;
@@ -822,6 +850,7 @@ int32_t vkptc_build_acceleration(vkptc_ctx* ctx) {
       return VKPTC_OK;
     }
   }
+  release_refit(ctx);
   int32_t grc = ensure_geo(ctx);
   if (grc != VKPTC_OK) return grc;
   const auto t0 = std::chrono::steady_clock::now();
@@ -903,6 +932,85 @@ int32_t vkptc_get_accel_info(vkptc_ctx* ctx, vkptc_accel_info* out) {
   return VKPTC_OK;
 }
 
+namespace {
+
+// The checks of a transform update; fills the refit records.
+int32_t check_updates(vkptc_ctx* ctx, const vkptc_instance_update* updates, uint32_t count,
+                      std::vector<RefitUpdate>& ups) {
+  if (count && !updates) return fail(ctx, VKPTC_INVALID_ARGUMENT, "updates is null");
+  if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "transform update before build_or_update_acceleration");
+  const uint32_t ninst = static_cast<uint32_t>(ctx->raw_instances.size() / 3);
+  for (uint32_t u = 0; u < count; ++u) {
+    const uint32_t i = updates[u].instance_index;
+    if (i >= ninst && ctx->geo_ready && ctx->raw_instances.empty())
+      return fail(ctx, VKPTC_UNSUPPORTED, "transform updates need the device build");
+    if (i >= ninst) return fail(ctx, VKPTC_INVALID_ARGUMENT, "transform update references an unknown instance");
+    const uint32_t* loc = ctx->raw_instance_local.empty() ? nullptr : &ctx->raw_instance_local[5 * i];
+    if (!loc || (loc[0] & 1u) == 0u || loc[2] == 0u || loc[4] == 0u)
+      return fail(ctx, VKPTC_UNSUPPORTED, "transform update needs dynamic local geometry metadata");
+    if (!ctx->refit) return fail(ctx, VKPTC_UNSUPPORTED, "transform updates need the device build");
+    // refit_instance_primitives' checks (32-bit index arithmetic)
+    const uint32_t tri_count = ctx->raw_instances[3 * i + 1];
+    if (ctx->refit->host_inst_count[i] != tri_count)
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, "failed while refitting instance primitives");
+    const uint32_t local_end = loc[1] + loc[2];
+    for (uint32_t k = 0; k < tri_count; ++k) {
+      const uint32_t base = loc[3] + k * 3u;
+      if (base >= 0xFFFFFFFEu || base + 2u >= ctx->raw_local_indices_host.size())
+        return fail(ctx, VKPTC_INVALID_ARGUMENT, "failed while refitting instance primitives");
+      for (int j = 0; j < 3; ++j) {
+        const uint32_t v = loc[1] + ctx->raw_local_indices_host[base + j];
+        if (v >= local_end || v >= ctx->raw_local_vertex_count)
+          return fail(ctx, VKPTC_INVALID_ARGUMENT, "failed while refitting instance primitives");
+      }
+    }
+    RefitUpdate r{};
+    r.instance = i;
+    r.prim_first = ctx->refit->host_inst_first[i];
+    r.prim_count = tri_count;
+    r.local_first_vertex = loc[1];
+    r.local_first_index = loc[3];
+    r.material = ctx->raw_instances[3 * i + 2];
+    const vkptc_instance_update& up = updates[u];
+    const float t[10] = {up.translation[0], up.translation[1], up.translation[2], up.rotation[0], up.rotation[1],
+                         up.rotation[2], up.rotation[3], up.scale[0], up.scale[1], up.scale[2]};
+    std::copy(t, t + 10, r.transform);
+    ups.push_back(r);
+  }
+  return VKPTC_OK;
+}
+
+}  // namespace
+
+int32_t vkptc_check_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_update* updates, uint32_t count) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  std::vector<RefitUpdate> ups;
+  const int32_t rc = check_updates(ctx, updates, count, ups);
+  if (rc == VKPTC_OK) ctx->last_error.clear();
+  return rc;
+}
+
+int32_t vkptc_update_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_update* updates, uint32_t count) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  std::vector<RefitUpdate> ups;
+  const int32_t rc = check_updates(ctx, updates, count, ups);
+  if (rc != VKPTC_OK) return rc;
+  cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, RefitOnDevice(*ctx->refit, ups, ctx->d_raw_local_vertices.ptr, ctx->d_raw_local_indices.ptr,
+                                ctx->d_ref_nodes, ctx->d_ref_order, ctx->ref_count, ctx->d_nodes.ptr,
+                                ctx->accel.wide_node_count, ctx->d_tris.ptr, ctx->d_tie.ptr, ctx->d_shade.ptr,
+                                ctx->stream), "instance refit");
+  // the scene metadata follows (ApplyInstanceTransformUpdates, metadata only)
+  for (uint32_t u = 0; u < count; ++u) {
+    const uint32_t i = updates[u].instance_index;
+    ctx->raw_instance_local[5 * i] |= updates[u].flags;
+    std::copy(ups[u].transform, ups[u].transform + 10, ctx->raw_instance_transforms.begin() + 10 * i);
+  }
+  ctx->geo_ready = false;   // a host flatten (external BVH) must use the new transforms
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
 int32_t vkptc_read_accel(vkptc_ctx* ctx, uint32_t what, void* out, uint64_t capacity, uint64_t* bytes) {
   if (!ctx || !bytes) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->accel_valid) return fail(ctx, VKPTC_NOT_READY, "acceleration structure not built");
@@ -966,6 +1074,8 @@ int32_t vkptc_shutdown(vkptc_ctx* ctx) {
   ctx->d_raw_local_indices.release();
   ctx->raw_instance_local.clear();
   ctx->raw_instance_transforms.clear();
+  ctx->raw_local_indices_host.clear();
+  release_refit(ctx);
   ctx->prim_count = 0;
   ctx->wide = WideBvh{};
   ctx->d_nodes.release();

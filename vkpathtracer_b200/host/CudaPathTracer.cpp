@@ -2,6 +2,7 @@
 #include "CudaPathTracer.h"
 
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "vkptc.h"
@@ -171,6 +172,8 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
     v.local_indices = scene.local_indices.data();
     v.local_index_count = static_cast<uint32_t>(scene.local_indices.size());
   }
+  m_instance_entities.clear();
+  for (const auto& r : scene.instances) m_instance_entities.push_back(r.entity_id);
   const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
   if (st) m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
   return st;
@@ -281,6 +284,86 @@ pt::FilmLdr CudaPathTracer::resolve_ldr() const {
     return pt::FilmLdr{};
   }
   return out;
+}
+
+namespace {
+
+// RTInstanceTransformUpdate -> the C ABI record; the instance resolved by index, else by entity id
+// (resolve_instance_index, src/pathtracer/CpuBvhAccelerator.cpp:507-525).
+bool resolve_updates(std::span<const pt::RTInstanceTransformUpdate> updates,
+                     const std::vector<vkpt::core::StableId>& entities, std::vector<vkptc_instance_update>& out) {
+  out.clear();
+  for (const auto& u : updates) {
+    uint32_t index = u.instance_index;
+    if (index >= entities.size() && u.entity_id != 0u) {
+      for (size_t i = 0; i < entities.size(); ++i) {
+        if (entities[i] == u.entity_id) {
+          index = static_cast<uint32_t>(i);
+          break;
+        }
+      }
+    }
+    if (index >= entities.size()) return false;
+    vkptc_instance_update r{};
+    r.instance_index = index;
+    r.flags = u.flags;
+    r.translation[0] = u.translation.x;
+    r.translation[1] = u.translation.y;
+    r.translation[2] = u.translation.z;
+    r.rotation[0] = u.rotation.x;
+    r.rotation[1] = u.rotation.y;
+    r.rotation[2] = u.rotation.z;
+    r.rotation[3] = u.rotation.w;
+    r.scale[0] = u.scale.x;
+    r.scale[1] = u.scale.y;
+    r.scale[2] = u.scale.z;
+    out.push_back(r);
+  }
+  return true;
+}
+
+pt::InstanceTransformUpdateStatus status_of(int32_t rc) {
+  if (rc == VKPTC_OK) return pt::InstanceTransformUpdateStatus::AppliedDynamicAccelUpdate;
+  if (rc == VKPTC_UNSUPPORTED) return pt::InstanceTransformUpdateStatus::BlockedNeedsFullStaticAccelRebuild;
+  return pt::InstanceTransformUpdateStatus::Failed;
+}
+
+}  // namespace
+
+pt::InstanceTransformPlan CudaPathTracer::plan_instance_transform_update(
+    std::span<const pt::RTInstanceTransformUpdate> updates, const pt::InstanceTransformUpdateOptions&) const {
+  const uint32_t n = static_cast<uint32_t>(updates.size());
+  std::vector<vkptc_instance_update> ups;
+  if (!m_ctx || !resolve_updates(updates, m_instance_entities, ups))
+    return {pt::InstanceTransformUpdateStatus::Failed, n, 0u, "transform update references an unknown instance"};
+  const int32_t rc = vkptc_check_instance_transforms(m_ctx, ups.data(), n);
+  m_last_error = rc == VKPTC_OK ? "" : vkptc_last_error(m_ctx);
+  return {status_of(rc), n, rc == VKPTC_OK ? n : 0u,
+          rc == VKPTC_OK ? "cuda backend refits dynamic instance transforms on the device" : m_last_error.c_str()};
+}
+
+pt::InstanceTransformUpdateResult CudaPathTracer::apply_instance_transform_update(
+    std::span<const pt::RTInstanceTransformUpdate> updates, const pt::InstanceTransformUpdateOptions&) {
+  const uint32_t n = static_cast<uint32_t>(updates.size());
+  std::vector<vkptc_instance_update> ups;
+  if (!m_ctx || !resolve_updates(updates, m_instance_entities, ups)) {
+    m_last_error = "transform update references an unknown instance";
+    return {pt::InstanceTransformUpdateStatus::Failed, n, 0u, 0.0, 0.0, 0.0, 0.0, m_last_error.c_str()};
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  const int32_t rc = vkptc_update_instance_transforms(m_ctx, ups.data(), n);
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (rc != VKPTC_OK) {
+    m_last_error = vkptc_last_error(m_ctx);
+    return {status_of(rc), n, 0u, 0.0, 0.0, 0.0, 0.0, m_last_error.c_str()};
+  }
+  m_last_error.clear();
+  return {pt::InstanceTransformUpdateStatus::AppliedDynamicAccelUpdate, n, n, 0.0, 0.0, ms, 0.0,
+          "cuda backend refit dynamic instance transforms"};
+}
+
+bool CudaPathTracer::update_instance_transforms(const std::vector<pt::RTInstanceTransformUpdate>& updates) {
+  return apply_instance_transform_update(updates, pt::InstanceTransformUpdateOptions{}).applied();
 }
 
 pt::FilmReadbackToken CudaPathTracer::request_film_readback() {

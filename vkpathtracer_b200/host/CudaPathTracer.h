@@ -51,6 +51,13 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   bool supports_tile_batching() const override { return true; }
   vkpt::pathtracer::FilmLdr resolve_ldr() const override;
   vkpt::pathtracer::FilmReadbackToken request_film_readback() override;
+  bool update_instance_transforms(const std::vector<vkpt::pathtracer::RTInstanceTransformUpdate>& updates) override;
+  vkpt::pathtracer::InstanceTransformPlan plan_instance_transform_update(
+      std::span<const vkpt::pathtracer::RTInstanceTransformUpdate> updates,
+      const vkpt::pathtracer::InstanceTransformUpdateOptions& options) const override;
+  vkpt::pathtracer::InstanceTransformUpdateResult apply_instance_transform_update(
+      std::span<const vkpt::pathtracer::RTInstanceTransformUpdate> updates,
+      const vkpt::pathtracer::InstanceTransformUpdateOptions& options) override;
   vkpt::pathtracer::FilmReadbackResult poll_film(vkpt::pathtracer::FilmReadbackToken token) override;
   vkpt::pathtracer::FilmHdr resolve_hdr() const override;
   vkpt::pathtracer::SampleCounters read_counters() const override;
@@ -67,6 +74,7 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   vkpt::pathtracer::FilmResolveSettings m_resolve{};
   mutable vkpt::pathtracer::FilmBuffer m_film;
   mutable std::string m_last_error;
+  std::vector<vkpt::core::StableId> m_instance_entities;   // entity id per instance (update resolution)
 };
 
 }  // namespace vkpt::gpu::cuda

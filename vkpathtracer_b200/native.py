@@ -62,6 +62,11 @@ class SceneView(ctypes.Structure):
 SDF_SPHERE, SDF_BOX, SDF_ROUNDED_BOX, SDF_PLANE, SDF_TORUS, SDF_CAPSULE = range(6)
 
 
+class InstanceUpdate(ctypes.Structure):
+    _fields_ = [("instance_index", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("translation", ctypes.c_float * 3),
+                ("rotation", ctypes.c_float * 4), ("scale", ctypes.c_float * 3)]
+
+
 class FilmResolve(ctypes.Structure):
     _fields_ = [("exposure", ctypes.c_float), ("white_balance_kelvin", ctypes.c_float), ("tone_map", ctypes.c_uint32),
                 ("output_transform", ctypes.c_uint32), ("gamma", ctypes.c_float), ("clamp_output", ctypes.c_uint32)]
@@ -167,6 +172,8 @@ SIGNATURES = {
     "vkptc_get_accel_info": (I32, [P, ctypes.POINTER(AccelInfo)]),
     "vkptc_read_accel": (I32, [P, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_resolve_ldr": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.c_void_p]),
+    "vkptc_update_instance_transforms": (I32, [P, ctypes.c_void_p, ctypes.c_uint32]),
+    "vkptc_check_instance_transforms": (I32, [P, ctypes.c_void_p, ctypes.c_uint32]),
     "vkptc_request_ldr_readback": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_poll_ldr_readback": (I32, [P, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),

@@ -207,6 +207,19 @@ class CudaPathTracer:
         self._check(self._lib.vkptc_get_accel_info(self._ctx, ctypes.byref(a)))
         return a.as_dict()
 
+    def update_instance_transforms(self, updates, check_only: bool = False):
+        """Instance transform updates ({"instance", "translation", "rotation",
+        "scale", "flags"}), refitted on the device (apply_instance_transform_update)."""
+        arr = (native.InstanceUpdate * max(1, len(updates)))()
+        for k, u in enumerate(updates):
+            arr[k].instance_index = u["instance"]
+            arr[k].flags = u.get("flags", 0)
+            arr[k].translation[:] = u.get("translation", (0.0, 0.0, 0.0))
+            arr[k].rotation[:] = u.get("rotation", (0.0, 0.0, 0.0, 1.0))
+            arr[k].scale[:] = u.get("scale", (1.0, 1.0, 1.0))
+        fn = self._lib.vkptc_check_instance_transforms if check_only else self._lib.vkptc_update_instance_transforms
+        self._check(fn(self._ctx, ctypes.cast(arr, ctypes.c_void_p), len(updates)))
+
     @staticmethod
     def film_resolve(exposure: float = 1.0, white_balance_kelvin: float = 6500.0, tone_map: str = "linear",
                      output_transform: str = "gamma", gamma: float = 2.2, clamp_output: bool = True):
