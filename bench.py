@@ -313,6 +313,30 @@ def bvh_build(device, cpu: bool = True):
                 ms.append(1e3 * (time.perf_counter() - t0))
             out[f"{build}_{bvh}_ms"] = min(ms)
     out["device_sah_triangles_per_s"] = n / (out["device_sah_ms"] / 1e3)
+    # moving objects: 4096 dynamic instances of one local mesh; every instance moved per frame,
+    # refit (apply_instance_transform_update) against a full rebuild of the moved scene
+    dyn = scenes.dynamic_sphere_field()
+    with CudaPathTracer(device=device, bvh="sah") as t:
+        t.configure(st)
+        t.load_scene_snapshot(dyn)
+        t.build_or_update_acceleration()
+        ids = [i for i in range(dyn.instances.shape[0]) if dyn.instance_local[i, 0] & 1]
+        ms = []
+        for k in range(6):
+            ups = [{"instance": i, "translation": (float(dyn.instance_transforms[i, 0]),
+                                                   float(dyn.instance_transforms[i, 1]) + 0.1 * (k + 1),
+                                                   float(dyn.instance_transforms[i, 2])),
+                    "rotation": tuple(float(x) for x in dyn.instance_transforms[i, 3:7]),
+                    "scale": tuple(float(x) for x in dyn.instance_transforms[i, 7:10])} for i in ids]
+            t0 = time.perf_counter()
+            t.update_instance_transforms(ups)
+            ms.append(1e3 * (time.perf_counter() - t0))
+        t0 = time.perf_counter()
+        t.build_or_update_acceleration()
+        rebuild = 1e3 * (time.perf_counter() - t0)
+    out["dynamic_refit"] = {"workload": "dynamic_sphere_field_64: 4096 instances of one 504-triangle local mesh, "
+                                        "every instance moved", "triangles": dyn.triangle_count,
+                            "refit_ms": float(np.median(ms)), "device_rebuild_ms": rebuild}
     out["speedup_device_vs_host_reference_tree"] = out["host_reference_ms"] / out["device_reference_ms"]
     if cpu:
         import oracle

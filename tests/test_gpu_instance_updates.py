@@ -115,3 +115,20 @@ def test_rejected_updates():
         with pytest.raises(native.VkptcError) as e:
             t.update_instance_transforms(make_updates(sc))
         assert e.value.code == native.UNSUPPORTED
+
+
+def test_dynamic_field_refit_matches_reference():
+    """Many instances of one local mesh (rotated, scaled), all moved."""
+    from vkpathtracer_b200 import scenes
+    sc = scenes.dynamic_sphere_field(grid=8)
+    st = scenes.RenderSettings(width=96, height=64, spp=4, max_depth=6, seed=11)
+    ups = cases.transform_updates(sc, count=64)
+    ref = oracle.load("auto").render(sc, st, per_sample=True, updates=ups)
+    with tracer(sc, st, "sah") as t:
+        t.update_instance_transforms(ups)
+        t.render_frame(0, st.spp)
+        g, cnt, _ = t.film()
+    rmse, fail, exact = report(g, ref["sum"], ref["samples"], st.spp)
+    print("dynamic field rmse", rmse, "3sigma", fail, "bit-exact", exact)
+    assert np.array_equal(cnt, ref["count"])
+    assert rmse < RMSE_REL_TOL and fail < SIGMA3_FAIL_FRAC and exact >= BIT_EXACT_FRAC

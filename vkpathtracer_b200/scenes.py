@@ -615,6 +615,46 @@ def sphere_field(grid: int, n_lat: int, n_lon: int, seed: int, spacing: float = 
                  (environment, environment, environment), cam, f"sphere_field_{grid}").contiguous()
 
 
+def dynamic_sphere_field(grid: int = 64, n_lat: int = 15, n_lon: int = 18, seed: int = 4) -> Scene:
+    """The sphere field as dynamic-transform instances: every sphere is an
+    instance of one local mesh (a displaced unit sphere) with its own
+    translation, rotation and scale, as the reference's scene conversion emits
+    physics-driven entities; a static ground plane.  grid 64: 4096 instances,
+    2,064,384 sphere triangles."""
+    st = Stream(seed)
+    dirs, tris = _displaced_unit_sphere_mesh(n_lat, n_lon, 0.05, seed * 17)
+    nt = tris.shape[0]
+    spacing, half = 3.0, 0.5 * (grid - 1) * 3.0
+    mats, inst, inst_local, inst_tr = [], [], [], []
+    for gy in range(grid):
+        for gx in range(grid):
+            r = st.uniform(0.7, 1.0)
+            a = st.uniform(0.0, 2.0 * math.pi)
+            t = (gx * spacing - half, r, gy * spacing - half)
+            mats.append(material(albedo=tuple(st.uniform(0.05, 0.9) for _ in range(3)),
+                                 roughness=(1.0, 0.3, 0.0)[st.randint(0, 2)], model=(0, 3, 2)[st.randint(0, 2)]))
+            inst.append((len(inst) * nt, nt, len(mats) - 1))
+            inst_local.append((1, 0, dirs.shape[0], 0, 3 * nt))
+            inst_tr.append(t + (0.0, math.sin(a / 2), 0.0, math.cos(a / 2)) + (r, r, r))
+    # global arrays: the world-space copies (used only where a local index is out of range)
+    glob_v = np.concatenate([dirs * tr[7] + np.array(tr[0:3]) for tr in inst_tr]).astype(np.float32)
+    glob_t = np.concatenate([tris + k * dirs.shape[0] for k in range(len(inst_tr))]).astype(np.uint32)
+    mats.append(material(albedo=(0.5, 0.5, 0.5), roughness=1.0))
+    g = half + 6.0
+    gv, gt = _quad((-g, 0.0, -g), (-g, 0.0, g), (g, 0.0, g), (g, 0.0, -g))
+    inst.append((glob_t.shape[0], gt.shape[0], len(mats) - 1))
+    inst_local.append((0, 0, 0, 0, 0))
+    inst_tr.append((0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0))
+    v = np.concatenate([glob_v, np.asarray(gv, np.float32)])
+    t = np.concatenate([glob_t, np.asarray(gt, np.uint32) + glob_v.shape[0]])
+    lights = [point_light((0.0, 14.0, 0.0), (1.0, 0.95, 0.9), 400.0)]
+    cam = Camera(position=(0.0, 0.55 * half + 6.0, 1.45 * half), target=(0.0, 0.0, 0.1 * half), fov_deg=50.0)
+    return Scene(v, t, np.array(inst, np.uint32), np.array(mats), np.array(lights), (0.1, 0.1, 0.1), cam,
+                 f"dynamic_sphere_field_{grid}", instance_local=np.array(inst_local, np.uint32),
+                 instance_transforms=np.array(inst_tr, np.float32), local_vertices=dirs.astype(np.float32),
+                 local_indices=tris.astype(np.uint32).reshape(-1)).contiguous()
+
+
 def sky_map(width: int = 128, height: int = 64, seed: int = 2, sun_dir=(0.4, 0.55, -0.73),
             sun_radiance: float = 40.0) -> np.ndarray:
     """Equirectangular sky, (height, width, 3) float32, row 0 toward +y, in the
