@@ -441,6 +441,9 @@ int32_t vkptc_batch_add_job(vkptc_batch* batch, const vkptc_scene_view* scene, c
 /* Clears every film, then renders samples [0, spp) (or sample_limit) of every job. */
 int32_t vkptc_batch_run(vkptc_batch* batch, uint32_t mode, const vkptc_batch_tuning* tuning);
 int32_t vkptc_batch_read_film(vkptc_batch* batch, uint32_t job_id, float* sum_rgb, uint32_t* count);
+/* Every job's film in one go: sums[j] (3*W*H floats) and counts[j] (W*H), either may be NULL per job;
+ * the copies are queued back to back and waited for once (pinned destinations copy fastest). */
+int32_t vkptc_batch_read_films(vkptc_batch* batch, float* const* sums, uint32_t* const* counts);
 int32_t vkptc_batch_get_stats(vkptc_batch* batch, vkptc_batch_stats* out);
 const char* vkptc_batch_last_error(vkptc_batch* batch);
 

@@ -163,3 +163,16 @@ def test_sdf_jobs_equal_across_drivers_and_match_oracle():
         exact = np.mean(np.all(bits(got) == bits(ref), axis=1))
         rel = np.sqrt(np.mean((got - ref) ** 2)) / (np.mean(ref) + 1e-9)
         assert exact >= 0.95 and rel < 1e-3, (sc.name, exact, rel)
+
+
+def test_read_films_equals_per_job_reads(batch):
+    """vkptc_batch_read_films (all jobs, one wait) returns what the per-job
+    reads return."""
+    n = len(small_jobs())
+    batch.run("loop")
+    ref = films(batch, n)
+    sums = [np.zeros_like(f) for f, _ in ref]
+    counts = [np.zeros_like(c) for _, c in ref]
+    batch.read_films(sums, counts)
+    for (f, c), s, k in zip(ref, sums, counts):
+        assert np.array_equal(bits(f), bits(s)) and np.array_equal(c, k)

@@ -137,6 +137,7 @@ struct vkptc_ctx {
   WideBvh wide;
   vkptc_accel_info accel{};
 
+  DevBuf<float> d_pack;                   // film sums packed to rgb for host readback
   // split LDR readback (request / poll)
   DevBuf<uint8_t> d_ldr;
   uint8_t* h_ldr = nullptr;               // pinned, 4 bytes per pixel
@@ -1163,22 +1164,29 @@ int32_t vkptc_synchronize(vkptc_ctx* ctx) {
   return check_device_error(ctx);
 }
 
+// Queues the copies of a film to host memory on `stream`: the sums packed to
+// rgb on the device, then copied straight into the caller's buffer.
+static int32_t enqueue_film_read(vkptc_ctx* ctx, cudaStream_t stream, float* sum_rgb, uint32_t* count) {
+  const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
+  if (sum_rgb && px) {
+    VKPTC_CUDA(ctx, ctx->d_pack.alloc(3 * px), "film read");
+    VKPTC_CUDA(ctx, LaunchPackFilm(film_of(ctx), ctx->d_pack.ptr, stream), "film read");
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(sum_rgb, ctx->d_pack.ptr, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, stream),
+               "film read");
+  }
+  if (count && px)
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(count, ctx->d_film_count.ptr, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
+               "film read");
+  return VKPTC_OK;
+}
+
 int32_t vkptc_read_film(vkptc_ctx* ctx, float* sum_rgb, uint32_t* count, float* invalid) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "film not configured");
   cudaSetDevice(ctx->device);
+  const int32_t rc = enqueue_film_read(ctx, ctx->stream, sum_rgb, count);
+  if (rc != VKPTC_OK) return rc;
   const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
-  if (sum_rgb) {
-    std::vector<float4> tmp(px);
-    VKPTC_CUDA(ctx, cudaMemcpyAsync(tmp.data(), ctx->d_film_sum.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream), "film read");
-    VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "film read");
-    for (size_t i = 0; i < px; ++i) {
-      sum_rgb[3 * i] = tmp[i].x;
-      sum_rgb[3 * i + 1] = tmp[i].y;
-      sum_rgb[3 * i + 2] = tmp[i].z;
-    }
-  }
-  if (count) VKPTC_CUDA(ctx, cudaMemcpyAsync(count, ctx->d_film_count.ptr, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream), "film read");
   if (invalid) VKPTC_CUDA(ctx, cudaMemcpyAsync(invalid, ctx->d_film_invalid.ptr, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream), "film read");
   VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "film read");
   return VKPTC_OK;
@@ -1953,6 +1961,22 @@ int32_t vkptc_batch_read_film(vkptc_batch* b, uint32_t job_id, float* sum_rgb, u
   const int32_t rc = vkptc_read_film(b->jobs[job_id], sum_rgb, count, nullptr);
   if (rc != VKPTC_OK) b->last_error = b->jobs[job_id]->last_error;
   return rc;
+}
+
+int32_t vkptc_batch_read_films(vkptc_batch* b, float* const* sums, uint32_t* const* counts) {
+  if (!b) return VKPTC_INVALID_ARGUMENT;
+  cudaSetDevice(b->device);
+  for (size_t j = 0; j < b->jobs.size(); ++j) {
+    vkptc_ctx* c = b->jobs[j];
+    const int32_t rc = enqueue_film_read(c, b->stream, sums ? sums[j] : nullptr, counts ? counts[j] : nullptr);
+    if (rc != VKPTC_OK) {
+      b->last_error = c->last_error;
+      return rc;
+    }
+  }
+  VKPTC_BCUDA(b, cudaStreamSynchronize(b->stream), "film read");
+  b->last_error.clear();
+  return VKPTC_OK;
 }
 
 int32_t vkptc_batch_get_stats(vkptc_batch* b, vkptc_batch_stats* out) {

@@ -458,6 +458,23 @@ __global__ void k_resolve_hdr(Film film, float* out) {
   }
 }
 
+__global__ void k_pack_film(const float4* __restrict__ sum, size_t npx, float* __restrict__ out) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npx;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float4 v = sum[i];
+    out[3 * i + 0] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+  }
+}
+
+cudaError_t LaunchPackFilm(const Film& film, float* rgb_out, cudaStream_t stream) {
+  const size_t npx = static_cast<size_t>(film.width) * film.height;
+  const int grid = static_cast<int>(std::min<size_t>(8192, std::max<size_t>(1, (npx + 255) / 256)));
+  k_pack_film<<<grid, 256, 0, stream>>>(film.sum, npx, rgb_out);
+  return cudaGetLastError();
+}
+
 // ApplyFilmResolve (src/pathtracer/FilmBuffer.cpp:253-325) per pixel, on the
 // film's per-pixel mean: exposure then white balance, non-finite to 0, tone
 // map, gamma (pow, FP64 rounded once in parity mode), clamp, and the x86

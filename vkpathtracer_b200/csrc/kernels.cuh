@@ -100,6 +100,8 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
 
 // Film helpers.
 cudaError_t LaunchResolveHdr(const Film& film, float* rgb_out, cudaStream_t stream);
+// The film's rgb sums packed to 3 floats per pixel (for host readback).
+cudaError_t LaunchPackFilm(const Film& film, float* rgb_out, cudaStream_t stream);
 
 // ApplyFilmResolve on the device; wb: the white-balance scale (host-computed).
 struct LdrResolve {

@@ -173,6 +173,7 @@ SIGNATURES = {
     "vkptc_read_accel": (I32, [P, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_resolve_ldr": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.c_void_p]),
     "vkptc_update_instance_transforms": (I32, [P, ctypes.c_void_p, ctypes.c_uint32]),
+    "vkptc_batch_read_films": (I32, [P, ctypes.c_void_p, ctypes.c_void_p]),
     "vkptc_check_instance_transforms": (I32, [P, ctypes.c_void_p, ctypes.c_uint32]),
     "vkptc_request_ldr_readback": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_poll_ldr_readback": (I32, [P, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),

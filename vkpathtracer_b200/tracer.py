@@ -513,6 +513,18 @@ class BatchRenderer:
         self._lib.vkptc_batch_get_stats(self._b, ctypes.byref(st))
         return st.as_dict()
 
+    def read_films(self, sums, counts=None):
+        """Every job's film into caller-owned arrays (sums[j]: (H, W, 3) float32,
+        counts[j]: (H, W) uint32 or None), one wait for all copies."""
+        n = len(self.settings)
+        ps = (ctypes.c_void_p * max(1, n))(*[s.ctypes.data if s is not None else None for s in sums])
+        pc = None
+        if counts is not None:
+            pc = (ctypes.c_void_p * max(1, n))(*[c.ctypes.data if c is not None else None for c in counts])
+        rc = self._lib.vkptc_batch_read_films(self._b, ps, pc)
+        if rc != native.OK:
+            raise native.VkptcError(rc, self._err())
+
     def film(self, job: int):
         st = self.settings[job]
         s = np.zeros((st.height, st.width, 3), np.float32)
