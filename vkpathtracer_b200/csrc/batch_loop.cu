@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(256) k_lp_sdf_shadow(const DevJob* __restrict_
 }
 
 template <bool kParity, bool kEffects>
-__global__ void __launch_bounds__(256) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr,
+__global__ void __launch_bounds__(256, 3) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr,
                                                   uint32_t sdf_staged) {
   const uint32_t cur = P.ctl[kLCur];
   const uint32_t n = P.ctl[kLCount0 + cur];

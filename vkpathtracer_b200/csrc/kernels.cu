@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_
 constexpr uint32_t kSmemLights = 64;   // lights staged in shared memory by the shade stage
 
 template <bool kParity, bool kEffects>
-__global__ void __launch_bounds__(256) k_shade(DevScene s, DevSettings st, WaveState w, uint32_t cur,
+__global__ void __launch_bounds__(256, 3) k_shade(DevScene s, DevSettings st, WaveState w, uint32_t cur,
                                                uint32_t depth, DevCounters* ctr) {
   __shared__ float sm_lights[16 * kSmemLights];
   const bool staged = s.light_count <= kSmemLights;
