@@ -148,6 +148,18 @@ typedef struct vkptc_scene_view {
   uint32_t local_vertex_count;
   const uint32_t* local_indices;
   uint32_t local_index_count;
+  /* Lens shape of the thin-lens camera (PathTracerSceneSnapshot camera_iris_blade_count,
+   * camera_iris_rotation_degrees, camera_iris_roundness, camera_anamorphic_squeeze,
+   * src/pathtracer/PathTracer.h:405-408), sampled as ScalarCpuPathTracer::camera_rays does
+   * (src/pathtracer/ScalarCpuPathTracer.Render.cpp:88-116): 3..64 blades with roundness below
+   * 0.999 give a polygonal aperture, the squeeze scales the lens offset along the camera's right
+   * axis.  camera_lens_set = 0: the snapshot's defaults (no blades, rotation 0, roundness 1,
+   * squeeze 1), whatever the four fields hold. */
+  uint32_t camera_lens_set;
+  uint32_t camera_iris_blade_count;
+  float camera_iris_rotation_degrees;
+  float camera_iris_roundness;
+  float camera_anamorphic_squeeze;
 } vkptc_scene_view;
 
 /* SdfShape (src/pathtracer/PathTracer.h:232-240). */
@@ -258,6 +270,60 @@ int32_t vkptc_update_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_up
 /* replaces IPathTracer::plan_instance_transform_update (src/pathtracer/PathTracer.h:1115-1122): the
  * same checks and return codes as vkptc_update_instance_transforms, nothing applied. */
 int32_t vkptc_check_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_update* updates, uint32_t count);
+
+/* The fields of RTCameraState (src/pathtracer/PathTracer.h:418-437) that the render reads; the
+ * exposure fields (f-stop, shutter, ISO, compensation, white balance) only change the film resolve
+ * settings, which the caller passes to vkptc_resolve_ldr. */
+typedef struct vkptc_camera {
+  float position[3];
+  float target[3];
+  float up[3];
+  float fov_deg;
+  float aperture_radius;       /* > 0: overrides vkptc_render_settings.camera_aperture_radius */
+  float focus_distance;        /* > 0: overrides vkptc_render_settings.camera_focus_distance */
+  uint32_t iris_blade_count;
+  float iris_rotation_degrees;
+  float iris_roundness;
+  float anamorphic_squeeze;
+} vkptc_camera;
+/* replaces IPathTracer::update_camera_state (src/pathtracer/PathTracer.h:1105) as
+ * ScalarCpuPathTracer implements it (src/pathtracer/ScalarCpuPathTracer.cpp:535-546, ApplyCameraState,
+ * src/pathtracer/PathTracer.cpp:343-362): the camera of the loaded scene is replaced, the next render
+ * uses it; no acceleration rebuild, the film is not reset (vkptc_reset does that).  VKPTC_NOT_READY
+ * before a scene is loaded. */
+int32_t vkptc_update_camera(vkptc_ctx* ctx, const vkptc_camera* camera);
+/* The loaded scene's camera (ExtractCameraState, src/pathtracer/PathTracer.cpp:320-341), for a caller
+ * that changes only some fields (IPathTracer::update_camera, src/pathtracer/PathTracer.h:1102). */
+int32_t vkptc_get_camera(vkptc_ctx* ctx, vkptc_camera* out);
+
+/* RTSceneDeltaUpdate (src/pathtracer/PathTracer.h:439-461) with its instance references resolved to
+ * instance indices: replacement material records (16 floats each, the layout of
+ * vkptc_scene_view.materials), replacement light records (16 floats each), new material indices of
+ * instances, and optionally a new constant environment colour. */
+typedef struct vkptc_scene_delta {
+  const uint32_t* material_indices;
+  const float* materials;
+  uint32_t material_count;
+  const uint32_t* light_indices;
+  const float* lights;
+  uint32_t light_count;
+  const uint32_t* instance_indices;
+  const uint32_t* instance_material_indices;
+  uint32_t instance_material_count;
+  uint32_t environment_changed;
+  float environment[3];
+} vkptc_scene_delta;
+/* replaces IPathTracer::update_scene_delta (src/pathtracer/PathTracer.h:1141) with
+ * ApplySceneDeltaUpdate's rules (src/pathtracer/PathTracer.cpp:427-483): every index is checked
+ * before anything is applied (a material or light index past the scene's tables, an instance index
+ * past its instances or an instance material past the materials: VKPTC_INVALID_ARGUMENT, nothing
+ * changed); records are replaced in order, so the last of two updates of one index wins; a delta that
+ * changes nothing (empty, or only instance materials already set) is VKPTC_INVALID_ARGUMENT as the
+ * reference's false.  Instance material changes rewrite the material of the instance's primitives in
+ * the built accelerator at once (as the GPU backends do, src/gpu/D3D12GpuPathTracer.Scene.cpp:614-624)
+ * and are kept for later builds.  No acceleration rebuild; the film is not reset.  A context set up
+ * for differentiable rendering must be set up again (vkptc_adjoint_setup) after a delta. */
+int32_t vkptc_update_scene_delta(vkptc_ctx* ctx, const vkptc_scene_delta* delta);
 /* Extension (no reference counterpart): copies one device array of the built
  * accelerator to host memory, for inspection and for checking the device
  * build against the host build.  what: VKPTC_ACCEL_WIDE_NODES (128 B each),

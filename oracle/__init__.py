@@ -56,6 +56,11 @@ class VkoScene(ctypes.Structure):
         ("local_vertex_count", ctypes.c_uint32),
         ("local_indices", ctypes.c_void_p),
         ("local_index_count", ctypes.c_uint32),
+        ("camera_lens_set", ctypes.c_uint32),
+        ("camera_iris_blade_count", ctypes.c_uint32),
+        ("camera_iris_rotation_degrees", ctypes.c_float),
+        ("camera_iris_roundness", ctypes.c_float),
+        ("camera_anamorphic_squeeze", ctypes.c_float),
     ]
 
 
@@ -166,6 +171,11 @@ class Oracle:
         s.camera_fov_deg = c.fov_deg
         s.camera_aperture_radius = c.aperture_radius
         s.camera_focus_distance = c.focus_distance
+        s.camera_lens_set = 1
+        s.camera_iris_blade_count = int(getattr(c, "iris_blade_count", 0))
+        s.camera_iris_rotation_degrees = float(getattr(c, "iris_rotation_degrees", 0.0))
+        s.camera_iris_roundness = float(getattr(c, "iris_roundness", 1.0))
+        s.camera_anamorphic_squeeze = float(getattr(c, "anamorphic_squeeze", 1.0))
         env = getattr(scene, "env_map", None)
         if env is not None:
             env = np.ascontiguousarray(env, np.float32)

@@ -165,6 +165,8 @@ struct World {
   double tan_half = 0.0;
   float fov = 60.0f;
   double aperture = 0.0, focus = 0.0;
+  uint32_t iris_blades = 0u;                 // lens shape (camera_rays' polygonal aperture)
+  double iris_rotation = 0.0, iris_roundness = 1.0, squeeze = 1.0;
 
   bool hit(P3 o, P3 d, double tmax, double& t_out, int& idx) const {
     double best = tmax;
@@ -282,10 +284,20 @@ V trace_path(const World& w, const Cfg& c, uint32_t x, uint32_t y, uint32_t samp
   if (w.aperture > 0.0 && w.focus > kEps) {
     const double lr = std::sqrt(static_cast<double>(crng.u()));
     const double lphi = 2.0 * kPi * crng.u();
-    const double rr = w.aperture * lr;
-    const P3 off{w.cam_right.x * rr * std::cos(lphi) + w.cam_up.x * rr * std::sin(lphi),
-                 w.cam_right.y * rr * std::cos(lphi) + w.cam_up.y * rr * std::sin(lphi),
-                 w.cam_right.z * rr * std::cos(lphi) + w.cam_up.z * rr * std::sin(lphi)};
+    double boundary = 1.0;
+    if (w.iris_blades >= 3u && w.iris_roundness < 0.999) {
+      const double sector = 2.0 * kPi / static_cast<double>(w.iris_blades);
+      const double local_phi = lphi - w.iris_rotation;
+      const double wrapped = local_phi - sector * std::floor(local_phi / sector);
+      const double centered = wrapped > sector * 0.5 ? wrapped - sector : wrapped;
+      const double polygon = std::cos(sector * 0.5) / std::max(0.1, std::cos(centered));
+      boundary = polygon * (1.0 - w.iris_roundness) + w.iris_roundness;
+    }
+    const double rr = w.aperture * lr * boundary;
+    const double rs = rr * w.squeeze;
+    const P3 off{w.cam_right.x * rs * std::cos(lphi) + w.cam_up.x * rr * std::sin(lphi),
+                 w.cam_right.y * rs * std::cos(lphi) + w.cam_up.y * rr * std::sin(lphi),
+                 w.cam_right.z * rs * std::cos(lphi) + w.cam_up.z * rr * std::sin(lphi)};
     const P3 fp{w.cam_pos.x + dir.x * w.focus, w.cam_pos.y + dir.y * w.focus, w.cam_pos.z + dir.z * w.focus};
     org = {w.cam_pos.x + off.x, w.cam_pos.y + off.y, w.cam_pos.z + off.z};
     dir = punit(psub(fp, org));
@@ -495,6 +507,13 @@ bool load_world(const vko_scene& s, const float* params, const float* rr_params,
   w.tan_half = std::tan(0.5 * (static_cast<double>(s.camera_fov_deg) * (kPi / 180.0)));
   w.aperture = s.camera_aperture_radius;
   w.focus = s.camera_focus_distance;
+  if (s.camera_lens_set) {
+    w.iris_blades = std::min(s.camera_iris_blade_count, 64u);
+    w.iris_rotation = static_cast<double>(s.camera_iris_rotation_degrees) * (kPi / 180.0);
+    const float rd = s.camera_iris_roundness;
+    w.iris_roundness = std::isfinite(rd) ? std::min(1.0f, std::max(0.0f, rd)) : 0.0;
+    w.squeeze = std::isfinite(s.camera_anamorphic_squeeze) ? std::max(0.01f, s.camera_anamorphic_squeeze) : 1.0;
+  }
   return true;
 }
 

@@ -380,6 +380,8 @@ struct World {
   }
   float fov = 60.0f;
   float aperture = 0.0f, focus = 0.0f;
+  uint32_t iris_blades = 0u;
+  float iris_rotation = 0.0f, iris_roundness = 1.0f, squeeze = 1.0f;
 
   // transform_instance_vertex: scale, rotate by the normalized quaternion, translate.
   static V3 instance_vertex(V3 l, const float* t) {
@@ -520,6 +522,12 @@ struct World {
     fov = s.camera_fov_deg;
     aperture = s.camera_aperture_radius;
     focus = s.camera_focus_distance;
+    if (s.camera_lens_set) {
+      iris_blades = s.camera_iris_blade_count;
+      iris_rotation = s.camera_iris_rotation_degrees;
+      iris_roundness = s.camera_iris_roundness;
+      squeeze = s.camera_anamorphic_squeeze;
+    }
     // camera basis
     cam_fwd = unit(sub(ld3(s.camera_target), cam_pos));
     cam_right = unit(cross(cam_fwd, ld3(s.camera_up)));
@@ -1063,8 +1071,22 @@ struct Integrator {
     if (w.aperture > 0.0f && w.focus > kEps) {
       const float lr = std::sqrt(crng.u());
       const float lphi = 2.0f * kPi * crng.u();
-      const float r = w.aperture * lr;
-      const V3 off = add(mul(w.cam_right, r * std::cos(lphi) * 1.0f), mul(w.cam_up, r * std::sin(lphi)));
+      // polygonal aperture and anamorphic squeeze
+      // (src/pathtracer/ScalarCpuPathTracer.Render.cpp:94-113)
+      float boundary = 1.0f;
+      const uint32_t blades = std::min(w.iris_blades, 64u);
+      const float roundness = clamp01(w.iris_roundness);
+      if (blades >= 3u && roundness < 0.999f) {
+        const float sector = 2.0f * kPi / static_cast<float>(blades);
+        const float local_phi = lphi - w.iris_rotation * (kPi / 180.0f);
+        const float wrapped = local_phi - sector * std::floor(local_phi / sector);
+        const float centered = wrapped > sector * 0.5f ? wrapped - sector : wrapped;
+        const float polygon = std::cos(sector * 0.5f) / fmax_std(0.1f, std::cos(centered));
+        boundary = polygon * (1.0f - roundness) + roundness;
+      }
+      const float r = w.aperture * lr * boundary;
+      const float sq = std::isfinite(w.squeeze) ? fmax_std(0.01f, w.squeeze) : 1.0f;
+      const V3 off = add(mul(w.cam_right, r * std::cos(lphi) * sq), mul(w.cam_up, r * std::sin(lphi)));
       const V3 fp = add(w.cam_pos, mul(dir, w.focus));
       o = add(w.cam_pos, off);
       d = unit(sub(fp, o));

@@ -139,6 +139,12 @@ pt::PathTracerSceneSnapshot to_snapshot(const vko_scene& s) {
   out.camera_fov_deg = s.camera_fov_deg;
   out.camera_aperture_radius = s.camera_aperture_radius;
   out.camera_focus_distance = s.camera_focus_distance;
+  if (s.camera_lens_set) {
+    out.camera_iris_blade_count = s.camera_iris_blade_count;
+    out.camera_iris_rotation_degrees = s.camera_iris_rotation_degrees;
+    out.camera_iris_roundness = s.camera_iris_roundness;
+    out.camera_anamorphic_squeeze = s.camera_anamorphic_squeeze;
+  }
   return out;
 }
 
@@ -286,7 +292,7 @@ int vko_apply_film_resolve(const float* hdr_rgb, uint32_t width, uint32_t height
 }
 
 // Snapshot dump of a converted scene document, little-endian:
-//   char[4] "VKSJ", u32 version (1)
+//   char[4] "VKSJ", u32 version (2)
 //   u32 nv, ni, ninst, nmat, nlight, nsdf, nlv, nli, env_w, env_h
 //   f32 vertices[3 nv]; u32 indices[ni]; u32 instances[3 ninst];
 //   u32 instance_local[5 ninst]; f32 instance_transforms[10 ninst];
@@ -294,6 +300,7 @@ int vko_apply_film_resolve(const float* hdr_rgb, uint32_t width, uint32_t height
 //   f32 local_vertices[3 nlv]; u32 local_indices[nli];
 //   f32 environment[3]; f32 camera[12] (position3, target3, up3, fov, aperture, focus);
 //   f32 environment_map_scale[3]; f32 environment_map[3 env_w env_h]
+//   u32 camera_iris_blade_count; f32 lens[3] (iris rotation degrees, iris roundness, anamorphic squeeze)
 // Record layouts as in vkpt_oracle.h (material and light word maps, SDF records).
 int vko_convert_scene_json(const char* path, const char* out_path) {
   quiet_logs();
@@ -312,7 +319,7 @@ int vko_convert_scene_json(const char* path, const char* out_path) {
   auto wu = [&](const std::vector<uint32_t>& v) { if (!v.empty()) std::fwrite(v.data(), 4, v.size(), fp); };
   auto wf = [&](const std::vector<float>& v) { if (!v.empty()) std::fwrite(v.data(), 4, v.size(), fp); };
   std::fwrite("VKSJ", 1, 4, fp);
-  const uint32_t head[11] = {1u,
+  const uint32_t head[11] = {2u,
                              static_cast<uint32_t>(s.vertices.size()),
                              static_cast<uint32_t>(s.indices.size()),
                              static_cast<uint32_t>(s.instances.size()),
@@ -377,6 +384,9 @@ int vko_convert_scene_json(const char* path, const char* out_path) {
   for (size_t i = 0; i < texels && i < s.environment_map.size(); ++i)
     f32.insert(f32.end(), {s.environment_map[i].x, s.environment_map[i].y, s.environment_map[i].z});
   f32.resize(3 * texels, 0.0f);
+  wf(f32);
+  wu({s.camera_iris_blade_count});
+  f32 = {s.camera_iris_rotation_degrees, s.camera_iris_roundness, s.camera_anamorphic_squeeze};
   wf(f32);
   std::fclose(fp);
   return 0;

@@ -71,6 +71,15 @@ typedef struct vko_scene {
   uint32_t local_vertex_count;
   const uint32_t* local_indices;
   uint32_t local_index_count;
+  /* lens shape (camera_iris_blade_count, camera_iris_rotation_degrees,
+   * camera_iris_roundness, camera_anamorphic_squeeze,
+   * src/pathtracer/PathTracer.h:405-408); camera_lens_set = 0: the defaults
+   * (0 blades, rotation 0, roundness 1, squeeze 1) */
+  uint32_t camera_lens_set;
+  uint32_t camera_iris_blade_count;
+  float camera_iris_rotation_degrees;
+  float camera_iris_roundness;
+  float camera_anamorphic_squeeze;
 } vko_scene;
 
 typedef struct vko_settings {

@@ -51,8 +51,47 @@ def _sdf_settings():
     return scenes.RenderSettings(width=48, height=36, spp=2, max_depth=6, seed=4321, enable_nee=True, enable_mis=True)
 
 
+def _lens():
+    """The Cornell box through a thin lens with the iris and squeeze of the
+    reference's shallow depth-of-field scene document (7 blades rotated 12
+    degrees, roundness 0.42, anamorphic squeeze 1.15)."""
+    sc = scenes.cornell_box(seed=1)
+    c = sc.camera
+    c.aperture_radius, c.focus_distance = 0.1, 1.5
+    c.iris_blade_count, c.iris_rotation_degrees, c.iris_roundness, c.anamorphic_squeeze = 7, 12.0, 0.42, 1.15
+    return sc
+
+
+# Lens shapes (blades, rotation degrees, roundness, squeeze) that reach each
+# branch and clamp of ScalarCpuPathTracer::camera_rays' thin-lens sampling.
+LENS_VARIANTS = {
+    "pentagon_sharp": (5, -30.0, 0.0, 1.0),
+    "many_blades": (64, 400.0, 0.5, 0.7),
+    "too_many_blades": (200, 3.0, 0.2, 2.0),        # clamped to 64
+    "two_blades": (2, 0.0, 0.0, 1.3),               # below 3: round
+    "round_enough": (6, 0.0, 0.9995, 1.0),          # roundness >= 0.999: round
+    "nan_roundness": (6, 10.0, float("nan"), 1.0),  # clamp01(NaN) = 0
+    "tiny_squeeze": (0, 0.0, 1.0, 0.001),           # at least 0.01
+    "inf_squeeze": (8, 0.0, 0.3, float("inf")),     # non-finite: 1
+}
+
+
+def lens_scene(variant):
+    """The Cornell box through a thin lens of LENS_VARIANTS[variant]."""
+    sc = scenes.cornell_box(seed=1)
+    c = sc.camera
+    c.aperture_radius, c.focus_distance = 0.12, 1.4
+    c.iris_blade_count, c.iris_rotation_degrees, c.iris_roundness, c.anamorphic_squeeze = LENS_VARIANTS[variant]
+    return sc
+
+
+def _lens_settings():
+    return scenes.RenderSettings(width=48, height=40, spp=4, max_depth=6, seed=99, enable_nee=True, enable_mis=True)
+
+
 CASES = {
     "box": (_box, _box_settings, _box_rays),
+    "lens": (_lens, _lens_settings, None),
     "field": (_field, _field_settings, _field_rays),
     "sphere": (_sphere, None, _sphere_rays),
     "sdf": (_sdf, _sdf_settings, None),
@@ -68,6 +107,8 @@ def scene_to_arrays(scene):
         "environment": np.array(scene.environment, np.float32),
         "camera": np.array(list(c.position) + list(c.target) + list(c.up) +
                            [c.fov_deg, c.aperture_radius, c.focus_distance], np.float32),
+        "camera_lens": np.array([c.iris_blade_count, c.iris_rotation_degrees, c.iris_roundness,
+                                 c.anamorphic_squeeze], np.float32),
     }
     if scene.sdf is not None:
         out["sdf"] = np.ascontiguousarray(scene.sdf, np.float32)
@@ -86,6 +127,10 @@ def scene_from_arrays(d):
     cam = d["camera"].astype(np.float64)
     camera = scenes.Camera(tuple(cam[0:3]), tuple(cam[3:6]), tuple(cam[6:9]), float(cam[9]), float(cam[10]),
                            float(cam[11]))
+    if "camera_lens" in d:
+        lens = d["camera_lens"].astype(np.float64)
+        camera.iris_blade_count = int(lens[0])
+        camera.iris_rotation_degrees, camera.iris_roundness, camera.anamorphic_squeeze = (float(x) for x in lens[1:])
     return scenes.Scene(d["vertices"], d["indices"], d["instances"], d["materials"], d["lights"],
                         tuple(float(x) for x in d["environment"]), camera, "fixture",
                         env_map=d.get("env_map"),

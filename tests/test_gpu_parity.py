@@ -154,7 +154,7 @@ def test_external_bvh_gives_same_hits():
 
 
 # ------------------------------------------------------------------ films
-@pytest.mark.parametrize("name", ["box", "field", "sdf"])
+@pytest.mark.parametrize("name", ["box", "field", "sdf", "lens"])
 def test_film_matches_reference_golden(name):
     d = cases.load_fixture(name)
     sc, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)

@@ -24,7 +24,7 @@ def port():
     return oracle.load("port")
 
 
-@pytest.mark.parametrize("name", ["box", "field", "sdf"])
+@pytest.mark.parametrize("name", ["box", "field", "sdf", "lens"])
 def test_port_film_matches_reference_golden(port, name):
     d = cases.load_fixture(name)
     scene, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
@@ -144,6 +144,31 @@ def test_port_matches_live_reference_sdf_primitives(port, variant, nee, mis):
               "triangle_tests", "bvh_node_visits"):
         assert a["counters"][k] == b["counters"][k], k
     assert a["counters"]["sdf_hits"] > 0
+
+
+def test_lens_golden_uses_the_lens_shape(port):
+    """The lens fixture's film depends on the iris and the squeeze: the same
+    render with a round, unsqueezed lens differs."""
+    d = cases.load_fixture("lens")
+    scene, st = cases.scene_from_arrays(d), cases.settings_from_arrays(d)
+    assert scene.camera.iris_blade_count == 7 and scene.camera.anamorphic_squeeze == np.float32(1.15)
+    scene.camera.iris_blade_count, scene.camera.anamorphic_squeeze = 0, 1.0
+    r = port.render(scene, st)
+    assert not np.array_equal(bits(r["sum"]), bits(d["film_sum"]))
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")
+@pytest.mark.parametrize("variant", list(cases.LENS_VARIANTS))
+def test_port_matches_live_reference_lens_shapes(port, variant):
+    """ScalarCpuPathTracer::camera_rays' polygonal aperture and anamorphic
+    squeeze, including its clamps (src/pathtracer/ScalarCpuPathTracer.Render.cpp:88-116)."""
+    ref = oracle.load("reference")
+    sc = cases.lens_scene(variant)
+    st = scenes.RenderSettings(width=32, height=24, spp=3, max_depth=4, seed=5)
+    a = ref.render(sc, st)
+    b = port.render(sc, st)
+    assert np.array_equal(bits(a["sum"]), bits(b["sum"]))
+    assert np.array_equal(a["count"], b["count"])
 
 
 @pytest.mark.skipif(not oracle.have_reference(), reason="reference oracle not built here")

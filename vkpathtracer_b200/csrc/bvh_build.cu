@@ -1527,15 +1527,20 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   if (nc) k_flat_write<<<grid_for(nc), kThreads, 0, stream>>>(f, flag, pos, pv, out.shade, blo, bhi, nonfinite);
   uint32_t bad = 0u;
   BB_TRY(read_scalar(nonfinite, bad, stream));
-  if (keep_refit && !bad) {
-    k_inst_first<<<grid_for(instance_count + 1u), kThreads, 0, stream>>>(pos, d_prefix, instance_count,
-                                                                          out.refit->inst_first);
-    std::vector<uint32_t> first(instance_count + 1u);
-    BB_TRY(cudaMemcpyAsync(first.data(), out.refit->inst_first, 4ull * first.size(), cudaMemcpyDeviceToHost, stream));
+  if (!bad) {
+    // Per-instance primitive ranges (scene deltas rewrite whole instances; refits).
+    uint32_t* d_first = keep_refit ? out.refit->inst_first : sc.get<uint32_t>(instance_count + 1u);
+    if (sc.err != cudaSuccess) return sc.err;
+    k_inst_first<<<grid_for(instance_count + 1u), kThreads, 0, stream>>>(pos, d_prefix, instance_count, d_first);
+    std::vector<uint32_t>& first = out.inst_first;
+    first.resize(instance_count + 1u);
+    BB_TRY(cudaMemcpyAsync(first.data(), d_first, 4ull * first.size(), cudaMemcpyDeviceToHost, stream));
     BB_TRY(cudaStreamSynchronize(stream));
-    out.refit->host_inst_first.assign(first.begin(), first.end() - 1);
-    out.refit->host_inst_count.resize(instance_count);
-    for (uint32_t i = 0; i < instance_count; ++i) out.refit->host_inst_count[i] = first[i + 1] - first[i];
+    if (keep_refit) {
+      out.refit->host_inst_first.assign(first.begin(), first.end() - 1);
+      out.refit->host_inst_count.resize(instance_count);
+      for (uint32_t i = 0; i < instance_count; ++i) out.refit->host_inst_count[i] = first[i + 1] - first[i];
+    }
   }
   if (bad) {
     FreeDeviceAccel(out);

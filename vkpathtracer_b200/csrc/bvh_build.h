@@ -43,6 +43,7 @@ struct DeviceAccelOut {
   uint32_t wide_nodes = 0, depth = 0, stack_required = 0;
   bool reference_topology = true;
   bool fallback = false;       // non-finite primitive bounds: use the host builder instead
+  std::vector<uint32_t> inst_first;    // per instance and one past the last: its first flattened primitive
   DeviceRefitState* refit = nullptr;   // kept for dynamic-instance scenes (owned; FreeDeviceAccel frees)
 };
 

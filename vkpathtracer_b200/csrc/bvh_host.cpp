@@ -129,6 +129,8 @@ bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* 
                   const InstanceGeometry* dyn) {
   out.prims.clear();
   out.boxes.clear();
+  out.inst_first.clear();
+  out.inst_count.clear();
   if (instance_count > 0 && instances == nullptr) {
     error = "instances pointer is null";
     return false;
@@ -140,6 +142,7 @@ bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* 
   const bool has_dyn = dyn && dyn->instance_local && dyn->instance_transforms;
   for (uint32_t i = 0; i < instance_count; ++i) {
     const uint32_t first = instances[3 * i], count = instances[3 * i + 1], mat = instances[3 * i + 2];
+    out.inst_first.push_back(static_cast<uint32_t>(out.prims.size()));
     const uint32_t* loc = has_dyn ? dyn->instance_local + 5 * static_cast<size_t>(i) : nullptr;
     const bool use_local = loc && (loc[0] & 1u) != 0u && loc[2] > 0u && loc[4] > 0u;
     for (uint32_t k = 0; k < count; ++k) {
@@ -202,6 +205,7 @@ bool FlattenScene(const float* vertices, uint32_t vertex_count, const uint32_t* 
       for (int ax = 0; ax < 3; ++ax) out.boxes.push_back(std::min({a[ax], b[ax], c[ax]}) - kPad);
       for (int ax = 0; ax < 3; ++ax) out.boxes.push_back(std::max({a[ax], b[ax], c[ax]}) + kPad);
     }
+    out.inst_count.push_back(static_cast<uint32_t>(out.prims.size()) - out.inst_first.back());
   }
   return true;
 }

@@ -55,6 +55,7 @@ struct alignas(16) TieNode {
 struct SceneGeometry {
   std::vector<HostPrim> prims;        // accelerator order (RayQueryHit::primitive_index)
   std::vector<float> boxes;           // 6 floats per prim: lo3, hi3 (padded by 1e-4)
+  std::vector<uint32_t> inst_first, inst_count;   // per instance: its flattened primitives
 };
 
 struct WideBvh {

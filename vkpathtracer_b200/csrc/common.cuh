@@ -159,6 +159,13 @@ struct DevScene {
   V3 cam_pos, cam_fwd, cam_right, cam_up;
   float tan_half_fov;
   float aperture, focus;
+  // Lens shape, prepared on the host by the reference's own float expressions:
+  // iris_on (3..64 blades, roundness below 0.999), the blade sector 2*pi/blades,
+  // cos(sector/2), the rotation in radians, roundness and 1 - roundness, and
+  // the anamorphic squeeze (non-finite: 1; else at least 0.01).
+  uint32_t iris_on;
+  float iris_sector, iris_cos_half, iris_rot, iris_round, iris_one_minus_round;
+  float squeeze;
   uint32_t stack_required;
   uint32_t reference_tree;   // 1: the traversal tree is the reference's own tree
   const float4* sdf;         // SDF primitive records (sdf.cuh), tested after the triangles

@@ -59,6 +59,8 @@ struct DevBuf {
 struct HostCamera {
   float pos[3], target[3], up[3];
   float fov, aperture, focus;
+  uint32_t iris_blades = 0u;                // lens shape (RTCameraState defaults)
+  float iris_rotation = 0.0f, iris_roundness = 1.0f, squeeze = 1.0f;
 };
 
 // Differentiable-rendering state of a context (vkptc_forward / vkptc_backward).
@@ -120,6 +122,10 @@ struct vkptc_ctx {
   uint32_t* d_ref_order = nullptr;
   uint32_t ref_count = 0;
   uint32_t prim_count = 0;                // flattened primitives of the built accelerator
+  uint32_t instance_count = 0;            // the loaded scene's instances
+  std::vector<uint32_t> instance_material;   // per instance: its material index (scene deltas)
+  std::vector<uint32_t> inst_prims;       // built accelerator: first primitive per instance, then the total
+  DevBuf<uint4> d_delta_ranges;           // scene deltas: instance ranges whose material changes
   std::vector<float> materials, lights;
   float env[3] = {0, 0, 0};
   uint32_t env_w = 0, env_h = 0;          // environment map size (0: constant environment)
@@ -232,6 +238,18 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.tan_half_fov = std::tan(0.5f * radians);
   s.aperture = c->cam.aperture > 0.0f ? c->cam.aperture : c->settings.camera_aperture_radius;
   s.focus = c->cam.focus > 0.0f ? c->cam.focus : c->settings.camera_focus_distance;
+  // Lens shape: the same float expressions as ScalarCpuPathTracer::camera_rays
+  // (src/pathtracer/ScalarCpuPathTracer.Render.cpp:44-49, 95-110), evaluated once.
+  const uint32_t blades = std::min(c->cam.iris_blades, 64u);
+  const float rd = c->cam.iris_roundness;
+  const float roundness = std::isfinite(rd) ? std::min(1.0f, std::max(0.0f, rd)) : 0.0f;
+  s.iris_on = (blades >= 3u && roundness < 0.999f) ? 1u : 0u;
+  s.iris_sector = s.iris_on ? 2.0f * kPi / static_cast<float>(blades) : 1.0f;
+  s.iris_cos_half = std::cos(s.iris_sector * 0.5f);
+  s.iris_rot = c->cam.iris_rotation * (kPi / 180.0f);
+  s.iris_round = roundness;
+  s.iris_one_minus_round = 1.0f - roundness;
+  s.squeeze = std::isfinite(c->cam.squeeze) ? std::max(0.01f, c->cam.squeeze) : 1.0f;
   s.stack_required = c->wide.stack_required;
   s.reference_tree = c->wide.reference_topology ? 1u : 0u;
   s.sdf = c->sdf_count ? c->d_sdf.ptr : nullptr;
@@ -369,6 +387,18 @@ int32_t check_device_error(vkptc_ctx* c) {
   return VKPTC_OK;
 }
 
+// Flags the kernels take from the material table: a transmissive material
+// (model 5 or transmission above 0.05) and a procedural effect.
+void scan_materials(vkptc_ctx* c) {
+  c->has_transmissive = false;
+  c->has_effects = false;
+  for (size_t i = 0; i < c->materials.size() / 16; ++i) {
+    const float* m = &c->materials[16 * i];
+    if (static_cast<uint32_t>(m[7] + 0.5f) == 5u || m[10] > 0.05f) c->has_transmissive = true;
+    if ((static_cast<uint32_t>(m[15] + 0.5f) & 1023u) != 0u) c->has_effects = true;
+  }
+}
+
 int32_t upload_accel(vkptc_ctx* c, const std::vector<BinNode>& bin, const std::vector<uint32_t>& prim_indices,
                      double build_ms) {
   // The reference tree always supplies tie order and the parallel-axis rule;
@@ -403,6 +433,8 @@ int32_t upload_accel(vkptc_ctx* c, const std::vector<BinNode>& bin, const std::v
   if (!shade.empty())
     VKPTC_CUDA(c, cudaMemcpy(c->d_shade.ptr, shade.data(), shade.size() * sizeof(float4), cudaMemcpyHostToDevice), "bvh upload");
   c->prim_count = static_cast<uint32_t>(c->geo.prims.size());
+  c->inst_prims.assign(c->geo.inst_first.begin(), c->geo.inst_first.end());
+  c->inst_prims.push_back(c->prim_count);
   c->accel = vkptc_accel_info{};
   c->accel.primitive_count = static_cast<uint32_t>(c->geo.prims.size());
   c->accel.binary_node_count = w.binary_nodes;
@@ -617,13 +649,11 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   }
   ctx->lights.assign(scene->lights, scene->lights + 16 * static_cast<size_t>(scene->light_count));
   for (size_t i = 0; i < ctx->lights.size() / 16; ++i) ctx->lights[16 * i + 7] = std::max(0.0f, ctx->lights[16 * i + 7]);
-  ctx->has_transmissive = false;
-  ctx->has_effects = false;
-  for (size_t i = 0; i < ctx->materials.size() / 16; ++i) {
-    const float* m = &ctx->materials[16 * i];
-    if (static_cast<uint32_t>(m[7] + 0.5f) == 5u || m[10] > 0.05f) ctx->has_transmissive = true;
-    if ((static_cast<uint32_t>(m[15] + 0.5f) & 1023u) != 0u) ctx->has_effects = true;
-  }
+  scan_materials(ctx);
+  ctx->instance_count = scene->instance_count;
+  ctx->instance_material.resize(scene->instance_count);
+  for (uint32_t i = 0; i < scene->instance_count; ++i) ctx->instance_material[i] = scene->instances[3 * i + 2];
+  ctx->inst_prims.clear();
   std::memcpy(ctx->env, scene->environment, sizeof(ctx->env));
   // Environment map: used when it holds width*height texels (as the reference checks).
   const uint64_t env_texels = static_cast<uint64_t>(scene->environment_map_width) * scene->environment_map_height;
@@ -709,6 +739,10 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   ctx->cam.fov = scene->camera_fov_deg;
   ctx->cam.aperture = scene->camera_aperture_radius;
   ctx->cam.focus = scene->camera_focus_distance;
+  ctx->cam.iris_blades = scene->camera_lens_set ? scene->camera_iris_blade_count : 0u;
+  ctx->cam.iris_rotation = scene->camera_lens_set ? scene->camera_iris_rotation_degrees : 0.0f;
+  ctx->cam.iris_roundness = scene->camera_lens_set ? scene->camera_iris_roundness : 1.0f;
+  ctx->cam.squeeze = scene->camera_lens_set ? scene->camera_anamorphic_squeeze : 1.0f;
   VKPTC_CUDA(ctx, ctx->d_materials.alloc(ctx->materials.size()), "material alloc");
   VKPTC_CUDA(ctx, cudaMemcpy(ctx->d_materials.ptr, ctx->materials.data(), ctx->materials.size() * sizeof(float),
                              cudaMemcpyHostToDevice), "material upload");
@@ -796,6 +830,7 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
   }
   if (out.fallback) return VKPTC_OK;
   const uint32_t n = out.prim_count;
+  c->inst_prims = std::move(out.inst_first);
   c->d_shade.adopt(out.shade, std::max<uint32_t>(1, n));
   if (n == 0u) {
     VKPTC_CUDA(c, c->d_nodes.alloc(1), "bvh alloc");
@@ -1008,6 +1043,122 @@ int32_t vkptc_update_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_up
     std::copy(ups[u].transform, ups[u].transform + 10, ctx->raw_instance_transforms.begin() + 10 * i);
   }
   ctx->geo_ready = false;   // a host flatten (external BVH) must use the new transforms
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_update_camera(vkptc_ctx* ctx, const vkptc_camera* camera) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured || !ctx->has_scene)
+    return fail(ctx, VKPTC_NOT_READY, "update_camera_state requires a configured tracer with a scene");
+  if (!camera) return fail(ctx, VKPTC_INVALID_ARGUMENT, "camera is null");
+  HostCamera& c = ctx->cam;
+  std::memcpy(c.pos, camera->position, 12);
+  std::memcpy(c.target, camera->target, 12);
+  std::memcpy(c.up, camera->up, 12);
+  c.fov = camera->fov_deg;
+  c.aperture = camera->aperture_radius;
+  c.focus = camera->focus_distance;
+  c.iris_blades = camera->iris_blade_count;
+  c.iris_rotation = camera->iris_rotation_degrees;
+  c.iris_roundness = camera->iris_roundness;
+  c.squeeze = camera->anamorphic_squeeze;
+  ctx->adj.forward_done = false;   // a backward pass must follow a forward pass with this camera
+  ctx->last_error.clear();
+  return VKPTC_OK;
+}
+
+int32_t vkptc_get_camera(vkptc_ctx* ctx, vkptc_camera* out) {
+  if (!ctx || !out) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "no scene loaded");
+  const HostCamera& c = ctx->cam;
+  std::memcpy(out->position, c.pos, 12);
+  std::memcpy(out->target, c.target, 12);
+  std::memcpy(out->up, c.up, 12);
+  out->fov_deg = c.fov;
+  out->aperture_radius = c.aperture;
+  out->focus_distance = c.focus;
+  out->iris_blade_count = c.iris_blades;
+  out->iris_rotation_degrees = c.iris_rotation;
+  out->iris_roundness = c.iris_roundness;
+  out->anamorphic_squeeze = c.squeeze;
+  return VKPTC_OK;
+}
+
+int32_t vkptc_update_scene_delta(vkptc_ctx* ctx, const vkptc_scene_delta* d) {
+  if (!ctx) return VKPTC_INVALID_ARGUMENT;
+  if (!ctx->configured || !ctx->has_scene)
+    return fail(ctx, VKPTC_NOT_READY, "update_scene_delta requires a configured tracer with a scene");
+  if (!d) return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene delta is null");
+  if ((d->material_count && (!d->material_indices || !d->materials)) ||
+      (d->light_count && (!d->light_indices || !d->lights)) ||
+      (d->instance_material_count && (!d->instance_indices || !d->instance_material_indices)))
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene delta array pointer is null");
+  // ApplySceneDeltaUpdate's checks, all before anything changes
+  // (src/pathtracer/PathTracer.cpp:428-451).
+  const uint32_t n_mat = static_cast<uint32_t>(ctx->materials.size() / 16);
+  const uint32_t n_light = static_cast<uint32_t>(ctx->lights.size() / 16);
+  for (uint32_t k = 0; k < d->material_count; ++k)
+    if (d->material_indices[k] >= n_mat)
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene delta did not apply: material index out of range");
+  for (uint32_t k = 0; k < d->light_count; ++k)
+    if (d->light_indices[k] >= n_light)
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene delta did not apply: light index out of range");
+  for (uint32_t k = 0; k < d->instance_material_count; ++k)
+    if (d->instance_indices[k] >= ctx->instance_count || d->instance_material_indices[k] >= n_mat)
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene delta did not apply: instance or material index out of range");
+  // Which instances end with a new material (the last update of an instance wins).
+  std::vector<uint32_t> next = ctx->instance_material;
+  bool changed = d->material_count > 0u || d->light_count > 0u || d->environment_changed != 0u;
+  for (uint32_t k = 0; k < d->instance_material_count; ++k) {
+    const uint32_t i = d->instance_indices[k];
+    if (next[i] != d->instance_material_indices[k]) changed = true;
+    next[i] = d->instance_material_indices[k];
+  }
+  if (!changed) return fail(ctx, VKPTC_INVALID_ARGUMENT, "scene delta did not apply: nothing changed");
+  cudaSetDevice(ctx->device);
+  // Renders already enqueued finish with the old tables.
+  VKPTC_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+  for (uint32_t k = 0; k < d->material_count; ++k)
+    std::copy(d->materials + 16ull * k, d->materials + 16ull * (k + 1), ctx->materials.begin() + 16ull * d->material_indices[k]);
+  for (uint32_t k = 0; k < d->light_count; ++k) {
+    float* w = &ctx->lights[16ull * d->light_indices[k]];
+    std::copy(d->lights + 16ull * k, d->lights + 16ull * (k + 1), w);
+    w[7] = std::max(0.0f, w[7]);
+  }
+  // Pageable copies on the context's stream: staged before the call returns,
+  // ordered before the next render.
+  if (d->material_count) {
+    scan_materials(ctx);
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(ctx->d_materials.ptr, ctx->materials.data(), ctx->materials.size() * sizeof(float),
+                                    cudaMemcpyHostToDevice, ctx->stream), "material upload");
+  }
+  if (d->light_count)
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(ctx->d_lights.ptr, ctx->lights.data(), ctx->lights.size() * sizeof(float),
+                                    cudaMemcpyHostToDevice, ctx->stream), "light upload");
+  if (d->environment_changed) std::memcpy(ctx->env, d->environment, sizeof(ctx->env));
+  // Instance materials: the instance table kept for later builds, the host
+  // flattening when there is one, and the shading records of the built
+  // accelerator.
+  std::vector<uint4> ranges;
+  for (uint32_t i = 0; i < ctx->instance_count; ++i) {
+    if (next[i] == ctx->instance_material[i]) continue;
+    ctx->instance_material[i] = next[i];
+    if (3ull * i + 2 < ctx->raw_instances.size()) ctx->raw_instances[3ull * i + 2] = next[i];
+    if (ctx->geo_ready && i < ctx->geo.inst_first.size())
+      for (uint32_t k = 0; k < ctx->geo.inst_count[i]; ++k) ctx->geo.prims[ctx->geo.inst_first[i] + k].material = next[i];
+    if (ctx->accel_valid && i + 1 < ctx->inst_prims.size() && ctx->inst_prims[i + 1] > ctx->inst_prims[i])
+      ranges.push_back(make_uint4(ctx->inst_prims[i], ctx->inst_prims[i + 1] - ctx->inst_prims[i], next[i], 0u));
+  }
+  if (!ranges.empty()) {
+    VKPTC_CUDA(ctx, ctx->d_delta_ranges.alloc(ranges.size()), "delta alloc");
+    VKPTC_CUDA(ctx, cudaMemcpyAsync(ctx->d_delta_ranges.ptr, ranges.data(), ranges.size() * sizeof(uint4),
+                                    cudaMemcpyHostToDevice, ctx->stream), "delta upload");
+    VKPTC_CUDA(ctx, LaunchSetInstanceMaterials(ctx->d_shade.ptr, ctx->d_delta_ranges.ptr,
+                                               static_cast<uint32_t>(ranges.size()), ctx->stream), "delta launch");
+  }
+  ctx->adj.setup = false;   // the adjoint's material tables were taken from the old scene
+  ctx->adj.forward_done = false;
   ctx->last_error.clear();
   return VKPTC_OK;
 }

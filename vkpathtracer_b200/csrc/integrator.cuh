@@ -356,8 +356,18 @@ __device__ __forceinline__ void camera_path(const DevScene& s, const DevSettings
   if (s.aperture > 0.0f && s.focus > kEps) {
     const float lr = sqrtf(next01(crng));
     const float lphi = 2.0f * kPi * next01(crng);
-    const float rr = s.aperture * lr * 1.0f;
-    const V3 off = add(mul(s.cam_right, rr * t_cos<kParity>(lphi) * 1.0f), mul(s.cam_up, rr * t_sin<kParity>(lphi)));
+    // Polygonal aperture: the lens radius shrinks per blade sector
+    // (ScalarCpuPathTracer::camera_rays, src/pathtracer/ScalarCpuPathTracer.Render.cpp:94-105).
+    float boundary = 1.0f;
+    if (s.iris_on) {
+      const float local_phi = lphi - s.iris_rot;
+      const float wrapped = local_phi - s.iris_sector * floorf(local_phi / s.iris_sector);
+      const float centered = wrapped > s.iris_sector * 0.5f ? wrapped - s.iris_sector : wrapped;
+      const float polygon = s.iris_cos_half / smax(0.1f, t_cos<kParity>(centered));
+      boundary = polygon * s.iris_one_minus_round + s.iris_round;
+    }
+    const float rr = s.aperture * lr * boundary;
+    const V3 off = add(mul(s.cam_right, rr * t_cos<kParity>(lphi) * s.squeeze), mul(s.cam_up, rr * t_sin<kParity>(lphi)));
     const V3 fp = add(s.cam_pos, mul(dir, s.focus));
     o = add(s.cam_pos, off);
     d = unit(sub(fp, o));

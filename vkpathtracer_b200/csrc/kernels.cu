@@ -475,6 +475,23 @@ cudaError_t LaunchPackFilm(const Film& film, float* rgb_out, cudaStream_t stream
   return cudaGetLastError();
 }
 
+// One block per instance range (strided), its threads over the range.
+__global__ void k_set_instance_materials(float4* __restrict__ shade, const uint4* __restrict__ ranges,
+                                         uint32_t range_count) {
+  for (uint32_t r = blockIdx.x; r < range_count; r += gridDim.x) {
+    const uint4 g = ranges[r];
+    const float m = __uint_as_float(g.z);
+    for (uint32_t k = threadIdx.x; k < g.y; k += blockDim.x) shade[g.x + k].w = m;
+  }
+}
+
+cudaError_t LaunchSetInstanceMaterials(float4* shade, const uint4* ranges, uint32_t range_count, cudaStream_t stream) {
+  if (range_count == 0u) return cudaSuccess;
+  const int grid = static_cast<int>(std::min<uint32_t>(range_count, 148u * 8u));
+  k_set_instance_materials<<<grid, 256, 0, stream>>>(shade, ranges, range_count);
+  return cudaGetLastError();
+}
+
 // ApplyFilmResolve (src/pathtracer/FilmBuffer.cpp:253-325) per pixel, on the
 // film's per-pixel mean: exposure then white balance, non-finite to 0, tone
 // map, gamma (pow, FP64 rounded once in parity mode), clamp, and the x86

@@ -103,6 +103,11 @@ cudaError_t LaunchResolveHdr(const Film& film, float* rgb_out, cudaStream_t stre
 // The film's rgb sums packed to 3 floats per pixel (for host readback).
 cudaError_t LaunchPackFilm(const Film& film, float* rgb_out, cudaStream_t stream);
 
+// Scene deltas: the material word (w) of the shading records of whole
+// instances.  ranges: per changed instance (first primitive, primitive count,
+// material index, 0), device memory; the ranges do not overlap.
+cudaError_t LaunchSetInstanceMaterials(float4* shade, const uint4* ranges, uint32_t range_count, cudaStream_t stream);
+
 // ApplyFilmResolve on the device; wb: the white-balance scale (host-computed).
 struct LdrResolve {
   float exposure, wb[3], gamma;

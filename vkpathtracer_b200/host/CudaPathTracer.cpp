@@ -13,6 +13,40 @@ namespace pt = vkpt::pathtracer;
 using vkpt::core::Status;
 using vkpt::core::StatusCode;
 
+namespace {
+
+// Standard GPU word maps (src/gpu/VulkanGpuPathTracer.cpp:323-338, 381-396).
+void material_words(const pt::RTMaterial& m, float* w) {
+  w[0] = m.albedo.x; w[1] = m.albedo.y; w[2] = m.albedo.z;
+  w[3] = m.emissive.x; w[4] = m.emissive.y; w[5] = m.emissive.z;
+  w[6] = m.roughness;
+  w[7] = static_cast<float>(m.material_model);
+  w[8] = m.metallic; w[9] = m.ior; w[10] = m.transmission; w[11] = m.clearcoat;
+  w[12] = m.sheen; w[13] = m.anisotropy; w[14] = m.alpha;
+  w[15] = static_cast<float>((m.material_effect & 1023u) | ((m.material_flags & 1u) ? 1024u : 0u));
+}
+
+void light_words(const pt::RTHitLight& l, float* w) {
+  w[0] = l.position.x; w[1] = l.position.y; w[2] = l.position.z;
+  w[3] = l.color.x; w[4] = l.color.y; w[5] = l.color.z;
+  w[6] = l.intensity; w[7] = std::max(0.0f, l.radius);
+  w[8] = l.direction.x; w[9] = l.direction.y; w[10] = l.direction.z;
+  w[11] = l.spot_inner_cos; w[12] = l.spot_outer_cos;
+}
+
+// The instance an update names: its index, else the instance with its entity
+// id (ApplySceneDeltaUpdate / resolve_instance_index); entities.size() when none.
+uint32_t resolve_instance(uint32_t index, vkpt::core::StableId entity,
+                          const std::vector<vkpt::core::StableId>& entities) {
+  if (index >= entities.size() && entity != 0u) {
+    for (size_t i = 0; i < entities.size(); ++i)
+      if (entities[i] == entity) return static_cast<uint32_t>(i);
+  }
+  return index < entities.size() ? index : static_cast<uint32_t>(entities.size());
+}
+
+}  // namespace
+
 CudaPathTracer::CudaPathTracer(CudaPathTracerConfig config) {
   vkptc_config c{};
   c.device = config.device;
@@ -63,6 +97,7 @@ Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
   s.camera_aperture_radius = settings.camera_aperture_radius;
   s.camera_focus_distance = settings.camera_focus_distance;
   const Status st = status_from(vkptc_configure(m_ctx, &s), "configure");
+  m_has_scene = false;
   if (st) {
     m_settings = settings;
     m_resolve = settings.film_resolve;
@@ -74,29 +109,10 @@ Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
 
 Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& scene) {
   if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
-  // Standard GPU word maps (src/gpu/VulkanGpuPathTracer.cpp:323-338, 381-396).
   std::vector<float> mats(16 * scene.materials.size(), 0.0f);
-  for (size_t i = 0; i < scene.materials.size(); ++i) {
-    const pt::RTMaterial& m = scene.materials[i];
-    float* w = &mats[16 * i];
-    w[0] = m.albedo.x; w[1] = m.albedo.y; w[2] = m.albedo.z;
-    w[3] = m.emissive.x; w[4] = m.emissive.y; w[5] = m.emissive.z;
-    w[6] = m.roughness;
-    w[7] = static_cast<float>(m.material_model);
-    w[8] = m.metallic; w[9] = m.ior; w[10] = m.transmission; w[11] = m.clearcoat;
-    w[12] = m.sheen; w[13] = m.anisotropy; w[14] = m.alpha;
-    w[15] = static_cast<float>((m.material_effect & 1023u) | ((m.material_flags & 1u) ? 1024u : 0u));
-  }
+  for (size_t i = 0; i < scene.materials.size(); ++i) material_words(scene.materials[i], &mats[16 * i]);
   std::vector<float> lights(16 * scene.lights.size(), 0.0f);
-  for (size_t i = 0; i < scene.lights.size(); ++i) {
-    const pt::RTHitLight& l = scene.lights[i];
-    float* w = &lights[16 * i];
-    w[0] = l.position.x; w[1] = l.position.y; w[2] = l.position.z;
-    w[3] = l.color.x; w[4] = l.color.y; w[5] = l.color.z;
-    w[6] = l.intensity; w[7] = std::max(0.0f, l.radius);
-    w[8] = l.direction.x; w[9] = l.direction.y; w[10] = l.direction.z;
-    w[11] = l.spot_inner_cos; w[12] = l.spot_outer_cos;
-  }
+  for (size_t i = 0; i < scene.lights.size(); ++i) light_words(scene.lights[i], &lights[16 * i]);
   std::vector<uint32_t> inst(3 * scene.instances.size());
   std::vector<uint32_t> inst_local(5 * scene.instances.size());
   std::vector<float> inst_tr(10 * scene.instances.size());
@@ -139,6 +155,11 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
   v.camera_fov_deg = scene.camera_fov_deg;
   v.camera_aperture_radius = scene.camera_aperture_radius;
   v.camera_focus_distance = scene.camera_focus_distance;
+  v.camera_lens_set = 1u;
+  v.camera_iris_blade_count = scene.camera_iris_blade_count;
+  v.camera_iris_rotation_degrees = scene.camera_iris_rotation_degrees;
+  v.camera_iris_roundness = scene.camera_iris_roundness;
+  v.camera_anamorphic_squeeze = scene.camera_anamorphic_squeeze;
   // The reference samples the map only when it holds width*height texels.
   const size_t env_texels = static_cast<size_t>(scene.environment_map_width) * scene.environment_map_height;
   if (env_texels > 0 && scene.environment_map.size() >= env_texels) {
@@ -175,7 +196,13 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
   m_instance_entities.clear();
   for (const auto& r : scene.instances) m_instance_entities.push_back(r.entity_id);
   const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
-  if (st) m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
+  m_has_scene = static_cast<bool>(st);
+  if (st) {
+    m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
+    m_camera = pt::ExtractCameraState(scene);
+    m_camera_scene = pt::PathTracerSceneSnapshot{};
+    pt::ApplyCameraState(m_camera_scene, m_camera);
+  }
   return st;
 }
 
@@ -360,6 +387,80 @@ pt::InstanceTransformUpdateResult CudaPathTracer::apply_instance_transform_updat
   m_last_error.clear();
   return {pt::InstanceTransformUpdateStatus::AppliedDynamicAccelUpdate, n, n, 0.0, 0.0, ms, 0.0,
           "cuda backend refit dynamic instance transforms"};
+}
+
+// ScalarCpuPathTracer::update_camera (src/pathtracer/ScalarCpuPathTracer.cpp:522-533): the current
+// camera state with a new position, target, up and field of view.
+bool CudaPathTracer::update_camera(const pt::Vec3& pos, const pt::Vec3& target, const pt::Vec3& up, float fov_deg) {
+  if (!m_ctx) return fail("no cuda context");
+  if (!m_has_scene) return fail("update_camera requires a configured tracer with a scene");
+  pt::RTCameraState camera = m_camera;
+  camera.position = pos;
+  camera.target = target;
+  camera.up = up;
+  camera.fov_deg = fov_deg;
+  return update_camera_state(camera);
+}
+
+// ScalarCpuPathTracer::update_camera_state (src/pathtracer/ScalarCpuPathTracer.cpp:535-546): the
+// device camera replaced, the film resolve settings adjusted for the new exposure controls.
+bool CudaPathTracer::update_camera_state(const pt::RTCameraState& camera) {
+  if (!m_ctx) return fail("no cuda context");
+  vkptc_camera c{};
+  const pt::Vec3 v[3] = {camera.position, camera.target, camera.up};
+  float* dst[3] = {c.position, c.target, c.up};
+  for (int k = 0; k < 3; ++k) {
+    dst[k][0] = v[k].x;
+    dst[k][1] = v[k].y;
+    dst[k][2] = v[k].z;
+  }
+  c.fov_deg = camera.fov_deg;
+  c.aperture_radius = camera.aperture_radius;
+  c.focus_distance = camera.focus_distance;
+  c.iris_blade_count = camera.iris_blade_count;
+  c.iris_rotation_degrees = camera.iris_rotation_degrees;
+  c.iris_roundness = camera.iris_roundness;
+  c.anamorphic_squeeze = camera.anamorphic_squeeze;
+  if (!status_from(vkptc_update_camera(m_ctx, &c), "update_camera_state")) return false;
+  m_camera = camera;
+  pt::ApplyCameraState(m_camera_scene, camera);
+  m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, m_camera_scene));
+  return true;
+}
+
+// ScalarCpuPathTracer::update_scene_delta (src/pathtracer/ScalarCpuPathTracer.cpp:701-720) over the
+// device tables; instances named by entity id are resolved here, as ApplySceneDeltaUpdate does.
+bool CudaPathTracer::update_scene_delta(const pt::RTSceneDeltaUpdate& update) {
+  if (!m_ctx) return fail("no cuda context");
+  std::vector<uint32_t> mat_index, light_index, inst_index, inst_mat;
+  std::vector<float> mats(16 * update.materials.size(), 0.0f), lights(16 * update.lights.size(), 0.0f);
+  for (size_t k = 0; k < update.materials.size(); ++k) {
+    mat_index.push_back(update.materials[k].material_index);
+    material_words(update.materials[k].material, &mats[16 * k]);
+  }
+  for (size_t k = 0; k < update.lights.size(); ++k) {
+    light_index.push_back(update.lights[k].light_index);
+    light_words(update.lights[k].light, &lights[16 * k]);
+  }
+  for (const auto& im : update.instance_materials) {
+    inst_index.push_back(resolve_instance(im.instance_index, im.entity_id, m_instance_entities));
+    inst_mat.push_back(im.material_index);
+  }
+  vkptc_scene_delta d{};
+  d.material_indices = mat_index.data();
+  d.materials = mats.data();
+  d.material_count = static_cast<uint32_t>(mat_index.size());
+  d.light_indices = light_index.data();
+  d.lights = lights.data();
+  d.light_count = static_cast<uint32_t>(light_index.size());
+  d.instance_indices = inst_index.data();
+  d.instance_material_indices = inst_mat.data();
+  d.instance_material_count = static_cast<uint32_t>(inst_index.size());
+  d.environment_changed = update.environment_color_changed ? 1u : 0u;
+  d.environment[0] = update.environment_color.x;
+  d.environment[1] = update.environment_color.y;
+  d.environment[2] = update.environment_color.z;
+  return static_cast<bool>(status_from(vkptc_update_scene_delta(m_ctx, &d), "update_scene_delta"));
 }
 
 bool CudaPathTracer::update_instance_transforms(const std::vector<pt::RTInstanceTransformUpdate>& updates) {

@@ -51,6 +51,10 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   bool supports_tile_batching() const override { return true; }
   vkpt::pathtracer::FilmLdr resolve_ldr() const override;
   vkpt::pathtracer::FilmReadbackToken request_film_readback() override;
+  bool update_camera(const vkpt::pathtracer::Vec3& pos, const vkpt::pathtracer::Vec3& target,
+                     const vkpt::pathtracer::Vec3& up, float fov_deg) override;
+  bool update_camera_state(const vkpt::pathtracer::RTCameraState& camera) override;
+  bool update_scene_delta(const vkpt::pathtracer::RTSceneDeltaUpdate& update) override;
   bool update_instance_transforms(const std::vector<vkpt::pathtracer::RTInstanceTransformUpdate>& updates) override;
   vkpt::pathtracer::InstanceTransformPlan plan_instance_transform_update(
       std::span<const vkpt::pathtracer::RTInstanceTransformUpdate> updates,
@@ -75,6 +79,11 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   mutable vkpt::pathtracer::FilmBuffer m_film;
   mutable std::string m_last_error;
   std::vector<vkpt::core::StableId> m_instance_entities;   // entity id per instance (update resolution)
+  bool m_has_scene = false;
+  // The loaded scene's camera; a snapshot holding only it gives the
+  // camera-adjusted film resolve settings after a camera update.
+  vkpt::pathtracer::RTCameraState m_camera{};
+  vkpt::pathtracer::PathTracerSceneSnapshot m_camera_scene{};
 };
 
 }  // namespace vkpt::gpu::cuda

@@ -56,7 +56,10 @@ class SceneView(ctypes.Structure):
                 ("sdf_primitives", ctypes.c_void_p), ("sdf_count", ctypes.c_uint32),
                 ("instance_local", ctypes.c_void_p), ("instance_transforms", ctypes.c_void_p),
                 ("local_vertices", ctypes.c_void_p), ("local_vertex_count", ctypes.c_uint32),
-                ("local_indices", ctypes.c_void_p), ("local_index_count", ctypes.c_uint32)]
+                ("local_indices", ctypes.c_void_p), ("local_index_count", ctypes.c_uint32),
+                ("camera_lens_set", ctypes.c_uint32), ("camera_iris_blade_count", ctypes.c_uint32),
+                ("camera_iris_rotation_degrees", ctypes.c_float), ("camera_iris_roundness", ctypes.c_float),
+                ("camera_anamorphic_squeeze", ctypes.c_float)]
 
 # vkptc_sdf_shape
 SDF_SPHERE, SDF_BOX, SDF_ROUNDED_BOX, SDF_PLANE, SDF_TORUS, SDF_CAPSULE = range(6)
@@ -65,6 +68,24 @@ SDF_SPHERE, SDF_BOX, SDF_ROUNDED_BOX, SDF_PLANE, SDF_TORUS, SDF_CAPSULE = range(
 class InstanceUpdate(ctypes.Structure):
     _fields_ = [("instance_index", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("translation", ctypes.c_float * 3),
                 ("rotation", ctypes.c_float * 4), ("scale", ctypes.c_float * 3)]
+
+
+class CameraC(ctypes.Structure):
+    """vkptc_camera: the RTCameraState fields the render reads."""
+    _fields_ = [("position", ctypes.c_float * 3), ("target", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+                ("fov_deg", ctypes.c_float), ("aperture_radius", ctypes.c_float), ("focus_distance", ctypes.c_float),
+                ("iris_blade_count", ctypes.c_uint32), ("iris_rotation_degrees", ctypes.c_float),
+                ("iris_roundness", ctypes.c_float), ("anamorphic_squeeze", ctypes.c_float)]
+
+
+class SceneDelta(ctypes.Structure):
+    """vkptc_scene_delta: RTSceneDeltaUpdate with instances resolved to indices."""
+    _fields_ = [("material_indices", ctypes.c_void_p), ("materials", ctypes.c_void_p),
+                ("material_count", ctypes.c_uint32),
+                ("light_indices", ctypes.c_void_p), ("lights", ctypes.c_void_p), ("light_count", ctypes.c_uint32),
+                ("instance_indices", ctypes.c_void_p), ("instance_material_indices", ctypes.c_void_p),
+                ("instance_material_count", ctypes.c_uint32),
+                ("environment_changed", ctypes.c_uint32), ("environment", ctypes.c_float * 3)]
 
 
 class FilmResolve(ctypes.Structure):
@@ -175,6 +196,9 @@ SIGNATURES = {
     "vkptc_update_instance_transforms": (I32, [P, ctypes.c_void_p, ctypes.c_uint32]),
     "vkptc_batch_read_films": (I32, [P, ctypes.c_void_p, ctypes.c_void_p]),
     "vkptc_check_instance_transforms": (I32, [P, ctypes.c_void_p, ctypes.c_uint32]),
+    "vkptc_update_camera": (I32, [P, ctypes.POINTER(CameraC)]),
+    "vkptc_get_camera": (I32, [P, ctypes.POINTER(CameraC)]),
+    "vkptc_update_scene_delta": (I32, [P, ctypes.POINTER(SceneDelta)]),
     "vkptc_request_ldr_readback": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_poll_ldr_readback": (I32, [P, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),

@@ -86,6 +86,11 @@ class Camera:
     fov_deg: float = 60.0
     aperture_radius: float = 0.0
     focus_distance: float = 0.0
+    # thin-lens shape (PathTracerSceneSnapshot camera_iris_* / camera_anamorphic_squeeze)
+    iris_blade_count: int = 0
+    iris_rotation_degrees: float = 0.0
+    iris_roundness: float = 1.0
+    anamorphic_squeeze: float = 1.0
 
 
 @dataclasses.dataclass
@@ -306,7 +311,8 @@ def load_snapshot_dump(path: str, name: str = "") -> Scene:
     if data[:4] != b"VKSJ":
         raise ValueError("not a snapshot dump")
     head = np.frombuffer(data, np.uint32, 11, 4)
-    if int(head[0]) != 1:
+    version = int(head[0])
+    if version not in (1, 2):
         raise ValueError("unknown snapshot dump version")
     nv, ni, ninst, nmat, nlight, nsdf, nlv, nli, ew, eh = (int(x) for x in head[1:])
     off = 48
@@ -332,6 +338,10 @@ def load_snapshot_dump(path: str, name: str = "") -> Scene:
     env_scale = take(np.float32, 3)
     env_map = take(np.float32, 3 * ew * eh).reshape(eh, ew, 3) if ew * eh else None
     camera = Camera(tuple(cam[0:3]), tuple(cam[3:6]), tuple(cam[6:9]), float(cam[9]), float(cam[10]), float(cam[11]))
+    if version >= 2:   # lens shape
+        camera.iris_blade_count = int(take(np.uint32, 1)[0])
+        lens = take(np.float32, 3).astype(np.float64)
+        camera.iris_rotation_degrees, camera.iris_roundness, camera.anamorphic_squeeze = (float(x) for x in lens)
     # trailing partial triangles are ignored by the accelerator (index checks), so keep the flat array
     return Scene(vertices, indices.reshape(-1, 3) if ni % 3 == 0 else indices, instances, materials, lights,
                  tuple(float(x) for x in env), camera, name or "snapshot", env_map=env_map,

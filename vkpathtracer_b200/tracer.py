@@ -18,7 +18,7 @@ from typing import Iterable, Optional, Sequence
 import numpy as np
 
 from . import native
-from .scenes import RenderSettings, Scene
+from .scenes import Camera, RenderSettings, Scene
 
 
 @dataclasses.dataclass
@@ -79,6 +79,15 @@ def settings_c(settings: RenderSettings) -> "native.RenderSettingsC":
     return s
 
 
+def set_lens(v, camera) -> None:
+    """The camera's lens shape into a vkptc_scene_view (camera_lens_set = 1)."""
+    v.camera_lens_set = 1
+    v.camera_iris_blade_count = int(camera.iris_blade_count)
+    v.camera_iris_rotation_degrees = float(camera.iris_rotation_degrees)
+    v.camera_iris_roundness = float(camera.iris_roundness)
+    v.camera_anamorphic_squeeze = float(camera.anamorphic_squeeze)
+
+
 def scene_view(scene: Scene):
     """POD view of a Scene; returns (view, arrays to keep alive during the call)."""
     v = native.SceneView()
@@ -98,6 +107,7 @@ def scene_view(scene: Scene):
     v.camera_fov_deg = c.fov_deg
     v.camera_aperture_radius = c.aperture_radius
     v.camera_focus_distance = c.focus_distance
+    set_lens(v, c)
     if scene.env_map is not None:
         env = np.ascontiguousarray(scene.env_map, np.float32)
         keep = keep + (env,)
@@ -219,6 +229,54 @@ class CudaPathTracer:
             arr[k].scale[:] = u.get("scale", (1.0, 1.0, 1.0))
         fn = self._lib.vkptc_check_instance_transforms if check_only else self._lib.vkptc_update_instance_transforms
         self._check(fn(self._ctx, ctypes.cast(arr, ctypes.c_void_p), len(updates)))
+
+    def get_camera(self) -> Camera:
+        """The loaded scene's camera (ExtractCameraState)."""
+        c = native.CameraC()
+        self._check(self._lib.vkptc_get_camera(self._ctx, ctypes.byref(c)))
+        return Camera(tuple(c.position), tuple(c.target), tuple(c.up), c.fov_deg, c.aperture_radius, c.focus_distance,
+                      c.iris_blade_count, c.iris_rotation_degrees, c.iris_roundness, c.anamorphic_squeeze)
+
+    def update_camera_state(self, camera: Camera) -> None:
+        """IPathTracer::update_camera_state: the whole camera replaced; no
+        rebuild, the film is kept (reset_accumulation clears it)."""
+        c = native.CameraC()
+        c.position[:], c.target[:], c.up[:] = camera.position, camera.target, camera.up
+        c.fov_deg, c.aperture_radius, c.focus_distance = camera.fov_deg, camera.aperture_radius, camera.focus_distance
+        c.iris_blade_count, c.iris_rotation_degrees = int(camera.iris_blade_count), camera.iris_rotation_degrees
+        c.iris_roundness, c.anamorphic_squeeze = camera.iris_roundness, camera.anamorphic_squeeze
+        self._check(self._lib.vkptc_update_camera(self._ctx, ctypes.byref(c)))
+
+    def update_camera(self, position, target, up, fov_deg: float) -> None:
+        """IPathTracer::update_camera: position, target, up and field of view
+        changed, the rest of the camera kept."""
+        cam = self.get_camera()
+        cam.position, cam.target, cam.up, cam.fov_deg = tuple(position), tuple(target), tuple(up), float(fov_deg)
+        self.update_camera_state(cam)
+
+    def update_scene_delta(self, materials=None, lights=None, instance_materials=None, environment=None) -> None:
+        """IPathTracer::update_scene_delta (ApplySceneDeltaUpdate): materials and
+        lights as {index: 16-float record}, instance_materials as
+        {instance index: material index} (or sequences of (index, value) pairs,
+        applied in order), environment an rgb colour or None."""
+        def pairs(x):
+            return list(x.items()) if isinstance(x, dict) else list(x or ())
+
+        materials, lights, inst = pairs(materials), pairs(lights), pairs(instance_materials)
+        mi = np.array([k for k, _ in materials], np.uint32)
+        mw = np.ascontiguousarray(np.array([v for _, v in materials], np.float32).reshape(-1, 16))
+        li = np.array([k for k, _ in lights], np.uint32)
+        lw = np.ascontiguousarray(np.array([v for _, v in lights], np.float32).reshape(-1, 16))
+        ii = np.array([k for k, _ in inst], np.uint32)
+        im = np.array([v for _, v in inst], np.uint32)
+        d = native.SceneDelta()
+        d.material_indices, d.materials, d.material_count = _ptr(mi), _ptr(mw), mi.size
+        d.light_indices, d.lights, d.light_count = _ptr(li), _ptr(lw), li.size
+        d.instance_indices, d.instance_material_indices, d.instance_material_count = _ptr(ii), _ptr(im), ii.size
+        if environment is not None:
+            d.environment_changed = 1
+            d.environment[:] = environment
+        self._check(self._lib.vkptc_update_scene_delta(self._ctx, ctypes.byref(d)))
 
     @staticmethod
     def film_resolve(exposure: float = 1.0, white_balance_kelvin: float = 6500.0, tone_map: str = "linear",
