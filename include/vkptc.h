@@ -72,13 +72,23 @@ typedef struct vkptc_config {
                                 the same reference tree, bit for bit, plus the traversal tree,
                                 built by CUDA kernels) or VKPTC_BUILD_HOST (the host restatement of
                                 ParallelBvhBuilder, kept as the parity mode) */
-  uint32_t reserved[3];
+  uint32_t triangle_test;    /* VKPTC_TRIANGLE_MT (default): the reference's Moller-Trumbore test
+                                (BvhTriangleIntersector.cpp:35-74), hit ids bit-exact against it;
+                                VKPTC_TRIANGLE_WATERTIGHT: the watertight test of Woop, Benthin and
+                                Wald (JCGT 2013) on the triangles' own vertices, so a ray through a
+                                shared edge or vertex of a closed mesh never passes between its
+                                triangles.  The watertight mode needs the device build; ray queries
+                                and renders of a context honour it, batches and the adjoint do not
+                                take it (VKPTC_UNSUPPORTED). */
+  uint32_t reserved[2];
 } vkptc_config;
 
 #define VKPTC_BVH_REFERENCE 0u
 #define VKPTC_BVH_SAH 1u
 #define VKPTC_BUILD_DEVICE 0u
 #define VKPTC_BUILD_HOST 1u
+#define VKPTC_TRIANGLE_MT 0u
+#define VKPTC_TRIANGLE_WATERTIGHT 1u
 
 /* Mirrors RenderSettings (src/pathtracer/PathTracer.h:134-178). */
 typedef struct vkptc_render_settings {

@@ -16,6 +16,7 @@ Two interchangeable implementations of oracle/vkpt_oracle.h:
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
 import subprocess
@@ -151,7 +152,19 @@ class Oracle:
                                     ctypes.POINTER(ctypes.c_double)]
         L.vko_last_error.restype = ctypes.c_char_p
         L.vko_impl_name.restype = ctypes.c_char_p
+        L.vko_set_triangle_test.restype = ctypes.c_int
+        L.vko_set_triangle_test.argtypes = [ctypes.c_uint32]
         self.kind = L.vko_impl_name().decode()
+
+    @contextlib.contextmanager
+    def triangle_test(self, mode: str):
+        """Traverse with "mt" (the reference's Moller-Trumbore) or "watertight"
+        (port only) inside the block; Moller-Trumbore again afterwards."""
+        self._check(self.lib.vko_set_triangle_test({"mt": 0, "watertight": 1}[mode]))
+        try:
+            yield self
+        finally:
+            self.lib.vko_set_triangle_test(0)
 
     # -- helpers
     @staticmethod

@@ -171,7 +171,67 @@ struct Light {
 struct Prim {
   uint32_t material, index;
   V3 v0, e1, e2, n;
+  V3 v1, v2;   // the other two vertices as given (the watertight test reads vertices, not edges)
 };
+
+// Triangle test of every traversal: 0 = the reference's Moller-Trumbore
+// (BvhTriangleIntersector.cpp:35-74), 1 = watertight (an extension the
+// reference does not have; see wt_test).
+int g_triangle_test = 0;
+
+// The watertight ray/triangle test of Woop, Benthin and Wald ("Watertight
+// Ray/Triangle Intersection", JCGT 2(1), 2013), without back-face culling:
+// shear the ray onto +z along its dominant axis (the first largest |d| on
+// ties, the other two axes swapped when d[kz] < 0), take the three 2D edge
+// functions of the sheared vertices (redone in double when one rounds to
+// exactly 0), reject mixed signs and a zero determinant, and return
+// t = T / det (-1 on a miss).
+struct WtRay {
+  int kx, ky, kz;
+  float sx, sy, sz;
+};
+
+inline float axis_of(V3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+WtRay prep_wt(V3 d) {
+  const float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+  int kz = 0;
+  float m = ax;
+  if (ay > m) {
+    kz = 1;
+    m = ay;
+  }
+  if (az > m) kz = 2;
+  int kx = kz == 2 ? 0 : kz + 1;
+  int ky = kx == 2 ? 0 : kx + 1;
+  const float dz = axis_of(d, kz);
+  if (dz < 0.0f) std::swap(kx, ky);
+  return WtRay{kx, ky, kz, axis_of(d, kx) / dz, axis_of(d, ky) / dz, 1.0f / dz};
+}
+
+float wt_test(const Prim& p, V3 o, const WtRay& w) {
+  const V3 a{p.v0.x - o.x, p.v0.y - o.y, p.v0.z - o.z};
+  const V3 b{p.v1.x - o.x, p.v1.y - o.y, p.v1.z - o.z};
+  const V3 c{p.v2.x - o.x, p.v2.y - o.y, p.v2.z - o.z};
+  const float akz = axis_of(a, w.kz), bkz = axis_of(b, w.kz), ckz = axis_of(c, w.kz);
+  const float Ax = axis_of(a, w.kx) - w.sx * akz, Ay = axis_of(a, w.ky) - w.sy * akz;
+  const float Bx = axis_of(b, w.kx) - w.sx * bkz, By = axis_of(b, w.ky) - w.sy * bkz;
+  const float Cx = axis_of(c, w.kx) - w.sx * ckz, Cy = axis_of(c, w.ky) - w.sy * ckz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    U = static_cast<float>(static_cast<double>(Cx) * By - static_cast<double>(Cy) * Bx);
+    V = static_cast<float>(static_cast<double>(Ax) * Cy - static_cast<double>(Ay) * Cx);
+    W = static_cast<float>(static_cast<double>(Bx) * Ay - static_cast<double>(By) * Ax);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return -1.0f;
+  const float det = U + V + W;
+  if (det == 0.0f) return -1.0f;
+  const float Az = w.sz * akz, Bz = w.sz * bkz, Cz = w.sz * ckz;
+  const float T = U * Az + V * Bz + W * Cz;
+  return T / det;
+}
 
 struct Box { float lo[3], hi[3]; };
 struct Node { Box box; int32_t left, right, first, count; };
@@ -447,6 +507,8 @@ struct World {
         p.material = mat;
         p.index = static_cast<uint32_t>(prims.size());
         p.v0 = v0;
+        p.v1 = v1;
+        p.v2 = v2;
         p.e1 = sub(v1, v0);
         p.e2 = sub(v2, v0);
         // normalize_vec3 of the accelerator: multiply by 1/sqrt(len^2).
@@ -538,12 +600,16 @@ struct World {
 
   // Slab test with per-axis early exit; axes with |d| <= 1e-4 use an inside test.
   struct RayBox { float o[3], inv[3]; bool par[3]; };
+  // The reference's slab setup: an axis with |d| <= 1e-4 counts as parallel
+  // (origin-inside-slab test).  With the watertight test the boxes are tested
+  // geometrically instead (only |d| < 1e-20 is parallel): the rule can cull a
+  // box that a ray drifting up to 1e-4 t along that axis enters.
   static RayBox prep(V3 o, V3 d) {
     RayBox r;
     const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
     for (int a = 0; a < 3; ++a) {
       r.o[a] = oo[a];
-      r.par[a] = std::fabs(dd[a]) <= kEps;
+      r.par[a] = g_triangle_test ? std::fabs(dd[a]) < 1e-20f : std::fabs(dd[a]) <= kEps;
       r.inv[a] = r.par[a] ? 0.0f : 1.0f / dd[a];
     }
     return r;
@@ -572,6 +638,7 @@ struct World {
     float best = std::numeric_limits<float>::infinity();
     int64_t hit = -1;
     const RayBox rb = prep(o, d);
+    const WtRay wr = g_triangle_test ? prep_wt(d) : WtRay{};
     std::vector<int32_t> stack;
     stack.reserve(128);
     stack.push_back(0);
@@ -591,6 +658,14 @@ struct World {
         for (int32_t i = 0; i < nd.count; ++i) {
           const uint32_t pi = order[static_cast<size_t>(nd.first + i)];
           const Prim& p = prims[pi];
+          if (g_triangle_test) {
+            const float t = wt_test(p, o, wr);
+            if (!(t > kEps) || !(t < best)) continue;   // a NaN t never commits
+            ++st.tri_hits;
+            best = t;
+            hit = pi;
+            continue;
+          }
           const float hx = d.y * p.e2.z - d.z * p.e2.y;
           const float hy = d.z * p.e2.x - d.x * p.e2.z;
           const float hz = d.x * p.e2.y - d.y * p.e2.x;
@@ -690,6 +765,8 @@ struct World {
         Prim& p = prims[inst_first[i] + k];
         p.material = mat;
         p.v0 = v[0];
+        p.v1 = v[1];
+        p.v2 = v[2];
         p.e1 = sub(v[1], v[0]);
         p.e2 = sub(v[2], v[0]);
         const V3 cr = cross(p.e1, p.e2);
@@ -1117,6 +1194,12 @@ extern "C" {
 
 const char* vko_last_error(void) { return g_error.c_str(); }
 const char* vko_impl_name(void) { return "port"; }
+
+int vko_set_triangle_test(uint32_t mode) {
+  if (mode > 1u) return fail("unknown triangle test");
+  g_triangle_test = static_cast<int>(mode);
+  return 0;
+}
 
 int vko_set_instance_updates(const vko_instance_update* updates, uint32_t count) {
   g_updates.assign(updates, updates + count);

@@ -394,6 +394,11 @@ int vko_convert_scene_json(const char* path, const char* out_path) {
 
 const char* vko_impl_name(void) { return "reference"; }
 
+int vko_set_triangle_test(uint32_t mode) {
+  // The reference traverses with Moller-Trumbore only.
+  return mode == 0u ? 0 : fail("the reference has no watertight triangle test");
+}
+
 int vko_render(const vko_scene* scene, const vko_settings* settings,
                uint32_t first_sample, uint32_t n_samples, uint32_t threads,
                const uint32_t* pixels, uint32_t pixel_count,

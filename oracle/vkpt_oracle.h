@@ -184,6 +184,11 @@ int vko_apply_film_resolve(const float* hdr_rgb, uint32_t width, uint32_t height
  * 0 on success. */
 int vko_convert_scene_json(const char* path, const char* out_path);
 
+/* Triangle test of later intersect and render calls: 0 = the reference's
+ * Moller-Trumbore (default), 1 = watertight (Woop, Benthin and Wald, JCGT
+ * 2013; an extension: the reference oracle accepts 0 only). */
+int vko_set_triangle_test(uint32_t mode);
+
 const char* vko_last_error(void);
 const char* vko_impl_name(void);
 

@@ -193,6 +193,7 @@ struct FlatIn {
   const unsigned long long* prefix;
   uint32_t ninst;
   uint32_t candidates;
+  uint32_t watertight;          // triangle records hold the vertices (a, b, c), not (v0, e1, e2)
 };
 
 // transform_instance_vertex (the host's TransformInstanceVertex, same operations).
@@ -301,9 +302,15 @@ __global__ void k_flat_write(FlatIn f, const uint32_t* __restrict__ flag, const 
     n = make_float4(nx * inv, ny * inv, nz * inv, __uint_as_float(mat));
   }
   const uint32_t p = pos[c];
-  pv[3 * p + 0] = make_float4(a[0], a[1], a[2], e1x);
-  pv[3 * p + 1] = make_float4(e1y, e1z, e2x, e2y);
-  pv[3 * p + 2] = make_float4(e2z, 0.0f, 0.0f, 0.0f);
+  if (f.watertight) {
+    pv[3 * p + 0] = make_float4(a[0], a[1], a[2], b[0]);
+    pv[3 * p + 1] = make_float4(b[1], b[2], cc[0], cc[1]);
+    pv[3 * p + 2] = make_float4(cc[2], 0.0f, 0.0f, 0.0f);
+  } else {
+    pv[3 * p + 0] = make_float4(a[0], a[1], a[2], e1x);
+    pv[3 * p + 1] = make_float4(e1y, e1z, e2x, e2y);
+    pv[3 * p + 2] = make_float4(e2z, 0.0f, 0.0f, 0.0f);
+  }
   shade[p] = n;
   const float4 lo = make_float4(min3(a[0], b[0], cc[0]) - kPadB, min3(a[1], b[1], cc[1]) - kPadB,
                                 min3(a[2], b[2], cc[2]) - kPadB, 0.0f);
@@ -1291,6 +1298,7 @@ struct RefitTri {
   uint32_t n_up;
   const float* lv;
   const uint32_t* li;
+  uint32_t watertight;      // records hold (a, b, c)
 };
 
 __global__ void k_refit_prims(RefitTri R, uint32_t total, const uint32_t* __restrict__ tri_pos, TriRecord* __restrict__ tris,
@@ -1327,12 +1335,12 @@ __global__ void k_refit_prims(RefitTri R, uint32_t total, const uint32_t* __rest
   r.v0x = a[0];
   r.v0y = a[1];
   r.v0z = a[2];
-  r.e1x = e1x;
-  r.e1y = e1y;
-  r.e1z = e1z;
-  r.e2x = e2x;
-  r.e2y = e2y;
-  r.e2z = e2z;
+  r.e1x = R.watertight ? b[0] : e1x;
+  r.e1y = R.watertight ? b[1] : e1y;
+  r.e1z = R.watertight ? b[2] : e1z;
+  r.e2x = R.watertight ? c[0] : e2x;
+  r.e2y = R.watertight ? c[1] : e2y;
+  r.e2z = R.watertight ? c[2] : e2z;
   blo[p] = make_float4(min3(a[0], b[0], c[0]) - kPadB, min3(a[1], b[1], c[1]) - kPadB, min3(a[2], b[2], c[2]) - kPadB, 0.0f);
   bhi[p] = make_float4(max3(a[0], b[0], c[0]) + kPadB, max3(a[1], b[1], c[1]) + kPadB, max3(a[2], b[2], c[2]) + kPadB, 0.0f);
 }
@@ -1432,7 +1440,8 @@ cudaError_t RefitOnDevice(DeviceRefitState& st, const std::vector<RefitUpdate>& 
   BB_TRY(cudaMemcpyAsync(d_up, updates.data(), updates.size() * sizeof(RefitUpdate), cudaMemcpyHostToDevice, stream));
   BB_TRY(cudaMemcpyAsync(d_off, offset.data(), offset.size() * 4, cudaMemcpyHostToDevice, stream));
   const uint32_t total = offset.back();
-  const RefitTri R{d_up, d_off, static_cast<uint32_t>(updates.size()), local_vertices, local_indices};
+  const RefitTri R{d_up, d_off, static_cast<uint32_t>(updates.size()), local_vertices, local_indices,
+                   st.watertight ? 1u : 0u};
   if (total)
     k_refit_prims<<<grid_for(total), kThreads, 0, stream>>>(R, total, st.tri_pos, reinterpret_cast<TriRecord*>(tris),
                                                             shade, st.blo, st.bhi);
@@ -1502,7 +1511,7 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   const FlatIn f{sc_in.vertices, sc_in.vertex_count, sc_in.indices, sc_in.index_count,
                  sc_in.local_vertices, dyn ? sc_in.local_vertex_count : 0u,
                  sc_in.local_indices, dyn ? sc_in.local_index_count : 0u,
-                 d_inst, d_inst_local, d_inst_tr, d_prefix, instance_count, nc};
+                 d_inst, d_inst_local, d_inst_tr, d_prefix, instance_count, nc, sc_in.watertight ? 1u : 0u};
   if (nc) k_flat_valid<<<grid_for(nc), kThreads, 0, stream>>>(f, flag);
   BB_TRY(exclusive_scan(flag, nc, pos, sc));
   uint32_t n = 0u;
@@ -1513,6 +1522,7 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   float4* bhi = nullptr;
   if (keep_refit) {
     out.refit = new DeviceRefitState();
+    out.refit->watertight = sc_in.watertight;
     BB_TRY(dmalloc(out.refit->blo, n));
     BB_TRY(dmalloc(out.refit->bhi, n));
     BB_TRY(dmalloc(out.refit->inst_first, instance_count + 1u));

@@ -28,6 +28,7 @@ struct DeviceRefitState {
   int32_t* slot_bin = nullptr;      // per wide node: the binary node of each slot (-1 unused)
   uint32_t* inst_first = nullptr;   // per instance: first flattened primitive (host copy below)
   std::vector<uint32_t> host_inst_first, host_inst_count;   // per instance: primitive range
+  bool watertight = false;          // triangle records hold the vertices (a, b, c)
 };
 
 struct DeviceAccelOut {
@@ -62,6 +63,8 @@ struct DeviceSceneArrays {
   uint32_t instance_count = 0;
   const uint32_t* instance_local = nullptr;   // host, 5 per instance (see InstanceGeometry), or null
   const float* instance_transforms = nullptr; // host, 10 per instance, or null
+  bool watertight = false;    // triangle records for the watertight test: vertices (a, b, c) in the
+                              // slots of (v0, e1, e2)
 };
 
 // Builds everything from the scene arrays.  sah: the traversal tree is a

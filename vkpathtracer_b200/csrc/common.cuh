@@ -168,6 +168,7 @@ struct DevScene {
   float squeeze;
   uint32_t stack_required;
   uint32_t reference_tree;   // 1: the traversal tree is the reference's own tree
+  uint32_t watertight;       // 1: triangle records hold vertices, tested watertight
   const float4* sdf;         // SDF primitive records (sdf.cuh), tested after the triangles
   uint32_t sdf_count;
 };

@@ -252,6 +252,7 @@ DevScene dev_scene(const vkptc_ctx* c) {
   s.squeeze = std::isfinite(c->cam.squeeze) ? std::max(0.01f, c->cam.squeeze) : 1.0f;
   s.stack_required = c->wide.stack_required;
   s.reference_tree = c->wide.reference_topology ? 1u : 0u;
+  s.watertight = c->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT ? 1u : 0u;
   s.sdf = c->sdf_count ? c->d_sdf.ptr : nullptr;
   s.sdf_count = c->sdf_count;
   return s;
@@ -303,7 +304,7 @@ int32_t launch_shape(vkptc_ctx* c, cudaStream_t stream, LaunchShape& ls, bool al
   const int32_t rc = ensure_stack_smem(c, ls);
   if (rc != VKPTC_OK) return rc;
   const size_t smem = StackSmemBytes(ls.block, ls.smem_entries);
-  const int per_sm = ExtendBlocksPerSm(ls.block, smem);
+  const int per_sm = ExtendBlocksPerSm(ls.block, smem, c->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT);
   ls.grid = c->sm_count * per_sm;
   const size_t spill = SpillEntries(ls);
   if (spill > 0) {
@@ -491,6 +492,10 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
   auto* c = new (std::nothrow) vkptc_ctx();
   if (!c) return VKPTC_ALLOC_FAILED;
   if (config) c->config = *config;
+  if (c->config.triangle_test > VKPTC_TRIANGLE_WATERTIGHT) {
+    delete c;
+    return VKPTC_INVALID_ARGUMENT;
+  }
   c->device = c->config.device;
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
@@ -823,6 +828,7 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
     a.instance_local = c->raw_instance_local.data();
     a.instance_transforms = c->raw_instance_transforms.data();
   }
+  a.watertight = c->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT;
   const cudaError_t e = BuildAccelOnDevice(a, c->config.bvh_mode == VKPTC_BVH_SAH, c->stream, out);
   if (e != cudaSuccess) {
     FreeDeviceAccel(out);
@@ -877,6 +883,9 @@ int32_t vkptc_build_acceleration(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "build_or_update_acceleration called before load_scene_snapshot");
   cudaSetDevice(ctx->device);
+  const bool watertight = ctx->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT;
+  if (watertight && ctx->config.build_mode == VKPTC_BUILD_HOST)
+    return fail(ctx, VKPTC_UNSUPPORTED, "the watertight triangle test needs the device build");
   if (ctx->config.build_mode != VKPTC_BUILD_HOST) {
     bool done = false;
     const int32_t rc = build_on_device(ctx, &done);
@@ -885,6 +894,8 @@ int32_t vkptc_build_acceleration(vkptc_ctx* ctx) {
       ctx->last_error.clear();
       return VKPTC_OK;
     }
+    // non-finite vertices: the host path builds Moller-Trumbore records only
+    if (watertight) return fail(ctx, VKPTC_UNSUPPORTED, "the watertight triangle test needs finite vertices");
   }
   release_refit(ctx);
   int32_t grc = ensure_geo(ctx);
@@ -903,6 +914,8 @@ int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "load_bvh called before load_scene_snapshot");
   if (!bvh || !bvh->nodes || !bvh->prim_indices) return fail(ctx, VKPTC_INVALID_ARGUMENT, "bvh view is null");
+  if (ctx->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT)
+    return fail(ctx, VKPTC_UNSUPPORTED, "the watertight triangle test needs the device build");
   cudaSetDevice(ctx->device);
   std::vector<BinNode> bin(bvh->node_count);
   for (uint32_t i = 0; i < bvh->node_count; ++i) {
@@ -2022,6 +2035,10 @@ int32_t vkptc_batch_create(const vkptc_config* config, vkptc_batch** out_batch) 
   auto* b = new (std::nothrow) vkptc_batch();
   if (!b) return VKPTC_ALLOC_FAILED;
   if (config) b->config = *config;
+  if (b->config.triangle_test != VKPTC_TRIANGLE_MT) {   // batch jobs use the Moller-Trumbore records
+    delete b;
+    return VKPTC_UNSUPPORTED;
+  }
   b->device = b->config.device;
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -2324,6 +2341,8 @@ int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, cons
     return fail(ctx, VKPTC_NOT_READY, "adjoint requires a configured tracer with a scene and a built acceleration structure");
   }
   if (desc->spp == 0u) return fail(ctx, VKPTC_INVALID_ARGUMENT, "spp must be positive");
+  if (ctx->config.triangle_test != VKPTC_TRIANGLE_MT)
+    return fail(ctx, VKPTC_UNSUPPORTED, "the adjoint uses the Moller-Trumbore triangle test");
   if (ctx->settings.max_depth > VKPTC_ADJ_MAX_DEPTH) {
     return fail(ctx, VKPTC_UNSUPPORTED, "adjoint supports max_depth <= " + std::to_string(VKPTC_ADJ_MAX_DEPTH));
   }

@@ -17,6 +17,7 @@
 // the stages add radiance terms in the reference's order (emission, then the
 // NEE term of the same bounce, then the next bounce).
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "integrator.cuh"
@@ -99,7 +100,7 @@ struct ShadowSource {  // any hit for the NEE queries; adds the term when visibl
   }
 };
 
-template <class Src, bool kAny, bool kStats>
+template <class Src, bool kAny, bool kStats, bool kWt = false>
 __device__ __forceinline__ void run_persistent(const Src& src, uint32_t n, uint32_t* fetch,
                                                int scap, int2* spill, int total, int steps,
                                                unsigned long long* c_nodes, unsigned long long* c_leaves,
@@ -111,7 +112,7 @@ __device__ __forceinline__ void run_persistent(const Src& src, uint32_t n, uint3
                     spill ? spill + gtid : nullptr, gstride, total};
   TraceStats st;
   uint32_t lerr = 0u;
-  persistent_traverse<Src, kAny, kStats>(src, n, fetch, stk, steps, st, lerr);
+  persistent_traverse<Src, kAny, kStats, kWt>(src, n, fetch, stk, steps, st, lerr);
   if (kStats) {
     warp_count(c_nodes, st.nodes);
     warp_count(c_leaves, st.leaves);
@@ -122,11 +123,11 @@ __device__ __forceinline__ void run_persistent(const Src& src, uint32_t n, uint3
 }
 
 // =============================================================== ray queries
-template <bool kAny, bool kStats>
+template <bool kAny, bool kStats, bool kWt>
 __global__ void __launch_bounds__(256) k_trace_rays(DevScene s, RaysSource src, uint32_t n, uint32_t* fetch, int scap,
                                                     int2* spill, int total, int steps, DevCounters* ctr, uint32_t* err) {
-  run_persistent<RaysSource, kAny, kStats>(src, n, fetch, scap, spill, total, steps, &ctr->nodes, &ctr->leaves,
-                                           &ctr->tris, &ctr->ext_rays, err);
+  run_persistent<RaysSource, kAny, kStats, kWt>(src, n, fetch, scap, spill, total, steps, &ctr->nodes, &ctr->leaves,
+                                                &ctr->tris, &ctr->ext_rays, err);
 }
 
 cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* tmax, uint64_t n, bool any_hit,
@@ -138,15 +139,19 @@ cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* t
   if (e != cudaSuccess) return e;
   const RaysSource src{geo_of(s), rays, tmax, prim_out, t_out, any_hit};
   const uint32_t n32 = static_cast<uint32_t>(n);
-#define VKPTC_TR(A, S) \
-  k_trace_rays<A, S><<<ls.grid, ls.block, smem, ls.stream>>>(s, src, n32, fetch, ls.smem_entries, ls.spill, ls.stack_cap, ls.steps, ctr, err)
+#define VKPTC_TR(A, S, W) \
+  k_trace_rays<A, S, W><<<ls.grid, ls.block, smem, ls.stream>>>(s, src, n32, fetch, ls.smem_entries, ls.spill, ls.stack_cap, ls.steps, ctr, err)
+#define VKPTC_TR2(A, S) \
+  if (s.watertight) VKPTC_TR(A, S, true); \
+  else VKPTC_TR(A, S, false)
   if (any_hit) {
-    if (ctr) VKPTC_TR(true, true);
-    else VKPTC_TR(true, false);
+    if (ctr) VKPTC_TR2(true, true);
+    else VKPTC_TR2(true, false);
   } else {
-    if (ctr) VKPTC_TR(false, true);
-    else VKPTC_TR(false, false);
+    if (ctr) VKPTC_TR2(false, true);
+    else VKPTC_TR2(false, false);
   }
+#undef VKPTC_TR2
 #undef VKPTC_TR
   return cudaGetLastError();
 }
@@ -181,7 +186,7 @@ __global__ void __launch_bounds__(256) k_raygen(DevScene s, DevSettings st, Wave
 // ==================================================================== extend
 // Closest-hit traversal of the current extension queue (persistent warps).
 // Zeroes the next queue's and the shadow queue's sizes for the shade stage.
-template <bool kStats>
+template <bool kStats, bool kWt>
 __global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_t cur, int scap, int2* spill,
                                                 int total, int steps, DevCounters* ctr, uint32_t* err) {
   const uint32_t n = w.counts[cur];
@@ -190,8 +195,8 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s, WaveState w, uint32_
     w.counts[2] = 0u;
   }
   const ExtendSource src{geo_of(s), w.q[cur], w.ray_o, w.ray_d, w.hit};
-  run_persistent<ExtendSource, false, kStats>(src, n, &w.counts[3], scap, spill, total, steps, &ctr->nodes,
-                                              &ctr->leaves, &ctr->tris, &ctr->ext_rays, err);
+  run_persistent<ExtendSource, false, kStats, kWt>(src, n, &w.counts[3], scap, spill, total, steps, &ctr->nodes,
+                                                   &ctr->leaves, &ctr->tris, &ctr->ext_rays, err);
 }
 
 constexpr uint32_t kSmemLights = 64;   // lights staged in shared memory by the shade stage
@@ -272,18 +277,18 @@ __global__ void __launch_bounds__(256, 3) k_shade(DevScene s, DevSettings st, Wa
 // ==================================================================== shadow
 // Any-hit visibility of the NEE queries (persistent warps); adds the NEE term
 // of every visible query to its path's radiance.
-template <bool kStats>
+template <bool kStats, bool kWt>
 __global__ void __launch_bounds__(256) k_shadow(DevScene s, WaveState w, int scap, int2* spill, int total, int steps,
                                                 DevCounters* ctr, uint32_t* err) {
   const uint32_t n = w.counts[2];
   const ShadowSource src{geo_of(s), w.sh_o, w.sh_d, w.sh_c, w.sh_path, w.rad};
-  run_persistent<ShadowSource, true, kStats>(src, n, &w.counts[4], scap, spill, total, steps, &ctr->shadow_nodes,
+  run_persistent<ShadowSource, true, kStats, kWt>(src, n, &w.counts[4], scap, spill, total, steps, &ctr->shadow_nodes,
                                              &ctr->shadow_leaves, &ctr->shadow_tris, &ctr->shadow_rays, err);
 }
 
 // Scenes with transmissive materials: the reference's closest-hit loop that
 // steps through up to 8 transmissive occluders (one query per thread).
-template <bool kStats>
+template <bool kStats, bool kWt>
 __global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveState w, int cap, DevCounters* ctr, uint32_t* err) {
   extern __shared__ int2 smem_stack[];
   SmemStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), cap};
@@ -300,16 +305,16 @@ __global__ void __launch_bounds__(256) k_shadow_transmissive(DevScene s, WaveSta
       float remain = o4.w;
       bool visible = true;
       if (!s.has_transmissive) {
-        const RayPrep r = prep_ray(so, sd, s.reference_tree != 0u);
-        visible = !trace_any<kStats>(s, r, remain, stk, st, local_err);
+        const RayPrep r = prep_ray(so, sd, s.reference_tree != 0u, kWt);
+        visible = !trace_any<kStats, kWt>(s, r, remain, stk, st, local_err);
       } else {
         // Closest-hit loop that steps through up to 8 transmissive occluders
         // (src/pathtracer/ScalarCpuPathTracer.cpp:1067-1087).
         for (uint32_t skips = 0; skips < 8u && remain > 0.004f; ++skips) {
-          const RayPrep r = prep_ray(so, sd, s.reference_tree != 0u);
+          const RayPrep r = prep_ray(so, sd, s.reference_tree != 0u, kWt);
           float t;
           uint32_t prim;
-          trace_closest<kStats>(s, r, stk, t, prim, st, local_err);
+          trace_closest<kStats, kWt>(s, r, stk, t, prim, st, local_err);
           if (s.sdf_count != 0u) sdf_closest(s.sdf, s.sdf_count, so, sd, t, prim, sdf_n);
           if (prim == kMiss || t >= remain) break;
           const uint32_t mat_index = (prim & kSdfTag) ? sdf_material(s.sdf, prim & ~kSdfTag)
@@ -405,12 +410,16 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
   uint32_t cur = 0u;
   for (uint32_t depth = 0; depth < st.max_depth; ++depth) {
     tm.begin(1, ls.stream);
-    if (stats)
-      k_extend<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.smem_entries, ls.spill, ls.stack_cap,
-                                                            ls.steps, ctr, err);
-    else
-      k_extend<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.smem_entries, ls.spill, ls.stack_cap,
-                                                             ls.steps, ctr, err);
+#define VKPTC_EXT(S, W) \
+  k_extend<S, W><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, cur, ls.smem_entries, ls.spill, ls.stack_cap, ls.steps, ctr, err)
+    if (s.watertight) {
+      if (stats) VKPTC_EXT(true, true);
+      else VKPTC_EXT(false, true);
+    } else {
+      if (stats) VKPTC_EXT(true, false);
+      else VKPTC_EXT(false, false);
+    }
+#undef VKPTC_EXT
     tm.end(ls.stream);
     tm.begin(2, ls.stream);
     if (s.has_effects) {
@@ -423,17 +432,29 @@ cudaError_t LaunchWave(const DevScene& s, const DevSettings& st, const WaveState
     tm.end(ls.stream);
     if (st.enable_nee) {
       tm.begin(3, ls.stream);
+#define VKPTC_SHT(S, W) \
+  k_shadow_transmissive<S, W><<<ls.grid, ls.block, smem_full, ls.stream>>>(s, w, ls.stack_cap, ctr, err)
+#define VKPTC_SH(S, W) \
+  k_shadow<S, W><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.smem_entries, ls.spill, ls.stack_cap, ls.steps, ctr, err)
       if (s.has_transmissive) {
-        if (stats) k_shadow_transmissive<true><<<ls.grid, ls.block, smem_full, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
-        else k_shadow_transmissive<false><<<ls.grid, ls.block, smem_full, ls.stream>>>(s, w, ls.stack_cap, ctr, err);
+        if (s.watertight) {
+          if (stats) VKPTC_SHT(true, true);
+          else VKPTC_SHT(false, true);
+        } else {
+          if (stats) VKPTC_SHT(true, false);
+          else VKPTC_SHT(false, false);
+        }
       } else {
-        if (stats)
-          k_shadow<true><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.smem_entries, ls.spill, ls.stack_cap,
-                                                                ls.steps, ctr, err);
-        else
-          k_shadow<false><<<ls.grid, ls.block, smem, ls.stream>>>(s, w, ls.smem_entries, ls.spill, ls.stack_cap,
-                                                                 ls.steps, ctr, err);
+        if (s.watertight) {
+          if (stats) VKPTC_SH(true, true);
+          else VKPTC_SH(false, true);
+        } else {
+          if (stats) VKPTC_SH(true, false);
+          else VKPTC_SH(false, false);
+        }
       }
+#undef VKPTC_SH
+#undef VKPTC_SHT
       tm.end(ls.stream);
     }
     cur ^= 1u;
@@ -559,22 +580,31 @@ static cudaError_t set_smem(K kernel, int bytes) {
 
 cudaError_t ConfigureStackSmem(size_t bytes) {
   const int b = static_cast<int>(bytes);
-  cudaError_t e = set_smem(k_trace_rays<true, true>, b);
-  if (e == cudaSuccess) e = set_smem(k_trace_rays<true, false>, b);
-  if (e == cudaSuccess) e = set_smem(k_trace_rays<false, true>, b);
-  if (e == cudaSuccess) e = set_smem(k_trace_rays<false, false>, b);
-  if (e == cudaSuccess) e = set_smem(k_extend<true>, b);
-  if (e == cudaSuccess) e = set_smem(k_extend<false>, b);
-  if (e == cudaSuccess) e = set_smem(k_shadow<true>, b);
-  if (e == cudaSuccess) e = set_smem(k_shadow<false>, b);
-  if (e == cudaSuccess) e = set_smem(k_shadow_transmissive<true>, b);
-  if (e == cudaSuccess) e = set_smem(k_shadow_transmissive<false>, b);
+  cudaError_t e = cudaSuccess;
+  const auto all = [&](auto wt) {
+    constexpr bool W = decltype(wt)::value;
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<true, true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<true, false, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<false, true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<false, false, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_extend<true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_extend<false, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_shadow<true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_shadow<false, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_shadow_transmissive<true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_shadow_transmissive<false, W>, b);
+  };
+  all(std::false_type{});
+  all(std::true_type{});
   return e;
 }
 
-int ExtendBlocksPerSm(int block, size_t smem) {
+int ExtendBlocksPerSm(int block, size_t smem, bool watertight) {
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_extend<false>, block, smem) != cudaSuccess) return 1;
+  const cudaError_t e = watertight
+      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_extend<false, true>, block, smem)
+      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_extend<false, false>, block, smem);
+  if (e != cudaSuccess) return 1;
   return blocks > 0 ? blocks : 1;
 }
 

@@ -64,7 +64,7 @@ size_t StackSmemBytes(int block, int cap);
 // Spill entries the launch needs beyond shared memory.
 size_t SpillEntries(const LaunchShape& ls);
 // Resident blocks per SM of the traversal stage for this block size and stack.
-int ExtendBlocksPerSm(int block, size_t smem);
+int ExtendBlocksPerSm(int block, size_t smem, bool watertight = false);
 // Raises the dynamic shared-memory limit of every stack-using kernel.
 cudaError_t ConfigureStackSmem(size_t bytes);
 

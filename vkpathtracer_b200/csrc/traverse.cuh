@@ -45,12 +45,20 @@ struct RayPrep {
 // (an exactly-zero component uses the inside rule, which is then exact) and
 // the rule is applied where it decides the result: a hit on a triangle counts
 // only if the origin lies inside its REFERENCE leaf's slab on those axes.
-__device__ __forceinline__ RayPrep prep_ray(V3 o, V3 d, bool reference_tree = true) {
+// watertight: no such rule anywhere.  The rule treats an axis with |d| <= 1e-4
+// as parallel although the ray drifts up to 1e-4 t along it, more than the
+// boxes' 1e-4 padding, so it can cull a box the ray enters; the watertight mode
+// tests every box geometrically (only |d| < 1e-20 uses the inside rule).
+__device__ __forceinline__ RayPrep prep_ray(V3 o, V3 d, bool reference_tree = true, bool watertight = false) {
   RayPrep r;
   r.ox = o.x; r.oy = o.y; r.oz = o.z;
   r.dx = d.x; r.dy = d.y; r.dz = d.z;
   r.par = (fabsf(d.x) <= kEps ? 1u : 0u) | (fabsf(d.y) <= kEps ? 2u : 0u) | (fabsf(d.z) <= kEps ? 4u : 0u);
-  if (reference_tree) {
+  if (watertight) {
+    r.par = (fabsf(d.x) < 1e-20f ? 1u : 0u) | (fabsf(d.y) < 1e-20f ? 2u : 0u) | (fabsf(d.z) < 1e-20f ? 4u : 0u);
+    r.node_par = r.par;
+    r.leaf_par = 0u;
+  } else if (reference_tree) {
     r.node_par = r.par;
     r.leaf_par = 0u;
   } else {
@@ -159,6 +167,87 @@ __device__ __forceinline__ float mt_test(const float4 a, const float4 b, const f
   return t;
 }
 
+// Per-ray constants of the watertight test (Woop, Benthin and Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2(1), 2013): kz is the axis of the largest
+// |d| (the first on ties), kx and ky follow it cyclically and are swapped when
+// d[kz] < 0, which keeps the triangles' winding; the shear maps the ray onto
+// +z: sx = d[kx]/d[kz], sy = d[ky]/d[kz], sz = 1/d[kz].
+struct WtRay {
+  int kx, ky, kz;
+  float sx, sy, sz;
+};
+
+__device__ __forceinline__ float axis_of(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
+
+__device__ __forceinline__ WtRay prep_wt(const RayPrep& r) {
+  const float ax = fabsf(r.dx), ay = fabsf(r.dy), az = fabsf(r.dz);
+  int kz = 0;
+  float m = ax;
+  if (ay > m) {
+    kz = 1;
+    m = ay;
+  }
+  if (az > m) kz = 2;
+  int kx = kz == 2 ? 0 : kz + 1;
+  int ky = kx == 2 ? 0 : kx + 1;
+  const float dz = axis_of(r.dx, r.dy, r.dz, kz);
+  if (dz < 0.0f) {
+    const int t = kx;
+    kx = ky;
+    ky = t;
+  }
+  WtRay w;
+  w.kx = kx;
+  w.ky = ky;
+  w.kz = kz;
+  w.sx = __fdiv_rn(axis_of(r.dx, r.dy, r.dz, kx), dz);
+  w.sy = __fdiv_rn(axis_of(r.dx, r.dy, r.dz, ky), dz);
+  w.sz = __fdiv_rn(1.0f, dz);
+  return w;
+}
+
+// The watertight test without back-face culling on a record holding the
+// vertices (a, b, c) in the slots of (v0, e1, e2).  The three edge functions
+// of the sheared 2D triangle are computed from the vertices themselves, so two
+// triangles sharing an edge evaluate it identically (up to sign) and no ray
+// passes between them; an edge function that rounds to exactly 0 is redone in
+// double (the products are exact there).  Returns t = T/det, or -1 on a miss.
+__device__ __forceinline__ float wt_test(const float4 p, const float4 q, const float4 s, const RayPrep& r,
+                                         const WtRay& w) {
+  const float ax = __fsub_rn(p.x, r.ox), ay = __fsub_rn(p.y, r.oy), az = __fsub_rn(p.z, r.oz);
+  const float bx = __fsub_rn(p.w, r.ox), by = __fsub_rn(q.x, r.oy), bz = __fsub_rn(q.y, r.oz);
+  const float cx = __fsub_rn(q.z, r.ox), cy = __fsub_rn(q.w, r.oy), cz = __fsub_rn(s.x, r.oz);
+  const float akz = axis_of(ax, ay, az, w.kz), bkz = axis_of(bx, by, bz, w.kz), ckz = axis_of(cx, cy, cz, w.kz);
+  const float Ax = __fsub_rn(axis_of(ax, ay, az, w.kx), __fmul_rn(w.sx, akz));
+  const float Ay = __fsub_rn(axis_of(ax, ay, az, w.ky), __fmul_rn(w.sy, akz));
+  const float Bx = __fsub_rn(axis_of(bx, by, bz, w.kx), __fmul_rn(w.sx, bkz));
+  const float By = __fsub_rn(axis_of(bx, by, bz, w.ky), __fmul_rn(w.sy, bkz));
+  const float Cx = __fsub_rn(axis_of(cx, cy, cz, w.kx), __fmul_rn(w.sx, ckz));
+  const float Cy = __fsub_rn(axis_of(cx, cy, cz, w.ky), __fmul_rn(w.sy, ckz));
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    U = __double2float_rn(__dsub_rn(__dmul_rn(Cx, By), __dmul_rn(Cy, Bx)));
+    V = __double2float_rn(__dsub_rn(__dmul_rn(Ax, Cy), __dmul_rn(Ay, Cx)));
+    W = __double2float_rn(__dsub_rn(__dmul_rn(Bx, Ay), __dmul_rn(By, Ax)));
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return -1.0f;
+  const float det = __fadd_rn(__fadd_rn(U, V), W);
+  if (det == 0.0f) return -1.0f;
+  const float Az = __fmul_rn(w.sz, akz), Bz = __fmul_rn(w.sz, bkz), Cz = __fmul_rn(w.sz, ckz);
+  const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+  return __fdiv_rn(T, det);
+}
+
+// The configured triangle test: the reference's Moller-Trumbore, or watertight.
+template <bool kWt>
+__device__ __forceinline__ float tri_test(const float4 a, const float4 b, const float4 c, const RayPrep& r,
+                                          const WtRay& w) {
+  if constexpr (kWt) return wt_test(a, b, c, r, w);
+  else return mt_test(a, b, c, r);
+}
+
 __device__ __forceinline__ void tie_box(const float4* tie, int32_t id, float lo[3], float hi[3]) {
   const float4 a = __ldg(tie + 2 * id);
   const float4 b = __ldg(tie + 2 * id + 1);
@@ -230,9 +319,11 @@ __device__ __forceinline__ int32_t leaf_count(int32_t ref) { return ((~ref) & 7)
 
 // Closest hit.  best_t = +inf and prim = kMiss on a miss.  `err` receives 1 on
 // a stack overflow (which the host-side sizing rules out).
-template <bool kStats>
+template <bool kStats, bool kWt = false>
 __device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& r, SmemStack stk, float& best_t,
                                               uint32_t& best_prim, TraceStats& st, uint32_t& err) {
+  WtRay w{};
+  if constexpr (kWt) w = prep_wt(r);
   best_t = kInf;
   best_prim = kMiss;
   uint32_t best_leaf = 0u, best_lane = 0u;
@@ -292,7 +383,7 @@ __device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& 
       for (int32_t i = 0; i < count; ++i) {
         const float4* tp = s.tris + 3 * (first + i);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
-        const float th = mt_test(a, b, cc, r);
+        const float th = tri_test<kWt>(a, b, cc, r, w);
         if (th <= kEps) continue;   // also rejects the -1 miss code
         if (r.leaf_par != 0u && !leaf_rule_ok(s.tie, __float_as_uint(cc.z), r)) continue;
         if (th < best_t) {
@@ -324,10 +415,12 @@ __device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& 
 }
 
 // Any hit with 1e-4 < t < tmax.  Returns true when occluded.
-template <bool kStats>
+template <bool kStats, bool kWt = false>
 __device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, float tmax, SmemStack stk,
                                           TraceStats& st, uint32_t& err) {
   if (s.prim_count == 0u || !(tmax > kEps)) return false;
+  WtRay w{};
+  if constexpr (kWt) w = prep_wt(r);
   int sp = 0;
   int32_t ref = 0;
   while (true) {
@@ -374,7 +467,7 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, f
       for (int32_t i = 0; i < count; ++i) {
         const float4* tp = s.tris + 3 * (first + i);
         const float4 tc = __ldg(tp + 2);
-        const float th = mt_test(__ldg(tp), __ldg(tp + 1), tc, r);
+        const float th = tri_test<kWt>(__ldg(tp), __ldg(tp + 1), tc, r, w);
         if (th > kEps && th < tmax && (r.leaf_par == 0u || leaf_rule_ok(s.tie, __float_as_uint(tc.z), r))) return true;
       }
     }
@@ -425,6 +518,7 @@ __host__ __device__ __forceinline__ GeoView geo_of(const DevScene& s) {
 struct LaneState {
   GeoView g;
   RayPrep r;
+  WtRay w;          // watertight test constants (unused by the Moller-Trumbore kernels)
   float t;          // closest: best distance so far; any: the query's upper bound
   uint32_t prim;    // closest: primitive; any: 1 when occluded
   uint32_t leaf, lane;
@@ -432,8 +526,10 @@ struct LaneState {
   int sp;
 };
 
+template <bool kWt = false>
 __device__ __forceinline__ void lane_begin(LaneState& L, V3 o, V3 d, float tmax, bool any) {
-  L.r = prep_ray(o, d, L.g.reference_tree != 0u);
+  L.r = prep_ray(o, d, L.g.reference_tree != 0u, kWt);
+  if constexpr (kWt) L.w = prep_wt(L.r);
   L.t = any ? tmax : kInf;
   L.prim = any ? 0u : kMiss;
   L.leaf = L.lane = 0u;
@@ -442,7 +538,7 @@ __device__ __forceinline__ void lane_begin(LaneState& L, V3 o, V3 d, float tmax,
 }
 
 // Returns true when the query has finished.
-template <bool kAny, bool kStats>
+template <bool kAny, bool kStats, bool kWt = false>
 __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk, TraceStats& st, uint32_t& err) {
   if (L.ref >= 0) {
     const float4* np = L.g.nodes + 8 * L.ref;
@@ -494,7 +590,7 @@ __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk
     for (int32_t i = 0; i < count; ++i) {
       const float4* tp = L.g.tris + 3 * (first + i);
       const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
-      const float th = mt_test(a, b, cc, L.r);
+      const float th = tri_test<kWt>(a, b, cc, L.r, L.w);
       if (th <= kEps) continue;
       if (L.r.leaf_par != 0u && !leaf_rule_ok(L.g.tie, __float_as_uint(cc.z), L.r)) continue;
       if (kAny) {
@@ -531,7 +627,7 @@ __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk
 // Each warp keeps its lanes busy: whenever lanes are idle it claims that many
 // query ids with one atomic (warp-aggregated) and refills them; lanes run up
 // to `steps` node/leaf steps between refills.
-template <class Src, bool kAny, bool kStats>
+template <class Src, bool kAny, bool kStats, bool kWt = false>
 __device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, uint32_t* fetch,
                                                     TwoLevelStack stk, int steps, TraceStats& st, uint32_t& err) {
   const unsigned lane_id = threadIdx.x & 31u;
@@ -552,7 +648,7 @@ __device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, 
           V3 o, d;
           float tmax;
           src.load(j, o, d, tmax, L.g);
-          lane_begin(L, o, d, tmax, kAny);
+          lane_begin<kWt>(L, o, d, tmax, kAny);
           if (L.g.prim_count == 0u || (kAny && !(tmax > kEps))) {
             src.finish(j, L.t, L.prim);
             if (kStats) ++st.rays;
@@ -566,7 +662,7 @@ __device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, 
     if (!__any_sync(0xffffffffu, active)) break;
     if (active) {
       for (int k = 0; k < steps; ++k) {
-        if (lane_step<kAny, kStats>(L, stk, st, err)) {
+        if (lane_step<kAny, kStats, kWt>(L, stk, st, err)) {
           src.finish(tag, L.t, L.prim);
           if (kStats) ++st.rays;
           active = false;

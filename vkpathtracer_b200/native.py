@@ -23,11 +23,12 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
                 ("math_mode", ctypes.c_uint32), ("collect_stats", ctypes.c_uint32), ("wave_paths", ctypes.c_uint32),
                 ("stage_timing", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("bvh_mode", ctypes.c_uint32),
-                ("build_mode", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
+                ("build_mode", ctypes.c_uint32), ("triangle_test", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2)]
 
 
 BVH_REFERENCE, BVH_SAH = 0, 1
 BUILD_DEVICE, BUILD_HOST = 0, 1
+TRIANGLE_MT, TRIANGLE_WATERTIGHT = 0, 1
 ACCEL_WIDE_NODES, ACCEL_TRIANGLES, ACCEL_TIE_NODES, ACCEL_SHADING = range(4)
 
 

@@ -492,22 +492,54 @@ def _uv_sphere(n_lat: int, n_lon: int):
 
 
 def displaced_sphere(resolution: int = 724, amplitude: float = 0.05, octaves: int = 8,
-                     seed: int = 2, scale: float = 16.0) -> Scene:
+                     seed: int = 2, scale: float = 16.0, weld_poles: bool = False) -> Scene:
     """Grid sphere (resolution x resolution vertices), radius 1 displaced radially by
     value-noise fBm of the given amplitude, then scaled uniformly.
 
     At resolution 724 this is 2*723*724 = 1,046,904 triangles.  The scale factor
     16 keeps triangles clear of the reference's absolute |det| < 1e-4 cull,
     which rejects every triangle of the unit-radius mesh.
+
+    sin(pi) is not 0 in floating point, so the last row is a ring of distinct
+    vertices about 1e-15 apart around the south pole: a hole no triangle
+    covers.  weld_poles=True moves each pole row onto one vertex, which makes
+    the mesh closed (for watertightness checks).
     """
     dirs, tris = _uv_sphere(resolution, resolution)
     r = 1.0 + amplitude * value_noise(dirs, octaves, seed)
     verts = (dirs * (r * scale)[:, None]).astype(np.float32)
+    if weld_poles:
+        verts[:resolution] = verts[0]
+        verts[-resolution:] = np.array([0.0, verts[-resolution:, 1].mean(), 0.0], np.float32)
     mats = np.array([material(albedo=(0.7, 0.7, 0.7), roughness=1.0)])
     inst = np.array([[0, tris.shape[0], 0]], dtype=np.uint32)
     cam = Camera(position=(0.0, 0.0, 3.0 * scale), target=(0.0, 0.0, 0.0), fov_deg=45.0)
     return Scene(verts, tris.astype(np.uint32), inst, mats, np.zeros((0, 16), np.float32),
                  (0.0, 0.0, 0.0), cam, "displaced_sphere").contiguous()
+
+
+def edge_probe_rays(scene: Scene, origins, edge_fracs=(0.5, 1.0 / 3.0), max_rays: int = 0,
+                    seed: int = 0) -> np.ndarray:
+    """(N,6) float32 rays from each origin aimed at every vertex of the scene
+    and at points along every edge (fractions edge_fracs): the rays that slip
+    between the triangles of a closed mesh when the triangle test is not
+    watertight.  max_rays > 0 keeps a seeded random subset of that size."""
+    v = np.asarray(scene.vertices, np.float64)
+    tri = np.asarray(scene.indices, np.int64).reshape(-1, 3)
+    edges = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]])
+    edges = np.unique(np.sort(edges, axis=1), axis=0)
+    targets = np.concatenate([v] + [v[edges[:, 0]] + f * (v[edges[:, 1]] - v[edges[:, 0]]) for f in edge_fracs])
+    out = []
+    for o in origins:
+        o = np.asarray(o, np.float64)
+        d = targets - o
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        out.append(np.concatenate([np.broadcast_to(o, d.shape), d], axis=1))
+    rays = np.concatenate(out).astype(np.float32)
+    if max_rays and rays.shape[0] > max_rays:
+        keep = np.sort(np.random.RandomState(seed).choice(rays.shape[0], max_rays, replace=False))
+        rays = rays[keep]
+    return np.ascontiguousarray(rays)
 
 
 def _normalize_f32(v: np.ndarray) -> np.ndarray:

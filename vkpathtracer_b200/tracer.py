@@ -137,7 +137,9 @@ class CudaPathTracer:
 
     def __init__(self, device: int = 0, block_size: int = 0, stack_depth: int = 0, math_mode: int = 0,
                  collect_stats: bool = False, wave_paths: int = 0, stage_timing: bool = False,
-                 steps: int = 0, bvh: str = "reference", build: str = "device"):
+                 steps: int = 0, bvh: str = "reference", build: str = "device", triangle_test: str = "mt"):
+        """triangle_test: "mt" (the reference's Moller-Trumbore, hit ids bit-exact
+        against it) or "watertight" (Woop, Benthin and Wald; device build only)."""
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -150,6 +152,7 @@ class CudaPathTracer:
         cfg.steps = steps
         cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
         cfg.build_mode = native.BUILD_HOST if build == "host" else native.BUILD_DEVICE
+        cfg.triangle_test = {"mt": native.TRIANGLE_MT, "watertight": native.TRIANGLE_WATERTIGHT}[triangle_test]
         handle = ctypes.c_void_p()
         rc = self._lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle))
         if rc != native.OK:
