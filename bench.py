@@ -559,6 +559,29 @@ def profile_build(local):
             print(json.dumps({"profile_build": bvh, "build_ms": t.accel_info()["build_ms"]}), flush=True)
 
 
+def profile_rays(local, triangle_test):
+    """Small fixed run for profilers: the 8,388,608 ray-query rays on the
+    1,046,904-triangle sphere (SAH traversal tree), closest hit twice then
+    any hit twice, with the given triangle test ("mt" or "watertight")."""
+    import torch
+    from vkpathtracer_b200.tracer import CudaPathTracer
+    sc = scenes.displaced_sphere()
+    rays = scenes.ray_query_rays(sc)
+    n = rays.shape[0]
+    with CudaPathTracer(device=local, bvh="sah", triangle_test=triangle_test) as t:
+        t.configure(scenes.RenderSettings(width=8, height=8, spp=1))
+        t.load_scene_snapshot(sc)
+        t.build_or_update_acceleration()
+        d_rays = torch.from_numpy(rays).cuda()
+        prim = torch.empty(n, dtype=torch.int32, device="cuda")
+        dist = torch.empty(n, dtype=torch.float32, device="cuda")
+        s = torch.cuda.Stream()
+        for mode in (0, 0, 1, 1):
+            t.trace_rays_device(d_rays.data_ptr(), 0, n, mode, prim.data_ptr(), dist.data_ptr(), s.cuda_stream)
+        s.synchronize()
+    print(json.dumps({"profile_rays": triangle_test, "rays": n, "triangles": sc.triangle_count}), flush=True)
+
+
 def profile_sdf(local):
     """Small fixed run for profilers: the SDF gallery (640x360, 4 spp, depth 8)
     rendered twice by the loop driver without a CUDA graph."""
@@ -738,6 +761,8 @@ def main():
                     help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
     ap.add_argument("--profile-build", action="store_true",
                     help="profiling aid: build the 2M-triangle sphere grid twice per traversal tree and exit")
+    ap.add_argument("--profile-rays", choices=["mt", "watertight"], default=None,
+                    help="profiling aid: trace the ray-query rays closest hit twice and any hit twice, and exit")
     ap.add_argument("--profile-sdf", action="store_true",
                     help="profiling aid: render the SDF gallery twice with the loop driver, no CUDA graph, and exit")
     ap.add_argument("--cpu-step-seconds", type=float, default=0.0,
@@ -751,6 +776,8 @@ def main():
             profile_build(local)
         elif args.profile_sdf:
             profile_sdf(local)
+        elif args.profile_rays:
+            profile_rays(local, args.profile_rays)
         elif args.profile_run:
             profile_run(args, local)
         elif args.impl == "reference":
