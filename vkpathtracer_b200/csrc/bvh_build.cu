@@ -346,27 +346,56 @@ struct BuildArrays {
   float* split;            // per slot (midpoint) / best bin (SAH, as bits)
   uint32_t* nl;            // per slot
   uint32_t* ident;         // per slot: 1 = order unchanged, count/2 split
-  uint32_t* counter;       // [0] next temporary node id, [1] next-level active count, [2] small count
+  uint32_t* counter;       // [0] next temporary node id, [1] next-level active count, [2] small count,
+                           // [4] this level's active count, [5] first temporary id of this level's children
 };
 
-__global__ void k_level_init(BuildArrays A, const uint32_t* __restrict__ act, uint32_t n_act) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_act) return;
-  A.slot_of[act[s]] = static_cast<int32_t>(s);
-  uint32_t* k = A.cb + 6 * s;
-  k[0] = k[1] = k[2] = 0xffffffffu;   // min keys
-  k[3] = k[4] = k[5] = 0u;            // max keys
+// The level loop runs without the host: every per-level kernel reads the
+// level's active count from counter[4] (0 after the last level: the kernels
+// return at once, so the host may queue levels ahead of its checks).
+__device__ __forceinline__ uint32_t level_active(const BuildArrays& A) { return A.counter[4]; }
+
+__device__ __forceinline__ uint32_t grid_thread() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t grid_threads() { return gridDim.x * blockDim.x; }
+
+__global__ void k_level_init(BuildArrays A, const uint32_t* __restrict__ act) {
+  const uint32_t n_act = level_active(A);
+  for (uint32_t s = grid_thread(); s < n_act; s += grid_threads()) {
+    A.slot_of[act[s]] = static_cast<int32_t>(s);
+    uint32_t* k = A.cb + 6 * s;
+    k[0] = k[1] = k[2] = 0xffffffffu;   // min keys
+    k[3] = k[4] = k[5] = 0u;            // max keys
+  }
 }
 
-__global__ void k_level_done(BuildArrays A, const uint32_t* __restrict__ act, uint32_t n_act) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n_act) A.slot_of[act[s]] = -1;
+__global__ void k_level_done(BuildArrays A, const uint32_t* __restrict__ act) {
+  const uint32_t n_act = level_active(A);
+  for (uint32_t s = grid_thread(); s < n_act; s += grid_threads()) A.slot_of[act[s]] = -1;
 }
+
+// End of a level: the children ids advance past this level's children, the
+// next level's active list becomes current, its counter is cleared.
+__global__ void k_level_advance(BuildArrays A) {
+  A.counter[5] += 2u * A.counter[4];
+  A.counter[4] = A.counter[1];
+  A.counter[1] = 0u;
+}
+
+// The scattered order of a level becomes the current one (skipped when the
+// level had no active node: its scatter wrote nothing).
+__global__ void k_copy_level(BuildArrays A, uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, uint32_t n) {
+  if (level_active(A) == 0u) return;
+  for (uint32_t i = grid_thread(); i < n; i += grid_threads()) dst[i] = src[i];
+}
+
+// After the last level: temporary ids of the small subtrees start after the levels' nodes.
+__global__ void k_small_base(BuildArrays A) { A.counter[0] = A.counter[5]; }
 
 // Centroid bounds of every active node: segmented warp reduction over runs of
 // positions of the same node, then one atomic per run and key.
 __global__ void k_centroid_bounds(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
                                   uint32_t n) {
+  if (level_active(A) == 0u) return;   // uniform over the grid
   const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned lane = threadIdx.x & 31u;
   int32_t s = -1;
@@ -432,26 +461,27 @@ __global__ void k_centroid_bounds(BuildArrays A, const uint32_t* __restrict__ id
 }
 
 // Widest centroid axis and its midpoint (BuildBinaryBvh's split).
-__global__ void k_midpoint_split(BuildArrays A, uint32_t n_act) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_act) return;
-  const uint32_t* k = A.cb + 6 * s;
-  float clo[3], chi[3];
-  for (int a = 0; a < 3; ++a) {
-    clo[a] = fval(k[a]);
-    chi[a] = fval(k[3 + a]);
-  }
-  int axis = 0;
-  float widest = chi[0] - clo[0];
-  for (int a = 1; a < 3; ++a) {
-    const float e = chi[a] - clo[a];
-    if (e > widest) {
-      widest = e;
-      axis = a;
+__global__ void k_midpoint_split(BuildArrays A) {
+  const uint32_t n_act = level_active(A);
+  for (uint32_t s = grid_thread(); s < n_act; s += grid_threads()) {
+    const uint32_t* k = A.cb + 6 * s;
+    float clo[3], chi[3];
+    for (int a = 0; a < 3; ++a) {
+      clo[a] = fval(k[a]);
+      chi[a] = fval(k[3 + a]);
     }
+    int axis = 0;
+    float widest = chi[0] - clo[0];
+    for (int a = 1; a < 3; ++a) {
+      const float e = chi[a] - clo[a];
+      if (e > widest) {
+        widest = e;
+        axis = a;
+      }
+    }
+    A.axis[s] = axis;
+    A.split[s] = 0.5f * (clo[axis] + chi[axis]);
   }
-  A.axis[s] = axis;
-  A.split[s] = 0.5f * (clo[axis] + chi[axis]);
 }
 
 __device__ __forceinline__ bool goes_left(const BuildArrays& A, uint32_t p, int32_t s, bool sah) {
@@ -468,6 +498,7 @@ __device__ __forceinline__ bool goes_left(const BuildArrays& A, uint32_t p, int3
 
 __global__ void k_flags(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
                         uint32_t n, uint32_t* __restrict__ flag, bool sah) {
+  if (level_active(A) == 0u) return;
   const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
   if (pos >= n) return;
   const int32_t s = A.slot_of[node_of[pos]];
@@ -476,11 +507,10 @@ __global__ void k_flags(BuildArrays A, const uint32_t* __restrict__ idx, const u
 
 // Children of every active node; big ones go to the next level's list, small
 // ones to the per-thread list, leaves nowhere.
-__global__ void k_children(BuildArrays A, const uint32_t* __restrict__ act, uint32_t n_act, uint32_t base,
-                           const uint32_t* __restrict__ excl, uint32_t* __restrict__ next_act,
-                           uint32_t* __restrict__ small) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_act) return;
+__global__ void k_children(BuildArrays A, const uint32_t* __restrict__ act, const uint32_t* __restrict__ excl,
+                           uint32_t* __restrict__ next_act, uint32_t* __restrict__ small) {
+  const uint32_t n_act = level_active(A), base = A.counter[5];
+  for (uint32_t s = grid_thread(); s < n_act; s += grid_threads()) {
   const uint32_t nd = act[s];
   TNode& t = A.nodes[nd];
   const uint32_t b = static_cast<uint32_t>(t.begin), n = static_cast<uint32_t>(t.count);
@@ -501,11 +531,13 @@ __global__ void k_children(BuildArrays A, const uint32_t* __restrict__ act, uint
     if (cnt[c] > kSmallNode) next_act[atomicAdd(&A.counter[1], 1u)] = id[c];
     else if (cnt[c] > kLeafMax) small[atomicAdd(&A.counter[2], 1u)] = id[c];
   }
+  }
 }
 
 __global__ void k_scatter(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
                           uint32_t n, const uint32_t* __restrict__ excl, uint32_t* __restrict__ idx2,
                           uint32_t* __restrict__ node2) {
+  if (level_active(A) == 0u) return;
   const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
   if (pos >= n) return;
   const uint32_t nd = node_of[pos];
@@ -671,17 +703,19 @@ __global__ void k_small(BuildArrays A, const uint32_t* __restrict__ small, uint3
 // ---------------------------------------------------------------- SAH binning of large nodes
 // Per active slot: 3 axes x 32 bins x (count, 6 bound keys).
 constexpr int kBinWords = 7;
-__global__ void k_sah_bin_init(uint32_t* __restrict__ bins, uint32_t n_act) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_act * 3u * kSahBins) return;
-  uint32_t* w = bins + kBinWords * i;
-  w[0] = 0u;
-  w[1] = w[2] = w[3] = 0xffffffffu;
-  w[4] = w[5] = w[6] = 0u;
+__global__ void k_sah_bin_init(BuildArrays A, uint32_t* __restrict__ bins) {
+  const uint32_t total = level_active(A) * 3u * kSahBins;
+  for (uint32_t i = grid_thread(); i < total; i += grid_threads()) {
+    uint32_t* w = bins + kBinWords * i;
+    w[0] = 0u;
+    w[1] = w[2] = w[3] = 0xffffffffu;
+    w[4] = w[5] = w[6] = 0u;
+  }
 }
 
 __global__ void k_sah_bin(BuildArrays A, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ node_of,
                           uint32_t n, uint32_t* __restrict__ bins) {
+  if (level_active(A) == 0u) return;   // uniform over the grid
   const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
   int32_t s = -1;
   uint32_t p = 0u;
@@ -726,10 +760,11 @@ __global__ void k_sah_bin(BuildArrays A, const uint32_t* __restrict__ idx, const
 // warp per node: lane b holds bin b; suffix and prefix counts and bounds by
 // shuffle scans, the cheapest plane by a warp argmin (lowest axis, then bin,
 // on equal cost, as the sequential sweep keeps the first minimum).
-__global__ void k_sah_split(BuildArrays A, const uint32_t* __restrict__ bins, uint32_t n_act) {
-  const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void k_sah_split(BuildArrays A, const uint32_t* __restrict__ bins) {
+  const uint32_t n_act = level_active(A);
   const int lane = static_cast<int>(threadIdx.x & 31u);
-  if (s >= n_act) return;
+  // one warp per node, warp-strided (s is uniform within a warp)
+  for (uint32_t s = grid_thread() >> 5; s < n_act; s += grid_threads() >> 5) {
   const uint32_t* k = A.cb + 6 * s;
   float best_cost = FLT_MAX;
   int best_axis = -1, best_bin = -1;
@@ -809,6 +844,7 @@ __global__ void k_sah_split(BuildArrays A, const uint32_t* __restrict__ bins, ui
   if (lane == 0) {
     A.axis[s] = best_axis;
     A.split[s] = __uint_as_float(static_cast<uint32_t>(best_bin < 0 ? 0 : best_bin));
+  }
   }
 }
 
@@ -943,7 +979,8 @@ struct WTemp {          // wide node under construction
 struct WideArrays {
   const BinNode* bin;
   WTemp* w;
-  uint32_t* counter;    // [0] next temporary wide id, [1] next-level count, [2] max depth, [3] max stack
+  uint32_t* counter;    // [0] next temporary wide id, [1] next-level count, [2] max depth, [3] max stack,
+                        // [4] this level's count
   uint32_t* size;       // subtree sizes
   uint32_t* visits;
   int32_t* final_id;
@@ -955,10 +992,12 @@ __device__ __forceinline__ float bin_area(const BinNode& n) {
   return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_wide_expand(WideArrays W, const uint32_t* __restrict__ cur, uint32_t n_cur, uint32_t level,
+// One level of the collapse; the level's count is read from counter[4] (0
+// after the last level, so levels queued ahead of the host's check return).
+__global__ void k_wide_expand(WideArrays W, const uint32_t* __restrict__ cur, uint32_t level,
                               uint32_t* __restrict__ next) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_cur) return;
+  const uint32_t n_cur = W.counter[4];
+  for (uint32_t i = grid_thread(); i < n_cur; i += grid_threads()) {
   const uint32_t wid = cur[i];
   WTemp& w = W.w[wid];
   const int32_t root = w.slot[0];
@@ -1008,6 +1047,12 @@ __global__ void k_wide_expand(WideArrays W, const uint32_t* __restrict__ cur, ui
     }
   }
   W.visits[wid] = 0u;
+  }
+}
+
+__global__ void k_wide_advance(WideArrays W) {
+  W.counter[4] = W.counter[1];
+  W.counter[1] = 0u;
 }
 
 __global__ void k_wide_sizes(WideArrays W, uint32_t n_wide) {
@@ -1144,7 +1189,7 @@ cudaError_t build_tree(const float4* blo, const float4* bhi, uint32_t n, bool sa
   uint32_t* act = sc.get<uint32_t>(max_act);
   uint32_t* next = sc.get<uint32_t>(max_act);
   uint32_t* small = sc.get<uint32_t>(n / (kLeafMax + 1u) + 2u);
-  uint32_t* counter = sc.get<uint32_t>(4);
+  uint32_t* counter = sc.get<uint32_t>(8);
   uint32_t* cb = sc.get<uint32_t>(6ull * max_act);
   int32_t* axis = sc.get<int32_t>(max_act);
   float* split = sc.get<float>(max_act);
@@ -1156,50 +1201,60 @@ cudaError_t build_tree(const float4* blo, const float4* bhi, uint32_t n, bool sa
   k_fill_u32<<<grid_for(cap_nodes), kThreads, 0, s>>>(reinterpret_cast<uint32_t*>(slot_of), cap_nodes, 0xffffffffu);
   k_fill_u32<<<grid_for(n), kThreads, 0, s>>>(node_of, n, 0u);
   k_root<<<1, 1, 0, s>>>(nodes, n, slot_of);
-  const uint32_t init[4] = {1u, 0u, 0u, 0u};
-  BB_TRY(cudaMemcpyAsync(counter, init, sizeof(init), cudaMemcpyHostToDevice, s));
-  uint32_t n_act = 0u, n_small = 0u;
+  // counter: next temporary id, next-level count, small count, -, this level's count, its children's first id
+  uint32_t init[8] = {1u, 0u, 0u, 0u, 0u, 1u, 0u, 0u};
   if (n > kSmallNode) {
+    init[4] = 1u;   // the root is the first level's one active node
     const uint32_t zero = 0u;
     BB_TRY(cudaMemcpyAsync(act, &zero, 4, cudaMemcpyHostToDevice, s));
-    n_act = 1u;
   } else if (n > kLeafMax) {
+    init[2] = 1u;   // the root is a small subtree
     const uint32_t zero = 0u;
     BB_TRY(cudaMemcpyAsync(small, &zero, 4, cudaMemcpyHostToDevice, s));
-    n_small = 1u;
-    BB_TRY(cudaMemcpyAsync(counter + 2, &n_small, 4, cudaMemcpyHostToDevice, s));
   }
+  BB_TRY(cudaMemcpyAsync(counter, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  // The levels are queued without waiting for their counts: every split
+  // leaves a largest child of at least half its parent, so at least
+  // floor(log2(n / 64)) levels run before every node is small; the host reads
+  // the count only from then on, every second level (a queued level after the
+  // last one finds no active node and its kernels return at once).
   uint32_t* idx = order;
-  uint32_t base = 1u;
-  while (n_act > 0u) {
-    k_level_init<<<grid_for(n_act), kThreads, 0, s>>>(A, act, n_act);
+  const uint32_t act_grid = std::min(grid_for(max_act), 148u * 8u);
+  const uint32_t bin_grid = std::min(grid_for(static_cast<uint64_t>(max_act) * 3u * kSahBins), 148u * 8u);
+  const uint32_t split_grid = std::min(grid_for(static_cast<uint64_t>(max_act) * 32u, 128), 148u * 16u);
+  uint32_t first_check = 1u;
+  for (uint64_t m = n / (kSmallNode + 1u); m > 1u; m >>= 1) ++first_check;
+  bool more = init[4] != 0u;
+  for (uint32_t level = 1u; more; ++level) {
+    k_level_init<<<act_grid, kThreads, 0, s>>>(A, act);
     k_centroid_bounds<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n);
     if (sah) {
-      k_sah_bin_init<<<grid_for(static_cast<uint64_t>(n_act) * 3u * kSahBins), kThreads, 0, s>>>(bins, n_act);
+      k_sah_bin_init<<<bin_grid, kThreads, 0, s>>>(A, bins);
       k_sah_bin<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, bins);
-      k_sah_split<<<grid_for(static_cast<uint64_t>(n_act) * 32u, 128), 128, 0, s>>>(A, bins, n_act);
+      k_sah_split<<<split_grid, 128, 0, s>>>(A, bins);
     } else {
-      k_midpoint_split<<<grid_for(n_act), kThreads, 0, s>>>(A, n_act);
+      k_midpoint_split<<<act_grid, kThreads, 0, s>>>(A);
     }
     k_flags<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, flag, sah);
     BB_TRY(exclusive_scan(flag, n, excl, sc));
-    BB_TRY(cudaMemsetAsync(counter + 1, 0, 4, s));
-    k_children<<<grid_for(n_act), kThreads, 0, s>>>(A, act, n_act, base, excl, next, small);
+    k_children<<<act_grid, kThreads, 0, s>>>(A, act, excl, next, small);
     k_scatter<<<grid_for(n), kThreads, 0, s>>>(A, idx, node_of, n, excl, idx2, node2);
-    k_level_done<<<grid_for(n_act), kThreads, 0, s>>>(A, act, n_act);
-    BB_TRY(cudaGetLastError());
+    k_level_done<<<act_grid, kThreads, 0, s>>>(A, act);
     // the scattered order becomes the current one (the caller's buffer keeps the final order)
-    BB_TRY(cudaMemcpyAsync(idx, idx2, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    k_copy_level<<<std::min(grid_for(n), 148u * 8u), kThreads, 0, s>>>(A, idx, idx2, n);
+    k_level_advance<<<1, 1, 0, s>>>(A);
+    BB_TRY(cudaGetLastError());
     std::swap(node_of, node2);
     std::swap(act, next);
-    base += 2u * n_act;
-    uint32_t cnt[3];
-    BB_TRY(cudaMemcpyAsync(cnt, counter, sizeof(cnt), cudaMemcpyDeviceToHost, s));
-    BB_TRY(cudaStreamSynchronize(s));
-    n_act = cnt[1];
-    n_small = cnt[2];
+    if (level >= first_check && (level - first_check) % 2u == 0u) {
+      uint32_t cur = 0u;
+      BB_TRY(read_scalar(counter + 4, cur, s));
+      more = cur != 0u;
+    }
   }
-  BB_TRY(cudaMemcpyAsync(counter, &base, 4, cudaMemcpyHostToDevice, s));
+  uint32_t n_small = 0u;
+  BB_TRY(read_scalar(counter + 2, n_small, s));
+  k_small_base<<<1, 1, 0, s>>>(A);
   if (n_small > 0u) {
     if (sah) k_small<true><<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
     else k_small<false><<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
@@ -1229,7 +1284,7 @@ cudaError_t collapse(const BinNode* bin, uint32_t n_bin, WideNode* out, uint32_t
                      uint32_t& stack_required, Scratch& sc, int32_t* slot_bin = nullptr) {
   cudaStream_t s = sc.s;
   const uint32_t cap = n_bin;   // wide nodes <= binary internal nodes + 1
-  WideArrays W{bin, sc.get<WTemp>(cap), sc.get<uint32_t>(4), sc.get<uint32_t>(cap), sc.get<uint32_t>(cap),
+  WideArrays W{bin, sc.get<WTemp>(cap), sc.get<uint32_t>(8), sc.get<uint32_t>(cap), sc.get<uint32_t>(cap),
                sc.get<int32_t>(cap), slot_bin};
   uint32_t* cur = sc.get<uint32_t>(cap);
   uint32_t* next = sc.get<uint32_t>(cap);
@@ -1239,18 +1294,30 @@ cudaError_t collapse(const BinNode* bin, uint32_t n_bin, WideNode* out, uint32_t
   root.parent = -1;
   root.stack_here = 0;
   BB_TRY(cudaMemcpyAsync(W.w, &root, sizeof(root), cudaMemcpyHostToDevice, s));
-  const uint32_t init[4] = {1u, 0u, 0u, 0u};
+  const uint32_t init[8] = {1u, 0u, 0u, 0u, 1u, 0u, 0u, 0u};
   BB_TRY(cudaMemcpyAsync(W.counter, init, sizeof(init), cudaMemcpyHostToDevice, s));
   const uint32_t zero = 0u;
   BB_TRY(cudaMemcpyAsync(cur, &zero, 4, cudaMemcpyHostToDevice, s));
-  uint32_t n_cur = 1u, level = 0u;
-  while (n_cur > 0u) {
-    BB_TRY(cudaMemsetAsync(W.counter + 1, 0, 4, s));
-    k_wide_expand<<<grid_for(n_cur), kThreads, 0, s>>>(W, cur, n_cur, level, next);
+  // Levels are queued without waiting for their counts: a wide node spans at
+  // most three binary levels and a binary tree of L leaves is at least
+  // log2(L) deep, so at least floor(log2(n_bin / 2) / 3) levels run; the host
+  // reads the count from then on, every second level.
+  uint32_t first_check = 1u, lg = 0u;
+  for (uint64_t m = n_bin / 2u; m > 1u; m >>= 1) ++lg;
+  first_check = std::max(1u, lg / 3u);
+  const uint32_t wide_grid = std::min(grid_for(cap), 148u * 8u);
+  bool more = true;
+  for (uint32_t level = 0u; more; ++level) {
+    k_wide_expand<<<wide_grid, kThreads, 0, s>>>(W, cur, level, next);
+    k_wide_advance<<<1, 1, 0, s>>>(W);
     BB_TRY(cudaGetLastError());
     std::swap(cur, next);
-    BB_TRY(read_scalar(W.counter + 1, n_cur, s));
-    ++level;
+    const uint32_t done = level + 1u;
+    if (done >= first_check && (done - first_check) % 2u == 0u) {
+      uint32_t n_cur = 0u;
+      BB_TRY(read_scalar(W.counter + 4, n_cur, s));
+      more = n_cur != 0u;
+    }
   }
   uint32_t cnt[4];
   BB_TRY(cudaMemcpyAsync(cnt, W.counter, sizeof(cnt), cudaMemcpyDeviceToHost, s));
