@@ -44,6 +44,7 @@ constexpr int kScanThreads = 512;
 constexpr uint32_t kScanBlock = 2 * kScanThreads;
 constexpr int kThreads = 256;
 constexpr int kSahBins = 32;
+constexpr int kBinWords = 7;     // per bin: count, 3 lower and 3 upper bound keys
 
 inline unsigned grid_for(uint64_t n, int threads = kThreads) {
   return static_cast<unsigned>(std::max<uint64_t>(1, (n + threads - 1) / threads));
@@ -566,7 +567,201 @@ __global__ void k_scatter(BuildArrays A, const uint32_t* __restrict__ idx, const
 }
 
 // Sequential build of one small subtree per thread (same split rules).
-template <bool kSah>
+// Small subtrees of the SAH tree, one warp each: the host SAH builder's
+// splits (32 bins per axis, the first minimum of the swept costs, a stable
+// partition, count/2 when one side is empty), with the node's primitives on the lanes (two per lane), the bins
+// filled by one leader per bin and slot (order-preserving keys, min and max are
+// exact) and the sweep done by shuffle scans with bin b on lane b.
+constexpr int kSmallWarps = 4;
+static_assert(kSahBins == 32, "k_small_sah keeps bin b on lane b");
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = bmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = bmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ int sah_bin_of(float c, float c0, float scale) {
+  const int k = static_cast<int>((c - c0) * scale);
+  return k < 0 ? 0 : (k > kSahBins - 1 ? kSahBins - 1 : k);
+}
+
+__global__ void __launch_bounds__(32 * kSmallWarps) k_small_sah(BuildArrays A, const uint32_t* __restrict__ small,
+                                                                uint32_t n_small, uint32_t* __restrict__ idx) {
+  __shared__ uint32_t s_stack[kSmallWarps][64];
+  __shared__ uint32_t s_bins[kSmallWarps][kSahBins * kBinWords];
+  const int wib = static_cast<int>(threadIdx.x >> 5);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t* stack = s_stack[wib];
+  uint32_t* bins = s_bins[wib];
+  const uint32_t nwarps = gridDim.x * kSmallWarps;
+  for (uint32_t w = blockIdx.x * kSmallWarps + static_cast<uint32_t>(wib); w < n_small; w += nwarps) {
+    if (lane == 0u) stack[0] = small[w];
+    int sp = 1;
+    __syncwarp();
+    while (sp > 0) {
+      const uint32_t nd = stack[--sp];
+      const TNode t = A.nodes[nd];
+      const uint32_t b = static_cast<uint32_t>(t.begin), n = static_cast<uint32_t>(t.count);
+      __syncwarp();
+      if (n <= kLeafMax) continue;
+      const bool h0 = lane < n, h1 = lane + 32u < n;
+      const uint32_t p0 = h0 ? idx[b + lane] : 0u, p1 = h1 ? idx[b + lane + 32u] : 0u;
+      float c0[3], c1[3], clo[3], chi[3];
+      for (int a = 0; a < 3; ++a) {
+        c0[a] = h0 ? centroid(A.blo, A.bhi, p0, a) : 0.0f;
+        c1[a] = h1 ? centroid(A.blo, A.bhi, p1, a) : 0.0f;
+        clo[a] = warp_min(bmin(h0 ? c0[a] : FLT_MAX, h1 ? c1[a] : FLT_MAX));
+        chi[a] = warp_max(bmax(h0 ? c0[a] : -FLT_MAX, h1 ? c1[a] : -FLT_MAX));
+      }
+      const float4 lo0 = h0 ? A.blo[p0] : make_float4(0.f, 0.f, 0.f, 0.f), hi0 = h0 ? A.bhi[p0] : lo0;
+      const float4 lo1 = h1 ? A.blo[p1] : make_float4(0.f, 0.f, 0.f, 0.f), hi1 = h1 ? A.bhi[p1] : lo1;
+      float best_cost = FLT_MAX;
+      int best_axis = -1, best_bin = -1;
+      for (int a = 0; a < 3; ++a) {
+        const float ext = chi[a] - clo[a];
+        if (!(ext > 0.0f)) continue;   // uniform
+        const float scale = static_cast<float>(kSahBins) / ext;
+        uint32_t* wb = bins + kBinWords * lane;   // bin `lane`
+        wb[0] = 0u;
+        wb[1] = wb[2] = wb[3] = 0xffffffffu;
+        wb[4] = wb[5] = wb[6] = 0u;
+        __syncwarp();
+        for (int slot = 0; slot < 2; ++slot) {
+          const bool h = slot == 0 ? h0 : h1;
+          const unsigned active = __ballot_sync(0xffffffffu, h);
+          if (h) {
+            const float4 lo = slot == 0 ? lo0 : lo1, hi = slot == 0 ? hi0 : hi1;
+            const int k = sah_bin_of(slot == 0 ? c0[a] : c1[a], clo[a], scale);
+            const unsigned grp = __match_any_sync(active, static_cast<uint32_t>(k));
+            const uint32_t m0 = __reduce_min_sync(grp, fkey(lo.x)), m1 = __reduce_min_sync(grp, fkey(lo.y)),
+                           m2 = __reduce_min_sync(grp, fkey(lo.z));
+            const uint32_t x0 = __reduce_max_sync(grp, fkey(hi.x)), x1 = __reduce_max_sync(grp, fkey(hi.y)),
+                           x2 = __reduce_max_sync(grp, fkey(hi.z));
+            if (static_cast<int>(lane) == __ffs(grp) - 1) {
+              uint32_t* q = bins + kBinWords * k;
+              q[0] += static_cast<uint32_t>(__popc(grp));
+              q[1] = min(q[1], m0);
+              q[2] = min(q[2], m1);
+              q[3] = min(q[3], m2);
+              q[4] = max(q[4], x0);
+              q[5] = max(q[5], x1);
+              q[6] = max(q[6], x2);
+            }
+          }
+          __syncwarp();
+        }
+        // the sweep: prefix over bins 0..lane, suffix over lane..31 (k_sah_split's scans)
+        const uint32_t cnt = wb[0];
+        float lo3[3], hi3[3];
+        for (int q = 0; q < 3; ++q) {
+          lo3[q] = cnt ? fval(wb[1 + q]) : FLT_MAX;
+          hi3[q] = cnt ? fval(wb[4 + q]) : -FLT_MAX;
+        }
+        __syncwarp();
+        uint32_t lc = cnt, rc = cnt;
+        float llo[3] = {lo3[0], lo3[1], lo3[2]}, lhi[3] = {hi3[0], hi3[1], hi3[2]};
+        float rlo[3] = {lo3[0], lo3[1], lo3[2]}, rhi[3] = {hi3[0], hi3[1], hi3[2]};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t lcu = __shfl_up_sync(0xffffffffu, lc, o);
+          const uint32_t rcd = __shfl_down_sync(0xffffffffu, rc, o);
+          float lu[6], rd[6];
+          for (int q = 0; q < 3; ++q) {
+            lu[q] = __shfl_up_sync(0xffffffffu, llo[q], o);
+            lu[3 + q] = __shfl_up_sync(0xffffffffu, lhi[q], o);
+            rd[q] = __shfl_down_sync(0xffffffffu, rlo[q], o);
+            rd[3 + q] = __shfl_down_sync(0xffffffffu, rhi[q], o);
+          }
+          if (static_cast<int>(lane) >= o) {
+            lc += lcu;
+            for (int q = 0; q < 3; ++q) {
+              llo[q] = bmin(llo[q], lu[q]);
+              lhi[q] = bmax(lhi[q], lu[3 + q]);
+            }
+          }
+          if (static_cast<int>(lane) + o < 32) {
+            rc += rcd;
+            for (int q = 0; q < 3; ++q) {
+              rlo[q] = bmin(rlo[q], rd[q]);
+              rhi[q] = bmax(rhi[q], rd[3 + q]);
+            }
+          }
+        }
+        const uint32_t rcn = __shfl_down_sync(0xffffffffu, rc, 1);
+        float rn[6];
+        for (int q = 0; q < 3; ++q) {
+          rn[q] = __shfl_down_sync(0xffffffffu, rlo[q], 1);
+          rn[3 + q] = __shfl_down_sync(0xffffffffu, rhi[q], 1);
+        }
+        float cost = FLT_MAX;
+        if (lane < 31u && lc != 0u && rcn != 0u) {
+          const float dx = lhi[0] - llo[0], dy = lhi[1] - llo[1], dz = lhi[2] - llo[2];
+          const float ex = rn[3] - rn[0], ey = rn[4] - rn[1], ez = rn[5] - rn[2];
+          cost = (dx * dy + dy * dz + dz * dx) * static_cast<float>(lc) +
+                 (ex * ey + ey * ez + ez * ex) * static_cast<float>(rcn);
+        }
+        float c = cost;
+        int bb = static_cast<int>(lane);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const float co = __shfl_xor_sync(0xffffffffu, c, o);
+          const int bo = __shfl_xor_sync(0xffffffffu, bb, o);
+          if (co < c || (co == c && bo < bb)) {
+            c = co;
+            bb = bo;
+          }
+        }
+        if (c < best_cost) {
+          best_cost = c;
+          best_axis = a;
+          best_bin = bb;
+        }
+      }
+      // stable partition: left in order, then right in order (ident: order unchanged, count/2)
+      uint32_t nl = 0u;
+      if (best_axis >= 0) {
+        const float cb0 = clo[best_axis];
+        const float scale = static_cast<float>(kSahBins) / (chi[best_axis] - cb0);
+        const bool l0 = h0 && sah_bin_of(c0[best_axis], cb0, scale) <= best_bin;
+        const bool l1 = h1 && sah_bin_of(c1[best_axis], cb0, scale) <= best_bin;
+        const unsigned v0 = __ballot_sync(0xffffffffu, h0), v1 = __ballot_sync(0xffffffffu, h1);
+        const unsigned b0 = __ballot_sync(0xffffffffu, l0), b1 = __ballot_sync(0xffffffffu, l1);
+        const uint32_t nl0 = static_cast<uint32_t>(__popc(b0));
+        nl = nl0 + static_cast<uint32_t>(__popc(b1));
+        const uint32_t nr0 = static_cast<uint32_t>(__popc(v0 & ~b0));
+        __syncwarp();   // every lane holds its primitives before any is moved
+        if (h0) idx[b + (l0 ? __popc(b0 & lt) : nl + __popc(v0 & ~b0 & lt))] = p0;
+        if (h1) idx[b + (l1 ? nl0 + __popc(b1 & lt) : nl + nr0 + __popc(v1 & ~b1 & lt))] = p1;
+      }
+      const bool ident = nl == 0u || nl == n;
+      if (ident) nl = n / 2u;
+      uint32_t l = 0u;
+      if (lane == 0u) {
+        l = atomicAdd(&A.counter[0], 2u);
+        const uint32_t r = l + 1u;
+        A.nodes[nd].left = static_cast<int32_t>(l);
+        A.nodes[nd].right = static_cast<int32_t>(r);
+        A.nodes[l] = TNode{static_cast<int32_t>(b), static_cast<int32_t>(nl), -1, -1, static_cast<int32_t>(nd)};
+        A.nodes[r] = TNode{static_cast<int32_t>(b + nl), static_cast<int32_t>(n - nl), -1, -1, static_cast<int32_t>(nd)};
+        if (sp + 2 <= 64) {
+          stack[sp] = r;
+          stack[sp + 1] = l;
+        }
+      }
+      if (sp + 2 <= 64) sp += 2;
+      __syncwarp();
+    }
+  }
+}
+
+// Small subtrees of the reference tree (midpoint splits), one thread each.
 __global__ void k_small(BuildArrays A, const uint32_t* __restrict__ small, uint32_t n_small, uint32_t* __restrict__ idx) {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= n_small) return;
@@ -588,106 +783,24 @@ __global__ void k_small(BuildArrays A, const uint32_t* __restrict__ small, uint3
         chi[a] = bmax(chi[a], c);
       }
     }
-    uint32_t nl = 0u;
-    bool ident;
-    if (!kSah) {
-      int axis = 0;
-      float widest = chi[0] - clo[0];
-      for (int a = 1; a < 3; ++a) {
-        const float e = chi[a] - clo[a];
-        if (e > widest) {
-          widest = e;
-          axis = a;
-        }
+    int axis = 0;
+    float widest = chi[0] - clo[0];
+    for (int a = 1; a < 3; ++a) {
+      const float e = chi[a] - clo[a];
+      if (e > widest) {
+        widest = e;
+        axis = a;
       }
-      const float split = 0.5f * (clo[axis] + chi[axis]);
-      uint32_t nr = 0u;
-      for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t p = idx[b + i];
-        if (centroid(A.blo, A.bhi, p, axis) < split) idx[b + nl++] = p;
-        else tmp[nr++] = p;
-      }
-      for (uint32_t i = 0; i < nr; ++i) idx[b + nl + i] = tmp[i];
-      ident = nl == 0u || nl == n;
-    } else {
-      // Binned SAH over the three axes (32 bins), counts and bounds per bin.
-      int best_axis = -1, best_bin = -1;
-      float best_cost = FLT_MAX;
-      for (int a = 0; a < 3; ++a) {
-        const float ext = chi[a] - clo[a];
-        if (!(ext > 0.0f)) continue;
-        const float scale = static_cast<float>(kSahBins) / ext;
-        uint32_t cnt[kSahBins];
-        float blo[kSahBins][3], bhi[kSahBins][3];
-        for (int k = 0; k < kSahBins; ++k) {
-          cnt[k] = 0u;
-          for (int q = 0; q < 3; ++q) {
-            blo[k][q] = FLT_MAX;
-            bhi[k][q] = -FLT_MAX;
-          }
-        }
-        for (uint32_t i = 0; i < n; ++i) {
-          const uint32_t p = idx[b + i];
-          int k = static_cast<int>((centroid(A.blo, A.bhi, p, a) - clo[a]) * scale);
-          k = k < 0 ? 0 : (k > kSahBins - 1 ? kSahBins - 1 : k);
-          ++cnt[k];
-          const float4 lo = A.blo[p], hi = A.bhi[p];
-          blo[k][0] = bmin(blo[k][0], lo.x);
-          blo[k][1] = bmin(blo[k][1], lo.y);
-          blo[k][2] = bmin(blo[k][2], lo.z);
-          bhi[k][0] = bmax(bhi[k][0], hi.x);
-          bhi[k][1] = bmax(bhi[k][1], hi.y);
-          bhi[k][2] = bmax(bhi[k][2], hi.z);
-        }
-        float rarea[kSahBins];
-        uint32_t rcnt[kSahBins];
-        float rlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-        uint32_t rc = 0u;
-        for (int k = kSahBins - 1; k > 0; --k) {
-          rc += cnt[k];
-          for (int q = 0; q < 3; ++q) {
-            rlo[q] = bmin(rlo[q], blo[k][q]);
-            rhi[q] = bmax(rhi[q], bhi[k][q]);
-          }
-          rcnt[k] = rc;
-          const float dx = rhi[0] - rlo[0], dy = rhi[1] - rlo[1], dz = rhi[2] - rlo[2];
-          rarea[k] = rc ? dx * dy + dy * dz + dz * dx : 0.0f;
-        }
-        float llo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, lhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-        uint32_t lc = 0u;
-        for (int k = 0; k < kSahBins - 1; ++k) {
-          lc += cnt[k];
-          for (int q = 0; q < 3; ++q) {
-            llo[q] = bmin(llo[q], blo[k][q]);
-            lhi[q] = bmax(lhi[q], bhi[k][q]);
-          }
-          if (lc == 0u || rcnt[k + 1] == 0u) continue;
-          const float dx = lhi[0] - llo[0], dy = lhi[1] - llo[1], dz = lhi[2] - llo[2];
-          const float cost = (dx * dy + dy * dz + dz * dx) * static_cast<float>(lc) +
-                             rarea[k + 1] * static_cast<float>(rcnt[k + 1]);
-          if (cost < best_cost) {
-            best_cost = cost;
-            best_axis = a;
-            best_bin = k;
-          }
-        }
-      }
-      if (best_axis >= 0) {
-        const float c0 = clo[best_axis];
-        const float scale = static_cast<float>(kSahBins) / (chi[best_axis] - c0);
-        uint32_t nr = 0u;
-        for (uint32_t i = 0; i < n; ++i) {
-          const uint32_t p = idx[b + i];
-          int k = static_cast<int>((centroid(A.blo, A.bhi, p, best_axis) - c0) * scale);
-          k = k < 0 ? 0 : (k > kSahBins - 1 ? kSahBins - 1 : k);
-          if (k <= best_bin) idx[b + nl++] = p;
-          else tmp[nr++] = p;
-        }
-        for (uint32_t i = 0; i < nr; ++i) idx[b + nl + i] = tmp[i];
-      }
-      ident = nl == 0u || nl == n;
     }
-    if (ident) nl = n / 2u;
+    const float split = 0.5f * (clo[axis] + chi[axis]);
+    uint32_t nl = 0u, nr = 0u;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t p = idx[b + i];
+      if (centroid(A.blo, A.bhi, p, axis) < split) idx[b + nl++] = p;
+      else tmp[nr++] = p;
+    }
+    for (uint32_t i = 0; i < nr; ++i) idx[b + nl + i] = tmp[i];
+    if (nl == 0u || nl == n) nl = n / 2u;
     const uint32_t l = atomicAdd(&A.counter[0], 2u), r = l + 1u;
     A.nodes[nd].left = static_cast<int32_t>(l);
     A.nodes[nd].right = static_cast<int32_t>(r);
@@ -701,8 +814,7 @@ __global__ void k_small(BuildArrays A, const uint32_t* __restrict__ small, uint3
 }
 
 // ---------------------------------------------------------------- SAH binning of large nodes
-// Per active slot: 3 axes x 32 bins x (count, 6 bound keys).
-constexpr int kBinWords = 7;
+// Per active slot: 3 axes x 32 bins x (count, 6 bound keys; kBinWords words).
 __global__ void k_sah_bin_init(BuildArrays A, uint32_t* __restrict__ bins) {
   const uint32_t total = level_active(A) * 3u * kSahBins;
   for (uint32_t i = grid_thread(); i < total; i += grid_threads()) {
@@ -1256,8 +1368,11 @@ cudaError_t build_tree(const float4* blo, const float4* bhi, uint32_t n, bool sa
   BB_TRY(read_scalar(counter + 2, n_small, s));
   k_small_base<<<1, 1, 0, s>>>(A);
   if (n_small > 0u) {
-    if (sah) k_small<true><<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
-    else k_small<false><<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
+    if (sah)
+      k_small_sah<<<std::min((n_small + kSmallWarps - 1u) / kSmallWarps, 148u * 16u), 32 * kSmallWarps, 0, s>>>(
+          A, small, n_small, idx);
+    else
+      k_small<<<grid_for(n_small, 64), 64, 0, s>>>(A, small, n_small, idx);
   }
   BB_TRY(cudaGetLastError());
   return read_scalar(counter, n_nodes, s);
