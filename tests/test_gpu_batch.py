@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
+from tests.golden import cases
 from vkpathtracer_b200 import scenes
 from vkpathtracer_b200.tracer import BatchRenderer
 
@@ -28,6 +29,9 @@ def small_jobs():
     jobs.append((scenes.sphere_field(5, 12, 14, seed=8, n_lights=4, light_size=2.0, light_height=6.0),
                  scenes.RenderSettings(width=64, height=64, spp=4, max_depth=16, seed=5, firefly_clamp=10.0)))
     jobs.append((scenes.cornell_box(seed=4), scenes.RenderSettings(width=33, height=17, spp=5, max_depth=4, seed=9)))
+    # thin lens with a polygonal iris and anamorphic squeeze
+    jobs.append((cases.lens_scene("pentagon_sharp"), scenes.RenderSettings(width=40, height=32, spp=3, max_depth=5,
+                                                                          seed=13)))
     return jobs
 
 
