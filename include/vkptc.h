@@ -30,7 +30,9 @@
 extern "C" {
 #endif
 
-#define VKPTC_ABI_VERSION 1u
+/* Version of the struct layouts below.  2: vkptc_scene_view gained the camera lens fields,
+ * vkptc_config.reserved[0] became triangle_test. */
+#define VKPTC_ABI_VERSION 2u
 
 typedef enum vkptc_status {
   VKPTC_OK = 0,
@@ -54,6 +56,10 @@ typedef enum vkptc_lifecycle {
 } vkptc_lifecycle;
 
 typedef struct vkptc_ctx vkptc_ctx;
+
+/* The VKPTC_ABI_VERSION the library was built with; a caller compiled against another version
+ * must not pass its structs to it. */
+uint32_t vkptc_abi_version(void);
 
 typedef struct vkptc_config {
   int32_t device;            /* CUDA device ordinal */

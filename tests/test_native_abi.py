@@ -19,7 +19,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "vkptc.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int32_t|const char\*)\s+(vkptc_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int32_t|uint32_t|const char\*)\s+(vkptc_\w+)\s*\(", text, re.M)))
+
+
+def test_abi_version_matches_the_header():
+    """vkptc_abi_version() is the VKPTC_ABI_VERSION the library was built with;
+    the bindings refuse a library with another struct layout."""
+    text = open(os.path.join(ROOT, "include", "vkptc.h")).read()
+    declared = int(re.search(r"#define VKPTC_ABI_VERSION (\d+)u", text).group(1))
+    assert native.load().vkptc_abi_version() == declared == native.ABI_VERSION
 
 
 def test_library_exports_every_declared_symbol():

@@ -486,6 +486,8 @@ uint32_t wave_paths(const vkptc_ctx* c) {
 
 extern "C" {
 
+uint32_t vkptc_abi_version(void) { return VKPTC_ABI_VERSION; }
+
 int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
   if (!out_ctx) return VKPTC_INVALID_ARGUMENT;
   *out_ctx = nullptr;

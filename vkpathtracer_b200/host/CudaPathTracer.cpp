@@ -48,6 +48,10 @@ uint32_t resolve_instance(uint32_t index, vkpt::core::StableId entity,
 }  // namespace
 
 CudaPathTracer::CudaPathTracer(CudaPathTracerConfig config) {
+  if (vkptc_abi_version() != VKPTC_ABI_VERSION) {
+    m_last_error = "libvkpt_cuda was built with another VKPTC_ABI_VERSION";
+    return;
+  }
   vkptc_config c{};
   c.device = config.device;
   c.block_size = config.block_size;

@@ -182,9 +182,11 @@ ADJ_MAX_DEPTH = 8
 
 P = ctypes.c_void_p
 U32, U64, I32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32
+ABI_VERSION = 2   # VKPTC_ABI_VERSION of the struct layouts above
 
 # name -> (restype, argtypes); every symbol include/vkptc.h declares.
 SIGNATURES = {
+    "vkptc_abi_version": (U32, []),
     "vkptc_create": (I32, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
     "vkptc_destroy": (I32, [P]),
     "vkptc_configure": (I32, [P, ctypes.POINTER(RenderSettingsC)]),
@@ -254,6 +256,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.vkptc_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"libvkpt_cuda.so has ABI version {lib.vkptc_abi_version()}, these bindings {ABI_VERSION}; "
+                           "rebuild it")
     _LIB = lib
     return lib
 
