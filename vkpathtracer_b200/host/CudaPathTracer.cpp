@@ -5,15 +5,19 @@
 #include <chrono>
 #include <vector>
 
+#include "pathtracer/PathTracerObservability.h"
 #include "vkptc.h"
 
 namespace vkpt::gpu::cuda {
 
 namespace pt = vkpt::pathtracer;
+namespace obs = vkpt::pathtracer::observability;
 using vkpt::core::Status;
 using vkpt::core::StatusCode;
 
 namespace {
+
+constexpr const char* kBackend = "cuda-wavefront";
 
 // Standard GPU word maps (src/gpu/VulkanGpuPathTracer.cpp:323-338, 381-396).
 void material_words(const pt::RTMaterial& m, float* w) {
@@ -69,6 +73,16 @@ CudaPathTracer::~CudaPathTracer() {
   if (m_ctx) vkptc_destroy(m_ctx);
 }
 
+uint64_t CudaPathTracer::accumulation_gen() const {
+  vkptc_tracer_status s{};
+  return m_ctx && vkptc_get_status(m_ctx, &s) == VKPTC_OK ? s.accumulation_gen : 0u;
+}
+
+bool CudaPathTracer::accel_valid() const {
+  vkptc_tracer_status s{};
+  return m_ctx && vkptc_get_status(m_ctx, &s) == VKPTC_OK && s.accel_valid != 0u;
+}
+
 bool CudaPathTracer::fail(const std::string& message) const {
   m_last_error = message;
   return false;
@@ -107,6 +121,7 @@ Status CudaPathTracer::configure(const pt::RenderSettings& settings) {
     m_resolve = settings.film_resolve;
     m_film = pt::FilmBuffer{settings.width, settings.height};
     m_film.set_resolve_settings(m_resolve);
+    obs::EmitPathTracerConfig(kBackend, settings.width, settings.height, settings.spp, settings.deterministic);
   }
   return st;
 }
@@ -201,7 +216,9 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
   for (const auto& r : scene.instances) m_instance_entities.push_back(r.entity_id);
   const Status st = status_from(vkptc_load_scene(m_ctx, &v), "load_scene_snapshot");
   m_has_scene = static_cast<bool>(st);
+  if (!st) obs::EmitPathTracerAnomaly(kBackend, "load_scene_snapshot", m_last_error, accumulation_gen());
   if (st) {
+    m_next_reset_reason = pt::PathTracerAccumulationResetReason::Topology;
     m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, scene));
     m_camera = pt::ExtractCameraState(scene);
     m_camera_scene = pt::PathTracerSceneSnapshot{};
@@ -212,12 +229,21 @@ Status CudaPathTracer::load_scene_snapshot(const pt::PathTracerSceneSnapshot& sc
 
 Status CudaPathTracer::build_or_update_acceleration() {
   if (!m_ctx) return Status::error(StatusCode::Unsupported, m_last_error);
-  return status_from(vkptc_build_acceleration(m_ctx), "build_or_update_acceleration");
+  const Status st = status_from(vkptc_build_acceleration(m_ctx), "build_or_update_acceleration");
+  vkptc_accel_info info{};
+  if (st && vkptc_get_accel_info(m_ctx, &info) == VKPTC_OK)
+    obs::EmitPathTracerStarted(kBackend, accumulation_gen(), info.primitive_count);
+  else if (!st)
+    obs::EmitPathTracerAnomaly(kBackend, "build_or_update_acceleration", m_last_error, accumulation_gen());
+  return st;
 }
 
 bool CudaPathTracer::reset_accumulation() {
   if (!m_ctx) return fail("no cuda context");
-  return static_cast<bool>(status_from(vkptc_reset(m_ctx), "reset_accumulation"));
+  const bool ok = static_cast<bool>(status_from(vkptc_reset(m_ctx), "reset_accumulation"));
+  obs::EmitAccumulationReset(accumulation_gen(), m_next_reset_reason, ok, accel_valid());
+  if (ok) m_next_reset_reason = pt::PathTracerAccumulationResetReason::External;
+  return ok;
 }
 
 bool CudaPathTracer::replace_film_history(const pt::FilmBuffer& film) {
@@ -374,7 +400,7 @@ pt::InstanceTransformPlan CudaPathTracer::plan_instance_transform_update(
 }
 
 pt::InstanceTransformUpdateResult CudaPathTracer::apply_instance_transform_update(
-    std::span<const pt::RTInstanceTransformUpdate> updates, const pt::InstanceTransformUpdateOptions&) {
+    std::span<const pt::RTInstanceTransformUpdate> updates, const pt::InstanceTransformUpdateOptions& options) {
   const uint32_t n = static_cast<uint32_t>(updates.size());
   std::vector<vkptc_instance_update> ups;
   if (!m_ctx || !resolve_updates(updates, m_instance_entities, ups)) {
@@ -389,6 +415,8 @@ pt::InstanceTransformUpdateResult CudaPathTracer::apply_instance_transform_updat
     return {status_of(rc), n, 0u, 0.0, 0.0, 0.0, 0.0, m_last_error.c_str()};
   }
   m_last_error.clear();
+  m_next_reset_reason = pt::AccumulationResetReasonFromUpdateReason(options.reason);
+  obs::EmitSceneDeltaApplied(accumulation_gen(), 0u, 0u, n, false, accel_valid());
   return {pt::InstanceTransformUpdateStatus::AppliedDynamicAccelUpdate, n, n, 0.0, 0.0, ms, 0.0,
           "cuda backend refit dynamic instance transforms"};
 }
@@ -426,6 +454,7 @@ bool CudaPathTracer::update_camera_state(const pt::RTCameraState& camera) {
   c.iris_roundness = camera.iris_roundness;
   c.anamorphic_squeeze = camera.anamorphic_squeeze;
   if (!status_from(vkptc_update_camera(m_ctx, &c), "update_camera_state")) return false;
+  m_next_reset_reason = pt::PathTracerAccumulationResetReason::Camera;
   m_camera = camera;
   pt::ApplyCameraState(m_camera_scene, camera);
   m_film.set_resolve_settings(pt::CameraAdjustedFilmResolveSettings(m_resolve, m_camera_scene));
@@ -464,7 +493,11 @@ bool CudaPathTracer::update_scene_delta(const pt::RTSceneDeltaUpdate& update) {
   d.environment[0] = update.environment_color.x;
   d.environment[1] = update.environment_color.y;
   d.environment[2] = update.environment_color.z;
-  return static_cast<bool>(status_from(vkptc_update_scene_delta(m_ctx, &d), "update_scene_delta"));
+  if (!status_from(vkptc_update_scene_delta(m_ctx, &d), "update_scene_delta")) return false;
+  m_next_reset_reason = pt::PathTracerAccumulationResetReason::Material;
+  obs::EmitSceneDeltaApplied(accumulation_gen(), update.materials.size(), update.lights.size(), 0u,
+                             update.environment_color_changed, accel_valid());
+  return true;
 }
 
 bool CudaPathTracer::update_instance_transforms(const std::vector<pt::RTInstanceTransformUpdate>& updates) {

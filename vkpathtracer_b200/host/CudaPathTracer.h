@@ -80,6 +80,11 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   mutable std::string m_last_error;
   std::vector<vkpt::core::StableId> m_instance_entities;   // entity id per instance (update resolution)
   bool m_has_scene = false;
+  // Why the next reset_accumulation clears the film (reported with the reset event).
+  vkpt::pathtracer::PathTracerAccumulationResetReason m_next_reset_reason =
+      vkpt::pathtracer::PathTracerAccumulationResetReason::External;
+  uint64_t accumulation_gen() const;
+  bool accel_valid() const;
   // The loaded scene's camera; a snapshot holding only it gives the
   // camera-adjusted film resolve settings after a camera update.
   vkpt::pathtracer::RTCameraState m_camera{};
