@@ -18,7 +18,7 @@ import oracle
 from tests.golden import cases
 from tests.test_gpu_parity import BIT_EXACT_FRAC, RMSE_REL_TOL, SIGMA3_FAIL_FRAC, film_report
 from vkpathtracer_b200 import native, scenes
-from vkpathtracer_b200.tracer import CudaPathTracer
+from vkpathtracer_b200.tracer import BatchRenderer, CudaPathTracer, RenderTile
 
 pytestmark = pytest.mark.gpu
 
@@ -140,8 +140,35 @@ def test_modes_without_watertight_records_refuse_it():
     assert e.value.code == native.UNSUPPORTED
     lib = native.load()
     cfg = native.Config()
-    cfg.triangle_test = native.TRIANGLE_WATERTIGHT
-    handle = ctypes.c_void_p()
-    assert lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(handle)) == native.UNSUPPORTED
     cfg.triangle_test = 2
+    handle = ctypes.c_void_p()
     assert lib.vkptc_create(ctypes.byref(cfg), ctypes.byref(handle)) == native.INVALID_ARGUMENT
+    assert lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(handle)) == native.INVALID_ARGUMENT
+
+
+def test_watertight_batch_equals_single_context_renders():
+    """The loop and plain batch drivers traverse watertight jobs with the
+    watertight test: every job's film equals that job rendered alone by a
+    watertight context; the persistent driver refuses them."""
+    jobs = [(scenes.cornell_box(seed=1), scenes.cornell_settings(48, 40, 3)),
+            (scenes.sphere_field(3, 9, 10, seed=21, n_lights=3, light_size=1.5, light_height=5.0),
+             scenes.RenderSettings(width=40, height=30, spp=2, max_depth=6, seed=77)),
+            (cases.lens_scene("many_blades"), scenes.RenderSettings(width=32, height=24, spp=2, max_depth=5, seed=3))]
+    with BatchRenderer(triangle_test="watertight") as b:
+        for sc, st in jobs:
+            b.add_job(sc, st)
+        with pytest.raises(native.VkptcError) as e:
+            b.run("persistent")
+        assert e.value.code == native.UNSUPPORTED
+        b.run("loop")
+        loop = [b.film(j) for j in range(len(jobs))]
+        b.run("plain")
+        plain = [b.film(j) for j in range(len(jobs))]
+    for (sc, st), (lf, lc), (pf, pc) in zip(jobs, loop, plain):
+        with wt_tracer(sc, st) as t:
+            assert t.reset_accumulation()
+            for s in range(st.spp):
+                assert t.render_tile(RenderTile(0, 0, st.width, st.height, s), 0)
+            g, cnt, _ = t.film()
+        assert np.array_equal(lc, cnt) and np.array_equal(pc, cnt)
+        assert np.array_equal(bits(lf), bits(g)) and np.array_equal(bits(pf), bits(g))

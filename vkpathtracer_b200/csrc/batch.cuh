@@ -54,6 +54,7 @@ struct BatchLaunch {
   bool sdf;     // some job has SDF primitives (loop driver: the two SDF stages run)
   int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
                   // (the persistent kernel; in the loop driver, its two traversal stages)
+  bool watertight;  // the jobs' triangle records hold vertices (watertight test; loop driver only)
 };
 
 // Number of control words the pool needs; word kBatchCtlIterations holds the
@@ -133,7 +134,8 @@ constexpr int kLoopCtlIterations = 18;  // iterations of the last run
 struct LoopGrids {
   int regen, extend, shade, shadow, finish, sdf;
 };
-LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count);
+LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count,
+                         bool watertight = false);
 cudaError_t ConfigureBatchLoopSmem(size_t bytes);
 cudaError_t LaunchBatchLoopInit(const LoopPool& pool, cudaStream_t stream);
 // One iteration of the five stages; the finish stage sets `handle` (the

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ job
   }
 }
 
-template <bool kStats, int kMinBlocks>
+template <bool kStats, int kMinBlocks, bool kWt>
 __global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __restrict__ jobs, LoopPool P, int scap,
                                                                int2* spill, int total_cap, int steps, DevCounters* ctr,
                                                                uint32_t* err) {
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __r
   TraceStats st;
   uint32_t lerr = 0u;
   const LoopExtendSource src{jobs, P.gen[cur], P.hit};
-  persistent_traverse<LoopExtendSource, false, kStats>(src, n, &P.ctl[kLFetchExt], stk, steps, st, lerr);
+  persistent_traverse<LoopExtendSource, false, kStats, kWt>(src, n, &P.ctl[kLFetchExt], stk, steps, st, lerr);
   flush_stats<kStats>(ctr, st, false);
   if (lerr) atomicOr(err, lerr);
 }
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256, 3) k_lp_shade(const DevJob* __restrict__ 
   warp_count(&ctr->shadow_tests, shadow_tests);
 }
 
-template <bool kStats, int kMinBlocks>
+template <bool kStats, int kMinBlocks, bool kWt>
 __global__ void __launch_bounds__(256, kMinBlocks) k_lp_shadow(const DevJob* __restrict__ jobs, LoopPool P, int scap,
                                                                int2* spill, int total_cap, int steps, DevCounters* ctr,
                                                                uint32_t* err) {
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_shadow(const DevJob* __r
   TraceStats st;
   uint32_t lerr = 0u;
   const LoopShadowSource src{jobs, P, P.gen[cur ^ 1u]};
-  persistent_traverse<LoopShadowSource, true, kStats>(src, n, &P.ctl[kLFetchShadow], stk, steps, st, lerr);
+  persistent_traverse<LoopShadowSource, true, kStats, kWt>(src, n, &P.ctl[kLFetchShadow], stk, steps, st, lerr);
   flush_stats<kStats>(ctr, st, true);
   if (lerr) atomicOr(err, lerr);
 }
@@ -371,31 +371,44 @@ cudaError_t set_smem_attr(K kernel, int bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-// Traversal stage variants: [stats][register variant] (at least 1..4
-// resident 256-thread blocks per SM; stats runs use the unconstrained one).
+// Traversal stage variants: [triangle test][stats][register variant] (at
+// least 1..4 resident 256-thread blocks per SM; stats runs use the
+// unconstrained one).
 using LoopTraceFn = void (*)(const DevJob*, LoopPool, int, int2*, int, int, DevCounters*, uint32_t*);
-LoopTraceFn extend_fn(bool stats, int occ) {
-  static const LoopTraceFn t[2][4] = {
-      {k_lp_extend<false, 1>, k_lp_extend<false, 2>, k_lp_extend<false, 3>, k_lp_extend<false, 4>},
-      {k_lp_extend<true, 1>, k_lp_extend<true, 1>, k_lp_extend<true, 1>, k_lp_extend<true, 1>}};
-  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+LoopTraceFn extend_fn(bool stats, int occ, bool wt) {
+  static const LoopTraceFn t[2][2][4] = {
+      {{k_lp_extend<false, 1, false>, k_lp_extend<false, 2, false>, k_lp_extend<false, 3, false>,
+        k_lp_extend<false, 4, false>},
+       {k_lp_extend<true, 1, false>, k_lp_extend<true, 1, false>, k_lp_extend<true, 1, false>,
+        k_lp_extend<true, 1, false>}},
+      {{k_lp_extend<false, 1, true>, k_lp_extend<false, 2, true>, k_lp_extend<false, 3, true>,
+        k_lp_extend<false, 4, true>},
+       {k_lp_extend<true, 1, true>, k_lp_extend<true, 1, true>, k_lp_extend<true, 1, true>,
+        k_lp_extend<true, 1, true>}}};
+  return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
 }
-LoopTraceFn shadow_fn(bool stats, int occ) {
-  static const LoopTraceFn t[2][4] = {
-      {k_lp_shadow<false, 1>, k_lp_shadow<false, 2>, k_lp_shadow<false, 3>, k_lp_shadow<false, 4>},
-      {k_lp_shadow<true, 1>, k_lp_shadow<true, 1>, k_lp_shadow<true, 1>, k_lp_shadow<true, 1>}};
-  return t[stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+LoopTraceFn shadow_fn(bool stats, int occ, bool wt) {
+  static const LoopTraceFn t[2][2][4] = {
+      {{k_lp_shadow<false, 1, false>, k_lp_shadow<false, 2, false>, k_lp_shadow<false, 3, false>,
+        k_lp_shadow<false, 4, false>},
+       {k_lp_shadow<true, 1, false>, k_lp_shadow<true, 1, false>, k_lp_shadow<true, 1, false>,
+        k_lp_shadow<true, 1, false>}},
+      {{k_lp_shadow<false, 1, true>, k_lp_shadow<false, 2, true>, k_lp_shadow<false, 3, true>,
+        k_lp_shadow<false, 4, true>},
+       {k_lp_shadow<true, 1, true>, k_lp_shadow<true, 1, true>, k_lp_shadow<true, 1, true>,
+        k_lp_shadow<true, 1, true>}}};
+  return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
 }
 
 }  // namespace
 
-LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count) {
+LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count, bool watertight) {
   LoopGrids g{};
   g.regen = sm_count * (parity ? blocks_per_sm(k_lp_regen<true>, block, 0) : blocks_per_sm(k_lp_regen<false>, block, 0));
-  g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy), block, smem);
+  g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy, watertight), block, smem);
   g.shade = sm_count * (parity ? blocks_per_sm(k_lp_shade<true, true>, block, 0)
                                : blocks_per_sm(k_lp_shade<false, true>, block, 0));
-  g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy), block, smem);
+  g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy, watertight), block, smem);
   g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
   g.sdf = sm_count * std::min(blocks_per_sm(k_lp_sdf, block, 0), blocks_per_sm(k_lp_sdf_shadow, block, 0));
   return g;
@@ -404,11 +417,12 @@ LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int oc
 cudaError_t ConfigureBatchLoopSmem(size_t bytes) {
   const int b = static_cast<int>(bytes);
   cudaError_t e = cudaSuccess;
-  for (int st = 0; st < 2 && e == cudaSuccess; ++st)
-    for (int o = 0; o < 4 && e == cudaSuccess; ++o) {
-      e = set_smem_attr(extend_fn(st != 0, o), b);
-      if (e == cudaSuccess) e = set_smem_attr(shadow_fn(st != 0, o), b);
-    }
+  for (int wt = 0; wt < 2 && e == cudaSuccess; ++wt)
+    for (int st = 0; st < 2 && e == cudaSuccess; ++st)
+      for (int o = 0; o < 4 && e == cudaSuccess; ++o) {
+        e = set_smem_attr(extend_fn(st != 0, o, wt != 0), b);
+        if (e == cudaSuccess) e = set_smem_attr(shadow_fn(st != 0, o, wt != 0), b);
+      }
   return e;
 }
 
@@ -430,7 +444,7 @@ cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, uns
   if (bl.parity) k_lp_regen<true><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
   else k_lp_regen<false><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
   mark(1);
-  extend_fn(bl.stats, bl.occupancy)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
+  extend_fn(bl.stats, bl.occupancy, bl.watertight)<<<g.extend, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
                                                                       bl.steps, ctr, err);
   if (bl.sdf) k_lp_sdf<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
   mark(2);
@@ -444,7 +458,7 @@ cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, uns
   }
   mark(3);
   if (bl.sdf) k_lp_sdf_shadow<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
-  shadow_fn(bl.stats, bl.occupancy)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
+  shadow_fn(bl.stats, bl.occupancy, bl.watertight)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
                                                                       bl.steps, ctr, err);
   mark(4);
   k_lp_finish<<<g.finish, bl.block, 0, s>>>(jobs, total, P, handle);

@@ -1717,6 +1717,9 @@ int32_t batch_run_plain(vkptc_batch* b, const vkptc_batch_tuning& t) {
 int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mode) {
   const bool parity = b->config.math_mode == 0u;
   const bool loop = mode == VKPTC_BATCH_LOOP;
+  const bool watertight = b->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT;
+  if (watertight && !loop)   // the persistent kernel is built with the Moller-Trumbore test only
+    return bfail(b, VKPTC_UNSUPPORTED, "the persistent driver takes Moller-Trumbore jobs only; use the loop driver");
   for (double& v : b->stats.stage_ms) v = 0.0;
   // ---- jobs table and stagings
   std::vector<DevJob> table(b->jobs.size());
@@ -1754,6 +1757,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   bl.stream = b->stream;
   bl.parity = parity;
   bl.stats = b->config.collect_stats != 0u;
+  bl.watertight = watertight;
   bl.effects = false;
   bl.sdf = false;
   for (vkptc_ctx* c : b->jobs) {
@@ -1771,7 +1775,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
       VKPTC_BCUDA(b, ConfigureBatchLoopSmem(smem), "shared memory limit");
       b->loop_smem_configured = smem;
     }
-    lg = BatchLoopGrids(bl.block, smem, parity, bl.stats, bl.occupancy, b->sm_count);
+    lg = BatchLoopGrids(bl.block, smem, parity, bl.stats, bl.occupancy, b->sm_count, watertight);
     if (lg.regen <= 0 || lg.extend <= 0 || lg.shade <= 0 || lg.shadow <= 0 || lg.finish <= 0) {
       return bfail(b, VKPTC_UNSUPPORTED, "a batch stage kernel does not fit on an SM with this block size");
     }
@@ -2037,9 +2041,9 @@ int32_t vkptc_batch_create(const vkptc_config* config, vkptc_batch** out_batch) 
   auto* b = new (std::nothrow) vkptc_batch();
   if (!b) return VKPTC_ALLOC_FAILED;
   if (config) b->config = *config;
-  if (b->config.triangle_test != VKPTC_TRIANGLE_MT) {   // batch jobs use the Moller-Trumbore records
+  if (b->config.triangle_test > VKPTC_TRIANGLE_WATERTIGHT) {
     delete b;
-    return VKPTC_UNSUPPORTED;
+    return VKPTC_INVALID_ARGUMENT;
   }
   b->device = b->config.device;
   int count = 0;

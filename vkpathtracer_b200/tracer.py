@@ -514,7 +514,9 @@ class BatchRenderer:
     """
 
     def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False, bvh: str = "reference",
-                 stage_timing: bool = False, build: str = "device"):
+                 stage_timing: bool = False, build: str = "device", triangle_test: str = "mt"):
+        """triangle_test "watertight": every job traverses with the watertight
+        test (the plain and loop drivers; the persistent driver refuses it)."""
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
@@ -523,6 +525,7 @@ class BatchRenderer:
         cfg.stage_timing = int(stage_timing)
         cfg.bvh_mode = native.BVH_SAH if bvh == "sah" else native.BVH_REFERENCE
         cfg.build_mode = native.BUILD_HOST if build == "host" else native.BUILD_DEVICE
+        cfg.triangle_test = {"mt": native.TRIANGLE_MT, "watertight": native.TRIANGLE_WATERTIGHT}[triangle_test]
         h = ctypes.c_void_p()
         rc = self._lib.vkptc_batch_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != native.OK:
