@@ -687,6 +687,16 @@ def run_ours(args, world, rank, local):
     # allocations resident, every cudaMalloc/cudaFree of a later acceleration
     # build costs several milliseconds more.
     b.close()
+    # the same jobs with the watertight triangle test (loop driver, the same tuning)
+    wt = None
+    if rank == 0 and mode == "loop" and not args.no_watertight:
+        with BatchRenderer(device=local, bvh="sah", triangle_test="watertight") as bw:
+            for j in jobs:
+                bw.add_job(j.scene, j.settings)
+            bw.run("loop", **tuning)
+            wms = min(bw.run("loop", **tuning)["device_ms"] for _ in range(2))
+        wt = {"paths_per_s": total_paths / (wms / 1e3), "driver": "loop", "tuning": tuning,
+              "relative_to_moller_trumbore": (total_paths / (wms / 1e3)) / (value / world)}
 
     roof = rq = ff = cpu = inv = sdf = bb = fr = None
     if rank == 0:
@@ -764,6 +774,7 @@ def run_ours(args, world, rank, local):
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
                 "inverse_rendering": inv, "sdf_scene": sdf, "bvh_build": bb, "film_resolve": fr,
+                "watertight_batch": wt,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     b.close()
@@ -783,6 +794,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-sdf", action="store_true")
     ap.add_argument("--no-build", action="store_true")
+    ap.add_argument("--no-watertight", action="store_true")
     ap.add_argument("--profile-run", choices=["loop", "persistent"], default=None,
                     help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
     ap.add_argument("--profile-build", action="store_true",
