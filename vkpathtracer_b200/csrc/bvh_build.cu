@@ -1446,9 +1446,15 @@ cudaError_t collapse(const BinNode* bin, uint32_t n_bin, WideNode* out, uint32_t
   return cudaGetLastError();
 }
 
+// The accelerator's own arrays come from the builder's stream-ordered pool
+// too: with many allocations resident in the process (a batch's job set),
+// cudaMalloc and cudaFree of a rebuild's arrays took tens of milliseconds.
 template <class T>
-cudaError_t dmalloc(T*& p, size_t n) {
-  return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(1, n) * sizeof(T));
+cudaError_t dmalloc(T*& p, size_t n, cudaStream_t s) {
+  const size_t bytes = std::max<size_t>(1, n) * sizeof(T);
+  cudaMemPool_t pool = build_pool();
+  return pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), bytes, pool, s)
+              : cudaMallocAsync(reinterpret_cast<void**>(&p), bytes, s);
 }
 
 __global__ void k_inst_first(const uint32_t* __restrict__ pos, const unsigned long long* __restrict__ prefix,
@@ -1592,16 +1598,20 @@ __global__ void k_refit_wide(WideNode* __restrict__ wide, uint32_t n_wide, const
 
 }  // namespace
 
-void FreeRefitState(DeviceRefitState*& st) {
+void FreeAccelArray(void* p, cudaStream_t stream) {
+  if (p) cudaFreeAsync(p, stream);
+}
+
+void FreeRefitState(DeviceRefitState*& st, cudaStream_t stream) {
   if (!st) return;
-  cudaFree(st->blo);
-  cudaFree(st->bhi);
-  cudaFree(st->tri_pos);
-  cudaFree(st->trav_nodes);
-  cudaFree(st->trav_order);
-  cudaFree(st->trav_parent);
-  cudaFree(st->slot_bin);
-  cudaFree(st->inst_first);
+  FreeAccelArray(st->blo, stream);
+  FreeAccelArray(st->bhi, stream);
+  FreeAccelArray(st->tri_pos, stream);
+  FreeAccelArray(st->trav_nodes, stream);
+  FreeAccelArray(st->trav_order, stream);
+  FreeAccelArray(st->trav_parent, stream);
+  FreeAccelArray(st->slot_bin, stream);
+  FreeAccelArray(st->inst_first, stream);
   delete st;
   st = nullptr;
 }
@@ -1646,14 +1656,14 @@ cudaError_t RefitOnDevice(DeviceRefitState& st, const std::vector<RefitUpdate>& 
   return cudaStreamSynchronize(stream);
 }
 
-void FreeDeviceAccel(DeviceAccelOut& out) {
-  FreeRefitState(out.refit);
-  cudaFree(out.nodes);
-  cudaFree(out.tris);
-  cudaFree(out.tie);
-  cudaFree(out.shade);
-  cudaFree(out.ref_nodes);
-  cudaFree(out.ref_order);
+void FreeDeviceAccel(DeviceAccelOut& out, cudaStream_t stream) {
+  FreeRefitState(out.refit, stream);
+  FreeAccelArray(out.nodes, stream);
+  FreeAccelArray(out.tris, stream);
+  FreeAccelArray(out.tie, stream);
+  FreeAccelArray(out.shade, stream);
+  FreeAccelArray(out.ref_nodes, stream);
+  FreeAccelArray(out.ref_order, stream);
   out = DeviceAccelOut{};
 }
 
@@ -1705,9 +1715,9 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   if (keep_refit) {
     out.refit = new DeviceRefitState();
     out.refit->watertight = sc_in.watertight;
-    BB_TRY(dmalloc(out.refit->blo, n));
-    BB_TRY(dmalloc(out.refit->bhi, n));
-    BB_TRY(dmalloc(out.refit->inst_first, instance_count + 1u));
+    BB_TRY(dmalloc(out.refit->blo, n, stream));
+    BB_TRY(dmalloc(out.refit->bhi, n, stream));
+    BB_TRY(dmalloc(out.refit->inst_first, instance_count + 1u, stream));
     blo = out.refit->blo;
     bhi = out.refit->bhi;
   } else {
@@ -1715,7 +1725,7 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
     bhi = sc.get<float4>(n);
   }
   if (sc.err != cudaSuccess) return sc.err;
-  BB_TRY(dmalloc(out.shade, n));
+  BB_TRY(dmalloc(out.shade, n, stream));
   if (nc) k_flat_write<<<grid_for(nc), kThreads, 0, stream>>>(f, flag, pos, pv, out.shade, blo, bhi, nonfinite);
   uint32_t bad = 0u;
   BB_TRY(read_scalar(nonfinite, bad, stream));
@@ -1735,7 +1745,7 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
     }
   }
   if (bad) {
-    FreeDeviceAccel(out);
+    FreeDeviceAccel(out, stream);
     out.fallback = true;
     return cudaSuccess;
   }
@@ -1746,13 +1756,13 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   uint32_t* ref_leaf = sc.get<uint32_t>(n);
   uint32_t* ref_lane = sc.get<uint32_t>(n);
   if (sc.err != cudaSuccess) return sc.err;
-  BB_TRY(dmalloc(out.ref_order, n));
+  BB_TRY(dmalloc(out.ref_order, n, stream));
   k_iota<<<grid_for(n), kThreads, 0, stream>>>(out.ref_order, n);
   uint32_t n_ref = 0u;
   BB_TRY(build_tree(blo, bhi, n, false, out.ref_order, tn, n_ref, sc));
-  BB_TRY(dmalloc(out.ref_nodes, n_ref));
+  BB_TRY(dmalloc(out.ref_nodes, n_ref, stream));
   TieNode* tie = nullptr;
-  BB_TRY(dmalloc(tie, n_ref));
+  BB_TRY(dmalloc(tie, n_ref, stream));
   out.tie = reinterpret_cast<float4*>(tie);
   BB_TRY(finish_tree(blo, bhi, out.ref_order, tn, n_ref, out.ref_nodes, tie, ref_leaf, ref_lane, sc));
   out.binary_nodes = n_ref;
@@ -1764,7 +1774,7 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
   uint32_t n_trav = n_ref;
   if (sah) {
     uint32_t* sah_order = nullptr;
-    if (keep_refit) BB_TRY(dmalloc(out.refit->trav_order, n));
+    if (keep_refit) BB_TRY(dmalloc(out.refit->trav_order, n, stream));
     sah_order = keep_refit ? out.refit->trav_order : sc.get<uint32_t>(n);
     TNode* sn = sc.get<TNode>(2ull * n);
     if (sc.err != cudaSuccess) return sc.err;
@@ -1772,8 +1782,8 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
     BB_TRY(build_tree(blo, bhi, n, true, sah_order, sn, n_trav, sc));
     BinNode* sah_nodes = nullptr;
     if (keep_refit) {
-      BB_TRY(dmalloc(out.refit->trav_nodes, n_trav));
-      BB_TRY(dmalloc(out.refit->trav_parent, n_trav));
+      BB_TRY(dmalloc(out.refit->trav_nodes, n_trav, stream));
+      BB_TRY(dmalloc(out.refit->trav_parent, n_trav, stream));
       out.refit->trav_count = n_trav;
       sah_nodes = out.refit->trav_nodes;
     } else {
@@ -1787,17 +1797,17 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& sc_in, bool sah, cudaStr
     out.reference_topology = false;
   }
   WideNode* wide = nullptr;
-  BB_TRY(dmalloc(wide, n_trav));
+  BB_TRY(dmalloc(wide, n_trav, stream));
   out.nodes = reinterpret_cast<float4*>(wide);
-  if (keep_refit) BB_TRY(dmalloc(out.refit->slot_bin, 4ull * n_trav));
+  if (keep_refit) BB_TRY(dmalloc(out.refit->slot_bin, 4ull * n_trav, stream));
   BB_TRY(collapse(trav, n_trav, wide, out.wide_nodes, out.depth, out.stack_required, sc,
                   keep_refit ? out.refit->slot_bin : nullptr));
   TriRecord* tris = nullptr;
-  BB_TRY(dmalloc(tris, n));
+  BB_TRY(dmalloc(tris, n, stream));
   out.tris = reinterpret_cast<float4*>(tris);
   k_tri_records<<<grid_for(n), kThreads, 0, stream>>>(trav_order, n, pv, ref_leaf, ref_lane, tris);
   if (keep_refit) {
-    BB_TRY(dmalloc(out.refit->tri_pos, n));
+    BB_TRY(dmalloc(out.refit->tri_pos, n, stream));
     k_tri_pos<<<grid_for(n), kThreads, 0, stream>>>(trav_order, n, out.refit->tri_pos);
   }
   BB_TRY(cudaGetLastError());

@@ -32,7 +32,8 @@ struct DeviceRefitState {
 };
 
 struct DeviceAccelOut {
-  // Device arrays allocated by the builder with cudaMalloc (caller frees).
+  // Device arrays from the builder's stream-ordered pool (the caller frees
+  // them with FreeAccelArray, FreeDeviceAccel or FreeRefitState).
   float4* nodes = nullptr;     // WideNode, 8 float4 each
   float4* tris = nullptr;      // TriRecord, 3 float4 each
   float4* tie = nullptr;       // TieNode, 2 float4 each
@@ -72,8 +73,11 @@ struct DeviceSceneArrays {
 // fallback, nothing is allocated.
 cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& scene, bool sah, cudaStream_t stream, DeviceAccelOut& out);
 
-void FreeDeviceAccel(DeviceAccelOut& out);
-void FreeRefitState(DeviceRefitState*& state);
+// Stream-ordered frees of the builder's arrays: after the work already queued
+// on `stream`, back into the pool (no device-wide synchronisation).
+void FreeAccelArray(void* p, cudaStream_t stream);
+void FreeDeviceAccel(DeviceAccelOut& out, cudaStream_t stream = nullptr);
+void FreeRefitState(DeviceRefitState*& state, cudaStream_t stream = nullptr);
 
 // One instance transform update, resolved to an instance of the scene.
 struct RefitUpdate {

@@ -33,11 +33,23 @@ template <typename T>
 struct DevBuf {
   T* ptr = nullptr;
   size_t count = 0;
+  bool pooled = false;            // from the builder's stream-ordered pool (adopt_pooled)
+  cudaStream_t pool_stream = nullptr;
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr && pooled) {
+      // after the queued work of the stream that used it; if that stream is gone, after all work
+      if (cudaFreeAsync(ptr, pool_stream) != cudaSuccess) {
+        cudaGetLastError();
+        cudaDeviceSynchronize();
+        cudaFreeAsync(ptr, nullptr);
+      }
+    } else if (ptr) {
+      cudaFree(ptr);
+    }
     ptr = nullptr;
     count = 0;
+    pooled = false;
   }
   cudaError_t alloc(size_t n) {
     if (n <= count && ptr) return cudaSuccess;
@@ -53,6 +65,11 @@ struct DevBuf {
     release();
     ptr = p;
     count = p ? n : 0;
+  }
+  void adopt_pooled(T* p, size_t n, cudaStream_t s) {
+    adopt(p, n);
+    pooled = p != nullptr;
+    pool_stream = s;
   }
 };
 
@@ -800,9 +817,9 @@ int32_t ensure_geo(vkptc_ctx* c) {
 }
 
 void release_refit(vkptc_ctx* c) {
-  FreeRefitState(c->refit);
-  cudaFree(c->d_ref_nodes);
-  cudaFree(c->d_ref_order);
+  FreeRefitState(c->refit, c->stream);
+  FreeAccelArray(c->d_ref_nodes, c->stream);
+  FreeAccelArray(c->d_ref_order, c->stream);
   c->d_ref_nodes = nullptr;
   c->d_ref_order = nullptr;
   c->ref_count = 0;
@@ -833,21 +850,21 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
   a.watertight = c->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT;
   const cudaError_t e = BuildAccelOnDevice(a, c->config.bvh_mode == VKPTC_BVH_SAH, c->stream, out);
   if (e != cudaSuccess) {
-    FreeDeviceAccel(out);
+    FreeDeviceAccel(out, c->stream);
     return cuda_fail(c, e, "device BVH build");
   }
   if (out.fallback) return VKPTC_OK;
   const uint32_t n = out.prim_count;
   c->inst_prims = std::move(out.inst_first);
-  c->d_shade.adopt(out.shade, std::max<uint32_t>(1, n));
+  c->d_shade.adopt_pooled(out.shade, std::max<uint32_t>(1, n), c->stream);
   if (n == 0u) {
     VKPTC_CUDA(c, c->d_nodes.alloc(1), "bvh alloc");
     VKPTC_CUDA(c, c->d_tris.alloc(1), "bvh alloc");
     VKPTC_CUDA(c, c->d_tie.alloc(1), "bvh alloc");
   } else {
-    c->d_nodes.adopt(out.nodes, 8ull * out.wide_nodes);
-    c->d_tris.adopt(out.tris, 3ull * n);
-    c->d_tie.adopt(out.tie, 2ull * out.binary_nodes);
+    c->d_nodes.adopt_pooled(out.nodes, 8ull * out.wide_nodes, c->stream);
+    c->d_tris.adopt_pooled(out.tris, 3ull * n, c->stream);
+    c->d_tie.adopt_pooled(out.tie, 2ull * out.binary_nodes, c->stream);
   }
   release_refit(c);
   if (out.refit) {
@@ -857,8 +874,8 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
     c->ref_count = out.binary_nodes;
     out.refit = nullptr;
   } else {
-    cudaFree(out.ref_nodes);
-    cudaFree(out.ref_order);
+    FreeAccelArray(out.ref_nodes, c->stream);
+    FreeAccelArray(out.ref_order, c->stream);
   }
   c->wide = WideBvh{};
   c->wide.binary_nodes = out.binary_nodes;
