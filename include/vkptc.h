@@ -84,9 +84,8 @@ typedef struct vkptc_config {
                                 Wald (JCGT 2013) on the triangles' own vertices, so a ray through a
                                 shared edge or vertex of a closed mesh never passes between its
                                 triangles.  The watertight mode needs the device build; ray queries,
-                                renders of a context and the plain and loop batch drivers honour it;
-                                the persistent batch driver and the adjoint do not take it
-                                (VKPTC_UNSUPPORTED). */
+                                renders of a context and every batch driver honour it; the adjoint
+                                does not take it (VKPTC_UNSUPPORTED). */
   uint32_t reserved[2];
 } vkptc_config;
 

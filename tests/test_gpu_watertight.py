@@ -147,9 +147,8 @@ def test_modes_without_watertight_records_refuse_it():
 
 
 def test_watertight_batch_equals_single_context_renders():
-    """The loop and plain batch drivers traverse watertight jobs with the
-    watertight test: every job's film equals that job rendered alone by a
-    watertight context; the persistent driver refuses them."""
+    """Every batch driver traverses watertight jobs with the watertight test:
+    each job's film equals that job rendered alone by a watertight context."""
     jobs = [(scenes.cornell_box(seed=1), scenes.cornell_settings(48, 40, 3)),
             (scenes.sphere_field(3, 9, 10, seed=21, n_lights=3, light_size=1.5, light_height=5.0),
              scenes.RenderSettings(width=40, height=30, spp=2, max_depth=6, seed=77)),
@@ -157,18 +156,18 @@ def test_watertight_batch_equals_single_context_renders():
     with BatchRenderer(triangle_test="watertight") as b:
         for sc, st in jobs:
             b.add_job(sc, st)
-        with pytest.raises(native.VkptcError) as e:
-            b.run("persistent")
-        assert e.value.code == native.UNSUPPORTED
+        b.run("persistent")
+        pers = [b.film(j) for j in range(len(jobs))]
         b.run("loop")
         loop = [b.film(j) for j in range(len(jobs))]
         b.run("plain")
         plain = [b.film(j) for j in range(len(jobs))]
-    for (sc, st), (lf, lc), (pf, pc) in zip(jobs, loop, plain):
+    for (sc, st), (lf, lc), (pf, pc), (sf, scn) in zip(jobs, loop, plain, pers):
         with wt_tracer(sc, st) as t:
             assert t.reset_accumulation()
             for s in range(st.spp):
                 assert t.render_tile(RenderTile(0, 0, st.width, st.height, s), 0)
             g, cnt, _ = t.film()
-        assert np.array_equal(lc, cnt) and np.array_equal(pc, cnt)
+        assert np.array_equal(lc, cnt) and np.array_equal(pc, cnt) and np.array_equal(scn, cnt)
         assert np.array_equal(bits(lf), bits(g)) and np.array_equal(bits(pf), bits(g))
+        assert np.array_equal(bits(sf), bits(g))

@@ -265,7 +265,7 @@ __device__ __forceinline__ void flush_traversal_stats(DevCounters* ctr, const Tr
 // ------------------------------------------------------- persistent driver
 // kMinBlocks: resident 256-thread blocks per SM the register allocation must
 // allow (0 = compiler's choice); the autotuner picks the occupancy/spill trade-off.
-template <bool kParity, bool kStats, int kMinBlocks>
+template <bool kParity, bool kStats, int kMinBlocks, bool kWt>
 __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restrict__ jobs, uint32_t job_count,
                                                            unsigned long long total, BatchPool P, int scap,
                                                            int2* spill, int total_cap, int steps, DevCounters* ctr,
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
     }
     {
       const BatchExtendSource src{jobs, P.ext[cur], P.job, P.ray_o, P.ray_d, P.hit};
-      persistent_traverse<BatchExtendSource, false, kStats>(src, n_ext, &P.ctl[kCtlFetchExt], stk, steps, st_e, lerr);
+      persistent_traverse<BatchExtendSource, false, kStats, kWt>(src, n_ext, &P.ctl[kCtlFetchExt], stk, steps, st_e, lerr);
     }
     if (!grid_barrier(P.ctl)) break;
 
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
     {
       const uint32_t n_sh = P.ctl[kCtlShadow];
       const BatchShadowSource src{jobs, P.shq, P.job, P.sh_o, P.sh_d, P.sh_c, P.rad};
-      persistent_traverse<BatchShadowSource, true, kStats>(src, n_sh, &P.ctl[kCtlFetchShadow], stk, steps, st_s, lerr);
+      persistent_traverse<BatchShadowSource, true, kStats, kWt>(src, n_sh, &P.ctl[kCtlFetchShadow], stk, steps, st_s, lerr);
     }
     if (!grid_barrier(P.ctl)) break;
 
@@ -379,35 +379,45 @@ cudaError_t set_smem_attr(K kernel, int bytes) {
 }
 }  // namespace
 
-// Kernel variant table: [parity][stats][occupancy variant].
+// Kernel variant table: [triangle test][parity][stats][occupancy variant].
 namespace {
 using BatchFn = void (*)(const DevJob*, uint32_t, unsigned long long, BatchPool, int, int2*, int, int, DevCounters*,
                          uint32_t*);
 constexpr int kOccVariants = 4;   // minBlocks 1, 2, 3, 4
-BatchFn batch_fn(bool parity, bool stats, int occ) {
+template <bool kWt>
+BatchFn batch_fn_of(bool parity, bool stats, int o) {
   static const BatchFn table[2][2][kOccVariants] = {
-      {{k_batch<false, false, 1>, k_batch<false, false, 2>, k_batch<false, false, 3>, k_batch<false, false, 4>},
-       {k_batch<false, true, 1>, k_batch<false, true, 1>, k_batch<false, true, 1>, k_batch<false, true, 1>}},
-      {{k_batch<true, false, 1>, k_batch<true, false, 2>, k_batch<true, false, 3>, k_batch<true, false, 4>},
-       {k_batch<true, true, 1>, k_batch<true, true, 1>, k_batch<true, true, 1>, k_batch<true, true, 1>}}};
-  const int o = occ < 0 ? 0 : (occ >= kOccVariants ? kOccVariants - 1 : occ);
+      {{k_batch<false, false, 1, kWt>, k_batch<false, false, 2, kWt>, k_batch<false, false, 3, kWt>,
+        k_batch<false, false, 4, kWt>},
+       {k_batch<false, true, 1, kWt>, k_batch<false, true, 1, kWt>, k_batch<false, true, 1, kWt>,
+        k_batch<false, true, 1, kWt>}},
+      {{k_batch<true, false, 1, kWt>, k_batch<true, false, 2, kWt>, k_batch<true, false, 3, kWt>,
+        k_batch<true, false, 4, kWt>},
+       {k_batch<true, true, 1, kWt>, k_batch<true, true, 1, kWt>, k_batch<true, true, 1, kWt>,
+        k_batch<true, true, 1, kWt>}}};
   return table[parity ? 1 : 0][stats ? 1 : 0][o];
+}
+BatchFn batch_fn(bool parity, bool stats, int occ, bool wt) {
+  const int o = occ < 0 ? 0 : (occ >= kOccVariants ? kOccVariants - 1 : occ);
+  return wt ? batch_fn_of<true>(parity, stats, o) : batch_fn_of<false>(parity, stats, o);
 }
 }  // namespace
 
 cudaError_t ConfigureBatchSmem(size_t bytes) {
   const int b = static_cast<int>(bytes);
   cudaError_t e = cudaSuccess;
-  for (int p = 0; p < 2 && e == cudaSuccess; ++p)
-    for (int st = 0; st < 2 && e == cudaSuccess; ++st)
-      for (int o = 0; o < kOccVariants && e == cudaSuccess; ++o)
-        e = set_smem_attr(batch_fn(p != 0, st != 0, o), b);
+  for (int wt = 0; wt < 2 && e == cudaSuccess; ++wt)
+    for (int p = 0; p < 2 && e == cudaSuccess; ++p)
+      for (int st = 0; st < 2 && e == cudaSuccess; ++st)
+        for (int o = 0; o < kOccVariants && e == cudaSuccess; ++o)
+          e = set_smem_attr(batch_fn(p != 0, st != 0, o, wt != 0), b);
   return e;
 }
 
-int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occ) {
+int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occ, bool watertight) {
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_fn(parity, stats, occ), block, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_fn(parity, stats, occ, watertight), block, smem) !=
+      cudaSuccess)
     return 0;
   return blocks;
 }
@@ -422,7 +432,7 @@ cudaError_t LaunchBatchPersistent(const DevJob* d_jobs, uint32_t job_count, unsi
   int scap = bl.smem_entries, tcap = bl.stack_cap, steps = bl.steps;
   int2* spill = bl.spill;
   void* args[] = {&jobs, &jc, &total, &P, &scap, &spill, &tcap, &steps, &ctr, &err};
-  const void* fn = reinterpret_cast<const void*>(batch_fn(bl.parity, bl.stats, bl.occupancy));
+  const void* fn = reinterpret_cast<const void*>(batch_fn(bl.parity, bl.stats, bl.occupancy, bl.watertight));
   return cudaLaunchCooperativeKernel(fn, dim3(bl.grid), dim3(bl.block), args, smem, bl.stream);
 }
 

@@ -54,7 +54,7 @@ struct BatchLaunch {
   bool sdf;     // some job has SDF primitives (loop driver: the two SDF stages run)
   int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
                   // (the persistent kernel; in the loop driver, its two traversal stages)
-  bool watertight;  // the jobs' triangle records hold vertices (watertight test; loop driver only)
+  bool watertight;  // the jobs' triangle records hold vertices (watertight test)
 };
 
 // Number of control words the pool needs; word kBatchCtlIterations holds the
@@ -88,7 +88,7 @@ cudaError_t LaunchStagingAccumulate(const DevJob* d_jobs, uint32_t job_count, un
 cudaError_t LaunchBatchInit(const BatchPool& pool, cudaStream_t stream);
 
 // Resident blocks per SM of the persistent batch kernel.
-int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occupancy);
+int BatchBlocksPerSm(int block, size_t smem, bool parity, bool stats, int occ, bool watertight = false);
 cudaError_t ConfigureBatchSmem(size_t bytes);
 
 // ------------------------------------------------------------ loop driver

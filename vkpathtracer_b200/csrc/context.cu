@@ -1735,8 +1735,6 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   const bool parity = b->config.math_mode == 0u;
   const bool loop = mode == VKPTC_BATCH_LOOP;
   const bool watertight = b->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT;
-  if (watertight && !loop)   // the persistent kernel is built with the Moller-Trumbore test only
-    return bfail(b, VKPTC_UNSUPPORTED, "the persistent driver takes Moller-Trumbore jobs only; use the loop driver");
   for (double& v : b->stats.stage_ms) v = 0.0;
   // ---- jobs table and stagings
   std::vector<DevJob> table(b->jobs.size());
@@ -1802,7 +1800,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
       VKPTC_BCUDA(b, ConfigureBatchSmem(smem), "shared memory limit");
       b->smem_configured = smem;
     }
-    const int per_sm = BatchBlocksPerSm(bl.block, smem, parity, bl.stats, bl.occupancy);
+    const int per_sm = BatchBlocksPerSm(bl.block, smem, parity, bl.stats, bl.occupancy, watertight);
     if (per_sm <= 0) return bfail(b, VKPTC_UNSUPPORTED, "persistent batch kernel does not fit on an SM with this block size");
     bl.grid = per_sm * b->sm_count;
   }

@@ -516,7 +516,7 @@ class BatchRenderer:
     def __init__(self, device: int = 0, math_mode: int = 0, collect_stats: bool = False, bvh: str = "reference",
                  stage_timing: bool = False, build: str = "device", triangle_test: str = "mt"):
         """triangle_test "watertight": every job traverses with the watertight
-        test (the plain and loop drivers; the persistent driver refuses it)."""
+        test, in every driver."""
         self._lib = native.load()
         cfg = native.Config()
         cfg.device = device
