@@ -75,29 +75,35 @@ DEFAULT_MODES = ("loop", "persistent")
 
 def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS,
                stacks=DEFAULT_STACKS, steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1,
-               repeats: int = 2, use_cache: bool = True, log: Optional[callable] = None) -> Dict:
+               repeats: int = 2, use_cache: bool = True, log: Optional[callable] = None,
+               refine_samples: Optional[int] = 0) -> Dict:
     """Returns {"mode", "pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials"}.
 
     Coordinate search per driver: the pool capacity first (other parameters
     at their defaults), then block size x stack entries x steps x register
     variant; the fastest over both drivers wins.  Trials replay a CUDA graph
-    (the way the runs are timed), so the loop driver is measured as it runs."""
+    (the way the runs are timed), so the loop driver is measured as it runs.
+    Then the winner and the pool sizes next to it are timed again on a longer
+    run (refine_samples per job, 0 = every sample, None = no refinement):
+    short trials under-fill large pools."""
     cache = _load_cache() if use_cache else {}
-    ckey = f"batch/{_gpu_name()}/{'+'.join(modes)}/{key}"
+    ckey = f"batch/{_gpu_name()}/{'+'.join(modes)}/r{refine_samples}/{key}"   # r0: refined on the full run
     if use_cache and ckey in cache:
         return dict(cache[ckey], cached=True)
     best = None
     trials = []
     t0 = time.time()
 
+    def measure(cfg, samples):
+        mode = cfg["mode"]
+        args = {k: v for k, v in cfg.items() if k not in ("mode", "ms")}
+        batch.run(mode, sample_limit=samples, use_graph=True, **args)   # capture
+        return min(batch.run(mode, sample_limit=samples, use_graph=True, **args)["device_ms"] for _ in range(repeats))
+
     def trial(cfg):
         nonlocal best
         try:
-            mode = cfg["mode"]
-            args = {k: v for k, v in cfg.items() if k != "mode"}
-            batch.run(mode, sample_limit=sample_limit, use_graph=True, **args)   # capture
-            ms = min(batch.run(mode, sample_limit=sample_limit, use_graph=True, **args)["device_ms"]
-                     for _ in range(repeats))
+            ms = measure(cfg, sample_limit)
         except Exception as e:   # a shape that does not fit (e.g. shared memory) is skipped
             trials.append(dict(cfg, error=str(e)))
             return None
@@ -125,6 +131,23 @@ def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks
     for tr in trials:
         if "ms" in tr and (tr["mode"] not in per_mode or tr["ms"] < per_mode[tr["mode"]]["ms"]):
             per_mode[tr["mode"]] = dict(tr)
+    if refine_samples is not None and (refine_samples == 0 or refine_samples > sample_limit):
+        base = {k: v for k, v in best.items() if k != "ms"}
+        i = list(pools).index(base["pool_paths"]) if base["pool_paths"] in pools else -1
+        cands = [base] + [dict(base, pool_paths=pools[j]) for j in (i - 1, i + 1) if i >= 0 and 0 <= j < len(pools)]
+        refined = None
+        for c in cands:
+            try:
+                ms = measure(c, refine_samples)
+            except Exception as e:
+                trials.append(dict(c, error=str(e), refine_samples=refine_samples))
+                continue
+            trials.append(dict(c, ms=ms, refine_samples=refine_samples))
+            if refined is None or ms < refined["ms"]:
+                refined = dict(c, ms=ms)
+        if refined is not None:
+            best = dict(refined, refine_samples=refine_samples)
+            per_mode[best["mode"]] = {k: v for k, v in best.items()}
     best["per_mode"] = per_mode
     best["trials"] = len(trials)
     best["tune_seconds"] = time.time() - t0
