@@ -41,8 +41,8 @@ WORKLOAD = "batch_64_uneven_jobs"
 NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
 PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
 # DRAM bytes (read + write) per extension ray of k_lp_extend, from one ncu
-# capture of the 4-job case (profiles/k_lp_extend_batch_4_jobs.md: 62.79 MB
-# for a launch of 1,048,576 rays).
+# capture of a steady-state launch of the 4-job case (62.79 MB for a launch of
+# 1,048,576 rays).
 TRAFFIC_BYTES_PER_EXT_RAY = 62789632 / 1048576
 
 
@@ -150,29 +150,87 @@ def make_jobs(count: int, seed: int = 5):
 
 
 # ------------------------------------------------------------------ CPU side
-def cpu_sample(jobs, seconds: float, threads: int, kind: str, seed: int = 0, frac: float = 2e-3):
-    """Times the CPU oracle on a random pixel subset of every job at the job's
-    full spp; the subset grows until the render takes about `seconds`.
-    Returns (paths/s, description).  The reference has no firefly clamp, so the
-    reference kind renders the jobs unclamped (same work per path)."""
+# The CPU baseline renders this fraction of every job's pixels (a seeded random
+# subset, distinct pixels) at the job's full spp, in both the reference arm and
+# the cpu_baseline leg of this arm.
+PIXEL_FRACTION = 0.01
+CPU_TRACER = ("ScalarCpuPathTracer::render_sample_pixels on a pool of {t} worker threads created once per "
+              "call (one tracer per worker and job over the job's shared CpuBvhAccelerator, as "
+              "TiledCpuPathTracer's tiles share theirs); a chunk of pixels renders all its samples in order")
+
+
+def workload_config(jobs):
+    """The `config` of both arms' lines: the workload and its sizes."""
+    return {"workload": WORKLOAD, "jobs": len(jobs),
+            "paths_per_step": sum(j.settings.width * j.settings.height * j.settings.spp for j in jobs),
+            "triangles": sum(j.scene.triangle_count for j in jobs),
+            "l2": "inputs larger than L2 (all scenes, BVHs and the path pool resident in HBM)"}
+
+
+def cpu_batch(jobs, frac: float, threads: int, kind: str, seed: int = 0):
+    """The CPU oracle over a seeded random `frac` of every job's pixels at the
+    job's spp (vko_render_jobs).  Returns a dict with the paths, the render
+    time (the timed region: the workers' render phases only, scene set-up
+    excluded as ptbench excludes it), the pixel lists and the films."""
     import oracle
     o = oracle.load(kind)
     rng = np.random.default_rng(seed)
-    while True:
-        paths, ms = 0, 0.0
-        for j in jobs:
-            st = j.settings
-            if kind == "reference":
-                st = scenes.RenderSettings(**{**st.__dict__, "firefly_clamp": 0.0})
-            npx = st.width * st.height
-            k = max(8, int(npx * frac))
-            px = np.sort(rng.choice(npx, size=min(k, npx), replace=False)).astype(np.uint32)
-            r = o.render(j.scene, st, first_sample=0, n_samples=st.spp, threads=threads, pixels=px)
-            paths += px.size * st.spp
-            ms += r["counters"]["render_ms"]
-        if ms >= 1000.0 * seconds * 0.5 or frac >= 1.0:
-            return paths / (ms / 1e3), {"pixel_fraction": frac, "paths": paths, "render_ms": ms}
-        frac = min(1.0, frac * max(2.0, 1000.0 * seconds / max(ms, 1.0)))
+    specs = []
+    for j in jobs:
+        npx = j.settings.width * j.settings.height
+        k = min(npx, max(1, int(round(npx * frac))))
+        specs.append((j.scene, j.settings, np.sort(rng.choice(npx, size=k, replace=False)).astype(np.uint32)))
+    t0 = time.perf_counter()
+    outs, ms = o.render_jobs(specs, threads=threads)
+    wall = time.perf_counter() - t0
+    paths = sum(px.size * st.spp for _, st, px in specs)
+    return {"paths": paths, "render_ms": ms, "wall_s": wall, "paths_per_s": paths / (ms / 1e3),
+            "specs": specs, "outs": outs}
+
+
+def tiled_check(jobs, threads: int, kind: str):
+    """The reference's own TiledCpuPathTracer (worker_count = threads, 16-row
+    tiles) rendering one whole job, the one whose path count is closest to
+    one million: a cross-check that the pooled harness is not slower than
+    the reference's tiled tracer on the same host."""
+    import oracle
+    o = oracle.load(kind)
+    j = min(jobs, key=lambda j: abs(j.settings.width * j.settings.height * j.settings.spp - 1_000_000))
+    r = o.render(j.scene, j.settings, threads=threads)
+    paths = j.settings.width * j.settings.height * j.settings.spp
+    return {"tracer": "TiledCpuPathTracer" if kind == "reference" else "port", "worker_count": threads,
+            "tile_height": 16, "job": {"side": j.settings.width, "spp": j.settings.spp,
+                                       "depth": j.settings.max_depth, "triangles": j.scene.triangle_count},
+            "paths": paths, "render_ms": r["counters"]["render_ms"],
+            "paths_per_s": paths / (r["counters"]["render_ms"] / 1e3)}
+
+
+def film_parity(cpu, sums, counts):
+    """GPU films (full films per job) against the CPU oracle's films of the same
+    jobs on the oracle's pixel subset: bit-identical pixels, relative RMSE of
+    the per-pixel means, the fraction of channels outside 3 sigma of the
+    oracle's own per-sample spread, and sample-count mismatches."""
+    exact = px_total = fails = chans = count_bad = 0
+    dsq = rsum = 0.0
+    for (sc, st, px), out, g, c in zip(cpu["specs"], cpu["outs"], sums, counts):
+        gs = np.ascontiguousarray(g.reshape(-1, 3)[px], np.float32)
+        gc = np.asarray(c).reshape(-1)[px].astype(np.uint32)
+        rs, rc, m2 = out["sum"], out["count"], out["m2"].astype(np.float64)
+        count_bad += int(np.sum(gc != rc))
+        exact += int(np.sum(np.all(gs.view(np.uint32) == rs.view(np.uint32), axis=1)))
+        px_total += px.size
+        n = np.maximum(rc, 1).astype(np.float64)[:, None]
+        gm, rm = gs / n, rs.astype(np.float64) / n
+        diff = gm - rm
+        dsq += float(np.sum(diff ** 2))
+        rsum += float(np.sum(rm))
+        chans += diff.size
+        var = np.maximum(0.0, (m2 - rs.astype(np.float64) ** 2 / n) / np.maximum(n - 1.0, 1.0))
+        fails += int(np.sum(np.abs(diff) > 3.0 * np.sqrt(var / n) + 1e-6 * (1.0 + np.abs(rm))))
+    mean = rsum / max(1, chans)
+    return {"pixels": px_total, "bit_exact_frac": exact / max(1, px_total),
+            "rmse_rel": (dsq / max(1, chans)) ** 0.5 / max(mean, 1e-12),
+            "sigma3_fail": fails / max(1, chans), "count_mismatch": count_bad}
 
 
 def run_reference(args, world, rank):
@@ -182,25 +240,33 @@ def run_reference(args, world, rank):
     kind = "reference" if oracle.have_reference() else "port"
     threads = os.cpu_count() or 1
     jobs = make_jobs(args.jobs)
-    per_step_s = args.cpu_step_seconds or max(1.5, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
-    vals, sample, frac = [], None, 2e-3
+    cfg = workload_config(jobs)
+    frac = args.cpu_fraction or PIXEL_FRACTION
+    paths = render_ms = 0.0
+    sample = None
     for i in range(args.warmup + args.steps):
-        v, sample = cpu_sample(jobs, per_step_s, threads, kind, seed=i, frac=frac)
-        frac = sample["pixel_fraction"]
+        r = cpu_batch(jobs, frac, threads, kind, seed=i)
+        sample = r
         if i >= args.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
-    total_paths = sum(j.settings.width * j.settings.height * j.settings.spp for j in jobs)
+            paths += r["paths"]
+            render_ms += r["render_ms"]
+    value = paths / (render_ms / 1e3)
+    tiled = tiled_check(jobs, threads, kind)
+    tracer = CPU_TRACER.format(t=threads) if kind == "reference" else f"the oracle port on {threads} threads"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_paths / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": render_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "jobs": len(jobs), "paths": total_paths,
-                       "triangles": sum(j.scene.triangle_count for j in jobs), "parallelism": "cpu threads"},
+            "data": "synthetic (seeded generator)", "config": cfg, "parallelism": f"cpu threads x{threads}",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"random {sample['pixel_fraction']:.4f} of every job's pixels at the job's "
-                                       f"spp per step ({sample['paths']} paths), scalar tracers over a shared "
-                                       f"accelerator on {threads} threads"},
+                             "sample": f"random {frac:g} of every job's pixels at the job's spp per step "
+                                       f"({sample['paths']} paths per step; {tracer})",
+                             "tracer": "ScalarCpuPathTracer" if kind == "reference" else "port",
+                             "threads": threads, "pixel_fraction": frac},
+            "timing": {"ms_per_step": "measured render time of each step's sampled paths (scene set-up "
+                                      "excluded, as ptbench times only its render loop)",
+                       "full_workload_ms_estimate": 1e3 * cfg["paths_per_step"] / value,
+                       "step_wall_s_with_setup": sample["wall_s"]},
+            "tiled_check": tiled,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -245,12 +311,12 @@ def full_frame(device, tunings=None):
     return out
 
 
-def sdf_scene(device, cpu_seconds: float = 0.0):
+def sdf_scene(device, cpu_fraction: float = 0.0):
     """SDF primitives next to the triangle BVH (the SDF gallery: analytic
     ellipsoid, five sphere-traced shapes, a triangle ground) at 1280x720,
     16 spp, depth 8, as one job of the loop driver; per-stage times from a
     host-driven run; SDF work from one counted sample through the wavefront
-    path; optionally the CPU oracle on a bounded pixel sample of the same job."""
+    path; optionally the CPU oracle on a random fraction of the same job's pixels."""
     from vkpathtracer_b200.tracer import BatchRenderer, CudaPathTracer
     sc = scenes.sdf_gallery()
     st = scenes.RenderSettings(width=1280, height=720, spp=16, max_depth=8, seed=1234)
@@ -279,15 +345,15 @@ def sdf_scene(device, cpu_seconds: float = 0.0):
                            "sdf_tests": c["sdf_tests"] / (st.width * st.height),
                            "sdf_steps": c["sdf_steps"] / (st.width * st.height)}
         out["sdf_steps_per_s"] = out["per_path"]["sdf_steps"] * out["paths_per_s"]
-    if cpu_seconds > 0.0:
+    if cpu_fraction > 0.0:
         import oracle
         kind = "reference" if oracle.have_reference() else "port"
         threads = os.cpu_count() or 1
-        v, sample = cpu_sample([scenes.Job(sc, st, 0)], cpu_seconds, threads, kind)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-                               "sample": f"random {sample['pixel_fraction']:.4f} of the pixels at 16 spp "
-                                         f"({sample['paths']} paths)"}
-        out["speedup_vs_cpu"] = out["paths_per_s"] / v
+        r = cpu_batch([scenes.Job(sc, st, 0)], cpu_fraction, threads, kind)
+        out["cpu_baseline"] = {"value": r["paths_per_s"], "unit": UNIT, "cores": threads, "kind": kind,
+                               "sample": f"random {cpu_fraction:g} of the pixels at 16 spp ({r['paths']} paths; "
+                                         + CPU_TRACER.format(t=threads) + ")"}
+        out["speedup_vs_cpu"] = out["paths_per_s"] / r["paths_per_s"]
     return out
 
 
@@ -420,13 +486,35 @@ def ray_query(device):
                     e1.record(s)
                 s.synchronize()
                 out[f"{prefix}{name}_mrays_per_s"] = n / (e0.elapsed_time(e1) / 10) / 1e3
+                if test == "mt" and name == "any":
+                    occluded = prim.cpu().numpy().astype(np.uint32)
             closest[test] = prim.cpu().numpy()
+            if test == "mt":
+                # kept for the parity block (not printed)
+                out["_ids"] = (sc, rays, closest["mt"].view(np.uint32).copy(), dist.cpu().numpy(), occluded)
             if test == "mt":
                 t0 = time.perf_counter()
                 t.trace_rays(rays)
                 out["closest_e2e_mrays_per_s"] = n / (time.perf_counter() - t0) / 1e6
     out["watertight_ids_equal_to_mt"] = float(np.mean(closest["mt"] == closest["watertight"]))
     return out
+
+
+def ray_query_parity(ids, threads: int, kind: str):
+    """Closest-hit primitive ids and distances of the ray-query workload
+    (8,388,608 rays, 1,046,904 triangles) against the CPU oracle's
+    CpuBvhAccelerator::intersect on the same rays, and any-hit (unbounded)
+    against 'the closest hit exists'."""
+    import oracle
+    sc, rays, prim, dist, occluded = ids
+    t0 = time.perf_counter()
+    rp, rt, _, ms = oracle.load(kind).intersect(sc, rays, threads=threads)
+    wall = time.perf_counter() - t0
+    return {"ray_query": {"rays": int(rays.shape[0]), "ids_mismatch": int(np.sum(prim != rp)),
+                          "t_mismatch": int(np.sum(dist.view(np.uint32) != rt.view(np.uint32))),
+                          "any_hit_mismatch": int(np.sum(occluded.astype(bool) != np.isfinite(rt))),
+                          "against": f"{kind} CpuBvhAccelerator::intersect on {threads} threads "
+                                     f"({wall:.1f} s with its build)"}}
 
 
 def inverse_rendering(device, gd_steps: int = 200):
@@ -678,7 +766,11 @@ def run_ours(args, world, rank, local):
     e2e_ms = reduce_over_ranks(world, 1e3 * (time.perf_counter() - w0), "max", dev)
     e2e = {"value": all_paths / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
            "path": f"vkptc_batch_run ({mode} driver, graph) + vkptc_batch_read_films (every job's rgb sums and "
-                   "sample counts into pinned host buffers), every step; scenes and BVHs uploaded once before timing"}
+                   "sample counts into pinned host buffers), every step",
+           "inputs": "no per-step input copies: the scenes, their BVHs and the job table are uploaded and built "
+                     f"once before timing ({setup_s:.2f} s of set-up for the {len(jobs)} jobs), as ptbench loads "
+                     "and builds the scene once before its timed render loop; each step's input is the work "
+                     "counter, reset on the device"}
     # both drivers, each with its own best tuning, on the same jobs
     drivers = {}
     for m, cfg in tune.get("per_mode", {}).items():
@@ -701,7 +793,7 @@ def run_ours(args, world, rank, local):
         wt = {"paths_per_s": total_paths / (wms / 1e3), "driver": "loop", "tuning": tuning,
               "relative_to_moller_trumbore": (total_paths / (wms / 1e3)) / (value / world)}
 
-    roof = rq = ff = cpu = inv = sdf = bb = fr = None
+    roof = rq = ff = cpu = inv = sdf = bb = fr = parity = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the dominant kernel
         # traversal work counted in a stats run (same rays: the traversal is deterministic)
@@ -726,8 +818,8 @@ def run_ours(args, world, rank, local):
             roof = {"kernel": "k_lp_extend (closest-hit traversal stage of the loop driver)", "bound": "hbm",
                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                     "peak_kind": f"{peak_kind} HBM copy bandwidth", "traffic": traffic,
-                    "traffic_note": "per launch: DRAM bytes per extension ray from the ncu capture of the 4-job "
-                                    "case (profiles/k_lp_extend_batch_4_jobs.md) x extension rays per launch",
+                    "traffic_note": "per launch: DRAM bytes per extension ray from an ncu capture of a "
+                                    "steady-state launch of the 4-job case x extension rays per launch",
                     "alg_bytes_per_launch": alg / iters, "avg_launch_ms": stage["extend"] / iters,
                     "launches": iters, "stage_ms": stage,
                     "stage_share": {k: v / max(1e-9, sum(stage.values())) for k, v in stage.items()},
@@ -749,28 +841,39 @@ def run_ours(args, world, rank, local):
         if not args.no_fullframe:
             ff = full_frame(local, {m: d["tuning"] for m, d in drivers.items()} or None)
         inv = None if args.no_adjoint else inverse_rendering(local)
-        sdf = None if args.no_sdf else sdf_scene(local, 0.0 if (args.no_cpu or world > 1) else 5.0)
+        sdf = None if args.no_sdf else sdf_scene(local, 0.0 if (args.no_cpu or world > 1) else 0.4)
         bb = None if args.no_build else bvh_build(local, cpu=not args.no_cpu and world == 1)
         fr = film_resolve(local, cpu=not args.no_cpu and world == 1)
         if world == 1 and not args.no_cpu:
             import oracle
             kind = "reference" if oracle.have_reference() else "port"
             threads = os.cpu_count() or 1
-            v, sample = cpu_sample(jobs, 15.0, threads, kind)
-            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-                   "sample": f"random {sample['pixel_fraction']:.4f} of every job's pixels at the job's spp "
-                             f"({sample['paths']} paths, {sample['render_ms']:.0f} ms on {threads} threads)"}
+            frac = args.cpu_fraction or PIXEL_FRACTION
+            r = cpu_batch(jobs, frac, threads, kind, seed=0)
+            tracer = CPU_TRACER.format(t=threads) if kind == "reference" else f"the oracle port on {threads} threads"
+            cpu = {"value": r["paths_per_s"], "unit": UNIT, "cores": threads, "kind": kind,
+                   "sample": f"random {frac:g} of every job's pixels at the job's spp ({r['paths']} paths, "
+                             f"{r['render_ms']:.0f} ms; {tracer})",
+                   "tracer": "ScalarCpuPathTracer" if kind == "reference" else "port", "threads": threads,
+                   "pixel_fraction": frac}
+            # the timed run's films against the CPU oracle on the same pixels
+            parity = {"films": film_parity(r, hostsums, hostcounts),
+                      "films_against": f"{kind} CPU tracer, the cpu_baseline pixel subset of every job "
+                                       "(the films of the last timed step)"}
+            if rq is not None and "_ids" in rq:
+                parity.update(ray_query_parity(rq.pop("_ids"), threads, kind))
+        if rq is not None:
+            rq.pop("_ids", None)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-                "config": {"workload": WORKLOAD, "jobs": len(jobs), "paths_per_step": total_paths,
-                           "triangles": sum(j.scene.triangle_count for j in jobs),
-                           "setup_s": setup_s, "bvh": "sah traversal tree (hit ids exact: ties and parallel-axis "
-                                                    "rule through the reference tree)",
-                           "driver": mode, "tuning": tuning,
-                           "autotune": {k: tune.get(k) for k in ("ms", "trials", "cached")},
-                           "l2": "inputs larger than L2 (all scenes, BVHs and the path pool resident in HBM)",
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "config": workload_config(jobs),
+                "parallelism": f"replicas x{world} (one job set per rank)" if world > 1 else "single GPU",
+                "run": {"setup_s": setup_s, "bvh": "sah traversal tree (hit ids exact: ties and parallel-axis "
+                                                   "rule through the reference tree)",
+                        "driver": mode, "tuning": tuning,
+                        "autotune": {k: tune.get(k) for k in ("ms", "trials", "cached")}},
+                "parity": parity,
                 "mrays_per_s": mrays, "plain_paths_per_s": plain_ps, "speedup_vs_plain": value / world / plain_ps,
                 "drivers": drivers,
                 "plain_kernel_launches": plain["kernel_launches"],
@@ -808,11 +911,23 @@ def main():
                     help="profiling aid: run the inverse-rendering forward and backward twice, and exit")
     ap.add_argument("--profile-sdf", action="store_true",
                     help="profiling aid: render the SDF gallery twice with the loop driver, no CUDA graph, and exit")
-    ap.add_argument("--cpu-step-seconds", type=float, default=0.0,
-                    help="CPU work per reference-arm step (0 = about a minute over all steps)")
+    ap.add_argument("--cpu-fraction", type=float, default=0.0,
+                    help=f"pixel fraction of every job the CPU baseline renders (0 = {PIXEL_FRACTION})")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # One process per GPU: re-launch this command under torchrun.
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}: launch one process per GPU")
     world, rank, local = dist_init(args)
     try:
         if args.profile_build:

@@ -2,7 +2,7 @@
  * vkptc.h -- C ABI of libvkpt_cuda, the sm_100a render backend for vkPathTracer.
  *
  * This is the boundary a `src/gpu/cuda` IPathTracer adapter in the reference
- * binds (see INTEGRATION.md).  Plain pointers and sizes only; every call
+ * binds.  Plain pointers and sizes only; every call
  * returns a vkptc_status_code (the numeric values of vkpt::core::StatusCode,
  * src/core/contracts/Result.h:13-23) and never throws.  Host buffers passed
  * in are read or written synchronously before the call returns; the context
@@ -445,6 +445,10 @@ int32_t vkptc_read_traversal_stats(vkptc_ctx* ctx, uint64_t* out);
 int32_t vkptc_get_status(vkptc_ctx* ctx, vkptc_tracer_status* out);
 /* Last error message of this context (empty when none); valid until the next call. */
 const char* vkptc_last_error(vkptc_ctx* ctx);
+/* The device a context renders on: its name (cudaDeviceProp::name, NUL-terminated, cut to
+ * capacity) for BenchmarkResult.device_info.gpu_name (src/benchmark/BenchmarkSchema.h:80-85),
+ * and optionally its SM count. */
+int32_t vkptc_device_name(vkptc_ctx* ctx, char* out, uint32_t capacity, uint32_t* sm_count);
 
 /* ---- ray queries --------------------------------------------------------------
  * replaces IRayAccelerator::intersect (src/pathtracer/PathTracer.h:1001-1036), one
@@ -456,7 +460,12 @@ const char* vkptc_last_error(vkptc_ctx* ctx);
 int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, uint64_t ray_count,
                          uint32_t mode, uint32_t* prim_out, float* t_out);
 /* Same with DEVICE pointers already resident in HBM, enqueued on `stream`
- * (a cudaStream_t; 0 = the context's stream).  No host synchronisation. */
+ * (a cudaStream_t; 0 = the context's stream).  No host synchronisation.
+ * When `stream` is not the context's stream, it first waits for the work
+ * queued on the context's stream and the context's stream then waits for the
+ * query (two events made with the context), so a later rebuild or upload on
+ * the context cannot overtake it; while either stream is being captured no
+ * such events are inserted and the caller orders the call itself. */
 int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float* d_tmax, uint64_t ray_count,
                                 uint32_t mode, uint32_t* d_prim_out, float* d_t_out, void* stream);
 
@@ -488,7 +497,11 @@ typedef struct vkptc_batch_tuning {
                                 (loop mode without a graph runs one host round trip per iteration) */
   uint32_t occupancy;        /* persistent kernel register variant: 0..3 = at least 1..4 resident
                                 256-thread blocks per SM (fewer registers, more warps) */
-  uint32_t reserved;
+  uint32_t barrier_spins;    /* persistent mode: bound of a grid-barrier wait in sleeps of ~128 ns
+                                (0 = 2^26, about 8.6 s); a block that waits longer aborts the run,
+                                every block leaves at its next barrier and vkptc_batch_run returns
+                                VKPTC_TIMEOUT with the batch still usable (the next run clears the
+                                films and renders them anew) */
 } vkptc_batch_tuning;
 
 typedef struct vkptc_batch_stats {
@@ -546,15 +559,43 @@ const char* vkptc_batch_last_error(vkptc_batch* batch);
  *   d_film_sum   W*H float4 per pixel (rgb sum; w untouched), 16-byte aligned
  *   d_film_count W*H uint32 sample counts
  * (W, H from vkptc_configure; device memory of the context's device).
- * A tile covering more than VKPTC_NOALLOC_MAX_PATHS pixels is rejected with
- * VKPTC_INVALID_ARGUMENT and a message naming the limit.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  Every call shares the one array and it keeps
- * the last call's contents, so calls whose GPU work overlaps (on different
- * streams, or from different contexts on the same device) race: the caller
- * must order them, e.g. on one stream.  Work is enqueued on `stream` (NULL =
- * the context's stream) and the call returns without synchronising. */
+ *
+ * Limits:
+ *  - A tile covering more than VKPTC_NOALLOC_MAX_PATHS pixels is rejected with
+ *    VKPTC_INVALID_ARGUMENT and a message naming the limit.
+ *  - The whole traversal stack must fit in shared memory (no spill buffer):
+ *    the BVH's worst-case stack (vkptc_accel_info.stack_required entries of
+ *    8 bytes per thread, times vkptc_config.block_size threads, 128 when 0)
+ *    must not exceed the device's opt-in shared memory per block (227 KB on
+ *    B200, i.e. 227 entries at 128 threads).  A deeper BVH is refused with
+ *    VKPTC_UNSUPPORTED, although vkptc_render succeeds on the same context.
+ *
+ * Set-up: the array's device address is looked up (cudaGetSymbolAddress)
+ * when the context is created, with its device current; this call itself
+ * makes no lookup.  A device reset (cudaDeviceReset) invalidates every
+ * context and that address with it: create new contexts after a reset.
+ *
+ * Sharing: every call shares the one array, and it keeps the last call's
+ * contents (each call sets what must start at zero).  Calls whose GPU work
+ * overlaps (on different streams, or from different contexts on the same
+ * device) race on it: the caller must order them, e.g. on one stream.
+ *
+ * Streams: work is enqueued on `stream` (NULL = the context's stream) and the
+ * call returns without synchronising.  When `stream` is not the context's
+ * stream, it first waits for the work already queued on the context's stream,
+ * and the context's stream then waits for this call's kernels (two events
+ * made with the context), so a later rebuild, scene reload or upload on the
+ * context cannot free or rewrite what these kernels read.  While either
+ * stream is being captured no such events are inserted, and the caller must
+ * order this call against the context's other work itself.
+ *
+ * Errors and counters: argument, lifecycle and launch errors are returned by
+ * this call.  The kernels write the context's device error word (a traversal
+ * stack overflow, which the stack sizing above rules out) and, with
+ * collect_stats, its traversal counters; both are read by the context's next
+ * synchronising call (vkptc_synchronize, vkptc_read_counters, ...), and the
+ * counters are shared with the context's own renders.  The caller's current
+ * device is restored before return. */
 #define VKPTC_NOALLOC_MAX_PATHS 65536u
 int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* tile, uint32_t frame, float* d_film_sum,
                                   uint32_t* d_film_count, void* stream);

@@ -28,7 +28,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libvkptref.so")
 PORT_LIB = os.path.join(HERE, "_build", "libvkptport.so")
 ADJ_LIB = os.path.join(HERE, "_build", "libvkptadj.so")
-REFERENCE_SRC = "/root/reference/src"
+# The reference checkout (read-only); VKPT_REFERENCE_DIR overrides the default location.
+REFERENCE_DIR = os.environ.get("VKPT_REFERENCE_DIR", "/root/reference")
+REFERENCE_SRC = os.path.join(REFERENCE_DIR, "src")
 
 
 class VkoScene(ctypes.Structure):
@@ -88,6 +90,13 @@ class VkoCounters(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class VkoJob(ctypes.Structure):
+    _fields_ = [("scene", ctypes.POINTER(VkoScene)), ("settings", ctypes.POINTER(VkoSettings)),
+                ("pixels", ctypes.c_void_p), ("pixel_count", ctypes.c_uint32), ("first_sample", ctypes.c_uint32),
+                ("n_samples", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("film_sum", ctypes.c_void_p),
+                ("film_count", ctypes.c_void_p), ("film_m2", ctypes.c_void_p), ("counters", VkoCounters)]
+
+
 class VkoInstanceUpdate(ctypes.Structure):
     _fields_ = [("instance_index", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("translation", ctypes.c_float * 3),
                 ("rotation", ctypes.c_float * 4), ("scale", ctypes.c_float * 3)]
@@ -113,8 +122,8 @@ def build_port(quiet: bool = True) -> str:
     """Compile the restatement with g++ (no reference sources needed)."""
     os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
     src = os.path.join(HERE, "port.cpp")
-    if (not os.path.exists(PORT_LIB)) or os.path.getmtime(PORT_LIB) < max(
-            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "vkpt_oracle.h"))):
+    deps = [src] + [os.path.join(HERE, f) for f in ("vkpt_oracle.h", "worker_pool.h")]
+    if (not os.path.exists(PORT_LIB)) or os.path.getmtime(PORT_LIB) < max(os.path.getmtime(d) for d in deps):
         cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-o", PORT_LIB, src, "-lpthread"]
         subprocess.run(cmd, check=True, capture_output=quiet)
     return PORT_LIB
@@ -150,6 +159,9 @@ class Oracle:
         L.vko_intersect.argtypes = [ctypes.POINTER(VkoScene), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.POINTER(ctypes.c_double)]
+        L.vko_render_jobs.restype = ctypes.c_int
+        L.vko_render_jobs.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.POINTER(ctypes.c_double)]
         L.vko_last_error.restype = ctypes.c_char_p
         L.vko_impl_name.restype = ctypes.c_char_p
         L.vko_set_triangle_test.restype = ctypes.c_int
@@ -257,6 +269,35 @@ class Oracle:
         self._check(rc)
         return {"sum": film, "count": count, "invalid": invalid, "samples": samples,
                 "counters": ctr.as_dict()}
+
+    def render_jobs(self, jobs, threads: int = 1):
+        """Many jobs on one pool of `threads` workers (vko_render_jobs).
+        jobs: [(scene, settings, pixels)] with pixels a 1-D array of distinct
+        y*W+x indices; every sample of each listed pixel is rendered.
+        Returns ([dict(sum=(n,3), count=(n,), m2=(n,3), counters)], render_ms)."""
+        recs = (VkoJob * max(1, len(jobs)))()
+        keep, outs = [], []
+        for k, (scene, settings, pixels) in enumerate(jobs):
+            sc, kp = self.make_scene(scene)
+            st = self.make_settings(settings)
+            px = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1)
+            out = {"sum": np.zeros((px.size, 3), np.float32), "count": np.zeros(px.size, np.uint32),
+                   "m2": np.zeros((px.size, 3), np.float32)}
+            keep.append((sc, st, kp, px))
+            outs.append(out)
+            r = recs[k]
+            r.scene, r.settings = ctypes.pointer(sc), ctypes.pointer(st)
+            r.pixels, r.pixel_count = _ptr(px), px.size
+            r.first_sample, r.n_samples = 0, settings.spp
+            r.film_sum, r.film_count, r.film_m2 = _ptr(out["sum"]), _ptr(out["count"]), _ptr(out["m2"])
+        ms = ctypes.c_double(0.0)
+        rc = self.lib.vko_render_jobs(ctypes.cast(recs, ctypes.c_void_p), len(jobs), max(1, threads),
+                                      ctypes.byref(ms))
+        self._check(rc)
+        for k, out in enumerate(outs):
+            out["counters"] = recs[k].counters.as_dict()
+        del keep
+        return outs, ms.value
 
     def apply_film_resolve(self, hdr: np.ndarray, exposure: float = 1.0, white_balance_kelvin: float = 6500.0,
                            tone_map: str = "linear", output_transform: str = "gamma", gamma: float = 2.2,

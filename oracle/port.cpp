@@ -33,8 +33,10 @@
 //                                   src/pathtracer/FilmBuffer.cpp:30-49, 216-224, 253-325
 
 #include "vkpt_oracle.h"
+#include "worker_pool.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -1287,6 +1289,77 @@ int vko_render(const vko_scene* scene, const vko_settings* settings, uint32_t fi
     }
     counters->render_ms = ms;
   }
+  return 0;
+}
+
+int vko_render_jobs(vko_job* jobs, uint32_t job_count, uint32_t threads, double* render_ms) {
+  if (!jobs && job_count) return fail("null job list");
+  const uint32_t nt = std::max(1u, threads);
+  vko::WorkerPool pool(nt);
+  double total_ms = 0.0;
+  for (uint32_t j = 0; j < job_count; ++j) {
+    vko_job& J = jobs[j];
+    std::memset(&J.counters, 0, sizeof(J.counters));
+    if (!J.scene || !J.settings) return fail("null scene or settings");
+    if (J.pixel_count == 0 || J.n_samples == 0) continue;
+    if (!J.pixels || !J.film_sum || !J.film_count) return fail("null pixel list or film");
+    const uint32_t W = J.settings->width, H = J.settings->height;
+    const size_t npx = static_cast<size_t>(W) * H;
+    for (uint32_t i = 0; i < J.pixel_count; ++i)
+      if (J.pixels[i] >= npx) return fail("pixel index outside the film");
+    World w;
+    w.load(*J.scene);
+    Integrator it{w, *J.settings};
+    const uint32_t chunk = vko::chunk_pixels(J.pixel_count, nt);
+    const uint32_t chunks = (J.pixel_count + chunk - 1) / chunk;
+    std::vector<float> sum(3u * J.pixel_count, 0.0f), m2(sum.size(), 0.0f);
+    std::vector<uint32_t> cnt(J.pixel_count, 0u);
+    std::vector<Stats> stats(nt);
+    std::vector<uint64_t> segs(nt, 0u), samples(nt, 0u);
+    std::atomic<uint32_t> next{0u};
+    const double ms = pool.run([&](uint32_t t) {
+      for (;;) {
+        const uint32_t c = next.fetch_add(1u);
+        if (c >= chunks) return;
+        const uint32_t b = c * chunk, e = std::min(J.pixel_count, b + chunk);
+        for (uint32_t k = 0; k < J.n_samples; ++k) {
+          const uint32_t s = J.first_sample + k;
+          for (uint32_t i = b; i < e; ++i) {
+            const uint32_t p = J.pixels[i];
+            V3 c3{};
+            if (!it.shade(p % W, p / W, s, c3, segs[t], stats[t])) continue;   // non-finite: dropped
+            ++samples[t];
+            sum[3 * i + 0] = sum[3 * i + 0] + c3.x;
+            sum[3 * i + 1] = sum[3 * i + 1] + c3.y;
+            sum[3 * i + 2] = sum[3 * i + 2] + c3.z;
+            m2[3 * i + 0] += c3.x * c3.x;
+            m2[3 * i + 1] += c3.y * c3.y;
+            m2[3 * i + 2] += c3.z * c3.z;
+            cnt[i] += 1u;
+          }
+        }
+      }
+    });
+    std::memcpy(J.film_sum, sum.data(), sum.size() * sizeof(float));
+    std::memcpy(J.film_count, cnt.data(), cnt.size() * sizeof(uint32_t));
+    if (J.film_m2) std::memcpy(J.film_m2, m2.data(), m2.size() * sizeof(float));
+    for (uint32_t t = 0; t < nt; ++t) {
+      J.counters.samples += samples[t];
+      J.counters.rays += segs[t];
+      J.counters.triangle_tests += stats[t].tri_tests;
+      J.counters.triangle_hits += stats[t].tri_hits;
+      J.counters.bvh_node_visits += stats[t].nodes;
+      J.counters.bvh_leaf_visits += stats[t].leaves;
+      J.counters.shadow_tests += stats[t].shadow;
+      J.counters.sdf_tests += stats[t].sdf_tests;
+      J.counters.sdf_steps += stats[t].sdf_steps;
+      J.counters.sdf_hits += stats[t].sdf_hits;
+      J.counters.sdf_misses += stats[t].sdf_misses;
+    }
+    J.counters.render_ms = ms;
+    total_ms += ms;
+  }
+  if (render_ms) *render_ms = total_ms;
   return 0;
 }
 

@@ -13,6 +13,7 @@
 // The product library never links this file.
 
 #include "../oracle/vkpt_oracle.h"
+#include "../oracle/worker_pool.h"
 
 #include "core/Logging.h"
 #include "cpu/ParallelBvhBuilder.h"
@@ -28,6 +29,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -522,6 +524,164 @@ int vko_render(const vko_scene* scene, const vko_settings* settings,
     for (auto& tr : tracers) add_counters(counters, tr->read_counters());
     counters->render_ms = ms;
   }
+  return 0;
+}
+
+// The batched CPU baseline: render_sample_pixels (src/pathtracer/ScalarCpuPathTracer.Render.cpp:335-381)
+// on one tracer per worker and job, all of a job's tracers sharing its
+// accelerator as the tiles of TiledCpuPathTracer share theirs
+// (src/cpu/TiledCpuPathTracer.cpp:279-323), on a pool created once per call.
+// Consecutive jobs are grouped while their tracers' films fit a memory budget;
+// a group's chunks form one work queue, so workers move on to the next job
+// instead of waiting at the end of each job.
+namespace {
+
+struct JobState {
+  pt::PathTracerSceneSnapshot snap;
+  pt::RenderSettings rs;
+  std::unique_ptr<pt::IRayAccelerator> accel;
+  std::vector<std::unique_ptr<pt::ScalarCpuPathTracer>> tracers;   // one per worker, created before the run
+  uint32_t chunk = 1, chunks = 0;
+  std::vector<uint32_t> owner;   // worker that rendered each chunk
+  std::vector<float> prev, m2;   // running sums seen and squared sample radiance (film_m2)
+};
+
+constexpr double kGroupFilmBytes = 4.0e9;   // film memory of one group's tracers
+
+}  // namespace
+
+int vko_render_jobs(vko_job* jobs, uint32_t job_count, uint32_t threads, double* render_ms) {
+  quiet_logs();
+  if (!jobs && job_count) return fail("null job list");
+  const uint32_t nt = std::max(1u, threads);
+  for (uint32_t j = 0; j < job_count; ++j) {
+    vko_job& J = jobs[j];
+    std::memset(&J.counters, 0, sizeof(J.counters));
+    if (!J.scene || !J.settings) return fail("null scene or settings");
+    if (J.settings->firefly_clamp != 0.0f) return fail("the reference has no firefly clamp");
+    if (J.pixel_count == 0 || J.n_samples == 0) continue;
+    if (!J.pixels || !J.film_sum || !J.film_count) return fail("null pixel list or film");
+    const std::size_t npx = static_cast<std::size_t>(J.settings->width) * J.settings->height;
+    for (uint32_t i = 0; i < J.pixel_count; ++i)
+      if (J.pixels[i] >= npx) return fail("pixel index outside the film");
+  }
+  vko::WorkerPool pool(nt);
+  double total_ms = 0.0;
+  uint32_t g0 = 0;
+  while (g0 < job_count) {
+    // ---- set-up of one group of jobs (not timed)
+    std::vector<JobState> st;
+    std::vector<std::pair<uint32_t, uint32_t>> items;   // (job in group, chunk)
+    double bytes = 0.0;
+    uint32_t g1 = g0;
+    while (g1 < job_count) {
+      const vko_job& J = jobs[g1];
+      const uint32_t chunk = vko::chunk_pixels(J.pixel_count, nt);
+      const uint32_t chunks = J.pixel_count ? (J.pixel_count + chunk - 1) / chunk : 0u;
+      const uint32_t nw = std::min(nt, chunks);
+      const double b = 32.0 * nw * static_cast<double>(J.settings->width) * J.settings->height;
+      if (g1 > g0 && bytes + b > kGroupFilmBytes) break;
+      bytes += b;
+      JobState s;
+      s.chunk = chunk;
+      s.chunks = (J.n_samples == 0) ? 0u : chunks;
+      if (s.chunks) {
+        s.snap = to_snapshot(*J.scene);
+        s.rs = to_settings(*J.settings, J.first_sample + J.n_samples);
+        s.accel = pt::CreateCpuBvhAccelerator();
+        if (!s.accel->build(s.snap, true)) return fail("accelerator build failed");
+        s.tracers.resize(nw);
+        for (auto& tr : s.tracers) {
+          tr = std::make_unique<pt::ScalarCpuPathTracer>();
+          if (!tr->configure(s.rs) || !tr->set_accelerator(s.accel.get()) || !tr->load_scene_snapshot(s.snap) ||
+              !tr->update_camera(s.snap.camera_position, s.snap.camera_target, s.snap.camera_up,
+                                 s.snap.camera_fov_deg) ||
+              !tr->reset_accumulation()) {
+            return fail("batched-render tracer setup failed");
+          }
+        }
+        s.owner.assign(s.chunks, 0u);
+        if (J.film_m2) {
+          s.prev.assign(3u * J.pixel_count, 0.0f);
+          s.m2.assign(3u * J.pixel_count, 0.0f);
+        }
+        for (uint32_t c = 0; c < s.chunks; ++c) items.emplace_back(g1 - g0, c);
+      }
+      st.push_back(std::move(s));
+      ++g1;
+    }
+    // ---- the group's render phase (timed): one work queue over its chunks.
+    // A worker renders chunks with its own tracer of the chunk's job; a job
+    // has fewer tracers than workers only when it has fewer chunks, and then
+    // worker w uses tracer w % count (one chunk per tracer at a time is
+    // ensured by the per-tracer lock).
+    std::vector<std::unique_ptr<std::mutex>> locks;
+    std::vector<uint32_t> lock_base(st.size(), 0u);
+    for (size_t k = 0; k < st.size(); ++k) {
+      lock_base[k] = static_cast<uint32_t>(locks.size());
+      for (size_t t = 0; t < st[k].tracers.size(); ++t) locks.push_back(std::make_unique<std::mutex>());
+    }
+    std::atomic<size_t> next{0};
+    std::atomic<int> bad{0};
+    const double ms = pool.run([&](uint32_t w) {
+      for (;;) {
+        const size_t it = next.fetch_add(1);
+        if (it >= items.size()) return;
+        const uint32_t k = items[it].first, c = items[it].second;
+        JobState& s = st[k];
+        const vko_job& J = jobs[g0 + k];
+        const uint32_t ti = w % static_cast<uint32_t>(s.tracers.size());
+        std::lock_guard<std::mutex> lk(*locks[lock_base[k] + ti]);
+        pt::ScalarCpuPathTracer& tr = *s.tracers[ti];
+        s.owner[c] = ti;
+        const uint32_t b = c * s.chunk, e = std::min(J.pixel_count, b + s.chunk);
+        for (uint32_t q = 0; q < J.n_samples; ++q) {
+          if (!tr.render_sample_pixels(J.pixels + b, e - b, J.first_sample + q, 0u)) {
+            bad.fetch_add(1);
+            return;
+          }
+          if (J.film_m2) {
+            // A sample's radiance is the change of the pixel's running sum.
+            const auto& raw = tr.film().raw();
+            for (uint32_t i = b; i < e; ++i) {
+              const auto& v = raw[J.pixels[i]];
+              const float cur[3] = {v.x, v.y, v.z};
+              for (int ch = 0; ch < 3; ++ch) {
+                const float x = cur[ch] - s.prev[3 * i + ch];
+                s.m2[3 * i + ch] += x * x;
+                s.prev[3 * i + ch] = cur[ch];
+              }
+            }
+          }
+        }
+      }
+    });
+    if (bad.load() != 0) return fail("render_sample_pixels failed");
+    total_ms += ms;
+    // ---- results of the group
+    for (size_t k = 0; k < st.size(); ++k) {
+      JobState& s = st[k];
+      vko_job& J = jobs[g0 + k];
+      for (uint32_t c = 0; c < s.chunks; ++c) {
+        const auto& film = s.tracers[s.owner[c]]->film();
+        const auto& raw = film.raw();
+        const auto& cnt = film.sample_counts();
+        const uint32_t b = c * s.chunk, e = std::min(J.pixel_count, b + s.chunk);
+        for (uint32_t i = b; i < e; ++i) {
+          const uint32_t p = J.pixels[i];
+          J.film_sum[3 * i + 0] = raw[p].x;
+          J.film_sum[3 * i + 1] = raw[p].y;
+          J.film_sum[3 * i + 2] = raw[p].z;
+          J.film_count[i] = cnt[p];
+        }
+      }
+      if (J.film_m2 && s.chunks) std::memcpy(J.film_m2, s.m2.data(), s.m2.size() * sizeof(float));
+      for (auto& tr : s.tracers) add_counters(&J.counters, tr->read_counters());
+      J.counters.render_ms = ms;   // the render phase of the job's group
+    }
+    g0 = g1;
+  }
+  if (render_ms) *render_ms = total_ms;
   return 0;
 }
 

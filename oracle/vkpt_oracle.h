@@ -130,6 +130,36 @@ int vko_render(const vko_scene* scene, const vko_settings* settings,
                float* film_sum, uint32_t* film_count, float* film_invalid,
                float* per_sample, vko_counters* counters);
 
+/* One job of vko_render_jobs: a scene, its settings and the pixels (y*W+x)
+ * to render, every sample [first_sample, first_sample + n_samples) of each.
+ * Outputs per listed pixel, in list order: film_sum (3 floats, the film's
+ * rgb sum), film_count (samples added), film_m2 (3 floats, optional: the sum
+ * of each sample's squared radiance, for a per-pixel variance).  counters
+ * receives the job's SampleCounters; counters.render_ms its render phase. */
+typedef struct vko_job {
+  const vko_scene* scene;
+  const vko_settings* settings;
+  const uint32_t* pixels;
+  uint32_t pixel_count;
+  uint32_t first_sample;
+  uint32_t n_samples;
+  uint32_t reserved;
+  float* film_sum;
+  uint32_t* film_count;
+  float* film_m2;
+  vko_counters counters;
+} vko_job;
+
+/* Renders many jobs on `threads` workers (the CPU baseline of the batched
+ * workload).  Jobs run one after the other; each job's accelerator and its
+ * per-worker tracers are set up first (not timed, as ptbench times only the
+ * render loop), then the workers, created once per call, pull chunks of the
+ * job's pixel list from a shared counter and render all samples of a chunk
+ * in sample order, so every pixel's film equals the full-frame render's.
+ * *render_ms: summed wall time of the jobs' render phases.  Pixel lists
+ * must not repeat a pixel. */
+int vko_render_jobs(vko_job* jobs, uint32_t job_count, uint32_t threads, double* render_ms);
+
 /* Binary BVH exactly as the accelerator builds it: triangle AABBs padded by
  * 1e-4, midpoint split, stable partition when deterministic != 0.
  * nodes_out: 10 x 32-bit words per node (min3 f32, max3 f32, left, right,

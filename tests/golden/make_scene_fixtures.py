@@ -24,7 +24,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 import oracle  # noqa: E402
 from tests.golden import cases  # noqa: E402
 
-SCENE_DIR = "/root/reference/assets/scenes"
+SCENE_DIR = os.path.join(oracle.REFERENCE_DIR, "assets", "scenes")
 
 
 def main():

@@ -68,7 +68,7 @@ def test_reference_arm_under_torchrun_rank0_only():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.join(ROOT, "bench.py"),
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--jobs", "2",
-           "--cpu-step-seconds", "0.2"]
+           "--cpu-fraction", "0.002"]
     r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
@@ -78,3 +78,26 @@ def test_reference_arm_under_torchrun_rank0_only():
     assert line["value"] > 0 and line["unit"] == "paths/s"
     assert line["cpu_baseline"]["kind"] in ("reference", "port")
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_gpus_flag_launches_one_process_per_rank_without_torchrun():
+    """bench.py --gpus 2 started as a plain process re-launches itself under
+    torchrun with two ranks; the reference arm's line then reports n_gpus 2."""
+    import oracle
+    oracle.build_port()
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    env["PYTHONPATH"] = ROOT
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "3", "--jobs", "2", "--cpu-fraction", "0.002"]
+    r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    assert lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
+
+
+def test_gpus_flag_must_match_world_size():
+    env = dict(os.environ, PYTHONPATH=ROOT, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1"]
+    r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "WORLD_SIZE" in r.stderr

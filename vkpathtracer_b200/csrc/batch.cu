@@ -17,8 +17,9 @@
 // is bit-identical to rendering the job one sample (one launch) at a time.
 //
 // The grid barrier is a counter/generation barrier whose wait is bounded: a
-// block that waits longer than ~8 s sets an abort word, and every block
-// leaves the loop at its next barrier; the host reports a timeout.  The
+// block that waits longer than its bound (BatchPool::barrier_spins sleeps of
+// ~128 ns, ~8.6 s by default) sets an abort word, and every block leaves the
+// loop at its next barrier; the host reports a timeout.  The
 // launch is cooperative, so all blocks are co-resident by construction.
 #include <cooperative_groups.h>
 
@@ -36,9 +37,9 @@ constexpr int kCtlFetchExt = 5, kCtlFetchShadow = 6;
 constexpr int kCtlWork = 8;      // 64-bit path counter (words 8, 9)
 constexpr int kCtlBarCount = 12, kCtlBarGen = 13, kCtlAbort = 15;
 constexpr int kCtlIter = kBatchCtlIterations;
-constexpr unsigned kBarrierSpinLimit = 1u << 26;   // x ~128 ns sleeps: ~8.6 s
 
-__device__ __forceinline__ bool grid_barrier(uint32_t* ctl) {
+// spin_limit: sleeps of ~128 ns a block waits before it raises the abort word.
+__device__ __forceinline__ bool grid_barrier(uint32_t* ctl, uint32_t spin_limit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile uint32_t* gen_p = ctl + kCtlBarGen;
@@ -53,7 +54,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* ctl) {
     } else {
       unsigned spins = 0u;
       while (*gen_p == gen && *abort_p == 0u) {
-        if (++spins > kBarrierSpinLimit) {
+        if (++spins > spin_limit) {
           atomicExch(ctl + kCtlAbort, 1u);
           break;
         }
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
   while (true) {
     if (leader) P.ctl[kCtlFetchExt] = 0u;
     phase_regen<kParity>(jobs, job_count, total, P, cur);
-    if (!grid_barrier(P.ctl)) break;
+    if (!grid_barrier(P.ctl, P.barrier_spins)) break;
 
     const uint32_t n_ext = P.ctl[cur];
     if (n_ext == 0u) break;   // no live path and no work left (same value in every block)
@@ -296,21 +297,21 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_batch(const DevJob* __restr
       const BatchExtendSource src{jobs, P.ext[cur], P.job, P.ray_o, P.ray_d, P.hit};
       persistent_traverse<BatchExtendSource, false, kStats, kWt>(src, n_ext, &P.ctl[kCtlFetchExt], stk, steps, st_e, lerr);
     }
-    if (!grid_barrier(P.ctl)) break;
+    if (!grid_barrier(P.ctl, P.barrier_spins)) break;
 
     shadow_tests += phase_shade<kParity>(jobs, P, cur, n_ext);
-    if (!grid_barrier(P.ctl)) break;
+    if (!grid_barrier(P.ctl, P.barrier_spins)) break;
 
     {
       const uint32_t n_sh = P.ctl[kCtlShadow];
       const BatchShadowSource src{jobs, P.shq, P.job, P.sh_o, P.sh_d, P.sh_c, P.rad};
       persistent_traverse<BatchShadowSource, true, kStats, kWt>(src, n_sh, &P.ctl[kCtlFetchShadow], stk, steps, st_s, lerr);
     }
-    if (!grid_barrier(P.ctl)) break;
+    if (!grid_barrier(P.ctl, P.barrier_spins)) break;
 
     phase_finish(jobs, P);
     if (leader) P.ctl[kCtlIter] += 1u;
-    if (!grid_barrier(P.ctl)) break;
+    if (!grid_barrier(P.ctl, P.barrier_spins)) break;
     cur ^= 1u;
   }
 

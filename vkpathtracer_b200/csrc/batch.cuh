@@ -41,7 +41,11 @@ struct BatchPool {
   uint32_t* fin;                  // slots whose path ended this iteration
   uint32_t* freel;                // free slots
   uint32_t* ctl;                  // control words, see batch.cu
+  uint32_t barrier_spins;         // bound of a grid-barrier wait, in ~128 ns sleeps
 };
+
+// Default bound of a grid-barrier wait: 2^26 sleeps of ~128 ns, about 8.6 s.
+constexpr uint32_t kBatchBarrierSpins = 1u << 26;
 
 struct BatchLaunch {
   int grid, block;

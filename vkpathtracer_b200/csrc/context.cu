@@ -102,6 +102,30 @@ struct AdjointState {
   }
 };
 
+// Scratch of vkptc_render_tile_noalloc, one file-scope device array per GPU
+// that loads the library, held until the process exits.  Path-state bytes per
+// path: rng (8) + seven float4 arrays (ray_o, ray_d, thr, rad, sh_o, sh_d,
+// sh_c: 112) + hit float2 (8) + three u32 queues (12); every array starts on
+// a 256-byte boundary.
+constexpr size_t kNoAllocPathBytes = 8 + 7 * 16 + 8 + 3 * 4;
+constexpr size_t kNoAllocArrays = 12;
+constexpr size_t kNoAllocBytes = VKPTC_NOALLOC_MAX_PATHS * kNoAllocPathBytes + (kNoAllocArrays + 1) * 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Makes `device` current for the scope and restores the caller's device after.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(device);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 }  // namespace
 
 struct vkptc_ctx {
@@ -110,6 +134,13 @@ struct vkptc_ctx {
   int sm_count = 148;
   cudaStream_t stream = nullptr;      // stream all work is enqueued on
   cudaStream_t own_stream = nullptr;  // the context's own stream
+  // Two events made with the context: they order kernels a call enqueues on a
+  // caller's stream against the work queued on `stream` (no allocation per call).
+  cudaEvent_t order_ev[2] = {nullptr, nullptr};
+  // Device address of g_noalloc_scratch on this context's device, looked up
+  // once when the context is created (its device current then).
+  unsigned char* noalloc_scratch = nullptr;
+  cudaError_t noalloc_lookup = cudaSuccess;
   std::string last_error;
   // per-stage timing
   StageTimer timer;
@@ -397,6 +428,41 @@ Film film_of(vkptc_ctx* c) {
   return f;
 }
 
+// Orders the kernels a call enqueues on a caller's stream `st` against the
+// context's stream: before the launch `st` waits for the work already queued
+// on the context's stream (a rebuild, scene reload or upload the kernels must
+// not overtake), and after it the context's stream waits for the launch, so
+// later work there (which may free or rewrite the arrays these kernels read)
+// cannot overtake them.  Nothing is inserted when `st` is the context's
+// stream, or while either stream is being captured: an event recorded in a
+// capture and waited on by a stream outside it would pull that stream into
+// the capture.  *active tells order_end whether to close the pair.
+int32_t order_begin(vkptc_ctx* c, cudaStream_t st, bool* active) {
+  *active = false;
+  if (st == c->stream) return VKPTC_OK;
+  cudaStreamCaptureStatus a = cudaStreamCaptureStatusNone, b = cudaStreamCaptureStatusNone;
+  VKPTC_CUDA(c, cudaStreamIsCapturing(st, &a), "stream capture status");
+  VKPTC_CUDA(c, cudaStreamIsCapturing(c->stream, &b), "stream capture status");
+  if (a != cudaStreamCaptureStatusNone || b != cudaStreamCaptureStatusNone) return VKPTC_OK;
+  VKPTC_CUDA(c, cudaEventRecord(c->order_ev[0], c->stream), "stream ordering");
+  VKPTC_CUDA(c, cudaStreamWaitEvent(st, c->order_ev[0], 0), "stream ordering");
+  *active = true;
+  return VKPTC_OK;
+}
+
+// Calls that rewrite or free device arrays the kernels read (scene and BVH
+// uploads, rebuilds, film writes) first wait for the work queued on the
+// context's stream: their synchronous copies run on the legacy stream, which
+// does not wait for the context's non-blocking stream.
+cudaError_t drain(vkptc_ctx* c) { return cudaStreamSynchronize(c->stream); }
+
+int32_t order_end(vkptc_ctx* c, cudaStream_t st, bool active) {
+  if (!active) return VKPTC_OK;
+  VKPTC_CUDA(c, cudaEventRecord(c->order_ev[1], st), "stream ordering");
+  VKPTC_CUDA(c, cudaStreamWaitEvent(c->stream, c->order_ev[1], 0), "stream ordering");
+  return VKPTC_OK;
+}
+
 int32_t check_device_error(vkptc_ctx* c) {
   uint32_t err = 0;
   VKPTC_CUDA(c, cudaMemcpyAsync(&err, c->d_err.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream), "error word");
@@ -545,6 +611,23 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
     delete c;
     return VKPTC_ALLOC_FAILED;
   }
+  for (auto& ev : c->order_ev) {
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      for (auto& e2 : c->order_ev)
+        if (e2) cudaEventDestroy(e2);
+      cudaStreamDestroy(c->stream);
+      delete c;
+      return VKPTC_INTERNAL_ERROR;
+    }
+  }
+  // The allocation-free entry point's scratch: host code cannot use the
+  // array's name as a device address, so its address on this device is looked
+  // up here, with the device current.  A failure is reported by that entry
+  // point; nothing else depends on it.
+  void* scratch = nullptr;
+  c->noalloc_lookup = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+  if (c->noalloc_lookup == cudaSuccess) c->noalloc_scratch = static_cast<unsigned char*>(scratch);
+  else cudaGetLastError();
   *out_ctx = c;
   return VKPTC_OK;
 }
@@ -557,6 +640,8 @@ int32_t vkptc_destroy(vkptc_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   cudaStream_t s = ctx->own_stream;
   for (auto& e : ctx->timer_events) cudaEventDestroy(e);
+  for (auto& e : ctx->order_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->ldr_event) cudaEventDestroy(ctx->ldr_event);
   if (ctx->h_ldr) cudaFreeHost(ctx->h_ldr);
   release_refit(ctx);
@@ -572,6 +657,7 @@ int32_t vkptc_configure(vkptc_ctx* ctx, const vkptc_render_settings* settings) {
   const uint64_t px = static_cast<uint64_t>(settings->width) * settings->height;
   if (px > (1ull << 28)) return fail(ctx, VKPTC_INVALID_ARGUMENT, "film larger than 2^28 pixels");
   cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   ctx->settings = *settings;
   VKPTC_CUDA(ctx, ctx->d_film_sum.alloc(std::max<uint64_t>(1, px)), "film alloc");
   VKPTC_CUDA(ctx, ctx->d_film_count.alloc(std::max<uint64_t>(1, px)), "film alloc");
@@ -600,6 +686,7 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   }
   ctx->adj.setup = false;
   cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   if (scene->instance_count > 0 && scene->instances == nullptr)
     return fail(ctx, VKPTC_INVALID_ARGUMENT, "instances pointer is null");
   const bool dyn = scene->instance_local != nullptr && scene->instance_transforms != nullptr;
@@ -902,6 +989,7 @@ int32_t vkptc_build_acceleration(vkptc_ctx* ctx) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   if (!ctx->has_scene) return fail(ctx, VKPTC_NOT_READY, "build_or_update_acceleration called before load_scene_snapshot");
   cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   const bool watertight = ctx->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT;
   if (watertight && ctx->config.build_mode == VKPTC_BUILD_HOST)
     return fail(ctx, VKPTC_UNSUPPORTED, "the watertight triangle test needs the device build");
@@ -936,6 +1024,7 @@ int32_t vkptc_load_bvh(vkptc_ctx* ctx, const vkptc_bvh_view* bvh) {
   if (ctx->config.triangle_test == VKPTC_TRIANGLE_WATERTIGHT)
     return fail(ctx, VKPTC_UNSUPPORTED, "the watertight triangle test needs the device build");
   cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   std::vector<BinNode> bin(bvh->node_count);
   for (uint32_t i = 0; i < bvh->node_count; ++i) {
     const uint32_t* w = bvh->nodes + 10 * static_cast<size_t>(i);
@@ -1064,6 +1153,7 @@ int32_t vkptc_update_instance_transforms(vkptc_ctx* ctx, const vkptc_instance_up
   const int32_t rc = check_updates(ctx, updates, count, ups);
   if (rc != VKPTC_OK) return rc;
   cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   VKPTC_CUDA(ctx, RefitOnDevice(*ctx->refit, ups, ctx->d_raw_local_vertices.ptr, ctx->d_raw_local_indices.ptr,
                                 ctx->d_ref_nodes, ctx->d_ref_order, ctx->ref_count, ctx->d_nodes.ptr,
                                 ctx->accel.wide_node_count, ctx->d_tris.ptr, ctx->d_tie.ptr, ctx->d_shade.ptr,
@@ -1323,6 +1413,16 @@ int32_t vkptc_render_frame(vkptc_ctx* ctx, uint32_t first_sample, uint32_t sampl
   return VKPTC_OK;
 }
 
+int32_t vkptc_device_name(vkptc_ctx* ctx, char* out, uint32_t capacity, uint32_t* sm_count) {
+  if (!ctx || !out || capacity == 0u) return VKPTC_INVALID_ARGUMENT;
+  cudaDeviceProp p{};
+  VKPTC_CUDA(ctx, cudaGetDeviceProperties(&p, ctx->device), "device properties");
+  std::strncpy(out, p.name, capacity - 1u);
+  out[capacity - 1u] = '\0';
+  if (sm_count) *sm_count = static_cast<uint32_t>(p.multiProcessorCount);
+  return VKPTC_OK;
+}
+
 int32_t vkptc_set_stream(vkptc_ctx* ctx, void* stream) {
   if (!ctx) return VKPTC_INVALID_ARGUMENT;
   ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
@@ -1380,6 +1480,7 @@ int32_t vkptc_write_film(vkptc_ctx* ctx, const float* sum_rgb, const uint32_t* c
   if (!ctx->configured) return fail(ctx, VKPTC_NOT_READY, "replace_film_history called before configure");
   if (!sum_rgb || !count) return fail(ctx, VKPTC_INVALID_ARGUMENT, "film arrays are null");
   cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   const size_t px = static_cast<size_t>(ctx->settings.width) * ctx->settings.height;
   std::vector<float4> tmp(px);
   for (size_t i = 0; i < px; ++i) tmp[i] = make_float4(sum_rgb[3 * i], sum_rgb[3 * i + 1], sum_rgb[3 * i + 2], 0.0f);
@@ -1574,11 +1675,14 @@ int32_t vkptc_trace_rays_device(vkptc_ctx* ctx, const float* d_rays, const float
   int32_t rc = launch_shape(ctx, st, ls);
   if (rc != VKPTC_OK) return rc;
   if (ray_count > 0xFFFFFFF0ull) return fail(ctx, VKPTC_INVALID_ARGUMENT, "at most 2^32 - 16 rays per call");
+  bool ordered = false;
+  rc = order_begin(ctx, st, &ordered);
+  if (rc != VKPTC_OK) return rc;
   VKPTC_CUDA(ctx, LaunchTraceRays(dev_scene(ctx), d_rays, d_tmax, ray_count, mode == VKPTC_QUERY_ANY, d_prim_out,
                                   d_t_out, ls, ctx->config.collect_stats ? ctx->d_ctr.ptr : nullptr, ctx->d_err.ptr,
                                   ctx->d_fetch.ptr),
              "trace launch");
-  return VKPTC_OK;
+  return order_end(ctx, st, ordered);
 }
 
 int32_t vkptc_trace_rays(vkptc_ctx* ctx, const float* rays, const float* tmax, uint64_t ray_count, uint32_t mode,
@@ -1883,6 +1987,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   P.fin = b->p_fin.ptr;
   P.freel = b->p_free.ptr;
   P.ctl = b->p_ctl.ptr;
+  P.barrier_spins = t.barrier_spins ? t.barrier_spins : kBatchBarrierSpins;
   }
 
   // ---- the run: film clear, pool reset, the pool iterations, in-order accumulation
@@ -1891,6 +1996,8 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
     int32_t rc = batch_clear_films(b);
     if (rc != VKPTC_OK) return rc;
     VKPTC_BCUDA(b, cudaMemsetAsync(b->d_ctr.ptr, 0, sizeof(DevCounters), b->stream), "counter clear");
+    // the error word of the previous run (a barrier timeout) must not outlive it
+    VKPTC_BCUDA(b, cudaMemsetAsync(b->d_err.ptr, 0, sizeof(uint32_t), b->stream), "error word clear");
     if (loop) VKPTC_BCUDA(b, LaunchBatchLoopInit(LP, b->stream), "pool init");
     else VKPTC_BCUDA(b, LaunchBatchInit(P, b->stream), "pool init");
     return VKPTC_OK;
@@ -1946,7 +2053,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   if (t.use_graph) {
     const std::string key = std::string(loop ? "loop/" : "persistent/") + std::to_string(cap) + "/" +
                             std::to_string(bl.block) + "/" + std::to_string(bl.smem_entries) +
-                            "/o" + std::to_string(bl.occupancy) +
+                            "/o" + std::to_string(bl.occupancy) + "/b" + std::to_string(t.barrier_spins) +
                             "/" + std::to_string(bl.steps) + "/" + std::to_string(t.sample_limit) + "/" +
                             std::to_string(b->jobs.size()) + "/" +
                             std::to_string(reinterpret_cast<uintptr_t>(b->staging.ptr)) + "/" +
@@ -2184,32 +2291,6 @@ const char* vkptc_batch_last_error(vkptc_batch* b) {
 // ============================================================ allocation-free
 namespace {
 
-// Path-state bytes per path: rng (8) + seven float4 arrays (ray_o, ray_d,
-// thr, rad, sh_o, sh_d, sh_c: 112) + hit float2 (8) + three u32 queues (12).
-constexpr size_t kNoAllocPathBytes = 8 + 7 * 16 + 8 + 3 * 4;
-constexpr size_t kNoAllocArrays = 12;   // each array starts on a 256-byte boundary
-constexpr size_t kNoAllocBytes = VKPTC_NOALLOC_MAX_PATHS * kNoAllocPathBytes + (kNoAllocArrays + 1) * 256;
-
-// The scratch of vkptc_render_tile_noalloc: one per device, for the whole process.
-static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
-
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_base[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on `device` (which must be current).
-cudaError_t noalloc_base(int device, unsigned char** out) {
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_base[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_base[device] = p;
-  }
-  *out = static_cast<unsigned char*>(g_noalloc_base[device]);
-  return cudaSuccess;
-}
-
 template <typename T>
 T* carve(unsigned char*& cursor, size_t count) {
   T* p = reinterpret_cast<T*>(cursor);
@@ -2239,10 +2320,13 @@ extern "C" int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* t
                 "tile of " + std::to_string(paths) + " pixels exceeds the allocation-free limit of " +
                     std::to_string(VKPTC_NOALLOC_MAX_PATHS) + " paths per call; split it into smaller tiles");
   }
-  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) return fail(ctx, VKPTC_UNSUPPORTED, "device ordinal above 63");
-  cudaSetDevice(ctx->device);
-  unsigned char* base = nullptr;
-  VKPTC_CUDA(ctx, noalloc_base(ctx->device, &base), "cudaGetSymbolAddress of the allocation-free scratch");
+  if (!ctx->noalloc_scratch) {
+    return fail(ctx, VKPTC_INTERNAL_ERROR, std::string("the allocation-free scratch has no device address: "
+                                                       "cudaGetSymbolAddress failed when the context was created: ") +
+                                               cudaGetErrorString(ctx->noalloc_lookup));
+  }
+  const DeviceGuard guard(ctx->device);   // the caller's current device is restored on return
+  unsigned char* const base = ctx->noalloc_scratch;
   const size_t n = VKPTC_NOALLOC_MAX_PATHS;
   unsigned char* cur = base;
   WaveState w{};
@@ -2262,8 +2346,11 @@ extern "C" int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* t
   w.capacity = VKPTC_NOALLOC_MAX_PATHS;
   if (static_cast<size_t>(cur - base) > kNoAllocBytes) return fail(ctx, VKPTC_INTERNAL_ERROR, "scratch layout overflow");
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  // The whole traversal stack in shared memory (no spill buffer, which would
+  // be an allocation): a BVH whose worst-case stack does not fit is refused
+  // with VKPTC_UNSUPPORTED by launch_shape.
   LaunchShape ls;
-  const int32_t rc = launch_shape(ctx, st, ls, /*allow_spill=*/false);
+  int32_t rc = launch_shape(ctx, st, ls, /*allow_spill=*/false);
   if (rc != VKPTC_OK) return rc;
   Film film{};
   film.sum = reinterpret_cast<float4*>(d_film_sum);
@@ -2272,9 +2359,14 @@ extern "C" int32_t vkptc_render_tile_noalloc(vkptc_ctx* ctx, const vkptc_tile* t
   film.width = ctx->settings.width;
   film.height = ctx->settings.height;
   const WaveTile wt{x0, y0, x1 - x0, y1 - y0, tile->sample_index, 1u};
+  bool ordered = false;
+  rc = order_begin(ctx, st, &ordered);
+  if (rc != VKPTC_OK) return rc;
   VKPTC_CUDA(ctx, LaunchWave(dev_scene(ctx), dev_settings(ctx, frame), w, wt, film, ctx->config.math_mode == 0u,
                              ctx->config.collect_stats != 0u, ls, ctx->d_ctr.ptr, ctx->d_err.ptr, nullptr),
              "allocation-free wave launch");
+  rc = order_end(ctx, st, ordered);
+  if (rc != VKPTC_OK) return rc;
   ctx->last_error.clear();
   return VKPTC_OK;
 }

@@ -3,6 +3,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
 #include <vector>
 
 #include "pathtracer/PathTracerObservability.h"
@@ -577,6 +581,85 @@ void CudaPathTracer::shutdown() {
   if (m_ctx) vkptc_shutdown(m_ctx);
   m_film = pt::FilmBuffer{};
   m_last_error.clear();
+}
+
+struct BenchmarkAccess {
+  static vkptc_ctx* ctx(const CudaPathTracer& t) { return t.m_ctx; }
+  static const pt::RenderSettings& settings(const CudaPathTracer& t) { return t.m_settings; }
+};
+
+namespace {
+
+std::string fmt(double v) {
+  char b[64];
+  std::snprintf(b, sizeof(b), "%.6g", v);
+  return b;
+}
+
+}  // namespace
+
+void FillBenchmarkResult(const CudaPathTracer& tracer, const CudaBenchmarkInputs& in,
+                         vkpt::benchmark::BenchmarkResult& result) {
+  vkptc_ctx* ctx = BenchmarkAccess::ctx(tracer);
+  const pt::RenderSettings& st = BenchmarkAccess::settings(tracer);
+  result.backend = "cuda";
+  result.renderer_path = in.renderer_path ? in.renderer_path : kBackend;
+  result.device_info.backend = result.backend;
+  result.device_info.renderer_path = result.renderer_path;
+  char name[256] = {0};
+  if (ctx && vkptc_device_name(ctx, name, sizeof(name), nullptr) == VKPTC_OK) result.device_info.gpu_name = name;
+  result.resolution = {st.width, st.height};
+  result.spp = st.spp;
+  result.seed = st.seed;
+  result.max_depth = st.max_depth;
+  result.timing.render_ms = in.render_ms;
+  result.timing.build_ms = in.build_ms;
+  result.timing.total_ms = in.total_ms > 0.0 ? in.total_ms : in.build_ms + in.render_ms;
+  const pt::SampleCounters c = tracer.read_counters();
+  const double render_s = in.render_ms / 1e3;
+  result.diagnostics.push_back(std::string("renderer=") + result.renderer_path);
+  if (render_s > 0.0) {
+    result.throughput.paths_per_sec = static_cast<double>(c.rays) / render_s;
+    result.throughput.samples_per_sec = static_cast<double>(c.samples) / render_s;
+    result.diagnostics.push_back("paths_per_sec_camera=" + fmt(static_cast<double>(c.samples) / render_s));
+    result.diagnostics.push_back("mrays_per_sec=" + fmt(static_cast<double>(c.rays + c.shadow_tests) / render_s / 1e6));
+  }
+  uint64_t tr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (ctx && render_s > 0.0 && in.peak_bandwidth_gbs > 0.0 && vkptc_read_traversal_stats(ctx, tr) == VKPTC_OK) {
+    // extension and shadow queries: rays, node visits, leaf visits, triangle tests
+    const double bytes = 128.0 * static_cast<double>(tr[1] + tr[5]) + 48.0 * static_cast<double>(tr[3] + tr[7]) +
+                         32.0 * static_cast<double>(tr[0] + tr[4]);
+    result.diagnostics.push_back("roofline_fraction=" + fmt(bytes / render_s / 1e9 / in.peak_bandwidth_gbs));
+  } else {
+    result.diagnostics.push_back("roofline_fraction=n/a");
+  }
+  if (in.reference) {
+    const auto& a = in.reference->raw();
+    const auto& ac = in.reference->sample_counts();
+    const auto& b = tracer.film().raw();
+    const auto& bc = tracer.film().sample_counts();
+    const size_t n = std::min(a.size(), b.size());
+    double se = 0.0, mean = 0.0;
+    size_t same = 0, fails = 0;
+    for (size_t i = 0; i < n; ++i) {
+      const double na = std::max(1u, ac[i]), nb = std::max(1u, bc[i]);
+      const float pa[3] = {a[i].x, a[i].y, a[i].z}, pb[3] = {b[i].x, b[i].y, b[i].z};
+      if (std::memcmp(pa, pb, sizeof(pa)) == 0 && ac[i] == bc[i]) ++same;
+      for (int ch = 0; ch < 3; ++ch) {
+        const double ma = pa[ch] / na, d = pb[ch] / nb - ma;
+        se += d * d;
+        mean += ma;
+        if (in.reference_m2 && in.reference_m2->size() >= 3 * n) {
+          const double var = std::max(0.0, ((*in.reference_m2)[3 * i + ch] - pa[ch] * ma) / std::max(1.0, na - 1.0));
+          if (std::fabs(d) > 3.0 * std::sqrt(var / na) + 1e-6 * (1.0 + std::fabs(ma))) ++fails;
+        }
+      }
+    }
+    const double m = mean / std::max<double>(1.0, 3.0 * n);
+    result.diagnostics.push_back("rmse=" + fmt(std::sqrt(se / std::max<double>(1.0, 3.0 * n)) / std::max(m, 1e-12)));
+    if (in.reference_m2) result.diagnostics.push_back("sigma3_fail_frac=" + fmt(fails / std::max<double>(1.0, 3.0 * n)));
+    result.diagnostics.push_back("bit_identical_frac=" + fmt(static_cast<double>(same) / std::max<size_t>(1, n)));
+  }
 }
 
 }  // namespace vkpt::gpu::cuda

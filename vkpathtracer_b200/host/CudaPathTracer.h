@@ -12,6 +12,7 @@
 #include <stop_token>
 #include <string>
 
+#include "benchmark/BenchmarkSchema.h"
 #include "pathtracer/PathTracer.h"
 
 struct vkptc_ctx;
@@ -89,6 +90,37 @@ class CudaPathTracer final : public vkpt::pathtracer::IPathTracer {
   // camera-adjusted film resolve settings after a camera update.
   vkpt::pathtracer::RTCameraState m_camera{};
   vkpt::pathtracer::PathTracerSceneSnapshot m_camera_scene{};
+
+  friend struct BenchmarkAccess;
 };
+
+// What ptbench's `run` command (src/benchmark/BenchmarkRuntime.cpp:598-830) fills
+// for a backend after its timed render loop, for the cuda backend.
+struct CudaBenchmarkInputs {
+  double render_ms = 0.0;          // the timed render loop (BenchmarkRuntime.cpp:680-695)
+  double build_ms = 0.0;           // scene upload + acceleration build
+  double total_ms = 0.0;
+  // Roofline denominator of the traversal (the measured HBM copy bandwidth of
+  // the device, GB/s); with collect_stats on, roofline_fraction = (128 B per
+  // wide-node visit + 48 B per triangle test + 32 B per ray) / render time / it.
+  double peak_bandwidth_gbs = 0.0;
+  // Optional CPU reference film of the same scene, settings and seed, for
+  // rmse= (relative RMSE of the per-pixel means) and bit_identical_frac=.
+  const vkpt::pathtracer::FilmBuffer* reference = nullptr;
+  // Optional, with `reference`: per pixel and channel the sum of the squared
+  // per-sample radiance of the reference (3 floats per pixel), for
+  // sigma3_fail_frac= (channels whose mean differs from the reference's by more
+  // than 3 standard errors of the reference's own samples).
+  const std::vector<float>* reference_m2 = nullptr;
+  const char* renderer_path = "cuda-wavefront";   // or "cuda-persistent" for the batched renderer
+};
+
+// Fills backend, renderer_path, device_info, timing, throughput (paths_per_sec
+// in ptbench's definition, counters.rays / render time, BenchmarkRuntime.cpp:762)
+// and appends the backend's diagnostics:
+//   renderer=, paths_per_sec_camera=, mrays_per_sec=, roofline_fraction=,
+//   rmse=, sigma3_fail_frac=, bit_identical_frac= (the last three with a reference).
+void FillBenchmarkResult(const CudaPathTracer& tracer, const CudaBenchmarkInputs& in,
+                         vkpt::benchmark::BenchmarkResult& result);
 
 }  // namespace vkpt::gpu::cuda

@@ -139,7 +139,7 @@ class AccelInfo(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("pool_paths", ctypes.c_uint32), ("block_size", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32),
                 ("steps", ctypes.c_uint32), ("sample_limit", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
-                ("occupancy", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("occupancy", ctypes.c_uint32), ("barrier_spins", ctypes.c_uint32)]
 
 
 class BatchStats(ctypes.Structure):
@@ -204,6 +204,7 @@ SIGNATURES = {
     "vkptc_update_scene_delta": (I32, [P, ctypes.POINTER(SceneDelta)]),
     "vkptc_request_ldr_readback": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_poll_ldr_readback": (I32, [P, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
+    "vkptc_device_name": (I32, [P, ctypes.c_char_p, U32, ctypes.POINTER(U32)]),
     "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),
     "vkptc_reset": (I32, [P]),
     "vkptc_shutdown": (I32, [P]),

@@ -761,7 +761,10 @@ def batch_jobs(count: int = 64, seed: int = 5, max_triangles: int = 500_000, max
                min_triangles: int = 1_000, min_side: int = 128) -> List[Job]:
     """Uneven render jobs: triangle count log-uniform in [min,max], square side
     log-uniform in [min_side,max_side], spp in {4,8,16,32,64}, depth in {4,8,16},
-    the sphere-field material mix; each job's seeds derive from the master seed."""
+    the sphere-field material mix; each job's seeds derive from the master seed.
+    No firefly clamp (the batched workload takes only the full frame's
+    material mix, and the reference has no clamp), so every job renders what
+    the reference's CPU tracer renders for the same scene and settings."""
     st = Stream(seed)
     jobs = []
     for k in range(count):
@@ -780,7 +783,7 @@ def batch_jobs(count: int = 64, seed: int = 5, max_triangles: int = 500_000, max
         scene = sphere_field(grid, n_lat, n_lon, job_seed % 100000 + 7, n_lights=min(16, max(1, grid)),
                              light_size=max(1.0, 0.1 * grid * 3.0), light_height=max(4.0, 0.25 * grid * 3.0))
         settings = RenderSettings(width=side, height=side, spp=spp, max_depth=depth, seed=job_seed,
-                                  enable_nee=True, enable_mis=True, firefly_clamp=10.0)
+                                  enable_nee=True, enable_mis=True)
         jobs.append(Job(scene, settings, int(tris)))
     return jobs
 

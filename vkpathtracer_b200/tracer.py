@@ -564,8 +564,10 @@ class BatchRenderer:
         return int(jid.value)
 
     def run(self, mode: str = "persistent", pool_paths: int = 0, block_size: int = 0, stack_depth: int = 0,
-            steps: int = 0, sample_limit: int = 0, use_graph: bool = True, occupancy: int = 0) -> dict:
-        t = native.BatchTuning(pool_paths, block_size, stack_depth, steps, sample_limit, int(use_graph), occupancy)
+            steps: int = 0, sample_limit: int = 0, use_graph: bool = True, occupancy: int = 0,
+            barrier_spins: int = 0) -> dict:
+        t = native.BatchTuning(pool_paths, block_size, stack_depth, steps, sample_limit, int(use_graph), occupancy,
+                               barrier_spins)
         modes = {"plain": native.BATCH_PLAIN, "persistent": native.BATCH_PERSISTENT, "loop": native.BATCH_LOOP}
         if mode not in modes:
             raise ValueError(f"mode must be one of {sorted(modes)}")
