@@ -46,6 +46,23 @@ PATH_STATE_BYTES = 2 * 64                            # path state read + written
 TRAFFIC_BYTES_PER_EXT_RAY = 62789632 / 1048576
 
 
+def l2_roofline(device, achieved_gbs):
+    """The L2 side of the traversal roofline: the device's L2 read bandwidth,
+    measured here by the library's own probe kernel (vkptc_measure_read_bandwidth:
+    16-byte loads cached in L2 only, 64 passes over a 48 MiB buffer, well under
+    the 126 MB L2), and the traversal stage's algorithmic bytes per second as a
+    fraction of it.  The probe's figure is measured by this function, apart
+    from the HBM peak read from MEASURED_PEAKS.json."""
+    from vkpathtracer_b200.tracer import CudaPathTracer
+    with CudaPathTracer(device=device) as t:
+        l2 = max(t.read_bandwidth(48 << 20, 64) for _ in range(3))
+    return {"l2_peak": l2, "l2_peak_kind": "measured here: L2-resident read probe (48 MiB x 64, ld.global.cg)",
+            "l2_frac": achieved_gbs / l2,
+            "bound_note": "the stage's DRAM traffic is a few percent of its algorithmic bytes (upper BVH levels "
+                          "and small scenes stay in L2/L1); l2_frac says how close the node and triangle "
+                          "stream is to the L2 bandwidth"}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -625,6 +642,8 @@ def profile_run(args, local):
     cache = autotune._load_cache()
     cached = next((v for k, v in cache.items() if k.startswith(prefix) and k.endswith("/" + key)), {})
     cfg = cached.get("per_mode", {}).get(args.profile_run, {})
+    if args.tuning:
+        cfg = json.loads(args.tuning)
     tuning = {k: cfg[k] for k in ("pool_paths", "block_size", "stack_depth", "steps", "occupancy") if k in cfg}
     with BatchRenderer(device=local, bvh="sah") as b:
         for j in jobs:
@@ -728,7 +747,7 @@ def run_ours(args, world, rank, local):
     tune = autotune.tune_batch(b, key, use_cache=not args.retune)
     keys = ("pool_paths", "block_size", "stack_depth", "steps", "occupancy")
     mode = tune["mode"]
-    tuning = {k: tune[k] for k in keys}
+    tuning = {k: tune.get(k, 0) for k in keys}
 
     # ---------------------------------------------------------- plain mode (one frame per launch)
     b.run("plain")   # warm-up: the first run allocates every job's wave buffers between its launches
@@ -774,7 +793,7 @@ def run_ours(args, world, rank, local):
     # both drivers, each with its own best tuning, on the same jobs
     drivers = {}
     for m, cfg in tune.get("per_mode", {}).items():
-        mt = {k: cfg[k] for k in keys}
+        mt = {k: cfg.get(k, 0) for k in keys}
         b.run(m, **mt)
         ms = min(b.run(m, **mt)["device_ms"] for _ in range(2))
         drivers[m] = {"paths_per_s": total_paths / (ms / 1e3), "tuning": mt}
@@ -826,6 +845,7 @@ def run_ours(args, world, rank, local):
                     "shadow_stage_achieved_gbs": (NODE_BYTES * ss["shadow_nodes"] + TRI_BYTES * ss["shadow_tris"]
                                                   + RAY_IO_BYTES * ss["shadow_queries"]) / (stage["shadow"] / 1e3) / 1e9,
                     "nodes_per_ray": nodes / max(1, rays), "tris_per_ray": tris / max(1, rays)}
+            roof.update(l2_roofline(local, achieved))
         else:
             alg = NODE_BYTES * nodes + TRI_BYTES * tris + RAY_IO_BYTES * rays + PATH_STATE_BYTES * ss["segments"] \
                 + 16 * ss["paths"]
@@ -903,6 +923,9 @@ def main():
     ap.add_argument("--no-watertight", action="store_true")
     ap.add_argument("--profile-run", choices=["loop", "persistent"], default=None,
                     help="profiling aid: render the job set twice with one driver, no CUDA graph, and exit")
+    ap.add_argument("--tuning", default="",
+                    help="profiling aid: JSON launch parameters for --profile-run (pool_paths, block_size, "
+                         "stack_depth, steps, occupancy) instead of the autotuner's cache")
     ap.add_argument("--profile-build", action="store_true",
                     help="profiling aid: build the 2M-triangle sphere grid twice per traversal tree and exit")
     ap.add_argument("--profile-rays", choices=["mt", "watertight"], default=None,

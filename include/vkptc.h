@@ -70,7 +70,9 @@ typedef struct vkptc_config {
   uint32_t collect_stats;    /* 1 = count node/leaf/triangle visits (device counters) */
   uint32_t wave_paths;       /* paths per wavefront wave (0 = 4 Mi) */
   uint32_t stage_timing;     /* 1 = CUDA-event timing of every stage launch */
-  uint32_t steps;            /* traversal steps between warp refills (0 = 4) */
+  uint32_t steps;            /* traversal steps between warp refills in the low 16 bits (0 = 4); the
+                                high 16 bits, when non-zero, refill a warp as soon as that many of its
+                                lanes are idle (at most 32), checked after every step */
   uint32_t bvh_mode;         /* traversal tree: VKPTC_BVH_REFERENCE (the reference builder's tree,
                                 flattened) or VKPTC_BVH_SAH (binned SAH); hit ids are the
                                 reference's in both (ties/parallel rule use the reference tree) */
@@ -445,6 +447,13 @@ int32_t vkptc_read_traversal_stats(vkptc_ctx* ctx, uint64_t* out);
 int32_t vkptc_get_status(vkptc_ctx* ctx, vkptc_tracer_status* out);
 /* Last error message of this context (empty when none); valid until the next call. */
 const char* vkptc_last_error(vkptc_ctx* ctx);
+/* Extension (no reference counterpart): read bandwidth of the context's device, for the
+ * roofline of the traversal stages.  Streams `reps` times through a zeroed device buffer of
+ * `bytes` (a multiple of 16) with 16-byte loads cached in L2 only, timed with CUDA events on
+ * the context's stream after one untimed pass: a buffer well under the L2 size (126 MB on
+ * B200) gives the L2 bandwidth, one far above it the HBM read bandwidth.  *gbs receives
+ * bytes * reps / time in GB/s.  Allocates (and frees) the buffer itself. */
+int32_t vkptc_measure_read_bandwidth(vkptc_ctx* ctx, uint64_t bytes, uint32_t reps, double* gbs);
 /* The device a context renders on: its name (cudaDeviceProp::name, NUL-terminated, cut to
  * capacity) for BenchmarkResult.device_info.gpu_name (src/benchmark/BenchmarkSchema.h:80-85),
  * and optionally its SM count. */
@@ -491,7 +500,9 @@ typedef struct vkptc_batch_tuning {
   uint32_t pool_paths;       /* path slots of the persistent launch ("queue capacity"); 0 = default */
   uint32_t block_size;       /* 0 = default */
   uint32_t stack_depth;      /* traversal stack entries in shared memory; 0 = default */
-  uint32_t steps;            /* traversal steps between warp refills; 0 = default */
+  uint32_t steps;            /* traversal steps between warp refills (low 16 bits; 0 = default) and
+                                an optional refill threshold in idle lanes (high 16 bits), as
+                                vkptc_config.steps */
   uint32_t sample_limit;     /* render at most this many samples per job (0 = each job's spp) */
   uint32_t use_graph;        /* persistent/loop modes: 1 = capture once, replay the CUDA graph
                                 (loop mode without a graph runs one host round trip per iteration) */

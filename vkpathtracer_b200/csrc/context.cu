@@ -337,6 +337,13 @@ constexpr int kDefaultSteps = 4;
 
 int32_t ensure_stack_smem(vkptc_ctx* c, const LaunchShape& ls);
 
+// The traversal's step word: low 16 bits the steps between refills (0: the
+// default), high 16 bits the refill threshold in idle lanes (at most 32).
+int steps_word(uint32_t v, int default_steps) {
+  const uint32_t low = v & 0xFFFFu, refill = std::min<uint32_t>(32u, v >> 16);
+  return static_cast<int>((low ? low : static_cast<uint32_t>(default_steps)) | (refill << 16));
+}
+
 // Block size, stack split (shared-memory entries + global spill), steps between
 // warp refills, and a grid of (resident blocks per SM) x SMs: the traversal
 // kernels are persistent.  allow_spill = false keeps the whole stack in
@@ -346,7 +353,7 @@ int32_t launch_shape(vkptc_ctx* c, cudaStream_t stream, LaunchShape& ls, bool al
   ls.stack_cap = stack_cap(c);
   const int asked = c->config.stack_depth ? static_cast<int>(c->config.stack_depth) : kDefaultSmemEntries;
   ls.smem_entries = allow_spill ? std::min(ls.stack_cap, std::max(1, asked)) : ls.stack_cap;
-  ls.steps = c->config.steps ? static_cast<int>(c->config.steps) : kDefaultSteps;
+  ls.steps = steps_word(c->config.steps, kDefaultSteps);
   ls.stream = stream;
   ls.spill = nullptr;
   const int32_t rc = ensure_stack_smem(c, ls);
@@ -1413,6 +1420,36 @@ int32_t vkptc_render_frame(vkptc_ctx* ctx, uint32_t first_sample, uint32_t sampl
   return VKPTC_OK;
 }
 
+int32_t vkptc_measure_read_bandwidth(vkptc_ctx* ctx, uint64_t bytes, uint32_t reps, double* gbs) {
+  if (!ctx || !gbs) return VKPTC_INVALID_ARGUMENT;
+  if (bytes < 16u || (bytes & 15u) != 0u || reps == 0u) {
+    return fail(ctx, VKPTC_INVALID_ARGUMENT, "bandwidth probe: bytes must be a non-zero multiple of 16, reps >= 1");
+  }
+  cudaSetDevice(ctx->device);
+  VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
+  DevBuf<float4> buf;
+  DevBuf<float> sink;
+  VKPTC_CUDA(ctx, buf.alloc(bytes / 16u), "bandwidth probe buffer");
+  VKPTC_CUDA(ctx, sink.alloc(1), "bandwidth probe buffer");
+  VKPTC_CUDA(ctx, cudaMemsetAsync(buf.ptr, 0, bytes, ctx->stream), "bandwidth probe clear");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  VKPTC_CUDA(ctx, cudaEventCreate(&e0), "event");
+  VKPTC_CUDA(ctx, cudaEventCreate(&e1), "event");
+  const int grid = ctx->sm_count * 8;   // 8 blocks of 256 threads per SM
+  cudaError_t e = LaunchReadProbe(buf.ptr, bytes, 1u, grid, sink.ptr, ctx->stream);   // warm-up pass
+  if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+  if (e == cudaSuccess) e = LaunchReadProbe(buf.ptr, bytes, reps, grid, sink.ptr, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  VKPTC_CUDA(ctx, e, "bandwidth probe");
+  *gbs = ms > 0.0f ? static_cast<double>(bytes) * reps / (ms / 1e3) / 1e9 : 0.0;
+  return VKPTC_OK;
+}
+
 int32_t vkptc_device_name(vkptc_ctx* ctx, char* out, uint32_t capacity, uint32_t* sm_count) {
   if (!ctx || !out || capacity == 0u) return VKPTC_INVALID_ARGUMENT;
   cudaDeviceProp p{};
@@ -1872,7 +1909,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   bl.block = t.block_size ? static_cast<int>(std::min(256u, std::max(32u, (t.block_size + 31u) / 32u * 32u))) : 128;
   bl.stack_cap = stack_cap;
   bl.smem_entries = std::min(stack_cap, t.stack_depth ? static_cast<int>(t.stack_depth) : kDefaultSmemEntries);
-  bl.steps = t.steps ? static_cast<int>(t.steps) : kDefaultSteps;
+  bl.steps = steps_word(t.steps, kDefaultSteps);
   bl.stream = b->stream;
   bl.parity = parity;
   bl.stats = b->config.collect_stats != 0u;

@@ -116,4 +116,11 @@ struct LdrResolve {
 cudaError_t LaunchResolveLdr(const Film& film, const LdrResolve& rs, bool parity, uint8_t* rgba_out,
                              cudaStream_t stream);
 
+// Bandwidth probe: `reps` passes of 16-byte reads over `bytes` of `buf`
+// (a multiple of 16), grid-strided, cached in L2 only (ld.global.cg), so a
+// buffer well under the L2 size measures L2 bandwidth and one far above it
+// HBM read bandwidth.  sink receives nothing unless the sum is impossible.
+cudaError_t LaunchReadProbe(const float4* buf, size_t bytes, uint32_t reps, int grid, float* sink,
+                            cudaStream_t stream);
+
 }  // namespace vkptc

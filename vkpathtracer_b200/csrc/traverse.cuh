@@ -30,6 +30,17 @@ namespace vkptc {
 
 #define kInf __int_as_float(0x7f800000)
 
+// 1: the persistent traversal steps one node or one triangle at a time
+// (lane_step_tri); 0: one node or one whole leaf (lane_step).
+#ifndef VKPTC_TRI_STEP
+#define VKPTC_TRI_STEP 1
+#endif
+#if VKPTC_TRI_STEP
+#define VKPTC_LANE_STEP lane_step_tri<kAny, kStats, kWt>
+#else
+#define VKPTC_LANE_STEP lane_step<kAny, kStats, kWt>
+#endif
+
 struct RayPrep {
   float ox, oy, oz, dx, dy, dz;
   float ix, iy, iz;      // 1/d (0 on axes the node test treats with the inside rule)
@@ -524,6 +535,7 @@ struct LaneState {
   uint32_t leaf, lane;
   int32_t ref;
   int sp;
+  int32_t tri, tri_end;   // lane_step_tri: triangle records of the leaf being tested, [tri, tri_end)
 };
 
 template <bool kWt = false>
@@ -535,6 +547,7 @@ __device__ __forceinline__ void lane_begin(LaneState& L, V3 o, V3 d, float tmax,
   L.leaf = L.lane = 0u;
   L.ref = 0;
   L.sp = 0;
+  L.tri = L.tri_end = 0;
 }
 
 // Returns true when the query has finished.
@@ -622,15 +635,121 @@ __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk
   return true;
 }
 
+// The same traversal with a step of one wide node OR one triangle: a leaf
+// reached by a step is tested one triangle per later step.  A warp's lanes
+// diverge between node and leaf work at every step; with whole leaves per
+// step a lane in a leaf holds the warp for up to eight triangle tests while
+// its neighbours wait, with single triangles the two branches cost about the
+// same.  Triangles are tested in the same order with the same rules, so hits
+// (and ties) are identical to lane_step's.  Returns true when the query has
+// finished.
+template <bool kAny, bool kStats, bool kWt = false>
+__device__ __forceinline__ void lane_enter(LaneState& L, int32_t ref, TraceStats& st) {
+  L.ref = ref;
+  if (ref < 0) {
+    L.tri = leaf_first(ref);
+    L.tri_end = L.tri + leaf_count(ref);
+    if (kStats) {
+      ++st.leaves;
+      st.tris += static_cast<uint32_t>(L.tri_end - L.tri);
+    }
+  }
+}
+
+template <bool kAny, bool kStats, bool kWt = false>
+__device__ __forceinline__ bool lane_step_tri(LaneState& L, const TwoLevelStack& stk, TraceStats& st,
+                                              uint32_t& err) {
+  if (L.tri < L.tri_end) {
+    const float4* tp = L.g.tris + 3 * L.tri;
+    ++L.tri;
+    const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+    const float th = tri_test<kWt>(a, b, cc, L.r, L.w);
+    if (th > kEps && (L.r.leaf_par == 0u || leaf_rule_ok(L.g.tie, __float_as_uint(cc.z), L.r))) {
+      if (kAny) {
+        if (th < L.t) {
+          L.prim = 1u;
+          return true;
+        }
+      } else if (th < L.t) {
+        L.t = th;
+        L.prim = __float_as_uint(cc.y);
+        L.leaf = __float_as_uint(cc.z);
+        L.lane = __float_as_uint(cc.w);
+      } else if (th == L.t &&
+                 tie_candidate_wins(L.g.tie, L.r, L.leaf, L.lane, __float_as_uint(cc.z), __float_as_uint(cc.w))) {
+        L.prim = __float_as_uint(cc.y);
+        L.leaf = __float_as_uint(cc.z);
+        L.lane = __float_as_uint(cc.w);
+      }
+    }
+    if (L.tri < L.tri_end) return false;
+  } else {
+    const float4* np = L.g.nodes + 8 * L.ref;
+    const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+    const int n = __ldg(reinterpret_cast<const int*>(np + 7));
+    if (kStats) ++st.nodes;
+    float t[4];
+    int32_t c[4] = {ch.x, ch.y, ch.z, ch.w};
+    const bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, L.r, L.t, t[0]);
+    const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, L.r, L.t, t[1]) && n > 1;
+    const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, L.r, L.t, t[2]) && n > 2;
+    const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, L.r, L.t, t[3]) && n > 3;
+    t[0] = h0 ? t[0] : kInf;
+    t[1] = h1 ? t[1] : kInf;
+    t[2] = h2 ? t[2] : kInf;
+    t[3] = h3 ? t[3] : kInf;
+    const int hits = int(h0) + int(h1) + int(h2) + int(h3);
+#define VKPTC_CSWAP(i, j)                            \
+  if (t[j] < t[i]) {                                 \
+    const float tt = t[i]; t[i] = t[j]; t[j] = tt;   \
+    const int32_t cc = c[i]; c[i] = c[j]; c[j] = cc; \
+  }
+    VKPTC_CSWAP(0, 1) VKPTC_CSWAP(2, 3) VKPTC_CSWAP(0, 2) VKPTC_CSWAP(1, 3) VKPTC_CSWAP(1, 2)
+#undef VKPTC_CSWAP
+    if (hits > 0) {
+#pragma unroll
+      for (int k = 3; k >= 1; --k) {
+        if (k < hits) {
+          if (L.sp < stk.total) {
+            stk.put(L.sp, make_int2(c[k], __float_as_int(t[k])));
+            ++L.sp;
+          } else {
+            err = 1u;
+          }
+        }
+      }
+      lane_enter<kAny, kStats, kWt>(L, c[0], st);
+      return false;
+    }
+  }
+  while (L.sp > 0) {
+    --L.sp;
+    const int2 e = stk.get(L.sp);
+    if (kAny || __int_as_float(e.y) <= L.t) {
+      lane_enter<kAny, kStats, kWt>(L, e.x, st);
+      return false;
+    }
+  }
+  return true;
+}
+
 // Persistent traversal over `n` queries supplied by Src:
 //   Src::load(j, o, d, tmax) and Src::finish(j, t, prim) (any-hit: prim = occluded).
 // Each warp keeps its lanes busy: whenever lanes are idle it claims that many
-// query ids with one atomic (warp-aggregated) and refills them; lanes run up
-// to `steps` node/leaf steps between refills.
+// query ids with one atomic (warp-aggregated) and refills them.  `steps`
+// packs two limits: the low 16 bits are the most traversal steps between
+// refills; the high bits, when non-zero, a refill threshold -- the warp
+// leaves the step loop for a refill as soon as that many lanes are idle
+// (checked after every step).  Without a threshold the lanes run the full
+// number of steps between refills.
 template <class Src, bool kAny, bool kStats, bool kWt = false>
 __device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, uint32_t* fetch,
                                                     TwoLevelStack stk, int steps, TraceStats& st, uint32_t& err) {
   const unsigned lane_id = threadIdx.x & 31u;
+  const int max_steps = steps & 0xFFFF;
+  const int refill_min = steps >> 16;
   LaneState L;
   bool active = false;
   bool exhausted = false;
@@ -660,14 +779,26 @@ __device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, 
       }
     }
     if (!__any_sync(0xffffffffu, active)) break;
-    if (active) {
-      for (int k = 0; k < steps; ++k) {
-        if (lane_step<kAny, kStats, kWt>(L, stk, st, err)) {
+    if (refill_min == 0) {
+      if (active) {
+        for (int k = 0; k < max_steps; ++k) {
+          if (VKPTC_LANE_STEP(L, stk, st, err)) {
+            src.finish(tag, L.t, L.prim);
+            if (kStats) ++st.rays;
+            active = false;
+            break;
+          }
+        }
+      }
+    } else {
+      for (int k = 0; k < max_steps; ++k) {
+        if (active && VKPTC_LANE_STEP(L, stk, st, err)) {
           src.finish(tag, L.t, L.prim);
           if (kStats) ++st.rays;
           active = false;
-          break;
         }
+        const unsigned idle_now = __ballot_sync(0xffffffffu, !active);
+        if (idle_now == 0xffffffffu || (!exhausted && __popc(idle_now) >= refill_min)) break;
       }
     }
   }

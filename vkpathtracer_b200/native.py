@@ -204,6 +204,7 @@ SIGNATURES = {
     "vkptc_update_scene_delta": (I32, [P, ctypes.POINTER(SceneDelta)]),
     "vkptc_request_ldr_readback": (I32, [P, ctypes.POINTER(FilmResolve), ctypes.POINTER(ctypes.c_uint64)]),
     "vkptc_poll_ldr_readback": (I32, [P, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
+    "vkptc_measure_read_bandwidth": (I32, [P, ctypes.c_uint64, U32, ctypes.POINTER(ctypes.c_double)]),
     "vkptc_device_name": (I32, [P, ctypes.c_char_p, U32, ctypes.POINTER(U32)]),
     "vkptc_build_binary_bvh": (I32, [ctypes.POINTER(SceneView), P, ctypes.POINTER(U32), P, ctypes.POINTER(U32)]),
     "vkptc_reset": (I32, [P]),

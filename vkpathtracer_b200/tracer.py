@@ -215,6 +215,14 @@ class CudaPathTracer:
         b = native.BvhView(_ptr(nodes), nodes.shape[0], _ptr(prim), prim.size)
         return self._status(self._lib.vkptc_load_bvh(self._ctx, ctypes.byref(b)))
 
+    def read_bandwidth(self, nbytes: int, reps: int) -> float:
+        """GB/s of 16-byte reads (cached in L2 only) streaming `reps` times over a
+        device buffer of `nbytes`: L2 bandwidth for a buffer well under the L2
+        size, HBM read bandwidth for one far above it."""
+        g = ctypes.c_double(0.0)
+        self._check(self._lib.vkptc_measure_read_bandwidth(self._ctx, nbytes, reps, ctypes.byref(g)))
+        return float(g.value)
+
     def accel_info(self) -> dict:
         a = native.AccelInfo()
         self._check(self._lib.vkptc_get_accel_info(self._ctx, ctypes.byref(a)))
