@@ -222,6 +222,20 @@ def tiled_check(jobs, threads: int, kind: str):
             "paths_per_s": paths / (r["counters"]["render_ms"] / 1e3)}
 
 
+def avx2_baseline(jobs, frac: float, threads: int, seed: int = 0):
+    """The same CPU sample through the reference's AVX2 build (its 8-wide
+    leaf test, -mavx2 -mfma): a second timing of the reference's CPU path, not
+    a parity checker (its leaves and arithmetic differ from the default build)."""
+    import oracle
+    if not oracle.have_reference_avx2():
+        return None
+    r = cpu_batch(jobs, frac, threads, "reference_avx2", seed=seed)
+    return {"value": r["paths_per_s"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "build": "-O2 -mavx2 -mfma -DPT_ENABLE_AVX2 (BvhTriangleIntersectorAvx2, leaf threshold 8)",
+            "sample": f"random {frac:g} of every job's pixels at the job's spp ({r['paths']} paths, "
+                      f"{r['render_ms']:.0f} ms; " + CPU_TRACER.format(t=threads) + ")"}
+
+
 def film_parity(cpu, sums, counts):
     """GPU films (full films per job) against the CPU oracle's films of the same
     jobs on the oracle's pixel subset: bit-identical pixels, relative RMSE of
@@ -269,6 +283,7 @@ def run_reference(args, world, rank):
             render_ms += r["render_ms"]
     value = paths / (render_ms / 1e3)
     tiled = tiled_check(jobs, threads, kind)
+    avx2 = avx2_baseline(jobs, frac, threads, seed=args.warmup + args.steps) if kind == "reference" else None
     tracer = CPU_TRACER.format(t=threads) if kind == "reference" else f"the oracle port on {threads} threads"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": render_ms / args.steps,
@@ -283,7 +298,7 @@ def run_reference(args, world, rank):
                                       "excluded, as ptbench times only its render loop)",
                        "full_workload_ms_estimate": 1e3 * cfg["paths_per_step"] / value,
                        "step_wall_s_with_setup": sample["wall_s"]},
-            "tiled_check": tiled,
+            "tiled_check": tiled, "avx2_build": avx2,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -797,10 +812,6 @@ def run_ours(args, world, rank, local):
         b.run(m, **mt)
         ms = min(b.run(m, **mt)["device_ms"] for _ in range(2))
         drivers[m] = {"paths_per_s": total_paths / (ms / 1e3), "tuning": mt}
-    # The job set's device memory goes before the other sections: with it
-    # resident, a later acceleration build of the 2M-triangle grid took 16-70 ms
-    # instead of 4-8 ms.
-    b.close()
     # the same jobs with the watertight triangle test (loop driver, the same tuning)
     wt = None
     if rank == 0 and mode == "loop" and not args.no_watertight:
@@ -812,7 +823,7 @@ def run_ours(args, world, rank, local):
         wt = {"paths_per_s": total_paths / (wms / 1e3), "driver": "loop", "tuning": tuning,
               "relative_to_moller_trumbore": (total_paths / (wms / 1e3)) / (value / world)}
 
-    roof = rq = ff = cpu = inv = sdf = bb = fr = parity = None
+    roof = rq = ff = cpu = inv = sdf = bb = fr = parity = cpu_avx2 = None
     if rank == 0:
         # ------------------------------------------------------ roofline of the dominant kernel
         # traversal work counted in a stats run (same rays: the traversal is deterministic)
@@ -882,6 +893,7 @@ def run_ours(args, world, rank, local):
                                        "(the films of the last timed step)"}
             if rq is not None and "_ids" in rq:
                 parity.update(ray_query_parity(rq.pop("_ids"), threads, kind))
+            cpu_avx2 = avx2_baseline(jobs, frac, threads)
         if rq is not None:
             rq.pop("_ids", None)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -901,7 +913,7 @@ def run_ours(args, world, rank, local):
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
                 "inverse_rendering": inv, "sdf_scene": sdf, "bvh_build": bb, "film_resolve": fr,
                 "watertight_batch": wt,
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu, "cpu_baseline_avx2": cpu_avx2}
         print(json.dumps(line), flush=True)
     b.close()
 

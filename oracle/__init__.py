@@ -26,6 +26,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libvkptref.so")
+# The reference's AVX2 build (timing only: its leaf size and arithmetic differ from the parity build).
+REF_AVX2_LIB = os.path.join(HERE, "_ref_avx2", "libvkptref.so")
 PORT_LIB = os.path.join(HERE, "_build", "libvkptport.so")
 ADJ_LIB = os.path.join(HERE, "_build", "libvkptadj.so")
 # The reference checkout (read-only); VKPT_REFERENCE_DIR overrides the default location.
@@ -134,6 +136,8 @@ def build_ref(quiet: bool = True) -> Optional[str]:
     if not os.path.isdir(REFERENCE_SRC):
         return REF_LIB if os.path.exists(REF_LIB) else None
     subprocess.run(["make", "-C", HERE, "ref", f"REF={REFERENCE_SRC}", "-j8"], check=True,
+                   capture_output=quiet)
+    subprocess.run(["make", "-C", HERE, "ref_avx2", f"REF={REFERENCE_SRC}", "-j8"], check=True,
                    capture_output=quiet)
     # The C++ IPathTracer adapter checker links the library; build it when the library exists.
     lib = os.path.join(os.path.dirname(HERE), "vkpathtracer_b200", "_lib", "libvkpt_cuda.so")
@@ -363,7 +367,8 @@ _CACHE = {}
 
 
 def load(kind: str = "auto") -> Oracle:
-    """kind: "reference", "port" or "auto" (reference when built, else port)."""
+    """kind: "reference", "port", "auto" (reference when built, else port) or
+    "reference_avx2" (the reference's AVX2 build: CPU timing only)."""
     if kind == "auto":
         kind = "reference" if os.path.exists(REF_LIB) else "port"
     if kind in _CACHE:
@@ -372,6 +377,10 @@ def load(kind: str = "auto") -> Oracle:
         if not os.path.exists(REF_LIB):
             raise FileNotFoundError("reference oracle not built (oracle/_ref/libvkptref.so)")
         o = Oracle(REF_LIB)
+    elif kind == "reference_avx2":
+        if not os.path.exists(REF_AVX2_LIB):
+            raise FileNotFoundError("reference AVX2 build missing (oracle/_ref_avx2/libvkptref.so)")
+        o = Oracle(REF_AVX2_LIB)
     elif kind == "port":
         o = Oracle(build_port())
     else:
@@ -382,6 +391,10 @@ def load(kind: str = "auto") -> Oracle:
 
 def have_reference() -> bool:
     return os.path.exists(REF_LIB)
+
+
+def have_reference_avx2() -> bool:
+    return os.path.exists(REF_AVX2_LIB)
 
 
 def build_adjoint(quiet: bool = True) -> str:

@@ -51,7 +51,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             sys.stderr.write(r.stderr)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + objs
+    # --no-undefined: a symbol no object defines fails the build instead of the first dlopen
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xlinker", "--no-undefined", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

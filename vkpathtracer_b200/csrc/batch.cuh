@@ -59,6 +59,7 @@ struct BatchLaunch {
   int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
                   // (the persistent kernel; in the loop driver, its two traversal stages)
   bool watertight;  // the jobs' triangle records hold vertices (watertight test)
+  bool exotic;      // some job has a transmissive, clear-coat, sheen or toon material or an environment map
 };
 
 // Number of control words the pool needs; word kBatchCtlIterations holds the

@@ -259,7 +259,11 @@ __global__ void __launch_bounds__(256) k_lp_sdf_shadow(const DevJob* __restrict_
   flush_sdf(ctr, c);
 }
 
-template <bool kParity, bool kEffects>
+// kSdf: some job has SDF primitives (the SDF stages run and the shading
+// stage takes their hits); without, the shading code carries no SDF steps.
+// kExotic: some job has a transmissive, clear-coat, sheen or toon material or
+// an environment map; without, those branches are compiled out.
+template <bool kParity, bool kEffects, bool kSdf, bool kExotic>
 __global__ void __launch_bounds__(256, 3) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr,
                                                   uint32_t sdf_staged) {
   const uint32_t cur = P.ctl[kLCur];
@@ -286,7 +290,8 @@ __global__ void __launch_bounds__(256, 3) k_lp_shade(const DevJob* __restrict__ 
       pr.rad = mk(r4.x, r4.y, r4.z);
       pr.segs = r4.w;
       pr.rng = A.rng[j];
-      R = shade_bounce<kParity, kEffects>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x, __float_as_uint(h2.y),
+      R = shade_bounce<kParity, kEffects, kSdf, kExotic>(J.scene, J.settings, J.scene.lights, depth, pr, h2.x,
+                                                         __float_as_uint(h2.y),
                                           sdf_staged != 0u);
       next = R.next;
       fin = !R.next;
@@ -400,14 +405,26 @@ LoopTraceFn shadow_fn(bool stats, int occ, bool wt) {
   return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
 }
 
+// Shading stage variants: [parity][effects][sdf][exotic].
+using LoopShadeFn = void (*)(const DevJob*, LoopPool, DevCounters*, uint32_t);
+template <bool kP, bool kE>
+LoopShadeFn shade_fn_pe(bool sdf, bool exotic) {
+  static const LoopShadeFn t[2][2] = {{k_lp_shade<kP, kE, false, false>, k_lp_shade<kP, kE, false, true>},
+                                      {k_lp_shade<kP, kE, true, false>, k_lp_shade<kP, kE, true, true>}};
+  return t[sdf ? 1 : 0][exotic ? 1 : 0];
+}
+LoopShadeFn shade_fn(bool parity, bool effects, bool sdf, bool exotic) {
+  if (parity) return effects ? shade_fn_pe<true, true>(sdf, exotic) : shade_fn_pe<true, false>(sdf, exotic);
+  return effects ? shade_fn_pe<false, true>(sdf, exotic) : shade_fn_pe<false, false>(sdf, exotic);
+}
+
 }  // namespace
 
 LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count, bool watertight) {
   LoopGrids g{};
   g.regen = sm_count * (parity ? blocks_per_sm(k_lp_regen<true>, block, 0) : blocks_per_sm(k_lp_regen<false>, block, 0));
   g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy, watertight), block, smem);
-  g.shade = sm_count * (parity ? blocks_per_sm(k_lp_shade<true, true>, block, 0)
-                               : blocks_per_sm(k_lp_shade<false, true>, block, 0));
+  g.shade = sm_count * blocks_per_sm(shade_fn(parity, true, true, true), block, 0);
   g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy, watertight), block, smem);
   g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
   g.sdf = sm_count * std::min(blocks_per_sm(k_lp_sdf, block, 0), blocks_per_sm(k_lp_sdf_shadow, block, 0));
@@ -449,13 +466,7 @@ cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, uns
   if (bl.sdf) k_lp_sdf<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
   mark(2);
   const uint32_t staged = bl.sdf ? 1u : 0u;
-  if (bl.effects) {
-    if (bl.parity) k_lp_shade<true, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
-    else k_lp_shade<false, true><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
-  } else {
-    if (bl.parity) k_lp_shade<true, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
-    else k_lp_shade<false, false><<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
-  }
+  shade_fn(bl.parity, bl.effects, bl.sdf, bl.exotic)<<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
   mark(3);
   if (bl.sdf) k_lp_sdf_shadow<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
   shadow_fn(bl.stats, bl.occupancy, bl.watertight)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,

@@ -76,6 +76,10 @@ cudaError_t BuildAccelOnDevice(const DeviceSceneArrays& scene, bool sah, cudaStr
 // Stream-ordered frees of the builder's arrays: after the work already queued
 // on `stream`, back into the pool (no device-wide synchronisation).
 void FreeAccelArray(void* p, cudaStream_t stream);
+// Returns the freed memory the build pool of the current device keeps mapped
+// to the driver (after the device's pending work); the library calls it when
+// the last context on a device is destroyed.
+void TrimBuildPool();
 void FreeDeviceAccel(DeviceAccelOut& out, cudaStream_t stream = nullptr);
 void FreeRefitState(DeviceRefitState*& state, cudaStream_t stream = nullptr);
 

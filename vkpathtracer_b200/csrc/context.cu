@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -112,6 +113,10 @@ constexpr size_t kNoAllocArrays = 12;
 constexpr size_t kNoAllocBytes = VKPTC_NOALLOC_MAX_PATHS * kNoAllocPathBytes + (kNoAllocArrays + 1) * 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+// Live contexts per device (a batch's jobs are contexts too): when the last
+// one goes, the device build pool's kept memory is returned to the driver.
+std::atomic<int> g_live_contexts[64];
+
 // Makes `device` current for the scope and restores the caller's device after.
 struct DeviceGuard {
   int prev = -1;
@@ -184,6 +189,7 @@ struct vkptc_ctx {
   HostCamera cam{};
   bool has_transmissive = false;
   bool has_effects = false;
+  bool has_exotic = false;      // a transmissive, clear-coat, sheen or toon material (shading variants)
 
   // device scene
   DevBuf<float4> d_nodes, d_tris, d_shade, d_tie;
@@ -483,10 +489,16 @@ int32_t check_device_error(vkptc_ctx* c) {
 void scan_materials(vkptc_ctx* c) {
   c->has_transmissive = false;
   c->has_effects = false;
+  c->has_exotic = false;
   for (size_t i = 0; i < c->materials.size() / 16; ++i) {
     const float* m = &c->materials[16 * i];
     if (static_cast<uint32_t>(m[7] + 0.5f) == 5u || m[10] > 0.05f) c->has_transmissive = true;
     if ((static_cast<uint32_t>(m[15] + 0.5f) & 1023u) != 0u) c->has_effects = true;
+    // The shading stage's tests (models 5..8, transmission, clear coat); a model
+    // word outside the plain range counts as exotic so no branch is dropped.
+    const float mw = m[7];
+    const bool plain_model = mw >= 0.0f && mw < 4.5f;
+    if (!plain_model || m[10] > 0.05f || m[11] > 0.05f) c->has_exotic = true;
   }
 }
 
@@ -635,6 +647,7 @@ int32_t vkptc_create(const vkptc_config* config, vkptc_ctx** out_ctx) {
   c->noalloc_lookup = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
   if (c->noalloc_lookup == cudaSuccess) c->noalloc_scratch = static_cast<unsigned char*>(scratch);
   else cudaGetLastError();
+  if (c->device < 64) g_live_contexts[c->device].fetch_add(1);
   *out_ctx = c;
   return VKPTC_OK;
 }
@@ -652,8 +665,10 @@ int32_t vkptc_destroy(vkptc_ctx* ctx) {
   if (ctx->ldr_event) cudaEventDestroy(ctx->ldr_event);
   if (ctx->h_ldr) cudaFreeHost(ctx->h_ldr);
   release_refit(ctx);
+  const int device = ctx->device;
   delete ctx;
   if (s) cudaStreamDestroy(s);
+  if (device < 64 && g_live_contexts[device].fetch_sub(1) == 1) TrimBuildPool();
   return VKPTC_OK;
 }
 
@@ -1916,9 +1931,11 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   bl.watertight = watertight;
   bl.effects = false;
   bl.sdf = false;
+  bl.exotic = false;
   for (vkptc_ctx* c : b->jobs) {
     bl.effects = bl.effects || c->has_effects;
     bl.sdf = bl.sdf || c->sdf_count != 0u;
+    bl.exotic = bl.exotic || c->has_exotic || c->env_w != 0u;
   }
   bl.occupancy = static_cast<int>(std::min(3u, t.occupancy));
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);

@@ -221,7 +221,7 @@ __device__ __forceinline__ V3 environment(const DevScene& s, V3 dir_in) {
 }
 
 // sample_direct_light without the visibility loop (which the shadow stage runs).
-template <bool kParity, bool kEffects = true>
+template <bool kParity, bool kEffects = true, bool kExotic = true>
 __device__ __forceinline__ NeeQuery nee_setup(const DevScene& s, const float* lights, V3 p, V3 n, uint32_t mat_index,
                                               V3 view, uint64_t& rng) {
   NeeQuery q;
@@ -253,8 +253,8 @@ __device__ __forceinline__ NeeQuery nee_setup(const DevScene& s, const float* li
   const float rough = clamp01(m.roughness);
   const bool mirror = m.model == 2u || rough <= 0.001f;
   const bool metal = m.model == 4u || m.metallic > 0.65f;
-  const bool trans = m.model == 5u || m.transmission > 0.05f;
-  const bool coat = m.model == 7u || m.clearcoat > 0.05f;
+  const bool trans = kExotic && (m.model == 5u || m.transmission > 0.05f);
+  const bool coat = kExotic && (m.model == 7u || m.clearcoat > 0.05f);
   const V3 alb = surface_albedo<kParity, kEffects>(m, p, n, neg(ldir));
   const V3 irr = mul(ld3(L + 3), (L[6] * sf) / (d2 + kEps));
   V3 acc = mk(0.0f, 0.0f, 0.0f);
@@ -398,14 +398,21 @@ struct ShadeOut {
 // intersect_scene does; an SDF hit becomes prim = kSdfTag | index.  In a
 // scene without transmissive materials the shadow query's SDF test runs here
 // too: a query an SDF occludes is never queued for the triangle any-hit.
+// kSdf = false compiles every SDF step out (for launches in which no scene
+// has SDF primitives), and kExotic = false the transmissive, clear-coat,
+// sheen and toon branches and the environment-map lookup (for launches whose
+// scenes have none: the host classifies the material tables with the same
+// tests), which keeps the shading kernel's hot code compact.
 // sdf_staged: a load-balanced stage has already folded the SDF hits into
 // (ht, prim) and tests the shadow queries itself (the loop driver).
-template <bool kParity, bool kEffects = true>
+template <bool kParity, bool kEffects = true, bool kSdf = true, bool kExotic = true>
 __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSettings& st, const float* lights,
                                                uint32_t depth, PathRegs& P, float ht, uint32_t prim,
                                                bool sdf_staged = false) {
   ShadeOut R;
-  if (s.sdf_count != 0u && !sdf_staged) sdf_closest(s.sdf, s.sdf_count, P.o, P.d, ht, prim, R.sdf);
+  if constexpr (kSdf) {
+    if (s.sdf_count != 0u && !sdf_staged) sdf_closest(s.sdf, s.sdf_count, P.o, P.d, ht, prim, R.sdf);
+  }
   R.next = false;
   R.shadow = false;
   R.shadow_tests = 0u;
@@ -416,12 +423,12 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
   uint64_t rng = P.rng;
   P.segs = P.segs + 1.0f;
   if (prim == kMiss) {
-    rad = add(rad, mulv(thr, environment<kParity>(s, d)));
+    rad = add(rad, mulv(thr, kExotic ? environment<kParity>(s, d) : s.env));
   } else {
     const V3 hp = add(o, mul(d, ht));
     V3 gn;
     uint32_t mat_index;
-    if (prim & kSdfTag) {
+    if (kSdf && (prim & kSdfTag)) {
       gn = sdf_hit_normal(s.sdf, prim & ~kSdfTag, o, d, ht);
       mat_index = sdf_material(s.sdf, prim & ~kSdfTag);
     } else {
@@ -439,11 +446,11 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
     const bool emissive_model = m.model == 1u || emissive_any;
     const bool mirror = m.model == 2u || rough <= 0.001f;
     const bool metal = m.model == 4u || m.metallic > 0.65f;
-    const bool trans = m.model == 5u || m.transmission > 0.05f;
+    const bool trans = kExotic && (m.model == 5u || m.transmission > 0.05f);
     const bool diffuse = rough >= 0.999f && !mirror && !metal && !trans;
-    const bool sheen = m.model == 6u;
-    const bool coat = m.model == 7u || m.clearcoat > 0.05f;
-    const bool toon = m.model == 8u;
+    const bool sheen = kExotic && m.model == 6u;
+    const bool coat = kExotic && (m.model == 7u || m.clearcoat > 0.05f);
+    const bool toon = kExotic && m.model == 8u;
 
     if (!st.enable_nee || depth == 0u) {
       rad = add(rad, mulv(thr, m.emissive));
@@ -454,7 +461,7 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
     }
 
     if (st.enable_nee && depth < st.max_depth - 1u) {
-      const NeeQuery nq = nee_setup<kParity, kEffects>(s, lights, hp, nrm, mat_index, neg(d), rng);
+      const NeeQuery nq = nee_setup<kParity, kEffects, kExotic>(s, lights, hp, nrm, mat_index, neg(d), rng);
       if (nq.valid) {
         R.shadow_tests = 1u;
         V3 c;
@@ -468,7 +475,7 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
           c = mulv(thr, nq.radiance);
         }
         if (nq.remain > 0.004f) {
-          R.shadow = !(s.sdf_count != 0u && !s.has_transmissive && !sdf_staged &&
+          R.shadow = !(kSdf && s.sdf_count != 0u && !s.has_transmissive && !sdf_staged &&
                        sdf_any(s.sdf, s.sdf_count, nq.origin, nq.dir, nq.remain, R.sdf));
           R.sh_o = nq.origin;
           R.sh_d = nq.dir;
