@@ -140,7 +140,7 @@ struct LoopGrids {
   int regen, extend, shade, shadow, finish, sdf;
 };
 LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count,
-                         bool watertight = false);
+                         bool watertight = false, bool effects = true, bool sdf = true, bool exotic = true);
 cudaError_t ConfigureBatchLoopSmem(size_t bytes);
 cudaError_t LaunchBatchLoopInit(const LoopPool& pool, cudaStream_t stream);
 // One iteration of the five stages; the finish stage sets `handle` (the

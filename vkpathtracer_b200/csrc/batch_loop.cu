@@ -263,8 +263,11 @@ __global__ void __launch_bounds__(256) k_lp_sdf_shadow(const DevJob* __restrict_
 // stage takes their hits); without, the shading code carries no SDF steps.
 // kExotic: some job has a transmissive, clear-coat, sheen or toon material or
 // an environment map; without, those branches are compiled out.
+#ifndef VKPTC_LEAN_SHADE_BLOCKS
+#define VKPTC_LEAN_SHADE_BLOCKS 3
+#endif
 template <bool kParity, bool kEffects, bool kSdf, bool kExotic>
-__global__ void __launch_bounds__(256, 3) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr,
+__global__ void __launch_bounds__(256, (kEffects || kSdf || kExotic) ? 3 : VKPTC_LEAN_SHADE_BLOCKS) k_lp_shade(const DevJob* __restrict__ jobs, LoopPool P, DevCounters* ctr,
                                                   uint32_t sdf_staged) {
   const uint32_t cur = P.ctl[kLCur];
   const uint32_t n = P.ctl[kLCount0 + cur];
@@ -420,11 +423,12 @@ LoopShadeFn shade_fn(bool parity, bool effects, bool sdf, bool exotic) {
 
 }  // namespace
 
-LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count, bool watertight) {
+LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int occupancy, int sm_count, bool watertight,
+                         bool effects, bool sdf, bool exotic) {
   LoopGrids g{};
   g.regen = sm_count * (parity ? blocks_per_sm(k_lp_regen<true>, block, 0) : blocks_per_sm(k_lp_regen<false>, block, 0));
   g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy, watertight), block, smem);
-  g.shade = sm_count * blocks_per_sm(shade_fn(parity, true, true, true), block, 0);
+  g.shade = sm_count * blocks_per_sm(shade_fn(parity, effects, sdf, exotic), block, 0);
   g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy, watertight), block, smem);
   g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
   g.sdf = sm_count * std::min(blocks_per_sm(k_lp_sdf, block, 0), blocks_per_sm(k_lp_sdf_shadow, block, 0));

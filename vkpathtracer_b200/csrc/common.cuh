@@ -90,6 +90,27 @@ __device__ __forceinline__ float t_cos(float x) {
   if constexpr (kParity) return parity_cos(x);
   else return cosf(x);
 }
+// cos and sin of one angle.  Parity mode: one FP64 sincos rounded to float
+// per result, which gives the FP64 sin and cos rounded once, like t_cos/t_sin.
+#ifndef VKPTC_SINCOS
+#define VKPTC_SINCOS 1
+#endif
+#if VKPTC_SINCOS
+static __device__ __noinline__ float2 parity_cos_sin(float x) {
+  double s = 0.0, c = 0.0;
+  sincos(static_cast<double>(x), &s, &c);
+  return make_float2(static_cast<float>(c), static_cast<float>(s));
+}
+#endif
+template <bool kParity>
+__device__ __forceinline__ float2 t_cos_sin(float x) {
+#if VKPTC_SINCOS
+  if constexpr (kParity) return parity_cos_sin(x);
+#else
+  if constexpr (kParity) return make_float2(parity_cos(x), parity_sin(x));
+#endif
+  else return make_float2(cosf(x), sinf(x));
+}
 template <bool kParity>
 __device__ __forceinline__ float t_pow(float x, float y) {
   if constexpr (kParity) return parity_pow(x, y);

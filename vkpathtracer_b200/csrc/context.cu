@@ -1948,7 +1948,8 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
       VKPTC_BCUDA(b, ConfigureBatchLoopSmem(smem), "shared memory limit");
       b->loop_smem_configured = smem;
     }
-    lg = BatchLoopGrids(bl.block, smem, parity, bl.stats, bl.occupancy, b->sm_count, watertight);
+    lg = BatchLoopGrids(bl.block, smem, parity, bl.stats, bl.occupancy, b->sm_count, watertight, bl.effects, bl.sdf,
+                        bl.exotic);
     if (lg.regen <= 0 || lg.extend <= 0 || lg.shade <= 0 || lg.shadow <= 0 || lg.finish <= 0) {
       return bfail(b, VKPTC_UNSUPPORTED, "a batch stage kernel does not fit on an SM with this block size");
     }

@@ -237,7 +237,8 @@ __device__ __forceinline__ NeeQuery nee_setup(const DevScene& s, const float* li
     const float uz = 1.0f - 2.0f * next01(rng);
     const float r = sqrtf(smax(0.0f, 1.0f - uz * uz));
     const float phi = 6.28318530718f * next01(rng);
-    lp = add(lp, mul(mk(r * t_cos<kParity>(phi), uz, r * t_sin<kParity>(phi)), radius));
+    const float2 cs = t_cos_sin<kParity>(phi);
+    lp = add(lp, mul(mk(r * cs.x, uz, r * cs.y), radius));
   }
   const V3 tl = sub(lp, p);
   const float d2 = dot(tl, tl);
@@ -289,7 +290,8 @@ __device__ __forceinline__ V3 sample_hemisphere(uint64_t& rng, V3 n) {
   const float u2 = next01(rng);
   const float r = sqrtf(smax(0.0f, 1.0f - u1));
   const float phi = 2.0f * kPi * u2;
-  const V3 loc = mk(r * t_cos<kParity>(phi), r * t_sin<kParity>(phi), sqrtf(smax(0.0f, u1)));
+  const float2 cs = t_cos_sin<kParity>(phi);
+  const V3 loc = mk(r * cs.x, r * cs.y, sqrtf(smax(0.0f, u1)));
   V3 t = cross((fabsf(n.z) < 0.999f) ? mk(0.0f, 0.0f, 1.0f) : mk(0.0f, 1.0f, 0.0f), n);
   t = unit(t);
   const V3 b = cross(n, t);
@@ -306,7 +308,8 @@ __device__ __forceinline__ V3 sample_phong(uint64_t& rng, V3 refl, float expo, V
   const V3 ref = (fabsf(refl.z) < 0.999f) ? mk(0.0f, 0.0f, 1.0f) : mk(0.0f, 1.0f, 0.0f);
   const V3 t = unit(cross(ref, refl));
   const V3 b = cross(refl, t);
-  V3 out = unit(add(add(mul(t, sn * t_cos<kParity>(phi)), mul(b, sn * t_sin<kParity>(phi))), mul(refl, ct)));
+  const float2 cs = t_cos_sin<kParity>(phi);
+  V3 out = unit(add(add(mul(t, sn * cs.x), mul(b, sn * cs.y)), mul(refl, ct)));
   if (dot(out, n) <= 0.0f) {
     out = sub(out, mul(n, 2.0f * dot(out, n)));
     if (dot(out, n) <= 0.0f) return sample_hemisphere<kParity>(rng, n);
