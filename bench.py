@@ -41,9 +41,9 @@ WORKLOAD = "batch_64_uneven_jobs"
 NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
 PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
 # DRAM bytes (read + write) per extension ray of k_lp_extend, from one ncu
-# capture of a steady-state launch of the 4-job case (62.79 MB for a launch of
-# 1,048,576 rays).
-TRAFFIC_BYTES_PER_EXT_RAY = 62789632 / 1048576
+# capture of a steady-state launch of the 4-job case (102.40 MB read + 9.86 MB
+# written for a launch of 2,097,152 rays).
+TRAFFIC_BYTES_PER_EXT_RAY = (102397952 + 9857280) / 2097152
 
 
 def l2_roofline(device, achieved_gbs):
@@ -215,11 +215,17 @@ def tiled_check(jobs, threads: int, kind: str):
     j = min(jobs, key=lambda j: abs(j.settings.width * j.settings.height * j.settings.spp - 1_000_000))
     r = o.render(j.scene, j.settings, threads=threads)
     paths = j.settings.width * j.settings.height * j.settings.spp
+    # the pooled harness on every pixel of the same job
+    outs, pool_ms = o.render_jobs([(j.scene, j.settings, np.arange(j.settings.width * j.settings.height,
+                                                                   dtype=np.uint32))], threads=threads)
     return {"tracer": "TiledCpuPathTracer" if kind == "reference" else "port", "worker_count": threads,
             "tile_height": 16, "job": {"side": j.settings.width, "spp": j.settings.spp,
                                        "depth": j.settings.max_depth, "triangles": j.scene.triangle_count},
             "paths": paths, "render_ms": r["counters"]["render_ms"],
-            "paths_per_s": paths / (r["counters"]["render_ms"] / 1e3)}
+            "paths_per_s": paths / (r["counters"]["render_ms"] / 1e3),
+            "pooled_harness_paths_per_s": paths / (pool_ms / 1e3),
+            "films_equal": bool(np.array_equal(r["sum"].reshape(-1, 3).view(np.uint32),
+                                               outs[0]["sum"].view(np.uint32)))}
 
 
 def avx2_baseline(jobs, frac: float, threads: int, seed: int = 0):
@@ -905,15 +911,15 @@ def run_ours(args, world, rank, local):
                                                    "rule through the reference tree)",
                         "driver": mode, "tuning": tuning,
                         "autotune": {k: tune.get(k) for k in ("ms", "trials", "cached")}},
-                "parity": parity,
-                "mrays_per_s": mrays, "plain_paths_per_s": plain_ps, "speedup_vs_plain": value / world / plain_ps,
-                "drivers": drivers,
+
+                "mrays_per_s": mrays, "drivers": drivers,
                 "plain_kernel_launches": plain["kernel_launches"],
                 "gpu_launches": sum(s["kernel_launches"] for s in stats),
                 "clocks": clocks.summary(), "e2e": e2e, "roofline": roof, "full_frame": ff, "ray_query": rq,
                 "inverse_rendering": inv, "sdf_scene": sdf, "bvh_build": bb, "film_resolve": fr,
                 "watertight_batch": wt,
-                "cpu_baseline": cpu, "cpu_baseline_avx2": cpu_avx2}
+                "cpu_baseline_avx2": cpu_avx2, "cpu_baseline": cpu, "parity": parity,
+                "plain_paths_per_s": plain_ps, "speedup_vs_plain": value / world / plain_ps}
         print(json.dumps(line), flush=True)
     b.close()
 
