@@ -16,6 +16,8 @@
 // then per-block partials, then a fixed-order FP64 reduction: the gradient is
 // deterministic for a given launch shape.
 #include "adjoint.cuh"
+#include <algorithm>
+
 #include "adjoint_launch.h"
 #include "traverse.cuh"
 
@@ -29,19 +31,21 @@ struct AdjRec {
   float4 c;   // throughput at the vertex xyz, roulette divisor applied after it
   uint4 e;    // RNG state lo, hi at the vertex, flags, material index
 };
+static_assert(sizeof(AdjRec) == kAdjRecordFloat4s * sizeof(float4), "record layout of the backward buffers");
+static_assert(kAdjVertexSlots == kAdjMaxDepth, "record slots per path");
 
 __device__ __forceinline__ uint32_t mat_slot(const DevScene& s, uint32_t mat_index) {
   return mat_index < s.material_count - 1u ? mat_index : s.material_count - 1u;
 }
 
 // The primal path of pixel (x, y), sample `sample`.  kRecord keeps the
-// vertex records for the reverse sweep.  Returns radiance xyz and, in w, the
+// vertex records for the reverse sweep: vertex k at rec[k * rec_stride].  Returns radiance xyz and, in w, the
 // bits of a 32-bit hash of the path's discrete decisions (hit primitives and
 // vertex flags): two evaluations with equal hashes took the same branches.
 template <bool kParity, bool kRecord>
 __device__ __forceinline__ float4 adj_primal(const DevScene& s, const DevSettings& st, const float* mat0,
                                              uint32_t x, uint32_t y, uint32_t sample, SmemStack stk,
-                                             uint32_t& err, AdjRec* rec, uint32_t& nrec) {
+                                             uint32_t& err, AdjRec* rec, uint32_t& nrec, uint32_t rec_stride = 1u) {
   V3 o, d;
   uint64_t rng;
   camera_path<kParity>(s, st, x, y, sample, o, d, rng);
@@ -58,7 +62,7 @@ __device__ __forceinline__ float4 adj_primal(const DevScene& s, const DevSetting
       rad = add(rad, mulv(thr, s.env));
       sig = mix64(sig ^ 0xFFFFFFFFull);
       if (kRecord) {
-        AdjRec& r = rec[nrec++];
+        AdjRec& r = rec[static_cast<size_t>(nrec++) * rec_stride];
         r.a = make_float4(o.x, o.y, o.z, 0.0f);
         r.b = make_float4(d.x, d.y, d.z, __uint_as_float(kMiss));
         r.c = make_float4(thr.x, thr.y, thr.z, 1.0f);
@@ -111,7 +115,7 @@ __device__ __forceinline__ float4 adj_primal(const DevScene& s, const DevSetting
     }
     sig = mix64(sig ^ (static_cast<uint64_t>(prim + 1u) | (static_cast<uint64_t>(flags | (cont ? kVfCont : 0u)) << 32)));
     if (kRecord) {
-      AdjRec& r = rec[nrec++];
+      AdjRec& r = rec[static_cast<size_t>(nrec++) * rec_stride];
       r.a = make_float4(o_at.x, o_at.y, o_at.z, t);
       r.b = make_float4(d_at.x, d_at.y, d_at.z, __uint_as_float(prim));
       r.c = make_float4(thr_at.x, thr_at.y, thr_at.z, rr);
@@ -222,7 +226,8 @@ __device__ __forceinline__ float warp_sum(float v) {
 // per-vertex gradients can be combined across lanes.
 template <bool kParity>
 __device__ __forceinline__ void adj_reverse(const DevScene& s, const DevSettings& st, const AdjRec* rec,
-                                            uint32_t nrec, bool lane_on, V3 g, float* warp_grad) {
+                                            uint32_t rec_stride, uint32_t nrec, bool lane_on, V3 g,
+                                            float* warp_grad) {
   const uint32_t kmax = __reduce_max_sync(0xffffffffu, lane_on ? nrec : 0u);
   const int lane = threadIdx.x & 31;
   V3 aT = mk(0.0f, 0.0f, 0.0f), aO = aT, aD = aT;
@@ -231,7 +236,7 @@ __device__ __forceinline__ void adj_reverse(const DevScene& s, const DevSettings
     uint32_t mat = kMiss;
     float gv[kAdjParams] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     if (act) {
-      const AdjRec r = rec[k];
+      const AdjRec r = rec[static_cast<size_t>(k) * rec_stride];
       const uint32_t flags = r.e.z;
       const V3 T = mk(r.c.x, r.c.y, r.c.z);
       if (flags & kVfMiss) {
@@ -333,60 +338,82 @@ __device__ __forceinline__ void adj_reverse(const DevScene& s, const DevSettings
   }
 }
 
-// 128 registers (4 blocks of 128 threads per SM, 16 warps): the reverse sweep's
-// dual numbers need 241 without a bound, which leaves 8 warps per SM; the
-// spills this costs are cheaper than the latency the extra warps hide
-// (backward 7.8 -> 6.9 ms on the 64-parameter workload).
+// The backward runs as two kernels per chunk of paths: the replay (the
+// primal path again, with the traversal) writes every path's vertex records
+// and its radiance adjoint to device memory, and the reverse sweep (the dual-
+// number vertex code) reads them.  Split, each kernel's code is small enough
+// for the instruction cache -- the fused kernel's warps waited on instruction
+// fetch more than on anything else -- and each gets its own register budget.
+// Records: vertex k of chunk path i at recs[k * count + i] (lanes of a warp
+// touch consecutive records).
 template <bool kParity>
-__global__ void __launch_bounds__(128, 4) k_adj_backward(DevScene s, DevSettings st, const float* mat0, uint32_t spp,
-                                                      uint32_t first_sample, int cap, const float4* adj,
-                                                      const float* path_weight, float* grad_part, uint32_t* err) {
+__global__ void __launch_bounds__(128, 5) k_adj_replay(DevScene s, DevSettings st, const float* mat0,
+                                                    uint32_t first_sample, int cap, const float4* adj,
+                                                    const float* path_weight, uint64_t base, uint32_t count,
+                                                    AdjRec* recs, float4* gout, uint32_t* err) {
   extern __shared__ int2 smem_dyn[];
-  const int warps = blockDim.x >> 5;
-  const uint32_t stride = s.material_count * kAdjParams;
-  float* grads = reinterpret_cast<float*>(smem_dyn + static_cast<size_t>(blockDim.x) * cap);
-  for (uint32_t i = threadIdx.x; i < stride * warps; i += blockDim.x) grads[i] = 0.0f;
-  __syncthreads();
   SmemStack stk{smem_dyn + threadIdx.x, static_cast<int>(blockDim.x), cap};
-  float* warp_grad = grads + (threadIdx.x >> 5) * stride;
   const uint32_t npx = st.width * st.height;
-  const uint64_t n = static_cast<uint64_t>(npx) * spp;
   uint32_t local_err = 0u;
-  AdjRec rec[kAdjMaxDepth];
-  for (uint64_t base = blockIdx.x * static_cast<uint64_t>(blockDim.x); base < n;
-       base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint64_t j = base + threadIdx.x;
-    bool on = j < n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint64_t j = base + i;
+    const uint32_t sl = static_cast<uint32_t>(j / npx), p = static_cast<uint32_t>(j % npx);
+    float4 a = adj[p];
+    if (path_weight) {
+      const float pw = path_weight[j];
+      a = make_float4(a.x * pw, a.y * pw, a.z * pw, 0.0f);
+    }
     V3 g = mk(0.0f, 0.0f, 0.0f);
     uint32_t nrec = 0u;
-    if (on) {
-      const uint32_t sl = static_cast<uint32_t>(j / npx), p = static_cast<uint32_t>(j % npx);
-      float4 a = adj[p];
-      if (path_weight) {
-        const float pw = path_weight[j];
-        a = make_float4(a.x * pw, a.y * pw, a.z * pw, 0.0f);
-      }
-      on = a.x != 0.0f || a.y != 0.0f || a.z != 0.0f;
-      if (on) {
-        // The replayed radiance decides what the film would have dropped or
-        // clamped (the replay may use other samples than the forward's).
-        const float4 rv = adj_primal<kParity, true>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk,
-                                                    local_err, rec, nrec);
-        const float fc = st.firefly_clamp;
-        g = mk((fc > 0.0f && rv.x > fc) ? 0.0f : a.x, (fc > 0.0f && rv.y > fc) ? 0.0f : a.y,
-               (fc > 0.0f && rv.z > fc) ? 0.0f : a.z);
-        on = isfinite(rv.x) && isfinite(rv.y) && isfinite(rv.z);
-      }
+    if (a.x != 0.0f || a.y != 0.0f || a.z != 0.0f) {
+      // The replayed radiance decides what the film would have dropped or
+      // clamped (the replay may use other samples than the forward's).
+      const float4 rv = adj_primal<kParity, true>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk,
+                                                  local_err, recs + i, nrec, count);
+      const float fc = st.firefly_clamp;
+      g = mk((fc > 0.0f && rv.x > fc) ? 0.0f : a.x, (fc > 0.0f && rv.y > fc) ? 0.0f : a.y,
+             (fc > 0.0f && rv.z > fc) ? 0.0f : a.z);
+      if (!(isfinite(rv.x) && isfinite(rv.y) && isfinite(rv.z))) nrec = 0u;
     }
-    adj_reverse<kParity>(s, st, rec, nrec, on, g, warp_grad);
+    gout[i] = make_float4(g.x, g.y, g.z, __uint_as_float(nrec));
+  }
+  if (local_err) atomicOr(err, local_err);
+}
+
+// The reverse sweep of one chunk: per-warp gradient slots in shared memory,
+// then one partial per block, added to the partials of the earlier chunks
+// (accumulate) in a fixed order, so the gradient is deterministic.
+#ifndef VKPTC_ADJ_REVERSE_BLOCKS
+#define VKPTC_ADJ_REVERSE_BLOCKS 4
+#endif
+template <bool kParity>
+__global__ void __launch_bounds__(128, VKPTC_ADJ_REVERSE_BLOCKS) k_adj_reverse(DevScene s, DevSettings st, uint32_t count,
+                                                     const AdjRec* recs, const float4* gout, float* grad_part,
+                                                     int accumulate) {
+  extern __shared__ float grads[];
+  const int warps = blockDim.x >> 5;
+  const uint32_t stride = s.material_count * kAdjParams;
+  for (uint32_t i = threadIdx.x; i < stride * warps; i += blockDim.x) grads[i] = 0.0f;
+  __syncthreads();
+  float* warp_grad = grads + (threadIdx.x >> 5) * stride;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    V3 g = mk(0.0f, 0.0f, 0.0f);
+    uint32_t nrec = 0u;
+    if (i < count) {
+      const float4 gv = gout[i];
+      g = mk(gv.x, gv.y, gv.z);
+      nrec = __float_as_uint(gv.w);
+    }
+    adj_reverse<kParity>(s, st, recs + (i < count ? i : 0u), count, nrec, nrec != 0u, g, warp_grad);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < stride; i += blockDim.x) {
     float v = 0.0f;
     for (int w = 0; w < warps; ++w) v += grads[w * stride + i];
-    grad_part[static_cast<size_t>(blockIdx.x) * stride + i] = v;
+    float* dst = grad_part + static_cast<size_t>(blockIdx.x) * stride + i;
+    *dst = accumulate ? *dst + v : v;
   }
-  if (local_err) atomicOr(err, local_err);
 }
 
 __global__ void k_adj_grad_reduce(const float* part, int blocks, uint32_t stride, float* grad) {
@@ -402,17 +429,28 @@ __global__ void k_adj_grad_reduce(const float* part, int blocks, uint32_t stride
 size_t AdjForwardSmem(int block, int stack_cap) { return static_cast<size_t>(block) * stack_cap * sizeof(int2); }
 
 size_t AdjBackwardSmem(int block, int stack_cap, uint32_t materials) {
-  return AdjForwardSmem(block, stack_cap) + static_cast<size_t>(block / 32) * materials * kAdjParams * sizeof(float);
+  return std::max(AdjForwardSmem(block, stack_cap), AdjReverseSmem(block, materials));
 }
 
-int AdjBlocksPerSm(bool backward, int block, size_t smem, bool parity) {
+size_t AdjReverseSmem(int block, uint32_t materials) {
+  return static_cast<size_t>(block / 32) * materials * kAdjParams * sizeof(float);
+}
+
+int AdjBlocksPerSm(AdjKernel k, int block, size_t smem, bool parity) {
   int n = 0;
-  if (backward) {
-    if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_backward<true>, block, smem);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_backward<false>, block, smem);
-  } else {
-    if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<true>, block, smem);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<false>, block, smem);
+  switch (k) {
+    case AdjKernel::kForward:
+      if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<true>, block, smem);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<false>, block, smem);
+      break;
+    case AdjKernel::kReplay:
+      if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_replay<true>, block, smem);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_replay<false>, block, smem);
+      break;
+    case AdjKernel::kReverse:
+      if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_reverse<true>, block, smem);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_reverse<false>, block, smem);
+      break;
   }
   return n > 0 ? n : 1;
 }
@@ -422,8 +460,10 @@ cudaError_t ConfigureAdjSmem(size_t bytes) {
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_adj_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
   if ((e = cudaFuncSetAttribute(k_adj_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-  if ((e = cudaFuncSetAttribute(k_adj_backward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-  return cudaFuncSetAttribute(k_adj_backward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if ((e = cudaFuncSetAttribute(k_adj_replay<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  if ((e = cudaFuncSetAttribute(k_adj_replay<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  if ((e = cudaFuncSetAttribute(k_adj_reverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  return cudaFuncSetAttribute(k_adj_reverse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 cudaError_t LaunchAdjForward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
@@ -445,17 +485,27 @@ cudaError_t LaunchAdjLoss(const DevSettings& st, uint32_t spp, const float4* rad
 }
 
 cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
-                              const float4* adj, const float* path_weight, float* grad_part, float* grad,
-                              uint32_t* err) {
-  const size_t smem = AdjBackwardSmem(l.block, l.stack_cap, s.material_count);
-  if (l.parity)
-    k_adj_backward<true><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, adj,
-                                                              path_weight, grad_part, err);
-  else
-    k_adj_backward<false><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, adj,
-                                                               path_weight, grad_part, err);
+                              const float4* adj, const float* path_weight, float4* recs, float4* gout,
+                              float* grad_part, float* grad, uint32_t* err) {
+  const size_t smem_replay = AdjForwardSmem(l.block, l.stack_cap);
+  const size_t smem_rev = AdjReverseSmem(l.block, s.material_count);
+  const uint64_t n = static_cast<uint64_t>(st.width) * st.height * l.spp;
+  AdjRec* r = reinterpret_cast<AdjRec*>(recs);
+  for (uint64_t base = 0; base < n; base += kAdjChunkPaths) {
+    const uint32_t count = static_cast<uint32_t>(std::min<uint64_t>(kAdjChunkPaths, n - base));
+    const int acc = base > 0 ? 1 : 0;
+    if (l.parity) {
+      k_adj_replay<true><<<l.grid, l.block, smem_replay, l.stream>>>(s, st, mat0, l.first_sample, l.stack_cap, adj,
+                                                                   path_weight, base, count, r, gout, err);
+      k_adj_reverse<true><<<l.grid_reverse, l.block, smem_rev, l.stream>>>(s, st, count, r, gout, grad_part, acc);
+    } else {
+      k_adj_replay<false><<<l.grid, l.block, smem_replay, l.stream>>>(s, st, mat0, l.first_sample, l.stack_cap, adj,
+                                                                    path_weight, base, count, r, gout, err);
+      k_adj_reverse<false><<<l.grid_reverse, l.block, smem_rev, l.stream>>>(s, st, count, r, gout, grad_part, acc);
+    }
+  }
   const uint32_t stride = s.material_count * kAdjParams;
-  k_adj_grad_reduce<<<(stride + 127) / 128, 128, 0, l.stream>>>(grad_part, l.grid, stride, grad);
+  k_adj_grad_reduce<<<(stride + 127) / 128, 128, 0, l.stream>>>(grad_part, l.grid_reverse, stride, grad);
   return cudaGetLastError();
 }
 

@@ -14,6 +14,7 @@ namespace vkptc {
 
 struct AdjLaunch {
   int grid, block;
+  int grid_reverse;       // the backward's reverse-sweep kernel (its own occupancy)
   int stack_cap;          // traversal stack entries per thread (all in shared memory)
   uint32_t spp, first_sample;
   bool parity;
@@ -32,17 +33,28 @@ cudaError_t LaunchAdjForward(const DevScene& s, const DevSettings& st, const flo
 cudaError_t LaunchAdjLoss(const DevSettings& st, uint32_t spp, const float4* rad, const float* target, float* image,
                           float4* adj, double* loss_part, double* loss, int grid, cudaStream_t stream);
 
-// Reverse sweep: per-block gradient partials grad_part[block][7 * materials],
-// then the fixed-order reduction into grad (7 floats per material).
-// path_weight (optional, one per path) scales each path's adjoint.  The
-// paths replayed are those of st.frame (the forward's, or independent ones).
-cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
-                              const float4* adj, const float* path_weight, float* grad_part, float* grad,
-                              uint32_t* err);
+// Paths per backward chunk: the replay writes kAdjRecordFloat4s float4 per
+// path and vertex slot for the chunk, the reverse sweep reads them.
+constexpr uint64_t kAdjChunkPaths = 1ull << 20;
+constexpr size_t kAdjRecordFloat4s = 4;     // one vertex record: 4 float4 (64 bytes)
+constexpr size_t kAdjVertexSlots = 8;       // records per path (the maximum depth)
 
+// Backward: per chunk of paths the replay (records to recs, kAdjVertexSlots *
+// kAdjRecordFloat4s float4 per chunk path, and the radiance adjoint to gout,
+// one float4 per chunk path) then the reverse sweep, whose per-block gradient
+// partials grad_part[block][7 * materials] add up over the chunks; then the
+// fixed-order reduction into grad (7 floats per material).  path_weight
+// (optional, one per path) scales each path's adjoint.  The paths replayed
+// are those of st.frame (the forward's, or independent ones).
+cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
+                              const float4* adj, const float* path_weight, float4* recs, float4* gout,
+                              float* grad_part, float* grad, uint32_t* err);
+
+enum class AdjKernel { kForward, kReplay, kReverse };
 size_t AdjBackwardSmem(int block, int stack_cap, uint32_t materials);
+size_t AdjReverseSmem(int block, uint32_t materials);
 size_t AdjForwardSmem(int block, int stack_cap);
-int AdjBlocksPerSm(bool backward, int block, size_t smem, bool parity);
+int AdjBlocksPerSm(AdjKernel k, int block, size_t smem, bool parity);
 cudaError_t ConfigureAdjSmem(size_t bytes);
 
 }  // namespace vkptc

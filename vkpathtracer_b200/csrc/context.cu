@@ -93,6 +93,7 @@ struct AdjointState {
   DevBuf<float> target, image;
   DevBuf<double> loss_part, loss;
   DevBuf<float> grad_part, grad;
+  DevBuf<float4> recs, gout;               // backward: vertex records and radiance adjoints of a chunk
   DevBuf<float> path_weight;
   int loss_grid = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -2487,7 +2488,9 @@ AdjLaunch adj_launch(vkptc_ctx* c, bool backward, int32_t& rc) {
       return l;
     }
   }
-  l.grid = c->sm_count * AdjBlocksPerSm(backward, l.block, smem, l.parity);
+  l.grid = c->sm_count * AdjBlocksPerSm(backward ? AdjKernel::kReplay : AdjKernel::kForward, l.block,
+                                         backward ? AdjForwardSmem(l.block, l.stack_cap) : smem, l.parity);
+  l.grid_reverse = c->sm_count * AdjBlocksPerSm(AdjKernel::kReverse, l.block, AdjReverseSmem(l.block, mats), l.parity);
   return l;
 }
 
@@ -2630,7 +2633,11 @@ int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float*
   int32_t rc = VKPTC_OK;
   const AdjLaunch l = adj_launch(ctx, true, rc);
   if (rc != VKPTC_OK) return rc;
-  VKPTC_CUDA(ctx, a.grad_part.alloc(static_cast<size_t>(l.grid) * stride), "gradient partials alloc");
+  VKPTC_CUDA(ctx, a.grad_part.alloc(static_cast<size_t>(l.grid_reverse) * stride), "gradient partials alloc");
+  const size_t chunk = static_cast<size_t>(std::min<uint64_t>(kAdjChunkPaths, a.stats.paths));
+  VKPTC_CUDA(ctx, a.recs.alloc(std::max<size_t>(1, chunk * kAdjVertexSlots * kAdjRecordFloat4s)),
+             "adjoint record alloc");
+  VKPTC_CUDA(ctx, a.gout.alloc(std::max<size_t>(1, chunk)), "adjoint record alloc");
   VKPTC_CUDA(ctx, a.grad.alloc(stride), "gradient alloc");
   if (path_weight) {
     VKPTC_CUDA(ctx, a.path_weight.alloc(a.stats.paths), "path weight alloc");
@@ -2641,8 +2648,8 @@ int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float*
   VKPTC_CUDA(ctx, cudaEventRecord(a.ev[2], ctx->stream), "event");
   const uint32_t replay_frame = (a.desc.flags & VKPTC_ADJ_DECORRELATED) ? a.desc.backward_frame : a.desc.frame;
   VKPTC_CUDA(ctx, LaunchAdjBackward(adj_scene(ctx), dev_settings(ctx, replay_frame), a.mat0.ptr, l, a.adj.ptr,
-                                    path_weight ? a.path_weight.ptr : nullptr, a.grad_part.ptr, a.grad.ptr,
-                                    ctx->d_err.ptr),
+                                    path_weight ? a.path_weight.ptr : nullptr, a.recs.ptr, a.gout.ptr,
+                                    a.grad_part.ptr, a.grad.ptr, ctx->d_err.ptr),
              "adjoint backward launch");
   VKPTC_CUDA(ctx, cudaEventRecord(a.ev[3], ctx->stream), "event");
   VKPTC_CUDA(ctx, cudaMemcpyAsync(grad, a.grad.ptr, stride * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
