@@ -18,7 +18,7 @@ import os
 import time
 from typing import Dict, Iterable, Optional
 
-DEFAULT_POOLS = (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+DEFAULT_POOLS = (1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24)
 DEFAULT_BLOCKS = (128, 256)
 DEFAULT_STACKS = (8, 16)
 DEFAULT_STEPS = (8, 16)
