@@ -490,6 +490,14 @@ __device__ __forceinline__ ShadeOut shade_bounce(const DevScene& s, const DevSet
       }
     }
 
+    // The last bounce samples no continuation: whatever it drew, the path ends
+    // with the radiance it has (the reference draws and discards it).
+    if (depth + 1u >= st.max_depth) {
+      P.thr = thr;
+      P.rad = rad;
+      P.rng = rng;
+      return R;
+    }
     V3 out;
     bool refracted = false;
     const V3 refl = sub(d, mul(nrm, 2.0f * dot(nrm, d)));
