@@ -51,6 +51,7 @@ struct BatchLaunch {
   int grid, block;
   int smem_entries, stack_cap, steps;
   int2* spill;
+  int2* spill_shadow;   // loop driver: the shadow stage's own spill area (it may run beside EXTEND)
   cudaStream_t stream;
   bool parity;
   bool stats;   // count traversal work (node/leaf/triangle visits)
@@ -143,12 +144,21 @@ LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int oc
                          bool watertight = false, bool effects = true, bool sdf = true, bool exotic = true);
 cudaError_t ConfigureBatchLoopSmem(size_t bytes);
 cudaError_t LaunchBatchLoopInit(const LoopPool& pool, cudaStream_t stream);
-// One iteration of the five stages; the finish stage sets `handle` (the
-// graph's while-condition; 0 outside a graph) and ctl[kLoopCtlMore].
-// marks (optional, outside a graph): 6 events recorded around the stages.
+// A second stream and two events: the shadow stage of an iteration (the
+// previous shading stage's NEE queries) then runs beside REGEN and EXTEND.
+struct LoopFork {
+  cudaStream_t side;
+  cudaEvent_t fork, join;
+};
+// One loop iteration: REGEN, EXTEND (+ SDF), the previous bounce's SHADOW
+// (+ SDF occlusion), DRAIN (finished paths to stagings), SHADE, and the
+// decision that sets `handle` (the graph's while-condition; 0 outside a graph)
+// and ctl[kLoopCtlMore].  marks (optional, outside a graph; no fork then): 6
+// events, interval k of them timing stage kLoopMarkStage[k].
+constexpr int kLoopMarkStage[5] = {0, 1, 3, 4, 2};   // regen, extend, shadow, finish (drain), shade
 cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
                                      const LoopPool& pool, const BatchLaunch& bl, const LoopGrids& grids,
                                      cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
-                                     cudaEvent_t* marks = nullptr);
+                                     cudaEvent_t* marks = nullptr, const LoopFork* fork = nullptr);
 
 }  // namespace vkptc

@@ -5,7 +5,7 @@
 // each stage as its own kernel, so a stage gets the register budget and
 // occupancy it needs (the traversal stages run at 64-80 registers, shading at
 // ~94), and the iterations are driven by the device: the stages form the body
-// of a CUDA graph while-node whose condition the finish stage sets.  One
+// of a CUDA graph while-node whose condition the last stage sets.  One
 // graph launch renders every job; no kernel ever waits on another.
 //
 // Path state is kept in two compacted generations (structure of arrays).
@@ -13,11 +13,17 @@
 //   REGEN   new camera paths from the 64-bit work counter are appended to
 //           generation `cur` until it holds `capacity` paths
 //   EXTEND  closest-hit traversal of generation `cur`, hit by position
+//   SHADOW  any-hit traversal of the NEE queries the previous SHADE queued; a
+//           visible query adds its term at its destination (a path of
+//           generation `cur` or the finished list).  It touches nothing REGEN
+//           and EXTEND touch, so in the graph it runs on a forked branch
+//           beside them and each fills the other's tail.
+//   DRAIN   the previous SHADE's finished paths to their jobs' staging slots
 //   SHADE   one bounce per path: survivors appended to generation cur^1,
 //           NEE queries to the shadow queue (with their destination), ended
 //           paths to the finished list
-//   SHADOW  any-hit traversal; a visible query adds its term at its destination
-//   FINISH  finished paths' radiance to the job's staging slot; cur ^= 1
+//   DECIDE  another iteration while paths, camera paths, queries or finished
+//           paths remain; cur ^= 1
 // With SDF primitives in some job, two load-balanced stages join them: after
 // EXTEND the SDF closest-hit test folds SDF hits into the hit buffer, and
 // before SHADOW the SDF occlusion test drops the queries an SDF occludes (one
@@ -37,7 +43,8 @@ namespace {
 
 constexpr int kLCur = 0;            // current generation
 constexpr int kLCount0 = 1;         // paths in generation 0 / 1: words 1, 2
-constexpr int kLShadow = 3, kLFin = 4;
+constexpr int kLShadow = 3;
+constexpr int kLFin0 = 12;          // finished-list length, by the generation that shaded it: words 12, 13
 constexpr int kLFetchExt = 5, kLFetchShadow = 6;
 constexpr int kLFetchSdf = 7, kLFetchSdfShadow = 11;
 constexpr int kLWork = 8;           // 64-bit path counter (words 8, 9)
@@ -178,7 +185,10 @@ __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ job
   // The count itself grows while this kernel appends; every block sizes its
   // share from the value the previous finish stage recorded.
   const uint32_t room = P.capacity - P.ctl[kLBase];
-  if (block_leader()) P.ctl[kLFetchExt] = 0u;
+  if (block_leader()) {
+    P.ctl[kLFetchExt] = 0u;
+    P.ctl[kLFetchSdf] = 0u;
+  }
   const PathSoA A = P.gen[cur];
   unsigned long long* work_next = reinterpret_cast<unsigned long long*>(P.ctl + kLWork);
   const uint32_t gthreads = gridDim.x * blockDim.x;
@@ -222,14 +232,6 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __r
   extern __shared__ int2 smem_stack[];
   const uint32_t cur = P.ctl[kLCur];
   const uint32_t n = P.ctl[kLCount0 + cur];
-  if (block_leader()) {
-    P.ctl[kLCount0 + (cur ^ 1u)] = 0u;
-    P.ctl[kLShadow] = 0u;
-    P.ctl[kLFin] = 0u;
-    P.ctl[kLFetchShadow] = 0u;
-    P.ctl[kLFetchSdf] = 0u;
-    P.ctl[kLFetchSdfShadow] = 0u;
-  }
   if (n == 0u) return;
   const TwoLevelStack stk = loop_stack(smem_stack, scap, spill, total_cap);
   TraceStats st;
@@ -312,7 +314,7 @@ __global__ void __launch_bounds__(256, (kEffects || kSdf || kExotic) ? 3 : VKPTC
       B.thr[qn] = make_float4(pr.thr.x, pr.thr.y, pr.thr.z, 0.0f);
       B.rad[qn] = make_float4(pr.rad.x, pr.rad.y, pr.rad.z, pr.segs);
     }
-    const uint32_t qf = warp_append(&P.ctl[kLFin], fin);
+    const uint32_t qf = warp_append(&P.ctl[kLFin0 + cur], fin);
     if (fin) {
       P.fin_rad[qf] = make_float4(pr.rad.x, pr.rad.y, pr.rad.z, pr.segs);
       P.fin_job[qf] = jb;
@@ -340,31 +342,47 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_lp_shadow(const DevJob* __r
   const TwoLevelStack stk = loop_stack(smem_stack, scap, spill, total_cap);
   TraceStats st;
   uint32_t lerr = 0u;
-  const LoopShadowSource src{jobs, P, P.gen[cur ^ 1u]};
+  // The queries of the previous shading stage; their survivors are generation `cur` now.
+  const LoopShadowSource src{jobs, P, P.gen[cur]};
   persistent_traverse<LoopShadowSource, true, kStats, kWt>(src, n, &P.ctl[kLFetchShadow], stk, steps, st, lerr);
   flush_stats<kStats>(ctr, st, true);
   if (lerr) atomicOr(err, lerr);
 }
 
-__global__ void __launch_bounds__(256) k_lp_finish(const DevJob* __restrict__ jobs, unsigned long long total,
-                                                   LoopPool P, cudaGraphConditionalHandle handle) {
+// Finished paths of the previous shading stage (their visible NEE terms
+// added by the shadow stage) to their jobs' staging slots; then the words the
+// coming shading stage appends to start from zero.
+__global__ void __launch_bounds__(256) k_lp_drain(const DevJob* __restrict__ jobs, LoopPool P) {
   const uint32_t cur = P.ctl[kLCur];
   if (block_leader()) {
-    // Everything this decision reads was final before this kernel started.
-    const unsigned long long work = *reinterpret_cast<const unsigned long long*>(P.ctl + kLWork);
-    const uint32_t survivors = P.ctl[kLCount0 + (cur ^ 1u)];
-    const uint32_t more = (survivors > 0u || work < total) ? 1u : 0u;
-    P.ctl[kLMore] = more;
-    P.ctl[kLBase] = survivors;
-    P.ctl[kLCur] = cur ^ 1u;
-    P.ctl[kLIter] += 1u;
-    if (handle) cudaGraphSetConditional(handle, more);
+    P.ctl[kLCount0 + (cur ^ 1u)] = 0u;
+    P.ctl[kLFin0 + cur] = 0u;
+    P.ctl[kLShadow] = 0u;
+    P.ctl[kLFetchShadow] = 0u;
+    P.ctl[kLFetchSdfShadow] = 0u;
   }
-  const uint32_t n = P.ctl[kLFin];
+  const uint32_t n = P.ctl[kLFin0 + (cur ^ 1u)];
   for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
     const DevJob& J = jobs[P.fin_job[f]];
     J.staging[P.fin_local[f]] = P.fin_rad[f];
   }
+}
+
+// Loop condition after the shading stage: another iteration while paths
+// survive, camera paths remain, or the shading stage left NEE queries or
+// finished paths for the next iteration's shadow and drain stages.
+__global__ void k_lp_decide(unsigned long long total, LoopPool P, cudaGraphConditionalHandle handle) {
+  if (threadIdx.x != 0u) return;
+  const uint32_t cur = P.ctl[kLCur];
+  const unsigned long long work = *reinterpret_cast<const unsigned long long*>(P.ctl + kLWork);
+  const uint32_t survivors = P.ctl[kLCount0 + (cur ^ 1u)];
+  const uint32_t more =
+      (survivors > 0u || work < total || P.ctl[kLShadow] > 0u || P.ctl[kLFin0 + cur] > 0u) ? 1u : 0u;
+  P.ctl[kLMore] = more;
+  P.ctl[kLBase] = survivors;
+  P.ctl[kLCur] = cur ^ 1u;
+  P.ctl[kLIter] += 1u;
+  if (handle) cudaGraphSetConditional(handle, more);
 }
 
 template <typename K>
@@ -430,7 +448,7 @@ LoopGrids BatchLoopGrids(int block, size_t smem, bool parity, bool stats, int oc
   g.extend = sm_count * blocks_per_sm(extend_fn(stats, occupancy, watertight), block, smem);
   g.shade = sm_count * blocks_per_sm(shade_fn(parity, effects, sdf, exotic), block, 0);
   g.shadow = sm_count * blocks_per_sm(shadow_fn(stats, occupancy, watertight), block, smem);
-  g.finish = sm_count * blocks_per_sm(k_lp_finish, block, 0);
+  g.finish = sm_count * blocks_per_sm(k_lp_drain, block, 0);
   g.sdf = sm_count * std::min(blocks_per_sm(k_lp_sdf, block, 0), blocks_per_sm(k_lp_sdf_shadow, block, 0));
   return g;
 }
@@ -455,12 +473,28 @@ cudaError_t LaunchBatchLoopInit(const LoopPool& pool, cudaStream_t stream) {
 cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, unsigned long long total,
                                      const LoopPool& P, const BatchLaunch& bl, const LoopGrids& g,
                                      cudaGraphConditionalHandle handle, DevCounters* ctr, uint32_t* err,
-                                     cudaEvent_t* marks) {
+                                     cudaEvent_t* marks, const LoopFork* fork) {
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
   cudaStream_t s = bl.stream;
   auto mark = [&](int i) {
     if (marks) cudaEventRecord(marks[i], s);
   };
+  // The shadow branch: the previous shading stage's NEE queries, on the side
+  // stream when forked (it only touches the shadow queue, the finished list
+  // and the radiance words of generation `cur`, none of which REGEN or EXTEND
+  // touch), else after EXTEND.
+  auto shadow_branch = [&](cudaStream_t q) {
+    if (bl.sdf) k_lp_sdf_shadow<<<g.sdf, bl.block, 0, q>>>(jobs, P, ctr);
+    shadow_fn(bl.stats, bl.occupancy, bl.watertight)<<<g.shadow, bl.block, smem, q>>>(
+        jobs, P, bl.smem_entries, bl.spill_shadow, bl.stack_cap, bl.steps, ctr, err);
+  };
+  const bool forked = fork != nullptr && marks == nullptr;
+  if (forked) {
+    cudaEventRecord(fork->fork, s);
+    cudaStreamWaitEvent(fork->side, fork->fork, 0);
+    shadow_branch(fork->side);
+    cudaEventRecord(fork->join, fork->side);
+  }
   mark(0);
   if (bl.parity) k_lp_regen<true><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
   else k_lp_regen<false><<<g.regen, bl.block, 0, s>>>(jobs, job_count, total, P);
@@ -469,15 +503,15 @@ cudaError_t LaunchBatchLoopIteration(const DevJob* jobs, uint32_t job_count, uns
                                                                       bl.steps, ctr, err);
   if (bl.sdf) k_lp_sdf<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
   mark(2);
+  if (forked) cudaStreamWaitEvent(s, fork->join, 0);
+  else shadow_branch(s);
+  mark(3);
+  k_lp_drain<<<g.finish, bl.block, 0, s>>>(jobs, P);
+  mark(4);
   const uint32_t staged = bl.sdf ? 1u : 0u;
   shade_fn(bl.parity, bl.effects, bl.sdf, bl.exotic)<<<g.shade, bl.block, 0, s>>>(jobs, P, ctr, staged);
-  mark(3);
-  if (bl.sdf) k_lp_sdf_shadow<<<g.sdf, bl.block, 0, s>>>(jobs, P, ctr);
-  shadow_fn(bl.stats, bl.occupancy, bl.watertight)<<<g.shadow, bl.block, smem, s>>>(jobs, P, bl.smem_entries, bl.spill, bl.stack_cap,
-                                                                      bl.steps, ctr, err);
-  mark(4);
-  k_lp_finish<<<g.finish, bl.block, 0, s>>>(jobs, total, P, handle);
   mark(5);
+  k_lp_decide<<<1, 32, 0, s>>>(total, P, handle);
   return cudaGetLastError();
 }
 

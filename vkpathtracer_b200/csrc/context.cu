@@ -1793,6 +1793,8 @@ struct vkptc_batch {
   cudaGraphExec_t graph = nullptr;
   std::string graph_key;
   cudaStream_t body_stream = nullptr;   // captures the device-driven loop's body
+  cudaStream_t side_stream = nullptr;   // the body's forked shadow branch
+  cudaEvent_t fork_ev[2] = {nullptr, nullptr};
   cudaEvent_t marks[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // stage timing
   size_t loop_smem_configured = 48 * 1024;
   vkptc_batch_stats stats{};
@@ -1966,8 +1968,10 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   }
   const size_t spill_entries =
       bl.stack_cap > bl.smem_entries ? static_cast<size_t>(bl.grid) * bl.block * (bl.stack_cap - bl.smem_entries) : 0;
-  if (spill_entries) VKPTC_BCUDA(b, b->spill.alloc(spill_entries), "spill alloc");
+  // The loop driver's shadow stage may run beside EXTEND: it spills into a second half.
+  if (spill_entries) VKPTC_BCUDA(b, b->spill.alloc(loop ? 2 * spill_entries : spill_entries), "spill alloc");
   bl.spill = spill_entries ? b->spill.ptr : nullptr;
+  bl.spill_shadow = spill_entries && loop ? b->spill.ptr + spill_entries : bl.spill;
   // ---- pool
   const uint32_t cap = std::max<uint32_t>(1024u, t.pool_paths ? t.pool_paths : kDefaultPoolPaths);
   const size_t n = cap;
@@ -2093,10 +2097,16 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
       VKPTC_BCUDA(b, cudaStreamBeginCaptureToGraph(b->body_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                                    cudaStreamCaptureModeRelaxed),
                   "body capture");
+      if (!b->side_stream) {
+        VKPTC_BCUDA(b, cudaStreamCreateWithFlags(&b->side_stream, cudaStreamNonBlocking), "stream");
+        VKPTC_BCUDA(b, cudaEventCreateWithFlags(&b->fork_ev[0], cudaEventDisableTiming), "fork events");
+        VKPTC_BCUDA(b, cudaEventCreateWithFlags(&b->fork_ev[1], cudaEventDisableTiming), "fork events");
+      }
       BatchLaunch bb = bl;
       bb.stream = b->body_stream;
+      const LoopFork fork{b->side_stream, b->fork_ev[0], b->fork_ev[1]};
       const cudaError_t el = LaunchBatchLoopIteration(b->d_jobs.ptr, njobs, total, LP, bb, lg, handle, b->d_ctr.ptr,
-                                                      b->d_err.ptr);
+                                                      b->d_err.ptr, nullptr, &fork);
       cudaGraph_t body = nullptr;
       const cudaError_t ee = cudaStreamEndCapture(b->body_stream, &body);
       if (el != cudaSuccess) return bcuda(b, el, "loop body");
@@ -2165,7 +2175,7 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
         for (int i = 0; i < 5; ++i) {
           float m = 0.0f;
           cudaEventElapsedTime(&m, b->marks[i], b->marks[i + 1]);
-          stage_ms[i] += m;
+          stage_ms[kLoopMarkStage[i]] += m;
         }
       }
       if (!more) break;
@@ -2197,8 +2207,11 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
   b->stats.shadow_nodes = dc.shadow_nodes;
   b->stats.shadow_tris = dc.shadow_tris;
   b->stats.device_ms = ms;
-  // init, then one persistent kernel or five stage kernels per iteration, then accumulate per job
-  b->stats.kernel_launches = 1u + (loop ? 5ull * iterations : 1ull) + static_cast<uint64_t>(table.size());
+  // init, then one persistent kernel or the loop's stage kernels per iteration (regen, extend,
+  // shadow, drain, shade, decide; the two SDF stages when a job has SDF primitives), then
+  // accumulate per job
+  b->stats.kernel_launches = 1u + (loop ? (bl.sdf ? 8ull : 6ull) * iterations : 1ull) +
+                             static_cast<uint64_t>(table.size());
   b->stats.iterations = iterations;
   b->stats.graph_used = graph_used ? 1u : 0u;
   b->stats.grid = static_cast<uint32_t>(bl.grid);
@@ -2251,15 +2264,18 @@ int32_t vkptc_batch_destroy(vkptc_batch* b) {
   release_graph(b);
   for (vkptc_ctx* c : b->jobs) vkptc_destroy(c);
   b->jobs.clear();
-  cudaStream_t st = b->stream, bs = b->body_stream;
+  cudaStream_t st = b->stream, bs = b->body_stream, ss = b->side_stream;
   cudaEvent_t marks[6];
   std::copy(std::begin(b->marks), std::end(b->marks), marks);
-  cudaEvent_t e0 = b->ev0, e1 = b->ev1;
+  cudaEvent_t e0 = b->ev0, e1 = b->ev1, f0 = b->fork_ev[0], f1 = b->fork_ev[1];
   delete b;
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
+  if (f0) cudaEventDestroy(f0);
+  if (f1) cudaEventDestroy(f1);
   if (st) cudaStreamDestroy(st);
   if (bs) cudaStreamDestroy(bs);
+  if (ss) cudaStreamDestroy(ss);
   for (cudaEvent_t e : marks)
     if (e) cudaEventDestroy(e);
   return VKPTC_OK;
