@@ -76,18 +76,20 @@ DEFAULT_MODES = ("loop", "persistent")
 def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS,
                stacks=DEFAULT_STACKS, steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1,
                repeats: int = 2, use_cache: bool = True, log: Optional[callable] = None,
-               refine_samples: Optional[int] = 0) -> Dict:
+               refine_samples: Optional[int] = 0, refine_top: int = 4) -> Dict:
     """Returns {"mode", "pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials"}.
 
     Coordinate search per driver: the pool capacity first (other parameters
     at their defaults), then block size x stack entries x steps x register
     variant; the fastest over both drivers wins.  Trials replay a CUDA graph
     (the way the runs are timed), so the loop driver is measured as it runs.
-    Then the winner and the pool sizes next to it are timed again on a longer
-    run (refine_samples per job, 0 = every sample, None = no refinement):
-    short trials under-fill large pools."""
+    Then the fastest trials of the refine_top fastest (driver, block size,
+    stack entries) pairs, each with its pool and the pool sizes next to it, are
+    timed again on a longer run (refine_samples per job,
+    0 = every sample, None = no refinement): short trials under-fill large
+    pools and rank close shapes only roughly."""
     cache = _load_cache() if use_cache else {}
-    ckey = f"batch/{_gpu_name()}/{'+'.join(modes)}/r{refine_samples}/{key}"   # r0: refined on the full run
+    ckey = f"batch/{_gpu_name()}/{'+'.join(modes)}/r{refine_samples}t{refine_top}/{key}"   # r0: refined on the full run
     if use_cache and ckey in cache:
         return dict(cache[ckey], cached=True)
     best = None
@@ -132,9 +134,25 @@ def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks
         if "ms" in tr and (tr["mode"] not in per_mode or tr["ms"] < per_mode[tr["mode"]]["ms"]):
             per_mode[tr["mode"]] = dict(tr)
     if refine_samples is not None and (refine_samples == 0 or refine_samples > sample_limit):
-        base = {k: v for k, v in best.items() if k != "ms"}
-        i = list(pools).index(base["pool_paths"]) if base["pool_paths"] in pools else -1
-        cands = [base] + [dict(base, pool_paths=pools[j]) for j in (i - 1, i + 1) if i >= 0 and 0 <= j < len(pools)]
+        # For the refine_top fastest (driver, block size, stack entries) pairs of
+        # the short trials, their fastest trial with its pool and the pool sizes
+        # next to it: the short trials rank shapes only roughly (differences of
+        # ~1 % flip between short and full runs).
+        ranked = sorted((tr for tr in trials if "ms" in tr), key=lambda tr: tr["ms"])
+        shapes, cands = [], []
+        for tr in ranked:
+            shape = tuple(tr[k] for k in ("mode", "block_size", "stack_depth"))
+            if shape in shapes:
+                continue
+            shapes.append(shape)
+            base = {k: v for k, v in tr.items() if k != "ms"}
+            i = list(pools).index(base["pool_paths"]) if base["pool_paths"] in pools else -1
+            for c in [base] + [dict(base, pool_paths=pools[j]) for j in (i - 1, i + 1)
+                               if i >= 0 and 0 <= j < len(pools)]:
+                if c not in cands:
+                    cands.append(c)
+            if len(shapes) >= refine_top:
+                break
         refined = None
         for c in cands:
             try:
