@@ -4,9 +4,10 @@ Sweeps the launch parameters the kernels expose -- the driver (the
 cooperative persistent kernel or the device-driven stage loop), path-pool
 capacity (the device queue capacity), block size, traversal-stack entries
 kept in shared memory, traversal steps between warp refills and the register
-variant -- on a short run of the actual workload (one sample per job), keeps
-the fastest, and caches the choice in a JSON file keyed by GPU name and
-workload signature.  Films do not depend on these parameters
+variant -- on the actual workload (the whole job set for the loop driver,
+one sample per job for the persistent one, whose winner is then re-timed on
+the whole set), keeps the fastest, and caches the choice in a JSON file keyed
+by GPU name and workload signature.  Films do not depend on these parameters
 (tests/test_gpu_batch.py), only speed does.
 """
 from __future__ import annotations
@@ -76,96 +77,107 @@ DEFAULT_MODES = ("loop", "persistent")
 def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS,
                stacks=DEFAULT_STACKS, steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1,
                repeats: int = 2, use_cache: bool = True, log: Optional[callable] = None,
-               refine_samples: Optional[int] = 0, refine_top: int = 4) -> Dict:
-    """Returns {"mode", "pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials"}.
+               refine_samples: Optional[int] = 0, refine_top: int = 1, full_modes=("loop",)) -> Dict:
+    """Returns {"mode", "pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials",
+    "per_mode"}.
 
     Coordinate search per driver: the pool capacity first (other parameters
     at their defaults), then block size x stack entries x steps x register
-    variant; the fastest over both drivers wins.  Trials replay a CUDA graph
-    (the way the runs are timed), so the loop driver is measured as it runs.
-    Then the fastest trials of the refine_top fastest (driver, block size,
-    stack entries) pairs, each with its pool and the pool sizes next to it, are
-    timed again on a longer run (refine_samples per job,
-    0 = every sample, None = no refinement): short trials under-fill large
-    pools and rank close shapes only roughly."""
+    variant at that pool, then the pool sizes next to it with the chosen
+    shape.  Trials replay a CUDA graph (the way the runs are timed), so the
+    loop driver is measured as it runs.  Drivers in full_modes are searched on
+    the whole workload (refine_samples per job; 0 = every sample): short runs
+    under-fill large pools and rank close shapes only roughly (differences of
+    ~1 % flip between short and full runs).  The others are searched on short
+    runs (sample_limit per job), and the fastest trials of their refine_top
+    fastest (block size, stack entries) pairs, each with its pool and the pool
+    sizes next to it, are timed again on the whole workload (refine_samples
+    None: no refinement, the short-run times decide).  The fastest driver on
+    the whole workload wins."""
     cache = _load_cache() if use_cache else {}
-    ckey = f"batch/{_gpu_name()}/{'+'.join(modes)}/r{refine_samples}t{refine_top}/{key}"   # r0: refined on the full run
+    ckey = (f"batch/{_gpu_name()}/{'+'.join(modes)}/r{refine_samples}t{refine_top}"
+            f"f{'+'.join(m for m in modes if m in full_modes)}/{key}")
     if use_cache and ckey in cache:
         return dict(cache[ckey], cached=True)
-    best = None
     trials = []
     t0 = time.time()
 
     def measure(cfg, samples):
         mode = cfg["mode"]
-        args = {k: v for k, v in cfg.items() if k not in ("mode", "ms")}
+        args = {k: v for k, v in cfg.items() if k not in ("mode", "ms", "samples")}
         batch.run(mode, sample_limit=samples, use_graph=True, **args)   # capture
         return min(batch.run(mode, sample_limit=samples, use_graph=True, **args)["device_ms"] for _ in range(repeats))
 
-    def trial(cfg):
-        nonlocal best
+    def trial(cfg, samples):
         try:
-            ms = measure(cfg, sample_limit)
+            ms = measure(cfg, samples)
         except Exception as e:   # a shape that does not fit (e.g. shared memory) is skipped
-            trials.append(dict(cfg, error=str(e)))
+            trials.append(dict(cfg, error=str(e), samples=samples))
             return None
-        trials.append(dict(cfg, ms=ms))
+        trials.append(dict(cfg, ms=ms, samples=samples))
         if log:
             log(trials[-1])
-        if best is None or ms < best["ms"]:
-            best = dict(cfg, ms=ms)
         return ms
 
-    for mode in modes:
-        mode_best = None
-        for pool in pools:
-            cfg = {"mode": mode, "pool_paths": pool, "block_size": 0, "stack_depth": 0, "steps": 0, "occupancy": 0}
-            ms = trial(cfg)
-            if ms is not None and (mode_best is None or ms < mode_best[1]):
-                mode_best = (pool, ms)
-        pool = mode_best[0] if mode_best else pools[0]
-        for block, stack, st, occ in itertools.product(blocks, stacks, steps, occupancy):
-            trial({"mode": mode, "pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st,
-                   "occupancy": occ})
-    if best is None:
-        raise RuntimeError("autotune: no launch configuration ran")
+    def neighbours(cfg):
+        i = list(pools).index(cfg["pool_paths"]) if cfg["pool_paths"] in pools else -1
+        return [dict(cfg, pool_paths=pools[j]) for j in (i - 1, i + 1) if i >= 0 and 0 <= j < len(pools)]
+
+    full = refine_samples if refine_samples is not None else sample_limit
     per_mode = {}
-    for tr in trials:
-        if "ms" in tr and (tr["mode"] not in per_mode or tr["ms"] < per_mode[tr["mode"]]["ms"]):
-            per_mode[tr["mode"]] = dict(tr)
-    if refine_samples is not None and (refine_samples == 0 or refine_samples > sample_limit):
-        # For the refine_top fastest (driver, block size, stack entries) pairs of
-        # the short trials, their fastest trial with its pool and the pool sizes
-        # next to it: the short trials rank shapes only roughly (differences of
-        # ~1 % flip between short and full runs).
-        ranked = sorted((tr for tr in trials if "ms" in tr), key=lambda tr: tr["ms"])
+    for mode in modes:
+        samples = full if mode in full_modes else sample_limit
+        mine = []   # (ms, cfg) of this driver's search
+
+        def run(cfg):
+            ms = trial(cfg, samples)
+            if ms is not None:
+                mine.append((ms, cfg))
+            return ms
+
+        for pool in pools:
+            run({"mode": mode, "pool_paths": pool, "block_size": 0, "stack_depth": 0, "steps": 0, "occupancy": 0})
+        if not mine:
+            continue
+        pool = min(mine, key=lambda r: r[0])[1]["pool_paths"]
+        for block, stack, st, occ in itertools.product(blocks, stacks, steps, occupancy):
+            run({"mode": mode, "pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st,
+                 "occupancy": occ})
+        tried = [c for _, c in mine]
+        for c in neighbours(min(mine, key=lambda r: r[0])[1]):
+            if c not in tried:
+                run(c)
+        if samples == full:
+            ms, cfg = min(mine, key=lambda r: r[0])
+            per_mode[mode] = dict(cfg, ms=ms, samples=samples)
+            continue
+        if refine_samples is None:
+            ms, cfg = min(mine, key=lambda r: r[0])
+            per_mode[mode] = dict(cfg, ms=ms, samples=samples)
+            continue
         shapes, cands = [], []
-        for tr in ranked:
-            shape = tuple(tr[k] for k in ("mode", "block_size", "stack_depth"))
+        for _, cfg in sorted(mine, key=lambda r: r[0]):
+            shape = (cfg["block_size"], cfg["stack_depth"])
             if shape in shapes:
                 continue
             shapes.append(shape)
-            base = {k: v for k, v in tr.items() if k != "ms"}
-            i = list(pools).index(base["pool_paths"]) if base["pool_paths"] in pools else -1
-            for c in [base] + [dict(base, pool_paths=pools[j]) for j in (i - 1, i + 1)
-                               if i >= 0 and 0 <= j < len(pools)]:
+            for c in [cfg] + neighbours(cfg):
                 if c not in cands:
                     cands.append(c)
             if len(shapes) >= refine_top:
                 break
-        refined = None
+        refined = []
         for c in cands:
-            try:
-                ms = measure(c, refine_samples)
-            except Exception as e:
-                trials.append(dict(c, error=str(e), refine_samples=refine_samples))
-                continue
-            trials.append(dict(c, ms=ms, refine_samples=refine_samples))
-            if refined is None or ms < refined["ms"]:
-                refined = dict(c, ms=ms)
-        if refined is not None:
-            best = dict(refined, refine_samples=refine_samples)
-            per_mode[best["mode"]] = {k: v for k, v in best.items()}
+            ms = trial(c, full)
+            if ms is not None:
+                refined.append((ms, c))
+        if refined:
+            ms, cfg = min(refined, key=lambda r: r[0])
+            per_mode[mode] = dict(cfg, ms=ms, samples=full)
+    if not per_mode:
+        raise RuntimeError("autotune: no launch configuration ran")
+    best = dict(min(per_mode.values(), key=lambda r: r["ms"]))
+    best["refine_samples"] = best.pop("samples")
     best["per_mode"] = per_mode
     best["trials"] = len(trials)
     best["tune_seconds"] = time.time() - t0
