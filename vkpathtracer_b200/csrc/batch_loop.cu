@@ -177,6 +177,35 @@ __global__ void k_lp_init(uint32_t* ctl) {
   if (i < static_cast<uint32_t>(kLoopCtlWords)) ctl[i] = 0u;
 }
 
+// Order in which REGEN hands out a sample's pixels: 1 = 8x4 tiles, band of
+// four rows by band (a warp's 32 camera rays cover a compact 8x4 block);
+// 0 = scanline order.  Each path still writes its own pixel's staging slot,
+// so films do not depend on the order.
+#ifndef VKPTC_TILE_ORDER
+#define VKPTC_TILE_ORDER 1
+#endif
+// The i-th pixel (y*W+x) of the tile order: bands of 4 rows (the last may be
+// shorter), each band cut into 8-pixel-wide tiles left to right (the last may
+// be narrower), each tile in row order.  A bijection on [0, W*H).
+__device__ __forceinline__ uint32_t tile_order_pixel(uint32_t i, uint32_t W, uint32_t H) {
+  const uint32_t band = i / (4u * W);
+  const uint32_t y0 = 4u * band;
+  const uint32_t bh = min(4u, H - y0);
+  const uint32_t r = i - y0 * W;                 // index inside the band
+  const uint32_t full = W / 8u;                  // full-width tiles in the band
+  uint32_t x, y;
+  if (r < full * 8u * bh) {
+    const uint32_t t = r / (8u * bh), k = r - t * 8u * bh;
+    x = 8u * t + (k & 7u);
+    y = y0 + (k >> 3);
+  } else {                                       // the narrow last tile
+    const uint32_t tw = W - 8u * full, k = r - full * 8u * bh;
+    x = 8u * full + k % tw;
+    y = y0 + k / tw;
+  }
+  return y * W + x;
+}
+
 template <bool kParity>
 __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ jobs, uint32_t job_count,
                                                   unsigned long long total, LoopPool P) {
@@ -207,9 +236,15 @@ __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ job
     if (ok) {
       const uint32_t jb = find_job(jobs, job_count, g);
       const DevJob& J = jobs[jb];
-      const uint32_t local = static_cast<uint32_t>(g - J.path_base);
-      const uint32_t sl = local / J.pixels, px = local - sl * J.pixels;
       const uint32_t W = J.settings.width;
+      const uint32_t idx = static_cast<uint32_t>(g - J.path_base);
+      const uint32_t sl = idx / J.pixels;
+#if VKPTC_TILE_ORDER
+      const uint32_t px = tile_order_pixel(idx - sl * J.pixels, W, J.settings.height);
+#else
+      const uint32_t px = idx - sl * J.pixels;
+#endif
+      const uint32_t local = sl * J.pixels + px;   // the staging slot: sample-major, then pixel (y*W+x)
       V3 o, d;
       uint64_t rng;
       camera_path<kParity>(J.scene, J.settings, px % W, px / W, J.first_sample + sl, o, d, rng);
