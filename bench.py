@@ -170,7 +170,7 @@ def make_jobs(count: int, seed: int = 5):
 # The CPU baseline renders this fraction of every job's pixels (a seeded random
 # subset, distinct pixels) at the job's full spp, in both the reference arm and
 # the cpu_baseline leg of this arm.
-PIXEL_FRACTION = 0.01
+PIXEL_FRACTION = 0.02
 CPU_TRACER = ("ScalarCpuPathTracer::render_sample_pixels on a pool of {t} worker threads created once per "
               "call (one tracer per worker and job over the job's shared CpuBvhAccelerator, as "
               "TiledCpuPathTracer's tiles share theirs); a chunk of pixels renders all its samples in order")
