@@ -528,13 +528,16 @@ typedef struct vkptc_batch_stats {
   uint32_t pool_paths;
   uint32_t stack_depth;
   uint32_t steps;
-  uint32_t iterations;       /* pool iterations (stage rounds) of the last persistent/loop run */
+  uint32_t iterations;       /* pool iterations (stage rounds) of the last persistent/loop run; the loop
+                                driver traces a round's NEE queries in the next round, so it runs one
+                                round more than the persistent driver */
   /* traversal work (filled when vkptc_config.collect_stats = 1) */
   uint64_t ext_rays, ext_nodes, ext_tris;
   uint64_t shadow_queries, shadow_nodes, shadow_tris;
   /* loop driver without a graph and vkptc_config.stage_timing = 1: device
    * time of each stage summed over the iterations (regen, extend, shade,
-   * shadow, finish; CUDA events around every stage launch) */
+   * shadow, finish = the drain of ended paths to the stagings; CUDA events
+   * around every stage launch, the stages then run one after the other) */
   double stage_ms[5];
 } vkptc_batch_stats;
 
