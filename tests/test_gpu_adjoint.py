@@ -200,6 +200,30 @@ def test_decorrelated_backward_replays_the_chosen_frame(problem):
     t.forward(p)
 
 
+def test_recorded_forward_gives_the_replayed_gradient(problem):
+    """An ordinary forward writes its paths' vertex records and the backward
+    skips the replay; a decorrelated setup whose backward frame is the
+    forward's replays the same paths.  Both gradients, with and without path
+    weights, are bit-identical, and a weighted backward leaves the records
+    for the next one untouched."""
+    t, sc, st, target, p, loss, grad = problem
+    w = np.random.default_rng(3).uniform(0.0, 2.0, st.width * st.height * 8).astype(np.float32)
+    w[::7] = 0.0
+    t.adjoint_setup(8, target)
+    t.forward(p)
+    rec_plain = t.backward()
+    rec_weighted = t.backward(path_weight=w)
+    assert np.array_equal(t.backward(), rec_plain)
+    t.adjoint_setup(8, target, frame=0, decorrelated=True, backward_frame=0)
+    t.forward(p)
+    assert np.array_equal(t.backward(), rec_plain)
+    assert np.array_equal(t.backward(path_weight=w), rec_weighted)
+    assert np.array_equal(rec_plain, grad)
+    assert not np.array_equal(rec_weighted, rec_plain)
+    t.adjoint_setup(8, target)
+    t.forward(p)
+
+
 def test_gradient_descent_lowers_loss():
     t, sc, st = setup(32, 32, 8)
     t.adjoint_setup(8)

@@ -128,9 +128,13 @@ __device__ __forceinline__ float4 adj_primal(const DevScene& s, const DevSetting
 }
 
 // 102 registers (5 blocks of 128 threads per SM): 1.98 -> 1.87 ms per forward pass.
-template <bool kParity>
+// kRecord: the forward also writes every path's vertex records (recs, the
+// backward's layout with all paths as one chunk) and their count (nrec), so
+// a backward over the same paths needs no replay.
+template <bool kParity, bool kRecord>
 __global__ void __launch_bounds__(128, 5) k_adj_forward(DevScene s, DevSettings st, const float* mat0, uint32_t spp,
-                                                     uint32_t first_sample, int cap, float4* rad, uint32_t* err) {
+                                                     uint32_t first_sample, int cap, float4* rad, AdjRec* recs,
+                                                     uint32_t* nrec_out, uint32_t* err) {
   extern __shared__ int2 smem_stack[];
   SmemStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), cap};
   const uint32_t npx = st.width * st.height;
@@ -139,9 +143,15 @@ __global__ void __launch_bounds__(128, 5) k_adj_forward(DevScene s, DevSettings 
   for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < n;
        j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     const uint32_t sl = static_cast<uint32_t>(j / npx), p = static_cast<uint32_t>(j % npx);
-    uint32_t nrec;
-    rad[j] = adj_primal<kParity, false>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk, local_err,
-                                        nullptr, nrec);
+    uint32_t nrec = 0u;
+    if (kRecord) {
+      rad[j] = adj_primal<kParity, true>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk, local_err,
+                                         recs + j, nrec, static_cast<uint32_t>(n));
+      nrec_out[j] = nrec;
+    } else {
+      rad[j] = adj_primal<kParity, false>(s, st, mat0, p % st.width, p / st.width, first_sample + sl, stk, local_err,
+                                          nullptr, nrec);
+    }
   }
   if (local_err) atomicOr(err, local_err);
 }
@@ -380,6 +390,33 @@ __global__ void __launch_bounds__(128, 5) k_adj_replay(DevScene s, DevSettings s
   if (local_err) atomicOr(err, local_err);
 }
 
+// What the replay hands the reverse sweep, for paths the forward recorded
+// (the same paths): each path's radiance adjoint (zero where the film
+// dropped or clamped the sample, the path's weight applied) and its record
+// count (0: nothing to sweep).
+__global__ void __launch_bounds__(256) k_adj_gout(DevSettings st, const float4* adj, const float* path_weight,
+                                                  const float4* rad, const uint32_t* nrec_fwd, uint32_t count,
+                                                  float4* gout) {
+  const uint32_t npx = st.width * st.height;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    float4 a = adj[i % npx];
+    if (path_weight) {
+      const float pw = path_weight[i];
+      a = make_float4(a.x * pw, a.y * pw, a.z * pw, 0.0f);
+    }
+    V3 g = mk(0.0f, 0.0f, 0.0f);
+    uint32_t nrec = 0u;
+    if (a.x != 0.0f || a.y != 0.0f || a.z != 0.0f) {
+      const float4 rv = rad[i];
+      const float fc = st.firefly_clamp;
+      g = mk((fc > 0.0f && rv.x > fc) ? 0.0f : a.x, (fc > 0.0f && rv.y > fc) ? 0.0f : a.y,
+             (fc > 0.0f && rv.z > fc) ? 0.0f : a.z);
+      nrec = (isfinite(rv.x) && isfinite(rv.y) && isfinite(rv.z)) ? nrec_fwd[i] : 0u;
+    }
+    gout[i] = make_float4(g.x, g.y, g.z, __uint_as_float(nrec));
+  }
+}
+
 // The reverse sweep of one chunk: per-warp gradient slots in shared memory,
 // then one partial per block, added to the partials of the earlier chunks
 // (accumulate) in a fixed order, so the gradient is deterministic.
@@ -440,8 +477,8 @@ int AdjBlocksPerSm(AdjKernel k, int block, size_t smem, bool parity) {
   int n = 0;
   switch (k) {
     case AdjKernel::kForward:
-      if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<true>, block, smem);
-      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<false>, block, smem);
+      if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<true, false>, block, smem);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_forward<false, false>, block, smem);
       break;
     case AdjKernel::kReplay:
       if (parity) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_replay<true>, block, smem);
@@ -458,8 +495,10 @@ int AdjBlocksPerSm(AdjKernel k, int block, size_t smem, bool parity) {
 cudaError_t ConfigureAdjSmem(size_t bytes) {
   const int b = static_cast<int>(bytes);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_adj_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-  if ((e = cudaFuncSetAttribute(k_adj_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  if ((e = cudaFuncSetAttribute(k_adj_forward<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  if ((e = cudaFuncSetAttribute(k_adj_forward<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  if ((e = cudaFuncSetAttribute(k_adj_forward<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+  if ((e = cudaFuncSetAttribute(k_adj_forward<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
   if ((e = cudaFuncSetAttribute(k_adj_replay<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
   if ((e = cudaFuncSetAttribute(k_adj_replay<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
   if ((e = cudaFuncSetAttribute(k_adj_reverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
@@ -467,12 +506,22 @@ cudaError_t ConfigureAdjSmem(size_t bytes) {
 }
 
 cudaError_t LaunchAdjForward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
-                             float4* rad, uint32_t* err) {
+                             float4* rad, uint32_t* err, float4* recs, uint32_t* nrec) {
   const size_t smem = AdjForwardSmem(l.block, l.stack_cap);
-  if (l.parity)
-    k_adj_forward<true><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, rad, err);
+  AdjRec* r = reinterpret_cast<AdjRec*>(recs);
+  const bool rec = recs != nullptr && nrec != nullptr;
+  if (l.parity && rec)
+    k_adj_forward<true, true><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, rad,
+                                                                   r, nrec, err);
+  else if (l.parity)
+    k_adj_forward<true, false><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap,
+                                                                    rad, nullptr, nullptr, err);
+  else if (rec)
+    k_adj_forward<false, true><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap,
+                                                                    rad, r, nrec, err);
   else
-    k_adj_forward<false><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap, rad, err);
+    k_adj_forward<false, false><<<l.grid, l.block, smem, l.stream>>>(s, st, mat0, l.spp, l.first_sample, l.stack_cap,
+                                                                     rad, nullptr, nullptr, err);
   return cudaGetLastError();
 }
 
@@ -486,11 +535,23 @@ cudaError_t LaunchAdjLoss(const DevSettings& st, uint32_t spp, const float4* rad
 
 cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
                               const float4* adj, const float* path_weight, float4* recs, float4* gout,
-                              float* grad_part, float* grad, uint32_t* err) {
+                              float* grad_part, float* grad, uint32_t* err, const float4* fwd_rad,
+                              const uint32_t* fwd_nrec) {
   const size_t smem_replay = AdjForwardSmem(l.block, l.stack_cap);
   const size_t smem_rev = AdjReverseSmem(l.block, s.material_count);
   const uint64_t n = static_cast<uint64_t>(st.width) * st.height * l.spp;
   AdjRec* r = reinterpret_cast<AdjRec*>(recs);
+  if (fwd_rad != nullptr && fwd_nrec != nullptr && n <= kAdjChunkPaths) {
+    // the forward recorded these paths: no replay
+    const uint32_t count = static_cast<uint32_t>(n);
+    k_adj_gout<<<static_cast<int>(std::min<uint64_t>(4096, (n + 255) / 256)), 256, 0, l.stream>>>(
+        st, adj, path_weight, fwd_rad, fwd_nrec, count, gout);
+    if (l.parity) k_adj_reverse<true><<<l.grid_reverse, l.block, smem_rev, l.stream>>>(s, st, count, r, gout, grad_part, 0);
+    else k_adj_reverse<false><<<l.grid_reverse, l.block, smem_rev, l.stream>>>(s, st, count, r, gout, grad_part, 0);
+    const uint32_t stride = s.material_count * kAdjParams;
+    k_adj_grad_reduce<<<(stride + 127) / 128, 128, 0, l.stream>>>(grad_part, l.grid_reverse, stride, grad);
+    return cudaGetLastError();
+  }
   for (uint64_t base = 0; base < n; base += kAdjChunkPaths) {
     const uint32_t count = static_cast<uint32_t>(std::min<uint64_t>(kAdjChunkPaths, n - base));
     const int acc = base > 0 ? 1 : 0;

@@ -25,8 +25,11 @@ struct AdjLaunch {
 // in w the bits of a 32-bit hash of the path's discrete decisions.
 // mat0 (16 floats per material) drives the Russian-roulette probabilities
 // and decisions; pass the scene's own table for the ordinary estimator.
+// recs and nrec (optional; at most kAdjChunkPaths paths): every path's vertex
+// records in the backward's layout (all paths one chunk) and their count, so
+// that a backward over the same paths skips its replay.
 cudaError_t LaunchAdjForward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
-                             float4* rad, uint32_t* err);
+                             float4* rad, uint32_t* err, float4* recs = nullptr, uint32_t* nrec = nullptr);
 
 // Image (sample-order accumulation exactly as the film does), loss partials
 // per block, and the per-pixel adjoint dL/d(sample radiance) (0 without a target).
@@ -45,10 +48,13 @@ constexpr size_t kAdjVertexSlots = 8;       // records per path (the maximum dep
 // partials grad_part[block][7 * materials] add up over the chunks; then the
 // fixed-order reduction into grad (7 floats per material).  path_weight
 // (optional, one per path) scales each path's adjoint.  The paths replayed
-// are those of st.frame (the forward's, or independent ones).
+// are those of st.frame (the forward's, or independent ones).  fwd_rad and
+// fwd_nrec (optional): the radiance and record counts of a forward that
+// recorded these same paths into recs; the replay is then skipped.
 cudaError_t LaunchAdjBackward(const DevScene& s, const DevSettings& st, const float* mat0, const AdjLaunch& l,
                               const float4* adj, const float* path_weight, float4* recs, float4* gout,
-                              float* grad_part, float* grad, uint32_t* err);
+                              float* grad_part, float* grad, uint32_t* err, const float4* fwd_rad = nullptr,
+                              const uint32_t* fwd_nrec = nullptr);
 
 enum class AdjKernel { kForward, kReplay, kReverse };
 size_t AdjBackwardSmem(int block, int stack_cap, uint32_t materials);

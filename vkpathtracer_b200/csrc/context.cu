@@ -94,6 +94,8 @@ struct AdjointState {
   DevBuf<double> loss_part, loss;
   DevBuf<float> grad_part, grad;
   DevBuf<float4> recs, gout;               // backward: vertex records and radiance adjoints of a chunk
+  DevBuf<uint32_t> fwd_nrec;               // records per path of a forward that recorded its paths
+  bool recorded = false;                   // recs hold every path of the last forward (no replay needed)
   DevBuf<float> path_weight;
   int loss_grid = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -2573,6 +2575,7 @@ int32_t vkptc_adjoint_setup(vkptc_ctx* ctx, const vkptc_adjoint_desc* desc, cons
   a.has_target = target_rgb != nullptr;
   a.setup = true;
   a.forward_done = false;
+  a.recorded = false;
   a.stats = vkptc_adjoint_stats{};
   a.stats.paths = paths;
   ctx->last_error.clear();
@@ -2606,8 +2609,20 @@ int32_t vkptc_forward(vkptc_ctx* ctx, const float* params, uint32_t param_count,
   if (rc != VKPTC_OK) return rc;
   VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_err.ptr, 0, sizeof(uint32_t), ctx->stream), "error clear");
   const DevSettings st = dev_settings(ctx, a.desc.frame);
+  // With the backward replaying the forward's own paths and all of them one
+  // chunk, the forward writes the vertex records itself and the backward
+  // skips the replay (the same records, so the same gradient).
+  const bool record = !(a.desc.flags & VKPTC_ADJ_DECORRELATED) && a.stats.paths <= kAdjChunkPaths;
+  a.recorded = false;
+  if (record) {
+    VKPTC_CUDA(ctx, a.recs.alloc(std::max<size_t>(1, a.stats.paths * kAdjVertexSlots * kAdjRecordFloat4s)),
+               "adjoint record alloc");
+    VKPTC_CUDA(ctx, a.fwd_nrec.alloc(std::max<size_t>(1, a.stats.paths)), "adjoint record alloc");
+  }
   VKPTC_CUDA(ctx, cudaEventRecord(a.ev[0], ctx->stream), "event");
-  VKPTC_CUDA(ctx, LaunchAdjForward(adj_scene(ctx), st, a.mat0.ptr, l, a.rad.ptr, ctx->d_err.ptr), "adjoint forward launch");
+  VKPTC_CUDA(ctx, LaunchAdjForward(adj_scene(ctx), st, a.mat0.ptr, l, a.rad.ptr, ctx->d_err.ptr,
+                                   record ? a.recs.ptr : nullptr, record ? a.fwd_nrec.ptr : nullptr),
+             "adjoint forward launch");
   VKPTC_CUDA(ctx, LaunchAdjLoss(st, a.desc.spp, a.rad.ptr, a.has_target ? a.target.ptr : nullptr, a.image.ptr, a.adj.ptr,
                                 a.loss_part.ptr, a.loss.ptr, a.loss_grid, ctx->stream),
              "adjoint loss launch");
@@ -2628,6 +2643,7 @@ int32_t vkptc_forward(vkptc_ctx* ctx, const float* params, uint32_t param_count,
   a.stats.block = static_cast<uint32_t>(l.block);
   if (loss) *loss = host_loss;
   a.forward_done = true;
+  a.recorded = record;
   ctx->last_error.clear();
   return VKPTC_OK;
 }
@@ -2663,9 +2679,11 @@ int32_t vkptc_backward_weighted(vkptc_ctx* ctx, const float* path_weight, float*
   VKPTC_CUDA(ctx, cudaMemsetAsync(ctx->d_err.ptr, 0, sizeof(uint32_t), ctx->stream), "error clear");
   VKPTC_CUDA(ctx, cudaEventRecord(a.ev[2], ctx->stream), "event");
   const uint32_t replay_frame = (a.desc.flags & VKPTC_ADJ_DECORRELATED) ? a.desc.backward_frame : a.desc.frame;
+  const bool use_records = a.recorded && !(a.desc.flags & VKPTC_ADJ_DECORRELATED);
   VKPTC_CUDA(ctx, LaunchAdjBackward(adj_scene(ctx), dev_settings(ctx, replay_frame), a.mat0.ptr, l, a.adj.ptr,
                                     path_weight ? a.path_weight.ptr : nullptr, a.recs.ptr, a.gout.ptr,
-                                    a.grad_part.ptr, a.grad.ptr, ctx->d_err.ptr),
+                                    a.grad_part.ptr, a.grad.ptr, ctx->d_err.ptr, use_records ? a.rad.ptr : nullptr,
+                                    use_records ? a.fwd_nrec.ptr : nullptr),
              "adjoint backward launch");
   VKPTC_CUDA(ctx, cudaEventRecord(a.ev[3], ctx->stream), "event");
   VKPTC_CUDA(ctx, cudaMemcpyAsync(grad, a.grad.ptr, stride * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
