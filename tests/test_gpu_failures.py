@@ -12,7 +12,9 @@
   accelerator build (src/pathtracer/CpuBvhAccelerator.cpp:173-247), an
   out-of-range material index is clamped to the last material
   (src/pathtracer/ScalarCpuPathTracer.cpp:1058, 1171); arrays the ABI cannot
-  read (a null pointer with a non-zero count) are VKPTC_INVALID_ARGUMENT.
+  read (a null pointer with a non-zero count), and instance ranges of more
+  triangles than the wide BVH's leaf references reach (2^28 - 8), are
+  VKPTC_INVALID_ARGUMENT.
 """
 import ctypes
 
@@ -125,5 +127,12 @@ def test_unreadable_scene_arrays_are_invalid_argument():
         v, keep = scene_view(sc)
         v.instances = None
         assert native.load().vkptc_load_scene(t._ctx, ctypes.byref(v)) == native.INVALID_ARGUMENT
+        # instance ranges adding up to more triangles than a wide-BVH leaf can reference
+        # (checked before any index is read)
+        big = scenes.Scene(sc.vertices, sc.indices, np.array([[0, 1 << 27, 0], [0, 1 << 27, 0]], np.uint32),
+                           sc.materials, sc.lights, sc.environment, sc.camera, "too_many_triangles")
+        v, keep = scene_view(big)
+        assert native.load().vkptc_load_scene(t._ctx, ctypes.byref(v)) == native.INVALID_ARGUMENT
+        assert "2^28" in t._err()
         # a well-formed scene afterwards loads and builds
         assert t.load_scene_snapshot(sc) and t.build_or_update_acceleration()

@@ -1222,7 +1222,7 @@ __global__ void k_wide_write(WideArrays W, uint32_t n_wide, WideNode* __restrict
   for (int k = 0; k < 4; ++k) {
     n.lox[k] = n.loy[k] = n.loz[k] = 1.0f;
     n.hix[k] = n.hiy[k] = n.hiz[k] = -1.0f;
-    n.child[k] = 0;
+    n.child[k] = kEmptyChild;
     n.meta[k] = 0;
   }
   n.meta[0] = w.nslots;

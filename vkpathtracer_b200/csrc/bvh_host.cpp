@@ -525,7 +525,7 @@ void CollapseToWide(const SceneGeometry& geo, const std::vector<BinNode>& bin,
     for (int k = 0; k < 4; ++k) {
       wn.lox[k] = wn.loy[k] = wn.loz[k] = 1.0f;
       wn.hix[k] = wn.hiy[k] = wn.hiz[k] = -1.0f;
-      wn.child[k] = 0;
+      wn.child[k] = kEmptyChild;
     }
     wn.meta[0] = static_cast<int32_t>(slots.size());
     for (size_t s = 0; s < slots.size(); ++s) {

@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include "bvh_layout.h"
+
 namespace vkptc {
 
 struct HostPrim {
@@ -23,7 +25,8 @@ struct BinNode {
 // Wide node: six float4 of child bounds as SoA (lo.x[4], hi.x[4], lo.y[4],
 // hi.y[4], lo.z[4], hi.z[4]), then int4 child refs, then int4 meta
 // (x = valid child count).  Child ref >= 0: wide node index; < 0: leaf,
-// ~ref = (first_triangle << 3) | (count - 1).  128 bytes, one cache line.
+// ~ref = (first_triangle << 3) | (count - 1); kEmptyChild: an unused slot
+// (so the traversal needs no child count).  128 bytes, one cache line.
 struct alignas(16) WideNode {
   float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
   int32_t child[4];

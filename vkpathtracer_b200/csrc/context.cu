@@ -714,6 +714,12 @@ int32_t vkptc_load_scene(vkptc_ctx* ctx, const vkptc_scene_view* scene) {
   VKPTC_CUDA(ctx, drain(ctx), "waiting for the work queued on the context's stream");
   if (scene->instance_count > 0 && scene->instances == nullptr)
     return fail(ctx, VKPTC_INVALID_ARGUMENT, "instances pointer is null");
+  {
+    uint64_t tris = 0;   // the instances' triangle ranges bound the flattened primitives
+    for (uint32_t i = 0; i < scene->instance_count; ++i) tris += scene->instances[3 * i + 1];
+    if (tris > kMaxTriangles)
+      return fail(ctx, VKPTC_INVALID_ARGUMENT, "more than 2^28 - 8 triangles (the wide BVH's leaf references)");
+  }
   const bool dyn = scene->instance_local != nullptr && scene->instance_transforms != nullptr;
   if ((scene->instance_local != nullptr) != (scene->instance_transforms != nullptr) ||
       (dyn && ((scene->local_vertex_count && !scene->local_vertices) || (scene->local_index_count && !scene->local_indices))))

@@ -18,12 +18,14 @@
 //    (left first when the entry distances are equal), since it traverses the
 //    binary tree depth first, near child first.  tie_candidate_wins()
 //    evaluates exactly that order from the binary tree kept beside the wide one.
-// Nodes are 128-byte lines fetched as eight 128-bit loads; triangles are
+// Nodes are 128-byte lines of which the traversal loads seven 128-bit words
+// (bounds and child refs; an unused slot's ref is kEmptyChild); triangles are
 // three 128-bit loads.  The stack holds (child ref, entry distance) pairs in
 // shared memory, interleaved per thread, and is sized on the host from the
 // BVH's exact worst case so it cannot overflow.
 #pragma once
 
+#include "bvh_layout.h"
 #include "common.cuh"
 
 namespace vkptc {
@@ -347,14 +349,13 @@ __device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& 
       const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
       const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
       const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
-      const int n = __ldg(reinterpret_cast<const int*>(np + 7));
       if (kStats) ++st.nodes;
       float t[4];
       int32_t c[4] = {ch.x, ch.y, ch.z, ch.w};
       bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, best_t, t[0]);
-      bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, best_t, t[1]) && n > 1;
-      bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, best_t, t[2]) && n > 2;
-      bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, best_t, t[3]) && n > 3;
+      bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, best_t, t[1]) && c[1] != kEmptyChild;
+      bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, best_t, t[2]) && c[2] != kEmptyChild;
+      bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, best_t, t[3]) && c[3] != kEmptyChild;
       t[0] = h0 ? t[0] : kInf;
       t[1] = h1 ? t[1] : kInf;
       t[2] = h2 ? t[2] : kInf;
@@ -440,13 +441,12 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, f
       const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
       const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
       const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
-      const int n = __ldg(reinterpret_cast<const int*>(np + 7));
       if (kStats) ++st.nodes;
       float t0, t1, t2, t3;
       const bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, tmax, t0);
-      const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, tmax, t1) && n > 1;
-      const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, tmax, t2) && n > 2;
-      const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, tmax, t3) && n > 3;
+      const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, tmax, t1) && ch.y != kEmptyChild;
+      const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, tmax, t2) && ch.z != kEmptyChild;
+      const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, tmax, t3) && ch.w != kEmptyChild;
       int32_t next = 0;
       bool have = false;
       const int32_t cs[4] = {ch.x, ch.y, ch.z, ch.w};
@@ -558,14 +558,13 @@ __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk
     const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
     const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
     const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
-    const int n = __ldg(reinterpret_cast<const int*>(np + 7));
     if (kStats) ++st.nodes;
     float t[4];
     int32_t c[4] = {ch.x, ch.y, ch.z, ch.w};
     const bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, L.r, L.t, t[0]);
-    const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, L.r, L.t, t[1]) && n > 1;
-    const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, L.r, L.t, t[2]) && n > 2;
-    const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, L.r, L.t, t[3]) && n > 3;
+    const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, L.r, L.t, t[1]) && c[1] != kEmptyChild;
+    const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, L.r, L.t, t[2]) && c[2] != kEmptyChild;
+    const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, L.r, L.t, t[3]) && c[3] != kEmptyChild;
     t[0] = h0 ? t[0] : kInf;
     t[1] = h1 ? t[1] : kInf;
     t[2] = h2 ? t[2] : kInf;
@@ -688,14 +687,13 @@ __device__ __forceinline__ bool lane_step_tri(LaneState& L, const TwoLevelStack&
     const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
     const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
     const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
-    const int n = __ldg(reinterpret_cast<const int*>(np + 7));
     if (kStats) ++st.nodes;
     float t[4];
     int32_t c[4] = {ch.x, ch.y, ch.z, ch.w};
     const bool h0 = node_slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, L.r, L.t, t[0]);
-    const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, L.r, L.t, t[1]) && n > 1;
-    const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, L.r, L.t, t[2]) && n > 2;
-    const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, L.r, L.t, t[3]) && n > 3;
+    const bool h1 = node_slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, L.r, L.t, t[1]) && c[1] != kEmptyChild;
+    const bool h2 = node_slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, L.r, L.t, t[2]) && c[2] != kEmptyChild;
+    const bool h3 = node_slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, L.r, L.t, t[3]) && c[3] != kEmptyChild;
     t[0] = h0 ? t[0] : kInf;
     t[1] = h1 ? t[1] : kInf;
     t[2] = h2 ? t[2] : kInf;
