@@ -980,7 +980,15 @@ int32_t build_on_device(vkptc_ctx* c, bool* done) {
     VKPTC_CUDA(c, c->d_tris.alloc(1), "bvh alloc");
     VKPTC_CUDA(c, c->d_tie.alloc(1), "bvh alloc");
   } else {
-    c->d_nodes.adopt_pooled(out.nodes, 8ull * out.wide_nodes, c->stream);
+    if (reinterpret_cast<uintptr_t>(out.nodes) % 32u == 0u) {
+      c->d_nodes.adopt_pooled(out.nodes, 8ull * out.wide_nodes, c->stream);
+    } else {
+      // the traversal reads node bounds with 32-byte loads: move the nodes to an aligned allocation
+      VKPTC_CUDA(c, c->d_nodes.alloc(8ull * out.wide_nodes), "bvh alloc");
+      VKPTC_CUDA(c, cudaMemcpyAsync(c->d_nodes.ptr, out.nodes, 128ull * out.wide_nodes, cudaMemcpyDeviceToDevice,
+                                    c->stream), "bvh copy");
+      FreeAccelArray(out.nodes, c->stream);
+    }
     c->d_tris.adopt_pooled(out.tris, 3ull * n, c->stream);
     c->d_tie.adopt_pooled(out.tie, 2ull * out.binary_nodes, c->stream);
   }

@@ -18,9 +18,9 @@
 //    (left first when the entry distances are equal), since it traverses the
 //    binary tree depth first, near child first.  tie_candidate_wins()
 //    evaluates exactly that order from the binary tree kept beside the wide one.
-// Nodes are 128-byte lines of which the traversal loads seven 128-bit words
-// (bounds and child refs; an unused slot's ref is kEmptyChild); triangles are
-// three 128-bit loads.  The stack holds (child ref, entry distance) pairs in
+// Nodes are 128-byte lines of which the traversal loads the bounds (three
+// 256-bit loads) and the child refs (one 128-bit load; an unused slot's ref is
+// kEmptyChild); triangles are three 128-bit loads.  The stack holds (child ref, entry distance) pairs in
 // shared memory, interleaved per thread, and is sized on the host from the
 // BVH's exact worst case so it cannot overflow.
 #pragma once
@@ -123,6 +123,34 @@ __device__ __forceinline__ bool ref_slab(const float lo[3], const float hi[3], c
   }
   tnear = t_min;
   return t_max > kEps;
+}
+
+// The six bound words of a wide node.  With VKPTC_NODE_LD256 (the default)
+// three 256-bit read-only loads (ld.global.nc.v8, sm_100) instead of six
+// 128-bit ones; node records are 128-byte lines of allocations whose base the
+// host checks for 32-byte alignment.
+#ifndef VKPTC_NODE_LD256
+#define VKPTC_NODE_LD256 1
+#endif
+__device__ __forceinline__ void ldg256(const float4* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+__device__ __forceinline__ void load_node_bounds(const float4* np, float4& lx, float4& hx, float4& ly, float4& hy,
+                                                 float4& lz, float4& hz) {
+#if VKPTC_NODE_LD256
+  ldg256(np, lx, hx);
+  ldg256(np + 2, ly, hy);
+  ldg256(np + 4, lz, hz);
+#else
+  lx = __ldg(np + 0);
+  hx = __ldg(np + 1);
+  ly = __ldg(np + 2);
+  hy = __ldg(np + 3);
+  lz = __ldg(np + 4);
+  hz = __ldg(np + 5);
+#endif
 }
 
 // Fused node test of one child slot; exact parallel-axis rule.
@@ -346,8 +374,8 @@ __device__ __forceinline__ void trace_closest(const DevScene& s, const RayPrep& 
   while (true) {
     if (ref >= 0) {
       const float4* np = s.nodes + 8 * ref;
-      const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+      float4 lx, hx, ly, hy, lz, hz;
+      load_node_bounds(np, lx, hx, ly, hy, lz, hz);
       const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
       if (kStats) ++st.nodes;
       float t[4];
@@ -438,8 +466,8 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, const RayPrep& r, f
   while (true) {
     if (ref >= 0) {
       const float4* np = s.nodes + 8 * ref;
-      const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+      float4 lx, hx, ly, hy, lz, hz;
+      load_node_bounds(np, lx, hx, ly, hy, lz, hz);
       const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
       if (kStats) ++st.nodes;
       float t0, t1, t2, t3;
@@ -555,8 +583,8 @@ template <bool kAny, bool kStats, bool kWt = false>
 __device__ __forceinline__ bool lane_step(LaneState& L, const TwoLevelStack& stk, TraceStats& st, uint32_t& err) {
   if (L.ref >= 0) {
     const float4* np = L.g.nodes + 8 * L.ref;
-    const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+    float4 lx, hx, ly, hy, lz, hz;
+    load_node_bounds(np, lx, hx, ly, hy, lz, hz);
     const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
     if (kStats) ++st.nodes;
     float t[4];
@@ -684,8 +712,8 @@ __device__ __forceinline__ bool lane_step_tri(LaneState& L, const TwoLevelStack&
     if (L.tri < L.tri_end) return false;
   } else {
     const float4* np = L.g.nodes + 8 * L.ref;
-    const float4 lx = __ldg(np + 0), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+    float4 lx, hx, ly, hy, lz, hz;
+    load_node_bounds(np, lx, hx, ly, hy, lz, hz);
     const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
     if (kStats) ++st.nodes;
     float t[4];
