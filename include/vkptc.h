@@ -506,8 +506,11 @@ typedef struct vkptc_batch_tuning {
   uint32_t sample_limit;     /* render at most this many samples per job (0 = each job's spp) */
   uint32_t use_graph;        /* persistent/loop modes: 1 = capture once, replay the CUDA graph
                                 (loop mode without a graph runs one host round trip per iteration) */
-  uint32_t occupancy;        /* persistent kernel register variant: 0..3 = at least 1..4 resident
-                                256-thread blocks per SM (fewer registers, more warps) */
+  uint32_t occupancy;        /* traversal kernels' register variant: 0..3 = at least 1..4 resident
+                                256-thread blocks per SM (fewer registers, more warps); 4 (loop
+                                driver; the persistent driver takes it as 3) = at least 7 resident
+                                128-thread blocks per SM (72 registers), and the launch's block
+                                size becomes 128 */
   uint32_t barrier_spins;    /* persistent mode: bound of a grid-barrier wait in sleeps of ~128 ns
                                 (0 = 2^26, about 8.6 s); a block that waits longer aborts the run,
                                 every block leaves at its next barrier and vkptc_batch_run returns

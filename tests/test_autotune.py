@@ -67,3 +67,12 @@ def test_refinement_can_be_switched_off(tmp_path, monkeypatch):
     best = autotune.tune_batch(b, "k", modes=("persistent",), refine_samples=None, **SHAPES)
     assert all(c[1] == 1 for c in b.calls)
     assert best["block_size"] == 128 and best["refine_samples"] == 1
+
+
+def test_loop_register_variants_run_at_128_threads(tmp_path, monkeypatch):
+    monkeypatch.setenv("VKPTC_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    b = FakeBatch()
+    autotune.tune_batch(b, "k", **SHAPES)
+    v4 = [c for c in b.calls if c[6] == 4]
+    assert v4 and all(c[0] == "loop" and c[3] == 128 for c in v4)
+    assert {(c[4], c[5]) for c in v4} == {(8, 8), (16, 8)}     # every stack / steps pair

@@ -100,6 +100,19 @@ def test_tuning_does_not_change_films(batch, mode, pool, block, stack, steps):
         assert np.array_equal(ca, cb) and np.array_equal(bits(a), bits(b))
 
 
+@pytest.mark.parametrize("mode,occupancy", [("loop", o) for o in range(5)] + [("persistent", o) for o in (0, 3, 4)])
+def test_register_variants_do_not_change_films(batch, mode, occupancy):
+    # Variant 4 runs the loop driver's stages in 128-thread blocks whatever the
+    # block size asked for; the persistent driver takes it as variant 3.
+    n = len(small_jobs())
+    batch.run("plain")
+    ref = films(batch, n)
+    batch.run(mode, block_size=256, stack_depth=16, steps=8, occupancy=occupancy)
+    got = films(batch, n)
+    for (a, ca), (b, cb) in zip(ref, got):
+        assert np.array_equal(ca, cb) and np.array_equal(bits(a), bits(b))
+
+
 def test_sample_limit(batch):
     n = len(small_jobs())
     s = batch.run("persistent", sample_limit=1)

@@ -24,6 +24,10 @@ DEFAULT_BLOCKS = (128, 256)
 DEFAULT_STACKS = (8, 16)
 DEFAULT_STEPS = (8, 16)
 DEFAULT_OCCUPANCY = (1, 2, 3)
+# Register variants only the loop driver has; they run its stages in 128-thread
+# blocks (variant 4: traversal stages at 72 registers, 28 warps per SM).
+DEFAULT_LOOP_VARIANTS = (4,)
+LOOP_VARIANT_BLOCK = 128
 
 
 def cache_path() -> str:
@@ -77,14 +81,16 @@ DEFAULT_MODES = ("loop", "persistent")
 def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks=DEFAULT_BLOCKS,
                stacks=DEFAULT_STACKS, steps=DEFAULT_STEPS, occupancy=DEFAULT_OCCUPANCY, sample_limit: int = 1,
                repeats: int = 2, use_cache: bool = True, log: Optional[callable] = None,
-               refine_samples: Optional[int] = 0, refine_top: int = 1, full_modes=("loop",)) -> Dict:
+               refine_samples: Optional[int] = 0, refine_top: int = 1, full_modes=("loop",),
+               loop_variants=DEFAULT_LOOP_VARIANTS) -> Dict:
     """Returns {"mode", "pool_paths", "block_size", "stack_depth", "steps", "occupancy", "ms", "trials",
     "per_mode"}.
 
     Coordinate search per driver: the pool capacity first (other parameters
     at their defaults), then block size x stack entries x steps x register
     variant at that pool, then the pool sizes next to it with the chosen
-    shape.  Trials replay a CUDA graph (the way the runs are timed), so the
+    shape (the loop driver also tries its own register variants, loop_variants,
+    with 128-thread blocks and every stack / steps pair).  Trials replay a CUDA graph (the way the runs are timed), so the
     loop driver is measured as it runs.  Drivers in full_modes are searched on
     the whole workload (refine_samples per job; 0 = every sample): short runs
     under-fill large pools and rank close shapes only roughly (differences of
@@ -96,7 +102,7 @@ def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks
     the whole workload wins."""
     cache = _load_cache() if use_cache else {}
     ckey = (f"batch/{_gpu_name()}/{'+'.join(modes)}/r{refine_samples}t{refine_top}"
-            f"f{'+'.join(m for m in modes if m in full_modes)}/{key}")
+            f"f{'+'.join(m for m in modes if m in full_modes)}v{'+'.join(map(str, loop_variants))}/{key}")
     if use_cache and ckey in cache:
         return dict(cache[ckey], cached=True)
     trials = []
@@ -140,7 +146,11 @@ def tune_batch(batch, key: str, modes=DEFAULT_MODES, pools=DEFAULT_POOLS, blocks
         if not mine:
             continue
         pool = min(mine, key=lambda r: r[0])[1]["pool_paths"]
-        for block, stack, st, occ in itertools.product(blocks, stacks, steps, occupancy):
+        shapes = list(itertools.product(blocks, stacks, steps, occupancy))
+        if mode == "loop":
+            shapes += [(LOOP_VARIANT_BLOCK, stack, st, occ)
+                       for stack, st, occ in itertools.product(stacks, steps, loop_variants)]
+        for block, stack, st, occ in shapes:
             run({"mode": mode, "pool_paths": pool, "block_size": block, "stack_depth": stack, "steps": st,
                  "occupancy": occ})
         tried = [c for _, c in mine]

@@ -57,7 +57,8 @@ struct BatchLaunch {
   bool stats;   // count traversal work (node/leaf/triangle visits)
   bool effects; // some job has a material with a procedural effect (loop driver: shading variant)
   bool sdf;     // some job has SDF primitives (loop driver: the two SDF stages run)
-  int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM
+  int occupancy;  // register-allocation variant: 0..3 = at least 1..4 resident 256-thread blocks per SM;
+                  // 4 (loop driver only) = at least 7 resident 128-thread blocks per SM
                   // (the persistent kernel; in the loop driver, its two traversal stages)
   bool watertight;  // the jobs' triangle records hold vertices (watertight test)
   bool exotic;      // some job has a transmissive, clear-coat, sheen or toon material or an environment map

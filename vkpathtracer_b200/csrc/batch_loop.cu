@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ job
   }
 }
 
-template <bool kStats, int kMinBlocks, bool kWt>
-__global__ void __launch_bounds__(256, kMinBlocks) k_lp_extend(const DevJob* __restrict__ jobs, LoopPool P, int scap,
+template <bool kStats, int kThreads, int kMinBlocks, bool kWt>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_lp_extend(const DevJob* __restrict__ jobs, LoopPool P, int scap,
                                                                int2* spill, int total_cap, int steps, DevCounters* ctr,
                                                                uint32_t* err) {
   extern __shared__ int2 smem_stack[];
@@ -366,8 +366,8 @@ __global__ void __launch_bounds__(256, (kEffects || kSdf || kExotic) ? 3 : VKPTC
   warp_count(&ctr->shadow_tests, shadow_tests);
 }
 
-template <bool kStats, int kMinBlocks, bool kWt>
-__global__ void __launch_bounds__(256, kMinBlocks) k_lp_shadow(const DevJob* __restrict__ jobs, LoopPool P, int scap,
+template <bool kStats, int kThreads, int kMinBlocks, bool kWt>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_lp_shadow(const DevJob* __restrict__ jobs, LoopPool P, int scap,
                                                                int2* spill, int total_cap, int steps, DevCounters* ctr,
                                                                uint32_t* err) {
   extern __shared__ int2 smem_stack[];
@@ -432,33 +432,35 @@ cudaError_t set_smem_attr(K kernel, int bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-// Traversal stage variants: [triangle test][stats][register variant] (at
-// least 1..4 resident 256-thread blocks per SM; stats runs use the
-// unconstrained one).
+// Traversal stage variants: [triangle test][stats][register variant].
+// Variants 0..3: at least 1..4 resident 256-thread blocks per SM (at most
+// 255, 128, 80 and 64 registers); variant 4: at least 7 resident 128-thread
+// blocks (at most 72 registers, 28 warps; launched with 128 threads only).  Stats runs use
+// the unconstrained variant at the launch's block size.
 using LoopTraceFn = void (*)(const DevJob*, LoopPool, int, int2*, int, int, DevCounters*, uint32_t*);
 LoopTraceFn extend_fn(bool stats, int occ, bool wt) {
-  static const LoopTraceFn t[2][2][4] = {
-      {{k_lp_extend<false, 1, false>, k_lp_extend<false, 2, false>, k_lp_extend<false, 3, false>,
-        k_lp_extend<false, 4, false>},
-       {k_lp_extend<true, 1, false>, k_lp_extend<true, 1, false>, k_lp_extend<true, 1, false>,
-        k_lp_extend<true, 1, false>}},
-      {{k_lp_extend<false, 1, true>, k_lp_extend<false, 2, true>, k_lp_extend<false, 3, true>,
-        k_lp_extend<false, 4, true>},
-       {k_lp_extend<true, 1, true>, k_lp_extend<true, 1, true>, k_lp_extend<true, 1, true>,
-        k_lp_extend<true, 1, true>}}};
-  return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+  static const LoopTraceFn t[2][2][5] = {
+      {{k_lp_extend<false, 256, 1, false>, k_lp_extend<false, 256, 2, false>, k_lp_extend<false, 256, 3, false>,
+        k_lp_extend<false, 256, 4, false>, k_lp_extend<false, 128, 7, false>},
+       {k_lp_extend<true, 256, 1, false>, k_lp_extend<true, 256, 1, false>, k_lp_extend<true, 256, 1, false>,
+        k_lp_extend<true, 256, 1, false>, k_lp_extend<true, 128, 1, false>}},
+      {{k_lp_extend<false, 256, 1, true>, k_lp_extend<false, 256, 2, true>, k_lp_extend<false, 256, 3, true>,
+        k_lp_extend<false, 256, 4, true>, k_lp_extend<false, 128, 7, true>},
+       {k_lp_extend<true, 256, 1, true>, k_lp_extend<true, 256, 1, true>, k_lp_extend<true, 256, 1, true>,
+        k_lp_extend<true, 256, 1, true>, k_lp_extend<true, 128, 1, true>}}};
+  return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 4 ? 4 : occ)];
 }
 LoopTraceFn shadow_fn(bool stats, int occ, bool wt) {
-  static const LoopTraceFn t[2][2][4] = {
-      {{k_lp_shadow<false, 1, false>, k_lp_shadow<false, 2, false>, k_lp_shadow<false, 3, false>,
-        k_lp_shadow<false, 4, false>},
-       {k_lp_shadow<true, 1, false>, k_lp_shadow<true, 1, false>, k_lp_shadow<true, 1, false>,
-        k_lp_shadow<true, 1, false>}},
-      {{k_lp_shadow<false, 1, true>, k_lp_shadow<false, 2, true>, k_lp_shadow<false, 3, true>,
-        k_lp_shadow<false, 4, true>},
-       {k_lp_shadow<true, 1, true>, k_lp_shadow<true, 1, true>, k_lp_shadow<true, 1, true>,
-        k_lp_shadow<true, 1, true>}}};
-  return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 3 ? 3 : occ)];
+  static const LoopTraceFn t[2][2][5] = {
+      {{k_lp_shadow<false, 256, 1, false>, k_lp_shadow<false, 256, 2, false>, k_lp_shadow<false, 256, 3, false>,
+        k_lp_shadow<false, 256, 4, false>, k_lp_shadow<false, 128, 7, false>},
+       {k_lp_shadow<true, 256, 1, false>, k_lp_shadow<true, 256, 1, false>, k_lp_shadow<true, 256, 1, false>,
+        k_lp_shadow<true, 256, 1, false>, k_lp_shadow<true, 128, 1, false>}},
+      {{k_lp_shadow<false, 256, 1, true>, k_lp_shadow<false, 256, 2, true>, k_lp_shadow<false, 256, 3, true>,
+        k_lp_shadow<false, 256, 4, true>, k_lp_shadow<false, 128, 7, true>},
+       {k_lp_shadow<true, 256, 1, true>, k_lp_shadow<true, 256, 1, true>, k_lp_shadow<true, 256, 1, true>,
+        k_lp_shadow<true, 256, 1, true>, k_lp_shadow<true, 128, 1, true>}}};
+  return t[wt ? 1 : 0][stats ? 1 : 0][occ < 0 ? 0 : (occ > 4 ? 4 : occ)];
 }
 
 // Shading stage variants: [parity][effects][sdf][exotic].
@@ -493,7 +495,7 @@ cudaError_t ConfigureBatchLoopSmem(size_t bytes) {
   cudaError_t e = cudaSuccess;
   for (int wt = 0; wt < 2 && e == cudaSuccess; ++wt)
     for (int st = 0; st < 2 && e == cudaSuccess; ++st)
-      for (int o = 0; o < 4 && e == cudaSuccess; ++o) {
+      for (int o = 0; o < 5 && e == cudaSuccess; ++o) {
         e = set_smem_attr(extend_fn(st != 0, o, wt != 0), b);
         if (e == cudaSuccess) e = set_smem_attr(shadow_fn(st != 0, o, wt != 0), b);
       }

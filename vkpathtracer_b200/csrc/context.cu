@@ -1956,7 +1956,10 @@ int32_t batch_run_pool(vkptc_batch* b, const vkptc_batch_tuning& t, uint32_t mod
     bl.sdf = bl.sdf || c->sdf_count != 0u;
     bl.exotic = bl.exotic || c->has_exotic || c->env_w != 0u;
   }
-  bl.occupancy = static_cast<int>(std::min(3u, t.occupancy));
+  // Register variant of the traversal kernels: 0..3 for both drivers; the loop
+  // driver's variant 4 runs its stages in 128-thread blocks.
+  bl.occupancy = static_cast<int>(std::min(loop ? 4u : 3u, t.occupancy));
+  if (loop && bl.occupancy == 4) bl.block = 128;
   const size_t smem = StackSmemBytes(bl.block, bl.smem_entries);
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
