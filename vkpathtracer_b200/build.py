@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libvkpt_cuda.so")
-SOURCES = ["kernels.cu", "trace_rays.cu", "batch.cu", "batch_loop.cu", "adjoint.cu", "context.cu", "bvh_build.cu", "bvh_host.cpp"]
+SOURCES = ["kernels.cu", "batch.cu", "batch_loop.cu", "adjoint.cu", "context.cu", "bvh_build.cu", "bvh_host.cpp"]
 HEADERS = ["bvh_layout.h", "common.cuh", "traverse.cuh", "kernels.cuh", "integrator.cuh", "batch.cuh", "bvh_host.h", "adjoint.cuh",
            "adjoint_launch.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

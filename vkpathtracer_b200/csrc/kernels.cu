@@ -34,6 +34,27 @@ size_t SpillEntries(const LaunchShape& ls) {
 
 // ============================================================ query sources
 // Each source supplies queries to persistent_traverse() and consumes results.
+struct RaysSource {   // batched ray queries from a ray array
+  GeoView geo;
+  const float* rays;
+  const float* tmax;
+  uint32_t* prim_out;
+  float* t_out;
+  bool any;
+  __device__ __forceinline__ void load(uint32_t j, V3& o, V3& d, float& tm, GeoView& g) const {
+    g = geo;
+    const float2* rp = reinterpret_cast<const float2*>(rays + 6ull * j);
+    const float2 a = __ldg(rp), b = __ldg(rp + 1), c = __ldg(rp + 2);
+    o = mk(a.x, a.y, b.x);
+    d = mk(b.y, c.x, c.y);
+    tm = tmax ? __ldg(tmax + j) : kInf;
+  }
+  __device__ __forceinline__ void finish(uint32_t j, float t, uint32_t prim) const {
+    prim_out[j] = prim;
+    if (t_out) t_out[j] = any ? (prim ? 0.0f : kInf) : t;
+  }
+};
+
 struct ExtendSource {  // closest hit for the queued paths of a wave
   GeoView geo;
   const uint32_t* q;
@@ -79,6 +100,61 @@ struct ShadowSource {  // any hit for the NEE queries; adds the term when visibl
   }
 };
 
+template <class Src, bool kAny, bool kStats, bool kWt = false>
+__device__ __forceinline__ void run_persistent(const Src& src, uint32_t n, uint32_t* fetch,
+                                               int scap, int2* spill, int total, int steps,
+                                               unsigned long long* c_nodes, unsigned long long* c_leaves,
+                                               unsigned long long* c_tris, unsigned long long* c_rays, uint32_t* err) {
+  extern __shared__ int2 smem_stack[];
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gstride = static_cast<int>(gridDim.x * blockDim.x);
+  TwoLevelStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), scap,
+                    spill ? spill + gtid : nullptr, gstride, total};
+  TraceStats st;
+  uint32_t lerr = 0u;
+  persistent_traverse<Src, kAny, kStats, kWt>(src, n, fetch, stk, steps, st, lerr);
+  if (kStats) {
+    warp_count(c_nodes, st.nodes);
+    warp_count(c_leaves, st.leaves);
+    warp_count(c_tris, st.tris);
+    warp_count(c_rays, st.rays);
+  }
+  if (lerr) atomicOr(err, lerr);
+}
+
+// =============================================================== ray queries
+template <bool kAny, bool kStats, bool kWt>
+__global__ void __launch_bounds__(256) k_trace_rays(DevScene s, RaysSource src, uint32_t n, uint32_t* fetch, int scap,
+                                                    int2* spill, int total, int steps, DevCounters* ctr, uint32_t* err) {
+  run_persistent<RaysSource, kAny, kStats, kWt>(src, n, fetch, scap, spill, total, steps, &ctr->nodes, &ctr->leaves,
+                                                &ctr->tris, &ctr->ext_rays, err);
+}
+
+cudaError_t LaunchTraceRays(const DevScene& s, const float* rays, const float* tmax, uint64_t n, bool any_hit,
+                            uint32_t* prim_out, float* t_out, const LaunchShape& ls, DevCounters* ctr,
+                            uint32_t* err, uint32_t* fetch) {
+  if (n == 0) return cudaSuccess;
+  const size_t smem = StackSmemBytes(ls.block, ls.smem_entries);
+  cudaError_t e = cudaMemsetAsync(fetch, 0, sizeof(uint32_t), ls.stream);
+  if (e != cudaSuccess) return e;
+  const RaysSource src{geo_of(s), rays, tmax, prim_out, t_out, any_hit};
+  const uint32_t n32 = static_cast<uint32_t>(n);
+#define VKPTC_TR(A, S, W) \
+  k_trace_rays<A, S, W><<<ls.grid, ls.block, smem, ls.stream>>>(s, src, n32, fetch, ls.smem_entries, ls.spill, ls.stack_cap, ls.steps, ctr, err)
+#define VKPTC_TR2(A, S) \
+  if (s.watertight) VKPTC_TR(A, S, true); \
+  else VKPTC_TR(A, S, false)
+  if (any_hit) {
+    if (ctr) VKPTC_TR2(true, true);
+    else VKPTC_TR2(true, false);
+  } else {
+    if (ctr) VKPTC_TR2(false, true);
+    else VKPTC_TR2(false, false);
+  }
+#undef VKPTC_TR2
+#undef VKPTC_TR
+  return cudaGetLastError();
+}
 
 // ==================================================================== raygen
 template <bool kParity>
@@ -529,6 +605,10 @@ cudaError_t ConfigureStackSmem(size_t bytes) {
   cudaError_t e = cudaSuccess;
   const auto all = [&](auto wt) {
     constexpr bool W = decltype(wt)::value;
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<true, true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<true, false, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<false, true, W>, b);
+    if (e == cudaSuccess) e = set_smem(k_trace_rays<false, false, W>, b);
     if (e == cudaSuccess) e = set_smem(k_extend<true, W>, b);
     if (e == cudaSuccess) e = set_smem(k_extend<false, W>, b);
     if (e == cudaSuccess) e = set_smem(k_shadow<true, W>, b);
@@ -538,7 +618,6 @@ cudaError_t ConfigureStackSmem(size_t bytes) {
   };
   all(std::false_type{});
   all(std::true_type{});
-  if (e == cudaSuccess) e = ConfigureTraceRaysSmem(bytes);
   return e;
 }
 

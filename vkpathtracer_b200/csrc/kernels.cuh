@@ -67,8 +67,6 @@ size_t SpillEntries(const LaunchShape& ls);
 int ExtendBlocksPerSm(int block, size_t smem, bool watertight = false);
 // Raises the dynamic shared-memory limit of every stack-using kernel.
 cudaError_t ConfigureStackSmem(size_t bytes);
-// Dynamic shared-memory limit of the ray-query kernels (trace_rays.cu); part of ConfigureStackSmem.
-cudaError_t ConfigureTraceRaysSmem(size_t bytes);
 
 // Ray queries over one scene (rays: 6 floats each).
 // `fetch` is a device counter the persistent kernel claims query ids from.

@@ -43,23 +43,6 @@ namespace vkptc {
 #define VKPTC_LANE_STEP lane_step<kAny, kStats, kWt>
 #endif
 
-// 1/x rounded to nearest: __frcp_rn and __fdiv_rn(1.0f, x) are both the
-// correctly rounded reciprocal, so they return the same bits; which sequence
-// runs faster depends on the kernel around it.  VKPTC_RCP_RAY selects
-// __frcp_rn for the per-ray reciprocal direction, VKPTC_RCP_TRI for the
-// per-triangle 1/det of the leaf test.
-#ifndef VKPTC_RCP_RAY
-#define VKPTC_RCP_RAY 0
-#endif
-#ifndef VKPTC_RCP_TRI
-#define VKPTC_RCP_TRI 0
-#endif
-template <bool kRcp>
-__device__ __forceinline__ float recip_rn(float x) {
-  if constexpr (kRcp) return __frcp_rn(x);
-  else return __fdiv_rn(1.0f, x);
-}
-
 struct RayPrep {
   float ox, oy, oz, dx, dy, dz;
   float ix, iy, iz;      // 1/d (0 on axes the node test treats with the inside rule)
@@ -95,9 +78,9 @@ __device__ __forceinline__ RayPrep prep_ray(V3 o, V3 d, bool reference_tree = tr
     r.node_par = (fabsf(d.x) < 1e-20f ? 1u : 0u) | (fabsf(d.y) < 1e-20f ? 2u : 0u) | (fabsf(d.z) < 1e-20f ? 4u : 0u);
     r.leaf_par = r.par;
   }
-  r.ix = (r.node_par & 1u) ? 0.0f : recip_rn<VKPTC_RCP_RAY>(d.x);
-  r.iy = (r.node_par & 2u) ? 0.0f : recip_rn<VKPTC_RCP_RAY>(d.y);
-  r.iz = (r.node_par & 4u) ? 0.0f : recip_rn<VKPTC_RCP_RAY>(d.z);
+  r.ix = (r.node_par & 1u) ? 0.0f : __fdiv_rn(1.0f, d.x);
+  r.iy = (r.node_par & 2u) ? 0.0f : __fdiv_rn(1.0f, d.y);
+  r.iz = (r.node_par & 4u) ? 0.0f : __fdiv_rn(1.0f, d.z);
   r.nix = -(o.x * r.ix);
   r.niy = -(o.y * r.iy);
   r.niz = -(o.z * r.iz);
@@ -212,7 +195,7 @@ __device__ __forceinline__ float mt_test(const float4 a, const float4 b, const f
   const float hz = __fsub_rn(__fmul_rn(r.dx, e2y), __fmul_rn(r.dy, e2x));
   const float det = __fadd_rn(__fadd_rn(__fmul_rn(e1x, hx), __fmul_rn(e1y, hy)), __fmul_rn(e1z, hz));
   if (fabsf(det) < kEps) return -1.0f;
-  const float inv = recip_rn<VKPTC_RCP_TRI>(det);
+  const float inv = __fdiv_rn(1.0f, det);
   const float sx = __fsub_rn(r.ox, v0x), sy = __fsub_rn(r.oy, v0y), sz = __fsub_rn(r.oz, v0z);
   const float u = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(sx, hx), __fmul_rn(sy, hy)), __fmul_rn(sz, hz)), inv);
   if (u < 0.0f || u > 1.0f) return -1.0f;
@@ -260,7 +243,7 @@ __device__ __forceinline__ WtRay prep_wt(const RayPrep& r) {
   w.kz = kz;
   w.sx = __fdiv_rn(axis_of(r.dx, r.dy, r.dz, kx), dz);
   w.sy = __fdiv_rn(axis_of(r.dx, r.dy, r.dz, ky), dz);
-  w.sz = recip_rn<VKPTC_RCP_RAY>(dz);
+  w.sz = __fdiv_rn(1.0f, dz);
   return w;
 }
 
@@ -845,31 +828,6 @@ __device__ __forceinline__ void persistent_traverse(const Src& src, uint32_t n, 
       }
     }
   }
-}
-
-// A persistent traversal kernel's body: the two-level stack of this thread
-// (shared-memory entries in the dynamic shared memory, the rest in `spill`),
-// the traversal, then the counters (stats runs) and the error word.
-template <class Src, bool kAny, bool kStats, bool kWt = false>
-__device__ __forceinline__ void run_persistent(const Src& src, uint32_t n, uint32_t* fetch,
-                                               int scap, int2* spill, int total, int steps,
-                                               unsigned long long* c_nodes, unsigned long long* c_leaves,
-                                               unsigned long long* c_tris, unsigned long long* c_rays, uint32_t* err) {
-  extern __shared__ int2 smem_stack[];
-  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int gstride = static_cast<int>(gridDim.x * blockDim.x);
-  TwoLevelStack stk{smem_stack + threadIdx.x, static_cast<int>(blockDim.x), scap,
-                    spill ? spill + gtid : nullptr, gstride, total};
-  TraceStats st;
-  uint32_t lerr = 0u;
-  persistent_traverse<Src, kAny, kStats, kWt>(src, n, fetch, stk, steps, st, lerr);
-  if (kStats) {
-    warp_count(c_nodes, st.nodes);
-    warp_count(c_leaves, st.leaves);
-    warp_count(c_tris, st.tris);
-    warp_count(c_rays, st.rays);
-  }
-  if (lerr) atomicOr(err, lerr);
 }
 
 }  // namespace vkptc
