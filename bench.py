@@ -41,9 +41,9 @@ WORKLOAD = "batch_64_uneven_jobs"
 NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 128, 48, 32   # wide node line, triangle record, ray in + hit out
 PATH_STATE_BYTES = 2 * 64                            # path state read + written per segment
 # DRAM bytes (read + write) per extension ray of k_lp_extend, from one ncu
-# capture of a steady-state launch of the 4-job case (102.40 MB read + 9.86 MB
+# capture of a steady-state launch of the 4-job case (102.30 MB read + 8.86 MB
 # written for a launch of 2,097,152 rays).
-TRAFFIC_BYTES_PER_EXT_RAY = (102397952 + 9857280) / 2097152
+TRAFFIC_BYTES_PER_EXT_RAY = (102304512 + 8858880) / 2097152
 
 
 def l2_roofline(device, achieved_gbs):
