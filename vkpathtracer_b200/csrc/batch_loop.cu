@@ -206,6 +206,11 @@ __device__ __forceinline__ uint32_t tile_order_pixel(uint32_t i, uint32_t W, uin
   return y * W + x;
 }
 
+// 1: REGEN claims work items and queue slots once per block and iteration;
+// 0: once per warp (ballot + shuffle).
+#ifndef VKPTC_REGEN_BLOCK
+#define VKPTC_REGEN_BLOCK 1
+#endif
 template <bool kParity>
 __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ jobs, uint32_t job_count,
                                                   unsigned long long total, LoopPool P) {
@@ -221,10 +226,33 @@ __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ job
   const PathSoA A = P.gen[cur];
   unsigned long long* work_next = reinterpret_cast<unsigned long long*>(P.ctl + kLWork);
   const uint32_t gthreads = gridDim.x * blockDim.x;
+#if VKPTC_REGEN_BLOCK
+  // One claim per block and iteration: the threads that take a path are a
+  // prefix of the block (j < room, and g < total with g rising with the
+  // thread index), so the leader claims the block's work items and queue
+  // slots with one atomic each and thread t takes item g0 + t, slot q0 + t.
+  __shared__ unsigned long long s_g0;
+  __shared__ uint32_t s_q0, s_k;
+#else
   const unsigned lane = threadIdx.x & 31u;
+#endif
   for (uint32_t base = blockIdx.x * blockDim.x; base < room; base += gthreads) {
-    const uint32_t j = base + threadIdx.x;
-    const bool want = j < room;
+#if VKPTC_REGEN_BLOCK
+    if (threadIdx.x == 0u) {
+      const uint32_t cnt = min(blockDim.x, room - base);
+      const unsigned long long g0 = atomicAdd(work_next, static_cast<unsigned long long>(cnt));
+      const uint32_t k = g0 >= total ? 0u : static_cast<uint32_t>(min(static_cast<unsigned long long>(cnt), total - g0));
+      s_g0 = g0;
+      s_k = k;
+      s_q0 = k ? atomicAdd(count, k) : 0u;
+    }
+    __syncthreads();
+    const unsigned long long g = s_g0 + threadIdx.x;
+    const bool ok = threadIdx.x < s_k;
+    const uint32_t q = s_q0 + threadIdx.x;
+    __syncthreads();   // the leader rewrites the shared words in the next iteration
+#else
+    const bool want = base + threadIdx.x < room;
     const unsigned mask = __ballot_sync(0xffffffffu, want);
     unsigned long long g0 = 0ull;
     const int lead = __ffs(mask) - 1;
@@ -233,6 +261,7 @@ __global__ void __launch_bounds__(256) k_lp_regen(const DevJob* __restrict__ job
     const unsigned long long g = g0 + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u)));
     const bool ok = want && g < total;
     const uint32_t q = warp_append(count, ok);
+#endif
     if (ok) {
       const uint32_t jb = find_job(jobs, job_count, g);
       const DevJob& J = jobs[jb];
